@@ -1,0 +1,156 @@
+"""Seeded synthetic protein workloads with the shapes of the benchmark
+configurations: log-normal lengths, i.i.d. residues from the Robinson
+background, and planted homologs mutated by BLOSUM62-conditional
+substitution to 30-90 % identity with geometric indels.
+
+A database is the reference's concatenated chunk layout
+``[delim s0 delim s1 ... delim]`` with ``offsets[i]`` = first residue of
+sequence i (src/database_chunk.h:282-300).  Queries use the protein-query
+framing ``[delim residues delim]`` (src/protein_query.cpp:39-49) and are
+concatenated sharing delimiters, ``offsets[i]`` = leading delimiter of query
+i (src/aligner_gpu.cpp:213-242).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import params as P
+
+
+@dataclass
+class Database:
+    codes: np.ndarray            # uint8, concatenated with delimiters
+    offsets: np.ndarray          # uint32, number_sequences + 1
+    number_sequences: int
+
+    @property
+    def length(self) -> int:
+        return int(self.codes.shape[0])
+
+
+@dataclass
+class Queries:
+    codes: np.ndarray            # uint8, concatenated, shared delimiters
+    offsets: np.ndarray          # uint32, leading delimiter of each query
+    lengths: np.ndarray          # uint32, residues + 2
+    cutoffs: np.ndarray          # int32 ungapped X-drop per query
+    triggers: np.ndarray         # int32 gapped-extension trigger per query
+    sources: np.ndarray = field(default=None)  # planted homolog source or -1
+
+    @property
+    def number(self) -> int:
+        return int(self.offsets.shape[0])
+
+
+def _background_probs():
+    f = np.zeros(len(P.REGULAR))
+    for ch, v in P.ROBINSON.items():
+        f[P.REGULAR.index(ch)] = v
+    return f / f.sum()
+
+
+def lognormal_lengths(rng, n, median, sigma, lo, hi):
+    x = rng.lognormal(mean=np.log(median), sigma=sigma, size=n)
+    return np.clip(np.rint(x), lo, hi).astype(np.int64)
+
+
+def random_residues(rng, n):
+    return rng.choice(len(P.REGULAR), size=n, p=_background_probs()).astype(np.uint8)
+
+
+def make_database(n_sequences, seed, median=300, sigma=0.6, lo=30, hi=3000):
+    rng = np.random.default_rng(seed)
+    lens = lognormal_lengths(rng, n_sequences, median, sigma, lo, hi)
+    total = int(lens.sum()) + n_sequences + 1
+    codes = np.empty(total, dtype=np.uint8)
+    offsets = np.empty(n_sequences + 1, dtype=np.uint32)
+    starts = np.concatenate([[1], 1 + np.cumsum(lens + 1)[:-1]]).astype(np.int64)
+    offsets[:-1] = starts
+    offsets[-1] = total
+    body = random_residues(rng, int(lens.sum()))
+    # scatter residues around the delimiters
+    codes[:] = P.DELIMITER
+    idx = np.repeat(starts, lens) + (np.arange(int(lens.sum())) -
+                                     np.repeat(np.cumsum(lens) - lens, lens))
+    codes[idx] = body
+    return Database(codes=codes, offsets=offsets, number_sequences=n_sequences)
+
+
+def _substitution_table(lam=0.3176):
+    m = P.blosum62()[:20, :20].astype(np.float64)
+    bg = _background_probs()
+    t = bg[None, :] * np.exp(lam * m)
+    np.fill_diagonal(t, 0.0)
+    return t / t.sum(axis=1, keepdims=True)
+
+
+def mutate(rng, seq, identity, indel_p=0.02, indel_mean=3.0):
+    """BLOSUM62-conditional substitutions at rate 1-identity, plus
+    insertions/deletions at indel_p per site with geometric lengths."""
+    table = _substitution_table()
+    seq = seq.copy()
+    sub = rng.random(len(seq)) < (1.0 - identity)
+    for i in np.nonzero(sub)[0]:
+        seq[i] = rng.choice(20, p=table[seq[i]])
+    out = []
+    i = 0
+    n = len(seq)
+    while i < n:
+        if rng.random() < indel_p:
+            k = int(rng.geometric(1.0 / indel_mean))
+            if rng.random() < 0.5:
+                out.append(random_residues(rng, k))
+            else:
+                i += k
+                continue
+        out.append(seq[i:i + 1])
+        i += 1
+    return np.concatenate(out) if out else seq[:1]
+
+
+def make_queries(db: Database, n_queries, seed, homolog_fraction=0.3,
+                 median=300, sigma=0.6, lo=30, hi=3000, cutoffs=None):
+    rng = np.random.default_rng(seed)
+    lens = lognormal_lengths(rng, n_queries, median, sigma, lo, hi)
+    seqs = []
+    sources = np.full(n_queries, -1, dtype=np.int64)
+    for i in range(n_queries):
+        if rng.random() < homolog_fraction:
+            s = int(rng.integers(db.number_sequences))
+            a, b = int(db.offsets[s]), int(db.offsets[s + 1]) - 1
+            src = db.codes[a:b]
+            ident = rng.uniform(0.3, 0.9)
+            seqs.append(mutate(rng, src, ident))
+            sources[i] = s
+        else:
+            seqs.append(random_residues(rng, int(lens[i])))
+    return pack_queries(seqs, sources=sources, cutoffs=cutoffs)
+
+
+def pack_queries(seqs, sources=None, cutoffs=None) -> Queries:
+    n = len(seqs)
+    lengths = np.array([len(s) + 2 for s in seqs], dtype=np.uint32)
+    total = int((lengths - 1).sum()) + 1
+    codes = np.empty(total, dtype=np.uint8)
+    offsets = np.empty(n, dtype=np.uint32)
+    off = 0
+    for i, s in enumerate(seqs):
+        offsets[i] = off
+        codes[off] = P.DELIMITER
+        codes[off + 1: off + 1 + len(s)] = s
+        off += len(s) + 1
+    codes[off] = P.DELIMITER
+    if cutoffs is None:
+        cut, trig = P.query_cutoffs(seqs)
+    else:
+        cut, trig = cutoffs
+    return Queries(codes=codes, offsets=offsets, lengths=lengths, cutoffs=cut,
+                   triggers=trig,
+                   sources=sources if sources is not None else np.full(n, -1))
+
+
+def query_sequences(q: Queries):
+    """Residue arrays (no delimiters) of every query."""
+    return [q.codes[int(o) + 1:int(o) + int(l) - 1] for o, l in zip(q.offsets, q.lengths)]

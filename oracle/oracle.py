@@ -1,0 +1,330 @@
+"""ctypes bindings of the CPU oracle (test infrastructure only).
+
+``Oracle`` wraps liboracle.so (the C restatement in gz_oracle.c);
+``Reference`` wraps _ref/libgzref.so (the reference's own units, present only
+where it was built from the reference checkout).  Used by the tests, the
+smoke check and the CPU-baseline leg of the benchmark, never by the engine.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libgzref.so")
+
+u8p = C.POINTER(C.c_uint8)
+u32p = C.POINTER(C.c_uint32)
+i32p = C.POINTER(C.c_int32)
+
+RESULT_DTYPE = np.dtype([
+    ("chunk_id", "<i4"), ("subject_id", "<i4"), ("score", "<i4"),
+    ("hit_q", "<u4"), ("hit_d", "<u4"), ("start_q", "<u4"), ("start_d", "<u4"),
+    ("end_q", "<u4"), ("end_d", "<u4"),
+])
+COUNTER_NAMES = ("distance_seeds", "ungapped_seeds", "ungapped_hits",
+                 "chained_hits", "gapped_extensions", "gapped_cells")
+
+
+def build(ref: bool = False) -> None:
+    subprocess.check_call(["make", "-s", "-C", HERE, "oracle"])
+    if ref and os.path.isdir("/root/reference/src"):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def _pp(params):
+    return C.c_void_p(params.__array_interface__["data"][0]) if hasattr(params, "__array_interface__") else C.c_void_p(np.asarray(params).ctypes.data)
+
+
+class _Params:
+    """Keeps a contiguous copy of a PARAMS_DTYPE record alive."""
+
+    def __init__(self, p):
+        self.arr = np.array([p], dtype=p.dtype)
+
+    @property
+    def ptr(self):
+        return C.c_void_p(self.arr.ctypes.data)
+
+
+class Oracle:
+    def __init__(self, path: str = LIB):
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        self.L = L
+        L.gzo_hash.argtypes = [C.c_void_p, u8p, u32p, u32p]
+        L.gzo_distance.argtypes = [C.c_void_p, u8p, C.c_uint32, u8p, C.c_uint32]
+        L.gzo_ungapped_one_side.argtypes = [C.c_void_p, u8p, u8p, C.c_int, C.c_int]
+        L.gzo_ungapped_with_trigger.argtypes = [C.c_void_p, u8p, C.c_uint32, u8p,
+                                                C.c_uint32, C.c_int, C.c_int]
+        L.gzo_gapped_one_side.argtypes = [C.c_void_p, u8p, u8p, C.c_int, C.c_int,
+                                          i32p, i32p, i32p, C.POINTER(C.c_uint64)]
+        L.gzo_chain_filter.argtypes = [C.c_void_p, u8p, C.c_uint32, C.c_int, u8p,
+                                       u32p, u32p, C.c_size_t]
+        L.gzo_chain_filter.restype = C.c_size_t
+        L.gzo_db_index_build.argtypes = [C.c_void_p, u8p, C.c_uint32]
+        L.gzo_db_index_build.restype = C.c_void_p
+        L.gzo_db_index_free.argtypes = [C.c_void_p]
+        L.gzo_db_index_array.argtypes = [C.c_void_p, C.c_int, C.POINTER(u32p)]
+        L.gzo_db_index_array.restype = C.c_size_t
+        L.gzo_query_lists_build.argtypes = [C.c_void_p, u8p, u32p, u32p, C.c_uint32]
+        L.gzo_query_lists_build.restype = C.c_void_p
+        L.gzo_query_lists_free.argtypes = [C.c_void_p]
+        L.gzo_query_lists_array.argtypes = [C.c_void_p, C.c_int, C.POINTER(u32p)]
+        L.gzo_query_lists_array.restype = C.c_size_t
+        L.gzo_presearch_run.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, u8p, u32p,
+                                        u32p, C.c_uint32, i32p, i32p, u8p, C.c_uint32,
+                                        u32p, C.c_uint32, C.c_uint32, C.c_uint32]
+        L.gzo_presearch_run.restype = C.c_void_p
+        L.gzo_presearch_free.argtypes = [C.c_void_p]
+        L.gzo_presearch_results.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]
+        L.gzo_presearch_results.restype = C.c_size_t
+        L.gzo_presearch_counters.argtypes = [C.c_void_p, C.POINTER(C.c_uint64 * 6)]
+        L.gzo_presearch_hits.argtypes = [C.c_void_p, C.POINTER(u32p), C.POINTER(u32p),
+                                         C.POINTER(u32p)]
+        L.gzo_presearch_hits.restype = C.c_size_t
+
+    # -- primitives ---------------------------------------------------------
+    def hash(self, params, seq, pos=0):
+        pr = _Params(params)
+        seq = np.ascontiguousarray(seq, dtype=np.uint8)
+        h = C.c_uint32()
+        ln = C.c_uint32()
+        r = self.L.gzo_hash(pr.ptr, C.cast(C.c_void_p(seq.ctypes.data + pos), u8p),
+                            C.byref(h), C.byref(ln))
+        return r, h.value, ln.value
+
+    def distance(self, params, seq0, c0, seq1, c1):
+        pr = _Params(params)
+        s0 = np.ascontiguousarray(seq0, dtype=np.uint8)
+        s1 = np.ascontiguousarray(seq1, dtype=np.uint8)
+        return self.L.gzo_distance(pr.ptr, _p(s0, u8p), c0, _p(s1, u8p), c1)
+
+    def ungapped_one_side(self, params, seq0, p0, seq1, p1, reversed_, cutoff):
+        pr = _Params(params)
+        s0 = np.ascontiguousarray(seq0, dtype=np.uint8)
+        s1 = np.ascontiguousarray(seq1, dtype=np.uint8)
+        return self.L.gzo_ungapped_one_side(
+            pr.ptr, C.cast(C.c_void_p(s0.ctypes.data + p0), u8p),
+            C.cast(C.c_void_p(s1.ctypes.data + p1), u8p), int(reversed_), int(cutoff))
+
+    def ungapped_with_trigger(self, params, query, qpos, db, dpos, cutoff, trigger):
+        pr = _Params(params)
+        q = np.ascontiguousarray(query, dtype=np.uint8)
+        d = np.ascontiguousarray(db, dtype=np.uint8)
+        return self.L.gzo_ungapped_with_trigger(pr.ptr, _p(q, u8p), qpos, _p(d, u8p),
+                                                dpos, int(cutoff), int(trigger))
+
+    def gapped_one_side(self, params, seq0, p0, seq1, p1, reversed_, cutoff):
+        pr = _Params(params)
+        s0 = np.ascontiguousarray(seq0, dtype=np.uint8)
+        s1 = np.ascontiguousarray(seq1, dtype=np.uint8)
+        b, q, d = C.c_int32(), C.c_int32(), C.c_int32()
+        cells = C.c_uint64()
+        self.L.gzo_gapped_one_side(
+            pr.ptr, C.cast(C.c_void_p(s0.ctypes.data + p0), u8p),
+            C.cast(C.c_void_p(s1.ctypes.data + p1), u8p), int(reversed_), int(cutoff),
+            C.byref(b), C.byref(q), C.byref(d), C.byref(cells))
+        return b.value, q.value, d.value, cells.value
+
+    def chain_filter(self, params, query, qlen, cutoff, db, hq, hd):
+        pr = _Params(params)
+        q = np.ascontiguousarray(query, dtype=np.uint8)
+        d = np.ascontiguousarray(db, dtype=np.uint8)
+        hq = np.array(hq, dtype=np.uint32)
+        hd = np.array(hd, dtype=np.uint32)
+        n = self.L.gzo_chain_filter(pr.ptr, _p(q, u8p), qlen, int(cutoff), _p(d, u8p),
+                                    _p(hq, u32p), _p(hd, u32p), len(hq))
+        return hq[:n].copy(), hd[:n].copy()
+
+    # -- index / lists --------------------------------------------------------
+    def db_index(self, params, db_codes):
+        pr = _Params(params)
+        d = np.ascontiguousarray(db_codes, dtype=np.uint8)
+        h = self.L.gzo_db_index_build(pr.ptr, _p(d, u8p), len(d))
+        out = {}
+        names = ("nc_keys", "nc_offsets", "nc_values", "rep_keys", "rep_offsets",
+                 "rep_cluster_ids", "rep_positions", "member_offsets", "member_positions")
+        for i, nm in enumerate(names):
+            ptr = u32p()
+            n = self.L.gzo_db_index_array(C.c_void_p(h), i, C.byref(ptr))
+            out[nm] = np.ctypeslib.as_array(ptr, shape=(n,)).copy() if n else np.zeros(0, np.uint32)
+        self.L.gzo_db_index_free(C.c_void_p(h))
+        return out
+
+    def query_lists(self, params, queries):
+        pr = _Params(params)
+        h = self.L.gzo_query_lists_build(pr.ptr, _p(queries.codes, u8p),
+                                         _p(queries.offsets, u32p),
+                                         _p(queries.lengths, u32p), queries.number)
+        out = {}
+        for i, nm in enumerate(("hashes", "offsets", "check_counts", "query_ids", "positions")):
+            ptr = u32p()
+            n = self.L.gzo_query_lists_array(C.c_void_p(h), i, C.byref(ptr))
+            out[nm] = np.ctypeslib.as_array(ptr, shape=(n,)).copy() if n else np.zeros(0, np.uint32)
+        self.L.gzo_query_lists_free(C.c_void_p(h))
+        return out
+
+    # -- presearch --------------------------------------------------------------
+    def presearch(self, params, db, queries, query_begin=0, query_end=None):
+        """Returns (results per query as RESULT_DTYPE arrays, counters dict,
+        ungapped survivors (qid, q, d))."""
+        pr = _Params(params)
+        dbc = np.ascontiguousarray(db.codes, dtype=np.uint8)
+        idx = self.L.gzo_db_index_build(pr.ptr, _p(dbc, u8p), len(dbc))
+        lists = self.L.gzo_query_lists_build(pr.ptr, _p(queries.codes, u8p),
+                                             _p(queries.offsets, u32p),
+                                             _p(queries.lengths, u32p), queries.number)
+        if query_end is None:
+            query_end = queries.number
+        cut = np.ascontiguousarray(queries.cutoffs, dtype=np.int32)
+        trig = np.ascontiguousarray(queries.triggers, dtype=np.int32)
+        offs = np.ascontiguousarray(db.offsets, dtype=np.uint32)
+        h = self.L.gzo_presearch_run(pr.ptr, C.c_void_p(idx), C.c_void_p(lists),
+                                     _p(queries.codes, u8p), _p(queries.offsets, u32p),
+                                     _p(queries.lengths, u32p), queries.number,
+                                     _p(cut, i32p), _p(trig, i32p), _p(dbc, u8p), len(dbc),
+                                     _p(offs, u32p), db.number_sequences,
+                                     query_begin, query_end)
+        results = []
+        for qi in range(queries.number):
+            ptr = C.c_void_p()
+            n = self.L.gzo_presearch_results(C.c_void_p(h), qi, C.byref(ptr))
+            if n:
+                buf = (C.c_char * (n * RESULT_DTYPE.itemsize)).from_address(ptr.value)
+                results.append(np.frombuffer(bytes(buf), dtype=RESULT_DTYPE).copy())
+            else:
+                results.append(np.zeros(0, dtype=RESULT_DTYPE))
+        cnt = (C.c_uint64 * 6)()
+        self.L.gzo_presearch_counters(C.c_void_p(h), C.byref(cnt))
+        counters = dict(zip(COUNTER_NAMES, [int(v) for v in cnt]))
+        a, b, c = u32p(), u32p(), u32p()
+        n = self.L.gzo_presearch_hits(C.c_void_p(h), C.byref(a), C.byref(b), C.byref(c))
+        hits = tuple(np.ctypeslib.as_array(x, shape=(n,)).copy() if n else np.zeros(0, np.uint32)
+                     for x in (a, b, c))
+        self.L.gzo_presearch_free(C.c_void_p(h))
+        self.L.gzo_query_lists_free(C.c_void_p(lists))
+        self.L.gzo_db_index_free(C.c_void_p(idx))
+        return results, counters, hits
+
+
+class Reference:
+    """The reference's own units (built from the reference checkout)."""
+
+    def __init__(self, path: str = REF_LIB):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        L = C.CDLL(path)
+        self.L = L
+        L.gzr_hash.argtypes = [C.c_void_p, u8p, u32p, u32p]
+        L.gzr_hash_many.argtypes = [C.c_void_p, u8p, C.c_uint32, i32p, u32p, u32p]
+        L.gzr_distances.argtypes = [C.c_void_p, u8p, u8p, C.c_size_t, u32p, u32p,
+                                    C.POINTER(C.c_int8)]
+        L.gzr_ungapped_one_side.argtypes = [C.c_void_p, u8p, u8p, C.c_int, C.c_int]
+        L.gzr_gapped_one_side.argtypes = [C.c_void_p, u8p, C.c_uint32, u8p, C.c_int,
+                                          C.c_int, i32p, i32p, i32p]
+        L.gzr_chain_filter.argtypes = [C.c_void_p, u8p, C.c_uint32, C.c_int, u8p, u32p,
+                                       u32p, C.c_size_t]
+        L.gzr_chain_filter.restype = C.c_size_t
+        L.gzr_db_index_build.argtypes = [C.c_void_p, u8p, C.c_uint32]
+        L.gzr_db_index_build.restype = C.c_void_p
+        L.gzr_db_index_free.argtypes = [C.c_void_p]
+        L.gzr_db_index_lookup.argtypes = [C.c_void_p, C.c_int, C.c_uint32, u32p, C.c_size_t]
+        L.gzr_db_index_lookup.restype = C.c_size_t
+        L.gzr_db_index_members.argtypes = [C.c_void_p, C.c_uint32, u32p, C.c_size_t]
+        L.gzr_db_index_members.restype = C.c_size_t
+        L.gzr_db_index_max_mismatches.argtypes = [C.c_void_p]
+        L.gzr_ungapped_karlin.argtypes = [C.c_void_p, u8p, C.c_uint32, C.POINTER(C.c_float),
+                                          C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.gzr_normalized_cutoff_to_nominal.argtypes = [C.c_float, C.c_float, C.c_float]
+        L.gzr_normalized_to_nominal.argtypes = [C.c_float, C.c_float, C.c_float]
+
+    def hash_many(self, params, seq):
+        pr = _Params(params)
+        seq = np.ascontiguousarray(seq, dtype=np.uint8)
+        n = len(seq) - 8
+        r = np.zeros(n, np.int32)
+        h = np.zeros(n, np.uint32)
+        ln = np.zeros(n, np.uint32)
+        self.L.gzr_hash_many(pr.ptr, _p(seq, u8p), n, _p(r, i32p), _p(h, u32p), _p(ln, u32p))
+        return r, h, ln
+
+    def distances(self, params, seq0, seq1, c0, c1):
+        pr = _Params(params)
+        s0 = np.ascontiguousarray(seq0, dtype=np.uint8)
+        s1 = np.ascontiguousarray(seq1, dtype=np.uint8)
+        c0 = np.ascontiguousarray(c0, dtype=np.uint32)
+        c1 = np.ascontiguousarray(c1, dtype=np.uint32)
+        out = np.zeros(len(c0), np.int8)
+        self.L.gzr_distances(pr.ptr, _p(s0, u8p), _p(s1, u8p), len(c0), _p(c0, u32p),
+                             _p(c1, u32p), out.ctypes.data_as(C.POINTER(C.c_int8)))
+        return out
+
+    def ungapped_one_side(self, params, seq0, p0, seq1, p1, reversed_, cutoff):
+        pr = _Params(params)
+        s0 = np.ascontiguousarray(seq0, dtype=np.uint8)
+        s1 = np.ascontiguousarray(seq1, dtype=np.uint8)
+        return self.L.gzr_ungapped_one_side(
+            pr.ptr, C.cast(C.c_void_p(s0.ctypes.data + p0), u8p),
+            C.cast(C.c_void_p(s1.ctypes.data + p1), u8p), int(reversed_), int(cutoff))
+
+    def gapped_one_side(self, params, seq0, p0, len0, seq1, p1, reversed_, cutoff):
+        pr = _Params(params)
+        s0 = np.ascontiguousarray(seq0, dtype=np.uint8)
+        s1 = np.ascontiguousarray(seq1, dtype=np.uint8)
+        b, q, d = C.c_int32(), C.c_int32(), C.c_int32()
+        self.L.gzr_gapped_one_side(
+            pr.ptr, C.cast(C.c_void_p(s0.ctypes.data + p0), u8p), len0,
+            C.cast(C.c_void_p(s1.ctypes.data + p1), u8p), int(reversed_), int(cutoff),
+            C.byref(b), C.byref(q), C.byref(d))
+        return b.value, q.value, d.value
+
+    def chain_filter(self, params, query, qlen, cutoff, db, hq, hd):
+        pr = _Params(params)
+        q = np.ascontiguousarray(query, dtype=np.uint8)
+        d = np.ascontiguousarray(db, dtype=np.uint8)
+        hq = np.array(hq, dtype=np.uint32)
+        hd = np.array(hd, dtype=np.uint32)
+        n = self.L.gzr_chain_filter(pr.ptr, _p(q, u8p), qlen, int(cutoff), _p(d, u8p),
+                                    _p(hq, u32p), _p(hd, u32p), len(hq))
+        return hq[:n].copy(), hd[:n].copy()
+
+    def db_index(self, params, db_codes):
+        pr = _Params(params)
+        d = np.ascontiguousarray(db_codes, dtype=np.uint8)
+        self._keep = d
+        return self.L.gzr_db_index_build(pr.ptr, _p(d, u8p), len(d))
+
+    def lookup(self, h, which, key, cap=1 << 22):
+        out = np.zeros(cap, np.uint32)
+        n = self.L.gzr_db_index_lookup(C.c_void_p(h), which, key, _p(out, u32p), cap)
+        return out[: (2 * n if which == 1 else n)].copy()
+
+    def members(self, h, cid, cap=1 << 22):
+        out = np.zeros(cap, np.uint32)
+        n = self.L.gzr_db_index_members(C.c_void_p(h), cid, _p(out, u32p), cap)
+        return out[:n].copy()
+
+    def free_index(self, h):
+        self.L.gzr_db_index_free(C.c_void_p(h))
+
+    def ungapped_karlin(self, params, seq_with_delims):
+        pr = _Params(params)
+        s = np.ascontiguousarray(seq_with_delims, dtype=np.uint8)
+        lam, k, h = C.c_float(), C.c_float(), C.c_float()
+        self.L.gzr_ungapped_karlin(pr.ptr, _p(s, u8p), len(s), C.byref(lam), C.byref(k),
+                                   C.byref(h))
+        return lam.value, k.value, h.value
+
+    def cutoffs(self, lam, k, ungapped_bits=7.0, trigger_bits=22.0):
+        return (self.L.gzr_normalized_cutoff_to_nominal(ungapped_bits, lam, k),
+                self.L.gzr_normalized_to_nominal(trigger_bits, lam, k))

@@ -1,0 +1,213 @@
+/*
+ * ref_wrap.cpp -- C entry points over the reference's own arithmetic units.
+ *
+ * TEST INFRASTRUCTURE ONLY.  oracle/Makefile compiles this file together
+ * with reference sources taken in place from the reference checkout into
+ * oracle/_ref/libgzref.so.  Tests use it to pin the C restatement in
+ * gz_oracle.c to the reference's behaviour.  Nothing here is shipped.
+ */
+#include <stdint.h>
+#include <string.h>
+#include <vector>
+#include <string>
+
+#include "gz_oracle.h"
+
+#include "alphabet_coder.h"
+#include "score_matrix.h"
+#include "reduced_alphabet_variable_hash_function.h"
+#include "distance_calculator.h"
+#include "ungapped_extender.h"
+#include "gapped_extender.h"
+#include "chain_filter.h"
+#include "seed_searcher_database_parameters.h"
+#include "statistics.h"
+#include "protein_type.h"
+
+static ScoreMatrix make_matrix(const gzo_params *p) {
+  std::vector<int> m(p->number_letters * p->number_letters);
+  for (int i = 0; i < p->number_letters * p->number_letters; ++i)
+    m[i] = p->score_matrix[i];
+  return ScoreMatrix("BLOSUM62", &m[0], p->number_letters);
+}
+
+/* The reference builds its hash function inside
+ * SeedSearcherDatabaseParameters::Build
+ * (src/seed_searcher_database_parameters.cpp:52-75); rebuild it the same way. */
+static ReducedAlphabetVariableHashFunction make_hash(const gzo_params *p) {
+  std::vector<AlphabetCoder::Code> map(p->map_size);
+  for (int i = 0; i < p->map_size; ++i) map[i] = p->hash_code_map[i];
+  std::vector<int> scores(p->max_indexing_code + 1);
+  for (int i = 0; i <= p->max_indexing_code; ++i) scores[i] = p->code_scores[i];
+  return ReducedAlphabetVariableHashFunction(
+      (AlphabetCoder::Code)p->max_indexing_code, p->seed_threshold,
+      p->max_hash_length, map, scores);
+}
+
+extern "C" {
+
+int gzr_hash(const gzo_params *p, const uint8_t *seq, uint32_t *hash,
+             uint32_t *hash_length) {
+  ReducedAlphabetVariableHashFunction f = make_hash(p);
+  return f.CalculateHash(seq, hash, hash_length);
+}
+
+int gzr_hash_many(const gzo_params *p, const uint8_t *seq, uint32_t n,
+                  int32_t *ret, uint32_t *hash, uint32_t *hash_length) {
+  ReducedAlphabetVariableHashFunction f = make_hash(p);
+  for (uint32_t i = 0; i < n; ++i)
+    ret[i] = f.CalculateHash(seq + i, &hash[i], &hash_length[i]);
+  return 0;
+}
+
+int gzr_distances(const gzo_params *p, const uint8_t *seq0,
+                  const uint8_t *seq1, size_t n, uint32_t *c0, uint32_t *c1,
+                  int8_t *out) {
+  std::vector<AlphabetCoder::Code> map(32);
+  for (int i = 0; i < 32; ++i) map[i] = p->similarity_code_map[i];
+  DistanceCalculator d;
+  d.SetQueries(seq0);
+  d.SetDatabase(seq1);
+  d.SetReducedCodeMap(&map[0]);
+  return d.CalculateDistances(n, c0, c1, p->subsequence_length, (char *)out);
+}
+
+int gzr_ungapped_one_side(const gzo_params *p, const uint8_t *seq0,
+                          const uint8_t *seq1, int reversed, int cutoff) {
+  ScoreMatrix m = make_matrix(p);
+  int best = 0;
+  UngappedExtender::ExtendOneSideScoreOnly(seq0, seq1, p->delimiter,
+                                           reversed != 0, m, cutoff, &best);
+  return best;
+}
+
+int gzr_gapped_one_side(const gzo_params *p, const uint8_t *seq0,
+                        uint32_t seq0_length, const uint8_t *seq1,
+                        int reversed, int cutoff, int *best_score,
+                        int *best_pos0, int *best_pos1) {
+  ScoreMatrix m = make_matrix(p);
+  GappedExtender e;
+  e.ExtendOneSide(seq0, seq0_length, seq1, p->delimiter, reversed != 0, m,
+                  p->gap_open, p->gap_extension, cutoff, best_score,
+                  best_pos0, best_pos1, NULL);
+  return 0;
+}
+
+size_t gzr_chain_filter(const gzo_params *p, const uint8_t *query,
+                        uint32_t query_length, int cutoff, const uint8_t *db,
+                        uint32_t *hit_q, uint32_t *hit_d, size_t n) {
+  ScoreMatrix m = make_matrix(p);
+  ChainFilter f(p->delimiter, m);
+  std::vector<ChainFilter::Hit> hits(n);
+  for (size_t i = 0; i < n; ++i) {
+    hits[i].query_sequence_position = hit_q[i];
+    hits[i].database_sequence_position = hit_d[i];
+    hits[i].k_mer_count = 1;
+  }
+  f.Filter(query, query_length, cutoff, db, hits);
+  for (size_t i = 0; i < hits.size(); ++i) {
+    hit_q[i] = hits[i].query_sequence_position;
+    hit_d[i] = hits[i].database_sequence_position;
+  }
+  return hits.size();
+}
+
+/* Database index built by the reference builder; looked up key by key. */
+struct gzr_db_index {
+  SeedSearcherDatabaseParameters params;
+  std::vector<AlphabetCoder::Code> seq;
+};
+
+void *gzr_db_index_build(const gzo_params *p, const uint8_t *db,
+                         uint32_t length) {
+  gzr_db_index *x = new gzr_db_index;
+  x->seq.assign(db, db + length);
+  SeedSearcherDatabaseParameters::BuildParameters bp;
+  bp.clustering = p->clustering != 0;
+  bp.subsequence_length = p->subsequence_length;
+  bp.max_indexing_code = (AlphabetCoder::Code)p->max_indexing_code;
+  bp.sequence_delimiter = (AlphabetCoder::Code)p->delimiter;
+  bp.seed_threshold = p->seed_threshold;
+  bp.threshold = 0.0f;
+  bp.number_threads = 1;
+  bp.hash_code_map.assign(p->hash_code_map, p->hash_code_map + p->map_size);
+  bp.similairty_code_map.assign(p->similarity_code_map,
+                                p->similarity_code_map + p->map_size);
+  bp.score_matrix = make_matrix(p);
+  x->params.Build(&x->seq[0], length, bp);
+  return x;
+}
+
+void gzr_db_index_free(void *h) { delete (gzr_db_index *)h; }
+
+/* which: 0 residual values, 1 representatives (cluster id, position) */
+size_t gzr_db_index_lookup(void *h, int which, uint32_t key, uint32_t *out,
+                           size_t cap) {
+  gzr_db_index *x = (gzr_db_index *)h;
+  if (which == 0) {
+    const uint32_t *v = NULL;
+    size_t n = 0;
+    if (x->params.GetSequencesIndex().GetValues(key, &v, &n)) return 0;
+    for (size_t i = 0; i < n && i < cap; ++i) out[i] = v[i];
+    return n;
+  }
+  const SeedSearcherDatabaseParameters::ClusteringSequencesIndex::
+      RepresentativeData *r = NULL;
+  size_t n = 0;
+  if (x->params.GetClusteringSequencesIndex().GetRepresentatives(key, &r, &n))
+    return 0;
+  for (size_t i = 0; i < n && 2 * i + 1 < cap; ++i) {
+    out[2 * i] = r[i].first;
+    out[2 * i + 1] = r[i].second;
+  }
+  return n;
+}
+
+size_t gzr_db_index_members(void *h, uint32_t cluster_id, uint32_t *out,
+                            size_t cap) {
+  gzr_db_index *x = (gzr_db_index *)h;
+  const uint32_t *m = NULL;
+  size_t n = 0;
+  if (x->params.GetClusteringSequencesIndex().GetMembers(cluster_id, &m, &n))
+    return 0;
+  for (size_t i = 0; i < n && i < cap; ++i) out[i] = m[i];
+  return n;
+}
+
+int gzr_db_index_max_mismatches(void *h) {
+  return ((gzr_db_index *)h)->params.GetNumberMaxMismatchs();
+}
+
+/* Cutoffs exactly as the reference derives them from bit scores
+ * (src/statistics.cpp:28-43, :191-249). */
+int gzr_ungapped_karlin(const gzo_params *p, const uint8_t *seq,
+                        uint32_t length, float *lambda, float *k, float *h) {
+  ProteinType t;
+  Statistics s(t);
+  ScoreMatrix m = make_matrix(p);
+  Statistics::KarlinParameters kp;
+  bool ok = s.CalculateUngappedKarlinParameters(seq, length, m, &kp);
+  if (!ok) s.CalculateUngappedIdealKarlinParameters(m, &kp);
+  *lambda = kp.lambda;
+  *k = kp.K;
+  *h = kp.H;
+  return ok ? 0 : 1;
+}
+
+int gzr_normalized_cutoff_to_nominal(float bits, float lambda, float k) {
+  Statistics::KarlinParameters kp;
+  kp.lambda = lambda;
+  kp.K = k;
+  kp.H = 0;
+  return Statistics::NormalizedCutoff2NominalCutoff(bits, kp);
+}
+
+int gzr_normalized_to_nominal(float bits, float lambda, float k) {
+  Statistics::KarlinParameters kp;
+  kp.lambda = lambda;
+  kp.K = k;
+  kp.H = 0;
+  return Statistics::Normalized2Nominal(bits, kp);
+}
+
+} /* extern "C" */

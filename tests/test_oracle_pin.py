@@ -1,0 +1,222 @@
+"""Pins the C restatement (oracle/gz_oracle.c) to the reference: the
+reference's own units compiled from its sources (oracle/_ref) on random
+inputs, and the known answers of the reference's unit tests."""
+import numpy as np
+import pytest
+
+from gzb import params as P
+from gzb import workload as W
+
+DNA_DELIM = 5  # "ACGT" + unknown N -> max code 4, delimiter 5
+
+
+def dna(s):
+    return np.array([DNA_DELIM] + ["ACGT".index(c) for c in s] + [DNA_DELIM], np.uint8)
+
+
+def dna_params():
+    """match 2 / mismatch -1 over 4 letters (test/gapped_extender_test.cpp:24-46)."""
+    m = np.full((4, 4), -1, np.int32)
+    np.fill_diagonal(m, 2)
+    p = P.make_params(matrix=m, gap_open=0, gap_extension=1)
+    p["delimiter"] = DNA_DELIM
+    return p
+
+
+# --- known answers of the reference unit tests ------------------------------
+def test_gapped_known_answer_cpu(oracle):
+    # test/gapped_extender_test.cpp:49-56: AGTCAC vs AGCAG, forward from the
+    # first residue, open 0 / extend 1, no X-drop -> 7 at (4, 3)
+    p = dna_params()
+    s0, s1 = dna("AGTCAC"), dna("AGCAG")
+    score, q, d, _ = oracle.gapped_one_side(p, s0, 1, s1, 1, False, 2**31 - 1)
+    assert (score, q, d) == (7, 4, 3)
+
+
+def test_gapped_known_answers_gpu_suite(oracle):
+    # test/gapped_extender_gpu_test.cu:40-253 (absolute positions returned)
+    p = dna_params()
+    s0, s1 = dna("AGCAC"), dna("AGCAG")
+    score, q, d, _ = oracle.gapped_one_side(p, s0, 1, s1, 1, False, 0)
+    assert (score, 1 + q, 1 + d) == (8, 4, 4)
+    s0, s1 = dna("AGTCAC"), dna("AGCAG")
+    score, q, d, _ = oracle.gapped_one_side(p, s0, 1, s1, 1, False, 2**31 - 1)
+    assert (score, 1 + q, 1 + d) == (7, 5, 4)
+    score, q, d, _ = oracle.gapped_one_side(p, s0, len(s0) - 3, s1, len(s1) - 3, True,
+                                            2**31 - 1)
+    assert (score, len(s0) - 3 + q, len(s1) - 3 + d) == (7, 1, 1)
+
+
+def test_ungapped_known_answers(oracle):
+    # test/ungapped_extender_test.cpp:18-114
+    p = dna_params()
+    s0, s1 = dna("AAAAAAC"), dna("AACAAAG")
+    fwd = oracle.ungapped_one_side(p, s0, 1, s1, 1, False, 2**31 - 1)
+    rev = oracle.ungapped_one_side(p, s0, len(s0) - 3, s1, len(s1) - 3, True, 2**31 - 1)
+    assert fwd == 9 and rev == fwd
+    assert oracle.ungapped_one_side(p, s0, 1, s1, 1, False, 1) == 4
+
+
+def test_distance_known_answers(oracle, params):
+    # test/distance_calculator_test.cpp:56-117 (L = 4, centres 2/6/10)
+    p = params.copy()
+    p["subsequence_length"] = 4
+    a = P.encode("IMEHQSIMEHQS")
+    b = P.encode("LMEHQALMEHQA")
+    assert [oracle.distance(p, a, c, b, c) for c in (2, 6, 10)] == [0, 1, 1]
+    p["subsequence_length"] = 6
+    assert oracle.distance(p, P.encode("GMEHQS"), 3, P.encode("GMEHQS"), 3) == 0
+    assert oracle.distance(p, P.encode("IMEHQS"), 3, P.encode("LMEHQA"), 3) == 1
+
+
+def test_chain_filter_known_answers(oracle):
+    # test/chain_filter_test.cpp:11-121
+    p = dna_params()
+    q = dna("AAAAAAC")
+    assert len(oracle.chain_filter(p, q, len(q), 1, dna("AAACAAG"), [1, 3], [1, 3])[0]) == 1
+    assert len(oracle.chain_filter(p, q, len(q), 1, dna("AACAAAG"), [1, 2], [1, 2])[0]) == 1
+    assert len(oracle.chain_filter(p, q, len(q), 1, dna("AACAAAG"), [1, 4], [1, 4])[0]) == 2
+
+
+def test_hash_known_answer(oracle, params):
+    # test/reduced_alphabet_variable_hash_function_test.cpp:104-127 idea:
+    # the hash of a k-mer is its reduced codes (+1) packed 4 bits each until
+    # the code-score sum reaches the threshold (6..8 codes).
+    rmap, _ = P.reduced_code_map()
+    seq = np.concatenate([P.encode("GMEHQSWWCC"), [P.DELIMITER]]).astype(np.uint8)
+    r, h, ln = oracle.hash(params, seq)
+    exp_h, score, k = 0, 0, 0
+    while k < 8 and not (k >= 6 and score >= 39):
+        c = int(rmap[seq[k]])
+        exp_h = (exp_h << 4) + c + 1
+        score += int(params["code_scores"][c])
+        k += 1
+    assert (r, h, ln) == (0, exp_h, k)
+
+
+# --- random differential against the reference's own units ------------------
+def _seq_with_noise(rng, n):
+    s = W.random_residues(rng, n)
+    noise = rng.random(n)
+    s[noise < 0.02] = 24  # X
+    s[(noise >= 0.02) & (noise < 0.03)] = 20  # B
+    s[(noise >= 0.03) & (noise < 0.05)] = P.DELIMITER
+    return s
+
+
+def test_hash_matches_reference(oracle, reference, params):
+    rng = np.random.default_rng(7)
+    seq = np.concatenate([[25], _seq_with_noise(rng, 20000), [25] * 16]).astype(np.uint8)
+    r, h, ln = reference.hash_many(params, seq)
+    for i in range(0, len(r), 7):
+        rr, hh, ll = oracle.hash(params, seq, i)
+        assert rr == r[i]
+        if rr == 0:
+            assert (hh, ll) == (h[i], ln[i])
+
+
+def test_distance_matches_reference(oracle, reference, params):
+    rng = np.random.default_rng(8)
+    a = W.random_residues(rng, 5000)
+    b = a.copy()
+    mut = rng.random(len(b)) < 0.2
+    b[mut] = W.random_residues(rng, int(mut.sum()))
+    c0 = rng.integers(5, 4990, 2000).astype(np.uint32)
+    c1 = np.clip(c0.astype(np.int64) + rng.integers(-3, 4, 2000), 5, 4990).astype(np.uint32)
+    ref = reference.distances(params, a, b, c0, c1)
+    mine = [oracle.distance(params, a, int(x), b, int(y)) for x, y in zip(c0, c1)]
+    assert np.array_equal(ref, np.array(mine, np.int8))
+
+
+def _pair(rng, n, ident):
+    a = W.random_residues(rng, n)
+    b = W.mutate(rng, a, ident)
+    return (np.concatenate([[25], a, [25]]).astype(np.uint8),
+            np.concatenate([[25], b, [25]]).astype(np.uint8))
+
+
+def test_ungapped_matches_reference(oracle, reference, params):
+    rng = np.random.default_rng(9)
+    for t in range(400):
+        a, b = _pair(rng, int(rng.integers(5, 300)), rng.uniform(0.2, 1.0))
+        pa = int(rng.integers(1, len(a) - 1))
+        pb = int(rng.integers(1, len(b) - 1))
+        cutoff = int(rng.integers(1, 40))
+        for rev in (False, True):
+            assert oracle.ungapped_one_side(params, a, pa, b, pb, rev, cutoff) == \
+                reference.ungapped_one_side(params, a, pa, b, pb, rev, cutoff)
+
+
+@pytest.mark.parametrize("seed", [10, 11, 12])
+def test_gapped_matches_reference(oracle, reference, params, seed):
+    rng = np.random.default_rng(seed)
+    for t in range(150):
+        a, b = _pair(rng, int(rng.integers(5, 600)), rng.uniform(0.25, 1.0))
+        pa = int(rng.integers(1, len(a) - 1))
+        pb = int(np.clip(pa + rng.integers(-5, 6), 1, len(b) - 2))
+        cutoff = int(rng.choice([0, 5, 15, 26, 40, 2**31 - 1]))
+        for rev in (False, True):
+            len0 = pa if rev else len(a) - pa
+            r = reference.gapped_one_side(params, a, pa, len0, b, pb, rev, cutoff)
+            m = oracle.gapped_one_side(params, a, pa, b, pb, rev, cutoff)[:3]
+            assert m == r, (t, rev, cutoff)
+
+
+def test_chain_filter_matches_reference(oracle, reference, params):
+    rng = np.random.default_rng(13)
+    for t in range(100):
+        a, b = _pair(rng, int(rng.integers(30, 400)), rng.uniform(0.4, 1.0))
+        n = int(rng.integers(1, 60))
+        diag = int(rng.integers(-5, 6))
+        hq = rng.integers(1, len(a) - 1, n)
+        hd = np.clip(hq + diag + rng.integers(-1, 2, n) * rng.integers(0, 2, n), 1, len(b) - 2)
+        # unique (q, d) pairs, as seeds are
+        pairs = sorted(set(zip(hq.tolist(), hd.tolist())))
+        hq = [x for x, _ in pairs]
+        hd = [y for _, y in pairs]
+        cutoff = int(rng.integers(1, 30))
+        rq, rd = reference.chain_filter(params, a, len(a), cutoff, b, hq, hd)
+        mq, md = oracle.chain_filter(params, a, len(a), cutoff, b, hq, hd)
+        assert sorted(zip(rq.tolist(), rd.tolist())) == sorted(zip(mq.tolist(), md.tolist()))
+        assert list(md) == sorted(md)
+
+
+def test_db_index_matches_reference(oracle, reference, params):
+    db = W.make_database(300, 21, median=120)
+    mine = oracle.db_index(params, db.codes)
+    h = reference.db_index(params, db.codes)
+    try:
+        # every hash of the database is either in the residual index, the
+        # representative index, or absent from both, exactly as in the reference
+        keys = set(mine["nc_keys"].tolist()) | set(mine["rep_keys"].tolist())
+        for k in range(len(mine["nc_keys"])):
+            key = int(mine["nc_keys"][k])
+            v = mine["nc_values"][mine["nc_offsets"][k]:mine["nc_offsets"][k + 1]]
+            assert np.array_equal(reference.lookup(h, 0, key), v)
+        ref_cluster_members = {}
+        for k in range(len(mine["rep_keys"])):
+            key = int(mine["rep_keys"][k])
+            lo, hi = mine["rep_offsets"][k], mine["rep_offsets"][k + 1]
+            r = reference.lookup(h, 1, key).reshape(-1, 2)
+            assert np.array_equal(r[:, 1], mine["rep_positions"][lo:hi])
+            for (rcid, _), cid in zip(r, mine["rep_cluster_ids"][lo:hi]):
+                mm = mine["member_positions"][mine["member_offsets"][cid]:mine["member_offsets"][cid + 1]]
+                assert np.array_equal(reference.members(h, int(rcid)), mm)
+        r_, hh, _ = reference.hash_many(params, np.concatenate([db.codes, [25] * 16]).astype(np.uint8))
+        for key in set(hh[r_ == 0].tolist()) - keys:
+            assert len(reference.lookup(h, 0, key)) == 0
+            assert len(reference.lookup(h, 1, key)) == 0
+        assert len(mine["rep_keys"]) > 0 and len(mine["member_positions"]) > 0
+    finally:
+        reference.free_index(h)
+
+
+def test_cutoffs_match_reference(reference, params):
+    rng = np.random.default_rng(14)
+    for _ in range(100):
+        s = W.random_residues(rng, int(rng.integers(20, 1000)))
+        lam, k, _ = reference.ungapped_karlin(params, np.concatenate([[25], s, [25]]))
+        ml, mk, _ = P.ungapped_karlin_for_query(s)
+        assert (np.float32(ml), np.float32(mk)) == (np.float32(lam), np.float32(k))
+        assert reference.cutoffs(lam, k) == (P.normalized_cutoff_to_nominal(7.0, ml),
+                                             P.normalized_to_nominal(22.0, ml, mk))
