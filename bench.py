@@ -1,0 +1,365 @@
+"""Benchmark of the presearch hot path on the 10,000-query x 2,000,000-protein
+workload (synthetic, seeded; DB 2M proteins with log-normal lengths, median
+300, sigma 0.6, 30-3000; 10k queries of the same law, 30 % planted homologs
+at 30-90 % identity; BLOSUM62, open 11 / extend 1, clustered index L=10,
+seed threshold 39, top 10 per query, one result per subject).
+
+One step = one presearch of all queries against the resident database
+chunk: device query-list lookup, seed search + distance filter + ungapped
+X-drop with trigger, chain filter, gapped X-drop on both sides, top-b merge.
+
+  value : queries/s with the queries already resident in HBM
+  e2e   : queries/s through the C ABI with host buffers: every step uploads
+          the queries (and builds their hash lists), runs the presearch and
+          reads the per-query top-b lists back.
+The database index build is not in the timed region (it is reported as
+index_build_s), as the reference's `db` step is separate from `aln`.
+
+Multi-GPU: replicas -- every rank runs the full workload on its own GPU
+(the reference's -g threads replicate the work too); value sums the ranks'
+queries over the slowest rank's device time.
+
+--impl reference times the reference algorithm on the host cores instead
+(the CPU restatement in oracle/, all host threads, one process per core).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _sub in ("ghostz-gpu_b200", "oracle"):
+    _p = os.path.join(ROOT, _sub)
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "queries/s and DP GCUPS, learned-batched vs plain GPU, bit-identical hits"
+UNIT = "queries/s"
+
+WORKLOADS = {
+    # name: (db sequences, db seed, queries, query seed)
+    "protein-10k-x-2M": (2_000_000, 201, 10_000, 202),
+    "protein-1k-x-200k": (200_000, 211, 1_000, 212),   # small case for profiling
+}
+
+# algorithmic bytes of the dominant kernels (measurement):
+# ungapped seed: two residue bytes per residue pair examined; distance seed:
+# 8 B of centres + 2L window bytes + 1 B result.
+BYTES_PER_UNGAPPED_STEP = 2
+BYTES_PER_DISTANCE_SEED = 8 + 2 * 10 + 1
+
+
+def log(msg):
+    print(msg, file=sys.stderr, flush=True)
+
+
+def make_workload(name):
+    from gzb import workload as W
+    ndb, sdb, nq, sq = WORKLOADS[name]
+    t = time.time()
+    db = W.make_database(ndb, sdb)
+    q = W.make_queries(db, nq, sq)
+    return db, q, time.time() - t
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(db, q, n_queries=4000, slice_sequences=20000, processes=1):
+    """Times the CPU restatement (oracle/) on a bounded sample: the first
+    n_queries queries against the first slice_sequences database sequences;
+    queries/s is scaled to the full chunk by the residue ratio (search work
+    grows linearly with the chunk)."""
+    from gzb import workload as W
+    n_queries = min(n_queries, q.number)
+    slice_sequences = min(slice_sequences, db.number_sequences)
+    end = int(db.offsets[slice_sequences])  # delimiter after the last sequence
+    sub_db = W.Database(codes=db.codes[:end].copy(),
+                        offsets=np.concatenate([db.offsets[:slice_sequences],
+                                                [end]]).astype(np.uint32),
+                        number_sequences=slice_sequences)
+    qend = int(q.offsets[n_queries - 1] + q.lengths[n_queries - 1])
+    sub_q = W.Queries(codes=q.codes[:qend].copy(), offsets=q.offsets[:n_queries].copy(),
+                      lengths=q.lengths[:n_queries].copy(), cutoffs=q.cutoffs[:n_queries].copy(),
+                      triggers=q.triggers[:n_queries].copy())
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    bounds = np.linspace(0, n_queries, processes + 1).astype(int)
+    # each worker builds the chunk index untimed (the reference's separate
+    # `db` step) and times its query lists + presearch; the step takes as
+    # long as the slowest worker
+    if processes == 1:
+        el = _oracle_range((sub_db, sub_q, 0, n_queries))
+    else:
+        with ctx.Pool(processes) as pool:
+            el = max(pool.map(_oracle_range, [(sub_db, sub_q, int(bounds[i]), int(bounds[i + 1]))
+                                               for i in range(processes)]))
+    scale = (end) / db.length
+    value = n_queries / el * scale
+    sample = (f"{n_queries} queries x first {slice_sequences} DB sequences "
+              f"({end} of {db.length} residues) in {el:.2f} s, scaled by the residue ratio")
+    return value, el, sample
+
+
+def _oracle_range(args):
+    db, q, b, e = args
+    import oracle as O
+    from gzb import params as P
+    _, counters, _ = O.Oracle().presearch(P.make_params(), db, q, query_begin=b, query_end=e)
+    return counters["search_seconds"]
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    db, q, gen_s = make_workload(args.workload)
+    cores = os.cpu_count() or 1
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, el, sample = cpu_baseline(db, q, n_queries=args.ref_queries, processes=cores)
+        if i >= args.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded generator, config shapes)",
+        "config": {"workload": args.workload, "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--schedule", default="plain", choices=["plain", "batched"])
+    ap.add_argument("--workload", default="protein-10k-x-2M", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-queries", type=int, default=10000)
+    ap.add_argument("--ref-queries", type=int, default=4000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+
+    import torch
+    from gzb import native as N
+    from gzb import params as P
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    db, q, gen_s = make_workload(args.workload)
+    params = P.make_params()
+    eng = N.PresearchEngine(local_rank)
+    eng.set_params(params)
+    t = time.time()
+    eng.set_database(db)
+    torch.cuda.synchronize()
+    index_s = time.time() - t
+    eng.set_queries(q)
+    schedule = N.SCHEDULE_PLAIN if args.schedule == "plain" else N.SCHEDULE_BATCHED
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident timed loop
+    for _ in range(args.warmup):
+        eng.reset_results()
+        eng.presearch(schedule)
+    barrier()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stage = {k: 0.0 for k in ("lookup", "seed_ungapped", "chain", "gapped", "merge", "total")}
+    ev0.record(stream)
+    for _ in range(args.steps):
+        eng.reset_results(stream)
+        eng.presearch(schedule, stream)
+        for k, v in eng.stage_ms().items():
+            stage[k] += v
+    ev1.record(stream)
+    barrier()
+    dev_ms = ev0.elapsed_time(ev1)
+    clocks = sampler.stop()
+    counters = eng.counters()
+    results = eng.results()
+
+    # ---- end-to-end loop through the C ABI with host buffers
+    import ctypes
+    pinned = {}
+    for name in ("codes", "offsets", "lengths", "cutoffs", "triggers"):
+        a = getattr(q, name)
+        t_pin = torch.empty(a.nbytes, dtype=torch.uint8).pin_memory()
+        t_pin.numpy()[:] = np.frombuffer(np.ascontiguousarray(a).tobytes(), dtype=np.uint8)
+        pinned[name] = (t_pin, a.dtype)
+    from gzb import workload as W
+    qp = W.Queries(**{n: pinned[n][0].numpy().view(pinned[n][1]) for n in pinned})
+    b = int(params["max_number_results"])
+    counts_pin = torch.empty(q.number * 4, dtype=torch.uint8).pin_memory()
+    res_pin = torch.empty(q.number * b * N.RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+    L = N.lib()
+
+    def e2e_step():
+        eng.set_queries(qp, stream)
+        eng.presearch(schedule, stream)
+        N.check(L.gzb_engine_get_results(eng.h, ctypes.c_void_p(counts_pin.data_ptr()),
+                                         ctypes.c_void_p(res_pin.data_ptr()),
+                                         ctypes.c_void_p(stream.cuda_stream)))
+
+    for _ in range(args.warmup):
+        e2e_step()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    h2d = sum(getattr(q, n).nbytes for n in ("codes", "offsets", "lengths", "cutoffs", "triggers"))
+    d2h = counts_pin.numel() + res_pin.numel()
+    # the e2e results must equal the device loop's
+    got = np.frombuffer(res_pin.numpy().tobytes(), dtype=N.RESULT_DTYPE).reshape(q.number, b)
+    cnt = np.frombuffer(counts_pin.numpy().tobytes(), dtype=np.uint32)
+    e2e_same = all(np.array_equal(got[i, :cnt[i]], results[i]) for i in range(q.number))
+
+    # max over ranks
+    t_dev, t_e2e = dev_ms, e2e_ms
+    if dist is not None:
+        tt = torch.tensor([dev_ms, e2e_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_dev, t_e2e = float(tt[0]), float(tt[1])
+    nq = q.number
+    value = world * nq * args.steps / (t_dev / 1e3)
+    e2e_value = world * nq * args.steps / (t_e2e / 1e3)
+    steps = args.steps
+    st = {k: v / steps for k, v in stage.items()}
+    gcups_stage = counters["gapped_cells"] / (st["gapped"] / 1e3) / 1e9 if st["gapped"] else 0.0
+    gcups_step = counters["gapped_cells"] / (t_dev / steps / 1e3) / 1e9
+    # roofline of the dominant stage
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    dominant = "seed_ungapped" if st["seed_ungapped"] >= st["gapped"] else "gapped"
+    steps_pairs = counters.get("ungapped_steps", 0)
+    seed_bytes = (counters["ungapped_seeds"] * 0 + counters["distance_seeds"] * BYTES_PER_DISTANCE_SEED
+                  + BYTES_PER_UNGAPPED_STEP * steps_pairs)
+    achieved = seed_bytes / (st["seed_ungapped"] / 1e3) / 1e9 if st["seed_ungapped"] else 0.0
+    roofline = {"bound": "hbm", "kernel": "seed_kernel (seed search + distance + ungapped)",
+                "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
+                "dominant_stage": dominant,
+                "note": "gapped DP is integer-pipe bound: see dp_gcups"}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": t_dev / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded generator with the config's shapes)",
+        "config": {"workload": args.workload, "schedule": args.schedule,
+                   "db_sequences": db.number_sequences, "db_residues": db.length,
+                   "queries": nq, "l2": "inputs larger than L2 (database chunk > 126 MB)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": t_e2e / steps,
+                "results_equal_device_loop": bool(e2e_same)},
+        "dp_gcups": {"gapped_stage": gcups_stage, "whole_step": gcups_step},
+        "stage_ms": st, "counters": counters, "index_build_s": index_s,
+        "workload_gen_s": gen_s, "clocks": clocks, "roofline": roofline,
+        "gpu_launches": int(counters.get("kernel_launches", 0)) * steps,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        v, el, sample = cpu_baseline(db, q, n_queries=args.cpu_queries, processes=1)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+                                "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

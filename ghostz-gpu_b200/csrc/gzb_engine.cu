@@ -1,0 +1,1669 @@
+// gzb_engine.cu -- device-resident presearch of one database chunk.
+//
+// Stage map (reference functions in parentheses):
+//   set_database : seed index with subsequence clustering, built on the device
+//                  (SeedSearcherDatabaseParameters::Build,
+//                   src/seed_searcher_database_parameters.cpp:41-319)
+//   set_queries  : query hash lists
+//                  (SeedSearcherGpuQueryParameters::Build,
+//                   src/seed_searcher_gpu_query_parameters.cpp:17-272)
+//   presearch    : seed search + distance filter + ungapped X-drop with
+//                  trigger, fused (SeedSearcherGpu::Search*,
+//                  src/seed_searcher_gpu.cpp:186-537; DistanceCalculatorGpu;
+//                  UngappedExtenderGpu::ExtendWithTriggerAsync)
+//                  -> chain filter (ChainFilter::Filter, src/chain_filter.cpp:24-99)
+//                  -> gapped X-drop both sides (GappedExtenderGpu)
+//                  -> top-b merge (AlignerCommon::AddResults,
+//                     src/aligner_common.h:147-274)
+#include <cuda_runtime.h>
+#include <cooperative_groups.h>
+#include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "ghostz_b200.h"
+#include "gzb_common.h"
+#include "gzb_index.cuh"
+#include "gzb_kernels.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace gzb {
+
+int run_gapped(const GappedJob &job, const int32_t *matrix, int number_letters,
+               int stride, size_t n, const uint32_t *order, int reverse, const uint8_t *dir,
+               uint32_t *d_qpos, uint32_t *d_dpos, int32_t *d_scores, uint32_t **spill,
+               size_t *spill_cap, uint32_t *counters, unsigned long long *cells,
+               int2 **band_pool, int *band_wmask, cudaStream_t s, uint32_t *n_fallback);
+
+constexpr uint64_t kPad = 256;  // delimiter bytes kept around device sequences
+
+// Growable device buffer.
+struct DBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  int ensure(size_t need) {
+    if (need <= bytes) return GZB_OK;
+    cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    size_t n = need + need / 4 + 256;
+    GZB_CUDA(cudaMalloc(&p, n));
+    bytes = n;
+    return GZB_OK;
+  }
+  void release() {
+    cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <class T>
+  T *as() const {
+    return (T *)p;
+  }
+};
+
+static unsigned grid1(uint64_t n, int block, unsigned cap = 148u * 32u) {
+  uint64_t g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (unsigned)g;
+}
+
+// ---------------------------------------------------------------------------
+// warp-aggregated append (ballot compaction)
+template <class T>
+__device__ __forceinline__ void append(T *buf, unsigned long long *count,
+                                       unsigned long long cap, const T &v) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  unsigned long long base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(count, (unsigned long long)g.size());
+  base = g.shfl(base, 0);
+  const unsigned long long slot = base + g.thread_rank();
+  if (slot < cap) buf[slot] = v;
+}
+
+__device__ __forceinline__ void add_counter(unsigned long long *c, unsigned long long v) {
+  v += __shfl_down_sync(0xffffffffu, v, 16);
+  v += __shfl_down_sync(0xffffffffu, v, 8);
+  v += __shfl_down_sync(0xffffffffu, v, 4);
+  v += __shfl_down_sync(0xffffffffu, v, 2);
+  v += __shfl_down_sync(0xffffffffu, v, 1);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(c, v);
+}
+
+// ---------------------------------------------------------------------------
+// database index kernels
+
+// Keep rule of the index build (:85-108): a k-mer is dropped when the next
+// position's k-mer is contained in it.
+__global__ void db_pairs_kernel(DevParams p, const uint8_t *__restrict__ db, uint64_t len,
+                                uint64_t *pairs, unsigned long long *count) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < len;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t h, h2;
+    int hl, hl2;
+    if (!seed_hash(p, db + i, &h, &hl)) continue;
+    if (i + 1 < len && seed_hash(p, db + i + 1, &h2, &hl2) && hl2 + 1 <= hl) continue;
+    append(pairs, count, len, ((uint64_t)h << 32) | (uint64_t)i);
+  }
+}
+
+// Per sorted entry: bucket start flag, non-clustering state and the packed
+// similarity window (4 bits per code).
+__global__ void db_entry_kernel(DevParams p, const uint8_t *__restrict__ db,
+                                const uint64_t *__restrict__ pairs, uint64_t n,
+                                uint8_t *flag_start, uint8_t *state, uint64_t *window) {
+  const int L = p.subsequence_length, half = L / 2;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = pairs[i];
+    flag_start[i] = (i == 0 || (pairs[i - 1] >> 32) != (k >> 32)) ? 1 : 0;
+    const uint32_t c = (uint32_t)k;
+    uint8_t st = 0;
+    uint64_t w = 0;
+    if ((int)c < half) {
+      st = 1;
+    } else {
+      for (int t = 0; t < L; ++t) {
+        const int x = db[c - half + t];
+        if (x == p.delimiter) {
+          st = 1;
+          break;
+        }
+        w |= (uint64_t)(p.sim_map[x] & 15) << (4 * t);
+      }
+    }
+    state[i] = st;
+    window[i] = w;
+  }
+}
+
+__device__ __forceinline__ int nibble_mismatches(uint64_t a, uint64_t b) {
+  uint64_t x = a ^ b;
+  x = (x | (x >> 1) | (x >> 2) | (x >> 3)) & 0x1111111111111111ull;
+  return __popcll(x);
+}
+
+// Greedy clustering inside each hash bucket (:117-205): walking the bucket
+// in position order, every still-free entry becomes a representative and
+// claims the later free entries within max_member_distance mismatches.
+// One warp per bucket.
+__global__ void cluster_kernel(const uint32_t *__restrict__ bucket_start, uint64_t n_buckets,
+                               uint64_t n, uint8_t *state, const uint64_t *__restrict__ window,
+                               uint32_t *rep_of, int max_mismatch) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t b = warp; b < n_buckets; b += nwarps) {
+    const uint64_t s = bucket_start[b];
+    const uint64_t e = (b + 1 < n_buckets) ? bucket_start[b + 1] : n;
+    if (e - s < 2) {
+      if (lane == 0 && state[s] == 0) state[s] = 2;
+      continue;
+    }
+    for (uint64_t i = s; i < e; ++i) {
+      const uint8_t st = state[i];  // uniform: written before the last __syncwarp
+      if (st != 0) continue;
+      const uint64_t wr = window[i];
+      if (lane == 0) state[i] = 2;
+      for (uint64_t j = i + 1 + lane; j < e; j += 32) {
+        if (state[j] == 0 && nibble_mismatches(wr, window[j]) <= max_mismatch) {
+          state[j] = 3;
+          rep_of[j] = (uint32_t)i;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+__global__ void member_count_kernel(const uint8_t *state, const uint32_t *rep_of, uint64_t n,
+                                    uint32_t *member_count) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    if (state[i] == 3) atomicAdd(&member_count[rep_of[i]], 1u);
+}
+
+// class flags: nc (0/1), rep (0/1)
+__global__ void classify_kernel(const uint8_t *state, const uint32_t *member_count, uint64_t n,
+                                uint8_t *is_nc, uint8_t *is_rep, uint8_t *is_member) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const bool rep = state[i] == 2 && member_count[i] > 0;
+    const bool mem = state[i] == 3;
+    is_rep[i] = rep;
+    is_member[i] = mem;
+    is_nc[i] = !rep && !mem;
+  }
+}
+
+__global__ void key_start_flags(const uint64_t *keys, uint64_t n, uint8_t *flag) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    flag[i] = (i == 0 || (keys[i - 1] >> 32) != (keys[i] >> 32)) ? 1 : 0;
+}
+
+__global__ void iota_u32(uint32_t *a, uint64_t n) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    a[i] = (uint32_t)i;
+}
+
+// keys/offsets/values of a CSR from hash-sorted (hash<<32|value) pairs and
+// the indices of segment starts.
+__global__ void csr_fill(const uint64_t *pairs, uint64_t n, const uint32_t *starts,
+                         uint64_t nseg, uint32_t *keys, uint32_t *offsets, uint32_t *values) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    values[i] = (uint32_t)pairs[i];
+  for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s <= nseg;
+       s += (uint64_t)gridDim.x * blockDim.x) {
+    if (s < nseg) {
+      keys[s] = (uint32_t)(pairs[starts[s]] >> 32);
+      offsets[s] = starts[s];
+    } else {
+      offsets[s] = (uint32_t)n;
+    }
+  }
+}
+
+// rank of each representative entry = its cluster id
+__global__ void scatter_cluster_ids(const uint32_t *rep_entries, uint64_t nrep,
+                                    uint32_t *cid_of_entry, uint32_t *cluster_ids) {
+  for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < nrep;
+       r += (uint64_t)gridDim.x * blockDim.x) {
+    cid_of_entry[rep_entries[r]] = (uint32_t)r;
+    cluster_ids[r] = (uint32_t)r;
+  }
+}
+
+__global__ void member_pairs_kernel(const uint32_t *member_entries, uint64_t nm,
+                                    const uint32_t *rep_of, const uint32_t *cid_of_entry,
+                                    const uint64_t *pairs, uint64_t *out, uint32_t *cnt) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nm;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t e = member_entries[i];
+    const uint32_t cid = cid_of_entry[rep_of[e]];
+    out[i] = ((uint64_t)cid << 32) | (uint32_t)pairs[e];
+    atomicAdd(&cnt[cid], 1u);
+  }
+}
+
+__global__ void low32(const uint64_t *in, uint64_t n, uint32_t *out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = (uint32_t)in[i];
+}
+
+// ---------------------------------------------------------------------------
+// query lists
+
+// One thread per query: every position of a delimiter-free stretch of at
+// least L residues is hashed; key = hash<<32 | nocheck<<31 | concat pos.
+__global__ void query_entries_kernel(DevParams p, const uint8_t *__restrict__ q,
+                                     const uint32_t *__restrict__ offsets,
+                                     const uint32_t *__restrict__ lengths, uint32_t nq,
+                                     uint64_t *keys, unsigned long long *count,
+                                     unsigned long long cap) {
+  const uint32_t L = (uint32_t)p.subsequence_length;
+  for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < nq;
+       qi += gridDim.x * blockDim.x) {
+    const uint8_t *s = q + offsets[qi];
+    const uint32_t len = lengths[qi];
+    uint32_t off = 0;
+    while (off < len) {
+      uint32_t end = off;
+      while (end < len && s[end] != p.delimiter) ++end;
+      if (end - off >= L) {
+        const uint32_t cs = off + L / 2, ce = end - L / 2;
+        for (uint32_t i = off; i < end; ++i) {
+          uint32_t h;
+          int hl;
+          if (seed_hash(p, s + i, &h, &hl)) {
+            const uint64_t nocheck = (cs <= i && i < ce) ? 0 : 1;
+            const uint64_t k = ((uint64_t)h << 32) | (nocheck << 31) |
+                               (uint64_t)(offsets[qi] + i);
+            const unsigned long long slot = atomicAdd(count, 1ull);
+            if (slot < cap) keys[slot] = k;
+          }
+        }
+      }
+      off = end + 1;
+    }
+  }
+}
+
+// lists from sorted entry keys: per list hash, offset and check count;
+// per entry the query id and concatenated position
+__global__ void list_fill_kernel(const uint64_t *keys, uint64_t n, const uint32_t *starts,
+                                 uint64_t nl, const uint32_t *q_offsets, uint32_t nq,
+                                 uint32_t *hash, uint32_t *offsets, uint32_t *nchk,
+                                 uint32_t *entry_qid, uint32_t *entry_cpos) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t cpos = (uint32_t)(keys[i] & 0x7fffffffu);
+    // query: largest qi with offsets[qi] <= cpos
+    uint32_t lo = 0, hi = nq - 1;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (q_offsets[mid] <= cpos)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    entry_qid[i] = lo;
+    entry_cpos[i] = cpos;
+  }
+  for (uint64_t l = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; l <= nl;
+       l += (uint64_t)gridDim.x * blockDim.x) {
+    if (l == nl) {
+      offsets[l] = (uint32_t)n;
+      continue;
+    }
+    const uint32_t b = starts[l];
+    const uint32_t e = (l + 1 < nl) ? starts[l + 1] : (uint32_t)n;
+    hash[l] = (uint32_t)(keys[b] >> 32);
+    offsets[l] = b;
+    // check entries (nocheck bit 0) come first
+    uint32_t lo = b, hi = e;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (((keys[mid] >> 31) & 1) == 0)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    nchk[l] = lo - b;
+  }
+}
+
+__global__ void list_lookup_kernel(DevLists L, DevIndex X, int clustering,
+                                   uint64_t *unit_counts) {
+  for (uint64_t l = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; l < L.n_lists;
+       l += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t h = L.hash[l];
+    uint32_t rb = 0, rc = 0, nb = 0, nc = 0;
+    if (clustering) {
+      const long long r = find_key(X.rep_keys, X.n_rep_keys, h);
+      if (r >= 0) {
+        rb = X.rep_offsets[r];
+        rc = X.rep_offsets[r + 1] - rb;
+      }
+    }
+    const long long v = find_key(X.nc_keys, X.n_nc_keys, h);
+    if (v >= 0) {
+      nb = X.nc_offsets[v];
+      nc = X.nc_offsets[v + 1] - nb;
+    }
+    L.rep_begin[l] = rb;
+    L.rep_count[l] = rc;
+    L.nc_begin[l] = nb;
+    L.nc_count[l] = nc;
+    unit_counts[l] = (uint64_t)rc + nc;  // exclusive-scanned into unit_offsets
+  }
+}
+
+// ---------------------------------------------------------------------------
+// presearch kernels
+
+struct SeedArgs {
+  DevParams p;
+  DevLists L;
+  DevIndex X;
+  const uint8_t *q;
+  const uint8_t *db;
+  const uint32_t *q_offsets;
+  const int32_t *cutoffs;
+  const int32_t *triggers;
+  const int32_t *matrix32;  // 32x32
+  int clustering;
+  int dbits, qbits;         // packed hit key: qid | d << qbits | q
+  uint64_t *hits;
+  unsigned long long *hit_count;
+  unsigned long long hit_cap;
+  uint2 *mwork;             // member work: (cluster id, entry index)
+  unsigned long long *mwork_count;
+  unsigned long long mwork_cap;
+  unsigned long long *ctr;  // [0] distance seeds [1] ungapped seeds [2] steps
+};
+
+__device__ __forceinline__ void emit_hit(const SeedArgs &a, uint32_t qid, uint32_t d,
+                                         uint32_t qp) {
+  const uint64_t key = ((uint64_t)qid << (a.dbits + a.qbits)) |
+                       ((uint64_t)d << a.qbits) | (uint64_t)qp;
+  append(a.hits, a.hit_count, a.hit_cap, key);
+}
+
+constexpr int kSeedBlock = 256;
+constexpr int kUnitsPerWarp = 256;
+
+// One unit = one representative or one residual database position of a list,
+// tried against every query position of that list.
+__global__ void __launch_bounds__(kSeedBlock)
+seed_kernel(SeedArgs a) {
+  __shared__ int sm[kMatrixStride * kMatrixStride];
+  __shared__ uint8_t simmap[256];
+  load_matrix(sm, a.matrix32, kMatrixStride, kMatrixStride);
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) simmap[i] = i < 32 ? a.p.sim_map[i] : 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint64_t U = a.L.n_units;
+  const int delim = a.p.delimiter;
+  const int thr = a.p.distance_threshold;
+  const int maxmd = a.p.max_member_distance;
+  const int Ls = a.p.subsequence_length;
+  unsigned long long n_dist = 0, n_seed = 0, n_steps = 0;
+  for (uint64_t base = warp * kUnitsPerWarp; base < U; base += nwarps * kUnitsPerWarp) {
+    const uint64_t last = min(base + kUnitsPerWarp, U) - 1;
+    // list range of this warp's units
+    uint64_t l_lo = 0, l_hi = 0;
+    if (lane == 0) {
+      l_lo = upper_segment(a.L.unit_offsets, 0, a.L.n_lists - 1, base);
+      l_hi = upper_segment(a.L.unit_offsets, l_lo, a.L.n_lists - 1, last);
+    }
+    l_lo = __shfl_sync(0xffffffffu, l_lo, 0);
+    l_hi = __shfl_sync(0xffffffffu, l_hi, 0);
+    for (uint64_t u = base + lane; u <= last; u += 32) {
+      const uint64_t l = upper_segment(a.L.unit_offsets, l_lo, l_hi, u);
+      const uint32_t j = (uint32_t)(u - a.L.unit_offsets[l]);
+      const uint32_t pb = a.L.offsets[l], pe = a.L.offsets[l + 1];
+      const uint32_t nchk = a.L.nchk[l];
+      const uint32_t nrep = a.L.rep_count[l];
+      if (j < nrep) {
+        // representative: distance filter for check positions
+        const uint32_t r = a.L.rep_begin[l] + j;
+        const uint32_t rpos = a.X.rep_positions[r];
+        const uint32_t cid = a.X.rep_cluster_ids[r];
+        const bool members = a.X.member_offsets[cid + 1] > a.X.member_offsets[cid];
+        const uint8_t *dptr = a.db + rpos;
+        for (uint32_t k = pb; k < pe; ++k) {
+          const uint32_t qid = a.L.entry_qid[k];
+          const uint32_t cpos = a.L.entry_cpos[k];
+          const uint8_t *qptr = a.q + cpos;
+          bool try_rep, pass;
+          if (k < pb + nchk) {
+            const int dist = window_distance(qptr, dptr, Ls, simmap);
+            ++n_dist;
+            try_rep = dist <= thr;
+            pass = max(dist - maxmd, 0) <= thr;
+          } else {
+            try_rep = true;
+            pass = true;
+          }
+          if (try_rep) {
+            int steps = 0;
+            ++n_seed;
+            if (ungapped_hit(qptr, dptr, delim, sm, a.cutoffs[qid], a.triggers[qid], &steps))
+              emit_hit(a, qid, rpos, cpos - a.q_offsets[qid]);
+            n_steps += steps;
+          }
+          if (pass && members) append(a.mwork, a.mwork_count, a.mwork_cap, make_uint2(cid, k));
+        }
+      } else {
+        const uint32_t d = a.X.nc_values[a.L.nc_begin[l] + (j - nrep)];
+        const uint8_t *dptr = a.db + d;
+        for (uint32_t k = pb; k < pe; ++k) {
+          const uint32_t qid = a.L.entry_qid[k];
+          const uint32_t cpos = a.L.entry_cpos[k];
+          int steps = 0;
+          ++n_seed;
+          if (ungapped_hit(a.q + cpos, dptr, delim, sm, a.cutoffs[qid], a.triggers[qid], &steps))
+            emit_hit(a, qid, d, cpos - a.q_offsets[qid]);
+          n_steps += steps;
+        }
+      }
+    }
+  }
+  __syncwarp();
+  add_counter(&a.ctr[0], n_dist);
+  add_counter(&a.ctr[1], n_seed);
+  add_counter(&a.ctr[2], n_steps);
+}
+
+__global__ void mwork_counts_kernel(const uint2 *mwork, uint64_t n, const uint32_t *member_offsets,
+                                    uint64_t *counts) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t cid = mwork[i].x;
+    counts[i] = member_offsets[cid + 1] - member_offsets[cid];
+  }
+}
+
+// Members of a representative's cluster against one passing query position.
+__global__ void __launch_bounds__(kSeedBlock)
+member_kernel(SeedArgs a, const uint2 *mwork, uint64_t n_work, const uint64_t *offs,
+              uint64_t total) {
+  __shared__ int sm[kMatrixStride * kMatrixStride];
+  load_matrix(sm, a.matrix32, kMatrixStride, kMatrixStride);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const int delim = a.p.delimiter;
+  unsigned long long n_seed = 0, n_steps = 0;
+  for (uint64_t base = warp * kUnitsPerWarp; base < total; base += nwarps * kUnitsPerWarp) {
+    const uint64_t last = min(base + kUnitsPerWarp, total) - 1;
+    uint64_t w_lo = 0, w_hi = 0;
+    if (lane == 0) {
+      w_lo = upper_segment(offs, 0, n_work - 1, base);
+      w_hi = upper_segment(offs, w_lo, n_work - 1, last);
+    }
+    w_lo = __shfl_sync(0xffffffffu, w_lo, 0);
+    w_hi = __shfl_sync(0xffffffffu, w_hi, 0);
+    for (uint64_t u = base + lane; u <= last; u += 32) {
+      const uint64_t w = upper_segment(offs, w_lo, w_hi, u);
+      const uint2 mw = mwork[w];
+      const uint32_t m = a.X.member_offsets[mw.x] + (uint32_t)(u - offs[w]);
+      const uint32_t d = a.X.member_positions[m];
+      const uint32_t qid = a.L.entry_qid[mw.y];
+      const uint32_t cpos = a.L.entry_cpos[mw.y];
+      int steps = 0;
+      ++n_seed;
+      if (ungapped_hit(a.q + cpos, a.db + d, delim, sm, a.cutoffs[qid], a.triggers[qid], &steps))
+        emit_hit(a, qid, d, cpos - a.q_offsets[qid]);
+      n_steps += steps;
+    }
+  }
+  __syncwarp();
+  add_counter(&a.ctr[1], n_seed);
+  add_counter(&a.ctr[2], n_steps);
+}
+
+// first hit index of every query (hits sorted by packed key)
+__global__ void hit_segments_kernel(const uint64_t *hits, uint64_t n, uint32_t nq, int shift,
+                                    uint64_t *begin) {
+  for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi <= nq;
+       qi += gridDim.x * blockDim.x) {
+    const uint64_t key = (uint64_t)qi << shift;
+    uint64_t lo = 0, hi = n;
+    while (lo < hi) {
+      const uint64_t mid = (lo + hi) >> 1;
+      if (hits[mid] < key)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    begin[qi] = lo;
+  }
+}
+
+// Chain filter, one thread per query, over its hits in (database, query)
+// position order; survivors are compacted to the front of the query's
+// segment.  slots: per-query scratch of query_length (diagonal, end) pairs.
+__global__ void chain_kernel(DevParams p, const uint8_t *__restrict__ q,
+                             const uint8_t *__restrict__ db, const uint32_t *q_offsets,
+                             const uint32_t *q_lengths, const int32_t *cutoffs,
+                             const int32_t *matrix32, uint32_t nq, uint64_t *hits,
+                             const uint64_t *begin, int qbits, int dbits, uint2 *slots,
+                             uint32_t *kept_count) {
+  const uint64_t qmask = (1ull << qbits) - 1, dmask = (1ull << dbits) - 1;
+  const int n = kMatrixStride;
+  for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < nq;
+       qi += gridDim.x * blockDim.x) {
+    const uint64_t b = begin[qi], e = begin[qi + 1];
+    if (b == e) {
+      kept_count[qi] = 0;
+      continue;
+    }
+    const uint8_t *qs = q + q_offsets[qi];
+    const uint32_t qlen = q_lengths[qi];
+    uint2 *slot = slots + q_offsets[qi] + qi;  // qlen entries of this query
+    for (uint32_t i = 0; i < qlen; ++i) slot[i] = make_uint2(0, 0);
+    const int cutoff = cutoffs[qi];
+    uint64_t w = b;
+    for (uint64_t i = b; i < e; ++i) {
+      const uint64_t key = hits[i];
+      const uint32_t hq = (uint32_t)(key & qmask);
+      const uint32_t hd = (uint32_t)((key >> qbits) & dmask);
+      const uint32_t diagonal = qlen - 1 + hd - hq;
+      uint2 &sl = slot[diagonal % qlen];  // x = diagonal, y = query end
+      bool connected = false;
+      if (sl.x == diagonal) {
+        if (hq <= sl.y + 1) {
+          connected = true;
+        } else {
+          // back-extension toward the chain end (ChainFilter::Connected)
+          uint32_t qo = hq, dof = hd;
+          int score = 0, best = 0, c = -cutoff;
+          do {
+            --dof;
+            --qo;
+            if (db[dof] == p.delimiter || qs[qo] == p.delimiter || qo <= sl.y) break;
+            score += matrix32[db[dof] * n + qs[qo]];
+            if (best < score) {
+              best = score;
+              c = best - cutoff;
+            }
+          } while (score > c);
+          connected = qo <= sl.y;
+        }
+      }
+      sl.y = hq;
+      if (!connected) {
+        sl.x = diagonal;
+        hits[w++] = key;
+      }
+    }
+    kept_count[qi] = (uint32_t)(w - b);
+  }
+}
+
+// extension seeds: reverse at (q-1, d-1), forward at (q, d), absolute
+// concatenated query / chunk positions
+__global__ void build_ext_kernel(const uint64_t *hits, const uint64_t *begin,
+                                 const uint32_t *kept, const uint64_t *surv_off, uint32_t nq,
+                                 const uint32_t *q_offsets, int qbits, int dbits,
+                                 uint64_t n_surv, uint32_t *eq, uint32_t *ed, uint8_t *dir) {
+  const uint64_t qmask = (1ull << qbits) - 1, dmask = (1ull << dbits) - 1;
+  for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < nq;
+       qi += gridDim.x * blockDim.x) {
+    const uint64_t b = begin[qi], o = surv_off[qi];
+    for (uint32_t k = 0; k < kept[qi]; ++k) {
+      const uint64_t key = hits[b + k];
+      const uint32_t hq = (uint32_t)(key & qmask);
+      const uint32_t hd = (uint32_t)((key >> qbits) & dmask);
+      eq[o + k] = q_offsets[qi] + hq - 1;
+      ed[o + k] = hd - 1;
+      dir[o + k] = 1;
+      eq[n_surv + o + k] = q_offsets[qi] + hq;
+      ed[n_surv + o + k] = hd;
+      dir[n_surv + o + k] = 0;
+    }
+  }
+}
+
+// ---- top-b merge -----------------------------------------------------------
+__device__ __forceinline__ int alignment_comp(const gzb_result &a, const gzb_result &b) {
+  if (a.score > b.score) return 1;
+  if (a.score < b.score) return -1;
+  const uint32_t aq = a.end_q - a.start_q, bq = b.end_q - b.start_q;
+  if (aq > bq) return 1;
+  if (aq < bq) return -1;
+  const uint32_t as = a.end_d - a.start_d, bs = b.end_d - b.start_d;
+  if (as > bs) return 1;
+  if (as < bs) return -1;
+  return (a.start_d < b.start_d) ? 1 : -1;
+}
+
+// strict order used for the stable sort: AlignmentComp, then input order
+// (AlignmentComp is antisymmetric except on full ties, where it returns -1
+// both ways; the reference's stable_sort keeps such ties in input order.)
+__device__ __forceinline__ bool before(const gzb_result *r, uint32_t i, uint32_t j) {
+  if (alignment_comp(r[i], r[j]) > 0) return true;
+  if (alignment_comp(r[j], r[i]) > 0) return false;
+  return i < j;
+}
+
+__device__ __forceinline__ bool is_contained(const gzb_result &a, const gzb_result &b) {
+  return (a.start_q == b.start_q && a.start_d == b.start_d) ||
+         (a.end_q == b.end_q && a.end_d == b.end_d) ||
+         (a.start_q <= b.start_q && b.end_q <= a.end_q && a.start_d <= b.start_d &&
+          b.end_d <= a.end_d);
+}
+
+__device__ __forceinline__ uint32_t subject_of(const uint32_t *off, uint32_t nseq,
+                                               uint32_t db_len, uint32_t pos) {
+  if (off[nseq - 1] <= pos && pos < db_len) return nseq - 1;
+  uint32_t lo = 0, hi = nseq;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (off[mid] <= pos)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo == 0 ? 0xFFFFFFFFu : lo - 1;
+}
+
+// heap of indices ordered so that the root is the first in sorted order
+__device__ void sift_down(const gzb_result *r, uint32_t *h, uint32_t n, uint32_t i) {
+  for (;;) {
+    uint32_t l = 2 * i + 1, best = i;
+    if (l < n && before(r, h[l], h[best])) best = l;
+    if (l + 1 < n && before(r, h[l + 1], h[best])) best = l + 1;
+    if (best == i) return;
+    const uint32_t t = h[i];
+    h[i] = h[best];
+    h[best] = t;
+    i = best;
+  }
+}
+
+// One thread per query: results of its survivors merged into its running
+// top-b list exactly as AlignerCommon::AddResults orders and prunes them.
+__global__ void merge_kernel(uint32_t nq, const uint64_t *hits, const uint64_t *begin,
+                             const uint32_t *kept, const uint64_t *surv_off,
+                             uint64_t n_surv, const uint32_t *eq, const uint32_t *ed,
+                             const int32_t *escore, const uint32_t *q_offsets, int qbits,
+                             int dbits, const uint32_t *db_offsets, uint32_t nseq,
+                             uint32_t db_len, int32_t chunk_id, int max_results,
+                             int max_one_subject, gzb_result *scratch, uint32_t *heap,
+                             gzb_result *results, uint32_t *counts) {
+  const uint64_t qmask = (1ull << qbits) - 1, dmask = (1ull << dbits) - 1;
+  for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < nq;
+       qi += gridDim.x * blockDim.x) {
+    const uint32_t k = kept[qi];
+    if (k == 0) continue;
+    const uint64_t b = begin[qi], o = surv_off[qi];
+    const uint32_t qoff = q_offsets[qi];
+    gzb_result *added = scratch + o;
+    uint32_t *h = heap + o;
+    for (uint32_t i = 0; i < k; ++i) {
+      const uint64_t key = hits[b + i];
+      gzb_result r;
+      r.chunk_id = chunk_id;
+      r.subject_id = 0;
+      r.hit_q = (uint32_t)(key & qmask);
+      r.hit_d = (uint32_t)((key >> qbits) & dmask);
+      r.score = escore[o + i] + escore[n_surv + o + i];
+      r.start_q = eq[o + i] - qoff;
+      r.start_d = ed[o + i];
+      r.end_q = eq[n_surv + o + i] - qoff;
+      r.end_d = ed[n_surv + o + i];
+      added[i] = r;
+      h[i] = i;
+    }
+    for (int i = (int)k / 2 - 1; i >= 0; --i) sift_down(added, h, k, (uint32_t)i);
+    uint32_t heap_n = k;
+    // previous list of this query (earlier chunks)
+    gzb_result *prev = results + (uint64_t)qi * max_results;
+    const uint32_t n_prev = counts[qi];
+    gzb_result old[32];
+    const uint32_t n_old = n_prev < 32 ? n_prev : 32;
+    for (uint32_t i = 0; i < n_old; ++i) old[i] = prev[i];
+    uint32_t ri = 0, n_out = 0;
+    // per-subject start lists of this chunk (subject, size, entries)
+    uint32_t subj[32];
+    uint32_t subj_n[32];
+    uint32_t sp_pos[32][4];
+    uint32_t sp_id[32][4];
+    uint32_t n_subj = 0;
+    while ((int)n_out < max_results && (heap_n > 0 || ri < n_old)) {
+      gzb_result a;
+      bool take_added;
+      if (heap_n == 0)
+        take_added = false;
+      else if (ri == n_old)
+        take_added = true;
+      else
+        take_added = alignment_comp(old[ri], added[h[0]]) < 0;
+      if (take_added) {
+        a = added[h[0]];
+        a.subject_id = (int32_t)subject_of(db_offsets, nseq, db_len, a.start_d);
+        h[0] = h[--heap_n];
+        sift_down(added, h, heap_n, 0);
+      } else {
+        a = old[ri++];
+      }
+      if (a.chunk_id == chunk_id) {
+        uint32_t si = 0;
+        while (si < n_subj && subj[si] != (uint32_t)a.subject_id) ++si;
+        if (si == n_subj) {
+          if (n_subj == 32) continue;  // cannot exceed max_results subjects
+          subj[si] = (uint32_t)a.subject_id;
+          subj_n[si] = 0;
+          ++n_subj;
+        }
+        const uint32_t cnt = subj_n[si];
+        if ((int)cnt < max_one_subject && cnt < 4) {
+          // std::lower_bound on .position, step for step
+          uint32_t first = 0, len = cnt;
+          while (len > 0) {
+            const uint32_t half = len / 2, mid = first + half;
+            if (sp_pos[si][mid] < a.start_d) {
+              first = mid + 1;
+              len = len - half - 1;
+            } else {
+              len = half;
+            }
+          }
+          const uint32_t ins = first;
+          uint32_t it = first;
+          len = cnt - first;
+          uint32_t f2 = first;
+          while (len > 0) {
+            const uint32_t half = len / 2, mid = f2 + half;
+            if (sp_pos[si][mid] < a.end_d) {
+              f2 = mid + 1;
+              len = len - half - 1;
+            } else {
+              len = half;
+            }
+          }
+          bool ok = true;
+          for (; it != f2; ++it) {
+            if (is_contained(prev[sp_id[si][it]], a)) {
+              ok = false;
+              break;
+            }
+          }
+          if (ok) {
+            for (uint32_t t = cnt; t > ins; --t) {
+              sp_pos[si][t] = sp_pos[si][t - 1];
+              sp_id[si][t] = sp_id[si][t - 1];
+            }
+            sp_pos[si][ins] = a.start_q;
+            sp_id[si][ins] = n_out;
+            subj_n[si] = cnt + 1;
+            prev[n_out++] = a;
+          }
+        }
+      } else {
+        prev[n_out++] = a;
+      }
+    }
+    counts[qi] = n_out;
+  }
+}
+
+}  // namespace gzb
+
+using namespace gzb;
+
+// ===========================================================================
+struct gzb_engine {
+  int device = 0;
+  gzb_params params{};
+  DevParams dp{};
+  bool have_params = false;
+  DBuf matrix32;
+  // database
+  int32_t chunk_id = 0;
+  DBuf db_buf;
+  uint64_t db_len = 0;
+  DBuf db_offsets;
+  uint32_t nseq = 0;
+  DevIndex X;
+  std::vector<DBuf> index_bufs;
+  bool have_db = false;
+  // queries
+  DBuf q_buf, q_offsets, q_lengths, q_cut, q_trig;
+  uint64_t q_len = 0;
+  uint32_t nq = 0;
+  uint32_t max_qlen = 0;
+  DevLists L;
+  std::vector<DBuf> list_bufs;
+  bool have_queries = false;
+  // results
+  DBuf results, counts;
+  // scratch
+  DBuf tmp, hits, hits_alt, mwork, mcount, moffs, begin, kept, surv_off, slots, eq, ed, edir,
+      escore, merge_scratch, heap, ctr, misc, hits_copy;
+  int qbits = 1, dbits = 1;
+  uint32_t *spill = nullptr;
+  size_t spill_cap = 0;
+  uint32_t *gcounters = nullptr;
+  unsigned long long *gcells = nullptr;
+  int2 *band_pool = nullptr;
+  int band_wmask = 0;
+  uint64_t hit_cap = 1ull << 22, mwork_cap = 1ull << 22;
+  gzb_counters counters{};
+  float stage_ms[6] = {0, 0, 0, 0, 0, 0};
+  cudaEvent_t ev[7] = {};
+};
+
+namespace {
+
+int bits_for(uint64_t v) {  // bits to hold values in [0, v]
+  int b = 1;
+  while (b < 64 && (v >> b) != 0) ++b;
+  return b;
+}
+
+// CUB wrappers using the engine's growable temp buffer
+int sort_keys_u64(gzb_engine *e, uint64_t *keys, uint64_t *alt, uint64_t n, int end_bit,
+                  cudaStream_t s, uint64_t **result) {
+  cub::DoubleBuffer<uint64_t> db(keys, alt);
+  size_t tb = 0;
+  GZB_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tb, db, (int64_t)n, 0, end_bit, s));
+  GZB_TRY(e->tmp.ensure(tb));
+  GZB_CUDA(cub::DeviceRadixSort::SortKeys(e->tmp.p, tb, db, (int64_t)n, 0, end_bit, s));
+  *result = db.Current();
+  return GZB_OK;
+}
+
+int select_flagged_index(gzb_engine *e, const uint8_t *flags, uint64_t n, uint32_t *out,
+                         uint64_t *n_out, cudaStream_t s) {
+  // indices i with flags[i] != 0, in order
+  GZB_TRY(e->misc.ensure(8));
+  thrust::counting_iterator<uint32_t> it(0);
+  size_t tb = 0;
+  GZB_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, it, flags, out, e->misc.as<uint64_t>(),
+                                      (int64_t)n, s));
+  GZB_TRY(e->tmp.ensure(tb));
+  GZB_CUDA(cub::DeviceSelect::Flagged(e->tmp.p, tb, it, flags, out, e->misc.as<uint64_t>(),
+                                      (int64_t)n, s));
+  uint64_t cnt = 0;
+  GZB_CUDA(cudaMemcpyAsync(&cnt, e->misc.p, 8, cudaMemcpyDeviceToHost, s));
+  GZB_CUDA(cudaStreamSynchronize(s));
+  *n_out = cnt;
+  return GZB_OK;
+}
+
+template <class T>
+int select_flagged(gzb_engine *e, const T *in, const uint8_t *flags, uint64_t n, T *out,
+                   uint64_t *n_out, cudaStream_t s) {
+  GZB_TRY(e->misc.ensure(8));
+  size_t tb = 0;
+  GZB_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, in, flags, out, e->misc.as<uint64_t>(),
+                                      (int64_t)n, s));
+  GZB_TRY(e->tmp.ensure(tb));
+  GZB_CUDA(cub::DeviceSelect::Flagged(e->tmp.p, tb, in, flags, out, e->misc.as<uint64_t>(),
+                                      (int64_t)n, s));
+  uint64_t cnt = 0;
+  GZB_CUDA(cudaMemcpyAsync(&cnt, e->misc.p, 8, cudaMemcpyDeviceToHost, s));
+  GZB_CUDA(cudaStreamSynchronize(s));
+  *n_out = cnt;
+  return GZB_OK;
+}
+
+template <class TIn, class TOut>
+int exclusive_sum(gzb_engine *e, const TIn *in, TOut *out, uint64_t n, cudaStream_t s) {
+  size_t tb = 0;
+  GZB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, in, out, (int64_t)n, s));
+  GZB_TRY(e->tmp.ensure(tb));
+  GZB_CUDA(cub::DeviceScan::ExclusiveSum(e->tmp.p, tb, in, out, (int64_t)n, s));
+  return GZB_OK;
+}
+
+int upload_padded(DBuf &buf, const uint8_t *codes, uint64_t len, uint8_t delim,
+                  cudaStream_t s) {
+  GZB_TRY(buf.ensure(len + 2 * kPad));
+  GZB_CUDA(cudaMemsetAsync(buf.p, delim, len + 2 * kPad, s));
+  GZB_CUDA(cudaMemcpyAsync((uint8_t *)buf.p + kPad, codes, len, cudaMemcpyHostToDevice, s));
+  return GZB_OK;
+}
+
+template <class T>
+int upload(DBuf &buf, const T *h, uint64_t n, cudaStream_t s) {
+  GZB_TRY(buf.ensure(sizeof(T) * (n ? n : 1)));
+  if (n) GZB_CUDA(cudaMemcpyAsync(buf.p, h, sizeof(T) * n, cudaMemcpyHostToDevice, s));
+  return GZB_OK;
+}
+
+int build_csr(gzb_engine *e, const uint64_t *pairs, uint64_t n, uint32_t **keys,
+              uint32_t **offsets, uint32_t **values, uint64_t *nkeys, int slot,
+              cudaStream_t s) {
+  DBuf &flags = e->index_bufs[slot];
+  DBuf &starts = e->index_bufs[slot + 1];
+  DBuf &kbuf = e->index_bufs[slot + 2];
+  DBuf &obuf = e->index_bufs[slot + 3];
+  DBuf &vbuf = e->index_bufs[slot + 4];
+  GZB_TRY(flags.ensure(n + 1));
+  GZB_TRY(starts.ensure(4 * (n + 1)));
+  if (n) {
+    key_start_flags<<<grid1(n, 256), 256, 0, s>>>(pairs, n, flags.as<uint8_t>());
+    GZB_CUDA(cudaGetLastError());
+  }
+  uint64_t nseg = 0;
+  if (n) GZB_TRY(select_flagged_index(e, flags.as<uint8_t>(), n, starts.as<uint32_t>(), &nseg, s));
+  GZB_TRY(kbuf.ensure(4 * (nseg + 1)));
+  GZB_TRY(obuf.ensure(4 * (nseg + 1)));
+  GZB_TRY(vbuf.ensure(4 * (n + 1)));
+  csr_fill<<<grid1(n + nseg + 1, 256), 256, 0, s>>>(pairs, n, starts.as<uint32_t>(), nseg,
+                                                      kbuf.as<uint32_t>(), obuf.as<uint32_t>(),
+                                                      vbuf.as<uint32_t>());
+  GZB_CUDA(cudaGetLastError());
+  *keys = kbuf.as<uint32_t>();
+  *offsets = obuf.as<uint32_t>();
+  *values = vbuf.as<uint32_t>();
+  *nkeys = nseg;
+  return GZB_OK;
+}
+
+int check_engine(gzb_engine *e) {
+  GZB_CHECK(e, GZB_ERR_INVALID, "null engine");
+  GZB_CUDA(cudaSetDevice(e->device));
+  return GZB_OK;
+}
+
+}  // namespace
+
+extern "C" int gzb_engine_create(int device, gzb_engine **out) {
+  GZB_CHECK(out, GZB_ERR_INVALID, "null output handle");
+  int ndev = 0;
+  GZB_CUDA(cudaGetDeviceCount(&ndev));
+  GZB_CHECK(device >= 0 && device < ndev, GZB_ERR_INVALID, "no CUDA device %d", device);
+  GZB_CUDA(cudaSetDevice(device));
+  gzb_engine *e = new (std::nothrow) gzb_engine();
+  GZB_CHECK(e, GZB_ERR_NOMEM, "host allocation failed");
+  e->device = device;
+  e->index_bufs.resize(40);
+  e->list_bufs.resize(16);
+  cudaError_t err = cudaMalloc(&e->gcounters, 64);
+  if (err == cudaSuccess) err = cudaMalloc(&e->gcells, 8);
+  if (err == cudaSuccess) err = cudaMemset(e->gcounters, 0, 64);
+  if (err == cudaSuccess) err = cudaMemset(e->gcells, 0, 8);
+  for (int i = 0; i < 7 && err == cudaSuccess; ++i) err = cudaEventCreate(&e->ev[i]);
+  if (err != cudaSuccess) {
+    gzb_engine_destroy(e);
+    return cuda_error(err, "engine set-up", __FILE__, __LINE__);
+  }
+  *out = e;
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_destroy(gzb_engine *e) {
+  if (!e) return GZB_OK;
+  cudaSetDevice(e->device);
+  for (auto &b : e->index_bufs) b.release();
+  for (auto &b : e->list_bufs) b.release();
+  DBuf *all[] = {&e->matrix32, &e->db_buf, &e->db_offsets, &e->q_buf, &e->q_offsets,
+                 &e->q_lengths, &e->q_cut, &e->q_trig, &e->results, &e->counts,
+                 &e->tmp, &e->hits, &e->hits_alt, &e->mwork, &e->mcount, &e->moffs,
+                 &e->begin, &e->kept, &e->surv_off, &e->slots, &e->eq, &e->ed, &e->edir,
+                 &e->escore, &e->merge_scratch, &e->heap, &e->ctr, &e->misc,
+                 &e->hits_copy};
+  for (DBuf *b : all) b->release();
+  cudaFree(e->spill);
+  cudaFree(e->gcounters);
+  cudaFree(e->gcells);
+  cudaFree(e->band_pool);
+  for (int i = 0; i < 7; ++i)
+    if (e->ev[i]) cudaEventDestroy(e->ev[i]);
+  delete e;
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_set_params(gzb_engine *e, const gzb_params *p) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(p, GZB_ERR_INVALID, "null params");
+  GZB_CHECK(p->number_letters > 0 && p->number_letters < 32, GZB_ERR_INVALID,
+            "number_letters out of range");
+  GZB_CHECK(p->map_size > 0 && p->map_size <= 32, GZB_ERR_INVALID, "map_size out of range");
+  GZB_CHECK(p->subsequence_length >= 1 && p->subsequence_length <= 16, GZB_ERR_INVALID,
+            "subsequence_length must be 1..16");
+  GZB_CHECK(p->max_hash_length >= 1 && p->max_hash_length <= 16, GZB_ERR_INVALID,
+            "max_hash_length out of range");
+  GZB_CHECK(p->max_number_results >= 1 && p->max_number_results <= 32, GZB_ERR_INVALID,
+            "max_number_results must be 1..32");
+  GZB_CHECK(p->max_number_one_subject_results >= 1, GZB_ERR_INVALID,
+            "max_number_one_subject_results must be >= 1");
+  GZB_CHECK(p->gap_open >= 0 && p->gap_extension >= 0, GZB_ERR_INVALID, "negative gap");
+  e->params = *p;
+  DevParams &d = e->dp;
+  memset(&d, 0, sizeof(d));
+  d.delimiter = p->delimiter;
+  d.number_letters = p->number_letters;
+  d.map_size = p->map_size;
+  d.max_indexing_code = p->max_indexing_code;
+  d.seed_threshold = p->seed_threshold;
+  d.max_hash_length = p->max_hash_length;
+  d.min_hash_length = p->min_hash_length;
+  d.subsequence_length = p->subsequence_length;
+  d.max_member_distance = p->max_member_distance;
+  d.distance_threshold = p->distance_threshold;
+  int shift = 0;
+  for (uint32_t c = 1; c < (uint32_t)p->max_indexing_code + 1u; c <<= 1) ++shift;
+  d.shift = shift;
+  GZB_CHECK(shift * p->max_hash_length <= 32, GZB_ERR_INVALID, "hash does not fit 32 bits");
+  for (int i = 0; i < 32; ++i) {
+    const int r = p->hash_code_map[i];
+    d.hash_map[i] = (i < p->map_size && r <= p->max_indexing_code) ? (uint8_t)(r + 1) : 0;
+    d.sim_map[i] = p->similarity_code_map[i];
+    GZB_CHECK(i >= p->map_size || p->similarity_code_map[i] < 16, GZB_ERR_INVALID,
+              "similarity codes must be < 16");
+  }
+  for (int c = 0; c <= p->max_indexing_code && c < 31; ++c) d.code_scores[c + 1] = p->code_scores[c];
+  // 32x32 score matrix tile (rows = database code)
+  int32_t m[32 * 32];
+  memset(m, 0, sizeof(m));
+  for (int r = 0; r < p->number_letters; ++r)
+    for (int c = 0; c < p->number_letters; ++c)
+      m[r * 32 + c] = p->score_matrix[r * p->number_letters + c];
+  GZB_TRY(e->matrix32.ensure(sizeof(m)));
+  GZB_CUDA(cudaMemcpy(e->matrix32.p, m, sizeof(m), cudaMemcpyHostToDevice));
+  e->have_params = true;
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_set_database(gzb_engine *e, int32_t chunk_id, const uint8_t *codes,
+                                       uint64_t length, const uint32_t *offsets,
+                                       uint32_t number_sequences, void *stream) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(e->have_params, GZB_ERR_INVALID, "set_params first");
+  GZB_CHECK(codes && offsets && number_sequences > 0 && length > 0, GZB_ERR_INVALID,
+            "empty database");
+  GZB_CHECK(length < (1ull << 31), GZB_ERR_OVERFLOW,
+            "database chunk of %llu residues exceeds 2^31", (unsigned long long)length);
+  cudaStream_t s = (cudaStream_t)stream;
+  e->have_db = false;
+  e->chunk_id = chunk_id;
+  e->db_len = length;
+  e->nseq = number_sequences;
+  GZB_TRY(upload_padded(e->db_buf, codes, length, (uint8_t)e->params.delimiter, s));
+  GZB_TRY(upload(e->db_offsets, offsets, number_sequences + 1, s));
+  const uint8_t *db = e->db_buf.as<uint8_t>() + kPad;
+  std::vector<DBuf> &B = e->index_bufs;
+  // 1. (hash, position) pairs
+  DBuf &pairs = B[0], &pairs_alt = B[1];
+  GZB_TRY(pairs.ensure(8 * (length + 1)));
+  GZB_TRY(pairs_alt.ensure(8 * (length + 1)));
+  GZB_TRY(e->ctr.ensure(64));
+  GZB_CUDA(cudaMemsetAsync(e->ctr.p, 0, 64, s));
+  db_pairs_kernel<<<grid1(length, 256, 148 * 64), 256, 0, s>>>(
+      e->dp, db, length, pairs.as<uint64_t>(), e->ctr.as<unsigned long long>());
+  GZB_CUDA(cudaGetLastError());
+  uint64_t np = 0;
+  GZB_CUDA(cudaMemcpyAsync(&np, e->ctr.p, 8, cudaMemcpyDeviceToHost, s));
+  GZB_CUDA(cudaStreamSynchronize(s));
+  uint64_t *sorted = nullptr;
+  GZB_TRY(sort_keys_u64(e, pairs.as<uint64_t>(), pairs_alt.as<uint64_t>(), np, 64, s, &sorted));
+  uint64_t *other = sorted == pairs.as<uint64_t>() ? pairs_alt.as<uint64_t>() : pairs.as<uint64_t>();
+  DevIndex &X = e->X;
+  X = DevIndex();
+  if (!e->params.clustering) {
+    GZB_TRY(build_csr(e, sorted, np, &X.nc_keys, &X.nc_offsets, &X.nc_values, &X.n_nc_keys, 10, s));
+    X.n_nc_values = np;
+    // empty representative / member indexes
+    GZB_TRY(B[20].ensure(16));
+    GZB_TRY(B[21].ensure(16));
+    GZB_CUDA(cudaMemsetAsync(B[20].p, 0, 16, s));
+    GZB_CUDA(cudaMemsetAsync(B[21].p, 0, 16, s));
+    X.rep_keys = B[20].as<uint32_t>();
+    X.rep_offsets = B[20].as<uint32_t>();
+    X.rep_cluster_ids = B[20].as<uint32_t>();
+    X.rep_positions = B[20].as<uint32_t>();
+    X.member_offsets = B[21].as<uint32_t>();
+    X.member_positions = B[21].as<uint32_t>();
+    GZB_CUDA(cudaStreamSynchronize(s));
+    e->have_db = true;
+    return GZB_OK;
+  }
+  // 2. clustering
+  DBuf &fstart = B[2], &state = B[3], &window = B[4], &bstart = B[5], &rep_of = B[6],
+       &mcount = B[7], &is_nc = B[8], &is_rep = B[9];
+  GZB_TRY(fstart.ensure(np + 1));
+  GZB_TRY(state.ensure(np + 1));
+  GZB_TRY(window.ensure(8 * (np + 1)));
+  GZB_TRY(bstart.ensure(4 * (np + 1)));
+  GZB_TRY(rep_of.ensure(4 * (np + 1)));
+  GZB_TRY(mcount.ensure(4 * (np + 1)));
+  GZB_TRY(is_nc.ensure(np + 1));
+  GZB_TRY(is_rep.ensure(np + 1));
+  DBuf &is_mem = B[30];
+  GZB_TRY(is_mem.ensure(np + 1));
+  db_entry_kernel<<<grid1(np, 256, 148 * 64), 256, 0, s>>>(
+      e->dp, db, sorted, np, fstart.as<uint8_t>(), state.as<uint8_t>(), window.as<uint64_t>());
+  GZB_CUDA(cudaGetLastError());
+  uint64_t nb = 0;
+  GZB_TRY(select_flagged_index(e, fstart.as<uint8_t>(), np, bstart.as<uint32_t>(), &nb, s));
+  cluster_kernel<<<grid1(nb * 32, 256, 148 * 16), 256, 0, s>>>(
+      bstart.as<uint32_t>(), nb, np, state.as<uint8_t>(), window.as<uint64_t>(),
+      rep_of.as<uint32_t>(), e->params.max_member_distance);
+  GZB_CUDA(cudaGetLastError());
+  GZB_CUDA(cudaMemsetAsync(mcount.p, 0, 4 * (np + 1), s));
+  member_count_kernel<<<grid1(np, 256), 256, 0, s>>>(state.as<uint8_t>(), rep_of.as<uint32_t>(),
+                                                      np, mcount.as<uint32_t>());
+  GZB_CUDA(cudaGetLastError());
+  classify_kernel<<<grid1(np, 256), 256, 0, s>>>(state.as<uint8_t>(), mcount.as<uint32_t>(), np,
+                                                  is_nc.as<uint8_t>(), is_rep.as<uint8_t>(),
+                                                  is_mem.as<uint8_t>());
+  GZB_CUDA(cudaGetLastError());
+  // residual index
+  uint64_t nnc = 0;
+  GZB_TRY(select_flagged(e, sorted, is_nc.as<uint8_t>(), np, other, &nnc, s));
+  GZB_TRY(build_csr(e, other, nnc, &X.nc_keys, &X.nc_offsets, &X.nc_values, &X.n_nc_keys, 10, s));
+  X.n_nc_values = nnc;
+  GZB_CUDA(cudaStreamSynchronize(s));
+  // representatives (order kept: hash, then position)
+  uint64_t nrep = 0;
+  GZB_TRY(select_flagged(e, sorted, is_rep.as<uint8_t>(), np, other, &nrep, s));
+  uint32_t *rk, *ro, *rv;
+  uint64_t nrk = 0;
+  GZB_TRY(build_csr(e, other, nrep, &rk, &ro, &rv, &nrk, 15, s));
+  X.rep_keys = rk;
+  X.rep_offsets = ro;
+  X.rep_positions = rv;
+  X.n_rep_keys = nrk;
+  X.n_reps = nrep;
+  DBuf &rep_entries = B[22], &cid_of_entry = B[23], &cids = B[24];
+  GZB_TRY(rep_entries.ensure(4 * (nrep + 1)));
+  GZB_TRY(cid_of_entry.ensure(4 * (np + 1)));
+  GZB_TRY(cids.ensure(4 * (nrep + 1)));
+  uint64_t tmpn = 0;
+  GZB_TRY(select_flagged_index(e, is_rep.as<uint8_t>(), np, rep_entries.as<uint32_t>(), &tmpn, s));
+  scatter_cluster_ids<<<grid1(nrep, 256), 256, 0, s>>>(rep_entries.as<uint32_t>(), nrep,
+                                                        cid_of_entry.as<uint32_t>(),
+                                                        cids.as<uint32_t>());
+  GZB_CUDA(cudaGetLastError());
+  X.rep_cluster_ids = cids.as<uint32_t>();
+  // members grouped by cluster, position order inside
+  DBuf &mem_entries = B[25], &mpairs = B[26], &mpairs_alt = B[27], &mcnt = B[28],
+       &moff = B[29], &mpos = B[31];
+  GZB_TRY(mem_entries.ensure(4 * (np + 1)));
+  uint64_t nm = 0;
+  GZB_TRY(select_flagged_index(e, is_mem.as<uint8_t>(), np, mem_entries.as<uint32_t>(), &nm, s));
+  GZB_TRY(mpairs.ensure(8 * (nm + 1)));
+  GZB_TRY(mpairs_alt.ensure(8 * (nm + 1)));
+  GZB_TRY(mcnt.ensure(4 * (nrep + 1)));
+  GZB_TRY(moff.ensure(4 * (nrep + 2)));
+  GZB_TRY(mpos.ensure(4 * (nm + 1)));
+  GZB_CUDA(cudaMemsetAsync(mcnt.p, 0, 4 * (nrep + 1), s));
+  member_pairs_kernel<<<grid1(nm, 256), 256, 0, s>>>(mem_entries.as<uint32_t>(), nm,
+                                                      rep_of.as<uint32_t>(),
+                                                      cid_of_entry.as<uint32_t>(), sorted,
+                                                      mpairs.as<uint64_t>(), mcnt.as<uint32_t>());
+  GZB_CUDA(cudaGetLastError());
+  uint64_t *msorted = nullptr;
+  GZB_TRY(sort_keys_u64(e, mpairs.as<uint64_t>(), mpairs_alt.as<uint64_t>(), nm, 64, s, &msorted));
+  low32<<<grid1(nm, 256), 256, 0, s>>>(msorted, nm, mpos.as<uint32_t>());
+  GZB_CUDA(cudaGetLastError());
+  GZB_TRY(exclusive_sum(e, mcnt.as<uint32_t>(), moff.as<uint32_t>(), nrep + 1, s));
+  X.member_offsets = moff.as<uint32_t>();
+  X.member_positions = mpos.as<uint32_t>();
+  X.n_members = nm;
+  GZB_CUDA(cudaStreamSynchronize(s));
+  e->have_db = true;
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_set_queries(gzb_engine *e, const uint8_t *codes, uint64_t length,
+                                      const uint32_t *offsets, const uint32_t *lengths,
+                                      uint32_t number_queries, const int32_t *cutoffs,
+                                      const int32_t *triggers, void *stream) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(e->have_params, GZB_ERR_INVALID, "set_params first");
+  GZB_CHECK(codes && offsets && lengths && cutoffs && triggers && number_queries > 0,
+            GZB_ERR_INVALID, "empty query set");
+  GZB_CHECK(length < (1ull << 31), GZB_ERR_OVERFLOW, "query buffer exceeds 2^31 residues");
+  cudaStream_t s = (cudaStream_t)stream;
+  e->have_queries = false;
+  uint32_t maxl = 0;
+  for (uint32_t i = 0; i < number_queries; ++i) {
+    GZB_CHECK(lengths[i] >= 2 && (uint64_t)offsets[i] + lengths[i] <= length, GZB_ERR_INVALID,
+              "query %u outside the buffer", i);
+    GZB_CHECK(i == 0 || offsets[i] >= offsets[i - 1], GZB_ERR_INVALID,
+              "query offsets must be non-decreasing");
+    maxl = std::max(maxl, lengths[i]);
+  }
+  e->nq = number_queries;
+  e->q_len = length;
+  e->max_qlen = maxl;
+  GZB_TRY(upload_padded(e->q_buf, codes, length, (uint8_t)e->params.delimiter, s));
+  GZB_TRY(upload(e->q_offsets, offsets, number_queries, s));
+  GZB_TRY(upload(e->q_lengths, lengths, number_queries, s));
+  GZB_TRY(upload(e->q_cut, cutoffs, number_queries, s));
+  GZB_TRY(upload(e->q_trig, triggers, number_queries, s));
+  std::vector<DBuf> &B = e->list_bufs;
+  DBuf &keys = B[0], &alt = B[1];
+  GZB_TRY(keys.ensure(8 * (length + 1)));
+  GZB_TRY(alt.ensure(8 * (length + 1)));
+  GZB_TRY(e->ctr.ensure(64));
+  GZB_CUDA(cudaMemsetAsync(e->ctr.p, 0, 8, s));
+  query_entries_kernel<<<grid1(number_queries, 128), 128, 0, s>>>(
+      e->dp, e->q_buf.as<uint8_t>() + kPad, e->q_offsets.as<uint32_t>(),
+      e->q_lengths.as<uint32_t>(), number_queries, keys.as<uint64_t>(),
+      e->ctr.as<unsigned long long>(), length + 1);
+  GZB_CUDA(cudaGetLastError());
+  uint64_t n = 0;
+  GZB_CUDA(cudaMemcpyAsync(&n, e->ctr.p, 8, cudaMemcpyDeviceToHost, s));
+  GZB_CUDA(cudaStreamSynchronize(s));
+  uint64_t *sorted = nullptr;
+  GZB_TRY(sort_keys_u64(e, keys.as<uint64_t>(), alt.as<uint64_t>(), n, 64, s, &sorted));
+  DBuf &flags = B[2], &starts = B[3];
+  GZB_TRY(flags.ensure(n + 1));
+  GZB_TRY(starts.ensure(4 * (n + 1)));
+  uint64_t nl = 0;
+  if (n) {
+    key_start_flags<<<grid1(n, 256), 256, 0, s>>>(sorted, n, flags.as<uint8_t>());
+    GZB_CUDA(cudaGetLastError());
+    GZB_TRY(select_flagged_index(e, flags.as<uint8_t>(), n, starts.as<uint32_t>(), &nl, s));
+  }
+  DevLists &L = e->L;
+  L = DevLists();
+  DBuf *bufs[] = {&B[4], &B[5], &B[6], &B[7], &B[8], &B[9], &B[10], &B[11], &B[12], &B[13]};
+  GZB_TRY(B[4].ensure(4 * (nl + 1)));   // hash
+  GZB_TRY(B[5].ensure(4 * (nl + 2)));   // offsets
+  GZB_TRY(B[6].ensure(4 * (nl + 1)));   // nchk
+  GZB_TRY(B[7].ensure(4 * (nl + 1)));   // rep_begin
+  GZB_TRY(B[8].ensure(4 * (nl + 1)));   // rep_count
+  GZB_TRY(B[9].ensure(4 * (nl + 1)));   // nc_begin
+  GZB_TRY(B[10].ensure(4 * (nl + 1)));  // nc_count
+  GZB_TRY(B[11].ensure(8 * (nl + 2)));  // unit offsets
+  GZB_TRY(B[12].ensure(4 * (n + 1)));   // entry qid
+  GZB_TRY(B[13].ensure(4 * (n + 1)));   // entry cpos
+  (void)bufs;
+  L.hash = B[4].as<uint32_t>();
+  L.offsets = B[5].as<uint32_t>();
+  L.nchk = B[6].as<uint32_t>();
+  L.rep_begin = B[7].as<uint32_t>();
+  L.rep_count = B[8].as<uint32_t>();
+  L.nc_begin = B[9].as<uint32_t>();
+  L.nc_count = B[10].as<uint32_t>();
+  L.unit_offsets = B[11].as<uint64_t>();
+  L.entry_qid = B[12].as<uint32_t>();
+  L.entry_cpos = B[13].as<uint32_t>();
+  L.n_lists = nl;
+  L.n_entries = n;
+  if (n) {
+    list_fill_kernel<<<grid1(n + nl + 1, 256), 256, 0, s>>>(
+        sorted, n, starts.as<uint32_t>(), nl, e->q_offsets.as<uint32_t>(), number_queries,
+        L.hash, L.offsets, L.nchk, L.entry_qid, L.entry_cpos);
+    GZB_CUDA(cudaGetLastError());
+  } else {
+    GZB_CUDA(cudaMemsetAsync(L.offsets, 0, 8, s));
+  }
+  // results of a new query set start empty
+  GZB_TRY(e->results.ensure(sizeof(gzb_result) * (uint64_t)number_queries *
+                            e->params.max_number_results));
+  GZB_TRY(e->counts.ensure(4 * (uint64_t)number_queries));
+  GZB_CUDA(cudaMemsetAsync(e->counts.p, 0, 4 * (uint64_t)number_queries, s));
+  GZB_CUDA(cudaStreamSynchronize(s));
+  e->have_queries = true;
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_reset_results(gzb_engine *e, void *stream) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(e->have_queries, GZB_ERR_INVALID, "no queries");
+  GZB_CUDA(cudaMemsetAsync(e->counts.p, 0, 4 * (uint64_t)e->nq, (cudaStream_t)stream));
+  return GZB_OK;
+}
+
+namespace {
+
+int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
+  (void)schedule;
+  uint64_t launches = 0;
+  DevLists &L = e->L;
+  const DevIndex &X = e->X;
+  const uint32_t nq = e->nq;
+  GZB_CUDA(cudaEventRecord(e->ev[0], s));
+  // ---- list lookup against this chunk's index
+  if (L.n_lists) {
+    GZB_TRY(e->list_bufs[14].ensure(8 * (L.n_lists + 1)));
+    uint64_t *unit_counts = e->list_bufs[14].as<uint64_t>();
+    list_lookup_kernel<<<grid1(L.n_lists, 256), 256, 0, s>>>(L, X, e->params.clustering,
+                                                              unit_counts);
+    GZB_CUDA(cudaGetLastError());
+    ++launches;
+    GZB_CUDA(cudaMemsetAsync(unit_counts + L.n_lists, 0, 8, s));
+    GZB_TRY(exclusive_sum(e, unit_counts, L.unit_offsets, L.n_lists + 1, s));
+    GZB_CUDA(cudaMemcpyAsync(&L.n_units, L.unit_offsets + L.n_lists, 8, cudaMemcpyDeviceToHost, s));
+    GZB_CUDA(cudaStreamSynchronize(s));
+  } else {
+    L.n_units = 0;
+  }
+  GZB_CUDA(cudaEventRecord(e->ev[1], s));
+  // ---- seed search + distance + ungapped with trigger
+  const int qbits = bits_for(e->max_qlen);
+  const int dbits = bits_for(e->db_len + 1);
+  const int nqbits = bits_for(nq);
+  GZB_CHECK(qbits + dbits + nqbits <= 64, GZB_ERR_OVERFLOW,
+            "hit key needs %d bits (queries %u, chunk %llu, longest query %u)",
+            qbits + dbits + nqbits, nq, (unsigned long long)e->db_len, e->max_qlen);
+  GZB_TRY(e->ctr.ensure(64));
+  uint64_t n_hits = 0, n_mwork = 0;
+  unsigned long long hctr[8];
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    GZB_TRY(e->hits.ensure(8 * e->hit_cap));
+    GZB_TRY(e->mwork.ensure(8 * e->mwork_cap));
+    GZB_CUDA(cudaMemsetAsync(e->ctr.p, 0, 64, s));
+    SeedArgs a;
+    a.p = e->dp;
+    a.L = L;
+    a.X = X;
+    a.q = e->q_buf.as<uint8_t>() + kPad;
+    a.db = e->db_buf.as<uint8_t>() + kPad;
+    a.q_offsets = e->q_offsets.as<uint32_t>();
+    a.cutoffs = e->q_cut.as<int32_t>();
+    a.triggers = e->q_trig.as<int32_t>();
+    a.matrix32 = e->matrix32.as<int32_t>();
+    a.clustering = e->params.clustering;
+    a.dbits = dbits;
+    a.qbits = qbits;
+    a.hits = e->hits.as<uint64_t>();
+    unsigned long long *c = e->ctr.as<unsigned long long>();
+    a.hit_count = c + 4;
+    a.hit_cap = e->hit_cap;
+    a.mwork = e->mwork.as<uint2>();
+    a.mwork_count = c + 5;
+    a.mwork_cap = e->mwork_cap;
+    a.ctr = c;
+    if (L.n_units) {
+      const uint64_t warps = (L.n_units + kUnitsPerWarp - 1) / kUnitsPerWarp;
+      seed_kernel<<<grid1(warps * 32, kSeedBlock, 148 * 16), kSeedBlock, 0, s>>>(a);
+      GZB_CUDA(cudaGetLastError());
+    ++launches;
+    }
+    GZB_CUDA(cudaMemcpyAsync(hctr, c, 64, cudaMemcpyDeviceToHost, s));
+    GZB_CUDA(cudaStreamSynchronize(s));
+    n_mwork = hctr[5];
+    if (n_mwork > e->mwork_cap) {
+      e->mwork_cap = n_mwork + n_mwork / 8 + 1024;
+      continue;
+    }
+    if (n_mwork) {
+      GZB_TRY(e->mcount.ensure(8 * (n_mwork + 1)));
+      GZB_TRY(e->moffs.ensure(8 * (n_mwork + 1)));
+      mwork_counts_kernel<<<grid1(n_mwork, 256), 256, 0, s>>>(
+          a.mwork, n_mwork, X.member_offsets, e->mcount.as<uint64_t>());
+      GZB_CUDA(cudaGetLastError());
+    ++launches;
+      GZB_CUDA(cudaMemsetAsync(e->mcount.as<uint64_t>() + n_mwork, 0, 8, s));
+      GZB_TRY(exclusive_sum(e, e->mcount.as<uint64_t>(), e->moffs.as<uint64_t>(), n_mwork + 1, s));
+      uint64_t total = 0;
+      GZB_CUDA(cudaMemcpyAsync(&total, e->moffs.as<uint64_t>() + n_mwork, 8,
+                               cudaMemcpyDeviceToHost, s));
+      GZB_CUDA(cudaStreamSynchronize(s));
+      if (total) {
+        const uint64_t warps = (total + kUnitsPerWarp - 1) / kUnitsPerWarp;
+        member_kernel<<<grid1(warps * 32, kSeedBlock, 148 * 16), kSeedBlock, 0, s>>>(
+            a, a.mwork, n_mwork, e->moffs.as<uint64_t>(), total);
+        GZB_CUDA(cudaGetLastError());
+    ++launches;
+      }
+      GZB_CUDA(cudaMemcpyAsync(hctr, c, 64, cudaMemcpyDeviceToHost, s));
+      GZB_CUDA(cudaStreamSynchronize(s));
+    }
+    n_hits = hctr[4];
+    if (n_hits > e->hit_cap) {
+      e->hit_cap = n_hits + n_hits / 8 + 1024;
+      continue;
+    }
+    break;
+  }
+  GZB_CHECK(n_hits <= e->hit_cap && n_mwork <= e->mwork_cap, GZB_ERR_OVERFLOW,
+            "seed buffers did not converge");
+  e->counters.distance_seeds = hctr[0];
+  e->counters.ungapped_steps = hctr[2];
+  e->counters.ungapped_seeds = hctr[1];
+  e->counters.ungapped_hits = n_hits;
+  // ---- sort hits by (query, database position, query position)
+  GZB_TRY(e->hits_alt.ensure(8 * (n_hits + 1)));
+  uint64_t *hits = e->hits.as<uint64_t>();
+  if (n_hits) {
+    uint64_t *sorted = nullptr;
+    GZB_TRY(sort_keys_u64(e, hits, e->hits_alt.as<uint64_t>(), n_hits,
+                          qbits + dbits + nqbits, s, &sorted));
+    hits = sorted;
+  }
+  GZB_TRY(e->hits_copy.ensure(8 * (n_hits + 1)));
+  if (n_hits)
+    GZB_CUDA(cudaMemcpyAsync(e->hits_copy.p, hits, 8 * n_hits, cudaMemcpyDeviceToDevice, s));
+  e->qbits = qbits;
+  e->dbits = dbits;
+  GZB_CUDA(cudaEventRecord(e->ev[2], s));
+  // ---- chain filter
+  GZB_TRY(e->begin.ensure(8 * (nq + 1)));
+  GZB_TRY(e->kept.ensure(4 * (nq + 1)));
+  GZB_TRY(e->surv_off.ensure(8 * (nq + 1)));
+  GZB_TRY(e->slots.ensure(8 * (e->q_len + nq + 1)));
+  uint64_t *begin = e->begin.as<uint64_t>();
+  uint32_t *kept = e->kept.as<uint32_t>();
+  uint64_t *surv_off = e->surv_off.as<uint64_t>();
+  hit_segments_kernel<<<grid1(nq + 1, 256), 256, 0, s>>>(hits, n_hits, nq, qbits + dbits, begin);
+  GZB_CUDA(cudaGetLastError());
+    ++launches;
+  chain_kernel<<<grid1(nq, 64), 64, 0, s>>>(
+      e->dp, e->q_buf.as<uint8_t>() + kPad, e->db_buf.as<uint8_t>() + kPad,
+      e->q_offsets.as<uint32_t>(), e->q_lengths.as<uint32_t>(), e->q_cut.as<int32_t>(),
+      e->matrix32.as<int32_t>(), nq, hits, begin, qbits, dbits, e->slots.as<uint2>(), kept);
+  GZB_CUDA(cudaGetLastError());
+    ++launches;
+  GZB_CUDA(cudaMemsetAsync(kept + nq, 0, 4, s));
+  GZB_TRY(exclusive_sum(e, kept, surv_off, nq + 1, s));
+  uint64_t n_surv = 0;
+  GZB_CUDA(cudaMemcpyAsync(&n_surv, surv_off + nq, 8, cudaMemcpyDeviceToHost, s));
+  GZB_CUDA(cudaStreamSynchronize(s));
+  e->counters.chained_hits = n_surv;
+  GZB_CUDA(cudaEventRecord(e->ev[3], s));
+  // ---- gapped extension, both sides
+  const uint64_t next = 2 * n_surv;
+  GZB_TRY(e->eq.ensure(4 * (next + 1)));
+  GZB_TRY(e->ed.ensure(4 * (next + 1)));
+  GZB_TRY(e->edir.ensure(next + 1));
+  GZB_TRY(e->escore.ensure(4 * (next + 1)));
+  if (n_surv) {
+    build_ext_kernel<<<grid1(nq, 128), 128, 0, s>>>(
+        hits, begin, kept, surv_off, nq, e->q_offsets.as<uint32_t>(), qbits, dbits, n_surv,
+        e->eq.as<uint32_t>(), e->ed.as<uint32_t>(), e->edir.as<uint8_t>());
+    GZB_CUDA(cudaGetLastError());
+    ++launches;
+    GZB_CUDA(cudaMemsetAsync(e->gcells, 0, 8, s));
+    GappedJob job;
+    job.query = e->q_buf.as<uint8_t>() + kPad;
+    job.db = e->db_buf.as<uint8_t>() + kPad;
+    job.delim = e->params.delimiter;
+    job.gap_open = e->params.gap_open;
+    job.gap_ext = e->params.gap_extension;
+    job.cutoff = e->params.gapped_cutoff;
+    uint32_t fb = 0;
+    GZB_TRY(run_gapped(job, e->matrix32.as<int32_t>(), 32, 32, next, nullptr, 0,
+                       e->edir.as<uint8_t>(), e->eq.as<uint32_t>(), e->ed.as<uint32_t>(),
+                       e->escore.as<int32_t>(), &e->spill, &e->spill_cap, e->gcounters,
+                       e->gcells, &e->band_pool, &e->band_wmask, s, &fb));
+    unsigned long long cells = 0;
+    GZB_CUDA(cudaMemcpyAsync(&cells, e->gcells, 8, cudaMemcpyDeviceToHost, s));
+    GZB_CUDA(cudaStreamSynchronize(s));
+    e->counters.gapped_cells = cells;
+    e->counters.gapped_fallbacks = fb;
+    launches += 3;
+  } else {
+    e->counters.gapped_cells = 0;
+    e->counters.gapped_fallbacks = 0;
+  }
+  e->counters.gapped_extensions = next;
+  GZB_CUDA(cudaEventRecord(e->ev[4], s));
+  // ---- top-b merge
+  if (n_surv) {
+    GZB_TRY(e->merge_scratch.ensure(sizeof(gzb_result) * (n_surv + 1)));
+    GZB_TRY(e->heap.ensure(4 * (n_surv + 1)));
+    merge_kernel<<<grid1(nq, 64), 64, 0, s>>>(
+        nq, hits, begin, kept, surv_off, n_surv, e->eq.as<uint32_t>(), e->ed.as<uint32_t>(),
+        e->escore.as<int32_t>(), e->q_offsets.as<uint32_t>(), qbits, dbits,
+        e->db_offsets.as<uint32_t>(), e->nseq, (uint32_t)e->db_len, e->chunk_id,
+        e->params.max_number_results, e->params.max_number_one_subject_results,
+        e->merge_scratch.as<gzb_result>(), e->heap.as<uint32_t>(), e->results.as<gzb_result>(),
+        e->counts.as<uint32_t>());
+    GZB_CUDA(cudaGetLastError());
+    ++launches;
+  }
+  GZB_CUDA(cudaEventRecord(e->ev[5], s));
+  GZB_CUDA(cudaEventSynchronize(e->ev[5]));
+  float t[6];
+  for (int i = 0; i < 5; ++i) GZB_CUDA(cudaEventElapsedTime(&t[i], e->ev[i], e->ev[i + 1]));
+  GZB_CUDA(cudaEventElapsedTime(&t[5], e->ev[0], e->ev[5]));
+  for (int i = 0; i < 6; ++i) e->stage_ms[i] = t[i];
+  e->counters.kernel_launches = launches;
+  return GZB_OK;
+}
+
+}  // namespace
+
+extern "C" int gzb_engine_presearch(gzb_engine *e, int schedule, void *stream) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(e->have_db && e->have_queries, GZB_ERR_INVALID,
+            "set_database and set_queries first");
+  GZB_CHECK(schedule == GZB_SCHEDULE_PLAIN || schedule == GZB_SCHEDULE_BATCHED,
+            GZB_ERR_INVALID, "unknown schedule %d", schedule);
+  GZB_CHECK(e->params.max_number_one_subject_results <= 4, GZB_ERR_INVALID,
+            "max_number_one_subject_results above 4 is not supported");
+  return presearch_impl(e, schedule, (cudaStream_t)stream);
+}
+
+extern "C" int gzb_engine_get_results(gzb_engine *e, uint32_t *counts, gzb_result *results,
+                                      void *stream) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(e->have_queries && counts && results, GZB_ERR_INVALID, "no results");
+  cudaStream_t s = (cudaStream_t)stream;
+  GZB_CUDA(cudaMemcpyAsync(counts, e->counts.p, 4 * (uint64_t)e->nq, cudaMemcpyDeviceToHost, s));
+  GZB_CUDA(cudaMemcpyAsync(results, e->results.p,
+                           sizeof(gzb_result) * (uint64_t)e->nq * e->params.max_number_results,
+                           cudaMemcpyDeviceToHost, s));
+  GZB_CUDA(cudaStreamSynchronize(s));
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_get_counters(gzb_engine *e, gzb_counters *out) {
+  GZB_CHECK(e && out, GZB_ERR_INVALID, "null argument");
+  *out = e->counters;
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_get_stage_ms(gzb_engine *e, float *ms6) {
+  GZB_CHECK(e && ms6, GZB_ERR_INVALID, "null argument");
+  for (int i = 0; i < 6; ++i) ms6[i] = e->stage_ms[i];
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_get_hits(gzb_engine *e, uint32_t *qid, uint32_t *qpos, uint32_t *dpos,
+                                   uint64_t capacity, uint64_t *count, void *stream) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(count, GZB_ERR_INVALID, "null count");
+  const uint64_t n = e->counters.ungapped_hits;
+  *count = n;
+  const uint64_t c = std::min(n, capacity);
+  if (c == 0 || !qid || !qpos || !dpos) return GZB_OK;
+  std::vector<uint64_t> keys(c);
+  cudaStream_t s = (cudaStream_t)stream;
+  GZB_CUDA(cudaMemcpyAsync(keys.data(), e->hits_copy.p, 8 * c, cudaMemcpyDeviceToHost, s));
+  GZB_CUDA(cudaStreamSynchronize(s));
+  const uint64_t qmask = (1ull << e->qbits) - 1, dmask = (1ull << e->dbits) - 1;
+  for (uint64_t i = 0; i < c; ++i) {
+    qpos[i] = (uint32_t)(keys[i] & qmask);
+    dpos[i] = (uint32_t)((keys[i] >> e->qbits) & dmask);
+    qid[i] = (uint32_t)(keys[i] >> (e->qbits + e->dbits));
+  }
+  return GZB_OK;
+}
+
+__global__ void entry_positions_kernel(const uint32_t *qid, const uint32_t *cpos, uint64_t n,
+                                       const uint32_t *q_offsets, uint32_t *out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = cpos[i] - q_offsets[qid[i]];
+}
+
+extern "C" int gzb_engine_get_list_array(gzb_engine *e, int which, uint32_t *out,
+                                         uint64_t capacity, uint64_t *count, void *stream) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(e->have_queries && count, GZB_ERR_INVALID, "no queries");
+  const DevLists &L = e->L;
+  cudaStream_t s = (cudaStream_t)stream;
+  const uint32_t *src = nullptr;
+  uint64_t n = 0;
+  switch (which) {
+    case 0: src = L.hash; n = L.n_lists; break;
+    case 1: src = L.offsets; n = L.n_lists + 1; break;
+    case 2: src = L.nchk; n = L.n_lists; break;
+    case 3: src = L.entry_qid; n = L.n_entries; break;
+    case 4: {
+      n = L.n_entries;
+      GZB_TRY(e->list_bufs[15].ensure(4 * (n + 1)));
+      if (n) {
+        entry_positions_kernel<<<grid1(n, 256), 256, 0, s>>>(L.entry_qid, L.entry_cpos, n,
+                                                             e->q_offsets.as<uint32_t>(),
+                                                             e->list_bufs[15].as<uint32_t>());
+        GZB_CUDA(cudaGetLastError());
+      }
+      src = e->list_bufs[15].as<uint32_t>();
+      break;
+    }
+    default: return set_error(GZB_ERR_INVALID, "unknown list array %d", which);
+  }
+  *count = n;
+  if (out && n) {
+    const uint64_t c = std::min(n, capacity);
+    GZB_CUDA(cudaMemcpyAsync(out, src, 4 * c, cudaMemcpyDeviceToHost, s));
+    GZB_CUDA(cudaStreamSynchronize(s));
+  }
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_get_index_array(gzb_engine *e, int which, uint32_t *out,
+                                          uint64_t capacity, uint64_t *count, void *stream) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(e->have_db && count, GZB_ERR_INVALID, "no database");
+  const DevIndex &X = e->X;
+  const uint32_t *src = nullptr;
+  uint64_t n = 0;
+  switch (which) {
+    case 0: src = X.nc_keys; n = X.n_nc_keys; break;
+    case 1: src = X.nc_offsets; n = X.n_nc_keys + 1; break;
+    case 2: src = X.nc_values; n = X.n_nc_values; break;
+    case 3: src = X.rep_keys; n = X.n_rep_keys; break;
+    case 4: src = X.rep_offsets; n = X.n_rep_keys + 1; break;
+    case 5: src = X.rep_cluster_ids; n = X.n_reps; break;
+    case 6: src = X.rep_positions; n = X.n_reps; break;
+    case 7: src = X.member_offsets; n = X.n_reps + 1; break;
+    case 8: src = X.member_positions; n = X.n_members; break;
+    default: return set_error(GZB_ERR_INVALID, "unknown index array %d", which);
+  }
+  *count = n;
+  if (out && n) {
+    const uint64_t c = std::min(n, capacity);
+    cudaStream_t s = (cudaStream_t)stream;
+    GZB_CUDA(cudaMemcpyAsync(out, src, 4 * c, cudaMemcpyDeviceToHost, s));
+    GZB_CUDA(cudaStreamSynchronize(s));
+  }
+  return GZB_OK;
+}

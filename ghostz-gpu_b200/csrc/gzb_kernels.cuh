@@ -1,0 +1,624 @@
+// gzb_kernels.cuh -- device kernels of the presearch engine (sm_100a).
+//
+// All arithmetic is int32 and reproduces the CPU reference bit for bit:
+//   * ungapped X-drop  : UngappedExtender::ExtendOneSideScoreOnly
+//                        (src/ungapped_extender.h:34-82)
+//   * distance         : DistanceCalculator::CalculateDistance
+//                        (src/distance_calculator.cpp:35-54)
+//   * gapped X-drop    : GappedExtender::ExtendOneSideScoreOnly
+//                        (src/gapped_extender.cpp:306-471)
+//
+// Gapped extension, one warp per extension.  The reference walks database
+// rows in order and, inside a row, evaluates query columns left to right,
+// pruning a cell when the running maximum minus its score exceeds the X-drop
+// and resetting the horizontal-gap chain at pruned cells.  The warp evaluates
+// 32 consecutive columns of a row at once and stays exact:
+//   - a pruned cell's score is always below the running maximum, so the
+//     running maximum before a cell equals the plain prefix maximum of the raw
+//     scores of the row (one warp max-scan);
+//   - without the reset, the horizontal gap F obeys
+//     F[c+1] = max(G[c] - gap_init, F[c] - gap_ext)  (G = max(diag, vertical)),
+//     a max-plus prefix scan.  Any value the reset would have removed is
+//     below (running max - X-drop), so it can neither keep a cell alive nor
+//     grow the band; decisions and stored values are unchanged as long as
+//     the initial score -1024 itself lies below every live threshold, i.e.
+//     X-drop < 1024.  X-drops of at least 2^30 can prune nothing and are
+//     exact as well.  Any other X-drop runs the serial fallback.
+//   - band edges (array_start / array_end / the sentinel column) follow the
+//     reference's rules, including its use of the old right edge when the
+//     band shrinks (src/gapped_extender.cpp:449-465).
+// The band lives in a per-warp circular buffer of W columns in shared
+// memory; an extension whose band would outgrow it is handed to the
+// fallback kernel, which keeps the band in a global circular buffer.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gzb {
+
+constexpr int kInitScore = -(1 << 10);  // src/gapped_extender.h:40
+constexpr int kNegBig = -(1 << 29);
+constexpr int kMatrixStride = 32;       // shared-memory score matrix row
+
+__device__ __forceinline__ int imax(int a, int b) { return a > b ? a : b; }
+__device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
+
+// Loads a score matrix with row stride `stride` into a 32x32 shared tile.
+__device__ __forceinline__ void load_matrix(int *sm, const int32_t *m,
+                                            int number_letters, int stride) {
+  for (int i = threadIdx.x; i < kMatrixStride * kMatrixStride; i += blockDim.x) {
+    int r = i / kMatrixStride, c = i % kMatrixStride;
+    sm[i] = (r < number_letters && c < number_letters) ? m[r * stride + c] : 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Ungapped one-side X-drop from s0[0]/s1[0] (query/database), stepping by
+// inc.  Returns the best prefix sum; stops early once it exceeds
+// stop_above (the caller only needs "> trigger").  *steps counts residue
+// pairs examined.
+__device__ __forceinline__ int ungapped_side(const uint8_t *__restrict__ s0,
+                                             const uint8_t *__restrict__ s1,
+                                             int inc, int delim, const int *sm,
+                                             int cutoff, int stop_above,
+                                             int *steps) {
+  int best = 0, run = 0, pos = 0, n = 0;
+  for (;;) {
+    const int a = s0[pos], b = s1[pos];
+    if (a == delim || b == delim) break;
+    run += sm[b * kMatrixStride + a];
+    pos += inc;
+    ++n;
+    if (run > 0) {
+      best += run;
+      run = 0;
+      if (best > stop_above) break;
+    } else if (run <= -cutoff) {
+      break;
+    }
+  }
+  *steps += n;
+  return best;
+}
+
+// Ungapped extension with trigger (SeedSearcher::UngappedExtend,
+// src/seed_searcher.h:133-158): true when the summed score exceeds trigger.
+__device__ __forceinline__ bool ungapped_hit(const uint8_t *q, const uint8_t *d,
+                                             int delim, const int *sm,
+                                             int cutoff, int trigger,
+                                             int *steps) {
+  int sum = ungapped_side(q - 1, d - 1, -1, delim, sm, cutoff, trigger, steps);
+  if (sum > trigger) return true;
+  sum += ungapped_side(q, d, 1, delim, sm, cutoff, trigger - sum, steps);
+  return sum > trigger;
+}
+
+// Reduced-alphabet mismatches over the L window centred on the seeds.
+__device__ __forceinline__ int window_distance(const uint8_t *q, const uint8_t *d,
+                                               int L, const uint8_t *map) {
+  const int half = L / 2;
+  int m = 0;
+  for (int i = 0; i < L; ++i) m += map[q[i - half]] != map[d[i - half]];
+  return m;
+}
+
+// ---------------------------------------------------------------------------
+// Gapped extension.
+struct GappedJob {
+  const uint8_t *query;     // concatenated queries
+  const uint8_t *db;        // database chunk
+  int delim, gap_open, gap_ext, cutoff;
+};
+
+struct GappedOut {
+  int score;
+  int pos0;  // best offset along the query (negative when reversed)
+  int pos1;  // best offset along the database
+  uint64_t cells;
+  bool overflow;
+};
+
+// Warp-cooperative first column >= c (band column numbering) whose query
+// residue is the delimiter, looking at most `limit` columns ahead; returns
+// c + limit when none is found.  Column c holds query residue (c-1)*inc.
+__device__ __forceinline__ int find_delimiter_column(const uint8_t *q0, int inc,
+                                                     int delim, int c,
+                                                     int limit) {
+  const int lane = threadIdx.x & 31;
+  for (int base = 0; base < limit; base += 32) {
+    const int k = base + lane;
+    bool is_delim = false;
+    if (k < limit) is_delim = q0[(c + k - 1) * inc] == delim;
+    const unsigned m = __ballot_sync(0xffffffffu, is_delim);
+    if (m) return c + base + __ffs(m) - 1;
+  }
+  return c + limit;
+}
+
+// One extension by one full warp.  `band` is a circular buffer of W int2
+// (x = best, y = best_gap) when W > 0; the caller guarantees exactness
+// conditions on the X-drop (see file comment).
+template <int W>
+__device__ GappedOut gapped_extend_warp(const GappedJob &job, const int *sm,
+                                        int2 *band, int wmask,
+                                        uint32_t qpos, uint32_t dpos,
+                                        bool reverse) {
+  const int lane = threadIdx.x & 31;
+  const int inc = reverse ? -1 : 1;
+  const int delim = job.delim;
+  const int ge = job.gap_ext;
+  const int gi = job.gap_open + job.gap_ext;
+  const int cutoff = job.cutoff;
+  const uint8_t *q0 = job.query + qpos;
+  const uint8_t *d0 = job.db + dpos;
+  GappedOut out;
+  out.score = 0;
+  out.pos0 = -inc;
+  out.pos1 = -inc;
+  out.cells = 0;
+  out.overflow = false;
+  if (q0[0] == delim || d0[0] == delim) return out;
+
+  // Row -1: horizontal gap run from column 1 while >= -cutoff
+  // (src/gapped_extender.cpp:345-364).
+  int k0;
+  if (-gi < -cutoff) {
+    k0 = 0;
+  } else if (ge == 0) {
+    k0 = 1 << 30;
+  } else {
+    long long kk = ((long long)cutoff - gi) / ge + 1;
+    k0 = kk > (1 << 30) ? (1 << 30) : (int)kk;
+  }
+  // stop at the delimiter
+  int col = find_delimiter_column(q0, inc, delim, 1, k0 > W ? W + 1 : k0);
+  if (col > W) {  // band [0, col) must fit the circular buffer
+    out.overflow = true;
+    return out;
+  }
+  const int init_cols = col - 1;  // columns 1..init_cols
+  for (int c = 1 + lane; c <= init_cols; c += 32) {
+    const int s = -gi - (c - 1) * ge;
+    band[c & wmask] = make_int2(s, s - gi);
+  }
+  if (lane == 0) band[0] = make_int2(0, -gi);
+  int bs = 0, be;
+  if (q0[(col - 1) * inc] != delim) {
+    if (col + 1 > W) {
+      out.overflow = true;
+      return out;
+    }
+    if (lane == 0) band[col & wmask] = make_int2(kInitScore, kInitScore);
+    be = col + 1;
+  } else {
+    be = col;
+  }
+  __syncwarp();
+
+  int maxs = 0, mp0 = -inc, mp1 = -inc;
+  uint64_t cells = 0;
+  for (int r = 0;; ++r) {
+    const int x = d0[r * inc];
+    if (x == delim) break;
+    const int *mrow = sm + x * kMatrixStride;
+    // column bs: vertical gap only (src/gapped_extender.cpp:397-408)
+    const int2 st0 = band[bs & wmask];
+    int diag = st0.x;
+    const int nb0 = (maxs - st0.y > cutoff) ? kInitScore : st0.y;
+    int F = nb0 - gi;
+    __syncwarp();
+    if (lane == 0) band[bs & wmask] = make_int2(nb0, st0.y - ge);
+    int M = maxs;
+    int first_kept = -1, last_kept = bs;
+    for (int cs = bs + 1; cs < be; cs += 32) {
+      const int c = cs + lane;
+      const bool active = c < be;
+      int2 st = make_int2(kInitScore, kInitScore);
+      int qres = 0;
+      if (active) {
+        st = band[c & wmask];
+        qres = q0[(c - 1) * inc];
+      }
+      int prev = __shfl_up_sync(0xffffffffu, st.x, 1);
+      if (lane == 0) prev = diag;
+      const int G = imax(prev + mrow[qres], st.y);
+      // F: exclusive max-plus scan of B(j) = G(j) - gi + (j+1)*ge
+      int P = active ? G - gi + (lane + 1) * ge : kNegBig;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, P, o);
+        if (lane >= o) P = imax(P, t);
+      }
+      int Pex = __shfl_up_sync(0xffffffffu, P, 1);
+      if (lane == 0) Pex = kNegBig;
+      const int Fl = imax(F, Pex) - lane * ge;
+      const int raw = imax(G, Fl);
+      // running maximum: inclusive prefix max of raw
+      int R = active ? raw : kNegBig;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, R, o);
+        if (lane >= o) R = imax(R, t);
+      }
+      const int Mrow = imax(M, R);
+      const bool pruned = (Mrow - raw > cutoff);
+      if (active) {
+        const int nb = pruned ? kInitScore : raw;
+        const int ng = pruned ? kInitScore : imax(raw - gi, st.y - ge);
+        band[c & wmask] = make_int2(nb, ng);
+      }
+      const int nact = imin(32, be - cs);
+      // new maximum: first column reaching the chunk maximum
+      const int cm = __shfl_sync(0xffffffffu, R, 31);
+      if (cm > M) {
+        const unsigned hitm = __ballot_sync(0xffffffffu, active && raw == cm);
+        const int l = __ffs(hitm) - 1;
+        maxs = cm;
+        mp0 = (cs + l - 1) * inc;
+        mp1 = r * inc;
+      }
+      const unsigned kept = __ballot_sync(0xffffffffu, active && !pruned);
+      if (kept) {
+        if (first_kept < 0) first_kept = cs + __ffs(kept) - 1;
+        last_kept = cs + 31 - __clz(kept);
+      }
+      // carries into the next chunk / the band-extension step
+      const int Plast = __shfl_sync(0xffffffffu, P, nact - 1);
+      F = imax(F, Plast) - nact * ge;
+      M = imax(M, cm);
+      diag = __shfl_sync(0xffffffffu, st.x, 31);
+      cells += (uint64_t)nact;
+    }
+    __syncwarp();
+    if (first_kept < 0) break;  // every cell pruned: array_start + 1 == array_end
+    bs = first_kept - 1;
+    bool edge_residue;
+    if (last_kept < be - 1) {
+      // shrink; the reference tests the residue of the old right edge
+      edge_residue = q0[(be - 1) * inc] != delim;
+      be = last_kept + 1;
+    } else {
+      // grow along the horizontal gap while F >= max - cutoff
+      int k;
+      const long long room = (long long)F - ((long long)maxs - cutoff);
+      if (room < 0) {
+        k = 0;
+      } else if (ge == 0) {
+        k = 1 << 30;
+      } else {
+        long long kk = room / ge + 1;
+        k = kk > (1 << 30) ? (1 << 30) : (int)kk;
+      }
+      if (k > 0) {
+        const int lim = (be + k - bs > W) ? (W - (be - bs) + 1) : k;
+        k = find_delimiter_column(q0, inc, delim, be, lim) - be;
+        if (be + k - bs > W) {
+          out.overflow = true;
+          return out;
+        }
+        for (int j = lane; j < k; j += 32) {
+          const int v = F - j * ge;
+          band[(be + j) & wmask] = make_int2(v, v - gi);
+        }
+        be += k;
+        cells += (uint64_t)k;
+      }
+      edge_residue = q0[(be - 1) * inc] != delim;
+    }
+    if (edge_residue) {
+      if (be + 1 - bs > W) {
+        out.overflow = true;
+        return out;
+      }
+      if (lane == 0) band[be & wmask] = make_int2(kInitScore, kInitScore);
+      ++be;
+    }
+    __syncwarp();
+  }
+  out.score = maxs;
+  out.pos0 = mp0;
+  out.pos1 = mp1;
+  out.cells = cells;
+  return out;
+}
+
+}  // namespace gzb
+
+namespace gzb {
+
+// Serial restatement of the same extension for one thread, with the band in
+// a circular global buffer of wmask+1 columns.  Exact for every X-drop; used
+// for extensions whose band outgrows the warp kernel's shared buffer and for
+// X-drops in [1024, 2^30).  Sets *too_long when the band would exceed the
+// buffer (the caller reports GZB_ERR_OVERFLOW).
+__device__ inline GappedOut gapped_extend_serial(const GappedJob &job,
+                                                 const int *sm, int2 *band,
+                                                 int wmask, uint32_t qpos,
+                                                 uint32_t dpos, bool reverse,
+                                                 bool *too_long) {
+  const int inc = reverse ? -1 : 1;
+  const int delim = job.delim;
+  const int ge = job.gap_ext;
+  const int gi = job.gap_open + job.gap_ext;
+  const int cutoff = job.cutoff;
+  const int W = wmask + 1;
+  const uint8_t *q0 = job.query + qpos;
+  const uint8_t *d0 = job.db + dpos;
+  GappedOut out;
+  out.score = 0;
+  out.pos0 = -inc;
+  out.pos1 = -inc;
+  out.cells = 0;
+  out.overflow = false;
+  *too_long = false;
+  if (q0[0] == delim || d0[0] == delim) return out;
+  int score = -gi;
+  int col = 1;
+  int p0 = 0;
+  band[0] = make_int2(0, -gi);
+  for (; q0[p0] != delim; ++col, p0 += inc) {
+    if (score < -cutoff) break;
+    if (col >= W) {
+      *too_long = true;
+      return out;
+    }
+    band[col & wmask] = make_int2(score, score - gi);
+    score -= ge;
+  }
+  int bs = 0, be;
+  if (q0[p0] != delim) {
+    if (col >= W) {
+      *too_long = true;
+      return out;
+    }
+    band[col & wmask] = make_int2(kInitScore, kInitScore);
+    be = col + 1;
+  } else {
+    be = col;
+  }
+  int maxs = 0, mp0 = -inc, mp1 = -inc;
+  uint64_t cells = 0;
+  for (int p1 = 0; d0[p1] != delim; p1 += inc) {
+    const int *mrow = sm + d0[p1] * kMatrixStride;
+    p0 = bs * inc;
+    int2 *c0 = &band[bs & wmask];
+    int diag = c0->x;
+    c0->x = (maxs - c0->y > cutoff) ? kInitScore : c0->y;
+    int row_gap = c0->x - gi;
+    c0->y -= ge;
+    int last = bs;
+    const int bs_row = bs;
+    for (int c = bs_row + 1; c < be; ++c, p0 += inc) {
+      int2 *cell = &band[c & wmask];
+      int s = diag + mrow[q0[p0]];
+      diag = cell->x;
+      const int vgap = cell->y;
+      ++cells;
+      if (s < vgap) s = vgap;
+      if (s < row_gap) s = row_gap;
+      if (maxs - s > cutoff) {
+        if (bs + 1 == c) ++bs;
+        cell->x = kInitScore;
+        cell->y = kInitScore;
+        row_gap = kInitScore;
+      } else {
+        last = c;
+        if (s > maxs) {
+          maxs = s;
+          mp0 = p0;
+          mp1 = p1;
+        }
+        cell->y = imax(s - gi, vgap - ge);
+        row_gap = imax(s - gi, row_gap - ge);
+        cell->x = s;
+      }
+    }
+    if (bs + 1 == be) break;
+    if (last < be - 1) {
+      be = last + 1;
+    } else {
+      while (row_gap >= maxs - cutoff && q0[p0] != delim) {
+        if (be - bs >= W) {
+          *too_long = true;
+          return out;
+        }
+        band[be & wmask] = make_int2(row_gap, row_gap - gi);
+        row_gap -= ge;
+        ++be;
+        p0 += inc;
+        ++cells;
+      }
+    }
+    if (q0[p0] != delim) {
+      if (be - bs >= W) {
+        *too_long = true;
+        return out;
+      }
+      band[be & wmask] = make_int2(kInitScore, kInitScore);
+      ++be;
+    }
+  }
+  out.score = maxs;
+  out.pos0 = mp0;
+  out.pos1 = mp1;
+  out.cells = cells;
+  return out;
+}
+
+// True when the warp kernel's no-reset scan is exact for this X-drop.
+__host__ __device__ inline bool warp_path_exact(int cutoff) {
+  return cutoff < 1024 || cutoff >= (1 << 30);
+}
+
+}  // namespace gzb
+
+namespace gzb {
+
+// ---------------------------------------------------------------------------
+// Gapped extension, one thread per extension (the common, narrow-band case).
+// The exact serial recurrence of GappedExtender::ExtendOneSideScoreOnly with
+// the band in shared memory: kLaneW columns per thread, each a packed int16
+// pair (best, best_gap), plus the query residue of each band column, laid
+// out [column][thread] so that a warp touching one column per thread is
+// bank-conflict free.  A band wider than kLaneW, or a value outside int16,
+// makes the extension overflow; the caller reruns it on the warp kernel.
+constexpr int kLaneW = 64;
+
+struct LaneBand {
+  uint32_t *cell;  // [kLaneW][stride]
+  uint32_t *res;   // [kLaneW/4][stride], 4 residues per word
+  int stride;
+  int t;           // this thread's column in the layout
+  __device__ __forceinline__ uint32_t &at(int c) { return cell[(c & (kLaneW - 1)) * stride + t]; }
+  __device__ __forceinline__ int residue(int c) const {
+    const int k = c & (kLaneW - 1);
+    return (res[(k >> 2) * stride + t] >> ((k & 3) * 8)) & 0xff;
+  }
+  __device__ __forceinline__ void set_residue(int c, int r) {
+    const int k = c & (kLaneW - 1);
+    uint32_t &w = res[(k >> 2) * stride + t];
+    const int sh = (k & 3) * 8;
+    w = (w & ~(0xffu << sh)) | ((uint32_t)r << sh);
+  }
+};
+
+__device__ __forceinline__ bool fits16(int v) { return v >= -32768 && v <= 32767; }
+__device__ __forceinline__ uint32_t pack16(int best, int gap) {
+  return ((uint32_t)(uint16_t)(int16_t)best) | ((uint32_t)(uint16_t)(int16_t)gap << 16);
+}
+__device__ __forceinline__ int lo16(uint32_t w) { return (int)(int16_t)(uint16_t)(w & 0xffff); }
+__device__ __forceinline__ int hi16(uint32_t w) { return (int)(int16_t)(uint16_t)(w >> 16); }
+
+__device__ inline GappedOut gapped_extend_lane(const GappedJob &job, const int *sm,
+                                               LaneBand band, uint32_t qpos, uint32_t dpos,
+                                               bool reverse) {
+  const int inc = reverse ? -1 : 1;
+  const int delim = job.delim;
+  const int ge = job.gap_ext;
+  const int gi = job.gap_open + job.gap_ext;
+  const int cutoff = job.cutoff;
+  const uint8_t *q0 = job.query + qpos;
+  const uint8_t *d0 = job.db + dpos;
+  GappedOut out;
+  out.score = 0;
+  out.pos0 = -inc;
+  out.pos1 = -inc;
+  out.cells = 0;
+  out.overflow = false;
+  if (q0[0] == delim || d0[0] == delim) return out;
+  bool ovf = false;
+  // row -1 (src/gapped_extender.cpp:345-364)
+  band.at(0) = pack16(0, -gi);
+  ovf |= !fits16(-gi);
+  int score = -gi;
+  int col = 1;
+  int r = q0[0];
+  for (;;) {
+    if (r == delim || score < -cutoff) break;
+    if (col >= kLaneW) {
+      out.overflow = true;
+      return out;
+    }
+    ovf |= !fits16(score) || !fits16(score - gi);
+    band.at(col) = pack16(score, score - gi);
+    band.set_residue(col, r);
+    score -= ge;
+    ++col;
+    r = q0[(col - 1) * inc];
+  }
+  int bs = 0, be;
+  if (r != delim) {
+    if (col >= kLaneW) {
+      out.overflow = true;
+      return out;
+    }
+    band.at(col) = pack16(kInitScore, kInitScore);
+    band.set_residue(col, r);
+    be = col + 1;
+  } else {
+    be = col;
+  }
+  int maxs = 0, mp0 = -inc, mp1 = -inc;
+  uint64_t cells = 0;
+  for (int p1 = 0;; p1 += inc) {
+    const int x = d0[p1];
+    if (x == delim) break;
+    const int *mrow = sm + x * kMatrixStride;
+    uint32_t &c0 = band.at(bs);
+    const uint32_t w0 = c0;
+    int diag = lo16(w0);
+    const int g0 = hi16(w0);
+    const int nb0 = (maxs - g0 > cutoff) ? kInitScore : g0;
+    int row_gap = nb0 - gi;
+    ovf |= !fits16(g0 - ge);
+    c0 = pack16(nb0, g0 - ge);
+    int last = bs;
+    const int bs_row = bs;
+    int pos0 = bs_row * inc;
+    for (int c = bs_row + 1; c < be; ++c, pos0 += inc) {
+      uint32_t &cw = band.at(c);
+      const uint32_t w = cw;
+      const int old_best = lo16(w), vgap = hi16(w);
+      int s = diag + mrow[band.residue(c)];
+      diag = old_best;
+      s = imax(s, imax(vgap, row_gap));
+      ++cells;
+      if (maxs - s > cutoff) {
+        if (bs + 1 == c) ++bs;
+        cw = pack16(kInitScore, kInitScore);
+        row_gap = kInitScore;
+      } else {
+        last = c;
+        if (s > maxs) {
+          maxs = s;
+          mp0 = pos0;
+          mp1 = p1;
+        }
+        const int ng = imax(s - gi, vgap - ge);
+        row_gap = imax(s - gi, row_gap - ge);
+        ovf |= !fits16(s) || !fits16(ng);
+        cw = pack16(s, ng);
+      }
+    }
+    if (bs + 1 == be) break;
+    int edge;  // residue the reference tests after the row (:461)
+    if (last < be - 1) {
+      edge = q0[(be - 1) * inc];  // old right edge
+      be = last + 1;
+    } else {
+      edge = q0[(be - 1) * inc];
+      while (row_gap >= maxs - cutoff && edge != delim) {
+        if (be - bs >= kLaneW) {
+          out.overflow = true;
+          return out;
+        }
+        ovf |= !fits16(row_gap) || !fits16(row_gap - gi);
+        band.at(be) = pack16(row_gap, row_gap - gi);
+        band.set_residue(be, edge);
+        row_gap -= ge;
+        ++be;
+        ++cells;
+        edge = q0[(be - 1) * inc];
+      }
+    }
+    if (edge != delim) {
+      if (be - bs >= kLaneW) {
+        out.overflow = true;
+        return out;
+      }
+      band.at(be) = pack16(kInitScore, kInitScore);
+      // the sentinel column's own residue (differs from `edge` when the band shrank)
+      band.set_residue(be, q0[(be - 1) * inc]);
+      ++be;
+    }
+  }
+  out.overflow = ovf;
+  out.score = maxs;
+  out.pos0 = mp0;
+  out.pos1 = mp1;
+  out.cells = cells;
+  return out;
+}
+
+}  // namespace gzb

@@ -1,0 +1,646 @@
+// gzb_operators.cu -- the per-operator C ABI: DistanceCalculatorGpu,
+// UngappedExtenderGpu and GappedExtenderGpu of the reference, one handle
+// each, with the same host/device split as the reference methods.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+#include <new>
+
+#include "ghostz_b200.h"
+#include "gzb_common.h"
+#include "gzb_kernels.cuh"
+
+namespace gzb {
+
+static thread_local char g_last_error[512] = "";
+
+int set_error(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+// --------------------------------------------------------------------------
+// kernels
+
+// Distance of every seed (one thread per seed).
+__global__ void distance_kernel(const uint8_t *__restrict__ q,
+                                const uint8_t *__restrict__ d,
+                                const uint8_t *__restrict__ map_g, int L,
+                                size_t n, const uint32_t *__restrict__ qc,
+                                const uint32_t *__restrict__ dc,
+                                int8_t *__restrict__ out) {
+  __shared__ uint8_t map[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) map[i] = i < 32 ? map_g[i] : 0;
+  __syncthreads();
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (int8_t)window_distance(q + qc[i], d + dc[i], L, map);
+}
+
+// Ungapped extension with trigger, one thread per seed.
+__global__ void ungapped_trigger_kernel(
+    const uint8_t *__restrict__ q, const uint8_t *__restrict__ d, int delim,
+    const int32_t *__restrict__ matrix, int number_letters, int stride,
+    const int32_t *__restrict__ cutoffs, const int32_t *__restrict__ triggers,
+    size_t n, const uint32_t *__restrict__ qid,
+    const uint32_t *__restrict__ qpos, const uint32_t *__restrict__ dpos,
+    int8_t *__restrict__ flags) {
+  __shared__ int sm[kMatrixStride * kMatrixStride];
+  load_matrix(sm, matrix, number_letters, stride);
+  __syncthreads();
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t id = qid[i];
+    int steps = 0;
+    flags[i] = ungapped_hit(q + qpos[i], d + dpos[i], delim, sm, cutoffs[id],
+                            triggers[id], &steps)
+                   ? 1
+                   : 0;
+  }
+}
+
+// set[start[i]] = i (the run-start scatter of SetQuerySeeds).
+__global__ void scatter_starts_kernel(size_t nseeds, const uint32_t *starts,
+                                      size_t size, uint32_t *out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nseeds;
+       i += (size_t)gridDim.x * blockDim.x)
+    if (starts[i] < size) out[starts[i]] = (uint32_t)i;
+}
+
+// In-place inclusive max-scan of one block-sized tile; tile maxima are
+// written to `tile_max`.  Hand-written replacement of the CUB max-scan.
+template <int B>
+__global__ void max_scan_tiles(uint32_t *a, size_t n, uint32_t *tile_max) {
+  __shared__ uint32_t warp_max[B / 32];
+  const size_t i = blockIdx.x * (size_t)B + threadIdx.x;
+  uint32_t v = i < n ? a[i] : 0;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v = max(v, t);
+  }
+  if (lane == 31) warp_max[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    uint32_t x = lane < B / 32 ? warp_max[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x = max(x, t);
+    }
+    if (lane < B / 32) warp_max[lane] = x;
+  }
+  __syncthreads();
+  if (w > 0) v = max(v, warp_max[w - 1]);
+  if (i < n) a[i] = v;
+  if (threadIdx.x == B - 1 && tile_max) tile_max[blockIdx.x] = v;
+}
+
+template <int B>
+__global__ void max_scan_apply(uint32_t *a, size_t n, const uint32_t *tile_prefix) {
+  const size_t i = blockIdx.x * (size_t)B + threadIdx.x;
+  if (blockIdx.x > 0 && i < n) a[i] = max(a[i], tile_prefix[blockIdx.x - 1]);
+}
+
+// Per-seed query id / concatenated position through the query-seed id.
+__global__ void set_query_seeds_kernel(size_t size, const uint32_t *list_qid,
+                                       const uint32_t *list_qpos,
+                                       const uint32_t *seed_ids,
+                                       const uint32_t *run_of,
+                                       uint32_t *out_qid, uint32_t *out_qpos) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < size;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t s = seed_ids[run_of[i]];
+    out_qid[i] = list_qid[s];
+    out_qpos[i] = list_qpos[s];
+  }
+}
+
+__global__ void gather_kernel(size_t n, const uint32_t *idx, const uint32_t *src,
+                              uint32_t *dst) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = src[idx[i]];
+}
+
+// Gapped extension kernels.  Every extension first runs on one thread
+// (gapped_lane_kernel); the few whose band outgrows the thread's shared
+// buffer go to one warp each (gapped_warp_kernel), and any left after that to
+// the serial kernel with a band in global memory.  Extension lists live in
+// device memory with device-side counts, so the three launches need no host
+// synchronisation.
+constexpr int kLaneBlock = 128;
+constexpr int kBandW = 256;
+constexpr int kSerialThreads = 4 * 128;
+constexpr int kSerialBand = 1 << 15;  // columns per fallback thread
+constexpr int kGappedWarps = 8;
+
+__device__ __forceinline__ void store_result(uint32_t e, uint32_t q, uint32_t d,
+                                             const GappedOut &o, uint32_t *qpos,
+                                             uint32_t *dpos, int32_t *scores) {
+  qpos[e] = q + (uint32_t)o.pos0;
+  dpos[e] = d + (uint32_t)o.pos1;
+  scores[e] = o.score;
+}
+
+__global__ void __launch_bounds__(kLaneBlock)
+gapped_lane_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number_letters,
+                   int stride, size_t n, const uint32_t *__restrict__ order, int reverse,
+                   const uint8_t *__restrict__ dir, uint32_t *qpos, uint32_t *dpos,
+                   int32_t *scores, uint32_t *spill, uint32_t *spill_count,
+                   unsigned long long *cells_total) {
+  __shared__ int sm[kMatrixStride * kMatrixStride];
+  __shared__ uint32_t cells_s[kLaneW * kLaneBlock];
+  __shared__ uint32_t res_s[(kLaneW / 4) * kLaneBlock];
+  load_matrix(sm, matrix, number_letters, stride);
+  __syncthreads();
+  LaneBand band{cells_s, res_s, kLaneBlock, (int)threadIdx.x};
+  unsigned long long cells = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t e = order ? order[i] : (uint32_t)i;
+    const bool rev = dir ? dir[e] != 0 : reverse != 0;
+    const uint32_t q = qpos[e], d = dpos[e];
+    GappedOut o = gapped_extend_lane(job, sm, band, q, d, rev);
+    if (o.overflow) {
+      spill[atomicAdd(spill_count, 1u)] = e;
+    } else {
+      cells += o.cells;
+      store_result(e, q, d, o, qpos, dpos, scores);
+    }
+  }
+  cells += __shfl_down_sync(0xffffffffu, cells, 16);
+  cells += __shfl_down_sync(0xffffffffu, cells, 8);
+  cells += __shfl_down_sync(0xffffffffu, cells, 4);
+  cells += __shfl_down_sync(0xffffffffu, cells, 2);
+  cells += __shfl_down_sync(0xffffffffu, cells, 1);
+  if ((threadIdx.x & 31) == 0 && cells) atomicAdd(cells_total, cells);
+}
+
+// One warp per listed extension (shared circular band of kBandW columns).
+__global__ void __launch_bounds__(kGappedWarps * 32)
+gapped_warp_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number_letters,
+                   int stride, const uint32_t *list, const uint32_t *list_count,
+                   int reverse, const uint8_t *__restrict__ dir, uint32_t *qpos,
+                   uint32_t *dpos, int32_t *scores, uint32_t *spill, uint32_t *spill_count,
+                   unsigned long long *cells_total) {
+  __shared__ int sm[kMatrixStride * kMatrixStride];
+  __shared__ int2 bands[kGappedWarps][kBandW];
+  load_matrix(sm, matrix, number_letters, stride);
+  __syncthreads();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t n = *list_count;
+  unsigned long long cells = 0;
+  for (size_t i = blockIdx.x * (size_t)kGappedWarps + w; i < n;
+       i += (size_t)gridDim.x * kGappedWarps) {
+    const uint32_t e = list[i];
+    const bool rev = dir ? dir[e] != 0 : reverse != 0;
+    const uint32_t q = qpos[e], d = dpos[e];
+    GappedOut o = gapped_extend_warp<kBandW>(job, sm, bands[w], kBandW - 1, q, d, rev);
+    if (o.overflow) {
+      if (lane == 0) spill[atomicAdd(spill_count, 1u)] = e;
+    } else {
+      cells += o.cells;
+      if (lane == 0) store_result(e, q, d, o, qpos, dpos, scores);
+    }
+    __syncwarp();
+  }
+  if (lane == 0 && cells) atomicAdd(cells_total, cells);
+}
+
+// Serial fallback over a listed set, one thread each, with a global
+// circular band of (wmask+1) columns per thread.
+__global__ void gapped_serial_kernel(GappedJob job, const int32_t *__restrict__ matrix,
+                                     int number_letters, int stride, const uint32_t *list,
+                                     const uint32_t *list_count, int reverse,
+                                     const uint8_t *__restrict__ dir, uint32_t *qpos,
+                                     uint32_t *dpos, int32_t *scores, int2 *band_pool,
+                                     int wmask, unsigned long long *cells_total,
+                                     uint32_t *too_long_count) {
+  __shared__ int sm[kMatrixStride * kMatrixStride];
+  load_matrix(sm, matrix, number_letters, stride);
+  __syncthreads();
+  const size_t count = *list_count;
+  const size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  int2 *band = band_pool + tid * (size_t)(wmask + 1);
+  unsigned long long cells = 0;
+  for (size_t i = tid; i < count; i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t e = list[i];
+    const bool rev = dir ? dir[e] != 0 : reverse != 0;
+    const uint32_t q = qpos[e], d = dpos[e];
+    bool too_long = false;
+    GappedOut o = gapped_extend_serial(job, sm, band, wmask, q, d, rev, &too_long);
+    if (too_long) {
+      atomicAdd(too_long_count, 1u);
+      continue;
+    }
+    cells += o.cells;
+    store_result(e, q, d, o, qpos, dpos, scores);
+  }
+  if (cells) atomicAdd(cells_total, cells);
+}
+
+static unsigned grid_for(size_t n, int block, int max_blocks = 148 * 16) {
+  size_t g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > (size_t)max_blocks) g = max_blocks;
+  return (unsigned)g;
+}
+
+}  // namespace gzb
+
+using namespace gzb;
+
+// --------------------------------------------------------------------------
+// C ABI: errors
+
+extern "C" const char *gzb_error_string(int code) {
+  switch (code) {
+    case GZB_OK: return "ok";
+    case GZB_ERR_INVALID: return "invalid argument or state";
+    case GZB_ERR_CUDA: return "CUDA runtime error";
+    case GZB_ERR_NOMEM: return "out of memory";
+    case GZB_ERR_OVERFLOW: return "size exceeds a limit";
+    case GZB_ERR_TIMEOUT: return "bounded device wait ran out";
+    default: return "unknown error";
+  }
+}
+
+extern "C" const char *gzb_last_error(void) { return g_last_error; }
+extern "C" int gzb_version(void) { return 10000; }
+
+// --------------------------------------------------------------------------
+// DistanceCalculatorGpu
+
+struct gzb_distance_calculator {
+  const uint8_t *queries = nullptr;
+  const uint8_t *db = nullptr;
+  const uint8_t *map = nullptr;
+  uint32_t L = 0;
+};
+
+extern "C" int gzb_distance_calculator_create(gzb_distance_calculator **out) {
+  GZB_CHECK(out, GZB_ERR_INVALID, "null output handle");
+  *out = new (std::nothrow) gzb_distance_calculator();
+  GZB_CHECK(*out, GZB_ERR_NOMEM, "host allocation failed");
+  return GZB_OK;
+}
+extern "C" int gzb_distance_calculator_destroy(gzb_distance_calculator *h) {
+  delete h;
+  return GZB_OK;
+}
+extern "C" int gzb_distance_calculator_set_queries(gzb_distance_calculator *h,
+                                                   const uint8_t *d) {
+  GZB_CHECK(h, GZB_ERR_INVALID, "null handle");
+  h->queries = d;
+  return GZB_OK;
+}
+extern "C" int gzb_distance_calculator_set_database(gzb_distance_calculator *h,
+                                                    const uint8_t *d) {
+  GZB_CHECK(h, GZB_ERR_INVALID, "null handle");
+  h->db = d;
+  return GZB_OK;
+}
+extern "C" int gzb_distance_calculator_set_reduced_code_map(
+    gzb_distance_calculator *h, const uint8_t *d) {
+  GZB_CHECK(h, GZB_ERR_INVALID, "null handle");
+  h->map = d;
+  return GZB_OK;
+}
+extern "C" int gzb_distance_calculator_set_subsequence_length(
+    gzb_distance_calculator *h, uint32_t L) {
+  GZB_CHECK(h, GZB_ERR_INVALID, "null handle");
+  h->L = L;
+  return GZB_OK;
+}
+extern "C" int gzb_distance_calculator_calculate_distances_async(
+    gzb_distance_calculator *h, size_t size, const uint32_t *qc,
+    const uint32_t *dc, int8_t *out, uint32_t *d_qc, uint32_t *d_dc,
+    int8_t *d_out, void *stream) {
+  GZB_CHECK(h && h->queries && h->db && h->map, GZB_ERR_INVALID,
+            "distance calculator not set up");
+  GZB_CHECK(h->L > 0 && h->L <= 64, GZB_ERR_INVALID, "bad subsequence length %u", h->L);
+  if (size == 0) return GZB_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (qc) GZB_CUDA(cudaMemcpyAsync(d_qc, qc, 4 * size, cudaMemcpyDefault, s));
+  if (dc) GZB_CUDA(cudaMemcpyAsync(d_dc, dc, 4 * size, cudaMemcpyDefault, s));
+  distance_kernel<<<grid_for(size, 256), 256, 0, s>>>(h->queries, h->db, h->map,
+                                                     (int)h->L, size, d_qc, d_dc, d_out);
+  GZB_CUDA(cudaGetLastError());
+  if (out) GZB_CUDA(cudaMemcpyAsync(out, d_out, size, cudaMemcpyDefault, s));
+  return GZB_OK;
+}
+
+// --------------------------------------------------------------------------
+// UngappedExtenderGpu
+
+struct gzb_ungapped_extender {
+  const uint32_t *list_qid = nullptr, *list_qpos = nullptr;
+  uint8_t delim = 0;
+  const uint8_t *queries = nullptr, *db = nullptr;
+  const int32_t *cutoffs = nullptr, *triggers = nullptr;
+  const int32_t *matrix = nullptr;
+  uint32_t number_letters = 0;
+};
+
+extern "C" int gzb_ungapped_extender_create(gzb_ungapped_extender **out) {
+  GZB_CHECK(out, GZB_ERR_INVALID, "null output handle");
+  *out = new (std::nothrow) gzb_ungapped_extender();
+  GZB_CHECK(*out, GZB_ERR_NOMEM, "host allocation failed");
+  return GZB_OK;
+}
+extern "C" int gzb_ungapped_extender_destroy(gzb_ungapped_extender *h) {
+  delete h;
+  return GZB_OK;
+}
+extern "C" int gzb_ungapped_extender_set_query_seed_data_list(
+    gzb_ungapped_extender *h, const uint32_t *qid, const uint32_t *qpos) {
+  GZB_CHECK(h, GZB_ERR_INVALID, "null handle");
+  h->list_qid = qid;
+  h->list_qpos = qpos;
+  return GZB_OK;
+}
+extern "C" int gzb_ungapped_extender_set_queries(gzb_ungapped_extender *h,
+                                                 uint8_t delim, const uint8_t *q,
+                                                 const int32_t *cut,
+                                                 const int32_t *trig) {
+  GZB_CHECK(h, GZB_ERR_INVALID, "null handle");
+  h->delim = delim;
+  h->queries = q;
+  h->cutoffs = cut;
+  h->triggers = trig;
+  return GZB_OK;
+}
+extern "C" int gzb_ungapped_extender_set_database(gzb_ungapped_extender *h,
+                                                  const uint8_t *d) {
+  GZB_CHECK(h, GZB_ERR_INVALID, "null handle");
+  h->db = d;
+  return GZB_OK;
+}
+extern "C" int gzb_ungapped_extender_set_score_matrix(gzb_ungapped_extender *h,
+                                                      const int32_t *m,
+                                                      uint32_t number_letters) {
+  GZB_CHECK(h, GZB_ERR_INVALID, "null handle");
+  GZB_CHECK(number_letters > 0 && number_letters < 32, GZB_ERR_INVALID,
+            "number_letters %u out of range", number_letters);
+  h->matrix = m;
+  h->number_letters = number_letters;
+  return GZB_OK;
+}
+
+static constexpr int kScanB = 256;
+
+extern "C" size_t gzb_ungapped_extender_query_seeds_temp_bytes(size_t size) {
+  size_t tiles = (size + kScanB - 1) / kScanB;
+  size_t tiles2 = (tiles + kScanB - 1) / kScanB;
+  return 4 * (tiles + tiles2 + 64);
+}
+
+// in-place inclusive max-scan over n elements using `tmp` (from
+// gzb_ungapped_extender_query_seeds_temp_bytes)
+static int max_scan(uint32_t *a, size_t n, uint32_t *tmp, cudaStream_t s, int depth = 0) {
+  if (n == 0) return GZB_OK;
+  const size_t tiles = (n + kScanB - 1) / kScanB;
+  GZB_CHECK(tiles < (1u << 31) && depth < 4, GZB_ERR_OVERFLOW, "scan too large");
+  max_scan_tiles<kScanB><<<(unsigned)tiles, kScanB, 0, s>>>(a, n, tmp);
+  GZB_CUDA(cudaGetLastError());
+  if (tiles > 1) {
+    GZB_TRY(max_scan(tmp, tiles, tmp + tiles, s, depth + 1));
+    max_scan_apply<kScanB><<<(unsigned)tiles, kScanB, 0, s>>>(a, n, tmp);
+    GZB_CUDA(cudaGetLastError());
+  }
+  return GZB_OK;
+}
+
+extern "C" int gzb_ungapped_extender_set_query_seeds(
+    gzb_ungapped_extender *h, size_t nseeds, size_t size, const uint32_t *seed_ids,
+    const uint32_t *seed_starts, size_t temp_bytes, void *d_temp,
+    uint32_t *d_seed_ids, uint32_t *d_seed_starts, uint32_t *d_qid,
+    uint32_t *d_qpos, uint32_t *temp_array, void *stream) {
+  GZB_CHECK(h && h->list_qid && h->list_qpos, GZB_ERR_INVALID,
+            "query seed data list not set");
+  if (size == 0) return GZB_OK;
+  GZB_CHECK(temp_bytes >= gzb_ungapped_extender_query_seeds_temp_bytes(size),
+            GZB_ERR_INVALID, "temp storage too small");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (seed_starts)
+    GZB_CUDA(cudaMemcpyAsync(d_seed_starts, seed_starts, 4 * nseeds, cudaMemcpyDefault, s));
+  GZB_CUDA(cudaMemsetAsync(d_qid, 0, 4 * size, s));
+  scatter_starts_kernel<<<grid_for(nseeds, 256), 256, 0, s>>>(nseeds, d_seed_starts, size, d_qid);
+  GZB_CUDA(cudaGetLastError());
+  GZB_CUDA(cudaMemcpyAsync(temp_array, d_qid, 4 * size, cudaMemcpyDeviceToDevice, s));
+  GZB_TRY(max_scan(temp_array, size, (uint32_t *)d_temp, s));
+  if (seed_ids)
+    GZB_CUDA(cudaMemcpyAsync(d_seed_ids, seed_ids, 4 * nseeds, cudaMemcpyDefault, s));
+  set_query_seeds_kernel<<<grid_for(size, 256), 256, 0, s>>>(
+      size, h->list_qid, h->list_qpos, d_seed_ids, temp_array, d_qid, d_qpos);
+  GZB_CUDA(cudaGetLastError());
+  return GZB_OK;
+}
+
+extern "C" int gzb_ungapped_extender_extend_with_trigger_async(
+    gzb_ungapped_extender *h, size_t size, const uint32_t *qid, const uint32_t *qpos,
+    const uint32_t *dpos, int8_t *flags, uint32_t *d_qid, uint32_t *d_qpos,
+    uint32_t *d_dpos, int8_t *d_flags, int32_t *d_temp, void *stream) {
+  (void)d_temp;
+  GZB_CHECK(h && h->queries && h->db && h->matrix && h->cutoffs && h->triggers,
+            GZB_ERR_INVALID, "ungapped extender not set up");
+  if (size == 0) return GZB_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (qid) GZB_CUDA(cudaMemcpyAsync(d_qid, qid, 4 * size, cudaMemcpyDefault, s));
+  if (qpos) GZB_CUDA(cudaMemcpyAsync(d_qpos, qpos, 4 * size, cudaMemcpyDefault, s));
+  if (dpos) GZB_CUDA(cudaMemcpyAsync(d_dpos, dpos, 4 * size, cudaMemcpyDefault, s));
+  ungapped_trigger_kernel<<<grid_for(size, 256), 256, 0, s>>>(
+      h->queries, h->db, h->delim, h->matrix, (int)h->number_letters,
+      (int)h->number_letters + 1, h->cutoffs, h->triggers, size, d_qid, d_qpos, d_dpos,
+      d_flags);
+  GZB_CUDA(cudaGetLastError());
+  if (flags) GZB_CUDA(cudaMemcpyAsync(flags, d_flags, size, cudaMemcpyDefault, s));
+  return GZB_OK;
+}
+
+// --------------------------------------------------------------------------
+// GappedExtenderGpu
+
+struct gzb_gapped_extender {
+  uint8_t delim = 0;
+  const uint8_t *queries = nullptr, *db = nullptr;
+  const int32_t *matrix = nullptr;
+  uint32_t number_letters = 0;
+  int gap_open = 0, gap_ext = 0, cutoff = 0;
+  // device scratch: spill list, counters, fallback bands
+  uint32_t *spill = nullptr;
+  size_t spill_cap = 0;
+  uint32_t *counters = nullptr;  // [0] spill count [1] too long
+  unsigned long long *cells = nullptr;
+  int2 *band_pool = nullptr;
+  int band_wmask = 0;
+  int serial_threads = 0;
+};
+
+
+extern "C" int gzb_gapped_extender_create(gzb_gapped_extender **out) {
+  GZB_CHECK(out, GZB_ERR_INVALID, "null output handle");
+  gzb_gapped_extender *h = new (std::nothrow) gzb_gapped_extender();
+  GZB_CHECK(h, GZB_ERR_NOMEM, "host allocation failed");
+  cudaError_t e = cudaMalloc(&h->counters, 64);
+  if (e == cudaSuccess) e = cudaMalloc(&h->cells, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemset(h->counters, 0, 64);
+  if (e == cudaSuccess) e = cudaMemset(h->cells, 0, sizeof(unsigned long long));
+  if (e != cudaSuccess) {
+    cudaFree(h->counters);
+    cudaFree(h->cells);
+    delete h;
+    return cuda_error(e, "gapped extender scratch", __FILE__, __LINE__);
+  }
+  *out = h;
+  return GZB_OK;
+}
+
+extern "C" int gzb_gapped_extender_destroy(gzb_gapped_extender *h) {
+  if (!h) return GZB_OK;
+  cudaFree(h->spill);
+  cudaFree(h->counters);
+  cudaFree(h->cells);
+  cudaFree(h->band_pool);
+  delete h;
+  return GZB_OK;
+}
+extern "C" int gzb_gapped_extender_set_queries(gzb_gapped_extender *h, uint8_t delim,
+                                               const uint8_t *q) {
+  GZB_CHECK(h, GZB_ERR_INVALID, "null handle");
+  h->delim = delim;
+  h->queries = q;
+  return GZB_OK;
+}
+extern "C" int gzb_gapped_extender_set_database(gzb_gapped_extender *h,
+                                                const uint8_t *d) {
+  GZB_CHECK(h, GZB_ERR_INVALID, "null handle");
+  h->db = d;
+  return GZB_OK;
+}
+extern "C" int gzb_gapped_extender_set_score_parameters(gzb_gapped_extender *h,
+                                                        const int32_t *m, uint32_t nl,
+                                                        int open, int ext, int cutoff) {
+  GZB_CHECK(h, GZB_ERR_INVALID, "null handle");
+  GZB_CHECK(nl > 0 && nl < 32, GZB_ERR_INVALID, "number_letters %u out of range", nl);
+  GZB_CHECK(open >= 0 && ext >= 0, GZB_ERR_INVALID, "negative gap penalty");
+  h->matrix = m;
+  h->number_letters = nl;
+  h->gap_open = open;
+  h->gap_ext = ext;
+  h->cutoff = cutoff;
+  return GZB_OK;
+}
+
+extern "C" int gzb_gapped_extender_convert_to_gapped_extension_seeds_async(
+    gzb_gapped_extender *h, size_t size, int reverse, const uint32_t *seed_positions,
+    const uint32_t *qpos, const uint32_t *dpos, uint32_t *d_seed_positions,
+    uint32_t *d_temp, uint32_t *d_qpos, uint32_t *d_dpos, void *stream) {
+  (void)reverse;
+  GZB_CHECK(h, GZB_ERR_INVALID, "null handle");
+  if (size == 0) return GZB_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  GZB_CUDA(cudaMemcpyAsync(d_seed_positions, seed_positions, 4 * size, cudaMemcpyDefault, s));
+  GZB_CUDA(cudaMemcpyAsync(d_temp, qpos, 4 * size, cudaMemcpyDefault, s));
+  gather_kernel<<<grid_for(size, 256), 256, 0, s>>>(size, d_seed_positions, d_temp, d_qpos);
+  GZB_CUDA(cudaGetLastError());
+  GZB_CUDA(cudaMemcpyAsync(d_temp, dpos, 4 * size, cudaMemcpyDefault, s));
+  gather_kernel<<<grid_for(size, 256), 256, 0, s>>>(size, d_seed_positions, d_temp, d_dpos);
+  GZB_CUDA(cudaGetLastError());
+  return GZB_OK;
+}
+
+namespace gzb {
+// Runs the three-level gapped extension over `n` extensions (optionally in
+// the order given by `order`) whose positions sit in d_qpos/d_dpos (updated
+// in place), writing d_scores.  counters: [0] spilled from the thread
+// kernel, [1] spilled from the warp kernel, [2] too long for the fallback.
+// `spill` needs room for 2n entries.  Synchronises `s` once at the end.
+int run_gapped(const GappedJob &job, const int32_t *matrix, int number_letters,
+               int stride, size_t n, const uint32_t *order, int reverse, const uint8_t *dir,
+               uint32_t *d_qpos, uint32_t *d_dpos, int32_t *d_scores, uint32_t **spill,
+               size_t *spill_cap, uint32_t *counters, unsigned long long *cells,
+               int2 **band_pool, int *band_wmask, cudaStream_t s, uint32_t *n_fallback) {
+  if (n == 0) return GZB_OK;
+  if (*spill_cap < 2 * n) {
+    cudaFree(*spill);
+    *spill = nullptr;
+    *spill_cap = 0;
+    GZB_CUDA(cudaMalloc(spill, 4 * 2 * n));
+    *spill_cap = 2 * n;
+  }
+  if (!*band_pool) {
+    GZB_CUDA(cudaMalloc(band_pool, sizeof(int2) * (size_t)kSerialThreads * kSerialBand));
+    *band_wmask = kSerialBand - 1;
+  }
+  GZB_CUDA(cudaMemsetAsync(counters, 0, 16, s));
+  uint32_t *spill1 = *spill, *spill2 = *spill + n;
+  const unsigned lane_blocks = (unsigned)std::min<size_t>((n + kLaneBlock - 1) / kLaneBlock,
+                                                          (size_t)148 * 40);
+  gapped_lane_kernel<<<lane_blocks, kLaneBlock, 0, s>>>(job, matrix, number_letters, stride, n,
+                                                        order, reverse, dir, d_qpos, d_dpos,
+                                                        d_scores, spill1, counters, cells);
+  GZB_CUDA(cudaGetLastError());
+  const uint32_t *serial_list = spill1, *serial_count = counters;
+  if (warp_path_exact(job.cutoff)) {
+    gapped_warp_kernel<<<148 * 4, kGappedWarps * 32, 0, s>>>(
+        job, matrix, number_letters, stride, spill1, counters, reverse, dir, d_qpos, d_dpos,
+        d_scores, spill2, counters + 1, cells);
+    GZB_CUDA(cudaGetLastError());
+    serial_list = spill2;
+    serial_count = counters + 1;
+  }
+  gapped_serial_kernel<<<kSerialThreads / 128, 128, 0, s>>>(
+      job, matrix, number_letters, stride, serial_list, serial_count, reverse, dir, d_qpos,
+      d_dpos, d_scores, *band_pool, *band_wmask, cells, counters + 2);
+  GZB_CUDA(cudaGetLastError());
+  uint32_t h[3] = {0, 0, 0};
+  GZB_CUDA(cudaMemcpyAsync(h, counters, 12, cudaMemcpyDeviceToHost, s));
+  GZB_CUDA(cudaStreamSynchronize(s));
+  GZB_CHECK(h[2] == 0, GZB_ERR_OVERFLOW,
+            "%u gapped extensions need a band wider than %d columns", h[2], kSerialBand);
+  if (n_fallback) *n_fallback = h[0];
+  return GZB_OK;
+}
+}  // namespace gzb
+
+extern "C" int gzb_gapped_extender_extend_one_side_score_only_async(
+    gzb_gapped_extender *h, size_t size, int reverse, uint32_t *qpos, uint32_t *dpos,
+    int32_t *scores, uint32_t *d_qpos, uint32_t *d_dpos, int32_t *d_scores,
+    void *stream) {
+  GZB_CHECK(h && h->queries && h->db && h->matrix, GZB_ERR_INVALID,
+            "gapped extender not set up");
+  if (size == 0) return GZB_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  GappedJob job;
+  job.query = h->queries;
+  job.db = h->db;
+  job.delim = h->delim;
+  job.gap_open = h->gap_open;
+  job.gap_ext = h->gap_ext;
+  job.cutoff = h->cutoff;
+  GZB_TRY(run_gapped(job, h->matrix, (int)h->number_letters, (int)h->number_letters + 1,
+                     size, nullptr, reverse, nullptr, d_qpos, d_dpos, d_scores, &h->spill,
+                     &h->spill_cap, h->counters, h->cells, &h->band_pool, &h->band_wmask, s,
+                     nullptr));
+  if (qpos) GZB_CUDA(cudaMemcpyAsync(qpos, d_qpos, 4 * size, cudaMemcpyDefault, s));
+  if (dpos) GZB_CUDA(cudaMemcpyAsync(dpos, d_dpos, 4 * size, cudaMemcpyDefault, s));
+  if (scores) GZB_CUDA(cudaMemcpyAsync(scores, d_scores, 4 * size, cudaMemcpyDefault, s));
+  return GZB_OK;
+}
+
+extern "C" int gzb_gapped_extender_cells(gzb_gapped_extender *h, uint64_t *cells) {
+  GZB_CHECK(h && cells, GZB_ERR_INVALID, "null argument");
+  unsigned long long c = 0;
+  GZB_CUDA(cudaMemcpy(&c, h->cells, sizeof(c), cudaMemcpyDeviceToHost));
+  *cells = c;
+  return GZB_OK;
+}

@@ -1,0 +1,386 @@
+"""ctypes bindings of libghostz_b200.so.
+
+The operator classes mirror the reference's GPU operator classes
+(DistanceCalculatorGpu, UngappedExtenderGpu, GappedExtenderGpu) method for
+method; device buffers are passed as integer device addresses (for example
+``tensor.data_ptr()`` of a CUDA torch tensor) and host buffers as numpy
+arrays.  Every call raises GzbError when the library reports a failure.
+The library must exist: nothing here falls back to a CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .build import LIB
+
+_lib = None
+
+
+class GzbError(RuntimeError):
+    pass
+
+
+def symbols_declared_in_header():
+    """Names of every function the public header declares."""
+    import re
+    hdr = os.path.join(os.path.dirname(os.path.dirname(LIB)), "include", "ghostz_b200.h")
+    text = open(hdr).read()
+    return sorted(set(re.findall(r"\b(gzb_[a-z0-9_]+)\s*\(", text)))
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            raise GzbError(f"{LIB} is missing: build it with gzb.build.build()")
+        _lib = C.CDLL(LIB)
+        _declare(_lib)
+    return _lib
+
+
+V = C.c_void_p
+SZ = C.c_size_t
+U32 = C.c_uint32
+I32 = C.c_int32
+
+
+def _declare(L):
+    L.gzb_last_error.restype = C.c_char_p
+    L.gzb_error_string.restype = C.c_char_p
+    L.gzb_ungapped_extender_query_seeds_temp_bytes.restype = SZ
+    L.gzb_ungapped_extender_query_seeds_temp_bytes.argtypes = [SZ]
+    sigs = {
+        "gzb_distance_calculator_create": [V],
+        "gzb_distance_calculator_destroy": [V],
+        "gzb_distance_calculator_set_queries": [V, V],
+        "gzb_distance_calculator_set_database": [V, V],
+        "gzb_distance_calculator_set_reduced_code_map": [V, V],
+        "gzb_distance_calculator_set_subsequence_length": [V, U32],
+        "gzb_distance_calculator_calculate_distances_async": [V, SZ, V, V, V, V, V, V, V],
+        "gzb_ungapped_extender_create": [V],
+        "gzb_ungapped_extender_destroy": [V],
+        "gzb_ungapped_extender_set_query_seed_data_list": [V, V, V],
+        "gzb_ungapped_extender_set_queries": [V, C.c_uint8, V, V, V],
+        "gzb_ungapped_extender_set_database": [V, V],
+        "gzb_ungapped_extender_set_score_matrix": [V, V, U32],
+        "gzb_ungapped_extender_set_query_seeds": [V, SZ, SZ, V, V, SZ, V, V, V, V, V, V, V],
+        "gzb_ungapped_extender_extend_with_trigger_async": [V, SZ, V, V, V, V, V, V, V, V, V, V],
+        "gzb_gapped_extender_create": [V],
+        "gzb_gapped_extender_destroy": [V],
+        "gzb_gapped_extender_set_queries": [V, C.c_uint8, V],
+        "gzb_gapped_extender_set_database": [V, V],
+        "gzb_gapped_extender_set_score_parameters": [V, V, U32, C.c_int, C.c_int, C.c_int],
+        "gzb_gapped_extender_convert_to_gapped_extension_seeds_async": [V, SZ, C.c_int, V, V, V, V, V, V, V, V],
+        "gzb_gapped_extender_extend_one_side_score_only_async": [V, SZ, C.c_int, V, V, V, V, V, V, V],
+        "gzb_gapped_extender_cells": [V, V],
+        "gzb_engine_create": [C.c_int, V],
+        "gzb_engine_destroy": [V],
+        "gzb_engine_set_params": [V, V],
+        "gzb_engine_set_database": [V, I32, V, C.c_uint64, V, U32, V],
+        "gzb_engine_set_queries": [V, V, C.c_uint64, V, V, U32, V, V, V],
+        "gzb_engine_presearch": [V, C.c_int, V],
+        "gzb_engine_reset_results": [V, V],
+        "gzb_engine_get_results": [V, V, V, V],
+        "gzb_engine_get_counters": [V, V],
+        "gzb_engine_get_hits": [V, V, V, V, C.c_uint64, V, V],
+        "gzb_engine_get_index_array": [V, C.c_int, V, C.c_uint64, V, V],
+        "gzb_engine_get_list_array": [V, C.c_int, V, C.c_uint64, V, V],
+        "gzb_engine_get_stage_ms": [V, V],
+    }
+    for name, args in sigs.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = C.c_int
+
+
+def check(rc):
+    if rc != 0:
+        L = lib()
+        raise GzbError(f"{L.gzb_error_string(rc).decode()}: {L.gzb_last_error().decode()}")
+
+
+def hptr(a):
+    """Host pointer of a numpy array (None -> NULL)."""
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def dptr(x):
+    """Device pointer of a torch tensor / int address (None -> NULL)."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return C.c_void_p(x)
+    return C.c_void_p(x.data_ptr())
+
+
+def stream_handle(stream=None):
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+
+class _Handle:
+    _kind = ""
+
+    def __init__(self):
+        h = C.c_void_p()
+        check(getattr(lib(), f"gzb_{self._kind}_create")(C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            getattr(lib(), f"gzb_{self._kind}_destroy")(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _call(self, name, *args):
+        check(getattr(lib(), f"gzb_{self._kind}_{name}")(self.h, *args))
+
+
+class DistanceCalculatorGpu(_Handle):
+    """src/distance_calculator_gpu.h:18-40"""
+    _kind = "distance_calculator"
+
+    def SetQueries(self, d_queries):
+        self._call("set_queries", dptr(d_queries))
+
+    def SetDatabase(self, d_db):
+        self._call("set_database", dptr(d_db))
+
+    def SetReducedCodeMap(self, d_map):
+        self._call("set_reduced_code_map", dptr(d_map))
+
+    def SetSubsequenceLength(self, length):
+        self._call("set_subsequence_length", int(length))
+
+    def CalculateDistancesAsync(self, size, h_q, h_d, h_out, d_q, d_d, d_out, stream=None):
+        self._call("calculate_distances_async", size, hptr(h_q), hptr(h_d), hptr(h_out),
+                   dptr(d_q), dptr(d_d), dptr(d_out), stream_handle(stream))
+
+
+class UngappedExtenderGpu(_Handle):
+    """src/ungapped_extender_gpu.h:21-76"""
+    _kind = "ungapped_extender"
+
+    def SetQuerySeedDataList(self, d_query_ids, d_query_positions):
+        self._call("set_query_seed_data_list", dptr(d_query_ids), dptr(d_query_positions))
+
+    def SetQueries(self, delimiter, d_queries, d_cutoffs, d_triggers):
+        self._call("set_queries", int(delimiter), dptr(d_queries), dptr(d_cutoffs),
+                   dptr(d_triggers))
+
+    def SetDatabase(self, d_db):
+        self._call("set_database", dptr(d_db))
+
+    def SetScoreMatrix(self, d_matrix, number_letters):
+        self._call("set_score_matrix", dptr(d_matrix), int(number_letters))
+
+    @staticmethod
+    def QuerySeedsTempBytes(size):
+        return int(lib().gzb_ungapped_extender_query_seeds_temp_bytes(size))
+
+    def SetQuerySeeds(self, query_seeds_size, size, h_seed_ids, h_seed_starts, temp_bytes,
+                      d_temp, d_seed_ids, d_seed_starts, d_query_ids, d_qpos, d_temp_array,
+                      stream=None):
+        self._call("set_query_seeds", query_seeds_size, size, hptr(h_seed_ids),
+                   hptr(h_seed_starts), temp_bytes, dptr(d_temp), dptr(d_seed_ids),
+                   dptr(d_seed_starts), dptr(d_query_ids), dptr(d_qpos), dptr(d_temp_array),
+                   stream_handle(stream))
+
+    def ExtendWithTriggerAsync(self, size, h_qid, h_qpos, h_dpos, h_flags, d_qid, d_qpos,
+                               d_dpos, d_flags, d_temp=None, stream=None):
+        self._call("extend_with_trigger_async", size, hptr(h_qid), hptr(h_qpos),
+                   hptr(h_dpos), hptr(h_flags), dptr(d_qid), dptr(d_qpos), dptr(d_dpos),
+                   dptr(d_flags), dptr(d_temp), stream_handle(stream))
+
+
+class GappedExtenderGpu(_Handle):
+    """src/gapped_extender_gpu.h:19-60"""
+    _kind = "gapped_extender"
+
+    def SetQueries(self, delimiter, d_queries):
+        self._call("set_queries", int(delimiter), dptr(d_queries))
+
+    def SetDatabase(self, d_db):
+        self._call("set_database", dptr(d_db))
+
+    def SetScoreParameters(self, d_matrix, number_letters, gap_open, gap_ext, cutoff):
+        self._call("set_score_parameters", dptr(d_matrix), int(number_letters),
+                   int(gap_open), int(gap_ext), int(cutoff))
+
+    def ConvertToGappedExtensionSeedsAsync(self, size, reverse, h_seed_pos, h_qpos, h_dpos,
+                                           d_seed_pos, d_temp, d_qpos, d_dpos, stream=None):
+        self._call("convert_to_gapped_extension_seeds_async", size, int(bool(reverse)),
+                   hptr(h_seed_pos), hptr(h_qpos), hptr(h_dpos), dptr(d_seed_pos),
+                   dptr(d_temp), dptr(d_qpos), dptr(d_dpos), stream_handle(stream))
+
+    def ExtendOneSideScoreOnlyAsync(self, size, reverse, h_qpos, h_dpos, h_scores, d_qpos,
+                                    d_dpos, d_scores, stream=None):
+        self._call("extend_one_side_score_only_async", size, int(bool(reverse)),
+                   hptr(h_qpos), hptr(h_dpos), hptr(h_scores), dptr(d_qpos), dptr(d_dpos),
+                   dptr(d_scores), stream_handle(stream))
+
+    def Cells(self):
+        c = C.c_uint64()
+        self._call("cells", C.byref(c))
+        return c.value
+
+
+PAD = 256  # readable bytes kept before and after every device sequence
+
+
+def device_sequence(codes, delimiter, device="cuda"):
+    """Uploads codes with PAD delimiter bytes on both sides; returns
+    (tensor, address of codes[0])."""
+    import torch
+    buf = np.full(len(codes) + 2 * PAD, delimiter, dtype=np.uint8)
+    buf[PAD:PAD + len(codes)] = codes
+    t = torch.from_numpy(buf).to(device)
+    return t, t.data_ptr() + PAD
+
+
+def device_matrix(matrix, device="cuda"):
+    """(n+1)^2 int32 with zero delimiter row/column (the reference's device
+    layout, src/aligner_gpu_data.cu:108-122)."""
+    import torch
+    m = np.asarray(matrix, dtype=np.int32)
+    n = m.shape[0]
+    out = np.zeros((n + 1, n + 1), dtype=np.int32)
+    out[:n, :n] = m
+    return torch.from_numpy(out.reshape(-1).copy()).to(device)
+
+
+RESULT_DTYPE = np.dtype([
+    ("chunk_id", "<i4"), ("subject_id", "<i4"), ("score", "<i4"),
+    ("hit_q", "<u4"), ("hit_d", "<u4"), ("start_q", "<u4"), ("start_d", "<u4"),
+    ("end_q", "<u4"), ("end_d", "<u4"),
+])
+COUNTER_NAMES = ("distance_seeds", "ungapped_seeds", "ungapped_hits",
+                 "chained_hits", "gapped_extensions", "gapped_cells", "gapped_fallbacks",
+                 "ungapped_steps", "kernel_launches")
+LIST_NAMES = ("hashes", "offsets", "check_counts", "query_ids", "positions")
+INDEX_NAMES = ("nc_keys", "nc_offsets", "nc_values", "rep_keys", "rep_offsets",
+               "rep_cluster_ids", "rep_positions", "member_offsets", "member_positions")
+SCHEDULE_PLAIN = 0
+SCHEDULE_BATCHED = 1
+
+
+class PresearchEngine:
+    """Device-resident presearch of one database chunk at a time: the seed
+    search, distance filter, ungapped and gapped extension and top-b merge
+    that AlignerGpuPresearchThread::Run drives
+    (src/aligner_gpu_presearch_thread.cpp:62-642)."""
+
+    def __init__(self, device: int = 0):
+        self.h = C.c_void_p()
+        check(lib().gzb_engine_create(int(device), C.byref(self.h)))
+        self.params = None
+        self.number_queries = 0
+
+    def close(self):
+        if self.h:
+            lib().gzb_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, params):
+        self.params = np.array([params], dtype=params.dtype)
+        check(lib().gzb_engine_set_params(self.h, C.c_void_p(self.params.ctypes.data)))
+
+    def set_database(self, db, chunk_id=0, stream=None):
+        codes = np.ascontiguousarray(db.codes, dtype=np.uint8)
+        offs = np.ascontiguousarray(db.offsets, dtype=np.uint32)
+        check(lib().gzb_engine_set_database(self.h, int(chunk_id), hptr(codes), len(codes),
+                                            hptr(offs), int(db.number_sequences),
+                                            _stream_or_null(stream)))
+
+    def set_queries(self, queries, stream=None):
+        codes = np.ascontiguousarray(queries.codes, dtype=np.uint8)
+        offs = np.ascontiguousarray(queries.offsets, dtype=np.uint32)
+        lens = np.ascontiguousarray(queries.lengths, dtype=np.uint32)
+        cut = np.ascontiguousarray(queries.cutoffs, dtype=np.int32)
+        trig = np.ascontiguousarray(queries.triggers, dtype=np.int32)
+        check(lib().gzb_engine_set_queries(self.h, hptr(codes), len(codes), hptr(offs),
+                                           hptr(lens), int(queries.number), hptr(cut),
+                                           hptr(trig), _stream_or_null(stream)))
+        self.number_queries = int(queries.number)
+
+    def presearch(self, schedule=SCHEDULE_PLAIN, stream=None):
+        check(lib().gzb_engine_presearch(self.h, int(schedule), _stream_or_null(stream)))
+
+    def reset_results(self, stream=None):
+        check(lib().gzb_engine_reset_results(self.h, _stream_or_null(stream)))
+
+    def results(self, stream=None):
+        b = int(self.params[0]["max_number_results"])
+        counts = np.zeros(self.number_queries, np.uint32)
+        res = np.zeros(self.number_queries * b, RESULT_DTYPE)
+        check(lib().gzb_engine_get_results(self.h, hptr(counts), hptr(res),
+                                           _stream_or_null(stream)))
+        res = res.reshape(self.number_queries, b)
+        return [res[i, :counts[i]].copy() for i in range(self.number_queries)]
+
+    def counters(self):
+        c = (C.c_uint64 * 9)()
+        check(lib().gzb_engine_get_counters(self.h, C.byref(c)))
+        return dict(zip(COUNTER_NAMES, [int(v) for v in c]))
+
+    def stage_ms(self):
+        t = (C.c_float * 6)()
+        check(lib().gzb_engine_get_stage_ms(self.h, C.byref(t)))
+        return dict(zip(("lookup", "seed_ungapped", "chain", "gapped", "merge", "total"),
+                        [float(v) for v in t]))
+
+    def hits(self, stream=None):
+        n = C.c_uint64()
+        check(lib().gzb_engine_get_hits(self.h, None, None, None, 0, C.byref(n),
+                                        _stream_or_null(stream)))
+        k = n.value
+        a, b, c = (np.zeros(k, np.uint32) for _ in range(3))
+        check(lib().gzb_engine_get_hits(self.h, hptr(a), hptr(b), hptr(c), k, C.byref(n),
+                                        _stream_or_null(stream)))
+        return a, b, c
+
+    def list_arrays(self, stream=None):
+        out = {}
+        for i, name in enumerate(LIST_NAMES):
+            n = C.c_uint64()
+            check(lib().gzb_engine_get_list_array(self.h, i, None, 0, C.byref(n),
+                                                  _stream_or_null(stream)))
+            a = np.zeros(n.value, np.uint32)
+            check(lib().gzb_engine_get_list_array(self.h, i, hptr(a), n.value, C.byref(n),
+                                                  _stream_or_null(stream)))
+            out[name] = a
+        return out
+
+    def index_arrays(self, stream=None):
+        out = {}
+        for i, name in enumerate(INDEX_NAMES):
+            n = C.c_uint64()
+            check(lib().gzb_engine_get_index_array(self.h, i, None, 0, C.byref(n),
+                                                   _stream_or_null(stream)))
+            a = np.zeros(n.value, np.uint32)
+            check(lib().gzb_engine_get_index_array(self.h, i, hptr(a), n.value, C.byref(n),
+                                                   _stream_or_null(stream)))
+            out[name] = a
+        return out
+
+
+def _stream_or_null(stream):
+    if stream is None:
+        return None
+    return C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))

@@ -56,25 +56,30 @@ def lognormal_lengths(rng, n, median, sigma, lo, hi):
     return np.clip(np.rint(x), lo, hi).astype(np.int64)
 
 
-def random_residues(rng, n):
-    return rng.choice(len(P.REGULAR), size=n, p=_background_probs()).astype(np.uint8)
+def random_residues(rng, n, chunk=1 << 26):
+    """n i.i.d. residue codes from the background, as uint8 (chunked inverse
+    CDF on 32-bit uniforms, so large draws need no 64-bit temporaries)."""
+    cdf = np.cumsum(_background_probs())
+    thresholds = np.minimum(np.round(cdf * 2.0**32), 2.0**32 - 1).astype(np.uint64)[:-1]
+    out = np.empty(n, dtype=np.uint8)
+    for a in range(0, n, chunk):
+        b = min(n, a + chunk)
+        u = rng.integers(0, 2**32, size=b - a, dtype=np.uint64)
+        out[a:b] = np.searchsorted(thresholds, u, side="right").astype(np.uint8)
+    return out
 
 
 def make_database(n_sequences, seed, median=300, sigma=0.6, lo=30, hi=3000):
     rng = np.random.default_rng(seed)
     lens = lognormal_lengths(rng, n_sequences, median, sigma, lo, hi)
     total = int(lens.sum()) + n_sequences + 1
-    codes = np.empty(total, dtype=np.uint8)
     offsets = np.empty(n_sequences + 1, dtype=np.uint32)
     starts = np.concatenate([[1], 1 + np.cumsum(lens + 1)[:-1]]).astype(np.int64)
     offsets[:-1] = starts
     offsets[-1] = total
-    body = random_residues(rng, int(lens.sum()))
-    # scatter residues around the delimiters
-    codes[:] = P.DELIMITER
-    idx = np.repeat(starts, lens) + (np.arange(int(lens.sum())) -
-                                     np.repeat(np.cumsum(lens) - lens, lens))
-    codes[idx] = body
+    codes = random_residues(rng, total)
+    codes[0] = P.DELIMITER
+    codes[starts + lens] = P.DELIMITER  # delimiter after every sequence
     return Database(codes=codes, offsets=offsets, number_sequences=n_sequences)
 
 
@@ -89,25 +94,31 @@ def _substitution_table(lam=0.3176):
 def mutate(rng, seq, identity, indel_p=0.02, indel_mean=3.0):
     """BLOSUM62-conditional substitutions at rate 1-identity, plus
     insertions/deletions at indel_p per site with geometric lengths."""
-    table = _substitution_table()
-    seq = seq.copy()
-    sub = rng.random(len(seq)) < (1.0 - identity)
-    for i in np.nonzero(sub)[0]:
-        seq[i] = rng.choice(20, p=table[seq[i]])
-    out = []
-    i = 0
-    n = len(seq)
-    while i < n:
-        if rng.random() < indel_p:
-            k = int(rng.geometric(1.0 / indel_mean))
-            if rng.random() < 0.5:
-                out.append(random_residues(rng, k))
-            else:
-                i += k
-                continue
-        out.append(seq[i:i + 1])
-        i += 1
-    return np.concatenate(out) if out else seq[:1]
+    table = np.cumsum(_substitution_table(), axis=1)
+    seq = np.asarray(seq, dtype=np.uint8).copy()
+    sub = np.nonzero(rng.random(len(seq)) < (1.0 - identity))[0]
+    if len(sub):
+        u = rng.random(len(sub))
+        rows = table[seq[sub]]
+        seq[sub] = np.minimum((rows < u[:, None]).sum(axis=1), 19).astype(np.uint8)
+    events = np.nonzero(rng.random(len(seq)) < indel_p)[0]
+    if len(events) == 0:
+        return seq
+    pieces = []
+    prev = 0
+    for i in events:
+        if i < prev:
+            continue
+        pieces.append(seq[prev:i])
+        k = int(rng.geometric(1.0 / indel_mean))
+        if rng.random() < 0.5:
+            pieces.append(random_residues(rng, k))
+            prev = i
+        else:
+            prev = i + k
+    pieces.append(seq[prev:])
+    out = np.concatenate(pieces)
+    return out if len(out) else seq[:1]
 
 
 def make_queries(db: Database, n_queries, seed, homolog_fraction=0.3,

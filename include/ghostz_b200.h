@@ -1,0 +1,278 @@
+/*
+ * ghostz_b200.h -- C ABI of the B200 presearch engine (libghostz_b200.so).
+ *
+ * The engine replaces the GPU operators of GHOSTZ-GPU's `aln` presearch:
+ * seed search over the clustered reduced-alphabet hash index, distance
+ * filtering, ungapped X-drop extension with trigger and gapped affine X-drop
+ * extension.  Two layers are exported:
+ *
+ *  1. Per-operator handles whose functions mirror, one to one, the methods of
+ *     the reference classes DistanceCalculatorGpu, UngappedExtenderGpu and
+ *     GappedExtenderGpu (argument order, meaning, host/device split).  Device
+ *     sequences are one byte per residue code (the reference uses a 5-bit
+ *     packed form); score matrices use the reference's device layout,
+ *     (number_letters + 1)^2 int32 with a zero delimiter row and column
+ *     (src/aligner_gpu_data.cu:108-122).
+ *  2. A presearch engine that keeps a database chunk, its index and the
+ *     queries resident in HBM and runs the whole seed -> ungapped -> chain
+ *     filter -> gapped -> top-b pipeline on the device
+ *     (the work of AlignerGpuPresearchThread::Run,
+ *     src/aligner_gpu_presearch_thread.cpp:62-642).
+ *
+ * All functions return GZB_OK or an error code (never exit); the message of
+ * the last failure on the calling thread is available from gzb_last_error().
+ * Handles are not shared between threads without external locking; several
+ * handles may use one device concurrently on different streams.
+ * `stream` arguments are cudaStream_t passed as void*.
+ */
+#ifndef GHOSTZ_B200_H_
+#define GHOSTZ_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GZB_OK 0
+#define GZB_ERR_INVALID 1   /* bad argument or state */
+#define GZB_ERR_CUDA 2      /* a CUDA runtime call failed */
+#define GZB_ERR_NOMEM 3     /* device or host allocation failed */
+#define GZB_ERR_OVERFLOW 4  /* a size exceeds a documented limit */
+#define GZB_ERR_TIMEOUT 5   /* a bounded device wait ran out */
+
+const char *gzb_error_string(int code);
+const char *gzb_last_error(void);
+int gzb_version(void);
+
+/* Search parameters (plain layout; 4-byte fields and byte arrays). */
+typedef struct {
+  int32_t delimiter;             /* sequence delimiter code (25 for protein) */
+  int32_t number_letters;        /* score matrix side (<= 31) */
+  int32_t score_matrix[32 * 32]; /* [db_code * number_letters + query_code] */
+  int32_t map_size;              /* entries used in the code maps (<= 32) */
+  uint8_t hash_code_map[32];     /* residue code -> seed-hash reduced code */
+  uint8_t similarity_code_map[32]; /* residue code -> similarity code */
+  int32_t max_indexing_code;     /* largest hashable reduced code */
+  int32_t code_scores[32];       /* per reduced code: max self score */
+  int32_t seed_threshold;        /* hash stops once code scores sum >= this */
+  int32_t max_hash_length;       /* 8 */
+  int32_t min_hash_length;       /* 6 */
+  int32_t subsequence_length;    /* distance / clustering window L */
+  int32_t max_member_distance;   /* L * (1 - 0.9f), truncated */
+  int32_t distance_threshold;    /* L - 0.8f * L, truncated */
+  int32_t gap_open;
+  int32_t gap_extension;
+  int32_t gapped_cutoff;         /* X-drop of the gapped extension */
+  int32_t max_number_results;    /* top-b per query (-b) */
+  int32_t max_number_one_subject_results; /* per subject (-v) */
+  int32_t clustering;            /* database built with -C T */
+} gzb_params;
+
+/* ---- DistanceCalculatorGpu (src/distance_calculator_gpu.h:18-40) ------- */
+typedef struct gzb_distance_calculator gzb_distance_calculator;
+int gzb_distance_calculator_create(gzb_distance_calculator **out);
+int gzb_distance_calculator_destroy(gzb_distance_calculator *h);
+/* SetQueries / SetDatabase / SetReducedCodeMap / SetSubsequenceLength
+ * (src/distance_calculator_gpu.cu:299-318) */
+int gzb_distance_calculator_set_queries(gzb_distance_calculator *h,
+                                        const uint8_t *d_query_sequence);
+int gzb_distance_calculator_set_database(gzb_distance_calculator *h,
+                                         const uint8_t *d_database_sequence);
+int gzb_distance_calculator_set_reduced_code_map(
+    gzb_distance_calculator *h, const uint8_t *d_reduced_code_map);
+int gzb_distance_calculator_set_subsequence_length(gzb_distance_calculator *h,
+                                                   uint32_t length);
+/* CalculateDistancesAsync (src/distance_calculator_gpu.cu:320-355): copies
+ * the centres to the device, computes one int8 distance per seed and copies
+ * them back, all on `stream`. */
+int gzb_distance_calculator_calculate_distances_async(
+    gzb_distance_calculator *h, size_t size,
+    const uint32_t *query_concatenated_centers,
+    const uint32_t *database_centers, int8_t *distances,
+    uint32_t *d_query_concatenated_centers, uint32_t *d_database_centers,
+    int8_t *d_distances, void *stream);
+
+/* ---- UngappedExtenderGpu (src/ungapped_extender_gpu.h:21-76) ----------- */
+typedef struct gzb_ungapped_extender gzb_ungapped_extender;
+int gzb_ungapped_extender_create(gzb_ungapped_extender **out);
+int gzb_ungapped_extender_destroy(gzb_ungapped_extender *h);
+/* SetQuerySeedDataList (src/ungapped_extender_gpu.cu:789-794) */
+int gzb_ungapped_extender_set_query_seed_data_list(
+    gzb_ungapped_extender *h, const uint32_t *d_query_ids,
+    const uint32_t *d_query_positions);
+/* SetQueries (src/ungapped_extender_gpu.cu:796-804) */
+int gzb_ungapped_extender_set_queries(gzb_ungapped_extender *h,
+                                      uint8_t sequence_delimiter,
+                                      const uint8_t *d_query_sequence,
+                                      const int32_t *d_ungapped_cutoffs,
+                                      const int32_t *d_gapped_triggers);
+int gzb_ungapped_extender_set_database(gzb_ungapped_extender *h,
+                                      const uint8_t *d_database_sequence);
+/* SetScoreMatrix (src/ungapped_extender_gpu.cu:811-816) */
+int gzb_ungapped_extender_set_score_matrix(gzb_ungapped_extender *h,
+                                           const int32_t *d_score_matrix,
+                                           uint32_t number_letters);
+/* Scratch bytes SetQuerySeeds needs in d_temp_storage for `size` seeds
+ * (the reference sizes a CUB scan, src/device_seeds_memory.cu:20-36). */
+size_t gzb_ungapped_extender_query_seeds_temp_bytes(size_t size);
+/* SetQuerySeeds (src/ungapped_extender_gpu.cu:818-852): expands run-length
+ * (query seed id, first seed index) pairs into per-seed query id and
+ * concatenated query position. */
+int gzb_ungapped_extender_set_query_seeds(
+    gzb_ungapped_extender *h, size_t query_seeds_size, size_t size,
+    const uint32_t *query_seed_ids, const uint32_t *query_seed_starts,
+    size_t temp_storage_bytes, void *d_temp_storage,
+    uint32_t *d_query_seed_ids, uint32_t *d_query_seed_starts,
+    uint32_t *d_query_ids, uint32_t *d_query_concatenated_positions,
+    uint32_t *temp_array, void *stream);
+/* ExtendWithTriggerAsync (src/ungapped_extender_gpu.cu:854-899): reverse
+ * X-drop from (q-1, d-1), forward from (q, d) while the sum is not above the
+ * query's trigger; flags[i] = 1 when the sum exceeds the trigger.  NULL host
+ * query ids / positions skip their upload (the device copies are reused). */
+int gzb_ungapped_extender_extend_with_trigger_async(
+    gzb_ungapped_extender *h, size_t size, const uint32_t *query_ids,
+    const uint32_t *query_concatenated_positions,
+    const uint32_t *database_positions, int8_t *flags, uint32_t *d_query_ids,
+    uint32_t *d_query_concatenated_positions, uint32_t *d_database_positions,
+    int8_t *d_flags, int32_t *d_temp_array, void *stream);
+
+/* ---- GappedExtenderGpu (src/gapped_extender_gpu.h:19-60) --------------- */
+typedef struct gzb_gapped_extender gzb_gapped_extender;
+int gzb_gapped_extender_create(gzb_gapped_extender **out);
+int gzb_gapped_extender_destroy(gzb_gapped_extender *h);
+/* SetQueries / SetDatabase / SetScoreParameters
+ * (src/gapped_extender_gpu.cu:748-767) */
+int gzb_gapped_extender_set_queries(gzb_gapped_extender *h,
+                                    uint8_t sequence_delimiter,
+                                    const uint8_t *d_query_sequence);
+int gzb_gapped_extender_set_database(gzb_gapped_extender *h,
+                                     const uint8_t *d_database_sequence);
+int gzb_gapped_extender_set_score_parameters(gzb_gapped_extender *h,
+                                             const int32_t *d_score_matrix,
+                                             uint32_t number_letters,
+                                             int gap_open, int gap_extension,
+                                             int cutoff);
+/* ConvertToGappedExtensionSeedsAsync (src/gapped_extender_gpu.cu:769-800):
+ * d_out[i] = positions[seed_positions[i]] for query and database
+ * positions, the host arrays being uploaded first. */
+int gzb_gapped_extender_convert_to_gapped_extension_seeds_async(
+    gzb_gapped_extender *h, size_t size, int reverse,
+    const uint32_t *seed_positions,
+    const uint32_t *query_concatenated_positions,
+    const uint32_t *database_positions, uint32_t *d_seed_positions,
+    uint32_t *d_temp_array, uint32_t *d_query_concatenated_positions,
+    uint32_t *d_database_positions, void *stream);
+/* ExtendOneSideScoreOnlyAsync (src/gapped_extender_gpu.cu:802-853): one
+ * score-only affine X-drop extension per seed from the device positions
+ * (query = sequence0, database = sequence1), forward or reverse.  Positions
+ * are replaced by the absolute positions of the best cell; positions and
+ * scores are copied back to the host arrays.  Bit-identical to the CPU
+ * GappedExtender::ExtendOneSideScoreOnly (src/gapped_extender.cpp:306-471)
+ * for every query length (no 128-residue limit). */
+int gzb_gapped_extender_extend_one_side_score_only_async(
+    gzb_gapped_extender *h, size_t size, int reverse,
+    uint32_t *query_concatenated_positions, uint32_t *database_positions,
+    int32_t *scores, uint32_t *d_query_concatenated_positions,
+    uint32_t *d_database_positions, int32_t *d_scores, void *stream);
+/* DP cells evaluated by this handle's extensions so far (synchronous). */
+int gzb_gapped_extender_cells(gzb_gapped_extender *h, uint64_t *cells);
+
+/* ---- presearch engine ---------------------------------------------------
+ * Replaces the device side of AlignerGpuPresearchThread::Run for one
+ * database chunk: the seed search of SeedSearcherGpu
+ * (src/seed_searcher_gpu.cpp:186-537) with the query lists of
+ * SeedSearcherGpuQueryParameters::Build
+ * (src/seed_searcher_gpu_query_parameters.cpp:17-272), distance filtering,
+ * ungapped extension with trigger, the chain filter
+ * (src/chain_filter.cpp:24-99), both gapped extensions and the top-b merge
+ * AlignerCommon::AddResults (src/aligner_common.h:147-274). */
+typedef struct gzb_engine gzb_engine;
+
+typedef struct {
+  int32_t chunk_id;
+  int32_t subject_id;   /* sequence index in the chunk */
+  int32_t score;        /* reverse + forward gapped score */
+  uint32_t hit_q, hit_d;     /* seed: position in query, in chunk */
+  uint32_t start_q, start_d; /* alignment start (inclusive) */
+  uint32_t end_q, end_d;     /* alignment end (inclusive) */
+} gzb_result;
+
+typedef struct {
+  uint64_t distance_seeds;     /* representative x check-position pairs */
+  uint64_t ungapped_seeds;     /* ungapped extensions run */
+  uint64_t ungapped_hits;      /* survivors (score > trigger) */
+  uint64_t chained_hits;       /* survivors of the chain filter */
+  uint64_t gapped_extensions;  /* one-side extensions */
+  uint64_t gapped_cells;       /* DP cells of the gapped extensions */
+  uint64_t gapped_fallbacks;   /* extensions the one-thread kernel handed on */
+  uint64_t ungapped_steps;     /* residue pairs examined by ungapped X-drop */
+  uint64_t kernel_launches;    /* engine kernels launched by the presearch */
+} gzb_counters;
+
+/* schedule of the gapped stage */
+#define GZB_SCHEDULE_PLAIN 0    /* one launch, one warp per extension */
+#define GZB_SCHEDULE_BATCHED 1  /* persistent warps on a device work queue,
+                                   seeds ordered longest first by the cost
+                                   model */
+
+int gzb_engine_create(int device, gzb_engine **out);
+int gzb_engine_destroy(gzb_engine *e);
+int gzb_engine_set_params(gzb_engine *e, const gzb_params *p);
+/* Uploads one database chunk (concatenated codes with delimiters,
+ * offsets[i] = first residue of sequence i, offsets[n] = length) and builds
+ * its seed index on the device. */
+int gzb_engine_set_database(gzb_engine *e, int32_t chunk_id,
+                            const uint8_t *codes, uint64_t length,
+                            const uint32_t *offsets,
+                            uint32_t number_sequences, void *stream);
+/* Uploads the queries (concatenated, shared delimiters; offsets[i] is the
+ * leading delimiter of query i; lengths[i] = residues + 2) with their
+ * per-query ungapped X-drop and trigger, and builds the query hash lists. */
+int gzb_engine_set_queries(gzb_engine *e, const uint8_t *codes,
+                           uint64_t length, const uint32_t *offsets,
+                           const uint32_t *lengths, uint32_t number_queries,
+                           const int32_t *ungapped_cutoffs,
+                           const int32_t *gapped_triggers, void *stream);
+/* Runs the presearch of the resident queries against the resident chunk
+ * and merges into the per-query top-b lists kept on the device.  Call
+ * gzb_engine_reset_results before the first chunk of a query set. */
+int gzb_engine_presearch(gzb_engine *e, int schedule, void *stream);
+int gzb_engine_reset_results(gzb_engine *e, void *stream);
+/* Copies the merged results to the host: counts[number_queries] and
+ * results[number_queries * max_number_results] (row i holds counts[i]
+ * valid entries, best first).  Synchronises `stream`. */
+int gzb_engine_get_results(gzb_engine *e, uint32_t *counts,
+                           gzb_result *results, void *stream);
+int gzb_engine_get_counters(gzb_engine *e, gzb_counters *out);
+/* Device-side ungapped survivors of the last presearch, sorted by
+ * (query, database position, query position): copies up to `capacity`
+ * triples and returns the total in *count.  Synchronises `stream`. */
+int gzb_engine_get_hits(gzb_engine *e, uint32_t *query_ids,
+                        uint32_t *query_positions,
+                        uint32_t *database_positions, uint64_t capacity,
+                        uint64_t *count, void *stream);
+/* Device-resident database index arrays (for inspection / tests):
+ * which = 0 nc_keys, 1 nc_offsets, 2 nc_values, 3 rep_keys, 4 rep_offsets,
+ * 5 rep_cluster_ids, 6 rep_positions, 7 member_offsets,
+ * 8 member_positions.  Copies up to `capacity` entries to `out` and returns
+ * the element count in *count.  Synchronises `stream`. */
+int gzb_engine_get_index_array(gzb_engine *e, int which, uint32_t *out,
+                               uint64_t capacity, uint64_t *count,
+                               void *stream);
+/* Device-resident query hash lists (for inspection / tests): which = 0 list
+ * hashes, 1 list offsets (lists + 1), 2 check positions per list (they come
+ * first in each list), 3 entry query ids, 4 entry positions within the
+ * query.  Same copy semantics as gzb_engine_get_index_array. */
+int gzb_engine_get_list_array(gzb_engine *e, int which, uint32_t *out,
+                              uint64_t capacity, uint64_t *count, void *stream);
+/* Time of the last presearch, per stage, in milliseconds (device events):
+ * [0] list lookup, [1] seed search + ungapped + sort, [2] chain filter,
+ * [3] gapped extension, [4] merge, [5] total. */
+int gzb_engine_get_stage_ms(gzb_engine *e, float *ms6);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

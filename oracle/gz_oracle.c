@@ -587,6 +587,21 @@ struct gzo_query_lists {
   size_t len[5];
 };
 
+typedef struct {
+  uint32_t hash, nocheck, qid, pos;
+} ent;
+
+static const ent *qsort_ent_base; /* qsort has no context argument */
+
+static int cmp_ent_order(const void *a, const void *b) {
+  const ent *x = &qsort_ent_base[*(const uint32_t *)a];
+  const ent *y = &qsort_ent_base[*(const uint32_t *)b];
+  if (x->hash != y->hash) return x->hash < y->hash ? -1 : 1;
+  if (x->nocheck != y->nocheck) return x->nocheck < y->nocheck ? -1 : 1;
+  uint32_t ia = *(const uint32_t *)a, ib = *(const uint32_t *)b;
+  return ia < ib ? -1 : (ia > ib ? 1 : 0);
+}
+
 gzo_query_lists *gzo_query_lists_build(const gzo_params *p,
                                        const uint8_t *queries,
                                        const uint32_t *offsets,
@@ -594,10 +609,6 @@ gzo_query_lists *gzo_query_lists_build(const gzo_params *p,
                                        uint32_t number_queries) {
   const uint32_t L = (uint32_t)p->subsequence_length;
   size_t cap = 1024, n = 0;
-  /* key: hash(32) | nocheck(1) | query(..) ; store entries separately */
-  typedef struct {
-    uint32_t hash, nocheck, qid, pos;
-  } ent;
   ent *e = (ent *)xmalloc(sizeof(ent) * cap);
   for (uint32_t qid = 0; qid < number_queries; ++qid) {
     const uint8_t *q = queries + offsets[qid];
@@ -627,16 +638,15 @@ gzo_query_lists *gzo_query_lists_build(const gzo_params *p,
       off = end + 1;
     }
   }
-  /* stable order: (hash, nocheck, qid, pos) -- already qid/pos ascending,
-   * so a counting pass over sorted keys suffices */
-  uint64_t *keys = (uint64_t *)xmalloc(sizeof(uint64_t) * (n ? n : 1));
-  for (size_t i = 0; i < n; ++i)
-    keys[i] = ((uint64_t)e[i].hash << 33) | ((uint64_t)e[i].nocheck << 32) |
-              (uint64_t)i;
-  qsort(keys, n, sizeof(uint64_t), cmp_u64);
+  /* order (hash, nocheck, entry index); entries are already in (query,
+   * position) order, so the index keeps that order inside each part */
+  qsort_ent_base = e;
+  uint32_t *order = (uint32_t *)xmalloc(sizeof(uint32_t) * (n ? n : 1));
+  for (size_t i = 0; i < n; ++i) order[i] = (uint32_t)i;
+  qsort(order, n, sizeof(uint32_t), cmp_ent_order);
   size_t nl = 0;
   for (size_t i = 0; i < n; ++i)
-    if (i == 0 || (keys[i] >> 33) != (keys[i - 1] >> 33)) ++nl;
+    if (i == 0 || e[order[i]].hash != e[order[i - 1]].hash) ++nl;
   gzo_query_lists *x = (gzo_query_lists *)xcalloc(1, sizeof(gzo_query_lists));
   x->arr[0] = (uint32_t *)xmalloc(4 * (nl ? nl : 1));
   x->arr[1] = (uint32_t *)xmalloc(4 * (nl + 1));
@@ -645,8 +655,8 @@ gzo_query_lists *gzo_query_lists_build(const gzo_params *p,
   x->arr[4] = (uint32_t *)xmalloc(4 * (n ? n : 1));
   size_t l = 0;
   for (size_t i = 0; i < n; ++i) {
-    const ent *t = &e[(uint32_t)keys[i]];
-    if (i == 0 || (keys[i] >> 33) != (keys[i - 1] >> 33)) {
+    const ent *t = &e[order[i]];
+    if (i == 0 || t->hash != e[order[i - 1]].hash) {
       x->arr[0][l] = t->hash;
       x->arr[1][l] = (uint32_t)i;
       ++l;
@@ -661,7 +671,7 @@ gzo_query_lists *gzo_query_lists_build(const gzo_params *p,
   x->len[2] = nl;
   x->len[3] = n;
   x->len[4] = n;
-  free(keys);
+  free(order);
   free(e);
   return x;
 }

@@ -99,7 +99,7 @@ class Oracle:
         seq = np.ascontiguousarray(seq, dtype=np.uint8)
         h = C.c_uint32()
         ln = C.c_uint32()
-        r = self.L.gzo_hash(pr.ptr, C.cast(C.c_void_p(seq.ctypes.data + pos), u8p),
+        r = self.L.gzo_hash(pr.ptr, C.cast(C.c_void_p(seq.ctypes.data + int(pos)), u8p),
                             C.byref(h), C.byref(ln))
         return r, h.value, ln.value
 
@@ -107,22 +107,22 @@ class Oracle:
         pr = _Params(params)
         s0 = np.ascontiguousarray(seq0, dtype=np.uint8)
         s1 = np.ascontiguousarray(seq1, dtype=np.uint8)
-        return self.L.gzo_distance(pr.ptr, _p(s0, u8p), c0, _p(s1, u8p), c1)
+        return self.L.gzo_distance(pr.ptr, _p(s0, u8p), int(c0), _p(s1, u8p), int(c1))
 
     def ungapped_one_side(self, params, seq0, p0, seq1, p1, reversed_, cutoff):
         pr = _Params(params)
         s0 = np.ascontiguousarray(seq0, dtype=np.uint8)
         s1 = np.ascontiguousarray(seq1, dtype=np.uint8)
         return self.L.gzo_ungapped_one_side(
-            pr.ptr, C.cast(C.c_void_p(s0.ctypes.data + p0), u8p),
-            C.cast(C.c_void_p(s1.ctypes.data + p1), u8p), int(reversed_), int(cutoff))
+            pr.ptr, C.cast(C.c_void_p(s0.ctypes.data + int(p0)), u8p),
+            C.cast(C.c_void_p(s1.ctypes.data + int(p1)), u8p), int(reversed_), int(cutoff))
 
     def ungapped_with_trigger(self, params, query, qpos, db, dpos, cutoff, trigger):
         pr = _Params(params)
         q = np.ascontiguousarray(query, dtype=np.uint8)
         d = np.ascontiguousarray(db, dtype=np.uint8)
-        return self.L.gzo_ungapped_with_trigger(pr.ptr, _p(q, u8p), qpos, _p(d, u8p),
-                                                dpos, int(cutoff), int(trigger))
+        return self.L.gzo_ungapped_with_trigger(pr.ptr, _p(q, u8p), int(qpos), _p(d, u8p),
+                                                int(dpos), int(cutoff), int(trigger))
 
     def gapped_one_side(self, params, seq0, p0, seq1, p1, reversed_, cutoff):
         pr = _Params(params)
@@ -131,8 +131,8 @@ class Oracle:
         b, q, d = C.c_int32(), C.c_int32(), C.c_int32()
         cells = C.c_uint64()
         self.L.gzo_gapped_one_side(
-            pr.ptr, C.cast(C.c_void_p(s0.ctypes.data + p0), u8p),
-            C.cast(C.c_void_p(s1.ctypes.data + p1), u8p), int(reversed_), int(cutoff),
+            pr.ptr, C.cast(C.c_void_p(s0.ctypes.data + int(p0)), u8p),
+            C.cast(C.c_void_p(s1.ctypes.data + int(p1)), u8p), int(reversed_), int(cutoff),
             C.byref(b), C.byref(q), C.byref(d), C.byref(cells))
         return b.value, q.value, d.value, cells.value
 
@@ -142,7 +142,7 @@ class Oracle:
         d = np.ascontiguousarray(db, dtype=np.uint8)
         hq = np.array(hq, dtype=np.uint32)
         hd = np.array(hd, dtype=np.uint32)
-        n = self.L.gzo_chain_filter(pr.ptr, _p(q, u8p), qlen, int(cutoff), _p(d, u8p),
+        n = self.L.gzo_chain_filter(pr.ptr, _p(q, u8p), int(qlen), int(cutoff), _p(d, u8p),
                                     _p(hq, u32p), _p(hd, u32p), len(hq))
         return hq[:n].copy(), hd[:n].copy()
 
@@ -178,9 +178,11 @@ class Oracle:
     def presearch(self, params, db, queries, query_begin=0, query_end=None):
         """Returns (results per query as RESULT_DTYPE arrays, counters dict,
         ungapped survivors (qid, q, d))."""
+        import time
         pr = _Params(params)
         dbc = np.ascontiguousarray(db.codes, dtype=np.uint8)
         idx = self.L.gzo_db_index_build(pr.ptr, _p(dbc, u8p), len(dbc))
+        t0 = time.perf_counter()  # search time: query lists + presearch
         lists = self.L.gzo_query_lists_build(pr.ptr, _p(queries.codes, u8p),
                                              _p(queries.offsets, u32p),
                                              _p(queries.lengths, u32p), queries.number)
@@ -195,6 +197,7 @@ class Oracle:
                                      _p(cut, i32p), _p(trig, i32p), _p(dbc, u8p), len(dbc),
                                      _p(offs, u32p), db.number_sequences,
                                      query_begin, query_end)
+        search_seconds = time.perf_counter() - t0
         results = []
         for qi in range(queries.number):
             ptr = C.c_void_p()
@@ -207,6 +210,7 @@ class Oracle:
         cnt = (C.c_uint64 * 6)()
         self.L.gzo_presearch_counters(C.c_void_p(h), C.byref(cnt))
         counters = dict(zip(COUNTER_NAMES, [int(v) for v in cnt]))
+        counters["search_seconds"] = search_seconds
         a, b, c = u32p(), u32p(), u32p()
         n = self.L.gzo_presearch_hits(C.c_void_p(h), C.byref(a), C.byref(b), C.byref(c))
         hits = tuple(np.ctypeslib.as_array(x, shape=(n,)).copy() if n else np.zeros(0, np.uint32)
@@ -274,8 +278,8 @@ class Reference:
         s0 = np.ascontiguousarray(seq0, dtype=np.uint8)
         s1 = np.ascontiguousarray(seq1, dtype=np.uint8)
         return self.L.gzr_ungapped_one_side(
-            pr.ptr, C.cast(C.c_void_p(s0.ctypes.data + p0), u8p),
-            C.cast(C.c_void_p(s1.ctypes.data + p1), u8p), int(reversed_), int(cutoff))
+            pr.ptr, C.cast(C.c_void_p(s0.ctypes.data + int(p0)), u8p),
+            C.cast(C.c_void_p(s1.ctypes.data + int(p1)), u8p), int(reversed_), int(cutoff))
 
     def gapped_one_side(self, params, seq0, p0, len0, seq1, p1, reversed_, cutoff):
         pr = _Params(params)
@@ -283,8 +287,8 @@ class Reference:
         s1 = np.ascontiguousarray(seq1, dtype=np.uint8)
         b, q, d = C.c_int32(), C.c_int32(), C.c_int32()
         self.L.gzr_gapped_one_side(
-            pr.ptr, C.cast(C.c_void_p(s0.ctypes.data + p0), u8p), len0,
-            C.cast(C.c_void_p(s1.ctypes.data + p1), u8p), int(reversed_), int(cutoff),
+            pr.ptr, C.cast(C.c_void_p(s0.ctypes.data + int(p0)), u8p), len0,
+            C.cast(C.c_void_p(s1.ctypes.data + int(p1)), u8p), int(reversed_), int(cutoff),
             C.byref(b), C.byref(q), C.byref(d))
         return b.value, q.value, d.value
 

@@ -1,0 +1,58 @@
+"""The C ABI library builds, loads without a GPU and exports every function
+the public header declares; error reporting works without a device."""
+import ctypes
+import os
+
+import pytest
+
+
+def test_library_exports_header_symbols():
+    from gzb import build as B
+    from gzb import native as N
+    if not os.path.exists(B.LIB):
+        B.build()
+    lib = ctypes.CDLL(B.LIB)
+    declared = N.symbols_declared_in_header()
+    assert len(declared) >= 35
+    missing = [s for s in declared if not hasattr(lib, s)]
+    assert missing == []
+
+
+def test_error_strings_without_device():
+    from gzb import native as N
+    L = N.lib()
+    assert L.gzb_error_string(0).decode() == "ok"
+    assert "invalid" in L.gzb_error_string(1).decode()
+    h = ctypes.c_void_p()
+    assert L.gzb_distance_calculator_create(ctypes.byref(h)) == 0
+    # using a handle before set-up reports GZB_ERR_INVALID with a message
+    rc = L.gzb_distance_calculator_calculate_distances_async(
+        h, 1, None, None, None, None, None, None, None)
+    assert rc == 1 and b"not set up" in L.gzb_last_error()
+    assert L.gzb_distance_calculator_destroy(h) == 0
+
+
+def test_engine_create_reports_missing_device():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("device present")
+    from gzb import native as N
+    with pytest.raises(N.GzbError):
+        N.PresearchEngine(0)
+
+
+def test_params_record_matches_header_layout(tmp_path):
+    import subprocess
+    from gzb import params as P
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "size.c"
+    src.write_text('#include "ghostz_b200.h"\n#include <stdio.h>\n#include <stddef.h>\n'
+                   'int main(void){printf("%zu %zu %zu\\n", sizeof(gzb_params), '
+                   'offsetof(gzb_params, code_scores), sizeof(gzb_result));return 0;}\n')
+    exe = tmp_path / "size"
+    subprocess.check_call(["gcc", "-I", os.path.join(root, "include"), str(src), "-o", str(exe)])
+    size, off, rsize = map(int, subprocess.check_output([str(exe)]).split())
+    assert size == P.PARAMS_DTYPE.itemsize
+    assert off == P.PARAMS_DTYPE.fields["code_scores"][1]
+    from gzb import native as N
+    assert rsize == N.RESULT_DTYPE.itemsize

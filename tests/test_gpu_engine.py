@@ -1,0 +1,108 @@
+"""Whole-presearch parity on the GPU: device index, seed survivors and the
+per-query top-b lists of the engine against the CPU oracle, bit for bit."""
+import numpy as np
+import pytest
+
+from gzb import params as P
+from gzb import workload as W
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def engine():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from gzb import native as N
+    e = N.PresearchEngine(0)
+    yield e
+    e.close()
+
+
+def _small(seed_db=501, seed_q=502, n_db=1500, n_q=120, median=250):
+    db = W.make_database(n_db, seed_db, median=median)
+    q = W.make_queries(db, n_q, seed_q, median=median)
+    return db, q
+
+
+def test_device_index_matches_oracle(engine, oracle, params):
+    db, _ = _small()
+    engine.set_params(params)
+    engine.set_database(db)
+    got = engine.index_arrays()
+    exp = oracle.db_index(params, db.codes)
+    for name in ("nc_keys", "nc_offsets", "nc_values", "rep_keys", "rep_offsets",
+                 "rep_positions", "member_offsets", "member_positions"):
+        assert np.array_equal(got[name], exp[name]), name
+
+
+def _compare(engine, oracle, params, db, q, schedule=0):
+    engine.set_params(params)
+    engine.set_database(db)
+    engine.set_queries(q)
+    # query hash lists (SeedSearcherGpuQueryParameters) and the device index
+    gl = engine.list_arrays()
+    el = oracle.query_lists(params, q)
+    for name in ("hashes", "offsets", "check_counts", "query_ids", "positions"):
+        assert np.array_equal(gl[name], el[name]), name
+    gi = engine.index_arrays()
+    ei = oracle.db_index(params, db.codes)
+    for name in ("nc_keys", "nc_offsets", "nc_values", "rep_keys", "rep_offsets",
+                 "rep_positions", "member_offsets", "member_positions"):
+        assert np.array_equal(gi[name], ei[name]), name
+    engine.presearch(schedule)
+    got = engine.results()
+    res, cnt, hits = oracle.presearch(params, db, q)
+    gh = engine.hits()
+    assert np.array_equal(gh[0], hits[0]) and np.array_equal(gh[1], hits[1]) and \
+        np.array_equal(gh[2], hits[2]), "ungapped survivors differ"
+    gc = engine.counters()
+    for k in ("distance_seeds", "ungapped_seeds", "ungapped_hits", "chained_hits",
+              "gapped_extensions", "gapped_cells"):
+        assert gc[k] == cnt[k], (k, gc[k], cnt[k])
+    for i in range(q.number):
+        assert np.array_equal(got[i], res[i]), i
+    return cnt
+
+
+def test_presearch_matches_oracle_small(engine, oracle, params):
+    db, q = _small()
+    cnt = _compare(engine, oracle, params, db, q)
+    assert cnt["chained_hits"] > 0 and cnt["gapped_cells"] > 0
+
+
+def test_presearch_without_clustering(engine, oracle):
+    p = P.make_params(clustering=False)
+    db, q = _small(601, 602, n_db=800, n_q=60)
+    _compare(engine, oracle, p, db, q)
+
+
+def test_presearch_v2_results(engine, oracle):
+    p = P.make_params(max_number_one_subject_results=3, max_number_results=5)
+    db, q = _small(701, 702, n_db=800, n_q=60)
+    _compare(engine, oracle, p, db, q)
+
+
+def test_presearch_edge_queries(engine, oracle, params):
+    # very short queries (no seeds), a query made of X, and a long homolog
+    db = W.make_database(400, 801, median=200)
+    rng = np.random.default_rng(9)
+    src = db.codes[db.offsets[3]:db.offsets[4] - 1]
+    seqs = [W.random_residues(rng, 5), np.full(40, 24, np.uint8), src.copy(),
+            W.mutate(rng, src, 0.7), W.random_residues(rng, 9)]
+    q = W.pack_queries(seqs)
+    _compare(engine, oracle, params, db, q)
+
+
+def test_presearch_repeated_calls_identical(engine, params):
+    db, q = _small(901, 902, n_db=600, n_q=50)
+    engine.set_params(params)
+    engine.set_database(db)
+    engine.set_queries(q)
+    engine.presearch(0)
+    a = engine.results()
+    engine.reset_results()
+    engine.presearch(0)
+    b = engine.results()
+    assert all(np.array_equal(x, y) for x, y in zip(a, b))
