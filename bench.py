@@ -49,7 +49,7 @@ WORKLOADS = {
     "protein-1k-x-200k": (200_000, 211, 1_000, 212),   # small case for profiling
 }
 
-# algorithmic bytes of the dominant kernels (measurement):
+# algorithmic bytes of the dominant kernels:
 # ungapped seed: two residue bytes per residue pair examined; distance seed:
 # 8 B of centres + 2L window bytes + 1 B result.
 BYTES_PER_UNGAPPED_STEP = 2

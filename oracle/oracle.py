@@ -16,6 +16,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libgzref.so")
+# reference checkout the pin library is compiled from (build-time only)
+REF_ROOT = os.environ.get("GZ_REFERENCE_ROOT", "/root/reference")
 
 u8p = C.POINTER(C.c_uint8)
 u32p = C.POINTER(C.c_uint32)
@@ -32,8 +34,8 @@ COUNTER_NAMES = ("distance_seeds", "ungapped_seeds", "ungapped_hits",
 
 def build(ref: bool = False) -> None:
     subprocess.check_call(["make", "-s", "-C", HERE, "oracle"])
-    if ref and os.path.isdir("/root/reference/src"):
-        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+    if ref and os.path.isdir(os.path.join(REF_ROOT, "src")):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF_ROOT={REF_ROOT}"])
 
 
 def _p(a, t):

@@ -56,3 +56,29 @@ def test_params_record_matches_header_layout(tmp_path):
     assert off == P.PARAMS_DTYPE.fields["code_scores"][1]
     from gzb import native as N
     assert rsize == N.RESULT_DTYPE.itemsize
+
+
+def test_cpp_adapters_compile_and_link(tmp_path):
+    """The header-only C++ classes with the reference's names compile and
+    link against the library (no GPU needed: nothing is called)."""
+    import subprocess
+    from gzb import build as B
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "use.cpp"
+    src.write_text(
+        '#include "ghostz_gpu_adapters.h"\n'
+        'using namespace ghostz_b200;\n'
+        'int run(cudaStream_t s) {\n'
+        '  DistanceCalculatorGpu d; UngappedExtenderGpu u; GappedExtenderGpu g;\n'
+        '  uint32_t *p = 0; char *f = 0; int *i = 0;\n'
+        '  d.SetSubsequenceLength(10);\n'
+        '  u.ExtendWithTriggerAsync(0, p, p, p, f, p, p, p, f, i, s);\n'
+        '  return g.ExtendOneSideScoreOnlyAsync(0, true, p, p, i, p, p, i, s);\n'
+        '}\n'
+        'int main() { return 0; }\n')
+    exe = tmp_path / "use"
+    subprocess.check_call([
+        "g++", "-std=c++11", "-I", os.path.join(root, "include"),
+        "-I", os.path.join(root, "ghostz-gpu_b200", "adapters"),
+        "-I", "/usr/local/cuda/include", str(src), "-o", str(exe),
+        B.LIB, "-Wl,-rpath," + os.path.dirname(B.LIB)])
