@@ -76,6 +76,9 @@ def _declare(L):
         "gzb_gapped_extender_convert_to_gapped_extension_seeds_async": [V, SZ, C.c_int, V, V, V, V, V, V, V, V],
         "gzb_gapped_extender_extend_one_side_score_only_async": [V, SZ, C.c_int, V, V, V, V, V, V, V],
         "gzb_gapped_extender_cells": [V, V],
+        "gzb_gapped_extend_one_side_score_only_noalloc": [V, V, C.c_uint8, V, U32, C.c_int,
+                                                          C.c_int, C.c_int, SZ, C.c_int, V, V,
+                                                          V, V],
         "gzb_engine_create": [C.c_int, V],
         "gzb_engine_destroy": [V],
         "gzb_engine_set_params": [V, V],

@@ -179,6 +179,28 @@ int gzb_gapped_extender_extend_one_side_score_only_async(
 /* DP cells evaluated by this handle's extensions so far (synchronous). */
 int gzb_gapped_extender_cells(gzb_gapped_extender *h, uint64_t *cells);
 
+/* Gapped one-side extension that allocates no device memory.  No
+ * counterpart in the reference: it is the same computation as
+ * gzb_gapped_extender_extend_one_side_score_only_async (device buffers only,
+ * positions updated in place, scores written; no host copies) for callers
+ * that cannot call cudaMalloc themselves -- code running under a host runtime
+ * that owns all device memory through its own pool, or a latency-critical
+ * loop that cannot take an allocation's implicit device synchronisation.
+ * Its scratch is one fixed device array in the library (about 12 MB, held on
+ * every GPU that loads the library until exit).  Limits: at most 2^20
+ * extensions per call, and extensions needing the serial fallback may use
+ * bands of at most 8192 columns; larger requests return GZB_ERR_OVERFLOW.
+ * Every call shares that array: calls that overlap on the GPU race and must
+ * be serialised by the caller.  The first call on a device looks up the
+ * array's address, so make it before any stream capture.  Synchronises
+ * `stream` before returning. */
+int gzb_gapped_extend_one_side_score_only_noalloc(
+    const uint8_t *d_query_sequence, const uint8_t *d_database_sequence,
+    uint8_t sequence_delimiter, const int32_t *d_score_matrix,
+    uint32_t number_letters, int gap_open, int gap_extension, int cutoff,
+    size_t size, int reverse, uint32_t *d_query_concatenated_positions,
+    uint32_t *d_database_positions, int32_t *d_scores, void *stream);
+
 /* ---- presearch engine ---------------------------------------------------
  * Replaces the device side of AlignerGpuPresearchThread::Run for one
  * database chunk: the seed search of SeedSearcherGpu
