@@ -200,7 +200,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--schedule", default="plain", choices=["plain", "batched"])
+    ap.add_argument("--schedule", default="batched", choices=["plain", "batched"])
+    ap.add_argument("--train-sets", type=int, default=8)
     ap.add_argument("--workload", default="protein-10k-x-2M", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-queries", type=int, default=10000)
     ap.add_argument("--ref-queries", type=int, default=4000)
@@ -233,35 +234,75 @@ def main():
     torch.cuda.synchronize()
     index_s = time.time() - t
     eng.set_queries(q)
-    schedule = N.SCHEDULE_PLAIN if args.schedule == "plain" else N.SCHEDULE_BATCHED
     stream = torch.cuda.current_stream()
+
+    # ---- cost model for the learned schedule (untimed set-up): pairs logged by
+    # the plain path on config-1-shaped runs (20,000 proteins, 1,000 queries x
+    # train_sets query seeds), trained on the GPU by the engine's own kernels
+    t = time.time()
+    train_pairs, train_loss = 0, None
+    if args.schedule == "batched":
+        from gzb import workload as W
+        tdb = W.make_database(20000, 101)
+        trainer = N.PresearchEngine(local_rank)
+        trainer.set_params(params)
+        trainer.set_database(tdb)
+        trainer.set_logging(True, 1 << 23)
+        for k in range(args.train_sets):
+            trainer.set_queries(W.make_queries(tdb, 1000, 102 + k))
+            trainer.presearch(N.SCHEDULE_PLAIN)
+        model, train_loss = trainer.train_cost_model(epochs=12, batch=4096, lr=3e-3, seed=7)
+        train_pairs = len(trainer.get_log()[1])
+        trainer.close()
+        eng.set_cost_model(model)
+        eng.set_queries(q)
+    train_s = time.time() - t
 
     def barrier():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
 
-    # ---- device-resident timed loop
-    for _ in range(args.warmup):
-        eng.reset_results()
-        eng.presearch(schedule)
-    barrier()
+    def timed(sched):
+        for _ in range(args.warmup):
+            eng.reset_results(stream)
+            eng.presearch(sched, stream)
+        barrier()
+        stage = {k: 0.0 for k in ("lookup", "seed_ungapped", "chain", "gapped", "merge", "total")}
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            eng.reset_results(stream)
+            eng.presearch(sched, stream)
+            for k, v in eng.stage_ms().items():
+                stage[k] += v
+        ev1.record(stream)
+        barrier()
+        return ev0.elapsed_time(ev1), {k: v / args.steps for k, v in stage.items()}
+
     sampler = ClockSampler(local_rank)
     sampler.start()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    stage = {k: 0.0 for k in ("lookup", "seed_ungapped", "chain", "gapped", "merge", "total")}
-    ev0.record(stream)
-    for _ in range(args.steps):
-        eng.reset_results(stream)
-        eng.presearch(schedule, stream)
-        for k, v in eng.stage_ms().items():
-            stage[k] += v
-    ev1.record(stream)
-    barrier()
-    dev_ms = ev0.elapsed_time(ev1)
+    runs = {}
+    order = ["plain"] + (["batched", "oracle"] if args.schedule == "batched" else [])
+    sched_id = {"plain": N.SCHEDULE_PLAIN, "batched": N.SCHEDULE_BATCHED,
+                "oracle": N.SCHEDULE_ORACLE}
+    results_by = {}
+    for name in order:
+        ms, st = timed(sched_id[name])
+        cnt = eng.counters()
+        runs[name] = {"ms": ms, "stage": st, "counters": cnt}
+        if name == "batched":
+            runs[name]["mean_abs_log2_cost_error"] = eng.schedule_stats()[0]
+        results_by[name] = eng.results()
     clocks = sampler.stop()
-    counters = eng.counters()
-    results = eng.results()
+    head = "batched" if args.schedule == "batched" else "plain"
+    dev_ms, stage = runs[head]["ms"], runs[head]["stage"]
+    counters = runs[head]["counters"]
+    results = results_by[head]
+    identical = all(all(np.array_equal(a, b) for a, b in zip(results_by["plain"], results_by[k]))
+                    for k in results_by)
+    schedule = sched_id[head]
 
     # ---- end-to-end loop through the C ABI with host buffers
     import ctypes
@@ -312,7 +353,22 @@ def main():
     value = world * nq * args.steps / (t_dev / 1e3)
     e2e_value = world * nq * args.steps / (t_e2e / 1e3)
     steps = args.steps
-    st = {k: v / steps for k, v in stage.items()}
+    st = stage
+    sched_report = {}
+    for name, r in runs.items():
+        sched_report[name] = {
+            "value": world * nq * steps / (r["ms"] / 1e3), "ms_per_step": r["ms"] / steps,
+            "gapped_ms": r["stage"]["gapped"], "seed_ungapped_ms": r["stage"]["seed_ungapped"],
+            "dp_gcups_gapped_stage": (r["counters"]["gapped_cells"] / (r["stage"]["gapped"] / 1e3)
+                                      / 1e9) if r["stage"]["gapped"] else None}
+        if "mean_abs_log2_cost_error" in r:
+            sched_report[name]["mean_abs_log2_cost_error"] = r["mean_abs_log2_cost_error"]
+    if "batched" in runs:
+        sched_report["batched_over_plain"] = runs["plain"]["ms"] / runs["batched"]["ms"]
+        sched_report["throughput_lost_vs_oracle"] = 1.0 - runs["oracle"]["ms"] / runs["batched"]["ms"]
+    sched_report["results_identical_across_schedules"] = bool(identical)
+    sched_report["cost_model"] = {"train_pairs": train_pairs, "train_mse_log2": train_loss,
+                                  "setup_s": train_s}
     gcups_stage = counters["gapped_cells"] / (st["gapped"] / 1e3) / 1e9 if st["gapped"] else 0.0
     gcups_step = counters["gapped_cells"] / (t_dev / steps / 1e3) / 1e9
     # roofline of the dominant stage
@@ -338,7 +394,9 @@ def main():
         "warmup": args.warmup, "ms_per_step": t_dev / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded generator with the config's shapes)",
-        "config": {"workload": args.workload, "schedule": args.schedule,
+        "config": {"workload": args.workload,
+                   "schedule": ("batched: learned cost order, persistent work queue"
+                                if args.schedule == "batched" else "plain"),
                    "db_sequences": db.number_sequences, "db_residues": db.length,
                    "queries": nq, "l2": "inputs larger than L2 (database chunk > 126 MB)",
                    "parallelism": f"replicas x{world}"},
@@ -346,7 +404,8 @@ def main():
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": t_e2e / steps,
                 "results_equal_device_loop": bool(e2e_same)},
         "dp_gcups": {"gapped_stage": gcups_stage, "whole_step": gcups_step},
-        "stage_ms": st, "counters": counters, "index_build_s": index_s,
+        "stage_ms": st, "counters": counters, "schedules": sched_report,
+        "index_build_s": index_s,
         "workload_gen_s": gen_s, "clocks": clocks, "roofline": roofline,
         "gpu_launches": int(counters.get("kernel_launches", 0)) * steps,
     }

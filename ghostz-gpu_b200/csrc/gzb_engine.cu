@@ -29,10 +29,29 @@
 #include "gzb_common.h"
 #include "gzb_index.cuh"
 #include "gzb_kernels.cuh"
+#include "gzb_cost.cuh"
 
 namespace cg = cooperative_groups;
 
 namespace gzb {
+
+int cost_predict(const float *d_params, const float *d_x, uint32_t n, float *d_out,
+                 cudaStream_t s);
+int cost_train(const float *d_x, const float *d_y, uint32_t n, float *params, int epochs,
+               int batch, float lr, uint64_t seed, float *final_loss, cudaStream_t s);
+__global__ void gapped_warp_kernel(GappedJob job, const int32_t *__restrict__ matrix,
+                                   int number_letters, int stride, const uint32_t *list,
+                                   const uint32_t *list_count, int reverse,
+                                   const uint8_t *__restrict__ dir, uint32_t *qpos,
+                                   uint32_t *dpos, int32_t *scores, uint32_t *spill,
+                                   uint32_t *spill_count, unsigned long long *cells_total);
+__global__ void gapped_serial_kernel(GappedJob job, const int32_t *__restrict__ matrix,
+                                     int number_letters, int stride, const uint32_t *list,
+                                     const uint32_t *list_count, int reverse,
+                                     const uint8_t *__restrict__ dir, uint32_t *qpos,
+                                     uint32_t *dpos, int32_t *scores, int2 *band_pool,
+                                     int wmask, unsigned long long *cells_total,
+                                     uint32_t *too_long_count);
 
 int run_gapped(const GappedJob &job, const int32_t *matrix, int number_letters,
                int stride, size_t n, const uint32_t *order, int reverse, const uint8_t *dir,
@@ -141,12 +160,6 @@ __global__ void db_entry_kernel(DevParams p, const uint8_t *__restrict__ db,
     state[i] = st;
     window[i] = w;
   }
-}
-
-__device__ __forceinline__ int nibble_mismatches(uint64_t a, uint64_t b) {
-  uint64_t x = a ^ b;
-  x = (x | (x >> 1) | (x >> 2) | (x >> 3)) & 0x1111111111111111ull;
-  return __popcll(x);
 }
 
 // Greedy clustering inside each hash bucket (:117-205): walking the bucket
@@ -342,6 +355,14 @@ __global__ void list_fill_kernel(const uint64_t *keys, uint64_t n, const uint32_
   }
 }
 
+__global__ void entry_window_kernel(DevParams p, const uint8_t *__restrict__ q,
+                                    const uint32_t *__restrict__ cpos, uint64_t n,
+                                    uint64_t *out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = pack_window(p, q + cpos[i]);
+}
+
 __global__ void list_lookup_kernel(DevLists L, DevIndex X, int clustering,
                                    uint64_t *unit_counts) {
   for (uint64_t l = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; l < L.n_lists;
@@ -407,9 +428,7 @@ constexpr int kUnitsPerWarp = 256;
 __global__ void __launch_bounds__(kSeedBlock)
 seed_kernel(SeedArgs a) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
-  __shared__ uint8_t simmap[256];
   load_matrix(sm, a.matrix32, kMatrixStride, kMatrixStride);
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) simmap[i] = i < 32 ? a.p.sim_map[i] : 0;
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
@@ -418,7 +437,6 @@ seed_kernel(SeedArgs a) {
   const int delim = a.p.delimiter;
   const int thr = a.p.distance_threshold;
   const int maxmd = a.p.max_member_distance;
-  const int Ls = a.p.subsequence_length;
   unsigned long long n_dist = 0, n_seed = 0, n_steps = 0;
   for (uint64_t base = warp * kUnitsPerWarp; base < U; base += nwarps * kUnitsPerWarp) {
     const uint64_t last = min(base + kUnitsPerWarp, U) - 1;
@@ -442,6 +460,7 @@ seed_kernel(SeedArgs a) {
         const uint32_t rpos = a.X.rep_positions[r];
         const uint32_t cid = a.X.rep_cluster_ids[r];
         const bool members = a.X.member_offsets[cid + 1] > a.X.member_offsets[cid];
+        const uint64_t rwin = a.X.rep_windows[r];
         const uint8_t *dptr = a.db + rpos;
         for (uint32_t k = pb; k < pe; ++k) {
           const uint32_t qid = a.L.entry_qid[k];
@@ -449,7 +468,7 @@ seed_kernel(SeedArgs a) {
           const uint8_t *qptr = a.q + cpos;
           bool try_rep, pass;
           if (k < pb + nchk) {
-            const int dist = window_distance(qptr, dptr, Ls, simmap);
+            const int dist = nibble_mismatches(a.L.entry_window[k], rwin);
             ++n_dist;
             try_rep = dist <= thr;
             pass = max(dist - maxmd, 0) <= thr;
@@ -617,25 +636,159 @@ __global__ void chain_kernel(DevParams p, const uint8_t *__restrict__ q,
 
 // extension seeds: reverse at (q-1, d-1), forward at (q, d), absolute
 // concatenated query / chunk positions
+__device__ __forceinline__ uint32_t subject_of(const uint32_t *off, uint32_t nseq,
+                                               uint32_t db_len, uint32_t pos);
+
 __global__ void build_ext_kernel(const uint64_t *hits, const uint64_t *begin,
                                  const uint32_t *kept, const uint64_t *surv_off, uint32_t nq,
-                                 const uint32_t *q_offsets, int qbits, int dbits,
-                                 uint64_t n_surv, uint32_t *eq, uint32_t *ed, uint8_t *dir) {
+                                 const uint32_t *q_offsets, const uint32_t *q_lengths,
+                                 const uint32_t *db_offsets, uint32_t nseq, uint32_t db_len,
+                                 int qbits, int dbits, uint64_t n_surv, uint32_t *eq,
+                                 uint32_t *ed, uint8_t *dir, uint32_t *elen0,
+                                 uint32_t *elen1, uint32_t *eqid) {
   const uint64_t qmask = (1ull << qbits) - 1, dmask = (1ull << dbits) - 1;
   for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < nq;
        qi += gridDim.x * blockDim.x) {
     const uint64_t b = begin[qi], o = surv_off[qi];
+    const uint32_t qlen = q_lengths[qi];
     for (uint32_t k = 0; k < kept[qi]; ++k) {
       const uint64_t key = hits[b + k];
       const uint32_t hq = (uint32_t)(key & qmask);
       const uint32_t hd = (uint32_t)((key >> qbits) & dmask);
+      const uint32_t sj = subject_of(db_offsets, nseq, db_len, hd);
+      const uint32_t s0 = db_offsets[sj], s1 = db_offsets[sj + 1] - 1;  // residues [s0, s1)
       eq[o + k] = q_offsets[qi] + hq - 1;
       ed[o + k] = hd - 1;
       dir[o + k] = 1;
+      elen0[o + k] = hq - 1;
+      elen1[o + k] = hd - s0;
+      eqid[o + k] = qi;
       eq[n_surv + o + k] = q_offsets[qi] + hq;
       ed[n_surv + o + k] = hd;
       dir[n_surv + o + k] = 0;
+      elen0[n_surv + o + k] = qlen - 1 - hq;
+      elen1[n_surv + o + k] = s1 - hd;
+      eqid[n_surv + o + k] = qi;
     }
+  }
+}
+
+__global__ void ext_features_kernel(const uint8_t *__restrict__ q, const uint8_t *__restrict__ db,
+                                    int delim, const int32_t *__restrict__ matrix32,
+                                    const int32_t *__restrict__ cutoffs, uint64_t n,
+                                    const uint32_t *eq, const uint32_t *ed, const uint8_t *dir,
+                                    const uint32_t *elen0, const uint32_t *elen1,
+                                    const uint32_t *eqid, float *feat) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    float f[kFeat];
+    const bool rev = dir[i] != 0;
+    extension_features(q + eq[i], db + ed[i], rev ? -1 : 1, delim, matrix32, cutoffs[eqid[i]],
+                       elen0[i], elen1[i], rev, f);
+    for (int k = 0; k < kFeat; ++k) feat[i * kFeat + k] = f[k];
+  }
+}
+
+// sort key: larger predicted cost first; ties keep extension order
+__global__ void cost_keys_kernel(const float *pred, const uint32_t *true_cells, uint64_t n,
+                                 uint32_t *keys, uint32_t *vals) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    float c = pred ? pred[i] : log2f(1.0f + (float)true_cells[i]);
+    if (!(c > -64.0f)) c = -64.0f;
+    if (c > 64.0f) c = 64.0f;
+    const uint32_t u = (uint32_t)((c + 64.0f) * 16777216.0f / 128.0f * 255.0f);
+    keys[i] = 0xFFFFFFFFu - u;
+    vals[i] = (uint32_t)i;
+  }
+}
+
+constexpr int kQueueBlock = 128;
+
+// The batched schedule's gapped kernel: persistent blocks take 32
+// consecutive extensions of the cost-sorted order per warp from a device
+// work queue, so the extensions a warp runs together have similar predicted
+// cost and the longest go first.  cells_out records every extension's DP
+// cells (UINT32_MAX when it was handed to the fallback).
+__global__ void __launch_bounds__(kQueueBlock)
+gapped_lane_queue_kernel(GappedJob job, const int32_t *__restrict__ matrix, uint64_t n,
+                         const uint32_t *__restrict__ order, unsigned long long *queue,
+                         const uint8_t *__restrict__ dir, uint32_t *qpos, uint32_t *dpos,
+                         int32_t *scores, uint32_t *spill, uint32_t *spill_count,
+                         unsigned long long *cells_total, uint32_t *cells_out) {
+  __shared__ int sm[kMatrixStride * kMatrixStride];
+  __shared__ uint32_t cells_s[kLaneW * kQueueBlock];
+  __shared__ uint32_t res_s[(kLaneW / 4) * kQueueBlock];
+  load_matrix(sm, matrix, kMatrixStride, kMatrixStride);
+  __syncthreads();
+  LaneBand band{cells_s, res_s, kQueueBlock, (int)threadIdx.x};
+  const int lane = threadIdx.x & 31;
+  unsigned long long cells = 0;
+  for (;;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(queue, 32ull);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    const uint64_t i = base + lane;
+    if (i < n) {
+      const uint32_t e = order ? order[i] : (uint32_t)i;
+      const bool rev = dir[e] != 0;
+      const uint32_t q = qpos[e], d = dpos[e];
+      GappedOut o = gapped_extend_lane(job, sm, band, q, d, rev);
+      if (o.overflow) {
+        spill[atomicAdd(spill_count, 1u)] = e;
+        if (cells_out) cells_out[e] = 0xFFFFFFFFu;
+      } else {
+        cells += o.cells;
+        qpos[e] = q + (uint32_t)o.pos0;
+        dpos[e] = d + (uint32_t)o.pos1;
+        scores[e] = o.score;
+        if (cells_out) cells_out[e] = o.cells > 0xFFFFFFFEull ? 0xFFFFFFFEu : (uint32_t)o.cells;
+      }
+    }
+    __syncwarp();
+  }
+  cells += __shfl_down_sync(0xffffffffu, cells, 16);
+  cells += __shfl_down_sync(0xffffffffu, cells, 8);
+  cells += __shfl_down_sync(0xffffffffu, cells, 4);
+  cells += __shfl_down_sync(0xffffffffu, cells, 2);
+  cells += __shfl_down_sync(0xffffffffu, cells, 1);
+  if (lane == 0 && cells) atomicAdd(cells_total, cells);
+}
+
+// appends (features, log2(1+cells)) of completed extensions to the log
+__global__ void log_pairs_kernel(const float *feat, const uint32_t *cells_out, uint64_t n,
+                                 float *log_x, float *log_y, unsigned long long *log_count,
+                                 unsigned long long cap) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t c = cells_out[i];
+    if (c == 0xFFFFFFFFu) continue;
+    const unsigned long long slot = atomicAdd(log_count, 1ull);
+    if (slot >= cap) continue;
+    for (int k = 0; k < kFeat; ++k) log_x[slot * kFeat + k] = feat[i * kFeat + k];
+    log_y[slot] = log2f(1.0f + (float)c);
+  }
+}
+
+// sum |pred - log2(1+cells)| and count over completed extensions
+__global__ void abs_error_kernel(const float *pred, const uint32_t *cells_out, uint64_t n,
+                                 double *acc) {
+  double s = 0.0, c = 0.0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t t = cells_out[i];
+    if (t == 0xFFFFFFFFu) continue;
+    s += fabs((double)pred[i] - (double)log2f(1.0f + (float)t));
+    c += 1.0;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_down_sync(0xffffffffu, s, o);
+    c += __shfl_down_sync(0xffffffffu, c, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&acc[0], s);
+    atomicAdd(&acc[1], c);
   }
 }
 
@@ -857,6 +1010,15 @@ struct gzb_engine {
   DBuf tmp, hits, hits_alt, mwork, mcount, moffs, begin, kept, surv_off, slots, eq, ed, edir,
       escore, merge_scratch, heap, ctr, misc, hits_copy;
   int qbits = 1, dbits = 1;
+  // schedule of the gapped stage
+  DBuf elen0, elen1, eqid, efeat, epred, ecells, okeys, okeys2, oidx, oidx2, queue, prev_cells,
+      model_d, mae_acc, log_x, log_y, log_ctr;
+  uint64_t prev_cells_n = 0;
+  bool logging = false;
+  uint64_t log_cap = 0;
+  bool have_model = false;
+  float last_mae = -1.0f;
+  uint64_t last_mae_n = 0;
   uint32_t *spill = nullptr;
   size_t spill_cap = 0;
   uint32_t *gcounters = nullptr;
@@ -870,6 +1032,64 @@ struct gzb_engine {
 };
 
 namespace {
+
+// Gapped stage on the scheduled path: the work-queue lane kernel over
+// `order` (nullptr = extension order), then the warp and serial fallbacks
+// of the regular extender for the extensions it hands on.
+int run_gapped_queue(gzb_engine *e, const GappedJob &job, uint64_t n, const uint32_t *order,
+                     uint32_t *cells_out, cudaStream_t s, uint32_t *n_fallback) {
+  if (n == 0) return GZB_OK;
+  if (e->spill_cap < 2 * n) {
+    cudaFree(e->spill);
+    e->spill = nullptr;
+    e->spill_cap = 0;
+    GZB_CUDA(cudaMalloc(&e->spill, 4 * 2 * n));
+    e->spill_cap = 2 * n;
+  }
+  constexpr int kSerialThreads = 4 * 128, kSerialBand = 1 << 15;
+  if (!e->band_pool) {
+    GZB_CUDA(cudaMalloc(&e->band_pool, sizeof(int2) * (size_t)kSerialThreads * kSerialBand));
+    e->band_wmask = kSerialBand - 1;
+  }
+  GZB_TRY(e->queue.ensure(8));
+  GZB_CUDA(cudaMemsetAsync(e->queue.p, 0, 8, s));
+  GZB_CUDA(cudaMemsetAsync(e->gcounters, 0, 16, s));
+  uint32_t *spill1 = e->spill, *spill2 = e->spill + n;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int per_sm = 4;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gapped_lane_queue_kernel, kQueueBlock, 0);
+  if (per_sm < 1) per_sm = 1;
+  const int32_t *m = e->matrix32.as<int32_t>();
+  gapped_lane_queue_kernel<<<sms * per_sm, kQueueBlock, 0, s>>>(
+      job, m, n, order, e->queue.as<unsigned long long>(), e->edir.as<uint8_t>(),
+      e->eq.as<uint32_t>(), e->ed.as<uint32_t>(), e->escore.as<int32_t>(), spill1, e->gcounters,
+      e->gcells, cells_out);
+  GZB_CUDA(cudaGetLastError());
+  const uint32_t *serial_list = spill1, *serial_count = e->gcounters;
+  if (warp_path_exact(job.cutoff)) {
+    gapped_warp_kernel<<<148 * 4, 256, 0, s>>>(job, m, 32, 32, spill1, e->gcounters, 0,
+                                                e->edir.as<uint8_t>(), e->eq.as<uint32_t>(),
+                                                e->ed.as<uint32_t>(), e->escore.as<int32_t>(),
+                                                spill2, e->gcounters + 1, e->gcells);
+    GZB_CUDA(cudaGetLastError());
+    serial_list = spill2;
+    serial_count = e->gcounters + 1;
+  }
+  gapped_serial_kernel<<<kSerialThreads / 128, 128, 0, s>>>(
+      job, m, 32, 32, serial_list, serial_count, 0, e->edir.as<uint8_t>(), e->eq.as<uint32_t>(),
+      e->ed.as<uint32_t>(), e->escore.as<int32_t>(), e->band_pool, e->band_wmask, e->gcells,
+      e->gcounters + 2);
+  GZB_CUDA(cudaGetLastError());
+  uint32_t h[3] = {0, 0, 0};
+  GZB_CUDA(cudaMemcpyAsync(h, e->gcounters, 12, cudaMemcpyDeviceToHost, s));
+  GZB_CUDA(cudaStreamSynchronize(s));
+  GZB_CHECK(h[2] == 0, GZB_ERR_OVERFLOW, "%u gapped extensions need a band wider than %d columns",
+            h[2], kSerialBand);
+  *n_fallback = h[0];
+  return GZB_OK;
+}
 
 int bits_for(uint64_t v) {  // bits to hold values in [0, v]
   int b = 1;
@@ -996,7 +1216,7 @@ extern "C" int gzb_engine_create(int device, gzb_engine **out) {
   GZB_CHECK(e, GZB_ERR_NOMEM, "host allocation failed");
   e->device = device;
   e->index_bufs.resize(40);
-  e->list_bufs.resize(16);
+  e->list_bufs.resize(20);
   cudaError_t err = cudaMalloc(&e->gcounters, 64);
   if (err == cudaSuccess) err = cudaMalloc(&e->gcells, 8);
   if (err == cudaSuccess) err = cudaMemset(e->gcounters, 0, 64);
@@ -1020,7 +1240,10 @@ extern "C" int gzb_engine_destroy(gzb_engine *e) {
                  &e->tmp, &e->hits, &e->hits_alt, &e->mwork, &e->mcount, &e->moffs,
                  &e->begin, &e->kept, &e->surv_off, &e->slots, &e->eq, &e->ed, &e->edir,
                  &e->escore, &e->merge_scratch, &e->heap, &e->ctr, &e->misc,
-                 &e->hits_copy};
+                 &e->hits_copy, &e->elen0, &e->elen1, &e->eqid, &e->efeat, &e->epred,
+                 &e->ecells, &e->okeys, &e->okeys2, &e->oidx, &e->oidx2, &e->queue,
+                 &e->prev_cells, &e->model_d, &e->mae_acc, &e->log_x, &e->log_y,
+                 &e->log_ctr};
   for (DBuf *b : all) b->release();
   cudaFree(e->spill);
   cudaFree(e->gcounters);
@@ -1133,6 +1356,7 @@ extern "C" int gzb_engine_set_database(gzb_engine *e, int32_t chunk_id, const ui
     X.rep_positions = B[20].as<uint32_t>();
     X.member_offsets = B[21].as<uint32_t>();
     X.member_positions = B[21].as<uint32_t>();
+    X.rep_windows = (uint64_t *)B[21].p;
     GZB_CUDA(cudaStreamSynchronize(s));
     e->have_db = true;
     return GZB_OK;
@@ -1176,6 +1400,12 @@ extern "C" int gzb_engine_set_database(gzb_engine *e, int32_t chunk_id, const ui
   // representatives (order kept: hash, then position)
   uint64_t nrep = 0;
   GZB_TRY(select_flagged(e, sorted, is_rep.as<uint8_t>(), np, other, &nrep, s));
+  DBuf &rwin = B[32];
+  GZB_TRY(rwin.ensure(8 * (nrep + 1)));
+  uint64_t nrw = 0;
+  GZB_TRY(select_flagged(e, window.as<uint64_t>(), is_rep.as<uint8_t>(), np,
+                         rwin.as<uint64_t>(), &nrw, s));
+  X.rep_windows = rwin.as<uint64_t>();
   uint32_t *rk, *ro, *rv;
   uint64_t nrk = 0;
   GZB_TRY(build_csr(e, other, nrep, &rk, &ro, &rv, &nrk, 15, s));
@@ -1303,10 +1533,15 @@ extern "C" int gzb_engine_set_queries(gzb_engine *e, const uint8_t *codes, uint6
   L.entry_cpos = B[13].as<uint32_t>();
   L.n_lists = nl;
   L.n_entries = n;
+  GZB_TRY(B[16].ensure(8 * (n + 1)));
+  L.entry_window = B[16].as<uint64_t>();
   if (n) {
     list_fill_kernel<<<grid1(n + nl + 1, 256), 256, 0, s>>>(
         sorted, n, starts.as<uint32_t>(), nl, e->q_offsets.as<uint32_t>(), number_queries,
         L.hash, L.offsets, L.nchk, L.entry_qid, L.entry_cpos);
+    GZB_CUDA(cudaGetLastError());
+    entry_window_kernel<<<grid1(n, 256), 256, 0, s>>>(e->dp, e->q_buf.as<uint8_t>() + kPad,
+                                                       L.entry_cpos, n, L.entry_window);
     GZB_CUDA(cudaGetLastError());
   } else {
     GZB_CUDA(cudaMemsetAsync(L.offsets, 0, 8, s));
@@ -1482,10 +1717,17 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
   GZB_TRY(e->ed.ensure(4 * (next + 1)));
   GZB_TRY(e->edir.ensure(next + 1));
   GZB_TRY(e->escore.ensure(4 * (next + 1)));
+  GZB_TRY(e->elen0.ensure(4 * (next + 1)));
+  GZB_TRY(e->elen1.ensure(4 * (next + 1)));
+  GZB_TRY(e->eqid.ensure(4 * (next + 1)));
+  e->last_mae = -1.0f;
+  e->last_mae_n = 0;
   if (n_surv) {
     build_ext_kernel<<<grid1(nq, 128), 128, 0, s>>>(
-        hits, begin, kept, surv_off, nq, e->q_offsets.as<uint32_t>(), qbits, dbits, n_surv,
-        e->eq.as<uint32_t>(), e->ed.as<uint32_t>(), e->edir.as<uint8_t>());
+        hits, begin, kept, surv_off, nq, e->q_offsets.as<uint32_t>(),
+        e->q_lengths.as<uint32_t>(), e->db_offsets.as<uint32_t>(), e->nseq, (uint32_t)e->db_len,
+        qbits, dbits, n_surv, e->eq.as<uint32_t>(), e->ed.as<uint32_t>(), e->edir.as<uint8_t>(),
+        e->elen0.as<uint32_t>(), e->elen1.as<uint32_t>(), e->eqid.as<uint32_t>());
     GZB_CUDA(cudaGetLastError());
     ++launches;
     GZB_CUDA(cudaMemsetAsync(e->gcells, 0, 8, s));
@@ -1496,17 +1738,88 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
     job.gap_open = e->params.gap_open;
     job.gap_ext = e->params.gap_extension;
     job.cutoff = e->params.gapped_cutoff;
+    const bool learned = schedule == GZB_SCHEDULE_BATCHED && e->have_model;
+    const bool oracle_order = schedule == GZB_SCHEDULE_ORACLE && e->prev_cells_n == next;
+    const bool scheduled = schedule != GZB_SCHEDULE_PLAIN || e->logging;
+    const bool want_feat = learned || e->logging;
+    if (want_feat) {
+      GZB_TRY(e->efeat.ensure(4 * kFeat * (next + 1)));
+      ext_features_kernel<<<grid1(next, 256), 256, 0, s>>>(
+          job.query, job.db, job.delim, e->matrix32.as<int32_t>(), e->q_cut.as<int32_t>(), next,
+          e->eq.as<uint32_t>(), e->ed.as<uint32_t>(), e->edir.as<uint8_t>(),
+          e->elen0.as<uint32_t>(), e->elen1.as<uint32_t>(), e->eqid.as<uint32_t>(),
+          e->efeat.as<float>());
+      GZB_CUDA(cudaGetLastError());
+      ++launches;
+    }
+    const uint32_t *order = nullptr;
+    if (learned || oracle_order) {
+      GZB_TRY(e->okeys.ensure(4 * (next + 1)));
+      GZB_TRY(e->okeys2.ensure(4 * (next + 1)));
+      GZB_TRY(e->oidx.ensure(4 * (next + 1)));
+      GZB_TRY(e->oidx2.ensure(4 * (next + 1)));
+      if (learned) {
+        GZB_TRY(e->epred.ensure(4 * (next + 1)));
+        GZB_TRY(cost_predict(e->model_d.as<float>(), e->efeat.as<float>(), (uint32_t)next,
+                             e->epred.as<float>(), s));
+        ++launches;
+      }
+      cost_keys_kernel<<<grid1(next, 256), 256, 0, s>>>(
+          learned ? e->epred.as<float>() : nullptr, e->prev_cells.as<uint32_t>(), next,
+          e->okeys.as<uint32_t>(), e->oidx.as<uint32_t>());
+      GZB_CUDA(cudaGetLastError());
+      ++launches;
+      cub::DoubleBuffer<uint32_t> kb(e->okeys.as<uint32_t>(), e->okeys2.as<uint32_t>());
+      cub::DoubleBuffer<uint32_t> vb(e->oidx.as<uint32_t>(), e->oidx2.as<uint32_t>());
+      size_t tb = 0;
+      GZB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb, (int64_t)next, 0, 32, s));
+      GZB_TRY(e->tmp.ensure(tb));
+      GZB_CUDA(cub::DeviceRadixSort::SortPairs(e->tmp.p, tb, kb, vb, (int64_t)next, 0, 32, s));
+      order = vb.Current();
+    }
     uint32_t fb = 0;
-    GZB_TRY(run_gapped(job, e->matrix32.as<int32_t>(), 32, 32, next, nullptr, 0,
-                       e->edir.as<uint8_t>(), e->eq.as<uint32_t>(), e->ed.as<uint32_t>(),
-                       e->escore.as<int32_t>(), &e->spill, &e->spill_cap, e->gcounters,
-                       e->gcells, &e->band_pool, &e->band_wmask, s, &fb));
+    if (scheduled) {
+      GZB_TRY(e->ecells.ensure(4 * (next + 1)));
+      GZB_TRY(run_gapped_queue(e, job, next, order, e->ecells.as<uint32_t>(), s, &fb));
+      launches += 3;
+      if (e->logging) {
+        log_pairs_kernel<<<grid1(next, 256), 256, 0, s>>>(
+            e->efeat.as<float>(), e->ecells.as<uint32_t>(), next, e->log_x.as<float>(),
+            e->log_y.as<float>(), e->log_ctr.as<unsigned long long>(), e->log_cap);
+        GZB_CUDA(cudaGetLastError());
+        ++launches;
+      }
+      if (learned) {
+        GZB_TRY(e->mae_acc.ensure(16));
+        GZB_CUDA(cudaMemsetAsync(e->mae_acc.p, 0, 16, s));
+        abs_error_kernel<<<grid1(next, 256), 256, 0, s>>>(e->epred.as<float>(),
+                                                          e->ecells.as<uint32_t>(), next,
+                                                          e->mae_acc.as<double>());
+        GZB_CUDA(cudaGetLastError());
+        ++launches;
+        double acc[2] = {0, 0};
+        GZB_CUDA(cudaMemcpyAsync(acc, e->mae_acc.p, 16, cudaMemcpyDeviceToHost, s));
+        GZB_CUDA(cudaStreamSynchronize(s));
+        e->last_mae = acc[1] > 0 ? (float)(acc[0] / acc[1]) : -1.0f;
+        e->last_mae_n = (uint64_t)acc[1];
+      }
+      // true costs of this extension list, for a later oracle-ordered run
+      GZB_TRY(e->prev_cells.ensure(4 * (next + 1)));
+      GZB_CUDA(cudaMemcpyAsync(e->prev_cells.p, e->ecells.p, 4 * next, cudaMemcpyDeviceToDevice,
+                               s));
+      e->prev_cells_n = next;
+    } else {
+      GZB_TRY(run_gapped(job, e->matrix32.as<int32_t>(), 32, 32, next, nullptr, 0,
+                         e->edir.as<uint8_t>(), e->eq.as<uint32_t>(), e->ed.as<uint32_t>(),
+                         e->escore.as<int32_t>(), &e->spill, &e->spill_cap, e->gcounters,
+                         e->gcells, &e->band_pool, &e->band_wmask, s, &fb));
+      launches += 3;
+    }
     unsigned long long cells = 0;
     GZB_CUDA(cudaMemcpyAsync(&cells, e->gcells, 8, cudaMemcpyDeviceToHost, s));
     GZB_CUDA(cudaStreamSynchronize(s));
     e->counters.gapped_cells = cells;
     e->counters.gapped_fallbacks = fb;
-    launches += 3;
   } else {
     e->counters.gapped_cells = 0;
     e->counters.gapped_fallbacks = 0;
@@ -1543,7 +1856,8 @@ extern "C" int gzb_engine_presearch(gzb_engine *e, int schedule, void *stream) {
   GZB_TRY(check_engine(e));
   GZB_CHECK(e->have_db && e->have_queries, GZB_ERR_INVALID,
             "set_database and set_queries first");
-  GZB_CHECK(schedule == GZB_SCHEDULE_PLAIN || schedule == GZB_SCHEDULE_BATCHED,
+  GZB_CHECK(schedule == GZB_SCHEDULE_PLAIN || schedule == GZB_SCHEDULE_BATCHED ||
+                schedule == GZB_SCHEDULE_ORACLE,
             GZB_ERR_INVALID, "unknown schedule %d", schedule);
   GZB_CHECK(e->params.max_number_one_subject_results <= 4, GZB_ERR_INVALID,
             "max_number_one_subject_results above 4 is not supported");
@@ -1665,5 +1979,69 @@ extern "C" int gzb_engine_get_index_array(gzb_engine *e, int which, uint32_t *ou
     GZB_CUDA(cudaMemcpyAsync(out, src, 4 * c, cudaMemcpyDeviceToHost, s));
     GZB_CUDA(cudaStreamSynchronize(s));
   }
+  return GZB_OK;
+}
+
+// ---- cost model and logging ----------------------------------------------
+
+extern "C" int gzb_engine_set_logging(gzb_engine *e, int enable, uint64_t capacity) {
+  GZB_TRY(check_engine(e));
+  e->logging = enable != 0;
+  if (e->logging) {
+    GZB_CHECK(capacity > 0, GZB_ERR_INVALID, "zero log capacity");
+    GZB_TRY(e->log_x.ensure(4 * kFeat * capacity));
+    GZB_TRY(e->log_y.ensure(4 * capacity));
+    GZB_TRY(e->log_ctr.ensure(8));
+    GZB_CUDA(cudaMemset(e->log_ctr.p, 0, 8));
+    e->log_cap = capacity;
+  }
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_get_log(gzb_engine *e, float *features, float *log_cells,
+                                  uint64_t capacity, uint64_t *count) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(count, GZB_ERR_INVALID, "null count");
+  uint64_t n = 0;
+  if (e->log_ctr.p) GZB_CUDA(cudaMemcpy(&n, e->log_ctr.p, 8, cudaMemcpyDeviceToHost));
+  n = std::min(n, e->log_cap);
+  *count = n;
+  const uint64_t c = std::min(n, capacity);
+  if (c && features) GZB_CUDA(cudaMemcpy(features, e->log_x.p, 4 * kFeat * c, cudaMemcpyDeviceToHost));
+  if (c && log_cells) GZB_CUDA(cudaMemcpy(log_cells, e->log_y.p, 4 * c, cudaMemcpyDeviceToHost));
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_set_cost_model(gzb_engine *e, const float *params) {
+  GZB_TRY(check_engine(e));
+  if (!params) {
+    e->have_model = false;
+    return GZB_OK;
+  }
+  GZB_TRY(e->model_d.ensure(4 * kParams));
+  GZB_CUDA(cudaMemcpy(e->model_d.p, params, 4 * kParams, cudaMemcpyHostToDevice));
+  e->have_model = true;
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_train_cost_model(gzb_engine *e, int epochs, int batch, float lr,
+                                           uint64_t seed, float *params, float *final_loss) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(params, GZB_ERR_INVALID, "null params");
+  uint64_t n = 0;
+  if (e->log_ctr.p) GZB_CUDA(cudaMemcpy(&n, e->log_ctr.p, 8, cudaMemcpyDeviceToHost));
+  n = std::min(n, e->log_cap);
+  GZB_CHECK(n > 0, GZB_ERR_INVALID, "no logged extensions to train on");
+  GZB_CHECK(n < (1ull << 32), GZB_ERR_OVERFLOW, "training set too large");
+  GZB_TRY(cost_train(e->log_x.as<float>(), e->log_y.as<float>(), (uint32_t)n, params, epochs,
+                     batch, lr, seed, final_loss, 0));
+  return gzb_engine_set_cost_model(e, params);
+}
+
+extern "C" int gzb_engine_get_schedule_stats(gzb_engine *e, float *mean_abs_log2_error,
+                                             uint64_t *count) {
+  GZB_CHECK(e && mean_abs_log2_error && count, GZB_ERR_INVALID, "null argument");
+  *mean_abs_log2_error = e->last_mae;
+  *count = e->last_mae_n;
   return GZB_OK;
 }

@@ -54,6 +54,7 @@ struct DevIndex {
   uint32_t *rep_keys = nullptr, *rep_offsets = nullptr;
   uint32_t *rep_cluster_ids = nullptr, *rep_positions = nullptr;
   uint32_t *member_offsets = nullptr, *member_positions = nullptr;
+  uint64_t *rep_windows = nullptr;  // packed similarity window per representative
   uint64_t n_nc_keys = 0, n_nc_values = 0, n_rep_keys = 0, n_reps = 0,
            n_members = 0;
 };
@@ -68,8 +69,29 @@ struct DevLists {
   uint64_t *unit_offsets = nullptr;                     // per list + 1
   uint32_t *entry_qid = nullptr;   // per entry: query id
   uint32_t *entry_cpos = nullptr;  // concatenated position
+  uint64_t *entry_window = nullptr;  // packed similarity window (check entries)
   uint64_t n_lists = 0, n_entries = 0, n_units = 0;
 };
+
+// Similarity codes of the L-window centred on `center`, 4 bits per code
+// (window[t] in bits 4t..4t+3); the distance of two windows is the number
+// of differing nibbles (DistanceCalculator::CalculateDistance,
+// src/distance_calculator.cpp:35-54).
+__device__ __forceinline__ uint64_t pack_window(const DevParams &p, const uint8_t *center) {
+  const int L = p.subsequence_length, half = L / 2;
+  uint64_t w = 0;
+  for (int t = 0; t < L; ++t) {
+    const int x = center[t - half];
+    w |= (uint64_t)((x < 32 ? p.sim_map[x] : 0) & 15) << (4 * t);
+  }
+  return w;
+}
+
+__device__ __forceinline__ int nibble_mismatches(uint64_t a, uint64_t b) {
+  uint64_t x = a ^ b;
+  x = (x | (x >> 1) | (x >> 2) | (x >> 3)) & 0x1111111111111111ull;
+  return __popcll(x);
+}
 
 // Binary search in a sorted key array; returns index or -1.
 __device__ __forceinline__ long long find_key(const uint32_t *keys, uint64_t n,

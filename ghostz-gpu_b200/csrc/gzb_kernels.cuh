@@ -55,21 +55,44 @@ __device__ __forceinline__ void load_matrix(int *sm, const int32_t *m,
 
 // ---------------------------------------------------------------------------
 // Ungapped one-side X-drop from s0[0]/s1[0] (query/database), stepping by
-// inc.  Returns the best prefix sum; stops early once it exceeds
-// stop_above (the caller only needs "> trigger").  *steps counts residue
-// pairs examined.
+// INC.  Returns the best prefix sum; stops early once it exceeds stop_above
+// (the caller only needs "> trigger").  *steps counts residue pairs
+// examined.  Residues are read a 32-bit word at a time (the sequences carry
+// readable padding around them), four residue pairs per pair of loads.
+template <int INC>
 __device__ __forceinline__ int ungapped_side(const uint8_t *__restrict__ s0,
-                                             const uint8_t *__restrict__ s1,
-                                             int inc, int delim, const int *sm,
-                                             int cutoff, int stop_above,
+                                             const uint8_t *__restrict__ s1, int delim,
+                                             const int *sm, int cutoff, int stop_above,
                                              int *steps) {
-  int best = 0, run = 0, pos = 0, n = 0;
+  const uint32_t *p0 = (const uint32_t *)((uintptr_t)s0 & ~(uintptr_t)3);
+  const uint32_t *p1 = (const uint32_t *)((uintptr_t)s1 & ~(uintptr_t)3);
+  int k0 = (int)((uintptr_t)s0 & 3), k1 = (int)((uintptr_t)s1 & 3);
+  uint32_t w0 = __ldg(p0), w1 = __ldg(p1);
+  int best = 0, run = 0, n = 0;
   for (;;) {
-    const int a = s0[pos], b = s1[pos];
+    const int a = (w0 >> (8 * k0)) & 0xff, b = (w1 >> (8 * k1)) & 0xff;
     if (a == delim || b == delim) break;
     run += sm[b * kMatrixStride + a];
-    pos += inc;
     ++n;
+    if (INC > 0) {
+      if (++k0 == 4) {
+        k0 = 0;
+        w0 = __ldg(++p0);
+      }
+      if (++k1 == 4) {
+        k1 = 0;
+        w1 = __ldg(++p1);
+      }
+    } else {
+      if (--k0 < 0) {
+        k0 = 3;
+        w0 = __ldg(--p0);
+      }
+      if (--k1 < 0) {
+        k1 = 3;
+        w1 = __ldg(--p1);
+      }
+    }
     if (run > 0) {
       best += run;
       run = 0;
@@ -88,9 +111,9 @@ __device__ __forceinline__ bool ungapped_hit(const uint8_t *q, const uint8_t *d,
                                              int delim, const int *sm,
                                              int cutoff, int trigger,
                                              int *steps) {
-  int sum = ungapped_side(q - 1, d - 1, -1, delim, sm, cutoff, trigger, steps);
+  int sum = ungapped_side<-1>(q - 1, d - 1, delim, sm, cutoff, trigger, steps);
   if (sum > trigger) return true;
-  sum += ungapped_side(q, d, 1, delim, sm, cutoff, trigger - sum, steps);
+  sum += ungapped_side<1>(q, d, delim, sm, cutoff, trigger - sum, steps);
   return sum > trigger;
 }
 

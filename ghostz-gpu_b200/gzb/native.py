@@ -52,6 +52,8 @@ def _declare(L):
     L.gzb_error_string.restype = C.c_char_p
     L.gzb_ungapped_extender_query_seeds_temp_bytes.restype = SZ
     L.gzb_ungapped_extender_query_seeds_temp_bytes.argtypes = [SZ]
+    L.gzb_cost_model_param_count.restype = C.c_int
+    L.gzb_cost_model_param_count.argtypes = []
     sigs = {
         "gzb_distance_calculator_create": [V],
         "gzb_distance_calculator_destroy": [V],
@@ -92,6 +94,15 @@ def _declare(L):
         "gzb_engine_get_index_array": [V, C.c_int, V, C.c_uint64, V, V],
         "gzb_engine_get_list_array": [V, C.c_int, V, C.c_uint64, V, V],
         "gzb_engine_get_stage_ms": [V, V],
+        "gzb_cost_model_init": [V, C.c_uint64],
+        "gzb_cost_model_gradients": [V, V, V, U32, V, V, V],
+        "gzb_cost_model_predict": [V, V, U32, V, V],
+        "gzb_cost_model_train": [V, V, U32, V, C.c_int, C.c_int, C.c_float, C.c_uint64, V, V],
+        "gzb_engine_set_logging": [V, C.c_int, C.c_uint64],
+        "gzb_engine_get_log": [V, V, V, C.c_uint64, V],
+        "gzb_engine_train_cost_model": [V, C.c_int, C.c_int, C.c_float, C.c_uint64, V, V],
+        "gzb_engine_set_cost_model": [V, V],
+        "gzb_engine_get_schedule_stats": [V, V, V],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -275,6 +286,18 @@ INDEX_NAMES = ("nc_keys", "nc_offsets", "nc_values", "rep_keys", "rep_offsets",
                "rep_cluster_ids", "rep_positions", "member_offsets", "member_positions")
 SCHEDULE_PLAIN = 0
 SCHEDULE_BATCHED = 1
+SCHEDULE_ORACLE = 2
+COST_FEATURES = 8
+
+
+def cost_param_count():
+    return int(lib().gzb_cost_model_param_count())
+
+
+def cost_model_init(seed=0):
+    p = np.zeros(cost_param_count(), np.float32)
+    check(lib().gzb_cost_model_init(hptr(p), int(seed)))
+    return p
 
 
 class PresearchEngine:
@@ -369,6 +392,39 @@ class PresearchEngine:
                                                   _stream_or_null(stream)))
             out[name] = a
         return out
+
+    # ---- cost model of the gapped stage
+    def set_logging(self, enable=True, capacity=1 << 24):
+        check(lib().gzb_engine_set_logging(self.h, int(bool(enable)), int(capacity)))
+
+    def get_log(self):
+        n = C.c_uint64()
+        check(lib().gzb_engine_get_log(self.h, None, None, 0, C.byref(n)))
+        k = n.value
+        x = np.zeros((k, COST_FEATURES), np.float32)
+        y = np.zeros(k, np.float32)
+        check(lib().gzb_engine_get_log(self.h, hptr(x), hptr(y), k, C.byref(n)))
+        return x, y
+
+    def train_cost_model(self, epochs=4, batch=4096, lr=3e-3, seed=0, init=None):
+        p = cost_model_init(seed) if init is None else np.array(init, np.float32)
+        loss = C.c_float()
+        check(lib().gzb_engine_train_cost_model(self.h, int(epochs), int(batch), float(lr),
+                                                int(seed), hptr(p), C.byref(loss)))
+        return p, float(loss.value)
+
+    def set_cost_model(self, params):
+        if params is None:
+            check(lib().gzb_engine_set_cost_model(self.h, None))
+        else:
+            p = np.ascontiguousarray(params, np.float32)
+            check(lib().gzb_engine_set_cost_model(self.h, hptr(p)))
+
+    def schedule_stats(self):
+        err = C.c_float()
+        n = C.c_uint64()
+        check(lib().gzb_engine_get_schedule_stats(self.h, C.byref(err), C.byref(n)))
+        return float(err.value), int(n.value)
 
     def index_arrays(self, stream=None):
         out = {}

@@ -233,11 +233,15 @@ typedef struct {
   uint64_t kernel_launches;    /* engine kernels launched by the presearch */
 } gzb_counters;
 
-/* schedule of the gapped stage */
-#define GZB_SCHEDULE_PLAIN 0    /* one launch, one warp per extension */
-#define GZB_SCHEDULE_BATCHED 1  /* persistent warps on a device work queue,
-                                   seeds ordered longest first by the cost
-                                   model */
+/* schedule of the gapped stage (results are identical under every one) */
+#define GZB_SCHEDULE_PLAIN 0    /* one launch over the extensions in hit order */
+#define GZB_SCHEDULE_BATCHED 1  /* persistent blocks on a device work queue,
+                                   extensions ordered longest-predicted first
+                                   by the cost model (plain order when no
+                                   model is set) */
+#define GZB_SCHEDULE_ORACLE 2   /* as BATCHED, ordered by the true costs of
+                                   the previous scheduled run of the same
+                                   extensions (a measuring stick) */
 
 int gzb_engine_create(int device, gzb_engine **out);
 int gzb_engine_destroy(gzb_engine *e);
@@ -289,6 +293,44 @@ int gzb_engine_get_index_array(gzb_engine *e, int which, uint32_t *out,
  * query.  Same copy semantics as gzb_engine_get_index_array. */
 int gzb_engine_get_list_array(gzb_engine *e, int which, uint32_t *out,
                               uint64_t capacity, uint64_t *count, void *stream);
+/* ---- cost model of the gapped stage -------------------------------------
+ * An 8 -> 32 -> 32 -> 1 ReLU MLP predicts log2(1 + DP cells) of every gapped
+ * extension from its ungapped score, ungapped length, positives and
+ * identities near the seed, remaining query and subject lengths and
+ * direction.  FP32 training with hand-written forward/backward kernels, BF16
+ * inference.  Parameters: gzb_cost_model_param_count() floats, layout
+ * W1[32][8] b1[32] W2[32][32] b2[32] W3[32] b3. */
+int gzb_cost_model_param_count(void);
+/* He-normal initial parameters from a seeded generator (host). */
+int gzb_cost_model_init(float *params, uint64_t seed);
+/* Gradient of the mean squared error over n samples (device buffers:
+ * d_x[n][8], d_y[n], d_grad[params]; d_loss receives the mean loss). */
+int gzb_cost_model_gradients(const float *d_params, const float *d_x,
+                             const float *d_y, uint32_t n, float *d_grad,
+                             float *d_loss, void *stream);
+/* BF16 inference: d_out[n] predicted log2(1 + cells). */
+int gzb_cost_model_predict(const float *d_params, const float *d_x, uint32_t n,
+                           float *d_out, void *stream);
+/* Minibatch Adam on device-resident samples; params in/out on the host. */
+int gzb_cost_model_train(const float *d_x, const float *d_y, uint32_t n,
+                         float *params, int epochs, int batch, float lr,
+                         uint64_t seed, float *final_loss, void *stream);
+/* Logging of (features, log2(1 + cells)) pairs for every gapped extension of
+ * the following presearch calls, up to `capacity` pairs (enabling resets
+ * the log). */
+int gzb_engine_set_logging(gzb_engine *e, int enable, uint64_t capacity);
+int gzb_engine_get_log(gzb_engine *e, float *features, float *log_cells,
+                       uint64_t capacity, uint64_t *count);
+/* Trains a model on the logged pairs (params: host in = initial values,
+ * out = trained) and installs it for GZB_SCHEDULE_BATCHED. */
+int gzb_engine_train_cost_model(gzb_engine *e, int epochs, int batch, float lr,
+                                uint64_t seed, float *params, float *final_loss);
+/* Installs host parameters (NULL removes the model). */
+int gzb_engine_set_cost_model(gzb_engine *e, const float *params);
+/* Mean |predicted - true| log2 cost of the last batched presearch and the
+ * number of extensions it covers (-1, 0 when none). */
+int gzb_engine_get_schedule_stats(gzb_engine *e, float *mean_abs_log2_error,
+                                  uint64_t *count);
 /* Time of the last presearch, per stage, in milliseconds (device events):
  * [0] list lookup, [1] seed search + ungapped + sort, [2] chain filter,
  * [3] gapped extension, [4] merge, [5] total. */
