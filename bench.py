@@ -194,6 +194,9 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+KERNEL_NAMES = {0: "flat", 1: "lane"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -206,6 +209,7 @@ def main():
     ap.add_argument("--cpu-queries", type=int, default=10000)
     ap.add_argument("--ref-queries", type=int, default=4000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -281,12 +285,32 @@ def main():
         barrier()
         return ev0.elapsed_time(ev1), {k: v / args.steps for k, v in stage.items()}
 
-    sampler = ClockSampler(local_rank)
-    sampler.start()
-    runs = {}
+    # autotuned tile of the gapped stage per schedule (untimed set-up; results
+    # do not depend on it): the flat kernel's bookkeeping threshold, then the
+    # thread kernel itself; the oracle order runs with the batched tile
     order = ["plain"] + (["batched", "oracle"] if args.schedule == "batched" else [])
     sched_id = {"plain": N.SCHEDULE_PLAIN, "batched": N.SCHEDULE_BATCHED,
                 "oracle": N.SCHEDULE_ORACLE}
+    tiles = {}
+    for name in order:
+        sid = sched_id[name]
+        if name == "oracle":
+            for w in (N.TILE_GAPPED_KERNEL, N.TILE_BOOK_THRESHOLD):
+                eng.set_tile(sid, w, eng.tile(N.SCHEDULE_BATCHED, w))
+        elif not args.no_autotune:
+            eng.set_tile(sid, N.TILE_GAPPED_KERNEL, N.GAPPED_KERNEL_FLAT)
+            thr, thr_ms = eng.autotune(sid, (4, 8, 12, 16, 24), N.TILE_BOOK_THRESHOLD)
+            ker, ker_ms = eng.autotune(sid, (N.GAPPED_KERNEL_FLAT, N.GAPPED_KERNEL_LANE),
+                                       N.TILE_GAPPED_KERNEL)
+            tiles[name] = {"gapped_ms_by_book_threshold": thr_ms,
+                           "gapped_ms_by_kernel": {KERNEL_NAMES[k]: v for k, v in ker_ms.items()}}
+        tiles.setdefault(name, {}).update(
+            kernel=KERNEL_NAMES[eng.tile(sid, N.TILE_GAPPED_KERNEL)],
+            book_threshold=eng.tile(sid, N.TILE_BOOK_THRESHOLD))
+
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    runs = {}
     results_by = {}
     for name in order:
         ms, st = timed(sched_id[name])
@@ -369,6 +393,7 @@ def main():
     sched_report["results_identical_across_schedules"] = bool(identical)
     sched_report["cost_model"] = {"train_pairs": train_pairs, "train_mse_log2": train_loss,
                                   "setup_s": train_s}
+    sched_report["tiles"] = tiles
     gcups_stage = counters["gapped_cells"] / (st["gapped"] / 1e3) / 1e9 if st["gapped"] else 0.0
     gcups_step = counters["gapped_cells"] / (t_dev / steps / 1e3) / 1e9
     # roofline of the dominant stage

@@ -25,25 +25,17 @@ constexpr int kOffW3 = kOffB2 + kHid;
 constexpr int kOffB3 = kOffW3 + kHid;
 constexpr int kParams = kOffB3 + 1;  // 1377
 
-// Features of one extension starting at q0/d0 (query/database), stepping
-// by inc: the ungapped X-drop score along the diagonal, the number of
-// residue pairs it examined, positives and identities among the first 16
-// pairs, remaining query / subject residues in the extension direction and
-// the direction itself.
-__device__ __forceinline__ void extension_features(const uint8_t *q0, const uint8_t *d0, int inc,
-                                                   int delim, const int *matrix32, int cutoff,
-                                                   uint32_t len0, uint32_t len1, bool reverse,
-                                                   float *f) {
-  int best = 0, run = 0, pos = 0, steps = 0, positives = 0, identities = 0;
+// Ungapped X-drop walk along the diagonal from q0/d0 (query/database),
+// stepping by inc, as the ungapped extension scores it: the best score and
+// the number of residue pairs examined before the drop (or a delimiter).
+__device__ __forceinline__ void diagonal_walk(const uint8_t *q0, const uint8_t *d0, int inc,
+                                              int delim, const int *matrix32, int cutoff,
+                                              int *best_out, int *steps_out) {
+  int best = 0, run = 0, pos = 0, steps = 0;
   for (int k = 0; k < 4096; ++k) {
     const int a = q0[pos], b = d0[pos];
     if (a == delim || b == delim) break;
-    const int sc = matrix32[b * 32 + a];
-    if (k < 16) {
-      positives += sc > 0;
-      identities += a == b;
-    }
-    run += sc;
+    run += matrix32[b * 32 + a];
     pos += inc;
     ++steps;
     if (run > 0) {
@@ -53,12 +45,27 @@ __device__ __forceinline__ void extension_features(const uint8_t *q0, const uint
       break;
     }
   }
-  f[0] = best * (1.0f / 32.0f);
+  *best_out = best;
+  *steps_out = steps;
+}
+
+// Features of one extension of a chained hit:
+//  f0 the hit's ungapped score (both directions' diagonal walks),
+//  f1/f2 remaining query / subject residues in the extension direction,
+//  f3 the direction, f4 this direction's walk score, f5 chained hits of the
+//  same query within 256 database residues (a homologous region yields
+//  many), f6 the walk length (local similarity of the residues along the
+//  diagonal), f7 the shorter remaining length.  Lengths and counts enter as
+//  log2(1 + x) / 8, scores as x / 32.
+__device__ __forceinline__ void extension_features(int best, int pair_best, int steps,
+                                                   uint32_t len0, uint32_t len1, bool reverse,
+                                                   uint32_t neighbours, float *f) {
+  f[0] = pair_best * (1.0f / 32.0f);
   f[1] = log2f(1.0f + (float)len0) * 0.125f;
   f[2] = log2f(1.0f + (float)len1) * 0.125f;
   f[3] = reverse ? 1.0f : 0.0f;
-  f[4] = positives * (1.0f / 16.0f);
-  f[5] = identities * (1.0f / 16.0f);
+  f[4] = best * (1.0f / 32.0f);
+  f[5] = log2f(1.0f + (float)neighbours) * 0.125f;
   f[6] = log2f(1.0f + (float)steps) * 0.125f;
   f[7] = log2f(1.0f + (float)(len0 < len1 ? len0 : len1)) * 0.125f;
 }

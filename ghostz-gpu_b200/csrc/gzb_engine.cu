@@ -53,11 +53,15 @@ __global__ void gapped_serial_kernel(GappedJob job, const int32_t *__restrict__ 
                                      int wmask, unsigned long long *cells_total,
                                      uint32_t *too_long_count);
 
-int run_gapped(const GappedJob &job, const int32_t *matrix, int number_letters,
-               int stride, size_t n, const uint32_t *order, int reverse, const uint8_t *dir,
-               uint32_t *d_qpos, uint32_t *d_dpos, int32_t *d_scores, uint32_t **spill,
-               size_t *spill_cap, uint32_t *counters, unsigned long long *cells,
-               int2 **band_pool, int *band_wmask, cudaStream_t s, uint32_t *n_fallback);
+extern GappedTile g_tile;
+int check_tile_value(int which, int value);
+int *tile_field(GappedTile &t, int which);
+int run_gapped(const GappedTile &tile, const GappedJob &job, const int32_t *matrix,
+               int number_letters, int stride, size_t n, const uint32_t *order, int reverse,
+               const uint8_t *dir, uint32_t *d_qpos, uint32_t *d_dpos, int32_t *d_scores,
+               uint32_t **spill, size_t *spill_cap, uint32_t *counters,
+               unsigned long long *cells, uint32_t *cells_out, int2 **band_pool,
+               int *band_wmask, cudaStream_t s, uint32_t *n_fallback);
 
 constexpr uint64_t kPad = 256;  // delimiter bytes kept around device sequences
 
@@ -645,16 +649,23 @@ __global__ void build_ext_kernel(const uint64_t *hits, const uint64_t *begin,
                                  const uint32_t *db_offsets, uint32_t nseq, uint32_t db_len,
                                  int qbits, int dbits, uint64_t n_surv, uint32_t *eq,
                                  uint32_t *ed, uint8_t *dir, uint32_t *elen0,
-                                 uint32_t *elen1, uint32_t *eqid) {
+                                 uint32_t *elen1, uint32_t *eqid, uint32_t *neighbours) {
   const uint64_t qmask = (1ull << qbits) - 1, dmask = (1ull << dbits) - 1;
+  constexpr uint32_t kReach = 256;  // database residues either side
   for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < nq;
        qi += gridDim.x * blockDim.x) {
     const uint64_t b = begin[qi], o = surv_off[qi];
     const uint32_t qlen = q_lengths[qi];
-    for (uint32_t k = 0; k < kept[qi]; ++k) {
+    const uint32_t nk = kept[qi];
+    uint32_t lo = 0, hi = 0;  // window of kept hits (database order) around k
+    for (uint32_t k = 0; k < nk; ++k) {
       const uint64_t key = hits[b + k];
       const uint32_t hq = (uint32_t)(key & qmask);
       const uint32_t hd = (uint32_t)((key >> qbits) & dmask);
+      while ((uint32_t)((hits[b + lo] >> qbits) & dmask) + kReach < hd) ++lo;
+      if (hi < k) hi = k;
+      while (hi + 1 < nk && (uint32_t)((hits[b + hi + 1] >> qbits) & dmask) <= hd + kReach) ++hi;
+      if (neighbours) neighbours[o + k] = hi - lo + 1;
       const uint32_t sj = subject_of(db_offsets, nseq, db_len, hd);
       const uint32_t s0 = db_offsets[sj], s1 = db_offsets[sj + 1] - 1;  // residues [s0, s1)
       eq[o + k] = q_offsets[qi] + hq - 1;
@@ -673,19 +684,29 @@ __global__ void build_ext_kernel(const uint64_t *hits, const uint64_t *begin,
   }
 }
 
+// Cost-model features of both extensions of every chained hit (one thread
+// per hit: reverse extension h, forward extension n_surv + h).
 __global__ void ext_features_kernel(const uint8_t *__restrict__ q, const uint8_t *__restrict__ db,
                                     int delim, const int32_t *__restrict__ matrix32,
-                                    const int32_t *__restrict__ cutoffs, uint64_t n,
-                                    const uint32_t *eq, const uint32_t *ed, const uint8_t *dir,
+                                    const int32_t *__restrict__ cutoffs, uint64_t n_surv,
+                                    const uint32_t *eq, const uint32_t *ed,
                                     const uint32_t *elen0, const uint32_t *elen1,
-                                    const uint32_t *eqid, float *feat) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    float f[kFeat];
-    const bool rev = dir[i] != 0;
-    extension_features(q + eq[i], db + ed[i], rev ? -1 : 1, delim, matrix32, cutoffs[eqid[i]],
-                       elen0[i], elen1[i], rev, f);
-    for (int k = 0; k < kFeat; ++k) feat[i * kFeat + k] = f[k];
+                                    const uint32_t *eqid, const uint32_t *neighbours,
+                                    float *feat) {
+  for (uint64_t h = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; h < n_surv;
+       h += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t r = h, f = n_surv + h;
+    const int cutoff = cutoffs[eqid[h]];
+    int best_r, steps_r, best_f, steps_f;
+    diagonal_walk(q + eq[r], db + ed[r], -1, delim, matrix32, cutoff, &best_r, &steps_r);
+    diagonal_walk(q + eq[f], db + ed[f], 1, delim, matrix32, cutoff, &best_f, &steps_f);
+    float x[kFeat];
+    extension_features(best_r, best_r + best_f, steps_r, elen0[r], elen1[r], true,
+                       neighbours[h], x);
+    for (int k = 0; k < kFeat; ++k) feat[r * kFeat + k] = x[k];
+    extension_features(best_f, best_r + best_f, steps_f, elen0[f], elen1[f], false,
+                       neighbours[h], x);
+    for (int k = 0; k < kFeat; ++k) feat[f * kFeat + k] = x[k];
   }
 }
 
@@ -701,59 +722,6 @@ __global__ void cost_keys_kernel(const float *pred, const uint32_t *true_cells, 
     keys[i] = 0xFFFFFFFFu - u;
     vals[i] = (uint32_t)i;
   }
-}
-
-constexpr int kQueueBlock = 128;
-
-// The batched schedule's gapped kernel: persistent blocks take 32
-// consecutive extensions of the cost-sorted order per warp from a device
-// work queue, so the extensions a warp runs together have similar predicted
-// cost and the longest go first.  cells_out records every extension's DP
-// cells (UINT32_MAX when it was handed to the fallback).
-__global__ void __launch_bounds__(kQueueBlock)
-gapped_lane_queue_kernel(GappedJob job, const int32_t *__restrict__ matrix, uint64_t n,
-                         const uint32_t *__restrict__ order, unsigned long long *queue,
-                         const uint8_t *__restrict__ dir, uint32_t *qpos, uint32_t *dpos,
-                         int32_t *scores, uint32_t *spill, uint32_t *spill_count,
-                         unsigned long long *cells_total, uint32_t *cells_out) {
-  __shared__ int sm[kMatrixStride * kMatrixStride];
-  __shared__ uint32_t cells_s[kLaneW * kQueueBlock];
-  __shared__ uint32_t res_s[(kLaneW / 4) * kQueueBlock];
-  load_matrix(sm, matrix, kMatrixStride, kMatrixStride);
-  __syncthreads();
-  LaneBand band{cells_s, res_s, kQueueBlock, (int)threadIdx.x};
-  const int lane = threadIdx.x & 31;
-  unsigned long long cells = 0;
-  for (;;) {
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(queue, 32ull);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base >= n) break;
-    const uint64_t i = base + lane;
-    if (i < n) {
-      const uint32_t e = order ? order[i] : (uint32_t)i;
-      const bool rev = dir[e] != 0;
-      const uint32_t q = qpos[e], d = dpos[e];
-      GappedOut o = gapped_extend_lane(job, sm, band, q, d, rev);
-      if (o.overflow) {
-        spill[atomicAdd(spill_count, 1u)] = e;
-        if (cells_out) cells_out[e] = 0xFFFFFFFFu;
-      } else {
-        cells += o.cells;
-        qpos[e] = q + (uint32_t)o.pos0;
-        dpos[e] = d + (uint32_t)o.pos1;
-        scores[e] = o.score;
-        if (cells_out) cells_out[e] = o.cells > 0xFFFFFFFEull ? 0xFFFFFFFEu : (uint32_t)o.cells;
-      }
-    }
-    __syncwarp();
-  }
-  cells += __shfl_down_sync(0xffffffffu, cells, 16);
-  cells += __shfl_down_sync(0xffffffffu, cells, 8);
-  cells += __shfl_down_sync(0xffffffffu, cells, 4);
-  cells += __shfl_down_sync(0xffffffffu, cells, 2);
-  cells += __shfl_down_sync(0xffffffffu, cells, 1);
-  if (lane == 0 && cells) atomicAdd(cells_total, cells);
 }
 
 // appends (features, log2(1+cells)) of completed extensions to the log
@@ -1014,6 +982,9 @@ struct gzb_engine {
   DBuf elen0, elen1, eqid, efeat, epred, ecells, okeys, okeys2, oidx, oidx2, queue, prev_cells,
       model_d, mae_acc, log_x, log_y, log_ctr;
   uint64_t prev_cells_n = 0;
+  uint64_t pred_n = 0;       // extensions with a prediction in epred (last run)
+  DBuf enb;                  // per surviving hit: chained neighbours (cost feature)
+  int tile[3][2] = {{-1, -1}, {-1, -1}, {-1, -1}};  // [schedule][which], -1 = default
   bool logging = false;
   uint64_t log_cap = 0;
   bool have_model = false;
@@ -1032,64 +1003,6 @@ struct gzb_engine {
 };
 
 namespace {
-
-// Gapped stage on the scheduled path: the work-queue lane kernel over
-// `order` (nullptr = extension order), then the warp and serial fallbacks
-// of the regular extender for the extensions it hands on.
-int run_gapped_queue(gzb_engine *e, const GappedJob &job, uint64_t n, const uint32_t *order,
-                     uint32_t *cells_out, cudaStream_t s, uint32_t *n_fallback) {
-  if (n == 0) return GZB_OK;
-  if (e->spill_cap < 2 * n) {
-    cudaFree(e->spill);
-    e->spill = nullptr;
-    e->spill_cap = 0;
-    GZB_CUDA(cudaMalloc(&e->spill, 4 * 2 * n));
-    e->spill_cap = 2 * n;
-  }
-  constexpr int kSerialThreads = 4 * 128, kSerialBand = 1 << 15;
-  if (!e->band_pool) {
-    GZB_CUDA(cudaMalloc(&e->band_pool, sizeof(int2) * (size_t)kSerialThreads * kSerialBand));
-    e->band_wmask = kSerialBand - 1;
-  }
-  GZB_TRY(e->queue.ensure(8));
-  GZB_CUDA(cudaMemsetAsync(e->queue.p, 0, 8, s));
-  GZB_CUDA(cudaMemsetAsync(e->gcounters, 0, 16, s));
-  uint32_t *spill1 = e->spill, *spill2 = e->spill + n;
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  int per_sm = 4;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gapped_lane_queue_kernel, kQueueBlock, 0);
-  if (per_sm < 1) per_sm = 1;
-  const int32_t *m = e->matrix32.as<int32_t>();
-  gapped_lane_queue_kernel<<<sms * per_sm, kQueueBlock, 0, s>>>(
-      job, m, n, order, e->queue.as<unsigned long long>(), e->edir.as<uint8_t>(),
-      e->eq.as<uint32_t>(), e->ed.as<uint32_t>(), e->escore.as<int32_t>(), spill1, e->gcounters,
-      e->gcells, cells_out);
-  GZB_CUDA(cudaGetLastError());
-  const uint32_t *serial_list = spill1, *serial_count = e->gcounters;
-  if (warp_path_exact(job.cutoff)) {
-    gapped_warp_kernel<<<148 * 4, 256, 0, s>>>(job, m, 32, 32, spill1, e->gcounters, 0,
-                                                e->edir.as<uint8_t>(), e->eq.as<uint32_t>(),
-                                                e->ed.as<uint32_t>(), e->escore.as<int32_t>(),
-                                                spill2, e->gcounters + 1, e->gcells);
-    GZB_CUDA(cudaGetLastError());
-    serial_list = spill2;
-    serial_count = e->gcounters + 1;
-  }
-  gapped_serial_kernel<<<kSerialThreads / 128, 128, 0, s>>>(
-      job, m, 32, 32, serial_list, serial_count, 0, e->edir.as<uint8_t>(), e->eq.as<uint32_t>(),
-      e->ed.as<uint32_t>(), e->escore.as<int32_t>(), e->band_pool, e->band_wmask, e->gcells,
-      e->gcounters + 2);
-  GZB_CUDA(cudaGetLastError());
-  uint32_t h[3] = {0, 0, 0};
-  GZB_CUDA(cudaMemcpyAsync(h, e->gcounters, 12, cudaMemcpyDeviceToHost, s));
-  GZB_CUDA(cudaStreamSynchronize(s));
-  GZB_CHECK(h[2] == 0, GZB_ERR_OVERFLOW, "%u gapped extensions need a band wider than %d columns",
-            h[2], kSerialBand);
-  *n_fallback = h[0];
-  return GZB_OK;
-}
 
 int bits_for(uint64_t v) {  // bits to hold values in [0, v]
   int b = 1;
@@ -1243,7 +1156,7 @@ extern "C" int gzb_engine_destroy(gzb_engine *e) {
                  &e->hits_copy, &e->elen0, &e->elen1, &e->eqid, &e->efeat, &e->epred,
                  &e->ecells, &e->okeys, &e->okeys2, &e->oidx, &e->oidx2, &e->queue,
                  &e->prev_cells, &e->model_d, &e->mae_acc, &e->log_x, &e->log_y,
-                 &e->log_ctr};
+                 &e->log_ctr, &e->enb};
   for (DBuf *b : all) b->release();
   cudaFree(e->spill);
   cudaFree(e->gcounters);
@@ -1720,14 +1633,17 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
   GZB_TRY(e->elen0.ensure(4 * (next + 1)));
   GZB_TRY(e->elen1.ensure(4 * (next + 1)));
   GZB_TRY(e->eqid.ensure(4 * (next + 1)));
+  GZB_TRY(e->enb.ensure(4 * (n_surv + 1)));
   e->last_mae = -1.0f;
   e->last_mae_n = 0;
+  e->pred_n = 0;
   if (n_surv) {
     build_ext_kernel<<<grid1(nq, 128), 128, 0, s>>>(
         hits, begin, kept, surv_off, nq, e->q_offsets.as<uint32_t>(),
         e->q_lengths.as<uint32_t>(), e->db_offsets.as<uint32_t>(), e->nseq, (uint32_t)e->db_len,
         qbits, dbits, n_surv, e->eq.as<uint32_t>(), e->ed.as<uint32_t>(), e->edir.as<uint8_t>(),
-        e->elen0.as<uint32_t>(), e->elen1.as<uint32_t>(), e->eqid.as<uint32_t>());
+        e->elen0.as<uint32_t>(), e->elen1.as<uint32_t>(), e->eqid.as<uint32_t>(),
+        e->enb.as<uint32_t>());
     GZB_CUDA(cudaGetLastError());
     ++launches;
     GZB_CUDA(cudaMemsetAsync(e->gcells, 0, 8, s));
@@ -1744,10 +1660,10 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
     const bool want_feat = learned || e->logging;
     if (want_feat) {
       GZB_TRY(e->efeat.ensure(4 * kFeat * (next + 1)));
-      ext_features_kernel<<<grid1(next, 256), 256, 0, s>>>(
-          job.query, job.db, job.delim, e->matrix32.as<int32_t>(), e->q_cut.as<int32_t>(), next,
-          e->eq.as<uint32_t>(), e->ed.as<uint32_t>(), e->edir.as<uint8_t>(),
-          e->elen0.as<uint32_t>(), e->elen1.as<uint32_t>(), e->eqid.as<uint32_t>(),
+      ext_features_kernel<<<grid1(n_surv, 256), 256, 0, s>>>(
+          job.query, job.db, job.delim, e->matrix32.as<int32_t>(), e->q_cut.as<int32_t>(),
+          n_surv, e->eq.as<uint32_t>(), e->ed.as<uint32_t>(), e->elen0.as<uint32_t>(),
+          e->elen1.as<uint32_t>(), e->eqid.as<uint32_t>(), e->enb.as<uint32_t>(),
           e->efeat.as<float>());
       GZB_CUDA(cudaGetLastError());
       ++launches;
@@ -1762,6 +1678,7 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
         GZB_TRY(e->epred.ensure(4 * (next + 1)));
         GZB_TRY(cost_predict(e->model_d.as<float>(), e->efeat.as<float>(), (uint32_t)next,
                              e->epred.as<float>(), s));
+        e->pred_n = next;
         ++launches;
       }
       cost_keys_kernel<<<grid1(next, 256), 256, 0, s>>>(
@@ -1778,10 +1695,17 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
       order = vb.Current();
     }
     uint32_t fb = 0;
+    GappedTile tile = g_tile;
+    for (int w = 0; w < 2; ++w)
+      if (e->tile[schedule][w] >= 0) *tile_field(tile, w) = e->tile[schedule][w];
+    if (scheduled) GZB_TRY(e->ecells.ensure(4 * (next + 1)));
+    GZB_TRY(run_gapped(tile, job, e->matrix32.as<int32_t>(), 32, 32, next, order, 0,
+                       e->edir.as<uint8_t>(), e->eq.as<uint32_t>(), e->ed.as<uint32_t>(),
+                       e->escore.as<int32_t>(), &e->spill, &e->spill_cap, e->gcounters,
+                       e->gcells, scheduled ? e->ecells.as<uint32_t>() : nullptr,
+                       &e->band_pool, &e->band_wmask, s, &fb));
+    launches += 3;
     if (scheduled) {
-      GZB_TRY(e->ecells.ensure(4 * (next + 1)));
-      GZB_TRY(run_gapped_queue(e, job, next, order, e->ecells.as<uint32_t>(), s, &fb));
-      launches += 3;
       if (e->logging) {
         log_pairs_kernel<<<grid1(next, 256), 256, 0, s>>>(
             e->efeat.as<float>(), e->ecells.as<uint32_t>(), next, e->log_x.as<float>(),
@@ -1808,12 +1732,6 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
       GZB_CUDA(cudaMemcpyAsync(e->prev_cells.p, e->ecells.p, 4 * next, cudaMemcpyDeviceToDevice,
                                s));
       e->prev_cells_n = next;
-    } else {
-      GZB_TRY(run_gapped(job, e->matrix32.as<int32_t>(), 32, 32, next, nullptr, 0,
-                         e->edir.as<uint8_t>(), e->eq.as<uint32_t>(), e->ed.as<uint32_t>(),
-                         e->escore.as<int32_t>(), &e->spill, &e->spill_cap, e->gcounters,
-                         e->gcells, &e->band_pool, &e->band_wmask, s, &fb));
-      launches += 3;
     }
     unsigned long long cells = 0;
     GZB_CUDA(cudaMemcpyAsync(&cells, e->gcells, 8, cudaMemcpyDeviceToHost, s));
@@ -2043,5 +1961,79 @@ extern "C" int gzb_engine_get_schedule_stats(gzb_engine *e, float *mean_abs_log2
   GZB_CHECK(e && mean_abs_log2_error && count, GZB_ERR_INVALID, "null argument");
   *mean_abs_log2_error = e->last_mae;
   *count = e->last_mae_n;
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_get_extension_costs(gzb_engine *e, float *predicted,
+                                              uint32_t *cells, uint64_t capacity,
+                                              uint64_t *count, void *stream) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(count, GZB_ERR_INVALID, "null count");
+  const uint64_t n = e->prev_cells_n;
+  *count = n;
+  if (!predicted && !cells) return GZB_OK;
+  GZB_CHECK(capacity >= n, GZB_ERR_INVALID, "capacity %llu below %llu extensions",
+            (unsigned long long)capacity, (unsigned long long)n);
+  GZB_CHECK(!predicted || e->pred_n == n, GZB_ERR_INVALID,
+            "the last run made no cost predictions (batched schedule with a model)");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (n && cells)
+    GZB_CUDA(cudaMemcpyAsync(cells, e->prev_cells.p, 4 * n, cudaMemcpyDefault, s));
+  if (n && predicted)
+    GZB_CUDA(cudaMemcpyAsync(predicted, e->epred.p, 4 * n, cudaMemcpyDefault, s));
+  GZB_CUDA(cudaStreamSynchronize(s));
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_set_tile(gzb_engine *e, int schedule, int which, int value) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(schedule >= 0 && schedule < 3, GZB_ERR_INVALID, "unknown schedule %d", schedule);
+  if (value != -1) GZB_TRY(check_tile_value(which, value));
+  else GZB_TRY(check_tile_value(which, which == GZB_TILE_GAPPED_KERNEL ? 0 : 1));
+  e->tile[schedule][which] = value;
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_get_tile(gzb_engine *e, int schedule, int which, int *value) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(value, GZB_ERR_INVALID, "null value");
+  GZB_CHECK(schedule >= 0 && schedule < 3, GZB_ERR_INVALID, "unknown schedule %d", schedule);
+  GZB_TRY(check_tile_value(which, which == GZB_TILE_GAPPED_KERNEL ? 0 : 1));
+  const int v = e->tile[schedule][which];
+  if (v >= 0) *value = v;
+  else GZB_TRY(gzb_get_tile_parameter(which, value));
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_autotune(gzb_engine *e, int schedule, int which, const int *candidates,
+                                   int n, int *best, float *ms, void *stream) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(candidates && n > 0 && best, GZB_ERR_INVALID, "no candidates");
+  GZB_CHECK(schedule >= 0 && schedule < 3, GZB_ERR_INVALID, "unknown schedule %d", schedule);
+  for (int i = 0; i < n; ++i) GZB_TRY(check_tile_value(which, candidates[i]));
+  const int keep = e->tile[schedule][which];
+  float best_ms = 1e30f;
+  int best_v = candidates[0];
+  for (int i = 0; i < n; ++i) {
+    e->tile[schedule][which] = candidates[i];
+    float t = 0.0f;
+    for (int rep = 0; rep < 2; ++rep) {  // the first run warms caches and buffers
+      int rc = gzb_engine_reset_results(e, stream);
+      if (rc == GZB_OK) rc = gzb_engine_presearch(e, schedule, stream);
+      if (rc != GZB_OK) {
+        e->tile[schedule][which] = keep;
+        return rc;
+      }
+      t = e->stage_ms[3];
+    }
+    if (ms) ms[i] = t;
+    if (t < best_ms) {
+      best_ms = t;
+      best_v = candidates[i];
+    }
+  }
+  e->tile[schedule][which] = best_v;
+  GZB_TRY(gzb_engine_reset_results(e, stream));
+  *best = best_v;
   return GZB_OK;
 }

@@ -32,10 +32,13 @@
 // fallback kernel, which keeps the band in a global circular buffer.
 #pragma once
 
+#include <cooperative_groups.h>
 #include <cstdint>
 #include <cuda_runtime.h>
 
 namespace gzb {
+
+namespace cg = cooperative_groups;
 
 constexpr int kInitScore = -(1 << 10);  // src/gapped_extender.h:40
 constexpr int kNegBig = -(1 << 29);
@@ -132,6 +135,14 @@ struct GappedJob {
   const uint8_t *query;     // concatenated queries
   const uint8_t *db;        // database chunk
   int delim, gap_open, gap_ext, cutoff;
+};
+
+// Launch shape of the one-thread-per-extension gapped level: which kernel
+// (GZB_GAPPED_KERNEL_FLAT / _LANE) and the flat kernel's bookkeeping
+// threshold.
+struct GappedTile {
+  int kernel;
+  int book_threshold;
 };
 
 struct GappedOut {
@@ -642,6 +653,262 @@ __device__ inline GappedOut gapped_extend_lane(const GappedJob &job, const int *
   out.pos1 = mp1;
   out.cells = cells;
   return out;
+}
+
+}  // namespace gzb
+
+namespace gzb {
+
+// ---------------------------------------------------------------------------
+// Gapped extension, one thread per extension, flattened.  Same recurrence as
+// gapped_extend_lane, but the row loop, the cell loop and the loop over
+// extensions are one loop that advances every lane by one DP cell per
+// iteration: a lane that reaches the end of its row, or of its extension,
+// does that bookkeeping and carries on with its next cell, so the lanes of a
+// warp never wait for the slowest one.  Band cells are int2 {best,
+// best_gap << 5 | query residue} in a kFlatW-column circular buffer per
+// thread ([column][thread] layout).  Extensions whose band outgrows it, or
+// that run past 2^24 rows (the packed gap field's bound), are handed on.
+constexpr int kFlatW = 48;
+constexpr int kFlatBlock = 128;
+
+struct FlatOut {
+  uint32_t *qpos, *dpos;
+  int32_t *scores;
+  uint32_t *spill, *spill_count;
+  uint32_t *cells_out;  // optional, per extension (UINT32_MAX when handed on)
+};
+
+__device__ __forceinline__ int flat_next(int s) { return s + 1 == kFlatW ? 0 : s + 1; }
+__device__ __forceinline__ int pack_gap(int gap, int res) {
+  return (int)(((uint32_t)gap << 5) | (uint32_t)res);
+}
+
+// Work source: queue (device counter over `n` items, optionally through
+// `order`).  Returns false when exhausted.
+__device__ __forceinline__ bool flat_fetch(unsigned long long *queue, uint64_t n,
+                                           const uint32_t *order, uint32_t *e) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  unsigned long long base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(queue, (unsigned long long)g.size());
+  base = g.shfl(base, 0);
+  const unsigned long long i = base + g.thread_rank();
+  if (i >= n) return false;
+  *e = order ? order[i] : (uint32_t)i;
+  return true;
+}
+
+__device__ __forceinline__ unsigned long long gapped_flat(const GappedJob &job, const int *sm,
+                                                          int2 *band, int S, uint64_t n,
+                                                          const uint32_t *order,
+                                                          unsigned long long *queue,
+                                                          int reverse_default,
+                                                          const uint8_t *dir, FlatOut out,
+                                                          int book_threshold) {
+  const int delim = job.delim;
+  const int ge = job.gap_ext;
+  const int gi = job.gap_open + job.gap_ext;
+  const int cutoff = job.cutoff;
+  unsigned long long cells_total = 0;
+  // per-lane state
+  uint32_t e = 0;
+  int inc = 1;
+  const uint8_t *q0 = nullptr, *d0 = nullptr;
+  int bs = 0, be = 0, bss = 0, bes = 0;   // band [bs, be) and the slots of bs / be
+  int c = 0, cs = 0, pos0 = 0;            // current column, its slot, its query offset
+  int last = 0, ls = 0;                   // last kept column and its slot
+  int diag = 0, row_gap = 0;
+  int maxs = 0, mp0 = 0, mp1 = 0;
+  int r = 0, p1 = 0, next_x = 0;
+  const int *mrow = sm;
+  uint32_t cells = 0;
+  bool have = false, done = false;
+  for (;;) {
+    // Every iteration starts with the whole warp converged.  Lanes that
+    // reached a row or extension boundary wait until at least
+    // `book_threshold` of them do (or no lane can take a cell step) and then
+    // do their bookkeeping together, so the long bookkeeping path runs with
+    // many lanes at once instead of with one lane per iteration.
+    __syncwarp();
+    const bool cell_ready = have && !done && c < be;
+    const bool book_ready = !done && !cell_ready;
+    const unsigned cm = __ballot_sync(0xffffffffu, cell_ready);
+    const unsigned bm = __ballot_sync(0xffffffffu, book_ready);
+    if ((cm | bm) == 0) break;
+    const bool book_turn = cm == 0 || __popc(bm) >= book_threshold;
+    if (!book_turn) {
+      if (!cell_ready) continue;
+      // ---- one DP cell (src/gapped_extender.cpp:410-443)
+      int2 &cell = band[cs * S];
+      const int2 w = cell;
+      const int res = w.y & 31;
+      const int vgap = w.y >> 5;
+      int s = diag + mrow[res];
+      diag = w.x;
+      s = imax(s, imax(vgap, row_gap));
+      ++cells;
+      if (maxs - s > cutoff) {
+        if (bs + 1 == c) {
+          bs = c;
+          bss = cs;
+        }
+        cell = make_int2(kInitScore, pack_gap(kInitScore, res));
+        row_gap = kInitScore;
+      } else {
+        last = c;
+        ls = cs;
+        if (s > maxs) {
+          maxs = s;
+          mp0 = pos0;
+          mp1 = p1;
+        }
+        const int ng = imax(s - gi, vgap - ge);
+        row_gap = imax(s - gi, row_gap - ge);
+        cell = make_int2(s, pack_gap(ng, res));
+      }
+      ++c;
+      pos0 += inc;
+      cs = flat_next(cs);
+      continue;
+    }
+    if (!book_ready) continue;
+    // ---- bookkeeping: row end, next row, next extension
+    bool finish = false, overflow = false;
+    if (have) {
+      // row end (src/gapped_extender.cpp:445-465)
+      if (bs + 1 == be) {
+        finish = true;
+      } else {
+        int edge;
+        const bool shrunk = last < be - 1;
+        if (shrunk) {
+          edge = q0[(be - 1) * inc];  // the old right edge is tested
+          be = last + 1;
+          bes = flat_next(ls);
+        } else {
+          edge = q0[(be - 1) * inc];
+          while (row_gap >= maxs - cutoff && edge != delim) {
+            if (be - bs >= kFlatW) {
+              overflow = true;
+              break;
+            }
+            band[bes * S] = make_int2(row_gap, pack_gap(row_gap - gi, edge));
+            row_gap -= ge;
+            ++be;
+            bes = flat_next(bes);
+            ++cells;
+            edge = q0[(be - 1) * inc];
+          }
+        }
+        if (!overflow && edge != delim) {
+          if (be - bs >= kFlatW) {
+            overflow = true;
+          } else {
+            // the sentinel column keeps its own residue
+            const int res = shrunk ? (band[bes * S].y & 31) : edge;
+            band[bes * S] = make_int2(kInitScore, pack_gap(kInitScore, res));
+            ++be;
+            bes = flat_next(bes);
+          }
+        }
+        ++r;
+        p1 += inc;
+      }
+    }
+    for (;;) {
+      if (have && !finish && !overflow) {
+        // row start (src/gapped_extender.cpp:382-408)
+        const int x = next_x;
+        if (x == delim) {
+          finish = true;
+        } else if (r >= (1 << 24)) {
+          overflow = true;
+        } else {
+          next_x = d0[p1 + inc];
+          mrow = sm + x * kMatrixStride;
+          int2 &c0 = band[bss * S];
+          const int2 w0 = c0;
+          const int g0 = w0.y >> 5;
+          diag = w0.x;
+          const int nb0 = (maxs - g0 > cutoff) ? kInitScore : g0;
+          row_gap = nb0 - gi;
+          c0 = make_int2(nb0, pack_gap(g0 - ge, w0.y & 31));
+          last = bs;
+          ls = bss;
+          c = bs + 1;
+          cs = flat_next(bss);
+          pos0 = bs * inc;
+          break;  // back to cell steps
+        }
+      }
+      if (have) {
+        if (overflow) {
+          out.spill[atomicAdd(out.spill_count, 1u)] = e;
+          if (out.cells_out) out.cells_out[e] = 0xFFFFFFFFu;
+        } else {
+          const uint32_t q = out.qpos[e], d = out.dpos[e];
+          out.qpos[e] = q + (uint32_t)mp0;
+          out.dpos[e] = d + (uint32_t)mp1;
+          out.scores[e] = maxs;
+          if (out.cells_out) out.cells_out[e] = cells;
+          cells_total += cells;
+        }
+        have = false;
+      }
+      // next extension
+      if (!flat_fetch(queue, n, order, &e)) {
+        done = true;
+        break;
+      }
+      have = true;
+      finish = false;
+      overflow = false;
+      const bool rev = dir ? dir[e] != 0 : reverse_default != 0;
+      inc = rev ? -1 : 1;
+      q0 = job.query + out.qpos[e];
+      d0 = job.db + out.dpos[e];
+      maxs = 0;
+      mp0 = -inc;
+      mp1 = -inc;
+      cells = 0;
+      r = 0;
+      p1 = 0;
+      if (q0[0] == delim || d0[0] == delim) {
+        finish = true;
+        continue;
+      }
+      // row -1 (src/gapped_extender.cpp:345-364)
+      band[0] = make_int2(0, pack_gap(-gi, 0));
+      int score = -gi, col = 1, res = q0[0];
+      for (;;) {
+        if (res == delim || score < -cutoff) break;
+        if (col >= kFlatW) {
+          overflow = true;
+          break;
+        }
+        band[col * S] = make_int2(score, pack_gap(score - gi, res));
+        score -= ge;
+        ++col;
+        res = q0[(col - 1) * inc];
+      }
+      if (overflow) continue;
+      if (res != delim) {
+        if (col >= kFlatW) {
+          overflow = true;
+          continue;
+        }
+        band[col * S] = make_int2(kInitScore, pack_gap(kInitScore, res));
+        be = col + 1;
+      } else {
+        be = col;
+      }
+      bs = 0;
+      bss = 0;
+      bes = be == kFlatW ? 0 : be;
+      next_x = d0[0];
+    }
+  }
+  return cells_total;
 }
 
 }  // namespace gzb

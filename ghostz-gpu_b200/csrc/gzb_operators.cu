@@ -184,6 +184,120 @@ gapped_lane_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
   if ((threadIdx.x & 31) == 0 && cells) atomicAdd(cells_total, cells);
 }
 
+// Flattened one-thread-per-extension kernel over a device work queue
+// (persistent blocks; `order` optional).  Dynamic shared memory:
+// kFlatW * blockDim.x int2.
+__global__ void __launch_bounds__(kFlatBlock)
+gapped_flat_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number_letters,
+                   int stride, uint64_t n, const uint32_t *__restrict__ order,
+                   unsigned long long *queue, int reverse, const uint8_t *__restrict__ dir,
+                   uint32_t *qpos, uint32_t *dpos, int32_t *scores, uint32_t *spill,
+                   uint32_t *spill_count, unsigned long long *cells_total,
+                   uint32_t *cells_out, int book_threshold) {
+  __shared__ int sm[kMatrixStride * kMatrixStride];
+  extern __shared__ int2 flat_band[];
+  load_matrix(sm, matrix, number_letters, stride);
+  __syncthreads();
+  FlatOut o{qpos, dpos, scores, spill, spill_count, cells_out};
+  const unsigned long long c = gapped_flat(job, sm, flat_band + threadIdx.x, (int)blockDim.x, n,
+                                           order, queue, reverse, dir, o, book_threshold);
+  if (c) atomicAdd(cells_total, c);
+}
+
+// Nested one-thread-per-extension kernel over a device work queue:
+// persistent blocks; each warp takes the next 32 extensions of `order` (or
+// of extension order) and runs them to completion together, so extensions
+// of similar cost placed next to each other keep the warp's lanes busy.
+// cells_out (optional) records every extension's DP cells, UINT32_MAX when
+// it was handed to the fallback.
+__global__ void __launch_bounds__(kLaneBlock)
+gapped_lane_queue_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number_letters,
+                         int stride, uint64_t n, const uint32_t *__restrict__ order,
+                         unsigned long long *queue, int reverse, const uint8_t *__restrict__ dir,
+                         uint32_t *qpos, uint32_t *dpos, int32_t *scores, uint32_t *spill,
+                         uint32_t *spill_count, unsigned long long *cells_total,
+                         uint32_t *cells_out) {
+  __shared__ int sm[kMatrixStride * kMatrixStride];
+  __shared__ uint32_t cells_s[kLaneW * kLaneBlock];
+  __shared__ uint32_t res_s[(kLaneW / 4) * kLaneBlock];
+  load_matrix(sm, matrix, number_letters, stride);
+  __syncthreads();
+  LaneBand band{cells_s, res_s, kLaneBlock, (int)threadIdx.x};
+  const int lane = threadIdx.x & 31;
+  unsigned long long cells = 0;
+  for (;;) {
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(queue, 32ull);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    const uint64_t i = base + lane;
+    if (i < n) {
+      const uint32_t e = order ? order[i] : (uint32_t)i;
+      const bool rev = dir ? dir[e] != 0 : reverse != 0;
+      const uint32_t q = qpos[e], d = dpos[e];
+      GappedOut o = gapped_extend_lane(job, sm, band, q, d, rev);
+      if (o.overflow) {
+        spill[atomicAdd(spill_count, 1u)] = e;
+        if (cells_out) cells_out[e] = 0xFFFFFFFFu;
+      } else {
+        cells += o.cells;
+        store_result(e, q, d, o, qpos, dpos, scores);
+        if (cells_out) cells_out[e] = o.cells > 0xFFFFFFFEull ? 0xFFFFFFFEu : (uint32_t)o.cells;
+      }
+    }
+    __syncwarp();
+  }
+  cells += __shfl_down_sync(0xffffffffu, cells, 16);
+  cells += __shfl_down_sync(0xffffffffu, cells, 8);
+  cells += __shfl_down_sync(0xffffffffu, cells, 4);
+  cells += __shfl_down_sync(0xffffffffu, cells, 2);
+  cells += __shfl_down_sync(0xffffffffu, cells, 1);
+  if (lane == 0 && cells) atomicAdd(cells_total, cells);
+}
+
+// process-wide tile defaults (gzb_set_tile_parameter)
+GappedTile g_tile = {GZB_GAPPED_KERNEL_FLAT, 8};
+
+template <typename K>
+static int persistent_blocks(K kernel, int block, size_t smem, uint64_t n, uint64_t *blocks) {
+  int dev = 0, sms = 148, per_sm = 1;
+  GZB_CUDA(cudaGetDevice(&dev));
+  GZB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  GZB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem));
+  if (per_sm < 1) per_sm = 1;
+  uint64_t b = (uint64_t)sms * per_sm;
+  const uint64_t need = (n + block - 1) / block;
+  if (need < b) b = need ? need : 1;
+  *blocks = b;
+  return GZB_OK;
+}
+
+int launch_gapped_thread(const GappedTile &tile, const GappedJob &job, const int32_t *matrix,
+                         int number_letters, int stride, uint64_t n, const uint32_t *order,
+                         unsigned long long *queue, int reverse, const uint8_t *dir,
+                         uint32_t *qpos, uint32_t *dpos, int32_t *scores, uint32_t *spill,
+                         uint32_t *spill_count, unsigned long long *cells_total,
+                         uint32_t *cells_out, cudaStream_t s) {
+  GZB_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s));
+  uint64_t blocks = 1;
+  if (tile.kernel == GZB_GAPPED_KERNEL_LANE) {
+    GZB_TRY(persistent_blocks(gapped_lane_queue_kernel, kLaneBlock, 0, n, &blocks));
+    gapped_lane_queue_kernel<<<(unsigned)blocks, kLaneBlock, 0, s>>>(
+        job, matrix, number_letters, stride, n, order, queue, reverse, dir, qpos, dpos, scores,
+        spill, spill_count, cells_total, cells_out);
+  } else {
+    const size_t smem = sizeof(int2) * (size_t)kFlatW * kFlatBlock;
+    GZB_CUDA(cudaFuncSetAttribute(gapped_flat_kernel,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GZB_TRY(persistent_blocks(gapped_flat_kernel, kFlatBlock, smem, n, &blocks));
+    gapped_flat_kernel<<<(unsigned)blocks, kFlatBlock, smem, s>>>(
+        job, matrix, number_letters, stride, n, order, queue, reverse, dir, qpos, dpos, scores,
+        spill, spill_count, cells_total, cells_out, tile.book_threshold);
+  }
+  GZB_CUDA(cudaGetLastError());
+  return GZB_OK;
+}
+
 // One warp per listed extension (shared circular band of kBandW columns).
 __global__ void __launch_bounds__(kGappedWarps * 32)
 gapped_warp_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number_letters,
@@ -561,14 +675,17 @@ extern "C" int gzb_gapped_extender_convert_to_gapped_extension_seeds_async(
 namespace gzb {
 // Runs the three-level gapped extension over `n` extensions (optionally in
 // the order given by `order`) whose positions sit in d_qpos/d_dpos (updated
-// in place), writing d_scores.  counters: [0] spilled from the thread
+// in place), writing d_scores (and each extension's DP cells to cells_out,
+// if given, UINT32_MAX for those the thread kernel handed on).  The first
+// level is the thread kernel `tile` names.  counters: [0] spilled from the thread
 // kernel, [1] spilled from the warp kernel, [2] too long for the fallback.
 // `spill` needs room for 2n entries.  Synchronises `s` once at the end.
-int run_gapped(const GappedJob &job, const int32_t *matrix, int number_letters,
-               int stride, size_t n, const uint32_t *order, int reverse, const uint8_t *dir,
-               uint32_t *d_qpos, uint32_t *d_dpos, int32_t *d_scores, uint32_t **spill,
-               size_t *spill_cap, uint32_t *counters, unsigned long long *cells,
-               int2 **band_pool, int *band_wmask, cudaStream_t s, uint32_t *n_fallback) {
+int run_gapped(const GappedTile &tile, const GappedJob &job, const int32_t *matrix,
+               int number_letters, int stride, size_t n, const uint32_t *order, int reverse,
+               const uint8_t *dir, uint32_t *d_qpos, uint32_t *d_dpos, int32_t *d_scores,
+               uint32_t **spill, size_t *spill_cap, uint32_t *counters,
+               unsigned long long *cells, uint32_t *cells_out, int2 **band_pool,
+               int *band_wmask, cudaStream_t s, uint32_t *n_fallback) {
   if (n == 0) return GZB_OK;
   if (*spill_cap < 2 * n) {
     cudaFree(*spill);
@@ -583,12 +700,10 @@ int run_gapped(const GappedJob &job, const int32_t *matrix, int number_letters,
   }
   GZB_CUDA(cudaMemsetAsync(counters, 0, 16, s));
   uint32_t *spill1 = *spill, *spill2 = *spill + n;
-  const unsigned lane_blocks = (unsigned)std::min<size_t>((n + kLaneBlock - 1) / kLaneBlock,
-                                                          (size_t)148 * 40);
-  gapped_lane_kernel<<<lane_blocks, kLaneBlock, 0, s>>>(job, matrix, number_letters, stride, n,
-                                                        order, reverse, dir, d_qpos, d_dpos,
-                                                        d_scores, spill1, counters, cells);
-  GZB_CUDA(cudaGetLastError());
+  // counters[0..3]: spill counts; counters[8..9]: the work queue (64-bit)
+  GZB_TRY(launch_gapped_thread(tile, job, matrix, number_letters, stride, n, order,
+                               (unsigned long long *)(counters + 8), reverse, dir, d_qpos,
+                               d_dpos, d_scores, spill1, counters, cells, cells_out, s));
   const uint32_t *serial_list = spill1, *serial_count = counters;
   if (warp_path_exact(job.cutoff)) {
     gapped_warp_kernel<<<148 * 4, kGappedWarps * 32, 0, s>>>(
@@ -627,10 +742,10 @@ extern "C" int gzb_gapped_extender_extend_one_side_score_only_async(
   job.gap_open = h->gap_open;
   job.gap_ext = h->gap_ext;
   job.cutoff = h->cutoff;
-  GZB_TRY(run_gapped(job, h->matrix, (int)h->number_letters, (int)h->number_letters + 1,
-                     size, nullptr, reverse, nullptr, d_qpos, d_dpos, d_scores, &h->spill,
-                     &h->spill_cap, h->counters, h->cells, &h->band_pool, &h->band_wmask, s,
-                     nullptr));
+  GZB_TRY(run_gapped(g_tile, job, h->matrix, (int)h->number_letters,
+                     (int)h->number_letters + 1, size, nullptr, reverse, nullptr, d_qpos,
+                     d_dpos, d_scores, &h->spill, &h->spill_cap, h->counters, h->cells, nullptr,
+                     &h->band_pool, &h->band_wmask, s, nullptr));
   if (qpos) GZB_CUDA(cudaMemcpyAsync(qpos, d_qpos, 4 * size, cudaMemcpyDefault, s));
   if (dpos) GZB_CUDA(cudaMemcpyAsync(dpos, d_dpos, 4 * size, cudaMemcpyDefault, s));
   if (scores) GZB_CUDA(cudaMemcpyAsync(scores, d_scores, 4 * size, cudaMemcpyDefault, s));
@@ -642,5 +757,34 @@ extern "C" int gzb_gapped_extender_cells(gzb_gapped_extender *h, uint64_t *cells
   unsigned long long c = 0;
   GZB_CUDA(cudaMemcpy(&c, h->cells, sizeof(c), cudaMemcpyDeviceToHost));
   *cells = c;
+  return GZB_OK;
+}
+
+namespace gzb {
+int check_tile_value(int which, int value) {
+  if (which == GZB_TILE_GAPPED_KERNEL) {
+    GZB_CHECK(value == GZB_GAPPED_KERNEL_FLAT || value == GZB_GAPPED_KERNEL_LANE, GZB_ERR_INVALID,
+              "gapped kernel %d is neither GZB_GAPPED_KERNEL_FLAT nor _LANE", value);
+    return GZB_OK;
+  }
+  GZB_CHECK(which == GZB_TILE_BOOK_THRESHOLD, GZB_ERR_INVALID, "unknown tile parameter %d", which);
+  GZB_CHECK(value >= 1 && value <= 32, GZB_ERR_INVALID, "book threshold %d outside 1..32", value);
+  return GZB_OK;
+}
+int *tile_field(GappedTile &t, int which) {
+  return which == GZB_TILE_GAPPED_KERNEL ? &t.kernel : &t.book_threshold;
+}
+}  // namespace gzb
+
+extern "C" int gzb_set_tile_parameter(int which, int value) {
+  GZB_TRY(gzb::check_tile_value(which, value));
+  *gzb::tile_field(gzb::g_tile, which) = value;
+  return GZB_OK;
+}
+
+extern "C" int gzb_get_tile_parameter(int which, int *value) {
+  GZB_CHECK(value, GZB_ERR_INVALID, "null value");
+  GZB_TRY(gzb::check_tile_value(which, which == GZB_TILE_GAPPED_KERNEL ? 0 : 1));
+  *value = *gzb::tile_field(gzb::g_tile, which);
   return GZB_OK;
 }

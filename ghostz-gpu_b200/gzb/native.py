@@ -103,6 +103,12 @@ def _declare(L):
         "gzb_engine_train_cost_model": [V, C.c_int, C.c_int, C.c_float, C.c_uint64, V, V],
         "gzb_engine_set_cost_model": [V, V],
         "gzb_engine_get_schedule_stats": [V, V, V],
+        "gzb_set_tile_parameter": [C.c_int, C.c_int],
+        "gzb_get_tile_parameter": [C.c_int, V],
+        "gzb_engine_autotune": [V, C.c_int, C.c_int, V, C.c_int, V, V, V],
+        "gzb_engine_set_tile": [V, C.c_int, C.c_int, C.c_int],
+        "gzb_engine_get_tile": [V, C.c_int, C.c_int, V],
+        "gzb_engine_get_extension_costs": [V, V, V, C.c_uint64, V, V],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -287,6 +293,10 @@ INDEX_NAMES = ("nc_keys", "nc_offsets", "nc_values", "rep_keys", "rep_offsets",
 SCHEDULE_PLAIN = 0
 SCHEDULE_BATCHED = 1
 SCHEDULE_ORACLE = 2
+TILE_BOOK_THRESHOLD = 0
+TILE_GAPPED_KERNEL = 1
+GAPPED_KERNEL_FLAT = 0
+GAPPED_KERNEL_LANE = 1
 COST_FEATURES = 8
 
 
@@ -419,6 +429,38 @@ class PresearchEngine:
         else:
             p = np.ascontiguousarray(params, np.float32)
             check(lib().gzb_engine_set_cost_model(self.h, hptr(p)))
+
+    def autotune(self, schedule, candidates=(1, 2, 4, 8, 12, 16, 24), which=TILE_BOOK_THRESHOLD,
+                 stream=None):
+        """Picks the fastest value of tile parameter `which` for `schedule` on
+        the resident workload and keeps it for that schedule; returns (chosen
+        value, {candidate: gapped-stage ms}).  Clears the results."""
+        cand = np.array(candidates, np.int32)
+        ms = np.zeros(len(cand), np.float32)
+        best = C.c_int()
+        check(lib().gzb_engine_autotune(self.h, int(schedule), int(which), hptr(cand), len(cand),
+                                        C.byref(best), hptr(ms), _stream_or_null(stream)))
+        return int(best.value), {int(c): float(m) for c, m in zip(cand, ms)}
+
+    def set_tile(self, schedule, which, value):
+        """Tile of `schedule` (-1: the process-wide default)."""
+        check(lib().gzb_engine_set_tile(self.h, int(schedule), int(which), int(value)))
+
+    def tile(self, schedule, which):
+        v = C.c_int()
+        check(lib().gzb_engine_get_tile(self.h, int(schedule), int(which), C.byref(v)))
+        return int(v.value)
+
+    def extension_costs(self, predicted=True):
+        """(predicted log2(1+cells) or None, true DP cells) of the last
+        work-queue run, in extension order."""
+        n = C.c_uint64()
+        check(lib().gzb_engine_get_extension_costs(self.h, None, None, 0, C.byref(n), None))
+        cells = np.zeros(n.value, np.uint32)
+        pred = np.zeros(n.value, np.float32) if predicted else None
+        check(lib().gzb_engine_get_extension_costs(
+            self.h, hptr(pred) if predicted else None, hptr(cells), n.value, C.byref(n), None))
+        return pred, cells
 
     def schedule_stats(self):
         err = C.c_float()

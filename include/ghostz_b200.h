@@ -293,6 +293,47 @@ int gzb_engine_get_index_array(gzb_engine *e, int which, uint32_t *out,
  * query.  Same copy semantics as gzb_engine_get_index_array. */
 int gzb_engine_get_list_array(gzb_engine *e, int which, uint32_t *out,
                               uint64_t capacity, uint64_t *count, void *stream);
+/* Per-extension costs of the last run that used a work-queue schedule
+ * (batched, oracle, or plain with logging on), in extension order: the
+ * reverse extensions of the chained hits, then the forward ones.  cells:
+ * true DP cells (UINT32_MAX for extensions the thread kernel handed to a
+ * fallback); predicted: the model's log2(1 + cells), only after a batched
+ * run with a model.  *count = extensions; either array may be NULL. */
+int gzb_engine_get_extension_costs(gzb_engine *e, float *predicted, uint32_t *cells,
+                                   uint64_t capacity, uint64_t *count, void *stream);
+/* ---- tile parameters and the autotuner -----------------------------------
+ * The first level of the gapped stage runs one extension per thread in one
+ * of two kernels (GZB_TILE_GAPPED_KERNEL):
+ *   GZB_GAPPED_KERNEL_FLAT  every lane advances one DP cell per step; a lane
+ *       at a row or extension boundary waits until GZB_TILE_BOOK_THRESHOLD
+ *       lanes of its warp are (or no lane can step), then they do their
+ *       bookkeeping together (1..32) and take new extensions from the work
+ *       queue, so the lanes of a warp never wait for the slowest extension;
+ *   GZB_GAPPED_KERNEL_LANE  each warp takes the next 32 extensions from the
+ *       work queue and runs them to completion with a tight row/column loop,
+ *       fastest when neighbouring extensions cost the same (the batched
+ *       schedule orders them by predicted cost).
+ * gzb_set_tile_parameter sets the process-wide defaults that the operators
+ * and engines without a tuned tile use. */
+#define GZB_TILE_BOOK_THRESHOLD 0
+#define GZB_TILE_GAPPED_KERNEL 1
+#define GZB_GAPPED_KERNEL_FLAT 0
+#define GZB_GAPPED_KERNEL_LANE 1
+int gzb_set_tile_parameter(int which, int value);
+int gzb_get_tile_parameter(int which, int *value);
+/* Per-engine, per-schedule tile: value -1 falls back to the process-wide
+ * default.  gzb_engine_autotune stores its pick here. */
+int gzb_engine_set_tile(gzb_engine *e, int schedule, int which, int value);
+int gzb_engine_get_tile(gzb_engine *e, int schedule, int which, int *value);
+/* Times the gapped stage of the resident queries and chunk under each
+ * candidate value (candidates[n]) of tile parameter `which` with
+ * `schedule`, keeps the fastest for that schedule (gzb_engine_get_tile) and
+ * returns it in *best (gapped-stage ms per candidate in ms[n] if not
+ * NULL).  Runs the presearch twice per candidate and clears the engine's
+ * results.  Results are identical under every tile. */
+int gzb_engine_autotune(gzb_engine *e, int schedule, int which, const int *candidates,
+                        int n, int *best, float *ms, void *stream);
+
 /* ---- cost model of the gapped stage -------------------------------------
  * An 8 -> 32 -> 32 -> 1 ReLU MLP predicts log2(1 + DP cells) of every gapped
  * extension from its ungapped score, ungapped length, positives and

@@ -82,3 +82,19 @@ def test_cpp_adapters_compile_and_link(tmp_path):
         "-I", os.path.join(root, "ghostz-gpu_b200", "adapters"),
         "-I", "/usr/local/cuda/include", str(src), "-o", str(exe),
         B.LIB, "-Wl,-rpath," + os.path.dirname(B.LIB)])
+
+
+def test_tile_parameters_validate_without_device():
+    from gzb import native as N
+    L = N.lib()
+    v = ctypes.c_int()
+    for which in (N.TILE_BOOK_THRESHOLD, N.TILE_GAPPED_KERNEL):
+        assert L.gzb_get_tile_parameter(which, ctypes.byref(v)) == 0
+        keep = v.value
+        assert L.gzb_set_tile_parameter(which, keep) == 0
+    assert L.gzb_set_tile_parameter(N.TILE_BOOK_THRESHOLD, 0) == 1
+    assert L.gzb_set_tile_parameter(N.TILE_BOOK_THRESHOLD, 33) == 1
+    assert L.gzb_set_tile_parameter(N.TILE_GAPPED_KERNEL, 2) == 1
+    assert b"neither" in L.gzb_last_error()
+    assert L.gzb_set_tile_parameter(7, 1) == 1
+    assert L.gzb_get_tile_parameter(7, ctypes.byref(v)) == 1

@@ -60,3 +60,44 @@ def test_learned_schedule_identical_results_and_accurate(engine, params):
     engine.reset_results()
     engine.presearch(N.SCHEDULE_BATCHED)
     assert all(np.array_equal(a, b) for a, b in zip(plain, engine.results()))
+
+
+def _warp_cost(cells, order):
+    """DP cells the lane kernel pays when each warp runs 32 consecutive
+    extensions of `order` to completion: 32 x the costliest of each group."""
+    c = cells[order].astype(np.float64)
+    pad = (-len(c)) % 32
+    c = np.concatenate([c, np.zeros(pad)])
+    return 32.0 * c.reshape(-1, 32).max(axis=1).sum()
+
+
+def test_trained_model_reduces_lane_kernel_work(engine, params):
+    """What the network gains over the schedule without it: the same
+    extension list costs the lane kernel fewer warp-steps in predicted-cost
+    order than in the plain hit order (the method without a model), with the
+    true-cost order as the bound."""
+    from gzb import native as N
+    db = W.make_database(6000, 1301, median=300)
+    q = W.make_queries(db, 600, 1302, median=300)
+    engine.set_params(params)
+    engine.set_database(db)
+    engine.set_queries(q)
+    engine.set_logging(True, 1 << 22)
+    engine.presearch(N.SCHEDULE_PLAIN)
+    engine.train_cost_model(epochs=40, batch=2048, lr=3e-3, seed=5)
+    engine.set_logging(False)
+    db2 = W.make_database(6000, 1401, median=300)
+    q2 = W.make_queries(db2, 600, 1402, median=300)
+    engine.set_database(db2)
+    engine.set_queries(q2)
+    engine.reset_results()
+    engine.presearch(N.SCHEDULE_BATCHED)
+    pred, cells = engine.extension_costs()
+    assert len(cells) == engine.counters()["gapped_extensions"] and len(cells) > 1000
+    cells = np.where(cells == 0xFFFFFFFF, 0, cells)  # handed to the fallback kernels
+    plain = _warp_cost(cells, np.arange(len(cells)))
+    learned = _warp_cost(cells, np.argsort(-pred, kind="stable"))
+    best = _warp_cost(cells, np.argsort(-cells.astype(np.int64), kind="stable"))
+    print(f"lane-kernel work / DP cells: plain {plain / cells.sum():.3f} "
+          f"learned {learned / cells.sum():.3f} true-cost order {best / cells.sum():.3f}")
+    assert best <= learned < 0.95 * plain
