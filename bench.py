@@ -194,7 +194,7 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-KERNEL_NAMES = {0: "flat", 1: "lane"}
+KERNEL_NAMES = {0: "flat", 1: "lane", 2: "rows", 3: "static"}
 
 
 def main():
@@ -285,35 +285,43 @@ def main():
         barrier()
         return ev0.elapsed_time(ev1), {k: v / args.steps for k, v in stage.items()}
 
-    # autotuned tile of the gapped stage per schedule (untimed set-up; results
-    # do not depend on it): the flat kernel's bookkeeping threshold, then the
-    # thread kernel itself; the oracle order runs with the batched tile
-    order = ["plain"] + (["batched", "oracle"] if args.schedule == "batched" else [])
-    sched_id = {"plain": N.SCHEDULE_PLAIN, "batched": N.SCHEDULE_BATCHED,
-                "oracle": N.SCHEDULE_ORACLE}
+    # Schedules of the gapped stage, all with bit-identical results:
+    #   plain   the static schedule (one launch dealing extensions to threads
+    #           in hit order; no work queue, tile or model);
+    #   queue   the batched pipeline's persistent work-queue kernel with the
+    #           autotuned tile, hit order (the batched schedule without a model);
+    #   batched the same, ordered by the learned cost model (the headline);
+    #   oracle  the same, ordered by the true costs (a measuring stick).
+    # The autotuner (untimed set-up) picks the flat kernel's bookkeeping
+    # threshold, then the thread kernel, for the batched schedule.
+    order = ["plain"] + (["queue", "batched", "oracle"] if args.schedule == "batched" else [])
+    sched_id = {"plain": N.SCHEDULE_PLAIN, "queue": N.SCHEDULE_BATCHED,
+                "batched": N.SCHEDULE_BATCHED, "oracle": N.SCHEDULE_ORACLE}
     tiles = {}
-    for name in order:
-        sid = sched_id[name]
-        if name == "oracle":
-            for w in (N.TILE_GAPPED_KERNEL, N.TILE_BOOK_THRESHOLD):
-                eng.set_tile(sid, w, eng.tile(N.SCHEDULE_BATCHED, w))
-        elif not args.no_autotune:
+    if args.schedule == "batched":
+        sid = N.SCHEDULE_BATCHED
+        if not args.no_autotune:
             eng.set_tile(sid, N.TILE_GAPPED_KERNEL, N.GAPPED_KERNEL_FLAT)
             thr, thr_ms = eng.autotune(sid, (4, 8, 12, 16, 24), N.TILE_BOOK_THRESHOLD)
-            ker, ker_ms = eng.autotune(sid, (N.GAPPED_KERNEL_FLAT, N.GAPPED_KERNEL_LANE),
-                                       N.TILE_GAPPED_KERNEL)
-            tiles[name] = {"gapped_ms_by_book_threshold": thr_ms,
-                           "gapped_ms_by_kernel": {KERNEL_NAMES[k]: v for k, v in ker_ms.items()}}
-        tiles.setdefault(name, {}).update(
-            kernel=KERNEL_NAMES[eng.tile(sid, N.TILE_GAPPED_KERNEL)],
-            book_threshold=eng.tile(sid, N.TILE_BOOK_THRESHOLD))
+            ker, ker_ms = eng.autotune(sid, (N.GAPPED_KERNEL_FLAT, N.GAPPED_KERNEL_LANE,
+                                             N.GAPPED_KERNEL_ROWS), N.TILE_GAPPED_KERNEL)
+            tiles = {"gapped_ms_by_book_threshold": thr_ms,
+                     "gapped_ms_by_kernel": {KERNEL_NAMES[k]: v for k, v in ker_ms.items()}}
+        for w in (N.TILE_GAPPED_KERNEL, N.TILE_BOOK_THRESHOLD):
+            eng.set_tile(N.SCHEDULE_ORACLE, w, eng.tile(sid, w))
+        tiles.update(kernel=KERNEL_NAMES[eng.tile(sid, N.TILE_GAPPED_KERNEL)],
+                     book_threshold=eng.tile(sid, N.TILE_BOOK_THRESHOLD))
 
     sampler = ClockSampler(local_rank)
     sampler.start()
     runs = {}
     results_by = {}
     for name in order:
+        if name == "queue":
+            eng.set_cost_model(None)
         ms, st = timed(sched_id[name])
+        if name == "queue":
+            eng.set_cost_model(model)
         cnt = eng.counters()
         runs[name] = {"ms": ms, "stage": st, "counters": cnt}
         if name == "batched":
@@ -389,11 +397,13 @@ def main():
             sched_report[name]["mean_abs_log2_cost_error"] = r["mean_abs_log2_cost_error"]
     if "batched" in runs:
         sched_report["batched_over_plain"] = runs["plain"]["ms"] / runs["batched"]["ms"]
+        sched_report["queue_over_plain"] = runs["plain"]["ms"] / runs["queue"]["ms"]
+        sched_report["model_gain_over_queue"] = runs["queue"]["ms"] / runs["batched"]["ms"]
         sched_report["throughput_lost_vs_oracle"] = 1.0 - runs["oracle"]["ms"] / runs["batched"]["ms"]
     sched_report["results_identical_across_schedules"] = bool(identical)
     sched_report["cost_model"] = {"train_pairs": train_pairs, "train_mse_log2": train_loss,
                                   "setup_s": train_s}
-    sched_report["tiles"] = tiles
+    sched_report["batched_tile"] = tiles
     gcups_stage = counters["gapped_cells"] / (st["gapped"] / 1e3) / 1e9 if st["gapped"] else 0.0
     gcups_step = counters["gapped_cells"] / (t_dev / steps / 1e3) / 1e9
     # roofline of the dominant stage

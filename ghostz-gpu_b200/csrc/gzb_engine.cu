@@ -1698,6 +1698,7 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
     GappedTile tile = g_tile;
     for (int w = 0; w < 2; ++w)
       if (e->tile[schedule][w] >= 0) *tile_field(tile, w) = e->tile[schedule][w];
+    if (schedule == GZB_SCHEDULE_PLAIN) tile.kernel = GZB_GAPPED_KERNEL_STATIC;
     if (scheduled) GZB_TRY(e->ecells.ensure(4 * (next + 1)));
     GZB_TRY(run_gapped(tile, job, e->matrix32.as<int32_t>(), 32, 32, next, order, 0,
                        e->edir.as<uint8_t>(), e->eq.as<uint32_t>(), e->ed.as<uint32_t>(),

@@ -493,28 +493,22 @@ namespace gzb {
 // Gapped extension, one thread per extension (the common, narrow-band case).
 // The exact serial recurrence of GappedExtender::ExtendOneSideScoreOnly with
 // the band in shared memory: kLaneW columns per thread, each a packed int16
-// pair (best, best_gap), plus the query residue of each band column, laid
-// out [column][thread] so that a warp touching one column per thread is
-// bank-conflict free.  A band wider than kLaneW, or a value outside int16,
-// makes the extension overflow; the caller reruns it on the warp kernel.
+// pair (best, best_gap), plus the query residue of each band column (one
+// byte), laid out [column][thread] so that a warp touching one column per
+// thread is bank-conflict free.  A band wider than kLaneW, or a value
+// outside int16, makes the extension overflow; the caller reruns it on the
+// warp kernel.
 constexpr int kLaneW = 64;
 
 struct LaneBand {
   uint32_t *cell;  // [kLaneW][stride]
-  uint32_t *res;   // [kLaneW/4][stride], 4 residues per word
+  uint8_t *res;    // [kLaneW][stride]
   int stride;
   int t;           // this thread's column in the layout
-  __device__ __forceinline__ uint32_t &at(int c) { return cell[(c & (kLaneW - 1)) * stride + t]; }
-  __device__ __forceinline__ int residue(int c) const {
-    const int k = c & (kLaneW - 1);
-    return (res[(k >> 2) * stride + t] >> ((k & 3) * 8)) & 0xff;
-  }
-  __device__ __forceinline__ void set_residue(int c, int r) {
-    const int k = c & (kLaneW - 1);
-    uint32_t &w = res[(k >> 2) * stride + t];
-    const int sh = (k & 3) * 8;
-    w = (w & ~(0xffu << sh)) | ((uint32_t)r << sh);
-  }
+  __device__ __forceinline__ int slot(int c) const { return (c & (kLaneW - 1)) * stride + t; }
+  __device__ __forceinline__ uint32_t &at(int c) { return cell[slot(c)]; }
+  __device__ __forceinline__ int residue(int c) const { return res[slot(c)]; }
+  __device__ __forceinline__ void set_residue(int c, int r) { res[slot(c)] = (uint8_t)r; }
 };
 
 __device__ __forceinline__ bool fits16(int v) { return v >= -32768 && v <= 32767; }
@@ -524,134 +518,173 @@ __device__ __forceinline__ uint32_t pack16(int best, int gap) {
 __device__ __forceinline__ int lo16(uint32_t w) { return (int)(int16_t)(uint16_t)(w & 0xffff); }
 __device__ __forceinline__ int hi16(uint32_t w) { return (int)(int16_t)(uint16_t)(w >> 16); }
 
-__device__ inline GappedOut gapped_extend_lane(const GappedJob &job, const int *sm,
-                                               LaneBand band, uint32_t qpos, uint32_t dpos,
-                                               bool reverse) {
+// State of one extension on the lane kernels, kept in registers between
+// rows: band [bs, be) of absolute columns, the running maximum and its
+// position, the database offset of the next row and the cell count.
+struct LaneExt {
+  const uint8_t *q0, *d0;
+  int inc;
+  int bs, be;
+  int maxs, mp0, mp1;
+  int p1;
+  uint32_t cells;
+  bool ovf;
+};
+
+enum : int { kLaneRunning = 0, kLaneDone = 1, kLaneOverflow = 2 };
+
+// Row -1 of GappedExtender::ExtendOneSideScoreOnly
+// (src/gapped_extender.cpp:345-364): the gap-open row along the query until
+// it drops below -cutoff, plus the sentinel column.
+__device__ __forceinline__ int lane_init(const GappedJob &job, LaneBand &band, LaneExt &x,
+                                         const uint8_t *q0, const uint8_t *d0, bool reverse) {
   const int inc = reverse ? -1 : 1;
   const int delim = job.delim;
   const int ge = job.gap_ext;
   const int gi = job.gap_open + job.gap_ext;
-  const int cutoff = job.cutoff;
-  const uint8_t *q0 = job.query + qpos;
-  const uint8_t *d0 = job.db + dpos;
-  GappedOut out;
-  out.score = 0;
-  out.pos0 = -inc;
-  out.pos1 = -inc;
-  out.cells = 0;
-  out.overflow = false;
-  if (q0[0] == delim || d0[0] == delim) return out;
-  bool ovf = false;
-  // row -1 (src/gapped_extender.cpp:345-364)
+  x.q0 = q0;
+  x.d0 = d0;
+  x.inc = inc;
+  x.maxs = 0;
+  x.mp0 = -inc;
+  x.mp1 = -inc;
+  x.p1 = 0;
+  x.cells = 0;
+  x.ovf = false;
+  if (q0[0] == delim || d0[0] == delim) return kLaneDone;
+  // every value a row keeps lies in [maxs - cutoff - gi, maxs] with maxs >= 0,
+  // so checking maxs once per row is enough when cutoff + gi fits
+  x.ovf = job.cutoff + gi > 32767;
   band.at(0) = pack16(0, -gi);
-  ovf |= !fits16(-gi);
+  x.ovf |= !fits16(-gi);
   int score = -gi;
   int col = 1;
   int r = q0[0];
   for (;;) {
-    if (r == delim || score < -cutoff) break;
-    if (col >= kLaneW) {
-      out.overflow = true;
-      return out;
-    }
-    ovf |= !fits16(score) || !fits16(score - gi);
+    if (r == delim || score < -job.cutoff) break;
+    if (col >= kLaneW) return kLaneOverflow;
+    x.ovf |= !fits16(score) || !fits16(score - gi);
     band.at(col) = pack16(score, score - gi);
     band.set_residue(col, r);
     score -= ge;
     ++col;
     r = q0[(col - 1) * inc];
   }
-  int bs = 0, be;
+  x.bs = 0;
   if (r != delim) {
-    if (col >= kLaneW) {
-      out.overflow = true;
-      return out;
-    }
+    if (col >= kLaneW) return kLaneOverflow;
     band.at(col) = pack16(kInitScore, kInitScore);
     band.set_residue(col, r);
-    be = col + 1;
+    x.be = col + 1;
   } else {
-    be = col;
+    x.be = col;
   }
-  int maxs = 0, mp0 = -inc, mp1 = -inc;
-  uint64_t cells = 0;
-  for (int p1 = 0;; p1 += inc) {
-    const int x = d0[p1];
-    if (x == delim) break;
-    const int *mrow = sm + x * kMatrixStride;
-    uint32_t &c0 = band.at(bs);
-    const uint32_t w0 = c0;
-    int diag = lo16(w0);
-    const int g0 = hi16(w0);
-    const int nb0 = (maxs - g0 > cutoff) ? kInitScore : g0;
-    int row_gap = nb0 - gi;
-    ovf |= !fits16(g0 - ge);
-    c0 = pack16(nb0, g0 - ge);
-    int last = bs;
-    const int bs_row = bs;
-    int pos0 = bs_row * inc;
-    for (int c = bs_row + 1; c < be; ++c, pos0 += inc) {
-      uint32_t &cw = band.at(c);
-      const uint32_t w = cw;
-      const int old_best = lo16(w), vgap = hi16(w);
-      int s = diag + mrow[band.residue(c)];
-      diag = old_best;
-      s = imax(s, imax(vgap, row_gap));
-      ++cells;
-      if (maxs - s > cutoff) {
-        if (bs + 1 == c) ++bs;
-        cw = pack16(kInitScore, kInitScore);
-        row_gap = kInitScore;
-      } else {
-        last = c;
-        if (s > maxs) {
-          maxs = s;
-          mp0 = pos0;
-          mp1 = p1;
-        }
-        const int ng = imax(s - gi, vgap - ge);
-        row_gap = imax(s - gi, row_gap - ge);
-        ovf |= !fits16(s) || !fits16(ng);
-        cw = pack16(s, ng);
-      }
-    }
-    if (bs + 1 == be) break;
-    int edge;  // residue the reference tests after the row (:461)
-    if (last < be - 1) {
-      edge = q0[(be - 1) * inc];  // old right edge
-      be = last + 1;
+  return kLaneRunning;
+}
+
+// One database row of the recurrence (src/gapped_extender.cpp:366-470):
+// the cells of the band, the X-drop trimming of its left edge, and the
+// right edge moving or growing along the gap row.
+__device__ __forceinline__ int lane_row(const GappedJob &job, const int *sm, LaneBand &band,
+                                        LaneExt &x) {
+  const int inc = x.inc;
+  const int delim = job.delim;
+  const int ge = job.gap_ext;
+  const int gi = job.gap_open + job.gap_ext;
+  const int cutoff = job.cutoff;
+  const uint8_t *q0 = x.q0;
+  const int p1 = x.p1;
+  const int xr = x.d0[p1];
+  if (xr == delim) return kLaneDone;
+  const int *mrow = sm + xr * kMatrixStride;
+  int bs = x.bs, be = x.be, maxs = x.maxs;
+  bool ovf = x.ovf;
+  uint32_t &c0 = band.at(bs);
+  const uint32_t w0 = c0;
+  int diag = lo16(w0);
+  const int g0 = hi16(w0);
+  const int nb0 = (maxs - g0 > cutoff) ? kInitScore : g0;
+  int row_gap = nb0 - gi;
+  ovf |= !fits16(g0 - ge);
+  c0 = pack16(nb0, g0 - ge);
+  int last = bs;
+  const int bs_row = bs;
+  const int maxs_in = maxs;
+  int maxc = bs_row;
+  for (int c = bs_row + 1; c < be; ++c) {
+    const int k = band.slot(c);
+    const uint32_t w = band.cell[k];
+    const int old_best = lo16(w), vgap = hi16(w);
+    int s = diag + mrow[band.res[k]];
+    diag = old_best;
+    s = imax(s, imax(vgap, row_gap));
+    if (maxs - s > cutoff) {
+      if (bs + 1 == c) ++bs;
+      band.cell[k] = pack16(kInitScore, kInitScore);
+      row_gap = kInitScore;
     } else {
-      edge = q0[(be - 1) * inc];
-      while (row_gap >= maxs - cutoff && edge != delim) {
-        if (be - bs >= kLaneW) {
-          out.overflow = true;
-          return out;
-        }
-        ovf |= !fits16(row_gap) || !fits16(row_gap - gi);
-        band.at(be) = pack16(row_gap, row_gap - gi);
-        band.set_residue(be, edge);
-        row_gap -= ge;
-        ++be;
-        ++cells;
-        edge = q0[(be - 1) * inc];
+      last = c;
+      if (s > maxs) {
+        maxs = s;
+        maxc = c;
       }
-    }
-    if (edge != delim) {
-      if (be - bs >= kLaneW) {
-        out.overflow = true;
-        return out;
-      }
-      band.at(be) = pack16(kInitScore, kInitScore);
-      // the sentinel column's own residue (differs from `edge` when the band shrank)
-      band.set_residue(be, q0[(be - 1) * inc]);
-      ++be;
+      const int ng = imax(s - gi, vgap - ge);
+      row_gap = imax(s - gi, row_gap - ge);
+      band.cell[k] = pack16(s, ng);
     }
   }
-  out.overflow = ovf;
-  out.score = maxs;
-  out.pos0 = mp0;
-  out.pos1 = mp1;
-  out.cells = cells;
+  const uint32_t cells = (uint32_t)(be - bs_row - 1);
+  if (maxs > maxs_in) {
+    x.mp0 = (maxc - 1) * inc;
+    x.mp1 = p1;
+  }
+  ovf |= maxs > 32767;
+  x.cells += cells;
+  x.maxs = maxs;
+  x.ovf = ovf;
+  x.bs = bs;
+  if (bs + 1 == be) return kLaneDone;
+  int edge;  // residue the reference tests after the row (:461)
+  if (last < be - 1) {
+    edge = q0[(be - 1) * inc];  // old right edge
+    be = last + 1;
+  } else {
+    edge = q0[(be - 1) * inc];
+    while (row_gap >= maxs - cutoff && edge != delim) {
+      if (be - bs >= kLaneW) return kLaneOverflow;
+      x.ovf |= !fits16(row_gap) || !fits16(row_gap - gi);
+      band.at(be) = pack16(row_gap, row_gap - gi);
+      band.set_residue(be, edge);
+      row_gap -= ge;
+      ++be;
+      ++x.cells;
+      edge = q0[(be - 1) * inc];
+    }
+  }
+  if (edge != delim) {
+    if (be - bs >= kLaneW) return kLaneOverflow;
+    band.at(be) = pack16(kInitScore, kInitScore);
+    // the sentinel column's own residue (differs from `edge` when the band shrank)
+    band.set_residue(be, q0[(be - 1) * inc]);
+    ++be;
+  }
+  x.be = be;
+  x.p1 = p1 + inc;
+  return kLaneRunning;
+}
+
+__device__ inline GappedOut gapped_extend_lane(const GappedJob &job, const int *sm,
+                                               LaneBand band, uint32_t qpos, uint32_t dpos,
+                                               bool reverse) {
+  LaneExt x;
+  int st = lane_init(job, band, x, job.query + qpos, job.db + dpos, reverse);
+  while (st == kLaneRunning) st = lane_row(job, sm, band, x);
+  GappedOut out;
+  out.overflow = st == kLaneOverflow || x.ovf;
+  out.score = x.maxs;
+  out.pos0 = x.mp0;
+  out.pos1 = x.mp1;
+  out.cells = x.cells;
   return out;
 }
 

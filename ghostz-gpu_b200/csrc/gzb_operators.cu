@@ -155,10 +155,10 @@ gapped_lane_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
                    int stride, size_t n, const uint32_t *__restrict__ order, int reverse,
                    const uint8_t *__restrict__ dir, uint32_t *qpos, uint32_t *dpos,
                    int32_t *scores, uint32_t *spill, uint32_t *spill_count,
-                   unsigned long long *cells_total) {
+                   unsigned long long *cells_total, uint32_t *cells_out) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
   __shared__ uint32_t cells_s[kLaneW * kLaneBlock];
-  __shared__ uint32_t res_s[(kLaneW / 4) * kLaneBlock];
+  __shared__ uint8_t res_s[kLaneW * kLaneBlock];
   load_matrix(sm, matrix, number_letters, stride);
   __syncthreads();
   LaneBand band{cells_s, res_s, kLaneBlock, (int)threadIdx.x};
@@ -171,9 +171,11 @@ gapped_lane_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
     GappedOut o = gapped_extend_lane(job, sm, band, q, d, rev);
     if (o.overflow) {
       spill[atomicAdd(spill_count, 1u)] = e;
+      if (cells_out) cells_out[e] = 0xFFFFFFFFu;
     } else {
       cells += o.cells;
       store_result(e, q, d, o, qpos, dpos, scores);
+      if (cells_out) cells_out[e] = (uint32_t)o.cells;
     }
   }
   cells += __shfl_down_sync(0xffffffffu, cells, 16);
@@ -219,7 +221,7 @@ gapped_lane_queue_kernel(GappedJob job, const int32_t *__restrict__ matrix, int 
                          uint32_t *cells_out) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
   __shared__ uint32_t cells_s[kLaneW * kLaneBlock];
-  __shared__ uint32_t res_s[(kLaneW / 4) * kLaneBlock];
+  __shared__ uint8_t res_s[kLaneW * kLaneBlock];
   load_matrix(sm, matrix, number_letters, stride);
   __syncthreads();
   LaneBand band{cells_s, res_s, kLaneBlock, (int)threadIdx.x};
@@ -255,8 +257,66 @@ gapped_lane_queue_kernel(GappedJob job, const int32_t *__restrict__ matrix, int 
   if (lane == 0 && cells) atomicAdd(cells_total, cells);
 }
 
+// Row-granular work queue: every lane runs its own extension one database
+// row per step and takes the next extension from the queue as soon as its
+// own ends, so the lanes of a warp wait for each other only within a row
+// (the widest band of the step), never for the longest extension.
+__global__ void __launch_bounds__(kLaneBlock)
+gapped_rows_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number_letters,
+                   int stride, uint64_t n, const uint32_t *__restrict__ order,
+                   unsigned long long *queue, int reverse, const uint8_t *__restrict__ dir,
+                   uint32_t *qpos, uint32_t *dpos, int32_t *scores, uint32_t *spill,
+                   uint32_t *spill_count, unsigned long long *cells_total,
+                   uint32_t *cells_out) {
+  __shared__ int sm[kMatrixStride * kMatrixStride];
+  __shared__ uint32_t cells_s[kLaneW * kLaneBlock];
+  __shared__ uint8_t res_s[kLaneW * kLaneBlock];
+  load_matrix(sm, matrix, number_letters, stride);
+  __syncthreads();
+  LaneBand band{cells_s, res_s, kLaneBlock, (int)threadIdx.x};
+  LaneExt x;
+  uint32_t e = 0, q = 0, d = 0;
+  bool have = false, done = false;
+  unsigned long long cells = 0;
+  for (;;) {
+    int st = kLaneRunning;
+    if (have) st = lane_row(job, sm, band, x);
+    while (st != kLaneRunning || (!have && !done)) {
+      if (have) {  // the extension ended: write it out
+        if (st == kLaneOverflow || x.ovf) {
+          spill[atomicAdd(spill_count, 1u)] = e;
+          if (cells_out) cells_out[e] = 0xFFFFFFFFu;
+        } else {
+          cells += x.cells;
+          qpos[e] = q + (uint32_t)x.mp0;
+          dpos[e] = d + (uint32_t)x.mp1;
+          scores[e] = x.maxs;
+          if (cells_out) cells_out[e] = x.cells;
+        }
+        have = false;
+      }
+      if (!flat_fetch(queue, n, order, &e)) {
+        done = true;
+        break;
+      }
+      const bool rev = dir ? dir[e] != 0 : reverse != 0;
+      q = qpos[e];
+      d = dpos[e];
+      st = lane_init(job, band, x, job.query + q, job.db + d, rev);
+      have = true;
+    }
+    if (__all_sync(0xffffffffu, done)) break;
+  }
+  cells += __shfl_down_sync(0xffffffffu, cells, 16);
+  cells += __shfl_down_sync(0xffffffffu, cells, 8);
+  cells += __shfl_down_sync(0xffffffffu, cells, 4);
+  cells += __shfl_down_sync(0xffffffffu, cells, 2);
+  cells += __shfl_down_sync(0xffffffffu, cells, 1);
+  if ((threadIdx.x & 31) == 0 && cells) atomicAdd(cells_total, cells);
+}
+
 // process-wide tile defaults (gzb_set_tile_parameter)
-GappedTile g_tile = {GZB_GAPPED_KERNEL_FLAT, 8};
+GappedTile g_tile = {GZB_GAPPED_KERNEL_ROWS, 16};
 
 template <typename K>
 static int persistent_blocks(K kernel, int block, size_t smem, uint64_t n, uint64_t *blocks) {
@@ -280,7 +340,19 @@ int launch_gapped_thread(const GappedTile &tile, const GappedJob &job, const int
                          uint32_t *cells_out, cudaStream_t s) {
   GZB_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s));
   uint64_t blocks = 1;
-  if (tile.kernel == GZB_GAPPED_KERNEL_LANE) {
+  if (tile.kernel == GZB_GAPPED_KERNEL_STATIC) {
+    // one launch, extensions dealt to threads round-robin, no work queue
+    blocks = (n + kLaneBlock - 1) / kLaneBlock;
+    if (blocks > 148 * 40) blocks = 148 * 40;
+    gapped_lane_kernel<<<(unsigned)blocks, kLaneBlock, 0, s>>>(
+        job, matrix, number_letters, stride, n, order, reverse, dir, qpos, dpos, scores, spill,
+        spill_count, cells_total, cells_out);
+  } else if (tile.kernel == GZB_GAPPED_KERNEL_ROWS) {
+    GZB_TRY(persistent_blocks(gapped_rows_kernel, kLaneBlock, 0, n, &blocks));
+    gapped_rows_kernel<<<(unsigned)blocks, kLaneBlock, 0, s>>>(
+        job, matrix, number_letters, stride, n, order, queue, reverse, dir, qpos, dpos, scores,
+        spill, spill_count, cells_total, cells_out);
+  } else if (tile.kernel == GZB_GAPPED_KERNEL_LANE) {
     GZB_TRY(persistent_blocks(gapped_lane_queue_kernel, kLaneBlock, 0, n, &blocks));
     gapped_lane_queue_kernel<<<(unsigned)blocks, kLaneBlock, 0, s>>>(
         job, matrix, number_letters, stride, n, order, queue, reverse, dir, qpos, dpos, scores,
@@ -763,8 +835,9 @@ extern "C" int gzb_gapped_extender_cells(gzb_gapped_extender *h, uint64_t *cells
 namespace gzb {
 int check_tile_value(int which, int value) {
   if (which == GZB_TILE_GAPPED_KERNEL) {
-    GZB_CHECK(value == GZB_GAPPED_KERNEL_FLAT || value == GZB_GAPPED_KERNEL_LANE, GZB_ERR_INVALID,
-              "gapped kernel %d is neither GZB_GAPPED_KERNEL_FLAT nor _LANE", value);
+    GZB_CHECK(value >= GZB_GAPPED_KERNEL_FLAT && value <= GZB_GAPPED_KERNEL_STATIC,
+              GZB_ERR_INVALID,
+              "gapped kernel %d is none of GZB_GAPPED_KERNEL_FLAT/LANE/ROWS/STATIC", value);
     return GZB_OK;
   }
   GZB_CHECK(which == GZB_TILE_BOOK_THRESHOLD, GZB_ERR_INVALID, "unknown tile parameter %d", which);

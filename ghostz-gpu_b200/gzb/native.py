@@ -297,6 +297,8 @@ TILE_BOOK_THRESHOLD = 0
 TILE_GAPPED_KERNEL = 1
 GAPPED_KERNEL_FLAT = 0
 GAPPED_KERNEL_LANE = 1
+GAPPED_KERNEL_ROWS = 2
+GAPPED_KERNEL_STATIC = 3
 COST_FEATURES = 8
 
 

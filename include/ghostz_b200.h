@@ -234,11 +234,14 @@ typedef struct {
 } gzb_counters;
 
 /* schedule of the gapped stage (results are identical under every one) */
-#define GZB_SCHEDULE_PLAIN 0    /* one launch over the extensions in hit order */
-#define GZB_SCHEDULE_BATCHED 1  /* persistent blocks on a device work queue,
-                                   extensions ordered longest-predicted first
-                                   by the cost model (plain order when no
-                                   model is set) */
+#define GZB_SCHEDULE_PLAIN 0    /* the static schedule: one launch that deals
+                                   the extensions to threads in hit order
+                                   (GZB_GAPPED_KERNEL_STATIC), no work queue,
+                                   no tile, no model */
+#define GZB_SCHEDULE_BATCHED 1  /* persistent kernel of the engine's tile on a
+                                   device work queue, extensions ordered
+                                   longest-predicted first by the cost model
+                                   (hit order when no model is set) */
 #define GZB_SCHEDULE_ORACLE 2   /* as BATCHED, ordered by the true costs of
                                    the previous scheduled run of the same
                                    extensions (a measuring stick) */
@@ -303,7 +306,7 @@ int gzb_engine_get_extension_costs(gzb_engine *e, float *predicted, uint32_t *ce
                                    uint64_t capacity, uint64_t *count, void *stream);
 /* ---- tile parameters and the autotuner -----------------------------------
  * The first level of the gapped stage runs one extension per thread in one
- * of two kernels (GZB_TILE_GAPPED_KERNEL):
+ * of four kernels (GZB_TILE_GAPPED_KERNEL):
  *   GZB_GAPPED_KERNEL_FLAT  every lane advances one DP cell per step; a lane
  *       at a row or extension boundary waits until GZB_TILE_BOOK_THRESHOLD
  *       lanes of its warp are (or no lane can step), then they do their
@@ -312,13 +315,21 @@ int gzb_engine_get_extension_costs(gzb_engine *e, float *predicted, uint32_t *ce
  *   GZB_GAPPED_KERNEL_LANE  each warp takes the next 32 extensions from the
  *       work queue and runs them to completion with a tight row/column loop,
  *       fastest when neighbouring extensions cost the same (the batched
- *       schedule orders them by predicted cost).
+ *       schedule orders them by predicted cost);
+ *   GZB_GAPPED_KERNEL_ROWS  each lane runs its extension one database row
+ *       per step and takes the next extension from the queue as soon as its
+ *       own ends, so lanes wait for each other only within a row (the
+ *       process-wide default);
+ *   GZB_GAPPED_KERNEL_STATIC  one launch that deals extensions to threads
+ *       round-robin, no work queue: the plain schedule's kernel.
  * gzb_set_tile_parameter sets the process-wide defaults that the operators
  * and engines without a tuned tile use. */
 #define GZB_TILE_BOOK_THRESHOLD 0
 #define GZB_TILE_GAPPED_KERNEL 1
 #define GZB_GAPPED_KERNEL_FLAT 0
 #define GZB_GAPPED_KERNEL_LANE 1
+#define GZB_GAPPED_KERNEL_ROWS 2
+#define GZB_GAPPED_KERNEL_STATIC 3
 int gzb_set_tile_parameter(int which, int value);
 int gzb_get_tile_parameter(int which, int *value);
 /* Per-engine, per-schedule tile: value -1 falls back to the process-wide

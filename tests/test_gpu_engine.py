@@ -108,16 +108,18 @@ def test_presearch_repeated_calls_identical(engine, params):
     assert all(np.array_equal(x, y) for x, y in zip(a, b))
 
 
-@pytest.mark.parametrize("kernel,threshold", [(1, 8), (0, 1), (0, 32)])
+@pytest.mark.parametrize("kernel,threshold", [(0, 1), (0, 32), (1, 8), (2, 8), (3, 8)])
 def test_presearch_every_gapped_tile(engine, oracle, params, kernel, threshold):
-    # both one-thread-per-extension kernels, and the flat kernel's extreme
-    # bookkeeping thresholds, give the oracle's results
+    # every one-thread-per-extension kernel on the work-queue schedule (no
+    # model: hit order), and the flat kernel's extreme bookkeeping
+    # thresholds, give the oracle's results
     from gzb import native as N
-    engine.set_tile(N.SCHEDULE_PLAIN, N.TILE_GAPPED_KERNEL, kernel)
-    engine.set_tile(N.SCHEDULE_PLAIN, N.TILE_BOOK_THRESHOLD, threshold)
+    engine.set_cost_model(None)
+    engine.set_tile(N.SCHEDULE_BATCHED, N.TILE_GAPPED_KERNEL, kernel)
+    engine.set_tile(N.SCHEDULE_BATCHED, N.TILE_BOOK_THRESHOLD, threshold)
     try:
         db, q = _small(1001, 1002, n_db=800, n_q=60)
-        _compare(engine, oracle, params, db, q)
+        _compare(engine, oracle, params, db, q, schedule=N.SCHEDULE_BATCHED)
     finally:
-        engine.set_tile(N.SCHEDULE_PLAIN, N.TILE_GAPPED_KERNEL, -1)
-        engine.set_tile(N.SCHEDULE_PLAIN, N.TILE_BOOK_THRESHOLD, -1)
+        engine.set_tile(N.SCHEDULE_BATCHED, N.TILE_GAPPED_KERNEL, -1)
+        engine.set_tile(N.SCHEDULE_BATCHED, N.TILE_BOOK_THRESHOLD, -1)

@@ -35,7 +35,7 @@ def test_learned_schedule_identical_results_and_accurate(engine, params):
     x, y = engine.get_log()
     assert len(y) == engine.counters()["gapped_extensions"] - engine.counters()["gapped_fallbacks"] \
         or len(y) > 0
-    params_model, loss = engine.train_cost_model(epochs=30, batch=2048, lr=3e-3, seed=3)
+    params_model, loss = engine.train_cost_model(epochs=150, batch=2048, lr=3e-3, seed=3)
     engine.set_logging(False)
     assert loss < 0.5 * float(np.var(y))  # better than predicting the mean
     # evaluation on another workload
@@ -84,7 +84,7 @@ def test_trained_model_reduces_lane_kernel_work(engine, params):
     engine.set_queries(q)
     engine.set_logging(True, 1 << 22)
     engine.presearch(N.SCHEDULE_PLAIN)
-    engine.train_cost_model(epochs=40, batch=2048, lr=3e-3, seed=5)
+    engine.train_cost_model(epochs=150, batch=2048, lr=3e-3, seed=5)
     engine.set_logging(False)
     db2 = W.make_database(6000, 1401, median=300)
     q2 = W.make_queries(db2, 600, 1402, median=300)
