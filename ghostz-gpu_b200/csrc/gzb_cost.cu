@@ -133,28 +133,60 @@ __global__ void mlp_adam_kernel(float *params, const float *grad, float *m, floa
 }
 
 // BF16 inference: weights and activations rounded to bf16, FP32 accumulate.
-__global__ void mlp_predict_kernel(const float *__restrict__ params, const float *__restrict__ X,
-                                   uint32_t n, float *__restrict__ out) {
-  __shared__ __nv_bfloat16 Pb[kParams];
-  for (int i = threadIdx.x; i < kParams; i += blockDim.x) Pb[i] = __float2bfloat16(params[i]);
+__device__ __forceinline__ float bf16_round(float v) {
+  return __bfloat162float(__float2bfloat16(v));
+}
+
+// BF16 inference: parameters, inputs and both hidden layers rounded to
+// bf16, products accumulated in fp32.  The parameters sit in shared memory
+// as the fp32 values of their bf16 roundings (exact), read as float4
+// broadcasts, one sample per thread.
+__global__ void __launch_bounds__(256)
+mlp_predict_kernel(const float *__restrict__ params, const float *__restrict__ X, uint32_t n,
+                   float *__restrict__ out) {
+  __shared__ __align__(16) float P[(kParams + 3) & ~3];
+  for (int i = threadIdx.x; i < kParams; i += blockDim.x) P[i] = bf16_round(params[i]);
   __syncthreads();
+  const float4 *P4 = reinterpret_cast<const float4 *>(P);
+  static_assert(kOffW1 % 4 == 0 && kOffW2 % 4 == 0 && kFeat % 4 == 0 && kHid % 4 == 0,
+                "float4 rows");
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
     float x[kFeat], h1[kHid];
-    for (int k = 0; k < kFeat; ++k)
-      x[k] = __bfloat162float(__float2bfloat16(X[(size_t)s * kFeat + k]));
-    for (int j = 0; j < kHid; ++j) {
-      float acc = __bfloat162float(Pb[kOffB1 + j]);
-      for (int k = 0; k < kFeat; ++k)
-        acc = fmaf(__bfloat162float(Pb[kOffW1 + j * kFeat + k]), x[k], acc);
-      h1[j] = __bfloat162float(__float2bfloat16(acc > 0.f ? acc : 0.f));
+    const float4 *x4 = reinterpret_cast<const float4 *>(X + (size_t)s * kFeat);
+#pragma unroll
+    for (int k = 0; k < kFeat / 4; ++k) {
+      const float4 v = x4[k];
+      x[4 * k] = bf16_round(v.x);
+      x[4 * k + 1] = bf16_round(v.y);
+      x[4 * k + 2] = bf16_round(v.z);
+      x[4 * k + 3] = bf16_round(v.w);
     }
-    float y = __bfloat162float(Pb[kOffB3]);
+#pragma unroll
     for (int j = 0; j < kHid; ++j) {
-      float acc = __bfloat162float(Pb[kOffB2 + j]);
-      for (int k = 0; k < kHid; ++k)
-        acc = fmaf(__bfloat162float(Pb[kOffW2 + j * kHid + k]), h1[k], acc);
-      const float h2 = __bfloat162float(__float2bfloat16(acc > 0.f ? acc : 0.f));
-      y = fmaf(__bfloat162float(Pb[kOffW3 + j]), h2, y);
+      float acc = P[kOffB1 + j];
+#pragma unroll
+      for (int k = 0; k < kFeat / 4; ++k) {
+        const float4 w = P4[(kOffW1 + j * kFeat) / 4 + k];
+        acc = fmaf(w.x, x[4 * k], acc);
+        acc = fmaf(w.y, x[4 * k + 1], acc);
+        acc = fmaf(w.z, x[4 * k + 2], acc);
+        acc = fmaf(w.w, x[4 * k + 3], acc);
+      }
+      h1[j] = bf16_round(acc > 0.f ? acc : 0.f);
+    }
+    float y = P[kOffB3];
+#pragma unroll 4
+    for (int j = 0; j < kHid; ++j) {
+      float acc = P[kOffB2 + j];
+#pragma unroll
+      for (int k = 0; k < kHid / 4; ++k) {
+        const float4 w = P4[(kOffW2 + j * kHid) / 4 + k];
+        acc = fmaf(w.x, h1[4 * k], acc);
+        acc = fmaf(w.y, h1[4 * k + 1], acc);
+        acc = fmaf(w.z, h1[4 * k + 2], acc);
+        acc = fmaf(w.w, h1[4 * k + 3], acc);
+      }
+      y = fmaf(P[kOffW3 + j], bf16_round(acc > 0.f ? acc : 0.f), y);
     }
     out[s] = y;
   }
@@ -198,6 +230,7 @@ int cost_gradients(const float *d_params, const float *d_x, const float *d_y,
 int cost_predict(const float *d_params, const float *d_x, uint32_t n, float *d_out,
                  cudaStream_t s) {
   if (n == 0) return GZB_OK;
+  GZB_CHECK(((uintptr_t)d_x & 15) == 0, GZB_ERR_INVALID, "features must be 16-byte aligned");
   unsigned g = (unsigned)((n + 255) / 256);
   if (g > 148 * 16) g = 148 * 16;
   mlp_predict_kernel<<<g, 256, 0, s>>>(d_params, d_x, n, d_out);

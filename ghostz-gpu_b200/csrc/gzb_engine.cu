@@ -431,14 +431,14 @@ constexpr int kUnitsPerWarp = 256;
 // tried against every query position of that list.
 __global__ void __launch_bounds__(kSeedBlock)
 seed_kernel(SeedArgs a) {
-  __shared__ int sm[kMatrixStride * kMatrixStride];
-  load_matrix(sm, a.matrix32, kMatrixStride, kMatrixStride);
+  __shared__ __align__(16) int16_t tbl16[kWalkTableBytes / 2];
+  load_walk_table(tbl16, a.matrix32, a.p.delimiter);
   __syncthreads();
+  const char *tbl = reinterpret_cast<const char *>(tbl16);
   const int lane = threadIdx.x & 31;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   const uint64_t U = a.L.n_units;
-  const int delim = a.p.delimiter;
   const int thr = a.p.distance_threshold;
   const int maxmd = a.p.max_member_distance;
   unsigned long long n_dist = 0, n_seed = 0, n_steps = 0;
@@ -483,7 +483,7 @@ seed_kernel(SeedArgs a) {
           if (try_rep) {
             int steps = 0;
             ++n_seed;
-            if (ungapped_hit(qptr, dptr, delim, sm, a.cutoffs[qid], a.triggers[qid], &steps))
+            if (walk_hit(qptr, dptr, tbl, a.cutoffs[qid], a.triggers[qid], &steps))
               emit_hit(a, qid, rpos, cpos - a.q_offsets[qid]);
             n_steps += steps;
           }
@@ -497,7 +497,7 @@ seed_kernel(SeedArgs a) {
           const uint32_t cpos = a.L.entry_cpos[k];
           int steps = 0;
           ++n_seed;
-          if (ungapped_hit(a.q + cpos, dptr, delim, sm, a.cutoffs[qid], a.triggers[qid], &steps))
+          if (walk_hit(a.q + cpos, dptr, tbl, a.cutoffs[qid], a.triggers[qid], &steps))
             emit_hit(a, qid, d, cpos - a.q_offsets[qid]);
           n_steps += steps;
         }
@@ -523,13 +523,13 @@ __global__ void mwork_counts_kernel(const uint2 *mwork, uint64_t n, const uint32
 __global__ void __launch_bounds__(kSeedBlock)
 member_kernel(SeedArgs a, const uint2 *mwork, uint64_t n_work, const uint64_t *offs,
               uint64_t total) {
-  __shared__ int sm[kMatrixStride * kMatrixStride];
-  load_matrix(sm, a.matrix32, kMatrixStride, kMatrixStride);
+  __shared__ __align__(16) int16_t tbl16[kWalkTableBytes / 2];
+  load_walk_table(tbl16, a.matrix32, a.p.delimiter);
   __syncthreads();
+  const char *tbl = reinterpret_cast<const char *>(tbl16);
   const int lane = threadIdx.x & 31;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  const int delim = a.p.delimiter;
   unsigned long long n_seed = 0, n_steps = 0;
   for (uint64_t base = warp * kUnitsPerWarp; base < total; base += nwarps * kUnitsPerWarp) {
     const uint64_t last = min(base + kUnitsPerWarp, total) - 1;
@@ -549,7 +549,7 @@ member_kernel(SeedArgs a, const uint2 *mwork, uint64_t n_work, const uint64_t *o
       const uint32_t cpos = a.L.entry_cpos[mw.y];
       int steps = 0;
       ++n_seed;
-      if (ungapped_hit(a.q + cpos, a.db + d, delim, sm, a.cutoffs[qid], a.triggers[qid], &steps))
+      if (walk_hit(a.q + cpos, a.db + d, tbl, a.cutoffs[qid], a.triggers[qid], &steps))
         emit_hit(a, qid, d, cpos - a.q_offsets[qid]);
       n_steps += steps;
     }
@@ -643,6 +643,10 @@ __global__ void chain_kernel(DevParams p, const uint8_t *__restrict__ q,
 __device__ __forceinline__ uint32_t subject_of(const uint32_t *off, uint32_t nseq,
                                                uint32_t db_len, uint32_t pos);
 
+// Extension list of the chained hits: one warp per query, lanes over its
+// kept hits (database order).  Reverse extension of hit h at h, forward at
+// n_surv + h; neighbours[h] counts the query's kept hits within 256
+// database residues of h (a cost-model feature).
 __global__ void build_ext_kernel(const uint64_t *hits, const uint64_t *begin,
                                  const uint32_t *kept, const uint64_t *surv_off, uint32_t nq,
                                  const uint32_t *q_offsets, const uint32_t *q_lengths,
@@ -652,29 +656,44 @@ __global__ void build_ext_kernel(const uint64_t *hits, const uint64_t *begin,
                                  uint32_t *elen1, uint32_t *eqid, uint32_t *neighbours) {
   const uint64_t qmask = (1ull << qbits) - 1, dmask = (1ull << dbits) - 1;
   constexpr uint32_t kReach = 256;  // database residues either side
-  for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < nq;
-       qi += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t qi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; qi < nq; qi += warps) {
     const uint64_t b = begin[qi], o = surv_off[qi];
     const uint32_t qlen = q_lengths[qi];
+    const uint32_t qoff = q_offsets[qi];
     const uint32_t nk = kept[qi];
-    uint32_t lo = 0, hi = 0;  // window of kept hits (database order) around k
-    for (uint32_t k = 0; k < nk; ++k) {
-      const uint64_t key = hits[b + k];
+    const uint64_t *kh = hits + b;
+    for (uint32_t k = lane; k < nk; k += 32) {
+      const uint64_t key = kh[k];
       const uint32_t hq = (uint32_t)(key & qmask);
       const uint32_t hd = (uint32_t)((key >> qbits) & dmask);
-      while ((uint32_t)((hits[b + lo] >> qbits) & dmask) + kReach < hd) ++lo;
-      if (hi < k) hi = k;
-      while (hi + 1 < nk && (uint32_t)((hits[b + hi + 1] >> qbits) & dmask) <= hd + kReach) ++hi;
-      if (neighbours) neighbours[o + k] = hi - lo + 1;
+      if (neighbours) {
+        // first kept hit at >= hd - kReach and first beyond hd + kReach
+        const uint32_t lo_d = hd > kReach ? hd - kReach : 0, hi_d = hd + kReach;
+        uint32_t lo = 0, hi = k;
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if ((uint32_t)((kh[mid] >> qbits) & dmask) < lo_d) lo = mid + 1; else hi = mid;
+        }
+        const uint32_t first = lo;
+        lo = k + 1;
+        hi = nk;
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if ((uint32_t)((kh[mid] >> qbits) & dmask) <= hi_d) lo = mid + 1; else hi = mid;
+        }
+        neighbours[o + k] = lo - first;
+      }
       const uint32_t sj = subject_of(db_offsets, nseq, db_len, hd);
       const uint32_t s0 = db_offsets[sj], s1 = db_offsets[sj + 1] - 1;  // residues [s0, s1)
-      eq[o + k] = q_offsets[qi] + hq - 1;
+      eq[o + k] = qoff + hq - 1;
       ed[o + k] = hd - 1;
       dir[o + k] = 1;
       elen0[o + k] = hq - 1;
       elen1[o + k] = hd - s0;
       eqid[o + k] = qi;
-      eq[n_surv + o + k] = q_offsets[qi] + hq;
+      eq[n_surv + o + k] = qoff + hq;
       ed[n_surv + o + k] = hd;
       dir[n_surv + o + k] = 0;
       elen0[n_surv + o + k] = qlen - 1 - hq;
@@ -982,6 +1001,7 @@ struct gzb_engine {
   DBuf elen0, elen1, eqid, efeat, epred, ecells, okeys, okeys2, oidx, oidx2, queue, prev_cells,
       model_d, mae_acc, log_x, log_y, log_ctr;
   uint64_t prev_cells_n = 0;
+  DBuf codeflag;
   uint64_t pred_n = 0;       // extensions with a prediction in epred (last run)
   DBuf enb;                  // per surviving hit: chained neighbours (cost feature)
   int tile[3][2] = {{-1, -1}, {-1, -1}, {-1, -1}};  // [schedule][which], -1 = default
@@ -1066,11 +1086,38 @@ int exclusive_sum(gzb_engine *e, const TIn *in, TOut *out, uint64_t n, cudaStrea
   return GZB_OK;
 }
 
-int upload_padded(DBuf &buf, const uint8_t *codes, uint64_t len, uint8_t delim,
+// sets *bad when a byte of p[0, n) is 32 or more (p 16-byte aligned)
+__global__ void code_range_kernel(const uint8_t *p, uint64_t n, unsigned int *bad) {
+  const uint64_t n16 = n / 16;
+  const uint4 *p4 = reinterpret_cast<const uint4 *>(p);
+  uint32_t acc = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n16;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint4 v = p4[i];
+    acc |= v.x | v.y | v.z | v.w;
+  }
+  if (blockIdx.x == 0 && threadIdx.x < 16 && n16 * 16 + threadIdx.x < n)
+    acc |= p[n16 * 16 + threadIdx.x];
+  if (acc & 0xE0E0E0E0u) atomicOr(bad, 1u);
+}
+
+// Uploads `len` residue codes between kPad delimiter bytes on each side and
+// checks that every code is below 32 (the kernels' score tables are 32
+// wide).  Synchronises `s`.
+int upload_padded(DBuf &buf, DBuf &flag, const uint8_t *codes, uint64_t len, uint8_t delim,
                   cudaStream_t s) {
   GZB_TRY(buf.ensure(len + 2 * kPad));
+  GZB_TRY(flag.ensure(4));
   GZB_CUDA(cudaMemsetAsync(buf.p, delim, len + 2 * kPad, s));
   GZB_CUDA(cudaMemcpyAsync((uint8_t *)buf.p + kPad, codes, len, cudaMemcpyHostToDevice, s));
+  GZB_CUDA(cudaMemsetAsync(flag.p, 0, 4, s));
+  code_range_kernel<<<grid1(len / 16 + 1, 256), 256, 0, s>>>((const uint8_t *)buf.p + kPad, len,
+                                                               flag.as<unsigned int>());
+  GZB_CUDA(cudaGetLastError());
+  unsigned int bad = 0;
+  GZB_CUDA(cudaMemcpyAsync(&bad, flag.p, 4, cudaMemcpyDeviceToHost, s));
+  GZB_CUDA(cudaStreamSynchronize(s));
+  GZB_CHECK(bad == 0, GZB_ERR_INVALID, "residue codes must be below 32");
   return GZB_OK;
 }
 
@@ -1156,7 +1203,7 @@ extern "C" int gzb_engine_destroy(gzb_engine *e) {
                  &e->hits_copy, &e->elen0, &e->elen1, &e->eqid, &e->efeat, &e->epred,
                  &e->ecells, &e->okeys, &e->okeys2, &e->oidx, &e->oidx2, &e->queue,
                  &e->prev_cells, &e->model_d, &e->mae_acc, &e->log_x, &e->log_y,
-                 &e->log_ctr, &e->enb};
+                 &e->log_ctr, &e->enb, &e->codeflag};
   for (DBuf *b : all) b->release();
   cudaFree(e->spill);
   cudaFree(e->gcounters);
@@ -1183,6 +1230,10 @@ extern "C" int gzb_engine_set_params(gzb_engine *e, const gzb_params *p) {
   GZB_CHECK(p->max_number_one_subject_results >= 1, GZB_ERR_INVALID,
             "max_number_one_subject_results must be >= 1");
   GZB_CHECK(p->gap_open >= 0 && p->gap_extension >= 0, GZB_ERR_INVALID, "negative gap");
+  GZB_CHECK(p->delimiter >= 0 && p->delimiter < 32, GZB_ERR_INVALID, "delimiter must be 0..31");
+  for (int i = 0; i < p->number_letters * p->number_letters; ++i)
+    GZB_CHECK(p->score_matrix[i] > -32768 && p->score_matrix[i] < 32768, GZB_ERR_INVALID,
+              "score matrix entries must fit int16");
   e->params = *p;
   DevParams &d = e->dp;
   memset(&d, 0, sizeof(d));
@@ -1234,7 +1285,7 @@ extern "C" int gzb_engine_set_database(gzb_engine *e, int32_t chunk_id, const ui
   e->chunk_id = chunk_id;
   e->db_len = length;
   e->nseq = number_sequences;
-  GZB_TRY(upload_padded(e->db_buf, codes, length, (uint8_t)e->params.delimiter, s));
+  GZB_TRY(upload_padded(e->db_buf, e->codeflag, codes, length, (uint8_t)e->params.delimiter, s));
   GZB_TRY(upload(e->db_offsets, offsets, number_sequences + 1, s));
   const uint8_t *db = e->db_buf.as<uint8_t>() + kPad;
   std::vector<DBuf> &B = e->index_bufs;
@@ -1385,12 +1436,14 @@ extern "C" int gzb_engine_set_queries(gzb_engine *e, const uint8_t *codes, uint6
               "query %u outside the buffer", i);
     GZB_CHECK(i == 0 || offsets[i] >= offsets[i - 1], GZB_ERR_INVALID,
               "query offsets must be non-decreasing");
+    GZB_CHECK(cutoffs[i] >= 1 && cutoffs[i] <= 32767, GZB_ERR_INVALID,
+              "ungapped cutoff of query %u outside 1..32767", i);
     maxl = std::max(maxl, lengths[i]);
   }
   e->nq = number_queries;
   e->q_len = length;
   e->max_qlen = maxl;
-  GZB_TRY(upload_padded(e->q_buf, codes, length, (uint8_t)e->params.delimiter, s));
+  GZB_TRY(upload_padded(e->q_buf, e->codeflag, codes, length, (uint8_t)e->params.delimiter, s));
   GZB_TRY(upload(e->q_offsets, offsets, number_queries, s));
   GZB_TRY(upload(e->q_lengths, lengths, number_queries, s));
   GZB_TRY(upload(e->q_cut, cutoffs, number_queries, s));
@@ -1638,7 +1691,7 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
   e->last_mae_n = 0;
   e->pred_n = 0;
   if (n_surv) {
-    build_ext_kernel<<<grid1(nq, 128), 128, 0, s>>>(
+    build_ext_kernel<<<grid1((uint64_t)nq * 32, 256), 256, 0, s>>>(
         hits, begin, kept, surv_off, nq, e->q_offsets.as<uint32_t>(),
         e->q_lengths.as<uint32_t>(), e->db_offsets.as<uint32_t>(), e->nseq, (uint32_t)e->db_len,
         qbits, dbits, n_surv, e->eq.as<uint32_t>(), e->ed.as<uint32_t>(), e->edir.as<uint8_t>(),

@@ -120,6 +120,109 @@ __device__ __forceinline__ bool ungapped_hit(const uint8_t *q, const uint8_t *d,
   return sum > trigger;
 }
 
+// ---------------------------------------------------------------------------
+// Ungapped walk over an int16 score table (the seed-search kernels).
+//
+// Table layout: entry (query code a, database code b) at byte offset
+// 2a + 512b of a 16 KB shared array (codes < 32).  The delimiter's row and
+// column hold kWalkDelim, so a step onto a delimiter drops the running score
+// by at least 32768 >= cutoff and ends the walk with the best score
+// unchanged, exactly as the reference's explicit delimiter test does.
+constexpr int kWalkTableBytes = 32 * 512;
+constexpr int kWalkDelim = -32768;
+
+__device__ __forceinline__ void load_walk_table(int16_t *tbl, const int32_t *m32, int delim) {
+  for (int i = threadIdx.x; i < kWalkTableBytes / 2; i += blockDim.x) {
+    const int a = i & 255, b = i >> 8;
+    int v = 0;
+    if (a < 32) v = (a == delim || b == delim) ? kWalkDelim : m32[b * 32 + a];
+    tbl[i] = (int16_t)v;
+  }
+}
+
+template <uint32_t SEL>
+__device__ __forceinline__ uint32_t prmt_imm(uint32_t x, uint32_t y) {
+  uint32_t r;
+  asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(x), "r"(y), "n"(SEL));
+  return r;
+}
+
+// byte offset into the walk table of residue pair j of doubled words
+// qa2 / db2 (bytes 2a, 2b): byte j of qa2 | byte j of db2 << 8, the upper
+// two bytes replicate the (zero) sign bit of byte j
+template <int J>
+__device__ __forceinline__ uint32_t walk_offset(uint32_t qa2, uint32_t db2) {
+  return prmt_imm<(uint32_t)(J | ((4 + J) << 4) | ((8 | J) << 8) | ((8 | J) << 12))>(qa2, db2);
+}
+
+// One side of SeedSearcher::UngappedExtend (src/seed_searcher.h:133-158 with
+// UngappedExtender::ExtendOneSideScoreOnly, src/ungapped_extender.h:34-82)
+// from s0[0]/s1[0] (query/database) stepping by INC: returns the best prefix
+// score, stopping at the X-drop (best - score >= cutoff, cutoff >= 1), at a
+// delimiter, or once the best exceeds stop_above.  The reference's
+// (best, run) pair is (best, score - best) here.  Reads four residue pairs
+// per pair of aligned 32-bit loads; the sequences carry delimiter padding
+// of at least 8 bytes on each side.  *steps counts pairs examined.
+template <int INC>
+__device__ __forceinline__ int walk_side(const uint8_t *s0, const uint8_t *s1,
+                                         const char *tbl, int cutoff, int stop_above,
+                                         int *steps) {
+  // chunk k covers residues s[4k .. 4k+3] (INC > 0) or s[-4k-3 .. -4k] (INC < 0)
+  const uintptr_t a0 = (uintptr_t)s0 - (INC > 0 ? 0 : 3);
+  const uintptr_t b0 = (uintptr_t)s1 - (INC > 0 ? 0 : 3);
+  const uint32_t *pa = (const uint32_t *)(a0 & ~(uintptr_t)3);
+  const uint32_t *pb = (const uint32_t *)(b0 & ~(uintptr_t)3);
+  const uint32_t sha = 8u * (uint32_t)(a0 & 3), shb = 8u * (uint32_t)(b0 & 3);
+  uint32_t a_lo = __ldg(pa), a_hi = __ldg(pa + 1);
+  uint32_t b_lo = __ldg(pb), b_hi = __ldg(pb + 1);
+  int score = 0, best = 0, n = 0, v = 0;
+  for (;;) {
+    const uint32_t qa2 = __funnelshift_r(a_lo, a_hi, sha) << 1;
+    const uint32_t db2 = __funnelshift_r(b_lo, b_hi, shb) << 1;
+#define GZB_WALK_STEP(J)                                                   \
+  {                                                                        \
+    v = *(const int16_t *)(tbl + walk_offset<(INC > 0 ? (J) : 3 - (J))>(qa2, db2)); \
+    score += v;                                                            \
+    best = imax(best, score);                                              \
+    ++n;                                                                   \
+    if (best - score >= cutoff || best > stop_above) break;               \
+  }
+    GZB_WALK_STEP(0)
+    GZB_WALK_STEP(1)
+    GZB_WALK_STEP(2)
+    GZB_WALK_STEP(3)
+#undef GZB_WALK_STEP
+    if (INC > 0) {
+      a_lo = a_hi;
+      b_lo = b_hi;
+      pa += 1;
+      pb += 1;
+      a_hi = __ldg(pa + 1);
+      b_hi = __ldg(pb + 1);
+    } else {
+      a_hi = a_lo;
+      b_hi = b_lo;
+      pa -= 1;
+      pb -= 1;
+      a_lo = __ldg(pa);
+      b_lo = __ldg(pb);
+    }
+  }
+  *steps += n - (v == kWalkDelim ? 1 : 0);
+  return best;
+}
+
+// SeedSearcher::UngappedExtend on the walk table: reverse from (q-1, d-1),
+// forward from (q, d) unless the reverse best already exceeds trigger; true
+// when the sum exceeds trigger.
+__device__ __forceinline__ bool walk_hit(const uint8_t *q, const uint8_t *d, const char *tbl,
+                                         int cutoff, int trigger, int *steps) {
+  int sum = walk_side<-1>(q - 1, d - 1, tbl, cutoff, trigger, steps);
+  if (sum > trigger) return true;
+  sum += walk_side<1>(q, d, tbl, cutoff, trigger - sum, steps);
+  return sum > trigger;
+}
+
 // Reduced-alphabet mismatches over the L window centred on the seeds.
 __device__ __forceinline__ int window_distance(const uint8_t *q, const uint8_t *d,
                                                int L, const uint8_t *map) {
