@@ -359,12 +359,20 @@ __global__ void list_fill_kernel(const uint64_t *keys, uint64_t n, const uint32_
   }
 }
 
+// per entry: the packed similarity window and the query's ungapped cutoff
+// and trigger (cutoff << 16 | trigger as int16; both checked to fit)
 __global__ void entry_window_kernel(DevParams p, const uint8_t *__restrict__ q,
-                                    const uint32_t *__restrict__ cpos, uint64_t n,
-                                    uint64_t *out) {
+                                    const uint32_t *__restrict__ cpos,
+                                    const uint32_t *__restrict__ qid,
+                                    const int32_t *__restrict__ cutoffs,
+                                    const int32_t *__restrict__ triggers, uint64_t n,
+                                    uint64_t *out, uint32_t *ct) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x)
+       i += (uint64_t)gridDim.x * blockDim.x) {
     out[i] = pack_window(p, q + cpos[i]);
+    const uint32_t id = qid[i];
+    ct[i] = ((uint32_t)cutoffs[id] << 16) | (uint32_t)(uint16_t)(int16_t)triggers[id];
+  }
 }
 
 __global__ void list_lookup_kernel(DevLists L, DevIndex X, int clustering,
@@ -483,7 +491,8 @@ seed_kernel(SeedArgs a) {
           if (try_rep) {
             int steps = 0;
             ++n_seed;
-            if (walk_hit(qptr, dptr, tbl, a.cutoffs[qid], a.triggers[qid], &steps))
+            const uint32_t ct = a.L.entry_ct[k];
+            if (walk_hit(qptr, dptr, tbl, (int)(ct >> 16), (int)(int16_t)(ct & 0xffffu), &steps))
               emit_hit(a, qid, rpos, cpos - a.q_offsets[qid]);
             n_steps += steps;
           }
@@ -497,7 +506,9 @@ seed_kernel(SeedArgs a) {
           const uint32_t cpos = a.L.entry_cpos[k];
           int steps = 0;
           ++n_seed;
-          if (walk_hit(a.q + cpos, dptr, tbl, a.cutoffs[qid], a.triggers[qid], &steps))
+          const uint32_t ct = a.L.entry_ct[k];
+          if (walk_hit(a.q + cpos, dptr, tbl, (int)(ct >> 16), (int)(int16_t)(ct & 0xffffu),
+                       &steps))
             emit_hit(a, qid, d, cpos - a.q_offsets[qid]);
           n_steps += steps;
         }
@@ -510,19 +521,14 @@ seed_kernel(SeedArgs a) {
   add_counter(&a.ctr[2], n_steps);
 }
 
-__global__ void mwork_counts_kernel(const uint2 *mwork, uint64_t n, const uint32_t *member_offsets,
-                                    uint64_t *counts) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t cid = mwork[i].x;
-    counts[i] = member_offsets[cid + 1] - member_offsets[cid];
-  }
-}
-
-// Members of a representative's cluster against one passing query position.
+// Members of a representative's cluster against one passing query position
+// (one work item = (cluster id, list entry)).  Each warp loads 32 items
+// together, scans their member counts, and deals the (item, member) seeds
+// to its lanes 32 at a time: a lane finds its item with a five-step shuffle
+// search over the scan, so a seed costs one load (the member's position)
+// besides its walk.
 __global__ void __launch_bounds__(kSeedBlock)
-member_kernel(SeedArgs a, const uint2 *mwork, uint64_t n_work, const uint64_t *offs,
-              uint64_t total) {
+member_kernel(SeedArgs a, const uint2 *__restrict__ mwork, uint64_t n_work) {
   __shared__ __align__(16) int16_t tbl16[kWalkTableBytes / 2];
   load_walk_table(tbl16, a.matrix32, a.p.delimiter);
   __syncthreads();
@@ -531,27 +537,46 @@ member_kernel(SeedArgs a, const uint2 *mwork, uint64_t n_work, const uint64_t *o
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long n_seed = 0, n_steps = 0;
-  for (uint64_t base = warp * kUnitsPerWarp; base < total; base += nwarps * kUnitsPerWarp) {
-    const uint64_t last = min(base + kUnitsPerWarp, total) - 1;
-    uint64_t w_lo = 0, w_hi = 0;
-    if (lane == 0) {
-      w_lo = upper_segment(offs, 0, n_work - 1, base);
-      w_hi = upper_segment(offs, w_lo, n_work - 1, last);
+  for (uint64_t i0 = warp * 32; i0 < n_work; i0 += nwarps * 32) {
+    const uint64_t i = i0 + lane;
+    uint32_t mb = 0, cnt = 0, qid = 0, cpos = 0, ct = 0;
+    if (i < n_work) {
+      const uint2 mw = mwork[i];
+      mb = a.X.member_offsets[mw.x];
+      cnt = a.X.member_offsets[mw.x + 1] - mb;
+      qid = a.L.entry_qid[mw.y];
+      cpos = a.L.entry_cpos[mw.y];
+      ct = a.L.entry_ct[mw.y];
     }
-    w_lo = __shfl_sync(0xffffffffu, w_lo, 0);
-    w_hi = __shfl_sync(0xffffffffu, w_hi, 0);
-    for (uint64_t u = base + lane; u <= last; u += 32) {
-      const uint64_t w = upper_segment(offs, w_lo, w_hi, u);
-      const uint2 mw = mwork[w];
-      const uint32_t m = a.X.member_offsets[mw.x] + (uint32_t)(u - offs[w]);
-      const uint32_t d = a.X.member_positions[m];
-      const uint32_t qid = a.L.entry_qid[mw.y];
-      const uint32_t cpos = a.L.entry_cpos[mw.y];
-      int steps = 0;
-      ++n_seed;
-      if (walk_hit(a.q + cpos, a.db + d, tbl, a.cutoffs[qid], a.triggers[qid], &steps))
-        emit_hit(a, qid, d, cpos - a.q_offsets[qid]);
-      n_steps += steps;
+    uint32_t incl = cnt;  // inclusive scan of member counts
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += t;
+    }
+    const uint32_t excl = incl - cnt;
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    for (uint32_t base = 0; base < total; base += 32) {
+      const uint32_t p = base + lane;
+      // owner: the last lane whose exclusive offset is <= p (it has p < its
+      // inclusive offset, since every later lane starts beyond p)
+      int o = 0;
+      for (int step = 16; step >= 1; step >>= 1) {
+        const uint32_t e = __shfl_sync(0xffffffffu, excl, o + step);
+        if (o + step < 32 && e <= p) o += step;
+      }
+      const uint32_t m = __shfl_sync(0xffffffffu, mb, o) + (p - __shfl_sync(0xffffffffu, excl, o));
+      const uint32_t sq = __shfl_sync(0xffffffffu, qid, o);
+      const uint32_t sc = __shfl_sync(0xffffffffu, cpos, o);
+      const uint32_t sct = __shfl_sync(0xffffffffu, ct, o);
+      if (p < total) {
+        const uint32_t d = a.X.member_positions[m];
+        int steps = 0;
+        ++n_seed;
+        if (walk_hit(a.q + sc, a.db + d, tbl, (int)(sct >> 16), (int)(int16_t)(sct & 0xffffu),
+                     &steps))
+          emit_hit(a, sq, d, sc - a.q_offsets[sq]);
+        n_steps += steps;
+      }
     }
   }
   __syncwarp();
@@ -994,7 +1019,7 @@ struct gzb_engine {
   // results
   DBuf results, counts;
   // scratch
-  DBuf tmp, hits, hits_alt, mwork, mcount, moffs, begin, kept, surv_off, slots, eq, ed, edir,
+  DBuf tmp, hits, hits_alt, mwork, begin, kept, surv_off, slots, eq, ed, edir,
       escore, merge_scratch, heap, ctr, misc, hits_copy;
   int qbits = 1, dbits = 1;
   // schedule of the gapped stage
@@ -1197,7 +1222,7 @@ extern "C" int gzb_engine_destroy(gzb_engine *e) {
   for (auto &b : e->list_bufs) b.release();
   DBuf *all[] = {&e->matrix32, &e->db_buf, &e->db_offsets, &e->q_buf, &e->q_offsets,
                  &e->q_lengths, &e->q_cut, &e->q_trig, &e->results, &e->counts,
-                 &e->tmp, &e->hits, &e->hits_alt, &e->mwork, &e->mcount, &e->moffs,
+                 &e->tmp, &e->hits, &e->hits_alt, &e->mwork,
                  &e->begin, &e->kept, &e->surv_off, &e->slots, &e->eq, &e->ed, &e->edir,
                  &e->escore, &e->merge_scratch, &e->heap, &e->ctr, &e->misc,
                  &e->hits_copy, &e->elen0, &e->elen1, &e->eqid, &e->efeat, &e->epred,
@@ -1438,6 +1463,8 @@ extern "C" int gzb_engine_set_queries(gzb_engine *e, const uint8_t *codes, uint6
               "query offsets must be non-decreasing");
     GZB_CHECK(cutoffs[i] >= 1 && cutoffs[i] <= 32767, GZB_ERR_INVALID,
               "ungapped cutoff of query %u outside 1..32767", i);
+    GZB_CHECK(triggers[i] >= -32768 && triggers[i] <= 32767, GZB_ERR_INVALID,
+              "gapped trigger of query %u outside int16", i);
     maxl = std::max(maxl, lengths[i]);
   }
   e->nq = number_queries;
@@ -1501,13 +1528,16 @@ extern "C" int gzb_engine_set_queries(gzb_engine *e, const uint8_t *codes, uint6
   L.n_entries = n;
   GZB_TRY(B[16].ensure(8 * (n + 1)));
   L.entry_window = B[16].as<uint64_t>();
+  GZB_TRY(B[17].ensure(4 * (n + 1)));
+  L.entry_ct = B[17].as<uint32_t>();
   if (n) {
     list_fill_kernel<<<grid1(n + nl + 1, 256), 256, 0, s>>>(
         sorted, n, starts.as<uint32_t>(), nl, e->q_offsets.as<uint32_t>(), number_queries,
         L.hash, L.offsets, L.nchk, L.entry_qid, L.entry_cpos);
     GZB_CUDA(cudaGetLastError());
-    entry_window_kernel<<<grid1(n, 256), 256, 0, s>>>(e->dp, e->q_buf.as<uint8_t>() + kPad,
-                                                       L.entry_cpos, n, L.entry_window);
+    entry_window_kernel<<<grid1(n, 256), 256, 0, s>>>(
+        e->dp, e->q_buf.as<uint8_t>() + kPad, L.entry_cpos, L.entry_qid,
+        e->q_cut.as<int32_t>(), e->q_trig.as<int32_t>(), n, L.entry_window, L.entry_ct);
     GZB_CUDA(cudaGetLastError());
   } else {
     GZB_CUDA(cudaMemsetAsync(L.offsets, 0, 8, s));
@@ -1603,25 +1633,10 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
       continue;
     }
     if (n_mwork) {
-      GZB_TRY(e->mcount.ensure(8 * (n_mwork + 1)));
-      GZB_TRY(e->moffs.ensure(8 * (n_mwork + 1)));
-      mwork_counts_kernel<<<grid1(n_mwork, 256), 256, 0, s>>>(
-          a.mwork, n_mwork, X.member_offsets, e->mcount.as<uint64_t>());
+      member_kernel<<<grid1((n_mwork + 31) / 32 * 32, kSeedBlock, 148 * 16), kSeedBlock, 0, s>>>(
+          a, a.mwork, n_mwork);
       GZB_CUDA(cudaGetLastError());
-    ++launches;
-      GZB_CUDA(cudaMemsetAsync(e->mcount.as<uint64_t>() + n_mwork, 0, 8, s));
-      GZB_TRY(exclusive_sum(e, e->mcount.as<uint64_t>(), e->moffs.as<uint64_t>(), n_mwork + 1, s));
-      uint64_t total = 0;
-      GZB_CUDA(cudaMemcpyAsync(&total, e->moffs.as<uint64_t>() + n_mwork, 8,
-                               cudaMemcpyDeviceToHost, s));
-      GZB_CUDA(cudaStreamSynchronize(s));
-      if (total) {
-        const uint64_t warps = (total + kUnitsPerWarp - 1) / kUnitsPerWarp;
-        member_kernel<<<grid1(warps * 32, kSeedBlock, 148 * 16), kSeedBlock, 0, s>>>(
-            a, a.mwork, n_mwork, e->moffs.as<uint64_t>(), total);
-        GZB_CUDA(cudaGetLastError());
-    ++launches;
-      }
+      ++launches;
       GZB_CUDA(cudaMemcpyAsync(hctr, c, 64, cudaMemcpyDeviceToHost, s));
       GZB_CUDA(cudaStreamSynchronize(s));
     }

@@ -70,6 +70,7 @@ struct DevLists {
   uint32_t *entry_qid = nullptr;   // per entry: query id
   uint32_t *entry_cpos = nullptr;  // concatenated position
   uint64_t *entry_window = nullptr;  // packed similarity window (check entries)
+  uint32_t *entry_ct = nullptr;      // the entry's query cutoff << 16 | (uint16) trigger
   uint64_t n_lists = 0, n_entries = 0, n_units = 0;
 };
 
