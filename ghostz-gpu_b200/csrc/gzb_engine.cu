@@ -602,9 +602,13 @@ __global__ void hit_segments_kernel(const uint64_t *hits, uint64_t n, uint32_t n
   }
 }
 
-// Chain filter, one thread per query, over its hits in (database, query)
-// position order; survivors are compacted to the front of the query's
-// segment.  slots: per-query scratch of query_length (diagonal, end) pairs.
+// Chain filter (ChainFilter::Filter, src/chain_filter.cpp), one warp per
+// query, over its hits in (database, query) position order; survivors are
+// compacted to the front of the query's segment.  Hit i is handled by the
+// lane that owns its diagonal slot (slot % 32), so each slot sees its hits
+// in order; the warp steps through the hits together and the owner's
+// decision is shared by ballot.  slots: per-query scratch of query_length
+// (diagonal, end) pairs.
 __global__ void chain_kernel(DevParams p, const uint8_t *__restrict__ q,
                              const uint8_t *__restrict__ db, const uint32_t *q_offsets,
                              const uint32_t *q_lengths, const int32_t *cutoffs,
@@ -613,17 +617,19 @@ __global__ void chain_kernel(DevParams p, const uint8_t *__restrict__ q,
                              uint32_t *kept_count) {
   const uint64_t qmask = (1ull << qbits) - 1, dmask = (1ull << dbits) - 1;
   const int n = kMatrixStride;
-  for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < nq;
-       qi += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t qi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; qi < nq; qi += warps) {
     const uint64_t b = begin[qi], e = begin[qi + 1];
     if (b == e) {
-      kept_count[qi] = 0;
+      if (lane == 0) kept_count[qi] = 0;
       continue;
     }
     const uint8_t *qs = q + q_offsets[qi];
     const uint32_t qlen = q_lengths[qi];
     uint2 *slot = slots + q_offsets[qi] + qi;  // qlen entries of this query
-    for (uint32_t i = 0; i < qlen; ++i) slot[i] = make_uint2(0, 0);
+    for (uint32_t i = lane; i < qlen; i += 32) slot[i] = make_uint2(0, 0);
+    __syncwarp();
     const int cutoff = cutoffs[qi];
     uint64_t w = b;
     for (uint64_t i = b; i < e; ++i) {
@@ -631,35 +637,43 @@ __global__ void chain_kernel(DevParams p, const uint8_t *__restrict__ q,
       const uint32_t hq = (uint32_t)(key & qmask);
       const uint32_t hd = (uint32_t)((key >> qbits) & dmask);
       const uint32_t diagonal = qlen - 1 + hd - hq;
-      uint2 &sl = slot[diagonal % qlen];  // x = diagonal, y = query end
-      bool connected = false;
-      if (sl.x == diagonal) {
-        if (hq <= sl.y + 1) {
-          connected = true;
-        } else {
-          // back-extension toward the chain end (ChainFilter::Connected)
-          uint32_t qo = hq, dof = hd;
-          int score = 0, best = 0, c = -cutoff;
-          do {
-            --dof;
-            --qo;
-            if (db[dof] == p.delimiter || qs[qo] == p.delimiter || qo <= sl.y) break;
-            score += matrix32[db[dof] * n + qs[qo]];
-            if (best < score) {
-              best = score;
-              c = best - cutoff;
-            }
-          } while (score > c);
-          connected = qo <= sl.y;
+      const uint32_t si = diagonal % qlen;
+      bool keep = false;
+      if ((si & 31) == (uint32_t)lane) {
+        uint2 sl = slot[si];  // x = diagonal, y = query end
+        bool connected = false;
+        if (sl.x == diagonal) {
+          if (hq <= sl.y + 1) {
+            connected = true;
+          } else {
+            // back-extension toward the chain end (ChainFilter::Connected)
+            uint32_t qo = hq, dof = hd;
+            int score = 0, best = 0, c = -cutoff;
+            do {
+              --dof;
+              --qo;
+              if (db[dof] == p.delimiter || qs[qo] == p.delimiter || qo <= sl.y) break;
+              score += matrix32[db[dof] * n + qs[qo]];
+              if (best < score) {
+                best = score;
+                c = best - cutoff;
+              }
+            } while (score > c);
+            connected = qo <= sl.y;
+          }
         }
+        sl.y = hq;
+        if (!connected) sl.x = diagonal;
+        slot[si] = sl;
+        keep = !connected;
       }
-      sl.y = hq;
-      if (!connected) {
-        sl.x = diagonal;
-        hits[w++] = key;
+      if (__ballot_sync(0xffffffffu, keep)) {
+        if (keep) hits[w] = key;
+        ++w;
       }
     }
-    kept_count[qi] = (uint32_t)(w - b);
+    if (lane == 0) kept_count[qi] = (uint32_t)(w - b);
+    __syncwarp();
   }
 }
 
@@ -847,40 +861,40 @@ __device__ __forceinline__ uint32_t subject_of(const uint32_t *off, uint32_t nse
   return lo == 0 ? 0xFFFFFFFFu : lo - 1;
 }
 
-// heap of indices ordered so that the root is the first in sorted order
-__device__ void sift_down(const gzb_result *r, uint32_t *h, uint32_t n, uint32_t i) {
-  for (;;) {
-    uint32_t l = 2 * i + 1, best = i;
-    if (l < n && before(r, h[l], h[best])) best = l;
-    if (l + 1 < n && before(r, h[l + 1], h[best])) best = l + 1;
-    if (best == i) return;
-    const uint32_t t = h[i];
-    h[i] = h[best];
-    h[best] = t;
-    i = best;
-  }
+
+// index of the first (in `before` order) untaken candidate among
+// i = lane, lane + 32, ... (< k), or UINT32_MAX
+__device__ __forceinline__ uint32_t lane_first(const gzb_result *added, const uint8_t *taken,
+                                               uint32_t k, int lane) {
+  uint32_t best = 0xFFFFFFFFu;
+  for (uint32_t i = lane; i < k; i += 32)
+    if (!taken[i] && (best == 0xFFFFFFFFu || before(added, i, best))) best = i;
+  return best;
 }
 
-// One thread per query: results of its survivors merged into its running
-// top-b list exactly as AlignerCommon::AddResults orders and prunes them.
+// One warp per query: the lanes build the candidates of the query's
+// survivors and find, 32-wide, the next one in AlignerCommon::AddResults
+// order; lane 0 merges it with the query's running top-b list, exactly as
+// AddResults orders and prunes (src/aligner_common.cpp).
 __global__ void merge_kernel(uint32_t nq, const uint64_t *hits, const uint64_t *begin,
                              const uint32_t *kept, const uint64_t *surv_off,
                              uint64_t n_surv, const uint32_t *eq, const uint32_t *ed,
                              const int32_t *escore, const uint32_t *q_offsets, int qbits,
                              int dbits, const uint32_t *db_offsets, uint32_t nseq,
                              uint32_t db_len, int32_t chunk_id, int max_results,
-                             int max_one_subject, gzb_result *scratch, uint32_t *heap,
+                             int max_one_subject, gzb_result *scratch, uint8_t *taken_all,
                              gzb_result *results, uint32_t *counts) {
   const uint64_t qmask = (1ull << qbits) - 1, dmask = (1ull << dbits) - 1;
-  for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < nq;
-       qi += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t qi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; qi < nq; qi += warps) {
     const uint32_t k = kept[qi];
     if (k == 0) continue;
     const uint64_t b = begin[qi], o = surv_off[qi];
     const uint32_t qoff = q_offsets[qi];
     gzb_result *added = scratch + o;
-    uint32_t *h = heap + o;
-    for (uint32_t i = 0; i < k; ++i) {
+    uint8_t *taken = taken_all + o;
+    for (uint32_t i = lane; i < k; i += 32) {
       const uint64_t key = hits[b + i];
       gzb_result r;
       r.chunk_id = chunk_id;
@@ -893,98 +907,124 @@ __global__ void merge_kernel(uint32_t nq, const uint64_t *hits, const uint64_t *
       r.end_q = eq[n_surv + o + i] - qoff;
       r.end_d = ed[n_surv + o + i];
       added[i] = r;
-      h[i] = i;
+      taken[i] = 0;
     }
-    for (int i = (int)k / 2 - 1; i >= 0; --i) sift_down(added, h, k, (uint32_t)i);
-    uint32_t heap_n = k;
-    // previous list of this query (earlier chunks)
+    __syncwarp();
+    uint32_t mine = lane_first(added, taken, k, lane);
+    // lane 0's merge state: previous list of this query (earlier chunks)
     gzb_result *prev = results + (uint64_t)qi * max_results;
     const uint32_t n_prev = counts[qi];
     gzb_result old[32];
     const uint32_t n_old = n_prev < 32 ? n_prev : 32;
-    for (uint32_t i = 0; i < n_old; ++i) old[i] = prev[i];
-    uint32_t ri = 0, n_out = 0;
+    if (lane == 0)
+      for (uint32_t i = 0; i < n_old; ++i) old[i] = prev[i];
+    uint32_t ri = 0, n_out = 0, left = k;
     // per-subject start lists of this chunk (subject, size, entries)
     uint32_t subj[32];
     uint32_t subj_n[32];
     uint32_t sp_pos[32][4];
     uint32_t sp_id[32][4];
     uint32_t n_subj = 0;
-    while ((int)n_out < max_results && (heap_n > 0 || ri < n_old)) {
-      gzb_result a;
-      bool take_added;
-      if (heap_n == 0)
-        take_added = false;
-      else if (ri == n_old)
-        take_added = true;
-      else
-        take_added = alignment_comp(old[ri], added[h[0]]) < 0;
-      if (take_added) {
-        a = added[h[0]];
-        a.subject_id = (int32_t)subject_of(db_offsets, nseq, db_len, a.start_d);
-        h[0] = h[--heap_n];
-        sift_down(added, h, heap_n, 0);
-      } else {
-        a = old[ri++];
+    for (;;) {
+      // first untaken candidate of the warp
+      uint32_t g = mine;
+      for (int d = 16; d >= 1; d >>= 1) {
+        const uint32_t other = __shfl_xor_sync(0xffffffffu, g, d);
+        if (other != 0xFFFFFFFFu && (g == 0xFFFFFFFFu || before(added, other, g))) g = other;
       }
-      if (a.chunk_id == chunk_id) {
-        uint32_t si = 0;
-        while (si < n_subj && subj[si] != (uint32_t)a.subject_id) ++si;
-        if (si == n_subj) {
-          if (n_subj == 32) continue;  // cannot exceed max_results subjects
-          subj[si] = (uint32_t)a.subject_id;
-          subj_n[si] = 0;
-          ++n_subj;
+      int popped = -1, cont = 0;
+      if (lane == 0) {
+        if ((int)n_out < max_results && (left > 0 || ri < n_old)) {
+          cont = 1;
+          gzb_result a;
+          bool take_added;
+          if (left == 0)
+            take_added = false;
+          else if (ri == n_old)
+            take_added = true;
+          else
+            take_added = alignment_comp(old[ri], added[g]) < 0;
+          if (take_added) {
+            a = added[g];
+            a.subject_id = (int32_t)subject_of(db_offsets, nseq, db_len, a.start_d);
+            popped = (int)g;
+            --left;
+          } else {
+            a = old[ri++];
+          }
+          bool keep = true;
+          if (a.chunk_id == chunk_id) {
+            keep = false;
+            uint32_t si = 0;
+            while (si < n_subj && subj[si] != (uint32_t)a.subject_id) ++si;
+            bool room = true;
+            if (si == n_subj) {
+              if (n_subj == 32) {
+                room = false;  // cannot exceed max_results subjects
+              } else {
+                subj[si] = (uint32_t)a.subject_id;
+                subj_n[si] = 0;
+                ++n_subj;
+              }
+            }
+            const uint32_t cnt = room ? subj_n[si] : 0;
+            if (room && (int)cnt < max_one_subject && cnt < 4) {
+              // std::lower_bound on .position, step for step
+              uint32_t first = 0, len = cnt;
+              while (len > 0) {
+                const uint32_t half = len / 2, mid = first + half;
+                if (sp_pos[si][mid] < a.start_d) {
+                  first = mid + 1;
+                  len = len - half - 1;
+                } else {
+                  len = half;
+                }
+              }
+              const uint32_t ins = first;
+              uint32_t it = first;
+              len = cnt - first;
+              uint32_t f2 = first;
+              while (len > 0) {
+                const uint32_t half = len / 2, mid = f2 + half;
+                if (sp_pos[si][mid] < a.end_d) {
+                  f2 = mid + 1;
+                  len = len - half - 1;
+                } else {
+                  len = half;
+                }
+              }
+              bool ok = true;
+              for (; it != f2; ++it) {
+                if (is_contained(prev[sp_id[si][it]], a)) {
+                  ok = false;
+                  break;
+                }
+              }
+              if (ok) {
+                for (uint32_t t = cnt; t > ins; --t) {
+                  sp_pos[si][t] = sp_pos[si][t - 1];
+                  sp_id[si][t] = sp_id[si][t - 1];
+                }
+                sp_pos[si][ins] = a.start_q;
+                sp_id[si][ins] = n_out;
+                subj_n[si] = cnt + 1;
+                keep = true;
+              }
+            }
+          }
+          if (keep) prev[n_out++] = a;
         }
-        const uint32_t cnt = subj_n[si];
-        if ((int)cnt < max_one_subject && cnt < 4) {
-          // std::lower_bound on .position, step for step
-          uint32_t first = 0, len = cnt;
-          while (len > 0) {
-            const uint32_t half = len / 2, mid = first + half;
-            if (sp_pos[si][mid] < a.start_d) {
-              first = mid + 1;
-              len = len - half - 1;
-            } else {
-              len = half;
-            }
-          }
-          const uint32_t ins = first;
-          uint32_t it = first;
-          len = cnt - first;
-          uint32_t f2 = first;
-          while (len > 0) {
-            const uint32_t half = len / 2, mid = f2 + half;
-            if (sp_pos[si][mid] < a.end_d) {
-              f2 = mid + 1;
-              len = len - half - 1;
-            } else {
-              len = half;
-            }
-          }
-          bool ok = true;
-          for (; it != f2; ++it) {
-            if (is_contained(prev[sp_id[si][it]], a)) {
-              ok = false;
-              break;
-            }
-          }
-          if (ok) {
-            for (uint32_t t = cnt; t > ins; --t) {
-              sp_pos[si][t] = sp_pos[si][t - 1];
-              sp_id[si][t] = sp_id[si][t - 1];
-            }
-            sp_pos[si][ins] = a.start_q;
-            sp_id[si][ins] = n_out;
-            subj_n[si] = cnt + 1;
-            prev[n_out++] = a;
-          }
-        }
-      } else {
-        prev[n_out++] = a;
       }
+      cont = __shfl_sync(0xffffffffu, cont, 0);
+      if (!cont) break;
+      popped = __shfl_sync(0xffffffffu, popped, 0);
+      if (popped >= 0 && (uint32_t)popped % 32 == (uint32_t)lane) {
+        taken[popped] = 1;
+        mine = lane_first(added, taken, k, lane);
+      }
+      __syncwarp();
     }
-    counts[qi] = n_out;
+    if (lane == 0) counts[qi] = n_out;
   }
 }
 
@@ -1679,7 +1719,7 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
   hit_segments_kernel<<<grid1(nq + 1, 256), 256, 0, s>>>(hits, n_hits, nq, qbits + dbits, begin);
   GZB_CUDA(cudaGetLastError());
     ++launches;
-  chain_kernel<<<grid1(nq, 64), 64, 0, s>>>(
+  chain_kernel<<<grid1((uint64_t)nq * 32, 128), 128, 0, s>>>(
       e->dp, e->q_buf.as<uint8_t>() + kPad, e->db_buf.as<uint8_t>() + kPad,
       e->q_offsets.as<uint32_t>(), e->q_lengths.as<uint32_t>(), e->q_cut.as<int32_t>(),
       e->matrix32.as<int32_t>(), nq, hits, begin, qbits, dbits, e->slots.as<uint2>(), kept);
@@ -1816,13 +1856,13 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
   // ---- top-b merge
   if (n_surv) {
     GZB_TRY(e->merge_scratch.ensure(sizeof(gzb_result) * (n_surv + 1)));
-    GZB_TRY(e->heap.ensure(4 * (n_surv + 1)));
-    merge_kernel<<<grid1(nq, 64), 64, 0, s>>>(
+    GZB_TRY(e->heap.ensure(n_surv + 1));
+    merge_kernel<<<grid1((uint64_t)nq * 32, 128), 128, 0, s>>>(
         nq, hits, begin, kept, surv_off, n_surv, e->eq.as<uint32_t>(), e->ed.as<uint32_t>(),
         e->escore.as<int32_t>(), e->q_offsets.as<uint32_t>(), qbits, dbits,
         e->db_offsets.as<uint32_t>(), e->nseq, (uint32_t)e->db_len, e->chunk_id,
         e->params.max_number_results, e->params.max_number_one_subject_results,
-        e->merge_scratch.as<gzb_result>(), e->heap.as<uint32_t>(), e->results.as<gzb_result>(),
+        e->merge_scratch.as<gzb_result>(), e->heap.as<uint8_t>(), e->results.as<gzb_result>(),
         e->counts.as<uint32_t>());
     GZB_CUDA(cudaGetLastError());
     ++launches;
