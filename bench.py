@@ -194,7 +194,7 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-KERNEL_NAMES = {0: "flat", 1: "lane", 2: "rows", 3: "static"}
+KERNEL_NAMES = {0: "flat", 1: "lane", 2: "rows", 3: "static", 4: "deal"}
 
 
 def main():
@@ -304,7 +304,8 @@ def main():
             eng.set_tile(sid, N.TILE_GAPPED_KERNEL, N.GAPPED_KERNEL_FLAT)
             thr, thr_ms = eng.autotune(sid, (4, 8, 12, 16, 24), N.TILE_BOOK_THRESHOLD)
             ker, ker_ms = eng.autotune(sid, (N.GAPPED_KERNEL_FLAT, N.GAPPED_KERNEL_LANE,
-                                             N.GAPPED_KERNEL_ROWS), N.TILE_GAPPED_KERNEL)
+                                             N.GAPPED_KERNEL_ROWS, N.GAPPED_KERNEL_DEAL),
+                                       N.TILE_GAPPED_KERNEL)
             tiles = {"gapped_ms_by_book_threshold": thr_ms,
                      "gapped_ms_by_kernel": {KERNEL_NAMES[k]: v for k, v in ker_ms.items()}}
         for w in (N.TILE_GAPPED_KERNEL, N.TILE_BOOK_THRESHOLD):

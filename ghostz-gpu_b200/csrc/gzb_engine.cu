@@ -439,10 +439,10 @@ constexpr int kUnitsPerWarp = 256;
 // tried against every query position of that list.
 __global__ void __launch_bounds__(kSeedBlock)
 seed_kernel(SeedArgs a) {
-  __shared__ __align__(16) int16_t tbl16[kWalkTableBytes / 2];
-  load_walk_table(tbl16, a.matrix32, a.p.delimiter);
+  __shared__ __align__(16) int32_t tbl32[kWalkTableBytes / 4];
+  load_walk_table(tbl32, a.matrix32, a.p.delimiter);
   __syncthreads();
-  const char *tbl = reinterpret_cast<const char *>(tbl16);
+  const char *tbl = reinterpret_cast<const char *>(tbl32);
   const int lane = threadIdx.x & 31;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -529,10 +529,10 @@ seed_kernel(SeedArgs a) {
 // besides its walk.
 __global__ void __launch_bounds__(kSeedBlock)
 member_kernel(SeedArgs a, const uint2 *__restrict__ mwork, uint64_t n_work) {
-  __shared__ __align__(16) int16_t tbl16[kWalkTableBytes / 2];
-  load_walk_table(tbl16, a.matrix32, a.p.delimiter);
+  __shared__ __align__(16) int32_t tbl32[kWalkTableBytes / 4];
+  load_walk_table(tbl32, a.matrix32, a.p.delimiter);
   __syncthreads();
-  const char *tbl = reinterpret_cast<const char *>(tbl16);
+  const char *tbl = reinterpret_cast<const char *>(tbl32);
   const int lane = threadIdx.x & 31;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;

@@ -121,22 +121,24 @@ __device__ __forceinline__ bool ungapped_hit(const uint8_t *q, const uint8_t *d,
 }
 
 // ---------------------------------------------------------------------------
-// Ungapped walk over an int16 score table (the seed-search kernels).
+// Ungapped walk over a bank-swizzled score table (the seed-search kernels).
 //
-// Table layout: entry (query code a, database code b) at byte offset
-// 2a + 512b of a 16 KB shared array (codes < 32).  The delimiter's row and
-// column hold kWalkDelim, so a step onto a delimiter drops the running score
-// by at least 32768 >= cutoff and ends the walk with the best score
-// unchanged, exactly as the reference's explicit delimiter test does.
-constexpr int kWalkTableBytes = 32 * 512;
+// Table layout: the int32 score of (query code a, database code b) sits at
+// word (a ^ b) + 64a of an 8 KB shared array (codes < 32), so its bank is
+// a ^ b: residue pairs that share a query or a database code land in
+// different banks.  The delimiter's row and column hold kWalkDelim, so a
+// step onto a delimiter drops the running score by at least 32768 >= cutoff
+// and ends the walk with the best score unchanged, exactly as the
+// reference's explicit delimiter test does.
+constexpr int kWalkTableBytes = 64 * 32 * 4;
 constexpr int kWalkDelim = -32768;
 
-__device__ __forceinline__ void load_walk_table(int16_t *tbl, const int32_t *m32, int delim) {
-  for (int i = threadIdx.x; i < kWalkTableBytes / 2; i += blockDim.x) {
-    const int a = i & 255, b = i >> 8;
+__device__ __forceinline__ void load_walk_table(int32_t *tbl, const int32_t *m32, int delim) {
+  for (int i = threadIdx.x; i < kWalkTableBytes / 4; i += blockDim.x) {
+    const int a = i >> 6, x = i & 63, b = x ^ a;
     int v = 0;
-    if (a < 32) v = (a == delim || b == delim) ? kWalkDelim : m32[b * 32 + a];
-    tbl[i] = (int16_t)v;
+    if (x < 32) v = (a == delim || b == delim) ? kWalkDelim : m32[b * 32 + a];
+    tbl[i] = v;
   }
 }
 
@@ -147,12 +149,12 @@ __device__ __forceinline__ uint32_t prmt_imm(uint32_t x, uint32_t y) {
   return r;
 }
 
-// byte offset into the walk table of residue pair j of doubled words
-// qa2 / db2 (bytes 2a, 2b): byte j of qa2 | byte j of db2 << 8, the upper
-// two bytes replicate the (zero) sign bit of byte j
+// byte offset into the walk table of residue pair j: x4 holds 4(a ^ b) and
+// qa holds a in byte j; the result is byte j of x4 | byte j of qa << 8, the
+// upper two bytes replicating the (zero) sign bit of byte j of x4
 template <int J>
-__device__ __forceinline__ uint32_t walk_offset(uint32_t qa2, uint32_t db2) {
-  return prmt_imm<(uint32_t)(J | ((4 + J) << 4) | ((8 | J) << 8) | ((8 | J) << 12))>(qa2, db2);
+__device__ __forceinline__ uint32_t walk_offset(uint32_t x4, uint32_t qa) {
+  return prmt_imm<(uint32_t)(J | ((4 + J) << 4) | ((8 | J) << 8) | ((8 | J) << 12))>(x4, qa);
 }
 
 // One side of SeedSearcher::UngappedExtend (src/seed_searcher.h:133-158 with
@@ -177,11 +179,11 @@ __device__ __forceinline__ int walk_side(const uint8_t *s0, const uint8_t *s1,
   uint32_t b_lo = __ldg(pb), b_hi = __ldg(pb + 1);
   int score = 0, best = 0, n = 0, v = 0;
   for (;;) {
-    const uint32_t qa2 = __funnelshift_r(a_lo, a_hi, sha) << 1;
-    const uint32_t db2 = __funnelshift_r(b_lo, b_hi, shb) << 1;
+    const uint32_t qa = __funnelshift_r(a_lo, a_hi, sha);
+    const uint32_t x4 = (qa ^ __funnelshift_r(b_lo, b_hi, shb)) << 2;
 #define GZB_WALK_STEP(J)                                                   \
   {                                                                        \
-    v = *(const int16_t *)(tbl + walk_offset<(INC > 0 ? (J) : 3 - (J))>(qa2, db2)); \
+    v = *(const int32_t *)(tbl + walk_offset<(INC > 0 ? (J) : 3 - (J))>(x4, qa)); \
     score += v;                                                            \
     best = imax(best, score);                                              \
     ++n;                                                                   \
@@ -656,23 +658,42 @@ __device__ __forceinline__ int lane_init(const GappedJob &job, LaneBand &band, L
   x.ovf = false;
   if (q0[0] == delim || d0[0] == delim) return kLaneDone;
   // every value a row keeps lies in [maxs - cutoff - gi, maxs] with maxs >= 0,
-  // so checking maxs once per row is enough when cutoff + gi fits
+  // so checking maxs once per row is enough when cutoff + gi fits; the
+  // values written here lie in [-cutoff - gi, 0]
   x.ovf = job.cutoff + gi > 32767;
   band.at(0) = pack16(0, -gi);
-  x.ovf |= !fits16(-gi);
   int score = -gi;
   int col = 1;
-  int r = q0[0];
+  int r = 0;
+  // query residues q0[0], q0[inc], ... four per aligned word pair
+  const uintptr_t a0 = (uintptr_t)q0 - (inc > 0 ? 0 : 3);
+  const uint32_t *p = (const uint32_t *)(a0 & ~(uintptr_t)3);
+  const uint32_t sh = 8u * (uint32_t)(a0 & 3);
+  uint32_t lo = __ldg(p), hi = __ldg(p + 1);
   for (;;) {
-    if (r == delim || score < -job.cutoff) break;
-    if (col >= kLaneW) return kLaneOverflow;
-    x.ovf |= !fits16(score) || !fits16(score - gi);
-    band.at(col) = pack16(score, score - gi);
-    band.set_residue(col, r);
-    score -= ge;
-    ++col;
-    r = q0[(col - 1) * inc];
+    uint32_t w = __funnelshift_r(lo, hi, sh);
+    if (inc < 0) w = __byte_perm(w, 0, 0x0123);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      r = (int)((w >> (8 * j)) & 0xffu);
+      if (r == delim || score < -job.cutoff) goto init_done;
+      if (col >= kLaneW) return kLaneOverflow;
+      band.at(col) = pack16(score, score - gi);
+      band.set_residue(col, r);
+      score -= ge;
+      ++col;
+    }
+    if (inc > 0) {
+      lo = hi;
+      ++p;
+      hi = __ldg(p + 1);
+    } else {
+      hi = lo;
+      --p;
+      lo = __ldg(p);
+    }
   }
+init_done:
   x.bs = 0;
   if (r != delim) {
     if (col >= kLaneW) return kLaneOverflow;

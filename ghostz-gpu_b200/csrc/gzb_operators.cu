@@ -315,6 +315,77 @@ gapped_rows_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
   if ((threadIdx.x & 31) == 0 && cells) atomicAdd(cells_total, cells);
 }
 
+// Row-step refill with extensions dealt round-robin: lane t of the grid
+// runs extensions order[t], order[t + T], order[t + 2T], ... (T threads),
+// one database row per step like gapped_rows_kernel, and loads the
+// positions of its next extension while the current one runs.
+__global__ void __launch_bounds__(kLaneBlock)
+gapped_deal_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number_letters,
+                   int stride, uint64_t n, const uint32_t *__restrict__ order, int reverse,
+                   const uint8_t *__restrict__ dir, uint32_t *qpos, uint32_t *dpos,
+                   int32_t *scores, uint32_t *spill, uint32_t *spill_count,
+                   unsigned long long *cells_total, uint32_t *cells_out) {
+  __shared__ int sm[kMatrixStride * kMatrixStride];
+  __shared__ uint32_t cells_s[kLaneW * kLaneBlock];
+  __shared__ uint8_t res_s[kLaneW * kLaneBlock];
+  load_matrix(sm, matrix, number_letters, stride);
+  __syncthreads();
+  LaneBand band{cells_s, res_s, kLaneBlock, (int)threadIdx.x};
+  const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  // the next extension of this lane, loaded one extension ahead
+  uint32_t ne = 0, nq = 0, nd = 0;
+  bool nrev = false;
+  auto load_next = [&](uint64_t k) {
+    if (k < n) {
+      ne = order ? order[k] : (uint32_t)k;
+      nq = qpos[ne];
+      nd = dpos[ne];
+      nrev = dir ? dir[ne] != 0 : reverse != 0;
+    }
+  };
+  load_next(i);
+  LaneExt x;
+  uint32_t e = 0, q = 0, d = 0;
+  bool have = false;
+  unsigned long long cells = 0;
+  for (;;) {
+    int st = kLaneRunning;
+    if (have) st = lane_row(job, sm, band, x);
+    while (st != kLaneRunning || (!have && i < n)) {
+      if (have) {  // the extension ended: write it out
+        if (st == kLaneOverflow || x.ovf) {
+          spill[atomicAdd(spill_count, 1u)] = e;
+          if (cells_out) cells_out[e] = 0xFFFFFFFFu;
+        } else {
+          cells += x.cells;
+          qpos[e] = q + (uint32_t)x.mp0;
+          dpos[e] = d + (uint32_t)x.mp1;
+          scores[e] = x.maxs;
+          if (cells_out) cells_out[e] = x.cells;
+        }
+        have = false;
+        i += T;
+      }
+      if (i >= n) break;
+      e = ne;
+      q = nq;
+      d = nd;
+      const bool rev = nrev;
+      load_next(i + T);
+      st = lane_init(job, band, x, job.query + q, job.db + d, rev);
+      have = true;
+    }
+    if (!__any_sync(0xffffffffu, have)) break;
+  }
+  cells += __shfl_down_sync(0xffffffffu, cells, 16);
+  cells += __shfl_down_sync(0xffffffffu, cells, 8);
+  cells += __shfl_down_sync(0xffffffffu, cells, 4);
+  cells += __shfl_down_sync(0xffffffffu, cells, 2);
+  cells += __shfl_down_sync(0xffffffffu, cells, 1);
+  if ((threadIdx.x & 31) == 0 && cells) atomicAdd(cells_total, cells);
+}
+
 // process-wide tile defaults (gzb_set_tile_parameter)
 GappedTile g_tile = {GZB_GAPPED_KERNEL_ROWS, 16};
 
@@ -340,7 +411,12 @@ int launch_gapped_thread(const GappedTile &tile, const GappedJob &job, const int
                          uint32_t *cells_out, cudaStream_t s) {
   GZB_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s));
   uint64_t blocks = 1;
-  if (tile.kernel == GZB_GAPPED_KERNEL_STATIC) {
+  if (tile.kernel == GZB_GAPPED_KERNEL_DEAL) {
+    GZB_TRY(persistent_blocks(gapped_deal_kernel, kLaneBlock, 0, n, &blocks));
+    gapped_deal_kernel<<<(unsigned)blocks, kLaneBlock, 0, s>>>(
+        job, matrix, number_letters, stride, n, order, reverse, dir, qpos, dpos, scores, spill,
+        spill_count, cells_total, cells_out);
+  } else if (tile.kernel == GZB_GAPPED_KERNEL_STATIC) {
     // one launch, extensions dealt to threads round-robin, no work queue
     blocks = (n + kLaneBlock - 1) / kLaneBlock;
     if (blocks > 148 * 40) blocks = 148 * 40;
@@ -835,9 +911,9 @@ extern "C" int gzb_gapped_extender_cells(gzb_gapped_extender *h, uint64_t *cells
 namespace gzb {
 int check_tile_value(int which, int value) {
   if (which == GZB_TILE_GAPPED_KERNEL) {
-    GZB_CHECK(value >= GZB_GAPPED_KERNEL_FLAT && value <= GZB_GAPPED_KERNEL_STATIC,
+    GZB_CHECK(value >= GZB_GAPPED_KERNEL_FLAT && value <= GZB_GAPPED_KERNEL_DEAL,
               GZB_ERR_INVALID,
-              "gapped kernel %d is none of GZB_GAPPED_KERNEL_FLAT/LANE/ROWS/STATIC", value);
+              "gapped kernel %d is none of GZB_GAPPED_KERNEL_FLAT/LANE/ROWS/STATIC/DEAL", value);
     return GZB_OK;
   }
   GZB_CHECK(which == GZB_TILE_BOOK_THRESHOLD, GZB_ERR_INVALID, "unknown tile parameter %d", which);

@@ -299,6 +299,7 @@ GAPPED_KERNEL_FLAT = 0
 GAPPED_KERNEL_LANE = 1
 GAPPED_KERNEL_ROWS = 2
 GAPPED_KERNEL_STATIC = 3
+GAPPED_KERNEL_DEAL = 4
 COST_FEATURES = 8
 
 

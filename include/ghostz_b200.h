@@ -70,6 +70,11 @@ typedef struct {
   int32_t clustering;            /* database built with -C T */
 } gzb_params;
 
+/* Device sequence buffers given to the operators below hold one residue
+ * code (< 32) per byte, sequences separated by the delimiter, with at least
+ * 64 delimiter bytes before the first and after the last sequence: the
+ * kernels read aligned 32-bit words, a few bytes past a delimiter. */
+
 /* ---- DistanceCalculatorGpu (src/distance_calculator_gpu.h:18-40) ------- */
 typedef struct gzb_distance_calculator gzb_distance_calculator;
 int gzb_distance_calculator_create(gzb_distance_calculator **out);
@@ -306,7 +311,7 @@ int gzb_engine_get_extension_costs(gzb_engine *e, float *predicted, uint32_t *ce
                                    uint64_t capacity, uint64_t *count, void *stream);
 /* ---- tile parameters and the autotuner -----------------------------------
  * The first level of the gapped stage runs one extension per thread in one
- * of four kernels (GZB_TILE_GAPPED_KERNEL):
+ * of five kernels (GZB_TILE_GAPPED_KERNEL):
  *   GZB_GAPPED_KERNEL_FLAT  every lane advances one DP cell per step; a lane
  *       at a row or extension boundary waits until GZB_TILE_BOOK_THRESHOLD
  *       lanes of its warp are (or no lane can step), then they do their
@@ -321,7 +326,11 @@ int gzb_engine_get_extension_costs(gzb_engine *e, float *predicted, uint32_t *ce
  *       own ends, so lanes wait for each other only within a row (the
  *       process-wide default);
  *   GZB_GAPPED_KERNEL_STATIC  one launch that deals extensions to threads
- *       round-robin, no work queue: the plain schedule's kernel.
+ *       round-robin, no work queue: the plain schedule's kernel;
+ *   GZB_GAPPED_KERNEL_DEAL  the row-step refill of _ROWS with extensions
+ *       dealt to lanes round-robin in schedule order instead of queued, so
+ *       each lane loads its next extension while it runs the current one;
+ *       longest-first order keeps the lanes' totals even.
  * gzb_set_tile_parameter sets the process-wide defaults that the operators
  * and engines without a tuned tile use. */
 #define GZB_TILE_BOOK_THRESHOLD 0
@@ -330,6 +339,7 @@ int gzb_engine_get_extension_costs(gzb_engine *e, float *predicted, uint32_t *ce
 #define GZB_GAPPED_KERNEL_LANE 1
 #define GZB_GAPPED_KERNEL_ROWS 2
 #define GZB_GAPPED_KERNEL_STATIC 3
+#define GZB_GAPPED_KERNEL_DEAL 4
 int gzb_set_tile_parameter(int which, int value);
 int gzb_get_tile_parameter(int which, int *value);
 /* Per-engine, per-schedule tile: value -1 falls back to the process-wide

@@ -94,7 +94,7 @@ def test_tile_parameters_validate_without_device():
         assert L.gzb_set_tile_parameter(which, keep) == 0
     assert L.gzb_set_tile_parameter(N.TILE_BOOK_THRESHOLD, 0) == 1
     assert L.gzb_set_tile_parameter(N.TILE_BOOK_THRESHOLD, 33) == 1
-    assert L.gzb_set_tile_parameter(N.TILE_GAPPED_KERNEL, 4) == 1
+    assert L.gzb_set_tile_parameter(N.TILE_GAPPED_KERNEL, 5) == 1
     assert b"none of" in L.gzb_last_error()
     assert L.gzb_set_tile_parameter(7, 1) == 1
     assert L.gzb_get_tile_parameter(7, ctypes.byref(v)) == 1
