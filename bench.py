@@ -195,6 +195,7 @@ def run_reference(args, world, rank):
 
 
 KERNEL_NAMES = {0: "flat", 1: "lane", 2: "rows", 3: "static", 4: "deal"}
+ORDER_NAMES = {0: "hits", 1: "cost model"}
 
 
 def main():
@@ -306,12 +307,17 @@ def main():
             ker, ker_ms = eng.autotune(sid, (N.GAPPED_KERNEL_FLAT, N.GAPPED_KERNEL_LANE,
                                              N.GAPPED_KERNEL_ROWS, N.GAPPED_KERNEL_DEAL),
                                        N.TILE_GAPPED_KERNEL)
+            # whether the cost model's order pays for its features and
+            # prediction on this workload (hit order otherwise)
+            order_t, order_ms = eng.autotune(sid, (N.ORDER_MODEL, N.ORDER_HITS), N.TILE_ORDER)
             tiles = {"gapped_ms_by_book_threshold": thr_ms,
-                     "gapped_ms_by_kernel": {KERNEL_NAMES[k]: v for k, v in ker_ms.items()}}
+                     "gapped_ms_by_kernel": {KERNEL_NAMES[k]: v for k, v in ker_ms.items()},
+                     "gapped_ms_by_order": {ORDER_NAMES[k]: v for k, v in order_ms.items()}}
         for w in (N.TILE_GAPPED_KERNEL, N.TILE_BOOK_THRESHOLD):
             eng.set_tile(N.SCHEDULE_ORACLE, w, eng.tile(sid, w))
         tiles.update(kernel=KERNEL_NAMES[eng.tile(sid, N.TILE_GAPPED_KERNEL)],
-                     book_threshold=eng.tile(sid, N.TILE_BOOK_THRESHOLD))
+                     book_threshold=eng.tile(sid, N.TILE_BOOK_THRESHOLD),
+                     order=ORDER_NAMES[eng.tile(sid, N.TILE_ORDER)])
 
     sampler = ClockSampler(local_rank)
     sampler.start()
@@ -431,8 +437,10 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded generator with the config's shapes)",
         "config": {"workload": args.workload,
-                   "schedule": ("batched: learned cost order, persistent work queue"
-                                if args.schedule == "batched" else "plain"),
+                   "schedule": (f"batched: persistent work-queue kernel "
+                                f"'{tiles.get('kernel')}', order '{tiles.get('order')}' "
+                                f"(autotuned), cost model trained on the GPU"
+                                if args.schedule == "batched" else "plain static"),
                    "db_sequences": db.number_sequences, "db_residues": db.length,
                    "queries": nq, "l2": "inputs larger than L2 (database chunk > 126 MB)",
                    "parallelism": f"replicas x{world}"},

@@ -56,6 +56,7 @@ __global__ void gapped_serial_kernel(GappedJob job, const int32_t *__restrict__ 
 extern GappedTile g_tile;
 int check_tile_value(int which, int value);
 int *tile_field(GappedTile &t, int which);
+int any_tile_value(int which);
 int run_gapped(const GappedTile &tile, const GappedJob &job, const int32_t *matrix,
                int number_letters, int stride, size_t n, const uint32_t *order, int reverse,
                const uint8_t *dir, uint32_t *d_qpos, uint32_t *d_dpos, int32_t *d_scores,
@@ -1069,7 +1070,7 @@ struct gzb_engine {
   DBuf codeflag;
   uint64_t pred_n = 0;       // extensions with a prediction in epred (last run)
   DBuf enb;                  // per surviving hit: chained neighbours (cost feature)
-  int tile[3][2] = {{-1, -1}, {-1, -1}, {-1, -1}};  // [schedule][which], -1 = default
+  int tile[3][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}};  // [schedule][which], -1 = default
   bool logging = false;
   uint64_t log_cap = 0;
   bool have_model = false;
@@ -1762,7 +1763,12 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
     job.gap_open = e->params.gap_open;
     job.gap_ext = e->params.gap_extension;
     job.cutoff = e->params.gapped_cutoff;
-    const bool learned = schedule == GZB_SCHEDULE_BATCHED && e->have_model;
+    GappedTile tile = g_tile;
+    for (int w = 0; w < 3; ++w)
+      if (e->tile[schedule][w] >= 0) *tile_field(tile, w) = e->tile[schedule][w];
+    if (schedule == GZB_SCHEDULE_PLAIN) tile.kernel = GZB_GAPPED_KERNEL_STATIC;
+    const bool learned =
+        schedule == GZB_SCHEDULE_BATCHED && e->have_model && tile.order == GZB_ORDER_MODEL;
     const bool oracle_order = schedule == GZB_SCHEDULE_ORACLE && e->prev_cells_n == next;
     const bool scheduled = schedule != GZB_SCHEDULE_PLAIN || e->logging;
     const bool want_feat = learned || e->logging;
@@ -1803,10 +1809,6 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
       order = vb.Current();
     }
     uint32_t fb = 0;
-    GappedTile tile = g_tile;
-    for (int w = 0; w < 2; ++w)
-      if (e->tile[schedule][w] >= 0) *tile_field(tile, w) = e->tile[schedule][w];
-    if (schedule == GZB_SCHEDULE_PLAIN) tile.kernel = GZB_GAPPED_KERNEL_STATIC;
     if (scheduled) GZB_TRY(e->ecells.ensure(4 * (next + 1)));
     GZB_TRY(run_gapped(tile, job, e->matrix32.as<int32_t>(), 32, 32, next, order, 0,
                        e->edir.as<uint8_t>(), e->eq.as<uint32_t>(), e->ed.as<uint32_t>(),
@@ -2097,8 +2099,7 @@ extern "C" int gzb_engine_get_extension_costs(gzb_engine *e, float *predicted,
 extern "C" int gzb_engine_set_tile(gzb_engine *e, int schedule, int which, int value) {
   GZB_TRY(check_engine(e));
   GZB_CHECK(schedule >= 0 && schedule < 3, GZB_ERR_INVALID, "unknown schedule %d", schedule);
-  if (value != -1) GZB_TRY(check_tile_value(which, value));
-  else GZB_TRY(check_tile_value(which, which == GZB_TILE_GAPPED_KERNEL ? 0 : 1));
+  GZB_TRY(check_tile_value(which, value != -1 ? value : any_tile_value(which)));
   e->tile[schedule][which] = value;
   return GZB_OK;
 }
@@ -2107,7 +2108,7 @@ extern "C" int gzb_engine_get_tile(gzb_engine *e, int schedule, int which, int *
   GZB_TRY(check_engine(e));
   GZB_CHECK(value, GZB_ERR_INVALID, "null value");
   GZB_CHECK(schedule >= 0 && schedule < 3, GZB_ERR_INVALID, "unknown schedule %d", schedule);
-  GZB_TRY(check_tile_value(which, which == GZB_TILE_GAPPED_KERNEL ? 0 : 1));
+  GZB_TRY(check_tile_value(which, any_tile_value(which)));
   const int v = e->tile[schedule][which];
   if (v >= 0) *value = v;
   else GZB_TRY(gzb_get_tile_parameter(which, value));

@@ -242,12 +242,14 @@ struct GappedJob {
   int delim, gap_open, gap_ext, cutoff;
 };
 
-// Launch shape of the one-thread-per-extension gapped level: which kernel
-// (GZB_GAPPED_KERNEL_FLAT / _LANE) and the flat kernel's bookkeeping
-// threshold.
+// Tile of the gapped stage: the one-thread-per-extension kernel
+// (GZB_GAPPED_KERNEL_*), the flat kernel's bookkeeping threshold, and
+// whether the batched schedule orders extensions by the cost model
+// (GZB_ORDER_MODEL) or keeps hit order (GZB_ORDER_HITS).
 struct GappedTile {
   int kernel;
   int book_threshold;
+  int order;
 };
 
 struct GappedOut {

@@ -387,7 +387,7 @@ gapped_deal_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
 }
 
 // process-wide tile defaults (gzb_set_tile_parameter)
-GappedTile g_tile = {GZB_GAPPED_KERNEL_ROWS, 16};
+GappedTile g_tile = {GZB_GAPPED_KERNEL_ROWS, 16, GZB_ORDER_MODEL};
 
 template <typename K>
 static int persistent_blocks(K kernel, int block, size_t smem, uint64_t n, uint64_t *blocks) {
@@ -916,12 +916,25 @@ int check_tile_value(int which, int value) {
               "gapped kernel %d is none of GZB_GAPPED_KERNEL_FLAT/LANE/ROWS/STATIC/DEAL", value);
     return GZB_OK;
   }
+  if (which == GZB_TILE_ORDER) {
+    GZB_CHECK(value == GZB_ORDER_HITS || value == GZB_ORDER_MODEL, GZB_ERR_INVALID,
+              "order %d is neither GZB_ORDER_HITS nor GZB_ORDER_MODEL", value);
+    return GZB_OK;
+  }
   GZB_CHECK(which == GZB_TILE_BOOK_THRESHOLD, GZB_ERR_INVALID, "unknown tile parameter %d", which);
   GZB_CHECK(value >= 1 && value <= 32, GZB_ERR_INVALID, "book threshold %d outside 1..32", value);
   return GZB_OK;
 }
 int *tile_field(GappedTile &t, int which) {
-  return which == GZB_TILE_GAPPED_KERNEL ? &t.kernel : &t.book_threshold;
+  return which == GZB_TILE_GAPPED_KERNEL ? &t.kernel
+         : which == GZB_TILE_ORDER      ? &t.order
+                                        : &t.book_threshold;
+}
+// a valid value of tile parameter `which` (for checking `which` alone)
+int any_tile_value(int which) {
+  return which == GZB_TILE_GAPPED_KERNEL ? GZB_GAPPED_KERNEL_FLAT
+         : which == GZB_TILE_ORDER      ? GZB_ORDER_HITS
+                                        : 1;
 }
 }  // namespace gzb
 
@@ -933,7 +946,7 @@ extern "C" int gzb_set_tile_parameter(int which, int value) {
 
 extern "C" int gzb_get_tile_parameter(int which, int *value) {
   GZB_CHECK(value, GZB_ERR_INVALID, "null value");
-  GZB_TRY(gzb::check_tile_value(which, which == GZB_TILE_GAPPED_KERNEL ? 0 : 1));
+  GZB_TRY(gzb::check_tile_value(which, gzb::any_tile_value(which)));
   *value = *gzb::tile_field(gzb::g_tile, which);
   return GZB_OK;
 }

@@ -295,6 +295,9 @@ SCHEDULE_BATCHED = 1
 SCHEDULE_ORACLE = 2
 TILE_BOOK_THRESHOLD = 0
 TILE_GAPPED_KERNEL = 1
+TILE_ORDER = 2
+ORDER_HITS = 0
+ORDER_MODEL = 1
 GAPPED_KERNEL_FLAT = 0
 GAPPED_KERNEL_LANE = 1
 GAPPED_KERNEL_ROWS = 2

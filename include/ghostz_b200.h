@@ -335,6 +335,12 @@ int gzb_engine_get_extension_costs(gzb_engine *e, float *predicted, uint32_t *ce
  * and engines without a tuned tile use. */
 #define GZB_TILE_BOOK_THRESHOLD 0
 #define GZB_TILE_GAPPED_KERNEL 1
+/* GZB_TILE_ORDER: the batched schedule's order, GZB_ORDER_MODEL (the cost
+ * model's predicted cost, longest first; the default) or GZB_ORDER_HITS
+ * (hit order, skipping the features and the prediction). */
+#define GZB_TILE_ORDER 2
+#define GZB_ORDER_HITS 0
+#define GZB_ORDER_MODEL 1
 #define GZB_GAPPED_KERNEL_FLAT 0
 #define GZB_GAPPED_KERNEL_LANE 1
 #define GZB_GAPPED_KERNEL_ROWS 2
