@@ -54,6 +54,10 @@ WORKLOADS = {
 # 8 B of centres + 2L window bytes + 1 B result.
 BYTES_PER_UNGAPPED_STEP = 2
 BYTES_PER_DISTANCE_SEED = 8 + 2 * 10 + 1
+# DRAM bytes (read + write) of one launch of the seed-search kernels
+# (seed_kernel + member_kernel) on each workload, from one ncu capture of the
+# bench command (profiles/seed_kernels_dram_*.txt); None when not captured
+SEED_KERNEL_DRAM_BYTES = {}
 
 
 def log(msg):
@@ -273,7 +277,8 @@ def main():
             eng.reset_results(stream)
             eng.presearch(sched, stream)
         barrier()
-        stage = {k: 0.0 for k in ("lookup", "seed_ungapped", "chain", "gapped", "merge", "total")}
+        stage = {k: 0.0 for k in ("lookup", "seed_ungapped", "chain", "gapped", "merge", "total",
+                                  "seed_kernels")}
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
@@ -422,15 +427,23 @@ def main():
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     dominant = "seed_ungapped" if st["seed_ungapped"] >= st["gapped"] else "gapped"
+    # algorithmic bytes of the seed-search kernels: two residue bytes per
+    # ungapped step, and per distance seed the two positions, the two
+    # L-residue windows and the distance byte the reference moves
     steps_pairs = counters.get("ungapped_steps", 0)
-    seed_bytes = (counters["ungapped_seeds"] * 0 + counters["distance_seeds"] * BYTES_PER_DISTANCE_SEED
+    seed_bytes = (counters["distance_seeds"] * BYTES_PER_DISTANCE_SEED
                   + BYTES_PER_UNGAPPED_STEP * steps_pairs)
-    achieved = seed_bytes / (st["seed_ungapped"] / 1e3) / 1e9 if st["seed_ungapped"] else 0.0
-    roofline = {"bound": "hbm", "kernel": "seed_kernel (seed search + distance + ungapped)",
-                "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
+    achieved = seed_bytes / (st["seed_kernels"] / 1e3) / 1e9 if st["seed_kernels"] else 0.0
+    traffic = SEED_KERNEL_DRAM_BYTES.get(args.workload)
+    roofline = {"bound": "hbm", "kernel": "seed_kernel + member_kernel (seed search, distance, "
+                "ungapped X-drop)", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved / hbm_peak, "traffic": traffic,
+                "algorithmic_bytes": seed_bytes, "kernel_ms": st["seed_kernels"],
+                "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"
+                if peak_src == "measured" else "fallback 6650 GB/s",
                 "dominant_stage": dominant,
-                "note": "gapped DP is integer-pipe bound: see dp_gcups"}
+                "note": "latency and issue bound integer work, not HBM bound; the gapped "
+                        "DP is reported as dp_gcups"}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
         "warmup": args.warmup, "ms_per_step": t_dev / steps, "higher_is_better": True,

@@ -1084,7 +1084,7 @@ struct gzb_engine {
   int band_wmask = 0;
   uint64_t hit_cap = 1ull << 22, mwork_cap = 1ull << 22;
   gzb_counters counters{};
-  float stage_ms[6] = {0, 0, 0, 0, 0, 0};
+  float stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
   cudaEvent_t ev[7] = {};
 };
 
@@ -1694,6 +1694,7 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
   e->counters.ungapped_steps = hctr[2];
   e->counters.ungapped_seeds = hctr[1];
   e->counters.ungapped_hits = n_hits;
+  GZB_CUDA(cudaEventRecord(e->ev[6], s));
   // ---- sort hits by (query, database position, query position)
   GZB_TRY(e->hits_alt.ensure(8 * (n_hits + 1)));
   uint64_t *hits = e->hits.as<uint64_t>();
@@ -1875,6 +1876,7 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
   for (int i = 0; i < 5; ++i) GZB_CUDA(cudaEventElapsedTime(&t[i], e->ev[i], e->ev[i + 1]));
   GZB_CUDA(cudaEventElapsedTime(&t[5], e->ev[0], e->ev[5]));
   for (int i = 0; i < 6; ++i) e->stage_ms[i] = t[i];
+  GZB_CUDA(cudaEventElapsedTime(&e->stage_ms[6], e->ev[1], e->ev[6]));
   e->counters.kernel_launches = launches;
   return GZB_OK;
 }
@@ -1912,9 +1914,9 @@ extern "C" int gzb_engine_get_counters(gzb_engine *e, gzb_counters *out) {
   return GZB_OK;
 }
 
-extern "C" int gzb_engine_get_stage_ms(gzb_engine *e, float *ms6) {
-  GZB_CHECK(e && ms6, GZB_ERR_INVALID, "null argument");
-  for (int i = 0; i < 6; ++i) ms6[i] = e->stage_ms[i];
+extern "C" int gzb_engine_get_stage_ms(gzb_engine *e, float *ms7) {
+  GZB_CHECK(e && ms7, GZB_ERR_INVALID, "null argument");
+  for (int i = 0; i < 7; ++i) ms7[i] = e->stage_ms[i];
   return GZB_OK;
 }
 

@@ -382,10 +382,10 @@ class PresearchEngine:
         return dict(zip(COUNTER_NAMES, [int(v) for v in c]))
 
     def stage_ms(self):
-        t = (C.c_float * 6)()
+        t = (C.c_float * 7)()
         check(lib().gzb_engine_get_stage_ms(self.h, C.byref(t)))
-        return dict(zip(("lookup", "seed_ungapped", "chain", "gapped", "merge", "total"),
-                        [float(v) for v in t]))
+        return dict(zip(("lookup", "seed_ungapped", "chain", "gapped", "merge", "total",
+                         "seed_kernels"), [float(v) for v in t]))
 
     def hits(self, stream=None):
         n = C.c_uint64()

@@ -401,8 +401,9 @@ int gzb_engine_get_schedule_stats(gzb_engine *e, float *mean_abs_log2_error,
                                   uint64_t *count);
 /* Time of the last presearch, per stage, in milliseconds (device events):
  * [0] list lookup, [1] seed search + ungapped + sort, [2] chain filter,
- * [3] gapped extension, [4] merge, [5] total. */
-int gzb_engine_get_stage_ms(gzb_engine *e, float *ms6);
+ * [3] gapped extension, [4] merge, [5] total, [6] the seed-search kernels
+ * alone (part of [1]: seed and member kernels, without the hit sort). */
+int gzb_engine_get_stage_ms(gzb_engine *e, float *ms7);
 
 #ifdef __cplusplus
 }
