@@ -44,9 +44,12 @@ METRIC = "queries/s and DP GCUPS, learned-batched vs plain GPU, bit-identical hi
 UNIT = "queries/s"
 
 WORKLOADS = {
-    # name: (db sequences, db seed, queries, query seed)
-    "protein-10k-x-2M": (2_000_000, 201, 10_000, 202),
-    "protein-1k-x-200k": (200_000, 211, 1_000, 212),   # small case for profiling
+    # name: (db sequences, db seed, queries, query seed, query length law)
+    "protein-10k-x-2M": (2_000_000, 201, 10_000, 202, {}),
+    # uneven query lengths: log-normal median 250, sigma 1.0, clipped to 20-8000
+    "protein-50k-uneven-x-2M": (2_000_000, 201, 50_000, 402,
+                                {"median": 250, "sigma": 1.0, "lo": 20, "hi": 8000}),
+    "protein-1k-x-200k": (200_000, 211, 1_000, 212, {}),   # small case for profiling
 }
 
 # algorithmic bytes of the dominant kernels:
@@ -57,7 +60,7 @@ BYTES_PER_DISTANCE_SEED = 8 + 2 * 10 + 1
 # DRAM bytes (read + write) of one launch of the seed-search kernels
 # (seed_kernel + member_kernel) on each workload, from one ncu capture of the
 # bench command (profiles/seed_kernels_dram_*.txt); None when not captured
-SEED_KERNEL_DRAM_BYTES = {}
+SEED_KERNEL_DRAM_BYTES = {"protein-10k-x-2M": (40.96e9 + 0.074e9) + (64.54e9 + 0.005e9)}
 
 
 def log(msg):
@@ -66,10 +69,10 @@ def log(msg):
 
 def make_workload(name):
     from gzb import workload as W
-    ndb, sdb, nq, sq = WORKLOADS[name]
+    ndb, sdb, nq, sq, law = WORKLOADS[name]
     t = time.time()
     db = W.make_database(ndb, sdb)
-    q = W.make_queries(db, nq, sq)
+    q = W.make_queries(db, nq, sq, **law)
     return db, q, time.time() - t
 
 
@@ -307,16 +310,17 @@ def main():
     if args.schedule == "batched":
         sid = N.SCHEDULE_BATCHED
         if not args.no_autotune:
-            eng.set_tile(sid, N.TILE_GAPPED_KERNEL, N.GAPPED_KERNEL_FLAT)
-            thr, thr_ms = eng.autotune(sid, (4, 8, 12, 16, 24), N.TILE_BOOK_THRESHOLD)
             ker, ker_ms = eng.autotune(sid, (N.GAPPED_KERNEL_FLAT, N.GAPPED_KERNEL_LANE,
                                              N.GAPPED_KERNEL_ROWS, N.GAPPED_KERNEL_DEAL),
                                        N.TILE_GAPPED_KERNEL)
+            thr_ms = {}
+            if ker in (N.GAPPED_KERNEL_FLAT, N.GAPPED_KERNEL_ROWS):
+                thr, thr_ms = eng.autotune(sid, (1, 2, 4, 8, 16), N.TILE_BOOK_THRESHOLD)
             # whether the cost model's order pays for its features and
             # prediction on this workload (hit order otherwise)
             order_t, order_ms = eng.autotune(sid, (N.ORDER_MODEL, N.ORDER_HITS), N.TILE_ORDER)
-            tiles = {"gapped_ms_by_book_threshold": thr_ms,
-                     "gapped_ms_by_kernel": {KERNEL_NAMES[k]: v for k, v in ker_ms.items()},
+            tiles = {"gapped_ms_by_kernel": {KERNEL_NAMES[k]: v for k, v in ker_ms.items()},
+                     "gapped_ms_by_book_threshold": thr_ms,
                      "gapped_ms_by_order": {ORDER_NAMES[k]: v for k, v in order_ms.items()}}
         for w in (N.TILE_GAPPED_KERNEL, N.TILE_BOOK_THRESHOLD):
             eng.set_tile(N.SCHEDULE_ORACLE, w, eng.tile(sid, w))

@@ -258,16 +258,20 @@ gapped_lane_queue_kernel(GappedJob job, const int32_t *__restrict__ matrix, int 
 }
 
 // Row-granular work queue: every lane runs its own extension one database
-// row per step and takes the next extension from the queue as soon as its
-// own ends, so the lanes of a warp wait for each other only within a row
-// (the widest band of the step), never for the longest extension.
+// row per step and takes the next extension from the queue once its own has
+// ended, so the lanes of a warp wait for each other only within a row (the
+// widest band of the step), never for the longest extension.  A lane whose
+// extension ended writes it out at once and then idles until
+// `refill_threshold` lanes of its warp are idle (or no lane has work left):
+// those lanes then fetch, load and start their next extensions together, so
+// one round of memory latency and one pass of the set-up code serve them all.
 __global__ void __launch_bounds__(kLaneBlock)
 gapped_rows_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number_letters,
                    int stride, uint64_t n, const uint32_t *__restrict__ order,
                    unsigned long long *queue, int reverse, const uint8_t *__restrict__ dir,
                    uint32_t *qpos, uint32_t *dpos, int32_t *scores, uint32_t *spill,
                    uint32_t *spill_count, unsigned long long *cells_total,
-                   uint32_t *cells_out) {
+                   uint32_t *cells_out, int refill_threshold) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
   __shared__ uint32_t cells_s[kLaneW * kLaneBlock];
   __shared__ uint8_t res_s[kLaneW * kLaneBlock];
@@ -281,7 +285,11 @@ gapped_rows_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
   for (;;) {
     int st = kLaneRunning;
     if (have) st = lane_row(job, sm, band, x);
-    while (st != kLaneRunning || (!have && !done)) {
+    const unsigned idle = __ballot_sync(0xffffffffu, !done && (!have || st != kLaneRunning));
+    const unsigned busy = __ballot_sync(0xffffffffu, have && st == kLaneRunning);
+    if (idle == 0 && busy == 0) break;
+    const bool refill = __popc(idle) >= refill_threshold || busy == 0;
+    while (have ? st != kLaneRunning : (refill && !done)) {
       if (have) {  // the extension ended: write it out
         if (st == kLaneOverflow || x.ovf) {
           spill[atomicAdd(spill_count, 1u)] = e;
@@ -294,6 +302,8 @@ gapped_rows_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
           if (cells_out) cells_out[e] = x.cells;
         }
         have = false;
+        st = kLaneRunning;
+        if (!refill) break;
       }
       if (!flat_fetch(queue, n, order, &e)) {
         done = true;
@@ -305,7 +315,6 @@ gapped_rows_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
       st = lane_init(job, band, x, job.query + q, job.db + d, rev);
       have = true;
     }
-    if (__all_sync(0xffffffffu, done)) break;
   }
   cells += __shfl_down_sync(0xffffffffu, cells, 16);
   cells += __shfl_down_sync(0xffffffffu, cells, 8);
@@ -387,7 +396,7 @@ gapped_deal_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
 }
 
 // process-wide tile defaults (gzb_set_tile_parameter)
-GappedTile g_tile = {GZB_GAPPED_KERNEL_ROWS, 16, GZB_ORDER_MODEL};
+GappedTile g_tile = {GZB_GAPPED_KERNEL_ROWS, 4, GZB_ORDER_MODEL};
 
 template <typename K>
 static int persistent_blocks(K kernel, int block, size_t smem, uint64_t n, uint64_t *blocks) {
@@ -427,7 +436,7 @@ int launch_gapped_thread(const GappedTile &tile, const GappedJob &job, const int
     GZB_TRY(persistent_blocks(gapped_rows_kernel, kLaneBlock, 0, n, &blocks));
     gapped_rows_kernel<<<(unsigned)blocks, kLaneBlock, 0, s>>>(
         job, matrix, number_letters, stride, n, order, queue, reverse, dir, qpos, dpos, scores,
-        spill, spill_count, cells_total, cells_out);
+        spill, spill_count, cells_total, cells_out, tile.book_threshold);
   } else if (tile.kernel == GZB_GAPPED_KERNEL_LANE) {
     GZB_TRY(persistent_blocks(gapped_lane_queue_kernel, kLaneBlock, 0, n, &blocks));
     gapped_lane_queue_kernel<<<(unsigned)blocks, kLaneBlock, 0, s>>>(

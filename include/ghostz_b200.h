@@ -322,9 +322,11 @@ int gzb_engine_get_extension_costs(gzb_engine *e, float *predicted, uint32_t *ce
  *       fastest when neighbouring extensions cost the same (the batched
  *       schedule orders them by predicted cost);
  *   GZB_GAPPED_KERNEL_ROWS  each lane runs its extension one database row
- *       per step and takes the next extension from the queue as soon as its
- *       own ends, so lanes wait for each other only within a row (the
- *       process-wide default);
+ *       per step and takes the next extension from the queue once its own
+ *       has ended, so lanes wait for each other only within a row; finished
+ *       lanes refill together once GZB_TILE_BOOK_THRESHOLD lanes of the
+ *       warp are idle (or none has work left), sharing one round of memory
+ *       latency (the process-wide default, threshold 4);
  *   GZB_GAPPED_KERNEL_STATIC  one launch that deals extensions to threads
  *       round-robin, no work queue: the plain schedule's kernel;
  *   GZB_GAPPED_KERNEL_DEAL  the row-step refill of _ROWS with extensions

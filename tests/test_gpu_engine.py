@@ -108,7 +108,7 @@ def test_presearch_repeated_calls_identical(engine, params):
     assert all(np.array_equal(x, y) for x, y in zip(a, b))
 
 
-@pytest.mark.parametrize("kernel,threshold", [(0, 1), (0, 32), (1, 8), (2, 8), (3, 8), (4, 8)])
+@pytest.mark.parametrize("kernel,threshold", [(0, 1), (0, 32), (1, 8), (2, 1), (2, 8), (2, 32), (3, 8), (4, 8)])
 def test_presearch_every_gapped_tile(engine, oracle, params, kernel, threshold):
     # every one-thread-per-extension kernel on the work-queue schedule (no
     # model: hit order), and the flat kernel's extreme bookkeeping
