@@ -1060,7 +1060,7 @@ struct gzb_engine {
   // results
   DBuf results, counts;
   // scratch
-  DBuf tmp, hits, hits_alt, mwork, begin, kept, surv_off, slots, eq, ed, edir,
+  DBuf tmp, hits, hits_alt, mwork, mwork_alt, begin, kept, surv_off, slots, eq, ed, edir,
       escore, merge_scratch, heap, ctr, misc, hits_copy;
   int qbits = 1, dbits = 1;
   // schedule of the gapped stage
@@ -1263,7 +1263,7 @@ extern "C" int gzb_engine_destroy(gzb_engine *e) {
   for (auto &b : e->list_bufs) b.release();
   DBuf *all[] = {&e->matrix32, &e->db_buf, &e->db_offsets, &e->q_buf, &e->q_offsets,
                  &e->q_lengths, &e->q_cut, &e->q_trig, &e->results, &e->counts,
-                 &e->tmp, &e->hits, &e->hits_alt, &e->mwork,
+                 &e->tmp, &e->hits, &e->hits_alt, &e->mwork, &e->mwork_alt,
                  &e->begin, &e->kept, &e->surv_off, &e->slots, &e->eq, &e->ed, &e->edir,
                  &e->escore, &e->merge_scratch, &e->heap, &e->ctr, &e->misc,
                  &e->hits_copy, &e->elen0, &e->elen1, &e->eqid, &e->efeat, &e->epred,
@@ -1674,8 +1674,17 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
       continue;
     }
     if (n_mwork) {
+      // cluster-major order (stable, so entries keep their order within a
+      // cluster): the items a warp takes then share their members, whose
+      // database words stay in cache between query positions
+      GZB_TRY(e->mwork_alt.ensure(8 * (n_mwork + 1)));
+      uint64_t *sorted_mw = nullptr;
+      GZB_TRY(sort_keys_u64(e, reinterpret_cast<uint64_t *>(a.mwork),
+                            e->mwork_alt.as<uint64_t>(), n_mwork, bits_for(X.n_reps + 1), s,
+                            &sorted_mw));
+      launches += 1;
       member_kernel<<<grid1((n_mwork + 31) / 32 * 32, kSeedBlock, 148 * 16), kSeedBlock, 0, s>>>(
-          a, a.mwork, n_mwork);
+          a, reinterpret_cast<const uint2 *>(sorted_mw), n_mwork);
       GZB_CUDA(cudaGetLastError());
       ++launches;
       GZB_CUDA(cudaMemcpyAsync(hctr, c, 64, cudaMemcpyDeviceToHost, s));
