@@ -744,20 +744,17 @@ __device__ __forceinline__ int lane_row(const GappedJob &job, const int *sm, Lan
     int s = diag + mrow[band.res[k]];
     diag = old_best;
     s = imax(s, imax(vgap, row_gap));
-    if (maxs - s > cutoff) {
-      if (bs + 1 == c) ++bs;
-      band.cell[k] = pack16(kInitScore, kInitScore);
-      row_gap = kInitScore;
-    } else {
-      last = c;
-      if (s > maxs) {
-        maxs = s;
-        maxc = c;
-      }
-      const int ng = imax(s - gi, vgap - ge);
-      row_gap = imax(s - gi, row_gap - ge);
-      band.cell[k] = pack16(s, ng);
-    }
+    // branch-free: a pruned cell (X-drop) stores the initial score and resets
+    // the row gap; the left edge moves past a leading run of pruned cells
+    const bool drop = maxs - s > cutoff;
+    bs += (drop && bs + 1 == c) ? 1 : 0;
+    last = drop ? last : c;
+    maxc = s > maxs ? c : maxc;  // a pruned cell is below maxs
+    maxs = imax(maxs, s);
+    const int sg = s - gi;
+    const int ng = imax(sg, vgap - ge);
+    row_gap = drop ? kInitScore : imax(sg, row_gap - ge);
+    band.cell[k] = drop ? pack16(kInitScore, kInitScore) : pack16(s, ng);
   }
   const uint32_t cells = (uint32_t)(be - bs_row - 1);
   if (maxs > maxs_in) {
