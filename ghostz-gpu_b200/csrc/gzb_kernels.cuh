@@ -186,14 +186,17 @@ __device__ __forceinline__ int walk_side(const uint8_t *s0, const uint8_t *s1,
     v = *(const int32_t *)(tbl + walk_offset<(INC > 0 ? (J) : 3 - (J))>(x4, qa)); \
     score += v;                                                            \
     best = imax(best, score);                                              \
-    ++n;                                                                   \
-    if (best - score >= cutoff || best > stop_above) break;               \
+    if (best - score >= cutoff || best > stop_above) {                     \
+      n += (J) + 1;                                                        \
+      break;                                                               \
+    }                                                                      \
   }
     GZB_WALK_STEP(0)
     GZB_WALK_STEP(1)
     GZB_WALK_STEP(2)
     GZB_WALK_STEP(3)
 #undef GZB_WALK_STEP
+    n += 4;
     if (INC > 0) {
       a_lo = a_hi;
       b_lo = b_hi;
