@@ -215,7 +215,7 @@ def main():
     ap.add_argument("--train-sets", type=int, default=8)
     ap.add_argument("--workload", default="protein-10k-x-2M", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-queries", type=int, default=10000)
-    ap.add_argument("--ref-queries", type=int, default=4000)
+    ap.add_argument("--ref-queries", type=int, default=10000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()

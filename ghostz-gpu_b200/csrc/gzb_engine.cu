@@ -438,7 +438,7 @@ constexpr int kUnitsPerWarp = 256;
 
 // One unit = one representative or one residual database position of a list,
 // tried against every query position of that list.
-__global__ void __launch_bounds__(kSeedBlock)
+__global__ void __launch_bounds__(kSeedBlock, 5)
 seed_kernel(SeedArgs a) {
   __shared__ __align__(16) int32_t tbl32[kWalkTableBytes / 4];
   load_walk_table(tbl32, a.matrix32, a.p.delimiter);
@@ -528,7 +528,7 @@ seed_kernel(SeedArgs a) {
 // to its lanes 32 at a time: a lane finds its item with a five-step shuffle
 // search over the scan, so a seed costs one load (the member's position)
 // besides its walk.
-__global__ void __launch_bounds__(kSeedBlock)
+__global__ void __launch_bounds__(kSeedBlock, 5)
 member_kernel(SeedArgs a, const uint2 *__restrict__ mwork, uint64_t n_work) {
   __shared__ __align__(16) int32_t tbl32[kWalkTableBytes / 4];
   load_walk_table(tbl32, a.matrix32, a.p.delimiter);
