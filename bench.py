@@ -391,6 +391,18 @@ def main():
     cnt = np.frombuffer(counts_pin.numpy().tobytes(), dtype=np.uint32)
     e2e_same = all(np.array_equal(got[i, :cnt[i]], results[i]) for i in range(q.number))
 
+    # the build results step (traceback statistics of the merged results),
+    # outside the presearch metric: device time of one call after a warm-up
+    eng.build_alignments(stream)
+    b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b0.record(stream)
+    aligned = eng.build_alignments(stream)
+    b1.record(stream)
+    torch.cuda.synchronize()
+    n_aligned = int(sum(len(x) for x in aligned))
+    build_results = {"ms": b0.elapsed_time(b1), "alignments": n_aligned,
+                     "alignments_per_s": n_aligned / (b0.elapsed_time(b1) / 1e3)}
+
     # max over ranks
     t_dev, t_e2e = dev_ms, e2e_ms
     if dist is not None:
@@ -466,7 +478,7 @@ def main():
                 "results_equal_device_loop": bool(e2e_same)},
         "dp_gcups": {"gapped_stage": gcups_stage, "whole_step": gcups_step},
         "stage_ms": st, "counters": counters, "schedules": sched_report,
-        "index_build_s": index_s,
+        "index_build_s": index_s, "build_results": build_results,
         "workload_gen_s": gen_s, "clocks": clocks, "roofline": roofline,
         "gpu_launches": int(counters.get("kernel_launches", 0)) * steps,
     }

@@ -30,6 +30,7 @@
 #include "gzb_index.cuh"
 #include "gzb_kernels.cuh"
 #include "gzb_cost.cuh"
+#include "gzb_traceback.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -1068,6 +1069,9 @@ struct gzb_engine {
       model_d, mae_acc, log_x, log_y, log_ctr;
   uint64_t prev_cells_n = 0;
   DBuf codeflag;
+  // build results step
+  DBuf tb_cols, tb_band_off, tb_band, tb_ops_bytes, tb_ops_off, tb_rows, tb_rows_off, tb_walk_cap,
+      tb_walk_off, tb_ops, tb_row_meta, tb_walk, tb_walk_n, tb_score, tb_p0, tb_p1, tb_out;
   uint64_t pred_n = 0;       // extensions with a prediction in epred (last run)
   DBuf enb;                  // per surviving hit: chained neighbours (cost feature)
   int tile[3][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}};  // [schedule][which], -1 = default
@@ -1269,7 +1273,10 @@ extern "C" int gzb_engine_destroy(gzb_engine *e) {
                  &e->hits_copy, &e->elen0, &e->elen1, &e->eqid, &e->efeat, &e->epred,
                  &e->ecells, &e->okeys, &e->okeys2, &e->oidx, &e->oidx2, &e->queue,
                  &e->prev_cells, &e->model_d, &e->mae_acc, &e->log_x, &e->log_y,
-                 &e->log_ctr, &e->enb, &e->codeflag};
+                 &e->log_ctr, &e->enb, &e->codeflag, &e->tb_cols, &e->tb_band_off,
+                 &e->tb_band, &e->tb_ops_bytes, &e->tb_ops_off, &e->tb_rows, &e->tb_rows_off,
+                 &e->tb_walk_cap, &e->tb_walk_off, &e->tb_ops, &e->tb_row_meta, &e->tb_walk,
+                 &e->tb_walk_n, &e->tb_score, &e->tb_p0, &e->tb_p1, &e->tb_out};
   for (DBuf *b : all) b->release();
   cudaFree(e->spill);
   cudaFree(e->gcounters);
@@ -1912,6 +1919,89 @@ extern "C" int gzb_engine_get_results(gzb_engine *e, uint32_t *counts, gzb_resul
   GZB_CUDA(cudaMemcpyAsync(counts, e->counts.p, 4 * (uint64_t)e->nq, cudaMemcpyDeviceToHost, s));
   GZB_CUDA(cudaMemcpyAsync(results, e->results.p,
                            sizeof(gzb_result) * (uint64_t)e->nq * e->params.max_number_results,
+                           cudaMemcpyDeviceToHost, s));
+  GZB_CUDA(cudaStreamSynchronize(s));
+  return GZB_OK;
+}
+
+namespace {
+// exclusive scan of n + 1 entries (the last one zeroed first); returns the total
+int scan_total(gzb_engine *e, DBuf &in, DBuf &out, uint64_t n, cudaStream_t s,
+               uint64_t *total) {
+  GZB_TRY(out.ensure(8 * (n + 1)));
+  GZB_CUDA(cudaMemsetAsync(in.as<uint64_t>() + n, 0, 8, s));
+  GZB_TRY(exclusive_sum(e, in.as<uint64_t>(), out.as<uint64_t>(), n + 1, s));
+  GZB_CUDA(cudaMemcpyAsync(total, out.as<uint64_t>() + n, 8, cudaMemcpyDeviceToHost, s));
+  GZB_CUDA(cudaStreamSynchronize(s));
+  return GZB_OK;
+}
+}  // namespace
+
+extern "C" int gzb_engine_build_alignments(gzb_engine *e, uint32_t *counts,
+                                           gzb_alignment *alignments, void *stream) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(e->have_db && e->have_queries && counts && alignments, GZB_ERR_INVALID,
+            "build alignments needs the chunk, the queries and output arrays");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int b = e->params.max_number_results;
+  const uint64_t n_slots = (uint64_t)e->nq * b, n_sides = 2 * n_slots;
+  TbArgs a;
+  a.query = e->q_buf.as<uint8_t>() + kPad;
+  a.db = e->db_buf.as<uint8_t>() + kPad;
+  a.matrix32 = e->matrix32.as<int32_t>();
+  a.q_offsets = e->q_offsets.as<uint32_t>();
+  a.q_lengths = e->q_lengths.as<uint32_t>();
+  a.results = e->results.as<gzb_result>();
+  a.counts = e->counts.as<uint32_t>();
+  a.nq = e->nq;
+  a.max_results = b;
+  a.chunk_id = e->chunk_id;
+  a.delim = e->params.delimiter;
+  a.gap_open = e->params.gap_open;
+  a.gap_ext = e->params.gap_extension;
+  a.cutoff = e->params.gapped_cutoff;
+  // band columns per side, then the DP's storage per side
+  GZB_TRY(e->tb_cols.ensure(8 * (n_sides + 1)));
+  tb_band_kernel<<<grid1(n_sides, 256), 256, 0, s>>>(a, n_sides, e->tb_cols.as<uint64_t>());
+  GZB_CUDA(cudaGetLastError());
+  uint64_t band_total = 0;
+  GZB_TRY(scan_total(e, e->tb_cols, e->tb_band_off, n_sides, s, &band_total));
+  GZB_TRY(e->tb_band.ensure(sizeof(int2) * (band_total + 1)));
+  GZB_TRY(e->tb_ops_bytes.ensure(8 * (n_sides + 1)));
+  GZB_TRY(e->tb_rows.ensure(8 * (n_sides + 1)));
+  GZB_TRY(e->tb_walk_cap.ensure(8 * (n_sides + 1)));
+  tb_count_kernel<<<grid1(n_sides, 128), 128, 0, s>>>(
+      a, n_sides, e->tb_band_off.as<uint64_t>(), e->tb_band.as<int2>(),
+      e->tb_ops_bytes.as<uint64_t>(), e->tb_rows.as<uint64_t>(), e->tb_walk_cap.as<uint64_t>());
+  GZB_CUDA(cudaGetLastError());
+  uint64_t ops_total = 0, rows_total = 0, walk_total = 0;
+  GZB_TRY(scan_total(e, e->tb_ops_bytes, e->tb_ops_off, n_sides, s, &ops_total));
+  GZB_TRY(scan_total(e, e->tb_rows, e->tb_rows_off, n_sides, s, &rows_total));
+  GZB_TRY(scan_total(e, e->tb_walk_cap, e->tb_walk_off, n_sides, s, &walk_total));
+  GZB_TRY(e->tb_ops.ensure(ops_total + 1));
+  GZB_TRY(e->tb_row_meta.ensure(8 * (rows_total + 1)));
+  GZB_TRY(e->tb_walk.ensure(walk_total + 1));
+  GZB_TRY(e->tb_walk_n.ensure(4 * (n_sides + 1)));
+  GZB_TRY(e->tb_score.ensure(4 * (n_sides + 1)));
+  GZB_TRY(e->tb_p0.ensure(4 * (n_sides + 1)));
+  GZB_TRY(e->tb_p1.ensure(4 * (n_sides + 1)));
+  GZB_TRY(e->tb_out.ensure(sizeof(gzb_alignment) * (n_slots + 1)));
+  // a cell the DP prunes keeps op 0, as in a fresh GappedExtender
+  GZB_CUDA(cudaMemsetAsync(e->tb_ops.p, 0, ops_total + 1, s));
+  tb_walk_kernel<<<grid1(n_sides, 128), 128, 0, s>>>(
+      a, n_sides, e->tb_band_off.as<uint64_t>(), e->tb_band.as<int2>(),
+      e->tb_ops_off.as<uint64_t>(), e->tb_ops.as<uint8_t>(), e->tb_rows_off.as<uint64_t>(),
+      e->tb_row_meta.as<uint32_t>(), e->tb_walk_off.as<uint64_t>(), e->tb_walk.as<uint8_t>(),
+      e->tb_walk_n.as<uint32_t>(), e->tb_score.as<int32_t>(), e->tb_p0.as<int32_t>(),
+      e->tb_p1.as<int32_t>());
+  GZB_CUDA(cudaGetLastError());
+  tb_combine_kernel<<<grid1(n_slots, 128), 128, 0, s>>>(
+      a, n_slots, e->tb_walk_off.as<uint64_t>(), e->tb_walk.as<uint8_t>(),
+      e->tb_walk_n.as<uint32_t>(), e->tb_score.as<int32_t>(), e->tb_p0.as<int32_t>(),
+      e->tb_p1.as<int32_t>(), e->tb_out.as<gzb_alignment>());
+  GZB_CUDA(cudaGetLastError());
+  GZB_CUDA(cudaMemcpyAsync(counts, e->counts.p, 4 * (uint64_t)e->nq, cudaMemcpyDeviceToHost, s));
+  GZB_CUDA(cudaMemcpyAsync(alignments, e->tb_out.p, sizeof(gzb_alignment) * n_slots,
                            cudaMemcpyDeviceToHost, s));
   GZB_CUDA(cudaStreamSynchronize(s));
   return GZB_OK;

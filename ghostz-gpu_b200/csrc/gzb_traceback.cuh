@@ -1,0 +1,40 @@
+// gzb_traceback.cuh -- kernels of the build results step (gzb_traceback.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "ghostz_b200.h"
+
+namespace gzb {
+
+// Inputs shared by the build results kernels.  Sides are numbered
+// 2 * slot + {0 reverse, 1 forward}, slot = query * max_results + rank.
+struct TbArgs {
+  const uint8_t *query;  // concatenated queries (query id q starts at q_offsets[q])
+  const uint8_t *db;     // the resident chunk
+  const int32_t *matrix32;
+  const uint32_t *q_offsets, *q_lengths;
+  const gzb_result *results;
+  const uint32_t *counts;
+  uint32_t nq;
+  int max_results;
+  int32_t chunk_id;
+  int delim, gap_open, gap_ext, cutoff;
+};
+
+__global__ void tb_band_kernel(TbArgs a, uint64_t n_sides, uint64_t *band_cols);
+__global__ void tb_count_kernel(TbArgs a, uint64_t n_sides, const uint64_t *band_off,
+                                int2 *band, uint64_t *ops_bytes, uint64_t *rows,
+                                uint64_t *walk_cap);
+__global__ void tb_walk_kernel(TbArgs a, uint64_t n_sides, const uint64_t *band_off,
+                               int2 *band, const uint64_t *ops_off, uint8_t *ops,
+                               const uint64_t *rows_off, uint32_t *row_meta,
+                               const uint64_t *walk_off, uint8_t *walk, uint32_t *walk_n,
+                               int32_t *side_score, int32_t *side_p0, int32_t *side_p1);
+__global__ void tb_combine_kernel(TbArgs a, uint64_t n_slots, const uint64_t *walk_off,
+                                  const uint8_t *walk, const uint32_t *walk_n,
+                                  const int32_t *side_score, const int32_t *side_p0,
+                                  const int32_t *side_p1, gzb_alignment *out);
+
+}  // namespace gzb

@@ -109,6 +109,7 @@ def _declare(L):
         "gzb_engine_set_tile": [V, C.c_int, C.c_int, C.c_int],
         "gzb_engine_get_tile": [V, C.c_int, C.c_int, V],
         "gzb_engine_get_extension_costs": [V, V, V, C.c_uint64, V, V],
+        "gzb_engine_build_alignments": [V, V, V, V],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -284,6 +285,12 @@ RESULT_DTYPE = np.dtype([
     ("hit_q", "<u4"), ("hit_d", "<u4"), ("start_q", "<u4"), ("start_d", "<u4"),
     ("end_q", "<u4"), ("end_d", "<u4"),
 ])
+ALIGNMENT_DTYPE = np.dtype([
+    ("chunk_id", "<i4"), ("subject_id", "<i4"), ("score", "<i4"),
+    ("hit_q", "<u4"), ("hit_d", "<u4"), ("start_q", "<u4"), ("start_d", "<u4"),
+    ("end_q", "<u4"), ("end_d", "<u4"), ("alignment_length", "<u4"), ("mismatches", "<u4"),
+    ("gap_openings", "<u4"), ("gap_extensions", "<u4"), ("extension_score", "<i4"),
+])
 COUNTER_NAMES = ("distance_seeds", "ungapped_seeds", "ungapped_hits",
                  "chained_hits", "gapped_extensions", "gapped_cells", "gapped_fallbacks",
                  "ungapped_steps", "kernel_launches")
@@ -375,6 +382,18 @@ class PresearchEngine:
                                            _stream_or_null(stream)))
         res = res.reshape(self.number_queries, b)
         return [res[i, :counts[i]].copy() for i in range(self.number_queries)]
+
+    def build_alignments(self, stream=None):
+        """The build results step for the resident chunk: per query its
+        results with alignment length, mismatches, gap openings and gap
+        extensions (alignment_length 0 for results of other chunks)."""
+        b = int(self.params[0]["max_number_results"])
+        counts = np.zeros(self.number_queries, np.uint32)
+        out = np.zeros(self.number_queries * b, ALIGNMENT_DTYPE)
+        check(lib().gzb_engine_build_alignments(self.h, hptr(counts), hptr(out),
+                                                _stream_or_null(stream)))
+        out = out.reshape(self.number_queries, b)
+        return [out[i, :counts[i]].copy() for i in range(self.number_queries)]
 
     def counters(self):
         c = (C.c_uint64 * 9)()

@@ -279,6 +279,33 @@ int gzb_engine_reset_results(gzb_engine *e, void *stream);
  * valid entries, best first).  Synchronises `stream`. */
 int gzb_engine_get_results(gzb_engine *e, uint32_t *counts,
                            gzb_result *results, void *stream);
+/* Alignment statistics of one merged result (AlignerCommon::Result,
+ * src/aligner_common.h:80-92): the result's fields plus what
+ * AlignerCommon::BuildResult (src/aligner_common.h:275-340) derives from the
+ * edit path of both gapped extensions.  alignment_length == 0 marks a result
+ * of another chunk (not computed by this call). */
+typedef struct {
+  int32_t chunk_id;
+  int32_t subject_id;
+  int32_t score;
+  uint32_t hit_q, hit_d;
+  uint32_t start_q, start_d;
+  uint32_t end_q, end_d;
+  uint32_t alignment_length;  /* edit ops of the joined path */
+  uint32_t mismatches;
+  uint32_t gap_openings;
+  uint32_t gap_extensions;
+  int32_t extension_score;    /* both sides' scores again (equals score) */
+} gzb_alignment;
+/* The build results step for the resident chunk
+ * (AlignerBuildResultsThread::Run, src/aligner_build_results_thread.h:64-190):
+ * re-extends both sides of every merged result of this chunk with its edit
+ * path (GappedExtender::ExtendOneSide, src/gapped_extender.cpp:70-304, and
+ * PickOptimalPath, :473-531) and fills alignments[number_queries *
+ * max_number_results] (row i holds counts[i] entries, in result order) on
+ * the host.  Synchronises `stream`. */
+int gzb_engine_build_alignments(gzb_engine *e, uint32_t *counts, gzb_alignment *alignments,
+                                void *stream);
 int gzb_engine_get_counters(gzb_engine *e, gzb_counters *out);
 /* Device-side ungapped survivors of the last presearch, sorted by
  * (query, database position, query position): copies up to `capacity`

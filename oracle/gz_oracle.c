@@ -263,6 +263,250 @@ int gzo_gapped_one_side(const gzo_params *p, const uint8_t *seq0,
 }
 
 /* ------------------------------------------------------------------ */
+
+/* Edit ops of the DP (src/gapped_extender.h:46-52) */
+enum { TB_SUB = 0, TB_GAP0 = 1, TB_GAP1 = 2, TB_EXT0 = 4, TB_EXT1 = 8 };
+
+/* GappedExtender::ExtendOneSide with an edit script
+ * (src/gapped_extender.cpp:70-304): the score-only recurrence plus one op
+ * byte per kept cell, stored per row for the band's columns; then
+ * PickOptimalPath (:473-531) from the best cell back to the origin. */
+int gzo_gapped_one_side_edits(const gzo_params *p, const uint8_t *seq0,
+                              const uint8_t *seq1, int reversed, int cutoff,
+                              int *best_score, int *best_pos0, int *best_pos1,
+                              uint8_t *ops, size_t ops_cap, size_t *n_ops) {
+  const int inc = reversed ? -1 : 1;
+  const int delim = p->delimiter;
+  const int n = p->number_letters;
+  const int gap_ext = p->gap_extension;
+  const int gap_init = p->gap_open + p->gap_extension;
+  *best_score = 0;
+  *best_pos0 = -inc;
+  *best_pos1 = -inc;
+  *n_ops = 0;
+  if (seq0[0] == delim || seq1[0] == delim) return 0;
+  int len0 = 0, len1 = 0;
+  while (seq0[len0 * inc] != delim) ++len0;
+  while (seq1[len1 * inc] != delim) ++len1;
+  int *best = (int *)xmalloc(sizeof(int) * (size_t)(len0 + 2));
+  int *gap = (int *)xmalloc(sizeof(int) * (size_t)(len0 + 2));
+  /* per row r: ops of columns [row_start[r], row_start[r] + row_len[r]) at
+   * arena + row_off[r]; op bytes of pruned cells stay unset (never read) */
+  size_t arena_cap = 1024, arena_used = 0;
+  uint8_t *arena = (uint8_t *)calloc(arena_cap, 1);
+  if (!arena) abort();
+  size_t *row_off = (size_t *)xmalloc(sizeof(size_t) * (size_t)(len1 + 1));
+  int *row_start = (int *)xmalloc(sizeof(int) * (size_t)(len1 + 1));
+  int score = -gap_init, col = 1, pos0 = 0;
+  best[0] = 0;
+  gap[0] = -gap_init;
+  for (; seq0[pos0] != delim; ++col, pos0 += inc) {
+    if (score < -cutoff) break;
+    best[col] = score;
+    gap[col] = score - gap_init;
+    score -= gap_ext;
+  }
+  int band_start = 0, band_end;
+  if (seq0[pos0] != delim) {
+    best[col] = GZO_INIT_SCORE;
+    gap[col] = GZO_INIT_SCORE;
+    band_end = col + 1;
+  } else {
+    band_end = col;
+  }
+  int max_score = 0, max_pos0 = -inc, max_pos1 = -inc;
+  int pos1, r = 0;
+  for (pos1 = 0; seq1[pos1] != delim; pos1 += inc, ++r) {
+    /* room for this row: the band can grow by at most the remaining seq0 */
+    const size_t need = (size_t)(len0 + 2 - band_start);
+    while (arena_used + need > arena_cap) {
+      arena = (uint8_t *)realloc(arena, arena_cap * 2);
+      if (!arena) abort();
+      memset(arena + arena_cap, 0, arena_cap);
+      arena_cap *= 2;
+    }
+    row_off[r] = arena_used;
+    row_start[r] = band_start;
+    uint8_t *row_ops = arena + arena_used - band_start; /* indexed by column */
+    const int32_t *mrow = p->score_matrix + seq1[pos1] * n;
+    pos0 = band_start * inc;
+    int diag = best[band_start];
+    if (max_score - gap[band_start] > cutoff)
+      best[band_start] = GZO_INIT_SCORE;
+    else
+      best[band_start] = gap[band_start];
+    int row_gap = best[band_start] - gap_init;
+    gap[band_start] -= gap_ext;
+    row_ops[band_start] = TB_GAP0 + TB_EXT0;
+    int last_kept = band_start;
+    for (col = band_start + 1; col < band_end; ++col, pos0 += inc) {
+      int s = diag + mrow[seq0[pos0]];
+      const int vgap = gap[col];
+      diag = best[col];
+      int op = TB_SUB;
+      if (s < vgap) { op = TB_GAP0; s = vgap; }
+      if (s < row_gap) { op = TB_GAP1; s = row_gap; }
+      if (max_score - s > cutoff) {
+        if (band_start + 1 == col) ++band_start;
+        best[col] = GZO_INIT_SCORE;
+        gap[col] = GZO_INIT_SCORE;
+        row_gap = GZO_INIT_SCORE;
+      } else {
+        last_kept = col;
+        if (s > max_score) {
+          max_score = s;
+          max_pos0 = pos0;
+          max_pos1 = pos1;
+        }
+        /* a tie between opening and extending counts as extending (:426-437) */
+        if (vgap - gap_ext < s - gap_init) {
+          gap[col] = s - gap_init;
+        } else {
+          gap[col] = vgap - gap_ext;
+          op += TB_EXT0;
+        }
+        if (row_gap - gap_ext < s - gap_init) {
+          row_gap = s - gap_init;
+        } else {
+          row_gap -= gap_ext;
+          op += TB_EXT1;
+        }
+        row_ops[col] = (uint8_t)op;
+        best[col] = s;
+      }
+    }
+    if (band_start + 1 == band_end) { ++r; break; }
+    if (last_kept < band_end - 1) {
+      band_end = last_kept + 1;
+    } else {
+      while (row_gap >= max_score - cutoff && seq0[pos0] != delim) {
+        best[band_end] = row_gap;
+        gap[band_end] = row_gap - gap_init;
+        row_ops[band_end] = TB_GAP0 + TB_EXT0;
+        row_gap -= gap_ext;
+        ++band_end;
+        pos0 += inc;
+      }
+    }
+    if (seq0[pos0] != delim) {
+      best[band_end] = GZO_INIT_SCORE;
+      gap[band_end] = GZO_INIT_SCORE;
+      ++band_end;
+    }
+    /* the row keeps (final band end - its start) bytes, sentinel slot
+     * included, as the reference's gap-state accounting does (:464-466) */
+    arena_used += (size_t)(band_end - row_start[r]);
+  }
+  *best_score = max_score;
+  *best_pos0 = max_pos0;
+  *best_pos1 = max_pos1;
+  /* PickOptimalPath: positions in units of inc (row = pos1 * inc, c0 = pos0 * inc) */
+  size_t m = 0;
+  int ok = 1;
+#define TB_PUSH(o)                          \
+  do {                                      \
+    if (m >= ops_cap) { ok = 0; goto tb_done; } \
+    ops[m++] = (uint8_t)(o);                \
+  } while (0)
+  {
+    int op = TB_SUB;
+    int rr = max_pos1 * inc, c0 = max_pos0 * inc;
+    while (rr >= 0 && c0 >= 0) {
+      const int next = arena[row_off[rr] + (size_t)(c0 + 1 - row_start[rr])];
+      if (op == TB_GAP0) {
+        op = next & 3;
+        if (next & TB_EXT0) op = TB_GAP0;
+      } else if (op == TB_GAP1) {
+        op = next & 3;
+        if (next & TB_EXT1) op = TB_GAP1;
+      } else {
+        op = next & 3;
+      }
+      if (op == TB_GAP0) {
+        TB_PUSH(GZO_OP_GAP0);
+        --rr;
+      } else if (op == TB_GAP1) {
+        TB_PUSH(GZO_OP_GAP1);
+        --c0;
+      } else {
+        TB_PUSH(GZO_OP_SUB);
+        --rr;
+        --c0;
+      }
+    }
+    for (; rr >= 0; --rr) TB_PUSH(GZO_OP_GAP0);
+    for (; c0 >= 0; --c0) TB_PUSH(GZO_OP_GAP1);
+  }
+tb_done:
+#undef TB_PUSH
+  /* the path was collected from the best cell back to the origin; a forward
+   * side is reversed to run from the origin (EditBlocks::Reverse) */
+  if (ok && inc > 0)
+    for (size_t i = 0, j = m ? m - 1 : 0; i < j; ++i, --j) {
+      const uint8_t t = ops[i];
+      ops[i] = ops[j];
+      ops[j] = t;
+    }
+  *n_ops = m;
+  free(best);
+  free(gap);
+  free(arena);
+  free(row_off);
+  free(row_start);
+  return ok ? 0 : -1;
+}
+
+/* AlignerBuildResultsThread::Run (src/aligner_build_results_thread.h:110-160)
+ * and AlignerCommon::BuildResult (src/aligner_common.h:275-340). */
+int gzo_build_alignment(const gzo_params *p, const uint8_t *query, uint32_t hit_q,
+                        const uint8_t *db, uint32_t hit_d, gzo_alignment *out) {
+  size_t cap = 1 << 16;
+  uint8_t *rev = (uint8_t *)xmalloc(cap), *fwd = (uint8_t *)xmalloc(cap);
+  size_t nr = 0, nf = 0;
+  int sr, r0, r1, sf, f0, f1;
+  int rc = gzo_gapped_one_side_edits(p, query + hit_q - 1, db + hit_d - 1, 1, p->gapped_cutoff,
+                                     &sr, &r0, &r1, rev, cap, &nr);
+  if (rc == 0)
+    rc = gzo_gapped_one_side_edits(p, query + hit_q, db + hit_d, 0, p->gapped_cutoff, &sf, &f0,
+                                   &f1, fwd, cap, &nf);
+  if (rc != 0) {
+    free(rev);
+    free(fwd);
+    return -1;
+  }
+  out->score = sr + sf;
+  out->start_q = hit_q - 1 + (uint32_t)r0;
+  out->start_d = hit_d - 1 + (uint32_t)r1;
+  out->end_q = hit_q + (uint32_t)f0;
+  out->end_d = hit_d + (uint32_t)f1;
+  /* the reverse side's path runs from the hit toward the start: reversed,
+   * it starts at `start`; the forward path follows */
+  uint32_t qp = out->start_q, dp = out->start_d, mm = 0, o = 0, e = 0;
+  int prev = GZO_OP_SUB;
+  for (size_t i = 0; i < nr + nf; ++i) {
+    const int op = i < nr ? rev[nr - 1 - i] : fwd[i - nr];
+    if (op == GZO_OP_SUB) {
+      if (query[qp] != db[dp]) ++mm;
+      ++qp;
+      ++dp;
+    } else if (op == GZO_OP_GAP0) {
+      if (prev != GZO_OP_GAP0) ++o; else ++e;
+      ++dp;
+    } else {
+      if (prev != GZO_OP_GAP1) ++o; else ++e;
+      ++qp;
+    }
+    prev = op;
+  }
+  out->alignment_length = (uint32_t)(nr + nf);
+  out->mismatches = mm;
+  out->gap_openings = o;
+  out->gap_extensions = e;
+  free(rev);
+  free(fwd);
+  return 0;
+}
+
 /* Chain filter.  Restates ChainFilter::Filter / Connected
  * (src/chain_filter.cpp:24-99).  Hits are ordered by database position;
  * the reference's std::sort leaves equal database positions in an

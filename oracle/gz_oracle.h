@@ -63,6 +63,34 @@ int gzo_gapped_one_side(const gzo_params *p, const uint8_t *seq0,
                         const uint8_t *seq1, int reversed, int cutoff,
                         int *best_score, int *best_pos0, int *best_pos1,
                         uint64_t *cells);
+/* Affine X-drop extension with its edit path
+ * (GappedExtender::ExtendOneSide with EditBlocks, src/gapped_extender.cpp:70-304,
+ * and PickOptimalPath, :473-531).  Same score and positions as
+ * gzo_gapped_one_side; ops[0..*n_ops) receives the path expanded one op per
+ * aligned column in EditBlocks order (EditBlocks::ToVector,
+ * src/edit_blocks.cpp): GZO_OP_GAP0 (gap in seq0: a seq1 residue alone),
+ * GZO_OP_SUB, GZO_OP_GAP1.  Returns -1 when ops_cap is too small. */
+#define GZO_OP_GAP0 0
+#define GZO_OP_SUB 1
+#define GZO_OP_GAP1 2
+int gzo_gapped_one_side_edits(const gzo_params *p, const uint8_t *seq0,
+                              const uint8_t *seq1, int reversed, int cutoff,
+                              int *best_score, int *best_pos0, int *best_pos1,
+                              uint8_t *ops, size_t ops_cap, size_t *n_ops);
+/* Alignment statistics of one presearch result, as
+ * AlignerCommon::BuildResult computes them (src/aligner_common.h:275-340)
+ * after AlignerBuildResultsThread::Run (src/aligner_build_results_thread.h:
+ * 110-160) joined the reversed reverse-side path and the forward path.
+ * query / db: the concatenated sequences; hit_q is the hit's position in
+ * the concatenated query buffer, hit_d in the chunk.  Returns -1 when a
+ * side's path does not fit the scratch. */
+typedef struct {
+  int32_t score;
+  uint32_t start_q, start_d, end_q, end_d;  /* concatenated coordinates */
+  uint32_t alignment_length, mismatches, gap_openings, gap_extensions;
+} gzo_alignment;
+int gzo_build_alignment(const gzo_params *p, const uint8_t *query, uint32_t hit_q,
+                        const uint8_t *db, uint32_t hit_d, gzo_alignment *out);
 /* Chain filter over the hits of one query.  q/d are in place; returns the
  * number of hits kept (sorted by database position, ties by query pos). */
 size_t gzo_chain_filter(const gzo_params *p, const uint8_t *query,

@@ -70,6 +70,11 @@ class Oracle:
                                                 C.c_uint32, C.c_int, C.c_int]
         L.gzo_gapped_one_side.argtypes = [C.c_void_p, u8p, u8p, C.c_int, C.c_int,
                                           i32p, i32p, i32p, C.POINTER(C.c_uint64)]
+        L.gzo_gapped_one_side_edits.argtypes = [C.c_void_p, u8p, u8p, C.c_int, C.c_int,
+                                                i32p, i32p, i32p, u8p, C.c_size_t,
+                                                C.POINTER(C.c_size_t)]
+        L.gzo_build_alignment.argtypes = [C.c_void_p, u8p, C.c_uint32, u8p, C.c_uint32,
+                                          C.c_void_p]
         L.gzo_chain_filter.argtypes = [C.c_void_p, u8p, C.c_uint32, C.c_int, u8p,
                                        u32p, u32p, C.c_size_t]
         L.gzo_chain_filter.restype = C.c_size_t
@@ -137,6 +142,38 @@ class Oracle:
             C.cast(C.c_void_p(s1.ctypes.data + int(p1)), u8p), int(reversed_), int(cutoff),
             C.byref(b), C.byref(q), C.byref(d), C.byref(cells))
         return b.value, q.value, d.value, cells.value
+
+    def gapped_one_side_edits(self, params, seq0, p0, seq1, p1, reversed_, cutoff):
+        """(score, best pos0, best pos1, ops) of the traceback extension."""
+        pr = _Params(params)
+        s0 = np.ascontiguousarray(seq0, dtype=np.uint8)
+        s1 = np.ascontiguousarray(seq1, dtype=np.uint8)
+        b, q, d = C.c_int32(), C.c_int32(), C.c_int32()
+        cap = 1 << 18
+        ops = np.zeros(cap, np.uint8)
+        n = C.c_size_t()
+        rc = self.L.gzo_gapped_one_side_edits(
+            pr.ptr, C.cast(C.c_void_p(s0.ctypes.data + int(p0)), u8p),
+            C.cast(C.c_void_p(s1.ctypes.data + int(p1)), u8p), int(reversed_), int(cutoff),
+            C.byref(b), C.byref(q), C.byref(d), _p(ops, u8p), cap, C.byref(n))
+        assert rc == 0
+        return b.value, q.value, d.value, ops[:n.value].copy()
+
+    def build_alignment(self, params, query, hit_q, db, hit_d):
+        """AlignerCommon::BuildResult statistics of one hit (concatenated
+        coordinates): a dict with score, start_q, start_d, end_q, end_d,
+        alignment_length, mismatches, gap_openings, gap_extensions."""
+        pr = _Params(params)
+        q = np.ascontiguousarray(query, dtype=np.uint8)
+        d = np.ascontiguousarray(db, dtype=np.uint8)
+        out = (C.c_uint32 * 9)()
+        rc = self.L.gzo_build_alignment(pr.ptr, _p(q, u8p), int(hit_q), _p(d, u8p), int(hit_d),
+                                        C.byref(out))
+        assert rc == 0
+        v = list(out)
+        v[0] = C.c_int32(v[0]).value
+        return dict(zip(("score", "start_q", "start_d", "end_q", "end_d", "alignment_length",
+                         "mismatches", "gap_openings", "gap_extensions"), v))
 
     def chain_filter(self, params, query, qlen, cutoff, db, hq, hd):
         pr = _Params(params)
@@ -238,6 +275,9 @@ class Reference:
         L.gzr_ungapped_one_side.argtypes = [C.c_void_p, u8p, u8p, C.c_int, C.c_int]
         L.gzr_gapped_one_side.argtypes = [C.c_void_p, u8p, C.c_uint32, u8p, C.c_int,
                                           C.c_int, i32p, i32p, i32p]
+        L.gzr_gapped_one_side_edits.argtypes = [C.c_void_p, u8p, C.c_uint32, u8p, C.c_int,
+                                                C.c_int, i32p, i32p, i32p, u8p, C.c_size_t,
+                                                C.POINTER(C.c_size_t)]
         L.gzr_chain_filter.argtypes = [C.c_void_p, u8p, C.c_uint32, C.c_int, u8p, u32p,
                                        u32p, C.c_size_t]
         L.gzr_chain_filter.restype = C.c_size_t
@@ -293,6 +333,21 @@ class Reference:
             C.cast(C.c_void_p(s1.ctypes.data + int(p1)), u8p), int(reversed_), int(cutoff),
             C.byref(b), C.byref(q), C.byref(d))
         return b.value, q.value, d.value
+
+    def gapped_one_side_edits(self, params, seq0, p0, len0, seq1, p1, reversed_, cutoff):
+        pr = _Params(params)
+        s0 = np.ascontiguousarray(seq0, dtype=np.uint8)
+        s1 = np.ascontiguousarray(seq1, dtype=np.uint8)
+        b, q, d = C.c_int32(), C.c_int32(), C.c_int32()
+        cap = 1 << 18
+        ops = np.zeros(cap, np.uint8)
+        n = C.c_size_t()
+        rc = self.L.gzr_gapped_one_side_edits(
+            pr.ptr, C.cast(C.c_void_p(s0.ctypes.data + int(p0)), u8p), len0,
+            C.cast(C.c_void_p(s1.ctypes.data + int(p1)), u8p), int(reversed_), int(cutoff),
+            C.byref(b), C.byref(q), C.byref(d), _p(ops, u8p), cap, C.byref(n))
+        assert rc == 0
+        return b.value, q.value, d.value, ops[:n.value].copy()
 
     def chain_filter(self, params, query, qlen, cutoff, db, hq, hd):
         pr = _Params(params)

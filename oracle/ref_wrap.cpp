@@ -93,6 +93,27 @@ int gzr_gapped_one_side(const gzo_params *p, const uint8_t *seq0,
   return 0;
 }
 
+// GappedExtender::ExtendOneSide with EditBlocks (the traceback the build
+// results step uses); ops receive EditBlocks::ToVector().  Returns -1 when
+// ops_cap is too small.
+int gzr_gapped_one_side_edits(const gzo_params *p, const uint8_t *seq0,
+                              uint32_t seq0_length, const uint8_t *seq1,
+                              int reversed, int cutoff, int *best_score,
+                              int *best_pos0, int *best_pos1, uint8_t *ops,
+                              size_t ops_cap, size_t *n_ops) {
+  ScoreMatrix m = make_matrix(p);
+  GappedExtender e;
+  EditBlocks blocks;
+  e.ExtendOneSide(seq0, seq0_length, seq1, p->delimiter, reversed != 0, m,
+                  p->gap_open, p->gap_extension, cutoff, best_score,
+                  best_pos0, best_pos1, &blocks);
+  std::vector<EditBlocks::EditOpType> v = blocks.ToVector();
+  *n_ops = v.size();
+  if (v.size() > ops_cap) return -1;
+  for (size_t i = 0; i < v.size(); ++i) ops[i] = (uint8_t)v[i];
+  return 0;
+}
+
 size_t gzr_chain_filter(const gzo_params *p, const uint8_t *query,
                         uint32_t query_length, int cutoff, const uint8_t *db,
                         uint32_t *hit_q, uint32_t *hit_d, size_t n) {

@@ -220,3 +220,44 @@ def test_cutoffs_match_reference(reference, params):
         assert (np.float32(ml), np.float32(mk)) == (np.float32(lam), np.float32(k))
         assert reference.cutoffs(lam, k) == (P.normalized_cutoff_to_nominal(7.0, ml),
                                              P.normalized_to_nominal(22.0, ml, mk))
+
+
+# --- traceback (build results) ------------------------------------------------
+def test_edit_path_known_answer(oracle):
+    # test/gapped_extender_test.cpp:49-94: AGTCAC vs AGCAG, forward, open 0 /
+    # extend 1, no X-drop -> 7 at (4, 3) with path S S G1 S S
+    p = dna_params()
+    s0, s1 = dna("AGTCAC"), dna("AGCAG")
+    score, q, d, ops = oracle.gapped_one_side_edits(p, s0, 1, s1, 1, False, 2**31 - 1)
+    assert (score, q, d) == (7, 4, 3)
+    assert list(ops[:5]) == [1, 1, 2, 1, 1]
+
+
+@pytest.mark.parametrize("seed", [20, 21])
+def test_edit_path_matches_reference(oracle, reference, params, seed):
+    rng = np.random.default_rng(seed)
+    for t in range(120):
+        a, b = _pair(rng, int(rng.integers(5, 500)), rng.uniform(0.25, 1.0))
+        pa = int(rng.integers(1, len(a) - 1))
+        pb = int(np.clip(pa + rng.integers(-5, 6), 1, len(b) - 2))
+        cutoff = int(rng.choice([0, 5, 15, 26, 40, 2**31 - 1]))
+        for rev in (False, True):
+            len0 = pa if rev else len(a) - pa
+            r = reference.gapped_one_side_edits(params, a, pa, len0, b, pb, rev, cutoff)
+            m = oracle.gapped_one_side_edits(params, a, pa, b, pb, rev, cutoff)
+            assert m[:3] == r[:3], (t, rev, cutoff)
+            assert np.array_equal(m[3], r[3]), (t, rev, cutoff)
+            # same score and end point as the score-only extension
+            assert m[:3] == oracle.gapped_one_side(params, a, pa, b, pb, rev, cutoff)[:3]
+
+
+def test_alignment_statistics_by_hand(oracle):
+    # forward path S S G1 S S after a reverse side that stops at once: the
+    # alignment AG-CA against AGTCA (query AGTCAC, hit at its first residue)
+    p = dna_params()
+    p["gapped_cutoff"] = 2**31 - 1
+    q, d = dna("AGTCAC"), dna("AGCAG")
+    a = oracle.build_alignment(p, q, 1, d, 1)
+    assert (a["score"], a["start_q"], a["start_d"], a["end_q"], a["end_d"]) == (7, 1, 1, 5, 4)
+    assert (a["alignment_length"], a["mismatches"], a["gap_openings"],
+            a["gap_extensions"]) == (5, 0, 1, 0)
