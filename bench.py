@@ -177,6 +177,26 @@ def _oracle_range(args):
     return counters["search_seconds"]
 
 
+def build_results_cpu(db, q, aligned, budget_s=10.0):
+    """The oracle's build results step (traceback + BuildResult statistics)
+    on one core over the first merged results until budget_s has passed;
+    alignments per second."""
+    import oracle as O
+    from gzb import params as P
+    o, p = O.Oracle(), P.make_params()
+    n, t0 = 0, time.time()
+    for qi, rows in enumerate(aligned):
+        for a in rows:
+            o.build_alignment(p, q.codes, int(q.offsets[qi]) + int(a["hit_q"]), db.codes,
+                              int(a["hit_d"]))
+            n += 1
+        if time.time() - t0 > budget_s:
+            break
+    el = time.time() - t0
+    return {"value": n / el, "unit": "alignments/s", "cores": 1, "kind": "port",
+            "sample": f"{n} alignments of the first {qi + 1} queries in {el:.2f} s"}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
@@ -486,6 +506,7 @@ def main():
         v, el, sample = cpu_baseline(db, q, n_queries=args.cpu_queries, processes=1)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
                                 "sample": sample}
+        line["build_results"]["cpu_baseline"] = build_results_cpu(db, q, aligned)
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()
