@@ -251,12 +251,9 @@ def main():
     from gzb import native as N
     from gzb import params as P
 
+    from gzb.replicas import Replicas
     torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    reps = Replicas("nccl", timeout_s=600)
     db, q, gen_s = make_workload(args.workload)
     params = P.make_params()
     eng = N.PresearchEngine(local_rank)
@@ -291,8 +288,7 @@ def main():
     train_s = time.time() - t
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        reps.barrier()
         torch.cuda.synchronize()
 
     def timed(sched):
@@ -424,14 +420,10 @@ def main():
                      "alignments_per_s": n_aligned / (b0.elapsed_time(b1) / 1e3)}
 
     # max over ranks
-    t_dev, t_e2e = dev_ms, e2e_ms
-    if dist is not None:
-        tt = torch.tensor([dev_ms, e2e_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_dev, t_e2e = float(tt[0]), float(tt[1])
+    t_dev, t_e2e = reps.max([dev_ms, e2e_ms])
     nq = q.number
-    value = world * nq * args.steps / (t_dev / 1e3)
-    e2e_value = world * nq * args.steps / (t_e2e / 1e3)
+    value = reps.throughput(nq, args.steps, t_dev)
+    e2e_value = reps.throughput(nq, args.steps, t_e2e)
     steps = args.steps
     st = stage
     sched_report = {}
@@ -510,8 +502,7 @@ def main():
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()
-    if dist is not None:
-        dist.destroy_process_group()
+    reps.close()
 
 
 if __name__ == "__main__":
