@@ -637,6 +637,7 @@ struct LaneExt {
   int bs, be;
   int maxs, mp0, mp1;
   int p1;
+  int xr;  // database residue of row p1, loaded one row ahead
   uint32_t cells;
   bool ovf;
 };
@@ -661,7 +662,8 @@ __device__ __forceinline__ int lane_init(const GappedJob &job, LaneBand &band, L
   x.p1 = 0;
   x.cells = 0;
   x.ovf = false;
-  if (q0[0] == delim || d0[0] == delim) return kLaneDone;
+  x.xr = d0[0];
+  if (q0[0] == delim || x.xr == delim) return kLaneDone;
   // every value a row keeps lies in [maxs - cutoff - gi, maxs] with maxs >= 0,
   // so checking maxs once per row is enough when cutoff + gi fits; the
   // values written here lie in [-cutoff - gi, 0]
@@ -723,8 +725,9 @@ __device__ __forceinline__ int lane_row(const GappedJob &job, const int *sm, Lan
   const int cutoff = job.cutoff;
   const uint8_t *q0 = x.q0;
   const int p1 = x.p1;
-  const int xr = x.d0[p1];
+  const int xr = x.xr;
   if (xr == delim) return kLaneDone;
+  x.xr = x.d0[p1 + inc];  // the next row's residue (the chunk is padded)
   const int *mrow = sm + xr * kMatrixStride;
   int bs = x.bs, be = x.be, maxs = x.maxs;
   bool ovf = x.ovf;
