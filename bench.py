@@ -419,6 +419,18 @@ def main():
     build_results = {"ms": b0.elapsed_time(b1), "alignments": n_aligned,
                      "alignments_per_s": n_aligned / (b0.elapsed_time(b1) / 1e3)}
 
+    # the device index cache: export the chunk's index once, then set the
+    # chunk again from it instead of building (outside the timed region)
+    t = time.time()
+    blob = eng.export_index()
+    export_s = time.time() - t
+    t = time.time()
+    eng.set_database(db, index=blob)
+    torch.cuda.synchronize()
+    index_cache = {"blob_bytes": int(blob.nbytes), "export_s": export_s,
+                   "import_s": time.time() - t, "build_s": index_s}
+    del blob
+
     # max over ranks
     t_dev, t_e2e = reps.max([dev_ms, e2e_ms])
     nq = q.number
@@ -490,7 +502,7 @@ def main():
                 "results_equal_device_loop": bool(e2e_same)},
         "dp_gcups": {"gapped_stage": gcups_stage, "whole_step": gcups_step},
         "stage_ms": st, "counters": counters, "schedules": sched_report,
-        "index_build_s": index_s, "build_results": build_results,
+        "index_build_s": index_s, "index_cache": index_cache, "build_results": build_results,
         "workload_gen_s": gen_s, "clocks": clocks, "roofline": roofline,
         "gpu_launches": int(counters.get("kernel_launches", 0)) * steps,
     }

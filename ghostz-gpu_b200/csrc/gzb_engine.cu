@@ -1069,6 +1069,7 @@ struct gzb_engine {
       model_d, mae_acc, log_x, log_y, log_ctr;
   uint64_t prev_cells_n = 0;
   DBuf codeflag;
+  uint64_t db_check = 0;     // of the resident chunk (index cache key)
   // build results step
   DBuf tb_cols, tb_band_off, tb_band, tb_ops_bytes, tb_ops_off, tb_rows, tb_rows_off, tb_walk_cap,
       tb_walk_off, tb_ops, tb_row_meta, tb_walk, tb_walk_n, tb_score, tb_p0, tb_p1, tb_out;
@@ -1245,7 +1246,7 @@ extern "C" int gzb_engine_create(int device, gzb_engine **out) {
   gzb_engine *e = new (std::nothrow) gzb_engine();
   GZB_CHECK(e, GZB_ERR_NOMEM, "host allocation failed");
   e->device = device;
-  e->index_bufs.resize(40);
+  e->index_bufs.resize(50);
   e->list_bufs.resize(20);
   cudaError_t err = cudaMalloc(&e->gcounters, 64);
   if (err == cudaSuccess) err = cudaMalloc(&e->gcells, 8);
@@ -1344,6 +1345,97 @@ extern "C" int gzb_engine_set_params(gzb_engine *e, const gzb_params *p) {
   return GZB_OK;
 }
 
+namespace {
+
+// ---- device index cache ----------------------------------------------------
+// Blob: IndexHeader, then the index arrays in kIndexArrays order, each padded
+// to 8 bytes.
+constexpr uint64_t kIndexMagic = 0x3130584449425a47ull;  // "GZBIDX01"
+
+struct IndexHeader {
+  uint64_t magic;
+  uint64_t fingerprint;  // parameters the index depends on
+  uint64_t db_len, nseq, db_check;
+  uint64_t n_nc_keys, n_nc_values, n_rep_keys, n_reps, n_members;
+};
+
+uint64_t fnv1a(uint64_t h, const void *p, size_t n) {
+  const uint8_t *b = (const uint8_t *)p;
+  for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 0x100000001b3ull;
+  return h;
+}
+
+// the parameters the index build reads (hash, similarity windows, clustering)
+uint64_t index_fingerprint(const gzb_engine *e) {
+  const gzb_params &p = e->params;
+  uint64_t h = 0xcbf29ce484222325ull;
+  const int32_t v[] = {p.delimiter, p.number_letters, p.map_size, p.max_indexing_code,
+                       p.seed_threshold, p.max_hash_length, p.min_hash_length,
+                       p.subsequence_length, p.max_member_distance, p.clustering};
+  h = fnv1a(h, v, sizeof(v));
+  h = fnv1a(h, p.hash_code_map, sizeof(p.hash_code_map));
+  h = fnv1a(h, p.similarity_code_map, sizeof(p.similarity_code_map));
+  h = fnv1a(h, p.code_scores, sizeof(p.code_scores));
+  return h;
+}
+
+// a cheap check that the blob belongs to these residues: offsets, and up to
+// 64 KB of codes from each end
+uint64_t db_check(const uint8_t *codes, uint64_t length, const uint32_t *offsets, uint32_t nseq) {
+  uint64_t h = 0xcbf29ce484222325ull;
+  h = fnv1a(h, offsets, 4 * ((size_t)nseq + 1));
+  const uint64_t k = length < 65536 ? length : 65536;
+  h = fnv1a(h, codes, k);
+  h = fnv1a(h, codes + length - k, k);
+  return h;
+}
+
+struct IndexArray {
+  int slot;          // index_bufs slot on import
+  size_t elem;       // bytes per element
+};
+
+uint64_t pad8(uint64_t n) { return (n + 7) & ~7ull; }
+
+void index_array_sizes(const IndexHeader &h, uint64_t n[10]) {
+  n[0] = h.n_nc_keys;        // nc_keys
+  n[1] = h.n_nc_keys + 1;    // nc_offsets
+  n[2] = h.n_nc_values;      // nc_values
+  n[3] = h.n_rep_keys;       // rep_keys
+  n[4] = h.n_rep_keys + 1;   // rep_offsets
+  n[5] = h.n_reps;           // rep_positions
+  n[6] = h.n_reps;           // rep_cluster_ids
+  n[7] = h.n_reps;           // rep_windows (8 bytes each)
+  n[8] = h.n_reps + 1;       // member_offsets
+  n[9] = h.n_members;        // member_positions
+}
+
+uint64_t index_blob_bytes(const IndexHeader &h) {
+  uint64_t n[10];
+  index_array_sizes(h, n);
+  uint64_t b = sizeof(IndexHeader);
+  for (int i = 0; i < 10; ++i) b += pad8(n[i] * (i == 7 ? 8 : 4));
+  return b;
+}
+
+IndexHeader header_of(const gzb_engine *e) {
+  IndexHeader h;
+  memset(&h, 0, sizeof(h));
+  h.magic = kIndexMagic;
+  h.fingerprint = index_fingerprint(e);
+  h.db_len = e->db_len;
+  h.nseq = e->nseq;
+  h.db_check = e->db_check;
+  h.n_nc_keys = e->X.n_nc_keys;
+  h.n_nc_values = e->X.n_nc_values;
+  h.n_rep_keys = e->X.params_clustering ? e->X.n_rep_keys : 0;
+  h.n_reps = e->X.params_clustering ? e->X.n_reps : 0;
+  h.n_members = e->X.params_clustering ? e->X.n_members : 0;
+  return h;
+}
+
+}  // namespace
+
 extern "C" int gzb_engine_set_database(gzb_engine *e, int32_t chunk_id, const uint8_t *codes,
                                        uint64_t length, const uint32_t *offsets,
                                        uint32_t number_sequences, void *stream) {
@@ -1358,6 +1450,7 @@ extern "C" int gzb_engine_set_database(gzb_engine *e, int32_t chunk_id, const ui
   e->chunk_id = chunk_id;
   e->db_len = length;
   e->nseq = number_sequences;
+  e->db_check = db_check(codes, length, offsets, number_sequences);
   GZB_TRY(upload_padded(e->db_buf, e->codeflag, codes, length, (uint8_t)e->params.delimiter, s));
   GZB_TRY(upload(e->db_offsets, offsets, number_sequences + 1, s));
   const uint8_t *db = e->db_buf.as<uint8_t>() + kPad;
@@ -1379,6 +1472,7 @@ extern "C" int gzb_engine_set_database(gzb_engine *e, int32_t chunk_id, const ui
   uint64_t *other = sorted == pairs.as<uint64_t>() ? pairs_alt.as<uint64_t>() : pairs.as<uint64_t>();
   DevIndex &X = e->X;
   X = DevIndex();
+  X.params_clustering = e->params.clustering != 0;
   if (!e->params.clustering) {
     GZB_TRY(build_csr(e, sorted, np, &X.nc_keys, &X.nc_offsets, &X.nc_values, &X.n_nc_keys, 10, s));
     X.n_nc_values = np;
@@ -1487,6 +1581,106 @@ extern "C" int gzb_engine_set_database(gzb_engine *e, int32_t chunk_id, const ui
   X.member_offsets = moff.as<uint32_t>();
   X.member_positions = mpos.as<uint32_t>();
   X.n_members = nm;
+  GZB_CUDA(cudaStreamSynchronize(s));
+  e->have_db = true;
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_index_bytes(gzb_engine *e, uint64_t *bytes) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(bytes, GZB_ERR_INVALID, "null argument");
+  GZB_CHECK(e->have_db, GZB_ERR_INVALID, "no database chunk");
+  *bytes = index_blob_bytes(header_of(e));
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_export_index(gzb_engine *e, void *blob, uint64_t capacity,
+                                       void *stream) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(blob, GZB_ERR_INVALID, "null blob");
+  GZB_CHECK(e->have_db, GZB_ERR_INVALID, "no database chunk");
+  const IndexHeader h = header_of(e);
+  const uint64_t need = index_blob_bytes(h);
+  GZB_CHECK(capacity >= need, GZB_ERR_INVALID, "index blob needs %llu bytes",
+            (unsigned long long)need);
+  cudaStream_t s = (cudaStream_t)stream;
+  uint8_t *out = (uint8_t *)blob;
+  memcpy(out, &h, sizeof(h));
+  uint64_t at = sizeof(h), n[10];
+  index_array_sizes(h, n);
+  const void *src[10] = {e->X.nc_keys, e->X.nc_offsets, e->X.nc_values, e->X.rep_keys,
+                         e->X.rep_offsets, e->X.rep_positions, e->X.rep_cluster_ids,
+                         e->X.rep_windows, e->X.member_offsets, e->X.member_positions};
+  for (int i = 0; i < 10; ++i) {
+    const uint64_t bytes = n[i] * (i == 7 ? 8 : 4);
+    if (bytes) GZB_CUDA(cudaMemcpyAsync(out + at, src[i], bytes, cudaMemcpyDeviceToHost, s));
+    at += pad8(bytes);
+  }
+  GZB_CUDA(cudaStreamSynchronize(s));
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_set_database_with_index(gzb_engine *e, int32_t chunk_id,
+                                                  const uint8_t *codes, uint64_t length,
+                                                  const uint32_t *offsets,
+                                                  uint32_t number_sequences, const void *blob,
+                                                  uint64_t blob_bytes, void *stream) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(e->have_params, GZB_ERR_INVALID, "set_params first");
+  GZB_CHECK(codes && offsets && number_sequences > 0 && length > 0 && blob, GZB_ERR_INVALID,
+            "empty database or index");
+  GZB_CHECK(length < (1ull << 31), GZB_ERR_OVERFLOW,
+            "database chunk of %llu residues exceeds 2^31", (unsigned long long)length);
+  GZB_CHECK(blob_bytes >= sizeof(IndexHeader), GZB_ERR_INVALID, "index blob too short");
+  IndexHeader h;
+  memcpy(&h, blob, sizeof(h));
+  GZB_CHECK(h.magic == kIndexMagic, GZB_ERR_INVALID, "not an index blob of this library");
+  GZB_CHECK(h.fingerprint == index_fingerprint(e), GZB_ERR_INVALID,
+            "index blob was built with other index parameters");
+  GZB_CHECK(h.db_len == length && h.nseq == number_sequences &&
+                h.db_check == db_check(codes, length, offsets, number_sequences),
+            GZB_ERR_INVALID, "index blob belongs to another chunk");
+  GZB_CHECK(blob_bytes >= index_blob_bytes(h), GZB_ERR_INVALID, "index blob truncated");
+  cudaStream_t s = (cudaStream_t)stream;
+  e->have_db = false;
+  e->chunk_id = chunk_id;
+  e->db_len = length;
+  e->nseq = number_sequences;
+  e->db_check = h.db_check;
+  GZB_TRY(upload_padded(e->db_buf, e->codeflag, codes, length, (uint8_t)e->params.delimiter, s));
+  GZB_TRY(upload(e->db_offsets, offsets, number_sequences + 1, s));
+  std::vector<DBuf> &B = e->index_bufs;
+  uint64_t n[10], at = sizeof(h);
+  index_array_sizes(h, n);
+  void *dst[10];
+  for (int i = 0; i < 10; ++i) {
+    const uint64_t bytes = n[i] * (i == 7 ? 8 : 4);
+    DBuf &d = B[40 + i];
+    GZB_TRY(d.ensure(bytes + 16));
+    GZB_CUDA(cudaMemsetAsync(d.p, 0, 16, s));
+    if (bytes)
+      GZB_CUDA(cudaMemcpyAsync(d.p, (const uint8_t *)blob + at, bytes, cudaMemcpyHostToDevice, s));
+    dst[i] = d.p;
+    at += pad8(bytes);
+  }
+  DevIndex &X = e->X;
+  X = DevIndex();
+  X.nc_keys = (uint32_t *)dst[0];
+  X.nc_offsets = (uint32_t *)dst[1];
+  X.nc_values = (uint32_t *)dst[2];
+  X.rep_keys = (uint32_t *)dst[3];
+  X.rep_offsets = (uint32_t *)dst[4];
+  X.rep_positions = (uint32_t *)dst[5];
+  X.rep_cluster_ids = (uint32_t *)dst[6];
+  X.rep_windows = (uint64_t *)dst[7];
+  X.member_offsets = (uint32_t *)dst[8];
+  X.member_positions = (uint32_t *)dst[9];
+  X.n_nc_keys = h.n_nc_keys;
+  X.n_nc_values = h.n_nc_values;
+  X.n_rep_keys = h.n_rep_keys;
+  X.n_reps = h.n_reps;
+  X.n_members = h.n_members;
+  X.params_clustering = e->params.clustering != 0;
   GZB_CUDA(cudaStreamSynchronize(s));
   e->have_db = true;
   return GZB_OK;

@@ -57,6 +57,7 @@ struct DevIndex {
   uint64_t *rep_windows = nullptr;  // packed similarity window per representative
   uint64_t n_nc_keys = 0, n_nc_values = 0, n_rep_keys = 0, n_reps = 0,
            n_members = 0;
+  bool params_clustering = false;  // built with clustering (rep/member arrays)
 };
 
 // Query hash lists (SeedSearcherGpuQueryParameters, seed search inputs).

@@ -110,6 +110,10 @@ def _declare(L):
         "gzb_engine_get_tile": [V, C.c_int, C.c_int, V],
         "gzb_engine_get_extension_costs": [V, V, V, C.c_uint64, V, V],
         "gzb_engine_build_alignments": [V, V, V, V],
+        "gzb_engine_index_bytes": [V, V],
+        "gzb_engine_export_index": [V, V, C.c_uint64, V],
+        "gzb_engine_set_database_with_index": [V, C.c_int32, V, C.c_uint64, V, C.c_uint32, V,
+                                               C.c_uint64, V],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -350,12 +354,29 @@ class PresearchEngine:
         self.params = np.array([params], dtype=params.dtype)
         check(lib().gzb_engine_set_params(self.h, C.c_void_p(self.params.ctypes.data)))
 
-    def set_database(self, db, chunk_id=0, stream=None):
+    def set_database(self, db, chunk_id=0, stream=None, index=None):
+        """Uploads a chunk and builds its device index, or takes the index
+        from `index`, a blob export_index() wrote for the same chunk."""
         codes = np.ascontiguousarray(db.codes, dtype=np.uint8)
         offs = np.ascontiguousarray(db.offsets, dtype=np.uint32)
-        check(lib().gzb_engine_set_database(self.h, int(chunk_id), hptr(codes), len(codes),
-                                            hptr(offs), int(db.number_sequences),
+        if index is None:
+            check(lib().gzb_engine_set_database(self.h, int(chunk_id), hptr(codes), len(codes),
+                                                hptr(offs), int(db.number_sequences),
+                                                _stream_or_null(stream)))
+        else:
+            blob = np.ascontiguousarray(index, dtype=np.uint8)
+            check(lib().gzb_engine_set_database_with_index(
+                self.h, int(chunk_id), hptr(codes), len(codes), hptr(offs),
+                int(db.number_sequences), hptr(blob), blob.nbytes, _stream_or_null(stream)))
+
+    def export_index(self, stream=None):
+        """The resident chunk's device index as a host blob (numpy uint8)."""
+        n = C.c_uint64()
+        check(lib().gzb_engine_index_bytes(self.h, C.byref(n)))
+        blob = np.zeros(n.value, np.uint8)
+        check(lib().gzb_engine_export_index(self.h, hptr(blob), n.value,
                                             _stream_or_null(stream)))
+        return blob
 
     def set_queries(self, queries, stream=None):
         codes = np.ascontiguousarray(queries.codes, dtype=np.uint8)

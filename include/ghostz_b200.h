@@ -261,6 +261,20 @@ int gzb_engine_set_database(gzb_engine *e, int32_t chunk_id,
                             const uint8_t *codes, uint64_t length,
                             const uint32_t *offsets,
                             uint32_t number_sequences, void *stream);
+/* Device index cache (no counterpart in the reference, which loads the
+ * index files its `db` command wrote): gzb_engine_index_bytes gives the
+ * size of the resident chunk's index blob, gzb_engine_export_index copies
+ * it to host memory, and gzb_engine_set_database_with_index sets a chunk
+ * from its codes and such a blob instead of building the index.  The blob
+ * records the index parameters and a check of the chunk, and is refused for
+ * others. */
+int gzb_engine_index_bytes(gzb_engine *e, uint64_t *bytes);
+int gzb_engine_export_index(gzb_engine *e, void *blob, uint64_t capacity, void *stream);
+int gzb_engine_set_database_with_index(gzb_engine *e, int32_t chunk_id, const uint8_t *codes,
+                                       uint64_t length, const uint32_t *offsets,
+                                       uint32_t number_sequences, const void *blob,
+                                       uint64_t blob_bytes, void *stream);
+
 /* Uploads the queries (concatenated, shared delimiters; offsets[i] is the
  * leading delimiter of query i; lengths[i] = residues + 2) with their
  * per-query ungapped X-drop and trigger, and builds the query hash lists. */
