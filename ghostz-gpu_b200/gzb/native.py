@@ -54,6 +54,8 @@ def _declare(L):
     L.gzb_ungapped_extender_query_seeds_temp_bytes.argtypes = [SZ]
     L.gzb_cost_model_param_count.restype = C.c_int
     L.gzb_cost_model_param_count.argtypes = []
+    L.gzb_translated_query_length.restype = C.c_uint64
+    L.gzb_translated_query_length.argtypes = [U32]
     sigs = {
         "gzb_distance_calculator_create": [V],
         "gzb_distance_calculator_destroy": [V],
@@ -114,6 +116,7 @@ def _declare(L):
         "gzb_engine_export_index": [V, V, C.c_uint64, V],
         "gzb_engine_set_database_with_index": [V, C.c_int32, V, C.c_uint64, V, C.c_uint32, V,
                                                C.c_uint64, V],
+        "gzb_translate_dna_queries": [V, V, V, U32, V, C.c_uint8, V, V],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -531,3 +534,55 @@ def _stream_or_null(stream):
     if stream is None:
         return None
     return C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+
+# -- query preparation: six-frame translation ---------------------------------
+def translated_query_length(length):
+    """Codes of a read's translated query, both delimiters included
+    (TranslatedDnaQuery::GetSequenceLength, src/translated_dna_query.h:24-31;
+    2 for a read shorter than 3 bases)."""
+    return int(lib().gzb_translated_query_length(int(length)))
+
+
+def translated_layout(lengths):
+    """Shared-delimiter layout of the translated queries of reads with these
+    lengths: (out_offsets uint64, query lengths uint32, total codes)."""
+    n = np.asarray(lengths, dtype=np.int64)
+    ql = np.where(n < 3, 2, 7 + 6 * (n // 3)).astype(np.int64)
+    offs = np.zeros(len(ql), dtype=np.uint64)
+    if len(ql) > 1:
+        offs[1:] = np.cumsum(ql - 1)[:-1]
+    total = int((ql - 1).sum()) + 1 if len(ql) else 0
+    return offs, ql.astype(np.uint32), total
+
+
+def translate_dna_queries_async(d_dna, d_offsets, d_lengths, number_reads, d_out_offsets,
+                                d_out, delimiter, stream=None):
+    """gzb_translate_dna_queries on device buffers (addresses or tensors)."""
+    check(lib().gzb_translate_dna_queries(dptr(d_dna), dptr(d_offsets), dptr(d_lengths),
+                                          int(number_reads), dptr(d_out_offsets),
+                                          int(delimiter), dptr(d_out),
+                                          stream_handle(stream)))
+
+
+def translate_reads(dna, offsets, delimiter, device="cuda", stream=None):
+    """Translates reads on the GPU.  dna: uint8 ASCII bases of all reads
+    back to back; offsets: number_reads + 1 read boundaries.  Returns the
+    translated queries in the engine's shared-delimiter layout as host
+    arrays (codes uint8, offsets uint32, lengths uint32)."""
+    import torch
+    offsets = np.asarray(offsets, dtype=np.uint64)
+    n = len(offsets) - 1
+    lengths = np.diff(offsets).astype(np.uint32)
+    out_offs, qlen, total = translated_layout(lengths)
+    if n == 0:
+        return np.zeros(0, np.uint8), np.zeros(0, np.uint32), np.zeros(0, np.uint32)
+    d_dna = torch.from_numpy(np.ascontiguousarray(dna, dtype=np.uint8)).to(device)
+    d_offs = torch.from_numpy(offsets[:-1].view(np.int64).copy()).to(device)
+    d_lens = torch.from_numpy(lengths.view(np.int32).copy()).to(device)
+    d_out_offs = torch.from_numpy(out_offs.view(np.int64).copy()).to(device)
+    d_out = torch.empty(total, dtype=torch.uint8, device=device)
+    translate_dna_queries_async(d_dna, d_offs, d_lens, n, d_out_offs, d_out, delimiter,
+                                stream)
+    codes = d_out.cpu().numpy()
+    return codes, out_offs.astype(np.uint32), qlen

@@ -165,3 +165,97 @@ def pack_queries(seqs, sources=None, cutoffs=None) -> Queries:
 def query_sequences(q: Queries):
     """Residue arrays (no delimiters) of every query."""
     return [q.codes[int(o) + 1:int(o) + int(l) - 1] for o, l in zip(q.offsets, q.lengths)]
+
+
+# -- translated-DNA workload ----------------------------------------------------
+# the standard genetic code, codons in ACGT order (first base slowest)
+_CODON_LETTERS = "KNKNTTTTRSRSIIMIQHQHPPPPRRRRLLLLEDEDAAAAGGGGVVVV*Y*YSSSS*CWCLFLF"
+_BASES = np.frombuffer(b"ACGT", dtype=np.uint8)
+_COMPLEMENT = np.zeros(256, dtype=np.uint8)
+for _a, _b in zip(b"ACGT", b"TGCA"):
+    _COMPLEMENT[_a] = _b
+
+
+@dataclass
+class Reads:
+    dna: np.ndarray              # uint8 ASCII bases of all reads back to back
+    offsets: np.ndarray          # uint64, number_reads + 1 boundaries
+    sources: np.ndarray = field(default=None)  # planted fragment source or -1
+
+    @property
+    def number(self) -> int:
+        return int(self.offsets.shape[0]) - 1
+
+    def read(self, i) -> bytes:
+        return self.dna[int(self.offsets[i]):int(self.offsets[i + 1])].tobytes()
+
+
+def _codon_choices():
+    """(20, 6) codon indices per regular residue code and their counts."""
+    table = np.zeros((len(P.REGULAR), 6), dtype=np.int64)
+    count = np.zeros(len(P.REGULAR), dtype=np.int64)
+    for c, letter in enumerate(_CODON_LETTERS):
+        if letter in P.REGULAR:
+            a = P.REGULAR.index(letter)
+            table[a, count[a]] = c
+            count[a] += 1
+    return table, count
+
+
+def make_reads(db: Database, n_reads, seed, read_length=150, homolog_fraction=0.4,
+               error=0.01) -> Reads:
+    """Synthetic reads of one length with i.i.d. bases at 50 % GC; a
+    fraction are reverse-translated fragments of random database proteins
+    (uniform codon choice, random strand and frame) with per-base
+    substitution errors."""
+    rng = np.random.default_rng(seed)
+    reads = _BASES[rng.integers(0, 4, size=(n_reads, read_length))]
+    planted = rng.random(n_reads) < homolog_fraction
+    sources = np.full(n_reads, -1, dtype=np.int64)
+    idx = np.flatnonzero(planted)
+    if len(idx):
+        k = read_length // 3 + 1  # residues covering every frame offset
+        s = rng.integers(0, db.number_sequences, size=len(idx))
+        first = db.offsets[s].astype(np.int64)
+        plen = db.offsets[s + 1].astype(np.int64) - 1 - first
+        start = (rng.random(len(idx)) * np.maximum(plen - k + 1, 1)).astype(np.int64)
+        pos = start[:, None] + np.arange(k)[None, :]
+        inside = pos < plen[:, None]
+        res = db.codes[np.minimum(first[:, None] + pos, db.length - 1)].astype(np.int64)
+        res = np.where(inside & (res < len(P.REGULAR)), res,
+                       rng.integers(0, len(P.REGULAR), size=res.shape))
+        table, count = _codon_choices()
+        pick = (rng.random(res.shape) * count[res]).astype(np.int64)
+        codon = table[res, pick]                      # (m, k) codon indices
+        nt = np.stack([codon // 16, (codon // 4) % 4, codon % 4], axis=-1).reshape(len(idx), -1)
+        frame = rng.integers(0, 3, size=len(idx))
+        nt = np.take_along_axis(nt, frame[:, None] + np.arange(read_length)[None, :], axis=1)
+        frag = _BASES[nt]
+        rev = rng.random(len(idx)) < 0.5
+        frag[rev] = _COMPLEMENT[frag[rev][:, ::-1]]
+        hit = rng.random(frag.shape) < error
+        shift = rng.integers(1, 4, size=frag.shape)
+        code = np.searchsorted(_BASES, frag)
+        frag = np.where(hit, _BASES[(code + shift) % 4], frag)
+        reads[idx] = frag
+        sources[idx] = s
+    offsets = np.arange(n_reads + 1, dtype=np.uint64) * np.uint64(read_length)
+    return Reads(dna=reads.reshape(-1).copy(), offsets=offsets, sources=sources)
+
+
+def translated_queries(codes, offsets, lengths, sources=None, cutoffs=None) -> Queries:
+    """Queries over translated reads already laid out with shared
+    delimiters (the output of six-frame translation): per-query cutoffs
+    from each translated query's own composition, as
+    TranslatedDnaQuery::SetStaticalParameters does
+    (src/translated_dna_query.cpp:76-85)."""
+    offsets = np.asarray(offsets, dtype=np.uint32)
+    lengths = np.asarray(lengths, dtype=np.uint32)
+    if cutoffs is None:
+        seqs = [codes[int(o) + 1:int(o) + int(n) - 1] for o, n in zip(offsets, lengths)]
+        cutoffs = P.query_cutoffs(seqs)
+    cut, trig = cutoffs
+    n = len(offsets)
+    return Queries(codes=np.asarray(codes, dtype=np.uint8), offsets=offsets, lengths=lengths,
+                   cutoffs=cut, triggers=trig,
+                   sources=sources if sources is not None else np.full(n, -1))

@@ -448,6 +448,27 @@ int gzb_engine_get_schedule_stats(gzb_engine *e, float *mean_abs_log2_error,
  * alone (part of [1]: seed and member kernels, without the hit sort). */
 int gzb_engine_get_stage_ms(gzb_engine *e, float *ms7);
 
+
+/* ---- query preparation: six-frame translation of DNA reads ----
+ * Replaces the per-read TranslatedDnaQuery construction of
+ * Queries::BuildQuery (src/queries.cpp:83-107; layout
+ * src/translated_dna_query.cpp:44-74, codons src/translator.cpp:104-142)
+ * with filtering off.  gzb_translated_query_length gives a read's
+ * translated query length in codes, both delimiters included
+ * (TranslatedDnaQuery::GetSequenceLength, src/translated_dna_query.h:24-31;
+ * a read shorter than 3 bases gives 2, an empty query, where the reference
+ * writes past an empty buffer).  gzb_translate_dna_queries translates
+ * number_reads reads held on the device (ASCII, read r = d_dna[d_offsets[r]
+ * .. + d_lengths[r])) into d_out, query r starting at d_out_offsets[r]; to
+ * get the engine's shared-delimiter layout set d_out_offsets[r + 1] =
+ * d_out_offsets[r] + gzb_translated_query_length(length r) - 1.  Reads
+ * nothing back; asynchronous on `stream`. */
+uint64_t gzb_translated_query_length(uint32_t length);
+int gzb_translate_dna_queries(const uint8_t *d_dna, const uint64_t *d_offsets,
+                              const uint32_t *d_lengths, uint32_t number_reads,
+                              const uint64_t *d_out_offsets, uint8_t delimiter,
+                              uint8_t *d_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1375,3 +1375,77 @@ size_t gzo_presearch_hits(const gzo_presearch *x, const uint32_t **qid,
   *d = x->hits.d;
   return x->hits.n;
 }
+
+/* ---- six-frame translation (src/translator.cpp:20-142,
+ * src/translated_dna_query.cpp:44-74, src/dna_sequence.h:28-42) ---- */
+
+/* The standard genetic code, codons in ACGT order (first base slowest). */
+static const char kCodonTable[] =
+    "KNKNTTTTRSRSIIMIQHQHPPPPRRRRLLLLEDEDAAAAGGGGVVVV*Y*YSSSS*CWCLFLF";
+/* Protein code = index in this string (ProteinType regular letters, then
+ * the ambiguous ones, then the unknown letter). */
+static const char kProteinLetters[] = "ARNDCQEGHILKMFPSTWYVBJZ*X";
+
+static int base_index(char c) {
+  switch (c) {
+    case 'A': return 0;
+    case 'C': return 1;
+    case 'G': return 2;
+    case 'T': return 3;
+    default: return -1;  /* the codon table is case sensitive */
+  }
+}
+
+static char complement(char c) {
+  switch (c) {
+    case 'A': case 'a': return 'T';
+    case 'C': case 'c': return 'G';
+    case 'G': case 'g': return 'C';
+    case 'T': case 't': return 'A';
+    default: return 'N';
+  }
+}
+
+static uint8_t protein_code(char letter) {
+  for (uint8_t i = 0; kProteinLetters[i]; ++i)
+    if (kProteinLetters[i] == letter) return i;
+  return 24;
+}
+
+/* Translator::Translate keeps a "stopped" flag that is never set, so
+ * every codon found in the table is translated and every other codon
+ * becomes the unknown letter. */
+static uint8_t codon_code(char a, char b, char c) {
+  const int x = base_index(a), y = base_index(b), z = base_index(c);
+  if (x < 0 || y < 0 || z < 0) return protein_code('X');
+  return protein_code(kCodonTable[x * 16 + y * 4 + z]);
+}
+
+uint32_t gzo_translated_length(uint32_t length) {
+  return length < 3 ? 2 : 7 + 6 * (length / 3);
+}
+
+uint32_t gzo_translate_query(const char *dna, uint32_t length, uint8_t delimiter,
+                             uint8_t *out) {
+  out[0] = delimiter;
+  if (length < 3) {
+    out[1] = delimiter;
+    return 2;
+  }
+  char *rc = (char *)malloc(length);
+  for (uint32_t i = 0; i < length; ++i) rc[i] = complement(dna[length - 1 - i]);
+  const uint32_t base = length / 3;
+  uint32_t o = 1;
+  for (int frame = 0; frame < 6; ++frame) {
+    const char *s = frame < 3 ? dna : rc;
+    const uint32_t offset = (uint32_t)(frame % 3);
+    uint32_t n = 0;
+    for (uint32_t j = offset; j + 2 < length; j += 3, ++n)
+      out[o + n] = codon_code(s[j], s[j + 1], s[j + 2]);
+    o += n;
+    if (n < base) out[o++] = delimiter;
+    out[o++] = delimiter;
+  }
+  free(rc);
+  return o;
+}

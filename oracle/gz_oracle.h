@@ -178,6 +178,21 @@ size_t gzo_add_results(const gzo_params *p, const uint32_t *db_offsets,
                        gzo_result *added, size_t n_added,
                        gzo_result *results, size_t n_results);
 
+
+/* Six-frame translation of one DNA read into the reference's translated
+ * query layout (TranslatedDnaQuery::SetEncodedSequence,
+ * src/translated_dna_query.cpp:44-74, with Translator::Translate,
+ * src/translator.cpp:104-142, and no filter): a leading delimiter, then
+ * per frame (forward offsets 0,1,2, then the reverse complement's 0,1,2)
+ * its codons as protein codes, an extra delimiter when the frame has fewer
+ * than length/3 codons, and one closing delimiter.  Returns the bytes
+ * written: gzo_translated_length(length).  A read shorter than 3 bases
+ * gives [delimiter][delimiter] (the reference writes past an empty buffer
+ * for those). */
+uint32_t gzo_translated_length(uint32_t length);
+uint32_t gzo_translate_query(const char *dna, uint32_t length, uint8_t delimiter,
+                             uint8_t *out);
+
 #ifdef __cplusplus
 }
 #endif

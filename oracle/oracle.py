@@ -99,6 +99,10 @@ class Oracle:
         L.gzo_presearch_hits.argtypes = [C.c_void_p, C.POINTER(u32p), C.POINTER(u32p),
                                          C.POINTER(u32p)]
         L.gzo_presearch_hits.restype = C.c_size_t
+        L.gzo_translated_length.argtypes = [C.c_uint32]
+        L.gzo_translated_length.restype = C.c_uint32
+        L.gzo_translate_query.argtypes = [C.c_char_p, C.c_uint32, C.c_uint8, u8p]
+        L.gzo_translate_query.restype = C.c_uint32
 
     # -- primitives ---------------------------------------------------------
     def hash(self, params, seq, pos=0):
@@ -174,6 +178,15 @@ class Oracle:
         v[0] = C.c_int32(v[0]).value
         return dict(zip(("score", "start_q", "start_d", "end_q", "end_d", "alignment_length",
                          "mismatches", "gap_openings", "gap_extensions"), v))
+
+    def translate_query(self, dna, delimiter):
+        """Translated query codes of one DNA read (bytes): the six frames in
+        the reference's TranslatedDnaQuery layout, delimiters included."""
+        dna = bytes(dna)
+        out = np.zeros(self.L.gzo_translated_length(len(dna)), np.uint8)
+        n = self.L.gzo_translate_query(dna, len(dna), int(delimiter), _p(out, u8p))
+        assert n == len(out)
+        return out
 
     def chain_filter(self, params, query, qlen, cutoff, db, hq, hd):
         pr = _Params(params)
@@ -293,6 +306,8 @@ class Reference:
                                           C.POINTER(C.c_float), C.POINTER(C.c_float)]
         L.gzr_normalized_cutoff_to_nominal.argtypes = [C.c_float, C.c_float, C.c_float]
         L.gzr_normalized_to_nominal.argtypes = [C.c_float, C.c_float, C.c_float]
+        L.gzr_translate_query.argtypes = [C.c_void_p, C.c_char_p, C.c_uint32, u8p, C.c_uint32]
+        L.gzr_translate_query.restype = C.c_uint32
 
     def hash_many(self, params, seq):
         pr = _Params(params)
@@ -389,3 +404,15 @@ class Reference:
     def cutoffs(self, lam, k, ungapped_bits=7.0, trigger_bits=22.0):
         return (self.L.gzr_normalized_cutoff_to_nominal(ungapped_bits, lam, k),
                 self.L.gzr_normalized_to_nominal(trigger_bits, lam, k))
+
+    def translate_query(self, params, dna):
+        """The reference's TranslatedDnaQuery codes of one DNA read (bytes,
+        at least 3 bases)."""
+        pr = _Params(params)
+        dna = bytes(dna)
+        assert len(dna) >= 3
+        cap = 7 + 6 * (len(dna) // 3)
+        out = np.zeros(cap, np.uint8)
+        n = self.L.gzr_translate_query(pr.ptr, dna, len(dna), _p(out, u8p), cap)
+        assert n == cap
+        return out

@@ -23,6 +23,10 @@
 #include "seed_searcher_database_parameters.h"
 #include "statistics.h"
 #include "protein_type.h"
+#include "sequence.h"
+#include "translator.h"
+#include "translated_dna_query.h"
+#include "sequence_no_filter.h"
 
 static ScoreMatrix make_matrix(const gzo_params *p) {
   std::vector<int> m(p->number_letters * p->number_letters);
@@ -229,6 +233,30 @@ int gzr_normalized_to_nominal(float bits, float lambda, float k) {
   kp.K = k;
   kp.H = 0;
   return Statistics::Normalized2Nominal(bits, kp);
+}
+
+
+/* TranslatedDnaQuery as Queries::BuildQuery makes it for a DNA read with
+ * filtering off (src/queries.cpp:83-107, src/translated_dna_query.cpp:27-74);
+ * copies the translated codes to out (capacity cap) and returns their
+ * number.  Reads shorter than 3 bases are outside what the reference
+ * handles and must not be passed. */
+uint32_t gzr_translate_query(const gzo_params *p, const char *dna, uint32_t length,
+                             uint8_t *out, uint32_t cap) {
+  Sequence seq("read", std::string(dna, length));
+  Translator translator;
+  SequenceNoFilter filter;
+  ScoreMatrix m = make_matrix(p);
+  ProteinType t;
+  Statistics s(t);
+  Statistics::KarlinParameters ideal;
+  s.CalculateUngappedIdealKarlinParameters(m, &ideal);
+  TranslatedDnaQuery q(seq, p->delimiter, translator, &filter, m, ideal);
+  Query &base = q;  /* the static GetSequenceLength(uint32_t) hides the virtual one */
+  const uint32_t n = base.GetSequenceLength();
+  const AlphabetCoder::Code *codes = base.GetSequence();
+  for (uint32_t i = 0; i < n && i < cap; ++i) out[i] = codes[i];
+  return n;
 }
 
 } /* extern "C" */

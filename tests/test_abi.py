@@ -99,3 +99,18 @@ def test_tile_parameters_validate_without_device():
     assert L.gzb_set_tile_parameter(N.TILE_ORDER, 2) == 1
     assert L.gzb_set_tile_parameter(7, 1) == 1
     assert L.gzb_get_tile_parameter(7, ctypes.byref(v)) == 1
+
+
+def test_translated_layout_without_device(oracle):
+    import numpy as np
+    from gzb import native as N
+    for n in list(range(0, 50)) + [150, 151, 152, 99999]:
+        assert N.translated_query_length(n) == oracle.L.gzo_translated_length(n)
+    lengths = np.array([150, 2, 0, 7, 3], np.uint32)
+    offs, ql, total = N.translated_layout(lengths)
+    assert list(ql) == [7 + 6 * 50, 2, 2, 7 + 12, 13]
+    # consecutive queries share a delimiter
+    assert list(offs) == [0, 306, 307, 308, 326] and total == 326 + 13
+    # the device entry point refuses null buffers before touching a device
+    rc = N.lib().gzb_translate_dna_queries(None, None, None, 1, None, 25, None, None)
+    assert rc == 1

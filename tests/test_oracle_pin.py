@@ -261,3 +261,85 @@ def test_alignment_statistics_by_hand(oracle):
     assert (a["score"], a["start_q"], a["start_d"], a["end_q"], a["end_d"]) == (7, 1, 1, 5, 4)
     assert (a["alignment_length"], a["mismatches"], a["gap_openings"],
             a["gap_extensions"]) == (5, 0, 1, 0)
+
+
+# --- six-frame translation (query preparation) -------------------------------
+def _frames(codes, length):
+    """Split a translated query into its six frames (codes between the
+    frame delimiters)."""
+    slot = length // 3 + 1
+    out = []
+    for f in range(6):
+        s = codes[1 + f * slot: 1 + (f + 1) * slot]
+        out.append("".join(P.LETTERS[c] for c in s if c != P.DELIMITER))
+    return out
+
+
+def test_translation_known_answers(oracle):
+    # test/translator_test.cpp:22-43
+    read = b"GCCCGCCACCT"
+    q = oracle.translate_query(read, P.DELIMITER)
+    assert len(q) == 7 + 6 * 3
+    assert _frames(q, len(read)) == ["ARH", "PAT", "PPP", "RWR", "GGG", "VAG"]
+    read = b"GCCCGCCACC"
+    q = oracle.translate_query(read, P.DELIMITER)
+    assert _frames(q, len(read)) == ["ARH", "PAT", "PP", "GGG", "VAG", "WR"]
+    # a frame short of length/3 codons carries an extra delimiter
+    assert list(q[1 + 2 * 4 + 2:1 + 3 * 4]) == [P.DELIMITER, P.DELIMITER]
+
+
+def test_translation_frame_layout(oracle):
+    # test/translated_dna_query_test.cpp:29-31, :67-90: a 75-base read has
+    # 26-code frame slots, so position 27 opens frame 1 and 79 opens frame 3
+    read = b"AGCGAGAGCGAGTGGTGGGCAAAAAAACCTATACTGCAAAATTTTATGAAAGGTGCTTATTGTCCTCTGAATGAT"
+    q = oracle.translate_query(read, P.DELIMITER)
+    assert len(q) == 7 + 6 * 25
+    assert all(q[1 + 26 * f - 1] == P.DELIMITER for f in range(7))
+    assert q[27] != P.DELIMITER and q[79] != P.DELIMITER
+
+
+def test_translation_reverse_frames_are_complement_strand(oracle):
+    # test/test_dna.fa: test7 is the reverse complementary strand of test6
+    # (also test/dna_sequence_test.cpp:19-23)
+    t6 = b"GCTGCTGCTGCTGCTGCTGCTGCTGCTGCTGCTGCTGCTGCTGCTATGAAAGGTGCTTATTGTCCTCTGAATGAT"
+    t7 = b"ATCATTCAGAGGACAATAAGCACCTTTCATAGCAGCAGCAGCAGCAGCAGCAGCAGCAGCAGCAGCAGCAGCAGC"
+    f6 = _frames(oracle.translate_query(t6, P.DELIMITER), len(t6))
+    f7 = _frames(oracle.translate_query(t7, P.DELIMITER), len(t7))
+    assert f6[3:] == f7[:3] and f6[:3] == f7[3:]
+
+
+def test_translation_short_reads(oracle):
+    for read in (b"", b"A", b"AC"):
+        assert list(oracle.translate_query(read, P.DELIMITER)) == [P.DELIMITER] * 2
+
+
+def _random_read(rng, n):
+    # mostly ACGT with some N, lowercase and other IUPAC letters
+    letters = np.frombuffer(b"ACGTACGTACGTACGTacgtNNRYKM", np.uint8)
+    return bytes(letters[rng.integers(0, len(letters), n)])
+
+
+@pytest.mark.parametrize("seed", [30, 31])
+def test_translation_matches_reference(oracle, reference, params, seed):
+    rng = np.random.default_rng(seed)
+    for t in range(300):
+        n = int(rng.choice([3, 4, 5, 6, 7, 8, 150, int(rng.integers(3, 2000))]))
+        read = _random_read(rng, n)
+        r = reference.translate_query(params, read)
+        m = oracle.translate_query(read, params["delimiter"])
+        assert np.array_equal(m, r), (t, n)
+
+
+def test_translated_query_cutoffs_match_reference(oracle, reference, params):
+    # TranslatedDnaQuery::SetStaticalParameters (src/translated_dna_query.cpp:76-85)
+    # takes the composition of the whole translated query: delimiters, stop
+    # codons and unknown codons included
+    db = W.make_database(50, 33)
+    reads = W.make_reads(db, 60, 34)
+    for r in range(reads.number):
+        q = oracle.translate_query(reads.read(r), params["delimiter"])
+        lam, k, _ = reference.ungapped_karlin(params, q)
+        ml, mk, _ = P.ungapped_karlin_for_query(q[1:-1])
+        assert (np.float32(ml), np.float32(mk)) == (np.float32(lam), np.float32(k))
+        cut, trig = P.query_cutoffs([q[1:-1]])
+        assert reference.cutoffs(lam, k) == (int(cut[0]), int(trig[0]))
