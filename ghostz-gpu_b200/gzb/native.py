@@ -117,6 +117,7 @@ def _declare(L):
         "gzb_engine_set_database_with_index": [V, C.c_int32, V, C.c_uint64, V, C.c_uint32, V,
                                                C.c_uint64, V],
         "gzb_translate_dna_queries": [V, V, V, U32, V, C.c_uint8, V, V],
+        "gzb_query_karlin_cutoffs": [V, V, V, U32, V, U32, C.c_float, C.c_float, V, V, V, V],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -586,3 +587,40 @@ def translate_reads(dna, offsets, delimiter, device="cuda", stream=None):
                                 stream)
     codes = d_out.cpu().numpy()
     return codes, out_offs.astype(np.uint32), qlen
+
+
+# -- query preparation: per-query Karlin cutoffs ---------------------------------
+def query_karlin_cutoffs_async(d_codes, d_offsets, d_lengths, number_queries, matrix,
+                               d_cutoffs, d_triggers, d_karlin=None, ungapped_bits=7.0,
+                               trigger_bits=22.0, stream=None):
+    """gzb_query_karlin_cutoffs on device buffers; matrix is a host
+    (n, n) int32 score matrix."""
+    m = np.ascontiguousarray(matrix, dtype=np.int32)
+    check(lib().gzb_query_karlin_cutoffs(dptr(d_codes), dptr(d_offsets), dptr(d_lengths),
+                                         int(number_queries), hptr(m), int(m.shape[0]),
+                                         float(ungapped_bits), float(trigger_bits),
+                                         dptr(d_cutoffs), dptr(d_triggers), dptr(d_karlin),
+                                         stream_handle(stream)))
+
+
+def query_karlin_cutoffs(codes, offsets, lengths, matrix=None, ungapped_bits=7.0,
+                         trigger_bits=22.0, device="cuda"):
+    """Per-query ungapped X-drop and gapped-extension trigger computed on
+    the GPU for queries laid out in host arrays (whole queries, delimiters
+    included).  Returns (cutoffs int32, triggers int32, karlin float32 (n, 3)
+    = lambda, K, H)."""
+    import torch
+    from . import params as P
+    m = P.blosum62() if matrix is None else matrix
+    n = len(offsets)
+    if n == 0:
+        return np.zeros(0, np.int32), np.zeros(0, np.int32), np.zeros((0, 3), np.float32)
+    d_codes = torch.from_numpy(np.ascontiguousarray(codes, dtype=np.uint8)).to(device)
+    d_offs = torch.from_numpy(np.asarray(offsets, dtype=np.int64).copy()).to(device)
+    d_lens = torch.from_numpy(np.asarray(lengths, dtype=np.uint32).view(np.int32).copy()).to(device)
+    d_cut = torch.empty(n, dtype=torch.int32, device=device)
+    d_trig = torch.empty(n, dtype=torch.int32, device=device)
+    d_k = torch.empty(3 * n, dtype=torch.float32, device=device)
+    query_karlin_cutoffs_async(d_codes, d_offs, d_lens, n, m, d_cut, d_trig, d_k,
+                               ungapped_bits, trigger_bits)
+    return d_cut.cpu().numpy(), d_trig.cpu().numpy(), d_k.cpu().numpy().reshape(n, 3)

@@ -469,6 +469,28 @@ int gzb_translate_dna_queries(const uint8_t *d_dna, const uint64_t *d_offsets,
                               const uint64_t *d_out_offsets, uint8_t delimiter,
                               uint8_t *d_out, void *stream);
 
+
+/* ---- query preparation: per-query Karlin-Altschul cutoffs ----
+ * Replaces the per-query SetStaticalParameters of ProteinQuery and
+ * TranslatedDnaQuery (Statistics::CalculateUngappedKarlinParameters,
+ * src/statistics.cpp:205-229, over ext/karlin/src/karlin.c) and the cutoff
+ * conversion of AlignerGpu::SetQueriesData (src/aligner_gpu.cpp:228-238):
+ * for query r (codes d_codes[d_offsets[r] .. + d_lengths[r]), delimiters
+ * included) it computes lambda, K and H of its composition against the
+ * Robinson background and writes
+ *   d_cutoffs[r]  = floor(ungapped_bits * ln2 / lambda)           (X-drop)
+ *   d_triggers[r] = floor((trigger_bits * ln2 + ln K) / lambda)   (trigger)
+ * and, when d_karlin is not NULL, d_karlin[3r..3r+2] = lambda, K, H.  The
+ * aln defaults are ungapped_bits 7 and trigger_bits 22.  score_matrix is
+ * the host number_letters^2 protein matrix (20 regular letters first; at
+ * most 32 letters and a score range of at most 31).  Asynchronous on
+ * `stream`; nothing is allocated. */
+int gzb_query_karlin_cutoffs(const uint8_t *d_codes, const uint64_t *d_offsets,
+                             const uint32_t *d_lengths, uint32_t number_queries,
+                             const int32_t *score_matrix, uint32_t number_letters,
+                             float ungapped_bits, float trigger_bits, int32_t *d_cutoffs,
+                             int32_t *d_triggers, float *d_karlin, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

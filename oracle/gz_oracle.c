@@ -7,6 +7,7 @@
  */
 #include "gz_oracle.h"
 
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -1448,4 +1449,238 @@ uint32_t gzo_translate_query(const char *dna, uint32_t length, uint8_t delimiter
   }
   free(rc);
   return o;
+}
+
+/* ---- per-query Karlin-Altschul statistics ----
+ * The sums below keep the reference's order of operations (serial, one
+ * rounding per multiply and per add) so that the float results agree bit
+ * for bit; the series for K is the one of Karlin & Altschul (1990) as the
+ * reference's karlin.c evaluates it. */
+
+#define GZO_KARLIN_ITER_MAX 100
+#define GZO_SCORE_RANGE_MAX 11000
+
+/* Robinson & Robinson background, ARNDCQEGHILKMFPSTWYV order
+ * (src/statistics.cpp:154-176) */
+static const double kRobinson[20] = {78.05, 51.29, 44.87, 53.64, 19.25, 42.64, 62.95,
+                                     73.77, 21.99, 51.42, 90.19, 57.44, 22.43, 38.56,
+                                     52.03, 71.20, 58.41, 13.30, 32.16, 64.41};
+
+static int score_range_bad(int lo, int hi) {
+  return lo >= 0 || hi <= 0 || lo < -10000 || hi > 1000 || hi - lo > GZO_SCORE_RANGE_MAX;
+}
+
+static long gcd_long(long a, long b) {
+  long c;
+  b = b < 0 ? -b : b;
+  if (b > a) c = a, a = b, b = c;
+  while (b != 0) {
+    c = a % b;
+    a = b;
+    b = c;
+  }
+  return a;
+}
+
+/* lambda by bisection (karlin.c BlastKarlinLambdaBis) */
+static double lambda_bisect(const double *sp, int lo, int hi) {
+  if (score_range_bad(lo, hi)) return -1.0;
+  double lambda = 0.0, up = 0.5, sum, x0, x1;
+  for (;;) {
+    up *= 2;
+    x0 = exp(up);
+    x1 = pow(x0, lo - 1);
+    sum = 0.0;
+    if (x1 > 0.0) {
+      for (int i = lo; i <= hi; ++i) sum += sp[i] * (x1 *= x0);
+    } else {
+      for (int i = lo; i <= hi; ++i) sum += sp[i] * exp(up * i);
+    }
+    if (sum >= 1.0) break;
+    lambda = up;
+  }
+  for (int j = 0; j < 17; ++j) {
+    const double mid = (lambda + up) / 2.0;
+    x0 = exp(mid);
+    x1 = pow(x0, lo - 1);
+    sum = 0.0;
+    if (x1 > 0.0) {
+      for (int i = lo; i <= hi; ++i) sum += sp[i] * (x1 *= x0);
+    } else {
+      for (int i = lo; i <= hi; ++i) sum += sp[i] * exp(mid * i);
+    }
+    if (sum > 1.0)
+      up = mid;
+    else
+      lambda = mid;
+  }
+  return (lambda + up) / 2.0;
+}
+
+/* lambda by Newton-Raphson from 0.5 (karlin.c BlastKarlinLambdaNR) */
+static double lambda_newton(const double *sp, int lo, int hi) {
+  if (score_range_bad(lo, hi)) return -1.0;
+  double lambda = 0.5;
+  for (int j = 0; j < 20; ++j) {
+    double sum = -1.0, slope = 0.0;
+    if (lambda < 0.01) break;
+    const double x0 = exp(lambda);
+    double x1 = pow(x0, lo - 1);
+    if (x1 == 0.0) break;
+    for (int i = lo; i <= hi; ++i) {
+      const double t = sp[i] * (x1 *= x0);
+      sum += t;
+      slope += t * i;
+    }
+    const double step = sum / slope;
+    lambda -= step;
+    if (fabs(step / lambda) < 1.0e-5) {
+      if (lambda > 1.0e-5) return lambda;
+      break;
+    }
+  }
+  return lambda_bisect(sp, lo, hi);
+}
+
+/* relative entropy H (karlin.c BlastKarlinLtoH) */
+static double entropy(const double *sp, int lo, int hi, double lambda) {
+  if (lambda < 0.0 || score_range_bad(lo, hi)) return -1.0;
+  const double etolam = exp(lambda);
+  double etolami = pow(etolam, lo - 1), av = 0.0;
+  if (etolami > 0.0) {
+    for (int s = lo; s <= hi; ++s) av += sp[s] * s * (etolami *= etolam);
+  } else {
+    for (int s = lo; s <= hi; ++s) av += sp[s] * s * exp(lambda * s);
+  }
+  return lambda * av;
+}
+
+/* K from lambda and H (karlin.c BlastKarlinLHtoK): the series
+ * sum_j (1/j) [E(exp(lambda S_j); S_j < 0) + P(S_j >= 0)] over the j-fold
+ * convolutions of the score distribution, closed with a geometric tail. */
+static double karlin_k(const double *sp, int low, int high, double lambda, double H) {
+  if (lambda <= 0.0 || H <= 0.0) return -1.0;
+  const int range = high - low;
+  const double av = H / lambda;
+  const double etolam = exp(lambda);
+  if (low == -1 || high == 1) return av * (1.0 - 1.0 / etolam);
+  double sumlimit = 0.01;
+  const int iter = GZO_KARLIN_ITER_MAX;
+  if (iter * range + 1 > GZO_KARLIN_ITER_MAX * GZO_SCORE_RANGE_MAX + 1) return -1.0;
+  double *cur = (double *)calloc((size_t)iter * range + 1, sizeof(double));
+  double *nxt = (double *)calloc((size_t)iter * range + 1, sizeof(double));
+  const double *p = sp + low;  /* p[u] = probability of score low + u */
+  double sum = 1.0, oldsum = 1.0, oldsum2 = 1.0, total = 0.0, K;
+  int lo = 0, hi = 0, j = 0;
+  cur[0] = 1.0;
+  while (j < iter && sum > sumlimit) {
+    lo += low;
+    hi += high;
+    const int top = hi - lo;
+    /* next distribution: entry k takes u = first..last in increasing order */
+    for (int k = 0; k <= top; ++k) {
+      const int first = range - (top - k) > 0 ? range - (top - k) : 0;
+      const int last = k < range ? k : range;
+      double s = 0.0;
+      for (int u = first; u <= last; ++u) s += cur[k - u] * p[u];
+      nxt[k] = s;
+    }
+    double etolami = pow(etolam, lo - 1);
+    int i = lo, idx = 0;
+    double s = 0.0;
+    for (; i != 0; ++i, ++idx) {
+      etolami *= etolam;
+      s += nxt[idx] * etolami;
+    }
+    for (; i <= hi; ++i, ++idx) s += nxt[idx];
+    oldsum2 = oldsum;
+    oldsum = s;
+    double *t = cur;
+    cur = nxt;
+    nxt = t;
+    sum = s / ++j;
+    total += sum;
+  }
+  const double ratio = oldsum / oldsum2;
+  if (ratio >= (1.0 - sumlimit * 0.001)) {
+    K = -1.0;
+  } else {
+    sumlimit *= 0.01;
+    while (sum > sumlimit) {
+      oldsum *= ratio;
+      total += sum = oldsum / ++j;
+    }
+    long delta = -low;
+    for (int i = 1; i <= range && delta > 1; ++i)
+      if (p[i] != 0.0) delta = gcd_long(delta, i);
+    if (delta * etolam > 0.05) {
+      const double etolami = pow(etolam, -delta);
+      K = delta * exp(-2.0 * total) / (av * (1.0 - etolami));
+    } else {
+      K = -delta * exp(-2.0 * total) / (av * (exp(-delta * lambda) - 1));
+    }
+  }
+  free(cur);
+  free(nxt);
+  return K;
+}
+
+int gzo_query_karlin(const gzo_params *p, const uint8_t *seq, uint32_t length,
+                     float ungapped_bits, float trigger_bits, float *lambda, float *k,
+                     float *h, int32_t *cutoff, int32_t *trigger) {
+  const int n = p->number_letters;
+  const int max_code = n - 1, max_regular = 19;
+  double bg[64], freq[64];
+  /* background: Robinson, normalised (Statistics::Statistics and Normalize) */
+  double sum = 0.0;
+  for (int c = 0; c <= max_code; ++c) bg[c] = c < 20 ? kRobinson[c] : 0.0;
+  for (int c = 0; c <= max_code; ++c) sum += bg[c];
+  for (int c = 0; c <= max_code; ++c) {
+    bg[c] /= sum;
+    bg[c] *= 1.0;
+  }
+  /* query composition with a pseudo-count for absent letters
+   * (ComposeSequenceFrequency, then Normalize) */
+  for (int c = 0; c <= max_code; ++c) freq[c] = 0.0;
+  for (uint32_t i = 0; i < length; ++i)
+    if (seq[i] <= max_regular) ++freq[seq[i]];
+  for (int c = 0; c <= max_code; ++c)
+    if (freq[c] < 1.0) ++freq[c];
+  sum = 0.0;
+  for (int c = 0; c <= max_code; ++c) sum += freq[c];
+  for (int c = 0; c <= max_code; ++c) {
+    freq[c] /= sum;
+    freq[c] *= 1.0;
+  }
+  /* score probabilities (CalculateScoreProbabilities) */
+  int lo = p->score_matrix[0], hi = p->score_matrix[0];
+  for (int i = 0; i < n * n; ++i) {
+    lo = p->score_matrix[i] < lo ? p->score_matrix[i] : lo;
+    hi = p->score_matrix[i] > hi ? p->score_matrix[i] : hi;
+  }
+  double *sp0 = (double *)calloc((size_t)(hi - lo + 1), sizeof(double));
+  double *sp = sp0 - lo;
+  for (int c1 = 0; c1 <= max_code; ++c1)
+    for (int c2 = 0; c2 <= max_code; ++c2)
+      sp[p->score_matrix[c1 * n + c2]] += freq[c1] * bg[c2];
+  double ssum = 0.0;
+  for (int i = lo; i <= hi; ++i)
+    if (sp[i] > 0.0) ssum += sp[i];
+  for (int i = lo; i <= hi; ++i)
+    if (sp[i] > 0.0) sp[i] /= ssum;
+  /* BlastKarlinBlkCalc: each parameter rounded to float before the next */
+  const float l = (float)lambda_newton(sp, lo, hi);
+  const float hh = (float)entropy(sp, lo, hi, l);
+  const float kk = (float)karlin_k(sp, lo, hi, l, hh);
+  free(sp0);
+  *lambda = l;
+  *k = kk;
+  *h = hh;
+  /* NormalizedCutoff2NominalCutoff and Normalized2Nominal in float */
+  const float ln2 = (float)log(2.0);
+  const float c = (ungapped_bits * ln2) / l;
+  const float t = (trigger_bits * ln2 + logf(kk)) / l;
+  *cutoff = (int32_t)floorf(c);
+  *trigger = (int32_t)floorf(t);
+  return 0;
 }

@@ -193,6 +193,17 @@ uint32_t gzo_translated_length(uint32_t length);
 uint32_t gzo_translate_query(const char *dna, uint32_t length, uint8_t delimiter,
                              uint8_t *out);
 
+
+/* Ungapped Karlin-Altschul parameters of one query against the Robinson
+ * background and the integer cutoffs derived from them
+ * (Statistics::CalculateUngappedKarlinParameters, src/statistics.cpp:205-229,
+ * with ext/karlin/src/karlin.c BlastKarlinBlkCalc; cutoffs
+ * src/statistics.cpp:28-43 as used at src/aligner_gpu.cpp:228-238).  seq
+ * is the whole query, delimiters included; returns 0. */
+int gzo_query_karlin(const gzo_params *p, const uint8_t *seq, uint32_t length,
+                     float ungapped_bits, float trigger_bits, float *lambda, float *k,
+                     float *h, int32_t *cutoff, int32_t *trigger);
+
 #ifdef __cplusplus
 }
 #endif

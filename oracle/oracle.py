@@ -99,6 +99,9 @@ class Oracle:
         L.gzo_presearch_hits.argtypes = [C.c_void_p, C.POINTER(u32p), C.POINTER(u32p),
                                          C.POINTER(u32p)]
         L.gzo_presearch_hits.restype = C.c_size_t
+        L.gzo_query_karlin.argtypes = [C.c_void_p, u8p, C.c_uint32, C.c_float, C.c_float,
+                                       C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                       C.POINTER(C.c_float), i32p, i32p]
         L.gzo_translated_length.argtypes = [C.c_uint32]
         L.gzo_translated_length.restype = C.c_uint32
         L.gzo_translate_query.argtypes = [C.c_char_p, C.c_uint32, C.c_uint8, u8p]
@@ -178,6 +181,18 @@ class Oracle:
         v[0] = C.c_int32(v[0]).value
         return dict(zip(("score", "start_q", "start_d", "end_q", "end_d", "alignment_length",
                          "mismatches", "gap_openings", "gap_extensions"), v))
+
+    def query_karlin(self, params, seq, ungapped_bits=7.0, trigger_bits=22.0):
+        """(lambda, K, H, ungapped cutoff, gapped trigger) of one whole query
+        (delimiters included)."""
+        pr = _Params(params)
+        s = np.ascontiguousarray(seq, dtype=np.uint8)
+        lam, k, h = C.c_float(), C.c_float(), C.c_float()
+        cut, trig = np.zeros(1, np.int32), np.zeros(1, np.int32)
+        self.L.gzo_query_karlin(pr.ptr, _p(s, u8p), len(s), ungapped_bits, trigger_bits,
+                                C.byref(lam), C.byref(k), C.byref(h), _p(cut, i32p),
+                                _p(trig, i32p))
+        return lam.value, k.value, h.value, int(cut[0]), int(trig[0])
 
     def translate_query(self, dna, delimiter):
         """Translated query codes of one DNA read (bytes): the six frames in

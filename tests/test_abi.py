@@ -114,3 +114,20 @@ def test_translated_layout_without_device(oracle):
     # the device entry point refuses null buffers before touching a device
     rc = N.lib().gzb_translate_dna_queries(None, None, None, 1, None, 25, None, None)
     assert rc == 1
+
+
+def test_karlin_cutoffs_validate_without_device():
+    import numpy as np
+    from gzb import native as N
+    from gzb import params as P
+    m = P.blosum62()
+    L = N.lib()
+    f = L.gzb_query_karlin_cutoffs
+    # zero queries: validated and returns before touching a device
+    assert f(None, None, None, 0, N.hptr(np.ascontiguousarray(m, np.int32)), 25, 7.0, 22.0,
+             None, None, None, None) == 0
+    assert f(None, None, None, 0, None, 25, 7.0, 22.0, None, None, None, None) == 1
+    wide = np.ascontiguousarray(m * 3, np.int32)  # score range 45 > 31
+    assert f(None, None, None, 0, N.hptr(wide), 25, 7.0, 22.0, None, None, None, None) == 4
+    assert f(None, None, None, 1, N.hptr(np.ascontiguousarray(m, np.int32)), 25, 7.0, 22.0,
+             None, None, None, None) == 1

@@ -343,3 +343,26 @@ def test_translated_query_cutoffs_match_reference(oracle, reference, params):
         assert (np.float32(ml), np.float32(mk)) == (np.float32(lam), np.float32(k))
         cut, trig = P.query_cutoffs([q[1:-1]])
         assert reference.cutoffs(lam, k) == (int(cut[0]), int(trig[0]))
+
+
+# --- per-query Karlin statistics (query preparation) ---------------------------
+def test_query_karlin_matches_reference(oracle, reference, params):
+    # Statistics::CalculateUngappedKarlinParameters (src/statistics.cpp:205-229)
+    # and the cutoffs of src/aligner_gpu.cpp:228-238, on protein queries,
+    # translated queries and skewed short compositions
+    rng = np.random.default_rng(35)
+    db = W.make_database(40, 36)
+    reads = W.make_reads(db, 100, 37)
+    cases = [np.concatenate([[25], W.random_residues(rng, int(rng.integers(5, 3000))), [25]])
+             for _ in range(150)]
+    cases += [oracle.translate_query(reads.read(r), 25) for r in range(reads.number)]
+    for _ in range(150):
+        letters = rng.choice(25, size=int(rng.integers(1, 6)), replace=False)
+        body = rng.choice(letters, size=int(rng.integers(1, 400))).astype(np.uint8)
+        cases.append(np.concatenate([[25], body, [25]]).astype(np.uint8))
+    for q in cases:
+        lam, k, h = reference.ungapped_karlin(params, q)
+        ol, ok, oh, cut, trig = oracle.query_karlin(params, q)
+        assert (np.float32(ol), np.float32(ok), np.float32(oh)) == \
+            (np.float32(lam), np.float32(k), np.float32(h)), q
+        assert (cut, trig) == reference.cutoffs(lam, k)
