@@ -118,6 +118,8 @@ def _declare(L):
                                                C.c_uint64, V],
         "gzb_translate_dna_queries": [V, V, V, U32, V, C.c_uint8, V, V],
         "gzb_query_karlin_cutoffs": [V, V, V, U32, V, U32, C.c_float, C.c_float, V, V, V, V],
+        "gzb_seg_translated_queries": [V, V, V, U32, V, V],
+        "gzb_seg_protein_queries": [V, V, V, U32, V, V],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -624,3 +626,113 @@ def query_karlin_cutoffs(codes, offsets, lengths, matrix=None, ungapped_bits=7.0
     query_karlin_cutoffs_async(d_codes, d_offs, d_lens, n, m, d_cut, d_trig, d_k,
                                ungapped_bits, trigger_bits)
     return d_cut.cpu().numpy(), d_trig.cpu().numpy(), d_k.cpu().numpy().reshape(n, 3)
+
+
+# -- query preparation: SEG and whole-query preparation --------------------------
+SEG_WINDOW = 12
+
+
+def seg_translated_queries_async(d_queries, d_query_offsets, d_read_lengths, number_queries,
+                                 d_status=None, stream=None):
+    check(lib().gzb_seg_translated_queries(dptr(d_queries), dptr(d_query_offsets),
+                                           dptr(d_read_lengths), int(number_queries),
+                                           dptr(d_status), stream_handle(stream)))
+
+
+def seg_protein_queries_async(d_codes, d_offsets, d_lengths, number_queries, d_status=None,
+                              stream=None):
+    check(lib().gzb_seg_protein_queries(dptr(d_codes), dptr(d_offsets), dptr(d_lengths),
+                                        int(number_queries), dptr(d_status),
+                                        stream_handle(stream)))
+
+
+def encode_protein_for_seg(letters):
+    """Protein letters -> codes for gzb_seg_protein_queries: lower-case
+    letters (which the reference's SEG does not count) get code + 32."""
+    from . import params as P
+    raw = np.frombuffer(bytes(letters), dtype=np.uint8)
+    codes = P.encode(bytes(raw).decode("latin-1").upper()).astype(np.uint8)
+    lower = (raw >= ord("a")) & (raw <= ord("z"))
+    codes[lower] += 32
+    return codes
+
+
+def prepare_translated_queries(dna, offsets, filter=True, matrix=None, ungapped_bits=7.0,
+                               trigger_bits=22.0, device="cuda"):
+    """Query preparation of translated-DNA searches on the GPU: six-frame
+    translation, SEG (filter=True, the aln default) and per-query cutoffs.
+    dna: uint8 ASCII bases back to back; offsets: number_reads + 1 read
+    boundaries.  Returns host arrays (codes, offsets uint32, lengths uint32,
+    cutoffs int32, triggers int32) in the engine's query layout."""
+    import torch
+    from . import params as P
+    offsets = np.asarray(offsets, dtype=np.uint64)
+    n = len(offsets) - 1
+    lengths = np.diff(offsets).astype(np.uint32)
+    out_offs, qlen, total = translated_layout(lengths)
+    if n == 0:
+        z = np.zeros(0, np.uint32)
+        return np.zeros(0, np.uint8), z, z, z.astype(np.int32), z.astype(np.int32)
+    d_dna = torch.from_numpy(np.ascontiguousarray(dna, dtype=np.uint8)).to(device)
+    d_offs = torch.from_numpy(offsets[:-1].view(np.int64).copy()).to(device)
+    d_lens = torch.from_numpy(lengths.view(np.int32).copy()).to(device)
+    d_qoffs = torch.from_numpy(out_offs.view(np.int64).copy()).to(device)
+    d_qlen = torch.from_numpy(qlen.view(np.int32).copy()).to(device)
+    d_out = torch.empty(total, dtype=torch.uint8, device=device)
+    d_status = torch.zeros(1, dtype=torch.int32, device=device)
+    d_cut = torch.empty(n, dtype=torch.int32, device=device)
+    d_trig = torch.empty(n, dtype=torch.int32, device=device)
+    translate_dna_queries_async(d_dna, d_offs, d_lens, n, d_qoffs, d_out, P.DELIMITER)
+    if filter:
+        seg_translated_queries_async(d_out, d_qoffs, d_lens, n, d_status)
+    m = P.blosum62() if matrix is None else matrix
+    query_karlin_cutoffs_async(d_out, d_qoffs, d_qlen, n, m, d_cut, d_trig, None,
+                               ungapped_bits, trigger_bits)
+    if int(d_status.item()) != 0:
+        raise GzbError(f"SEG left {int(d_status.item())} frames unmasked")
+    return (d_out.cpu().numpy(), out_offs.astype(np.uint32), qlen, d_cut.cpu().numpy(),
+            d_trig.cpu().numpy())
+
+
+def prepare_protein_queries(codes, offsets, lengths, filter=True, matrix=None,
+                            ungapped_bits=7.0, trigger_bits=22.0, device="cuda"):
+    """Query preparation of protein searches on the GPU: SEG (filter=True,
+    the aln default) and per-query cutoffs, for queries in the engine layout
+    (codes from encode_protein_for_seg keep lower-case letters out of SEG's
+    compositions).  Returns host arrays (codes, cutoffs, triggers)."""
+    import torch
+    from . import params as P
+    offsets = np.asarray(offsets, dtype=np.uint64)
+    lengths = np.asarray(lengths, dtype=np.uint32)
+    n = len(offsets)
+    if n == 0:
+        return np.zeros(0, np.uint8), np.zeros(0, np.int32), np.zeros(0, np.int32)
+    d_codes = torch.from_numpy(np.ascontiguousarray(codes, dtype=np.uint8)).to(device)
+    d_offs = torch.from_numpy(offsets.view(np.int64).copy()).to(device)
+    d_lens = torch.from_numpy(lengths.view(np.int32).copy()).to(device)
+    d_status = torch.zeros(1, dtype=torch.int32, device=device)
+    d_cut = torch.empty(n, dtype=torch.int32, device=device)
+    d_trig = torch.empty(n, dtype=torch.int32, device=device)
+    m = P.blosum62() if matrix is None else matrix
+    if filter:
+        seg_protein_queries_async(d_codes, d_offs, d_lens, n, d_status)
+    query_karlin_cutoffs_async(d_codes, d_offs, d_lens, n, m, d_cut, d_trig, None,
+                               ungapped_bits, trigger_bits)
+    cut, trig = d_cut.cpu().numpy(), d_trig.cpu().numpy()
+    if filter:
+        # a protein the filter refuses (shorter than the window) is held as
+        # [delimiter] + zeros, its last code 0 rather than a delimiter, and
+        # its statistics are those of that buffer
+        short = np.flatnonzero(lengths - 2 < SEG_WINDOW)
+        if len(short):
+            bufs = [np.concatenate([[P.DELIMITER], np.zeros(int(lengths[i]) - 1, np.uint8)])
+                    for i in short]
+            sc, so, sl = (np.concatenate(bufs).astype(np.uint8),
+                          np.concatenate([[0], np.cumsum([len(b) for b in bufs])[:-1]]),
+                          np.array([len(b) for b in bufs], np.uint32))
+            c2, t2, _ = query_karlin_cutoffs(sc, so, sl, m, ungapped_bits, trigger_bits,
+                                             device)
+            cut[short], trig[short] = c2, t2
+    if int(d_status.item()) != 0:
+        raise GzbError(f"SEG left {int(d_status.item())} queries unmasked")
+    return d_codes.cpu().numpy(), cut, trig

@@ -491,6 +491,37 @@ int gzb_query_karlin_cutoffs(const uint8_t *d_codes, const uint64_t *d_offsets,
                              float ungapped_bits, float trigger_bits, int32_t *d_cutoffs,
                              int32_t *d_triggers, float *d_karlin, void *stream);
 
+
+/* ---- query preparation: SEG low-complexity masking (aln -F T, the
+ * default) ----
+ * Replaces SequenceSegFilter (src/sequence_seg_filter.cpp:17-23 over
+ * ext/seg/src/seg.cpp, window 12) as the query builders apply it, in place
+ * on device query codes:
+ *  - gzb_seg_translated_queries masks the six frames of each translated
+ *    query written by gzb_translate_dna_queries (d_query_offsets = its
+ *    d_out_offsets, d_read_lengths = the reads' base counts); a frame of
+ *    fewer than 12 codons becomes unknown codes
+ *    (src/translated_dna_query.cpp:56-73);
+ *  - gzb_seg_protein_queries masks the body of each protein query in the
+ *    engine layout (d_offsets = leading delimiter, d_lengths = residues +
+ *    2); a protein of fewer than 12 residues gets a body of code 0, the
+ *    zero-filled buffer ProteinQuery keeps when the filter refuses it
+ *    (src/protein_query.cpp:39-49).  Only codes 0-19 count as amino acids;
+ *    a caller that must keep a letter out of the compositions (the
+ *    reference's SEG ignores lower-case letters) passes its code + 32,
+ *    which comes back as the code.
+ * Masked residues become the unknown code 24.  d_status (optional, one
+ * zeroed uint32 on the device) counts sequences left unmasked because they
+ * exceed 65535 residues or nest the search deeper than the kernel's stack.
+ * The first call on a device uploads a 512 KB table (synchronously); later
+ * calls are asynchronous on `stream`. */
+int gzb_seg_translated_queries(uint8_t *d_queries, const uint64_t *d_query_offsets,
+                               const uint32_t *d_read_lengths, uint32_t number_queries,
+                               uint32_t *d_status, void *stream);
+int gzb_seg_protein_queries(uint8_t *d_codes, const uint64_t *d_offsets,
+                            const uint32_t *d_lengths, uint32_t number_queries,
+                            uint32_t *d_status, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -8,6 +8,7 @@
 #include "gz_oracle.h"
 
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -1683,4 +1684,213 @@ int gzo_query_karlin(const gzo_params *p, const uint8_t *seq, uint32_t length,
   *cutoff = (int32_t)floorf(c);
   *trigger = (int32_t)floorf(t);
   return 0;
+}
+
+/* ---- SEG (Wootton & Federhen) as the reference's ext/seg implements it ----
+ * Parameters: window 12, low cut 2.2 bits, high cut 2.5 bits, window
+ * entropies keyed by the window's first position, trimming over at most
+ * 100 shorter lengths (ext/seg/src/seg.cpp:58-76). */
+
+#define SEG_WINDOW 12
+#define SEG_LOW_CUT 2.2
+#define SEG_HIGH_CUT 2.5
+#define SEG_MAX_TRIM 100
+#define SEG_LN_FACT_SIZE 65536
+
+static double seg_ln_fact[SEG_LN_FACT_SIZE];
+static double seg_entropy12[SEG_WINDOW + 1];
+static int seg_ready = 0;
+
+double gzo_ln_factorial6(uint32_t n) {
+  /* ln(n!) from the long-double log-gamma, rounded to 6 decimals through
+   * its decimal text, which is how the reference's table is written */
+  char text[64];
+  snprintf(text, sizeof text, "%.6Lf", n < 2 ? 0.0L : lgammal((long double)n + 1.0L));
+  return strtod(text, NULL);
+}
+
+static void seg_init(void) {
+  if (seg_ready) return;
+  for (uint32_t n = 0; n < SEG_LN_FACT_SIZE; ++n) seg_ln_fact[n] = gzo_ln_factorial6(n);
+  const double w = SEG_WINDOW, ln2 = log(2.0);
+  for (int i = 1; i <= SEG_WINDOW; ++i) {
+    const double x = i / w;
+    seg_entropy12[i] = -x * log(x) / ln2;
+  }
+  seg_ready = 1;
+}
+
+/* index of an amino-acid letter SEG counts, or -1 (upper case only) */
+static int seg_class(char c) {
+  static const char *aa = "ACDEFGHIKLMNPQRSTVWY";
+  for (int i = 0; i < 20; ++i)
+    if (aa[i] == c) return i;
+  return -1;
+}
+
+/* counts of the window's letters, sorted in decreasing order, 0-terminated */
+static int seg_state(const char *s, int n, int *state) {
+  int comp[20] = {0};
+  for (int i = 0; i < n; ++i) {
+    const int k = seg_class(s[i]);
+    if (k >= 0) ++comp[k];
+  }
+  int m = 0;
+  for (int k = 0; k < 20; ++k)
+    if (comp[k]) state[m++] = comp[k];
+  for (int a = 1; a < m; ++a)  /* insertion sort, decreasing */
+    for (int b = a; b > 0 && state[b - 1] < state[b]; --b) {
+      const int t = state[b];
+      state[b] = state[b - 1];
+      state[b - 1] = t;
+    }
+  for (int k = m; k <= 20; ++k) state[k] = 0;
+  return m;
+}
+
+static double seg_entropy(const int *state) {
+  int total = 0, m = 0;
+  for (; state[m]; ++m) total += state[m];
+  double ent = 0.0;
+  if (total == SEG_WINDOW) {
+    for (int i = 0; i < m; ++i) ent += seg_entropy12[state[i]];
+    return ent;
+  }
+  if (total == 0) return 0.0;
+  const double r = 1.0 / (double)total;
+  for (int i = 0; i < m; ++i) {
+    const double v = state[i];
+    ent += v * log(v * r);
+  }
+  return -ent * r / log(2.0);
+}
+
+/* entropy of the window keyed by position i of a sequence of n letters:
+ * the window starting at i, or the last full window past n - 12 */
+static double seg_h(const char *s, int n, int i) {
+  int state[21];
+  const int start = i < n - SEG_WINDOW ? i : n - SEG_WINDOW;
+  seg_state(s + start, SEG_WINDOW, state);
+  return seg_entropy(state);
+}
+
+/* ln of the probability of the window's composition
+ * (Seg::GetProbability: LnAss + LnPerm - n ln 20) */
+static double seg_probability(const int *state, int total) {
+  double ass = seg_ln_fact[20];
+  if (state[0] != 0) {
+    int left = 20, run = 1, prev = state[0];
+    for (int i = 1; i < 20; ++i) {
+      const int v = state[i];
+      if (v == prev) {
+        ++run;
+      } else {
+        left -= run;
+        ass -= seg_ln_fact[run];
+        if (v == 0) {
+          run = left;
+          break;
+        }
+        run = 1;
+      }
+      prev = v;
+    }
+    ass -= seg_ln_fact[run];
+  }
+  double perm = seg_ln_fact[total];
+  for (int i = 0; state[i] != 0; ++i) perm -= seg_ln_fact[state[i]];
+  return ass + perm - (double)total * log(20.0);
+}
+
+/* Seg::Trim over s[0..n): the sub-window of length > max(1, n - 100) with
+ * the least probable composition (first found wins) */
+static void seg_trim(const char *s, int n, int *left, int *right) {
+  int best_left = 0, best_right = n - 1;
+  int min_length = 1;
+  if (n - SEG_MAX_TRIM > min_length) min_length = n - SEG_MAX_TRIM;
+  double best = 1.0;
+  int state[21];
+  for (int len = n; len > min_length; --len) {
+    for (int i = 0; i + len <= n; ++i) {
+      seg_state(s + i, len, state);
+      const double p = seg_probability(state, len);
+      if (p < best) {
+        best = p;
+        best_left = i;
+        best_right = len + i - 1;
+      }
+    }
+  }
+  *left += best_left;
+  *right -= n - best_right - 1;
+}
+
+/* Seg::MakeSeqments over s[0..n) (recursing into the part left of a
+ * trimmed segment), marking every segment in mask */
+static void seg_segments(const char *s, int n, unsigned char *mask) {
+  if (n < SEG_WINDOW) return;
+  int left_limit = 0;
+  for (int i = 0; i <= n - 1; ++i) {
+    if (seg_h(s, n, i) > SEG_LOW_CUT) continue;
+    int lo = i;
+    while (lo >= left_limit && seg_h(s, n, lo) <= SEG_HIGH_CUT) --lo;
+    const int left_i = lo + 1;
+    int hi = i;
+    while (hi <= n - 1 && seg_h(s, n, hi) <= SEG_HIGH_CUT) ++hi;
+    const int right_i = hi - 1;
+    int left_end = left_i, right_end = right_i;
+    seg_trim(s + left_end, right_end - left_end + 1, &left_end, &right_end);
+    if (i < left_end) seg_segments(s + left_i, left_end - left_i, mask + left_i);
+    for (int k = left_end; k <= right_end; ++k) mask[k] = 1;
+    i = right_i < right_end ? right_i : right_end;
+    left_limit = i + 1;
+  }
+}
+
+int gzo_seg_mask(const char *seq, uint32_t length, char *out) {
+  if (length < SEG_WINDOW) return 1;
+  seg_init();
+  unsigned char *mask = (unsigned char *)calloc(length, 1);
+  seg_segments(seq, (int)length, mask);
+  for (uint32_t i = 0; i < length; ++i) {
+    const char c = seq[i];
+    out[i] = mask[i] ? 'x' : (c >= 'a' && c <= 'z' ? (char)(c - 'a' + 'A') : c);
+  }
+  free(mask);
+  return 0;
+}
+
+uint32_t gzo_translate_query_seg(const char *dna, uint32_t length, uint8_t delimiter,
+                                 uint8_t *out) {
+  const uint32_t n = gzo_translate_query(dna, length, delimiter, out);
+  if (length < 3) return n;
+  const uint32_t slot = length / 3 + 1;
+  char letters[SEG_LN_FACT_SIZE], masked[SEG_LN_FACT_SIZE];
+  for (int f = 0; f < 6; ++f) {
+    uint8_t *q = out + 1 + f * slot;
+    uint32_t m = 0;
+    while (m < slot && q[m] != delimiter) ++m;
+    if (m >= SEG_LN_FACT_SIZE) return 0;
+    for (uint32_t i = 0; i < m; ++i) letters[i] = kProteinLetters[q[i]];
+    if (gzo_seg_mask(letters, m, masked) != 0) {
+      for (uint32_t i = 0; i < m; ++i) q[i] = protein_code('X');
+    } else {
+      for (uint32_t i = 0; i < m; ++i) q[i] = masked[i] == 'x' ? protein_code('X')
+                                                                : protein_code(masked[i]);
+    }
+  }
+  return n;
+}
+
+void gzo_protein_query_seg(const char *letters, uint32_t length, uint8_t delimiter,
+                           uint8_t *out) {
+  memset(out, 0, length + 2);
+  out[0] = delimiter;
+  char *masked = (char *)malloc(length + 1);
+  if (gzo_seg_mask(letters, length, masked) == 0) {
+    for (uint32_t i = 0; i < length; ++i)
+      out[1 + i] = masked[i] == 'x' ? protein_code('X') : protein_code(masked[i]);
+    out[length + 1] = delimiter;
+  }
+  free(masked);
 }

@@ -204,6 +204,31 @@ int gzo_query_karlin(const gzo_params *p, const uint8_t *seq, uint32_t length,
                      float ungapped_bits, float trigger_bits, float *lambda, float *k,
                      float *h, int32_t *cutoff, int32_t *trigger);
 
+
+/* SEG low-complexity masking of one protein string with window 12
+ * (seg::Seg::MaskSequence, ext/seg/src/seg.cpp:98-112, as
+ * SequenceSegFilter uses it, src/sequence_seg_filter.cpp:12-23).  Writes
+ * the masked string (letters upper-cased, masked residues 'x') to out and
+ * returns 0, or returns 1 without writing when the string is shorter than
+ * the window. */
+int gzo_seg_mask(const char *seq, uint32_t length, char *out);
+/* gzo_translate_query with the SEG filter on (Queries::GetFilter,
+ * src/queries.cpp:50-63): each frame is masked, and a frame shorter than
+ * the window becomes unknown codes (src/translated_dna_query.cpp:59-65). */
+uint32_t gzo_translate_query_seg(const char *dna, uint32_t length, uint8_t delimiter,
+                                 uint8_t *out);
+/* ln(n!) rounded to 6 decimals, as the SEG tables hold it; n <= 65535. */
+double gzo_ln_factorial6(uint32_t n);
+
+
+/* ProteinQuery's codes with the SEG filter on
+ * (ProteinQuery::SetEncodedSequence, src/protein_query.cpp:39-49): length + 2
+ * codes, [delimiter] masked body [delimiter]; a protein shorter than the
+ * window keeps the zero-filled buffer behind the leading delimiter (body
+ * and last code 0). */
+void gzo_protein_query_seg(const char *letters, uint32_t length, uint8_t delimiter,
+                           uint8_t *out);
+
 #ifdef __cplusplus
 }
 #endif

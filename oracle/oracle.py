@@ -102,6 +102,12 @@ class Oracle:
         L.gzo_query_karlin.argtypes = [C.c_void_p, u8p, C.c_uint32, C.c_float, C.c_float,
                                        C.POINTER(C.c_float), C.POINTER(C.c_float),
                                        C.POINTER(C.c_float), i32p, i32p]
+        L.gzo_seg_mask.argtypes = [C.c_char_p, C.c_uint32, C.c_char_p]
+        L.gzo_translate_query_seg.argtypes = [C.c_char_p, C.c_uint32, C.c_uint8, u8p]
+        L.gzo_translate_query_seg.restype = C.c_uint32
+        L.gzo_ln_factorial6.argtypes = [C.c_uint32]
+        L.gzo_protein_query_seg.argtypes = [C.c_char_p, C.c_uint32, C.c_uint8, u8p]
+        L.gzo_ln_factorial6.restype = C.c_double
         L.gzo_translated_length.argtypes = [C.c_uint32]
         L.gzo_translated_length.restype = C.c_uint32
         L.gzo_translate_query.argtypes = [C.c_char_p, C.c_uint32, C.c_uint8, u8p]
@@ -193,6 +199,29 @@ class Oracle:
                                 C.byref(lam), C.byref(k), C.byref(h), _p(cut, i32p),
                                 _p(trig, i32p))
         return lam.value, k.value, h.value, int(cut[0]), int(trig[0])
+
+    def seg_mask(self, seq):
+        """SEG-masked copy of a protein string (bytes), or None when it is
+        shorter than the window."""
+        seq = bytes(seq)
+        out = C.create_string_buffer(max(len(seq), 1))
+        rc = self.L.gzo_seg_mask(seq, len(seq), out)
+        return None if rc else out.raw[:len(seq)]
+
+    def protein_query_seg(self, letters, delimiter):
+        """ProteinQuery codes (length + 2) of one protein with SEG on."""
+        letters = bytes(letters)
+        out = np.zeros(len(letters) + 2, np.uint8)
+        self.L.gzo_protein_query_seg(letters, len(letters), int(delimiter), _p(out, u8p))
+        return out
+
+    def translate_query_seg(self, dna, delimiter):
+        """translate_query with the SEG filter on."""
+        dna = bytes(dna)
+        out = np.zeros(self.L.gzo_translated_length(len(dna)), np.uint8)
+        n = self.L.gzo_translate_query_seg(dna, len(dna), int(delimiter), _p(out, u8p))
+        assert n == len(out)
+        return out
 
     def translate_query(self, dna, delimiter):
         """Translated query codes of one DNA read (bytes): the six frames in
@@ -323,6 +352,14 @@ class Reference:
         L.gzr_normalized_to_nominal.argtypes = [C.c_float, C.c_float, C.c_float]
         L.gzr_translate_query.argtypes = [C.c_void_p, C.c_char_p, C.c_uint32, u8p, C.c_uint32]
         L.gzr_translate_query.restype = C.c_uint32
+        L.gzr_seg_mask.argtypes = [C.c_char_p, C.c_uint32, C.c_char_p]
+        L.gzr_translate_query_seg.argtypes = [C.c_void_p, C.c_char_p, C.c_uint32, u8p,
+                                              C.c_uint32]
+        L.gzr_translate_query_seg.restype = C.c_uint32
+        L.gzr_protein_query_seg.argtypes = [C.c_void_p, C.c_char_p, C.c_uint32, u8p,
+                                            C.c_uint32, C.POINTER(C.c_float),
+                                            C.POINTER(C.c_float)]
+        L.gzr_protein_query_seg.restype = C.c_uint32
 
     def hash_many(self, params, seq):
         pr = _Params(params)
@@ -431,3 +468,30 @@ class Reference:
         n = self.L.gzr_translate_query(pr.ptr, dna, len(dna), _p(out, u8p), cap)
         assert n == cap
         return out
+
+    def seg_mask(self, seq):
+        seq = bytes(seq)
+        out = C.create_string_buffer(max(len(seq), 1))
+        rc = self.L.gzr_seg_mask(seq, len(seq), out)
+        return None if rc else out.raw[:len(seq)]
+
+    def translate_query_seg(self, params, dna):
+        pr = _Params(params)
+        dna = bytes(dna)
+        assert len(dna) >= 3
+        cap = 7 + 6 * (len(dna) // 3)
+        out = np.zeros(cap, np.uint8)
+        n = self.L.gzr_translate_query_seg(pr.ptr, dna, len(dna), _p(out, u8p), cap)
+        assert n == cap
+        return out
+
+    def protein_query_seg(self, params, letters):
+        """(codes, lambda, K) of the reference's ProteinQuery with SEG on."""
+        pr = _Params(params)
+        letters = bytes(letters)
+        out = np.zeros(len(letters) + 2, np.uint8)
+        lam, k = C.c_float(), C.c_float()
+        n = self.L.gzr_protein_query_seg(pr.ptr, letters, len(letters), _p(out, u8p),
+                                         len(out), C.byref(lam), C.byref(k))
+        assert n == len(out)
+        return out, lam.value, k.value

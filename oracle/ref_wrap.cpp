@@ -27,6 +27,8 @@
 #include "translator.h"
 #include "translated_dna_query.h"
 #include "sequence_no_filter.h"
+#include "sequence_seg_filter.h"
+#include "protein_query.h"
 
 static ScoreMatrix make_matrix(const gzo_params *p) {
   std::vector<int> m(p->number_letters * p->number_letters);
@@ -256,6 +258,60 @@ uint32_t gzr_translate_query(const gzo_params *p, const char *dna, uint32_t leng
   const uint32_t n = base.GetSequenceLength();
   const AlphabetCoder::Code *codes = base.GetSequence();
   for (uint32_t i = 0; i < n && i < cap; ++i) out[i] = codes[i];
+  return n;
+}
+
+
+/* SequenceSegFilter::Filter (src/sequence_seg_filter.cpp:17-23) on one
+ * protein string: returns its code and, when 0, the masked string in out. */
+int gzr_seg_mask(const char *seq, uint32_t length, char *out) {
+  SequenceSegFilter filter;
+  std::string masked;
+  const int rc = filter.Filter(std::string(seq, length), &masked);
+  if (rc == 0) memcpy(out, masked.data(), masked.size());
+  return rc;
+}
+
+/* TranslatedDnaQuery with the SEG filter (Queries::GetFilter with filter
+ * on, src/queries.cpp:50-63). */
+uint32_t gzr_translate_query_seg(const gzo_params *p, const char *dna, uint32_t length,
+                                 uint8_t *out, uint32_t cap) {
+  Sequence seq("read", std::string(dna, length));
+  Translator translator;
+  SequenceSegFilter filter;
+  ScoreMatrix m = make_matrix(p);
+  ProteinType t;
+  Statistics s(t);
+  Statistics::KarlinParameters ideal;
+  s.CalculateUngappedIdealKarlinParameters(m, &ideal);
+  TranslatedDnaQuery q(seq, p->delimiter, translator, &filter, m, ideal);
+  Query &base = q;
+  const uint32_t n = base.GetSequenceLength();
+  const AlphabetCoder::Code *codes = base.GetSequence();
+  for (uint32_t i = 0; i < n && i < cap; ++i) out[i] = codes[i];
+  return n;
+}
+
+
+/* ProteinQuery with the SEG filter on: copies its length + 2 codes to out
+ * and its ungapped Karlin parameters. */
+uint32_t gzr_protein_query_seg(const gzo_params *p, const char *letters, uint32_t length,
+                               uint8_t *out, uint32_t cap, float *lambda, float *k) {
+  Sequence seq("query", std::string(letters, length));
+  SequenceSegFilter filter;
+  ScoreMatrix m = make_matrix(p);
+  ProteinType t;
+  Statistics s(t);
+  Statistics::KarlinParameters ideal;
+  s.CalculateUngappedIdealKarlinParameters(m, &ideal);
+  ProteinQuery q(seq, p->delimiter, &filter, m, ideal);
+  Query &base = q;
+  const uint32_t n = base.GetSequenceLength();
+  const AlphabetCoder::Code *codes = base.GetSequence();
+  for (uint32_t i = 0; i < n && i < cap; ++i) out[i] = codes[i];
+  Statistics::KarlinParameters kp = base.GetUngappedKarlinParameters();
+  *lambda = kp.lambda;
+  *k = kp.K;
   return n;
 }
 

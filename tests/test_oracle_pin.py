@@ -366,3 +366,94 @@ def test_query_karlin_matches_reference(oracle, reference, params):
         assert (np.float32(ol), np.float32(ok), np.float32(oh)) == \
             (np.float32(lam), np.float32(k), np.float32(h)), q
         assert (cut, trig) == reference.cutoffs(lam, k)
+
+
+# --- SEG low-complexity filter (query preparation) -----------------------------
+REF_LN_FACT = "/root/reference/ext/seg/src/ln_factrial_table.h"
+
+
+def test_seg_ln_factorial_table_matches_reference(oracle):
+    # ext/seg/src/ln_factrial_table.h: ln(n!) to 6 decimals, n = 0..10000
+    import os
+    import re
+    if not os.path.exists(REF_LN_FACT):
+        pytest.skip("reference checkout not present")
+    text = open(REF_LN_FACT).read()
+    body = text[text.index("{", text.index("kLnFactrialTable")) + 1:text.rindex("};")]
+    vals = [float(v) for v in re.findall(r"[0-9]+\.[0-9]+", body)]
+    assert len(vals) == 10001
+    assert all(oracle.L.gzo_ln_factorial6(n) == v for n, v in enumerate(vals))
+
+
+def _low_complexity_protein(rng, n):
+    """Random protein letters with planted low-complexity stretches (repeats
+    of 1-4 letters), stop and unknown letters, and some lower case."""
+    letters = np.frombuffer(b"ARNDCQEGHILKMFPSTWYV", np.uint8)
+    s = letters[rng.integers(0, 20, n)].copy()
+    for _ in range(int(rng.integers(0, 4))):
+        if n < 2:
+            break
+        a = int(rng.integers(0, n - 1))
+        b = min(n, a + int(rng.integers(5, 60)))
+        pool = letters[rng.choice(20, size=int(rng.integers(1, 5)), replace=False)]
+        s[a:b] = pool[rng.integers(0, len(pool), b - a)]
+    extra = rng.random(n)
+    s[extra < 0.02] = ord("*")
+    s[(extra >= 0.02) & (extra < 0.03)] = ord("X")
+    low = (extra >= 0.03) & (extra < 0.035)
+    s[low] = s[low] | 0x20
+    s[s == ord("*") | 0x20] = ord("*")
+    return bytes(s)
+
+
+@pytest.mark.parametrize("seed", [60, 61])
+def test_seg_mask_matches_reference(oracle, reference, seed):
+    rng = np.random.default_rng(seed)
+    masked_any = 0
+    for t in range(400):
+        n = int(rng.choice([0, 5, 11, 12, 13, 20, 50, int(rng.integers(12, 400)),
+                            int(rng.integers(400, 2500))]))
+        s = _low_complexity_protein(rng, n)
+        r = reference.seg_mask(s)
+        m = oracle.seg_mask(s)
+        assert m == r, (t, n, s)
+        masked_any += bool(m and b"x" in m)
+    assert masked_any > 50
+
+
+def test_seg_known_answer(oracle):
+    # a poly-Q stretch (positions 21-46) inside a random protein: windows are
+    # keyed by their first position, so the mask covers 21-44 and the last
+    # two Q stay; everything else is kept (as the reference's seg does)
+    s = b"MKTAYIAKQRQISFVKSHFSRQ" + b"Q" * 25 + b"LEERLGLIEVQAPILSRVGDGTQDNLSGAEKAVQVKVKALPDAQ"
+    m = oracle.seg_mask(s)
+    assert m == s[:21] + b"x" * 24 + s[45:]
+    assert oracle.seg_mask(b"QQQQQQQQQQQ") is None  # shorter than the window
+
+
+def test_translation_with_seg_matches_reference(oracle, reference, params):
+    rng = np.random.default_rng(62)
+    for t in range(300):
+        n = int(rng.choice([3, 20, 35, 36, 37, 150, int(rng.integers(3, 1500))]))
+        if rng.random() < 0.3:  # low-complexity DNA: short tandem repeats
+            unit = bytes(np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, int(rng.integers(1, 7)))])
+            read = (unit * (n // len(unit) + 1))[:n]
+        else:
+            read = _random_read(rng, n)
+        r = reference.translate_query_seg(params, read)
+        m = oracle.translate_query_seg(read, params["delimiter"])
+        assert np.array_equal(m, r), (t, n, read)
+
+
+def test_protein_query_with_seg_matches_reference(oracle, reference, params):
+    # ProteinQuery with SEG (src/protein_query.cpp:39-58): masked codes and
+    # the Karlin parameters of the whole held sequence, short proteins too
+    rng = np.random.default_rng(63)
+    for t in range(300):
+        n = int(rng.choice([0, 1, 5, 11, 12, 13, int(rng.integers(12, 600))]))
+        s = _low_complexity_protein(rng, n)
+        r, rl, rk = reference.protein_query_seg(params, s)
+        m = oracle.protein_query_seg(s, params["delimiter"])
+        assert np.array_equal(m, r), (t, n, s)
+        lam, k, _, _, _ = oracle.query_karlin(params, m)
+        assert (np.float32(lam), np.float32(k)) == (np.float32(rl), np.float32(rk)), (t, n)
