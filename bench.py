@@ -50,7 +50,13 @@ WORKLOADS = {
     "protein-50k-uneven-x-2M": (2_000_000, 201, 50_000, 402,
                                 {"median": 250, "sigma": 1.0, "lo": 20, "hi": 8000}),
     "protein-1k-x-200k": (200_000, 211, 1_000, 212, {}),   # small case for profiling
+    # translated DNA: 150-nt reads, 40 % reverse-translated DB fragments with
+    # 1 % substitutions; six-frame translation, SEG and cutoffs on the GPU
+    "dna-200k-reads-x-2M": (2_000_000, 201, 200_000, 302, {"read_length": 150}),
 }
+# reads of the query-preparation measurement (translated-DNA shape)
+PREP_READS = 200_000
+PREP_CPU_READS = 15_000  # oracle sample of the CPU baseline
 
 # algorithmic bytes of the dominant kernels:
 # ungapped seed: two residue bytes per residue pair examined; distance seed:
@@ -67,13 +73,121 @@ def log(msg):
     print(msg, file=sys.stderr, flush=True)
 
 
-def make_workload(name):
+def make_workload(name, prepare="gpu", limit=None):
+    """Database and queries of a workload.  Translated-DNA reads are
+    prepared (translation, SEG, cutoffs) on the GPU, or by the oracle for
+    the reference arm; both give the same queries."""
     from gzb import workload as W
     ndb, sdb, nq, sq, law = WORKLOADS[name]
     t = time.time()
     db = W.make_database(ndb, sdb)
-    q = W.make_queries(db, nq, sq, **law)
+    if "read_length" in law:
+        reads = W.make_reads(db, nq, sq, read_length=law["read_length"])
+        if prepare == "gpu":
+            from gzb import native as N
+            codes, offs, lens, cut, trig = N.prepare_translated_queries(reads.dna, reads.offsets)
+            q = W.translated_queries(codes, offs, lens, sources=reads.sources,
+                                     cutoffs=(cut, trig))
+        else:
+            q = oracle_translated_queries(reads, limit=limit)
+    else:
+        q = W.make_queries(db, nq, sq, **law)
     return db, q, time.time() - t
+
+
+def oracle_translated_queries(reads, limit=None):
+    """Translated queries of reads prepared by the oracle (CPU): translation
+    with SEG, then each query's cutoffs."""
+    import oracle as O
+    from gzb import native as N
+    from gzb import params as P
+    from gzb import workload as W
+    o = O.Oracle()
+    params = P.make_params()
+    n = reads.number if limit is None else min(limit, reads.number)
+    offs, lens, total = N.translated_layout(np.diff(reads.offsets[:n + 1]))
+    codes = np.empty(total, np.uint8)
+    cut = np.empty(n, np.int32)
+    trig = np.empty(n, np.int32)
+    for r in range(n):
+        tq = o.translate_query_seg(reads.read(r), P.DELIMITER)
+        codes[int(offs[r]):int(offs[r]) + len(tq)] = tq
+        cut[r], trig[r] = o.query_karlin(params, tq)[3:]
+    return W.translated_queries(codes, offs, lens, sources=reads.sources[:n], cutoffs=(cut, trig))
+
+
+def query_prep_bench(db, steps, warmup, cpu=True, seed=302):
+    """Query preparation of translated-DNA searches (six-frame translation,
+    SEG, per-query cutoffs) on the GPU over PREP_READS 150-nt reads held in
+    HBM, timed with CUDA events; the oracle prepares a bounded sample on one
+    core as the CPU baseline."""
+    import torch
+    from gzb import native as N
+    from gzb import params as P
+    from gzb import workload as W
+    reads = W.make_reads(db, PREP_READS, seed)
+    n = reads.number
+    lens = np.diff(reads.offsets).astype(np.uint32)
+    offs, qlen, total = N.translated_layout(lens)
+    dev = torch.device("cuda")
+    d_dna = torch.from_numpy(reads.dna).to(dev)
+    d_off = torch.from_numpy(reads.offsets[:-1].astype(np.int64)).to(dev)
+    d_len = torch.from_numpy(lens.view(np.int32)).to(dev)
+    d_qoff = torch.from_numpy(offs.view(np.int64)).to(dev)
+    d_qlen = torch.from_numpy(qlen.view(np.int32)).to(dev)
+    d_out = torch.empty(total, dtype=torch.uint8, device=dev)
+    d_cut = torch.empty(n, dtype=torch.int32, device=dev)
+    d_trig = torch.empty(n, dtype=torch.int32, device=dev)
+    d_status = torch.zeros(1, dtype=torch.int32, device=dev)
+    m = P.blosum62()
+    stream = torch.cuda.current_stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    parts = [0.0, 0.0, 0.0]
+
+    def step(timed):
+        if timed:
+            ev[0].record(stream)
+        N.translate_dna_queries_async(d_dna, d_off, d_len, n, d_qoff, d_out, P.DELIMITER)
+        if timed:
+            ev[1].record(stream)
+        N.seg_translated_queries_async(d_out, d_qoff, d_len, n, d_status)
+        if timed:
+            ev[2].record(stream)
+        N.query_karlin_cutoffs_async(d_out, d_qoff, d_qlen, n, m, d_cut, d_trig)
+        if timed:
+            ev[3].record(stream)
+            torch.cuda.synchronize()
+            for k in range(3):
+                parts[k] += ev[k].elapsed_time(ev[k + 1])
+
+    for _ in range(warmup):
+        step(False)
+    torch.cuda.synchronize()
+    for _ in range(steps):
+        step(True)
+    total_ms = sum(parts) / steps
+    assert int(d_status.item()) == 0
+    out = {"reads": n, "read_length": 150, "ms": total_ms,
+           "reads_per_s": n / (total_ms / 1e3),
+           "kernel_ms": {"translate": parts[0] / steps, "seg": parts[1] / steps,
+                         "karlin_cutoffs": parts[2] / steps},
+           "bytes_in": int(reads.dna.nbytes), "bytes_out": int(total)}
+    if not cpu:
+        return out
+    # CPU baseline: the oracle prepares the first PREP_CPU_READS reads
+    sample = min(PREP_CPU_READS, n)
+    t = time.time()
+    q_cpu = oracle_translated_queries(reads, limit=sample)
+    cpu_s = time.time() - t
+    same = (np.array_equal(d_cut.cpu().numpy()[:sample], q_cpu.cutoffs)
+            and np.array_equal(d_trig.cpu().numpy()[:sample], q_cpu.triggers)
+            and np.array_equal(d_out.cpu().numpy()[:len(q_cpu.codes)], q_cpu.codes))
+    out["matches_oracle_sample"] = bool(same)
+    out["cpu_baseline"] = {"value": sample / cpu_s, "unit": "reads/s", "cores": 1,
+                           "kind": "port",
+                           "sample": f"first {sample} reads prepared by the oracle "
+                                     f"(translation + SEG + cutoffs) in {cpu_s:.2f} s"}
+    return out
 
 
 class ClockSampler:
@@ -200,7 +314,7 @@ def build_results_cpu(db, q, aligned, budget_s=10.0):
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    db, q, gen_s = make_workload(args.workload)
+    db, q, gen_s = make_workload(args.workload, prepare="oracle", limit=args.ref_queries)
     cores = os.cpu_count() or 1
     vals = []
     for i in range(args.warmup + args.steps):
@@ -431,6 +545,11 @@ def main():
                    "import_s": time.time() - t, "build_s": index_s}
     del blob
 
+    # query preparation of translated-DNA searches (outside the presearch
+    # metric)
+    query_prep = query_prep_bench(db, args.steps, args.warmup,
+                                  cpu=(rank == 0 and not args.no_cpu_baseline))
+
     # max over ranks
     t_dev, t_e2e = reps.max([dev_ms, e2e_ms])
     nq = q.number
@@ -503,6 +622,7 @@ def main():
         "dp_gcups": {"gapped_stage": gcups_stage, "whole_step": gcups_step},
         "stage_ms": st, "counters": counters, "schedules": sched_report,
         "index_build_s": index_s, "index_cache": index_cache, "build_results": build_results,
+        "query_preparation": query_prep,
         "workload_gen_s": gen_s, "clocks": clocks, "roofline": roofline,
         "gpu_launches": int(counters.get("kernel_launches", 0)) * steps,
     }
