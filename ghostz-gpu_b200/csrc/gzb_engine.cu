@@ -1091,6 +1091,21 @@ struct gzb_engine {
   gzb_counters counters{};
   float stage_ms[7] = {0, 0, 0, 0, 0, 0, 0};
   cudaEvent_t ev[7] = {};
+  // stored database chunks (gzb_engine_swap_database): each holds a chunk's
+  // codes, offsets and the ten index arrays, compact
+  struct DbSlot {
+    bool have = false;
+    bool pending = false;          // a prefetch's copies may still run
+    int32_t chunk_id = 0;
+    DBuf db_buf, db_offsets, codeflag;
+    DBuf arrays[10];
+    uint64_t db_len = 0, db_check = 0;
+    uint32_t nseq = 0;
+    DevIndex X;
+    cudaEvent_t ready = nullptr;   // recorded after a prefetch's copies
+  };
+  std::vector<DbSlot> db_slots;
+  bool x_in_arrays = false;        // X points into index_bufs[40..49]
 };
 
 namespace {
@@ -1279,6 +1294,14 @@ extern "C" int gzb_engine_destroy(gzb_engine *e) {
                  &e->tb_walk_cap, &e->tb_walk_off, &e->tb_ops, &e->tb_row_meta, &e->tb_walk,
                  &e->tb_walk_n, &e->tb_score, &e->tb_p0, &e->tb_p1, &e->tb_out};
   for (DBuf *b : all) b->release();
+  for (auto &slot : e->db_slots) {
+    if (slot.ready) cudaEventSynchronize(slot.ready);
+    slot.db_buf.release();
+    slot.db_offsets.release();
+    slot.codeflag.release();
+    for (auto &b : slot.arrays) b.release();
+    if (slot.ready) cudaEventDestroy(slot.ready);
+  }
   cudaFree(e->spill);
   cudaFree(e->gcounters);
   cudaFree(e->gcells);
@@ -1447,6 +1470,7 @@ extern "C" int gzb_engine_set_database(gzb_engine *e, int32_t chunk_id, const ui
             "database chunk of %llu residues exceeds 2^31", (unsigned long long)length);
   cudaStream_t s = (cudaStream_t)stream;
   e->have_db = false;
+  e->x_in_arrays = false;
   e->chunk_id = chunk_id;
   e->db_len = length;
   e->nseq = number_sequences;
@@ -1643,6 +1667,7 @@ extern "C" int gzb_engine_set_database_with_index(gzb_engine *e, int32_t chunk_i
   GZB_CHECK(blob_bytes >= index_blob_bytes(h), GZB_ERR_INVALID, "index blob truncated");
   cudaStream_t s = (cudaStream_t)stream;
   e->have_db = false;
+  e->x_in_arrays = false;
   e->chunk_id = chunk_id;
   e->db_len = length;
   e->nseq = number_sequences;
@@ -1682,11 +1707,177 @@ extern "C" int gzb_engine_set_database_with_index(gzb_engine *e, int32_t chunk_i
   X.n_members = h.n_members;
   X.params_clustering = e->params.clustering != 0;
   GZB_CUDA(cudaStreamSynchronize(s));
+  e->x_in_arrays = true;
   e->have_db = true;
   return GZB_OK;
 }
 
-extern "C" int gzb_engine_set_queries(gzb_engine *e, const uint8_t *codes, uint64_t length,
+namespace {
+
+constexpr uint32_t kMaxDbSlots = 64;
+
+// validates an index blob against the engine's parameters and a chunk
+int check_index_blob(gzb_engine *e, const uint8_t *codes, uint64_t length,
+                     const uint32_t *offsets, uint32_t number_sequences, const void *blob,
+                     uint64_t blob_bytes, IndexHeader *out) {
+  GZB_CHECK(codes && offsets && number_sequences > 0 && length > 0 && blob, GZB_ERR_INVALID,
+            "empty database or index");
+  GZB_CHECK(length < (1ull << 31), GZB_ERR_OVERFLOW,
+            "database chunk of %llu residues exceeds 2^31", (unsigned long long)length);
+  GZB_CHECK(blob_bytes >= sizeof(IndexHeader), GZB_ERR_INVALID, "index blob too short");
+  IndexHeader h;
+  memcpy(&h, blob, sizeof(h));
+  GZB_CHECK(h.magic == kIndexMagic, GZB_ERR_INVALID, "not an index blob of this library");
+  GZB_CHECK(h.fingerprint == index_fingerprint(e), GZB_ERR_INVALID,
+            "index blob was built with other index parameters");
+  GZB_CHECK(h.db_len == length && h.nseq == number_sequences &&
+                h.db_check == db_check(codes, length, offsets, number_sequences),
+            GZB_ERR_INVALID, "index blob belongs to another chunk");
+  GZB_CHECK(blob_bytes >= index_blob_bytes(h), GZB_ERR_INVALID, "index blob truncated");
+  *out = h;
+  return GZB_OK;
+}
+
+// X over ten index arrays of a header's sizes
+void point_index(DevIndex &X, void *const dst[10], const IndexHeader &h, bool clustering) {
+  X = DevIndex();
+  X.nc_keys = (uint32_t *)dst[0];
+  X.nc_offsets = (uint32_t *)dst[1];
+  X.nc_values = (uint32_t *)dst[2];
+  X.rep_keys = (uint32_t *)dst[3];
+  X.rep_offsets = (uint32_t *)dst[4];
+  X.rep_positions = (uint32_t *)dst[5];
+  X.rep_cluster_ids = (uint32_t *)dst[6];
+  X.rep_windows = (uint64_t *)dst[7];
+  X.member_offsets = (uint32_t *)dst[8];
+  X.member_positions = (uint32_t *)dst[9];
+  X.n_nc_keys = h.n_nc_keys;
+  X.n_nc_values = h.n_nc_values;
+  X.n_rep_keys = h.n_rep_keys;
+  X.n_reps = h.n_reps;
+  X.n_members = h.n_members;
+  X.params_clustering = clustering;
+}
+
+// moves the resident chunk's index arrays into index_bufs[40..49] (device
+// copies), so that the chunk can be stored without the build's scratch
+int compact_index(gzb_engine *e, cudaStream_t s) {
+  const IndexHeader h = header_of(e);
+  uint64_t n[10];
+  index_array_sizes(h, n);
+  const void *src[10] = {e->X.nc_keys, e->X.nc_offsets, e->X.nc_values, e->X.rep_keys,
+                         e->X.rep_offsets, e->X.rep_positions, e->X.rep_cluster_ids,
+                         e->X.rep_windows, e->X.member_offsets, e->X.member_positions};
+  void *dst[10];
+  for (int i = 0; i < 10; ++i) {
+    const uint64_t bytes = n[i] * (i == 7 ? 8 : 4);
+    DBuf &d = e->index_bufs[40 + i];
+    GZB_TRY(d.ensure(bytes + 16));
+    GZB_CUDA(cudaMemsetAsync(d.p, 0, 16, s));
+    if (bytes) GZB_CUDA(cudaMemcpyAsync(d.p, src[i], bytes, cudaMemcpyDeviceToDevice, s));
+    dst[i] = d.p;
+  }
+  GZB_CUDA(cudaStreamSynchronize(s));
+  point_index(e->X, dst, h, e->X.params_clustering);
+  e->x_in_arrays = true;
+  return GZB_OK;
+}
+
+}  // namespace
+
+extern "C" int gzb_engine_swap_database(gzb_engine *e, uint32_t slot, void *stream) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(slot < kMaxDbSlots, GZB_ERR_INVALID, "database slot %u outside 0..%u", slot,
+            kMaxDbSlots - 1);
+  if (slot >= e->db_slots.size()) e->db_slots.resize(slot + 1);
+  gzb_engine::DbSlot &S = e->db_slots[slot];
+  cudaStream_t s = (cudaStream_t)stream;
+  if (S.pending) {
+    // a prefetched chunk: its copies must be done and its codes valid
+    GZB_CUDA(cudaEventSynchronize(S.ready));
+    S.pending = false;
+    unsigned int bad = 0;
+    GZB_CUDA(cudaMemcpy(&bad, S.codeflag.p, 4, cudaMemcpyDeviceToHost));
+    if (bad) {
+      S.have = false;
+      return set_error(GZB_ERR_INVALID, "prefetched chunk: residue codes must be below 32");
+    }
+  }
+  if (e->have_db && !e->x_in_arrays) GZB_TRY(compact_index(e, s));
+  // work already queued on `stream` may still read the resident chunk
+  GZB_CUDA(cudaStreamSynchronize(s));
+  std::swap(e->db_buf, S.db_buf);
+  std::swap(e->db_offsets, S.db_offsets);
+  std::swap(e->codeflag, S.codeflag);
+  for (int i = 0; i < 10; ++i) std::swap(e->index_bufs[40 + i], S.arrays[i]);
+  std::swap(e->chunk_id, S.chunk_id);
+  std::swap(e->db_len, S.db_len);
+  std::swap(e->db_check, S.db_check);
+  std::swap(e->nseq, S.nseq);
+  std::swap(e->X, S.X);
+  const bool had = e->have_db;
+  e->have_db = S.have;
+  S.have = had;
+  e->x_in_arrays = e->have_db;
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_prefetch_database_with_index(
+    gzb_engine *e, uint32_t slot, int32_t chunk_id, const uint8_t *codes, uint64_t length,
+    const uint32_t *offsets, uint32_t number_sequences, const void *blob, uint64_t blob_bytes,
+    void *stream) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(e->have_params, GZB_ERR_INVALID, "set_params first");
+  GZB_CHECK(slot < kMaxDbSlots, GZB_ERR_INVALID, "database slot %u outside 0..%u", slot,
+            kMaxDbSlots - 1);
+  IndexHeader h;
+  GZB_TRY(check_index_blob(e, codes, length, offsets, number_sequences, blob, blob_bytes, &h));
+  if (slot >= e->db_slots.size()) e->db_slots.resize(slot + 1);
+  gzb_engine::DbSlot &S = e->db_slots[slot];
+  if (S.pending) GZB_CUDA(cudaEventSynchronize(S.ready));
+  if (!S.ready) GZB_CUDA(cudaEventCreateWithFlags(&S.ready, cudaEventDisableTiming));
+  cudaStream_t s = (cudaStream_t)stream;
+  S.have = false;
+  S.pending = false;
+  // codes with their padding, and the range check that the swap reads
+  GZB_TRY(S.db_buf.ensure(length + 2 * kPad));
+  GZB_TRY(S.codeflag.ensure(4));
+  const uint8_t delim = (uint8_t)e->params.delimiter;
+  GZB_CUDA(cudaMemsetAsync(S.db_buf.p, delim, kPad, s));
+  GZB_CUDA(cudaMemsetAsync((uint8_t *)S.db_buf.p + kPad + length, delim, kPad, s));
+  GZB_CUDA(cudaMemcpyAsync((uint8_t *)S.db_buf.p + kPad, codes, length, cudaMemcpyHostToDevice,
+                           s));
+  GZB_CUDA(cudaMemsetAsync(S.codeflag.p, 0, 4, s));
+  code_range_kernel<<<grid1(length / 16 + 1, 256), 256, 0, s>>>(
+      (const uint8_t *)S.db_buf.p + kPad, length, S.codeflag.as<unsigned int>());
+  GZB_CUDA(cudaGetLastError());
+  GZB_TRY(upload(S.db_offsets, offsets, number_sequences + 1, s));
+  uint64_t n[10], at = sizeof(h);
+  index_array_sizes(h, n);
+  void *dst[10];
+  for (int i = 0; i < 10; ++i) {
+    const uint64_t bytes = n[i] * (i == 7 ? 8 : 4);
+    DBuf &d = S.arrays[i];
+    GZB_TRY(d.ensure(bytes + 16));
+    GZB_CUDA(cudaMemsetAsync(d.p, 0, 16, s));
+    if (bytes)
+      GZB_CUDA(cudaMemcpyAsync(d.p, (const uint8_t *)blob + at, bytes, cudaMemcpyHostToDevice, s));
+    dst[i] = d.p;
+    at += pad8(bytes);
+  }
+  point_index(S.X, dst, h, e->params.clustering != 0);
+  S.chunk_id = chunk_id;
+  S.db_len = length;
+  S.nseq = number_sequences;
+  S.db_check = h.db_check;
+  GZB_CUDA(cudaEventRecord(S.ready, s));
+  S.pending = true;
+  S.have = true;
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_set_queries(
+gzb_engine *e, const uint8_t *codes, uint64_t length,
                                       const uint32_t *offsets, const uint32_t *lengths,
                                       uint32_t number_queries, const int32_t *cutoffs,
                                       const int32_t *triggers, void *stream) {

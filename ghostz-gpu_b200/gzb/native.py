@@ -117,6 +117,9 @@ def _declare(L):
         "gzb_engine_set_database_with_index": [V, C.c_int32, V, C.c_uint64, V, C.c_uint32, V,
                                                C.c_uint64, V],
         "gzb_translate_dna_queries": [V, V, V, U32, V, C.c_uint8, V, V],
+        "gzb_engine_swap_database": [V, U32, V],
+        "gzb_engine_prefetch_database_with_index": [V, U32, C.c_int32, V, C.c_uint64, V, U32,
+                                                    V, C.c_uint64, V],
         "gzb_query_karlin_cutoffs": [V, V, V, U32, V, U32, C.c_float, C.c_float, V, V, V, V],
         "gzb_seg_translated_queries": [V, V, V, U32, V, V],
         "gzb_seg_protein_queries": [V, V, V, U32, V, V],
@@ -374,6 +377,22 @@ class PresearchEngine:
             check(lib().gzb_engine_set_database_with_index(
                 self.h, int(chunk_id), hptr(codes), len(codes), hptr(offs),
                 int(db.number_sequences), hptr(blob), blob.nbytes, _stream_or_null(stream)))
+
+    def swap_database(self, slot, stream=None):
+        """Exchanges the resident chunk with the chunk stored in `slot`."""
+        check(lib().gzb_engine_swap_database(self.h, int(slot), _stream_or_null(stream)))
+
+    def prefetch_database(self, slot, db, blob, chunk_id=0, stream=None):
+        """Fills `slot` from host arrays and an index blob with asynchronous
+        copies on `stream` (numpy arrays; pass pinned memory for overlap).
+        The arrays must stay alive until the slot is swapped in."""
+        codes = np.ascontiguousarray(db.codes, dtype=np.uint8)
+        offs = np.ascontiguousarray(db.offsets, dtype=np.uint32)
+        check(lib().gzb_engine_prefetch_database_with_index(
+            self.h, int(slot), int(chunk_id), hptr(codes), len(codes), hptr(offs),
+            int(db.number_sequences), hptr(blob), blob.nbytes, _stream_or_null(stream)))
+        self._pinned_refs = getattr(self, "_pinned_refs", {})
+        self._pinned_refs[int(slot)] = (codes, offs, blob)
 
     def export_index(self, stream=None):
         """The resident chunk's device index as a host blob (numpy uint8)."""

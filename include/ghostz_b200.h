@@ -275,6 +275,34 @@ int gzb_engine_set_database_with_index(gzb_engine *e, int32_t chunk_id, const ui
                                        uint32_t number_sequences, const void *blob,
                                        uint64_t blob_bytes, void *stream);
 
+/* Stored database chunks, for streaming a database of many chunks
+ * (the reference's chunk loop with its preloading thread,
+ * src/aligner_gpu_presearch_thread.cpp:214-640 and :259-274, and
+ * Database::Preload, src/database.h:556-608).  The engine holds one
+ * resident chunk plus up to 64 stored ones, each with its codes, offsets
+ * and index arrays.
+ *  - gzb_engine_swap_database exchanges the resident chunk with the one in
+ *    `slot` (either may be empty): a stored chunk becomes resident without
+ *    copies, and the resident one is stored (a chunk whose index was built
+ *    here first moves its index arrays out of the build's scratch, one
+ *    device copy).  It waits for the work queued on `stream` and for a
+ *    prefetch into the slot, and refuses a prefetched chunk with residue
+ *    codes of 32 or more.
+ *  - gzb_engine_prefetch_database_with_index fills `slot` from host codes,
+ *    offsets and an index blob (as gzb_engine_set_database_with_index,
+ *    same checks) with asynchronous copies on `stream`, touching only the
+ *    slot's own buffers, so the copies overlap a presearch running on
+ *    another stream; with pinned host buffers the host does not wait.
+ * A database whose chunks all fit in device memory can stay stored
+ * (set_database, then swap into its own slot, per chunk); a larger one
+ * streams through two slots. */
+int gzb_engine_swap_database(gzb_engine *e, uint32_t slot, void *stream);
+int gzb_engine_prefetch_database_with_index(gzb_engine *e, uint32_t slot, int32_t chunk_id,
+                                            const uint8_t *codes, uint64_t length,
+                                            const uint32_t *offsets,
+                                            uint32_t number_sequences, const void *blob,
+                                            uint64_t blob_bytes, void *stream);
+
 /* Uploads the queries (concatenated, shared delimiters; offsets[i] is the
  * leading delimiter of query i; lengths[i] = residues + 2) with their
  * per-query ungapped X-drop and trigger, and builds the query hash lists. */
