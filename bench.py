@@ -335,6 +335,295 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def train_cost_model(params, local_rank, train_sets):
+    """Cost model of the learned schedule (untimed set-up): pairs logged by
+    the plain path on config-1-shaped runs (20,000 proteins, 1,000 queries x
+    train_sets query seeds), trained on the GPU by the engine's own kernels.
+    Returns (parameters, final loss, pairs)."""
+    from gzb import native as N
+    from gzb import workload as W
+    tdb = W.make_database(20000, 101)
+    trainer = N.PresearchEngine(local_rank)
+    trainer.set_params(params)
+    trainer.set_database(tdb)
+    trainer.set_logging(True, 1 << 23)
+    for k in range(train_sets):
+        trainer.set_queries(W.make_queries(tdb, 1000, 102 + k))
+        trainer.presearch(N.SCHEDULE_PLAIN)
+    model, loss = trainer.train_cost_model(epochs=12, batch=4096, lr=3e-3, seed=7)
+    pairs = len(trainer.get_log()[1])
+    trainer.close()
+    return model, loss, pairs
+
+
+# a database of several chunks streamed through one GPU:
+# name: (chunks, sequences per chunk, first db seed, queries, query seed, query length law)
+MULTICHUNK_WORKLOADS = {
+    # 16 M proteins in 8 chunks of 2 M (seeds 501..508); 100 k mixed-length
+    # queries (log-normal median 250, sigma 1.0, clipped to 20-8000), planted
+    # homologs drawn from every chunk
+    "protein-100k-x-16M-8chunks": (8, 2_000_000, 501, 100_000, 502,
+                                   {"median": 250, "sigma": 1.0, "lo": 20, "hi": 8000}),
+    # small case of the same shape (checks and profiling)
+    "protein-2k-x-400k-4chunks": (4, 100_000, 521, 2_000, 522,
+                                  {"median": 250, "sigma": 1.0, "lo": 20, "hi": 8000}),
+}
+
+
+def make_multichunk(name, cutoffs_on_gpu=True):
+    from gzb import workload as W
+    n_chunks, nseq, sdb, nq, sq, law = MULTICHUNK_WORKLOADS[name]
+    t = time.time()
+    chunks = [W.make_database(nseq, sdb + k) for k in range(n_chunks)]
+    per = nq // n_chunks
+    seqs = []
+    zeros = (np.zeros(per, np.int32), np.zeros(per, np.int32))
+    for k, db in enumerate(chunks):
+        seqs += W.query_sequences(W.make_queries(db, per, sq + 1000 * k, cutoffs=zeros, **law))
+    q = W.pack_queries(seqs, cutoffs=(np.zeros(len(seqs), np.int32),
+                                      np.zeros(len(seqs), np.int32)))
+    if cutoffs_on_gpu:
+        from gzb import native as N
+        q.cutoffs, q.triggers, _ = N.query_karlin_cutoffs(q.codes, q.offsets.astype(np.uint64),
+                                                          q.lengths)
+    else:
+        q.cutoffs, q.triggers = __import__("gzb.params", fromlist=["x"]).query_cutoffs(seqs)
+    return chunks, q, time.time() - t
+
+
+def run_reference_multichunk(args, world, rank):
+    """The reference arm on the multi-chunk workload: the restatement on all
+    host cores, on a sample of queries against the first chunk's first
+    20,000 sequences, scaled to the whole database by the residue ratio."""
+    if rank != 0:
+        return
+    chunks, q, gen_s = make_multichunk(args.workload, cutoffs_on_gpu=False)
+    cores = os.cpu_count() or 1
+    total = sum(db.length for db in chunks)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, el, sample = cpu_baseline(chunks[0], q, n_queries=min(args.ref_queries, 4000),
+                                     processes=cores)
+        if i >= args.warmup:
+            vals.append(v * chunks[0].length / total)
+    value = float(np.mean(vals))
+    sample += f"; scaled to all {len(chunks)} chunks ({total} residues)"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded generator, config shapes)",
+        "config": {"workload": args.workload, "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_multichunk(args, world, rank, local_rank):
+    """A database of several chunks on one GPU.  Untimed set-up builds each
+    chunk's index on the device once (the reference's `db` step) and keeps
+    it two ways: stored on the device in its own slot (the whole database
+    fits in HBM), and as a pinned host blob.  A step searches every query
+    against every chunk and merges per query (top-b over chunks):
+      stored   - swap each stored chunk in, search, swap it back;
+      streamed - two slots: the next chunk's codes and index are copied
+                 from pinned host memory on a side stream while the current
+                 chunk is searched (the reference's preloading thread)."""
+    import ctypes
+    import torch
+    from gzb import native as N
+    from gzb import params as P
+    from gzb import workload as W
+    from gzb.replicas import Replicas
+    torch.cuda.set_device(local_rank)
+    reps = Replicas("nccl", timeout_s=1800)
+    chunks, q, gen_s = make_multichunk(args.workload)
+    n_chunks = len(chunks)
+    params = P.make_params()
+    eng = N.PresearchEngine(local_rank)
+    eng.set_params(params)
+    stream = torch.cuda.current_stream()
+    side = torch.cuda.Stream()
+    t = time.time()
+    pinned_chunks, blobs = [], []
+    for k, db in enumerate(chunks):
+        eng.set_database(db, chunk_id=k)
+        pb = torch.empty(eng.index_bytes(), dtype=torch.uint8).pin_memory()
+        blobs.append(eng.export_index(out=pb.numpy()))
+        pc = torch.empty(len(db.codes), dtype=torch.uint8).pin_memory()
+        pc.numpy()[:] = db.codes
+        po = torch.empty(len(db.offsets) * 4, dtype=torch.uint8).pin_memory()
+        po.numpy().view(np.uint32)[:] = db.offsets
+        pinned_chunks.append(W.Database(codes=pc.numpy(), offsets=po.numpy().view(np.uint32),
+                                        number_sequences=db.number_sequences))
+        eng.swap_database(k)  # stored in slot k
+    setup_s = time.time() - t
+    eng.set_queries(q)
+    model, train_loss, train_pairs = (None, None, 0)
+    if args.schedule == "batched":
+        model, train_loss, train_pairs = train_cost_model(params, local_rank, args.train_sets)
+        eng.set_cost_model(model)
+        eng.set_queries(q)
+    sched = N.SCHEDULE_BATCHED if args.schedule == "batched" else N.SCHEDULE_PLAIN
+    tiles = {}
+    if sched == N.SCHEDULE_BATCHED and not args.no_autotune:
+        eng.swap_database(0)
+        ker, _ = eng.autotune(sched, (N.GAPPED_KERNEL_LANE, N.GAPPED_KERNEL_ROWS),
+                              N.TILE_GAPPED_KERNEL)
+        thr, _ = eng.autotune(sched, (2, 4, 8, 16), N.TILE_BOOK_THRESHOLD)
+        order_t, _ = eng.autotune(sched, (N.ORDER_MODEL, N.ORDER_HITS), N.TILE_ORDER)
+        eng.swap_database(0)
+        tiles = {"kernel": KERNEL_NAMES[eng.tile(sched, N.TILE_GAPPED_KERNEL)],
+                 "book_threshold": eng.tile(sched, N.TILE_BOOK_THRESHOLD),
+                 "order": ORDER_NAMES[eng.tile(sched, N.TILE_ORDER)]}
+    stage_keys = ("lookup", "seed_ungapped", "chain", "gapped", "merge", "total", "seed_kernels")
+
+    def step_stored(acc):
+        eng.reset_results(stream)
+        for k in range(n_chunks):
+            eng.swap_database(k, stream)
+            eng.presearch(sched, stream)
+            if acc is not None:
+                for key, v in eng.stage_ms().items():
+                    acc["stage"][key] += v
+                for key, v in eng.counters().items():
+                    acc["counters"][key] = acc["counters"].get(key, 0) + v
+            eng.swap_database(k, stream)
+
+    # streaming uses slots n_chunks (first chunk) and n_chunks + 1 (the rest)
+    a_slot, b_slot = n_chunks, n_chunks + 1
+
+    def step_streamed(acc):
+        eng.reset_results(stream)
+        eng.prefetch_database(a_slot, pinned_chunks[0], blobs[0], chunk_id=0, stream=side)
+        eng.swap_database(a_slot, stream)
+        for k in range(n_chunks):
+            if k + 1 < n_chunks:
+                eng.prefetch_database(b_slot, pinned_chunks[k + 1], blobs[k + 1],
+                                      chunk_id=k + 1, stream=side)
+            eng.presearch(sched, stream)
+            if k + 1 < n_chunks:
+                eng.swap_database(b_slot, stream)
+        eng.swap_database(a_slot, stream)  # leaves no chunk resident
+
+    def timed(step):
+        for _ in range(args.warmup):
+            step(None)
+        reps.barrier()
+        torch.cuda.synchronize()
+        acc = {"stage": {k: 0.0 for k in stage_keys}, "counters": {}}
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step(acc)
+        e1.record(stream)
+        reps.barrier()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), acc
+
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    stored_ms, acc = timed(step_stored)
+    stored_results = eng.results()
+    streamed_ms, _ = timed(step_streamed)
+    streamed_results = eng.results()
+    clocks = sampler.stop()
+    same = all(np.array_equal(a, b) for a, b in zip(stored_results, streamed_results))
+
+    # end to end through the C ABI: queries from pinned host memory, the
+    # stored chunks, results read back
+    pinned = {}
+    for name in ("codes", "offsets", "lengths", "cutoffs", "triggers"):
+        a = getattr(q, name)
+        t_pin = torch.empty(a.nbytes, dtype=torch.uint8).pin_memory()
+        t_pin.numpy()[:] = np.frombuffer(np.ascontiguousarray(a).tobytes(), dtype=np.uint8)
+        pinned[name] = (t_pin, a.dtype)
+    qp = W.Queries(**{n: pinned[n][0].numpy().view(pinned[n][1]) for n in pinned})
+    b = int(params["max_number_results"])
+    counts_pin = torch.empty(q.number * 4, dtype=torch.uint8).pin_memory()
+    res_pin = torch.empty(q.number * b * N.RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+    L = N.lib()
+
+    def e2e_step(acc):
+        eng.set_queries(qp, stream)
+        step_stored(None)
+        N.check(L.gzb_engine_get_results(eng.h, ctypes.c_void_p(counts_pin.data_ptr()),
+                                         ctypes.c_void_p(res_pin.data_ptr()),
+                                         ctypes.c_void_p(stream.cuda_stream)))
+
+    e2e_ms, _ = timed(e2e_step)
+    got = np.frombuffer(res_pin.numpy().tobytes(), dtype=N.RESULT_DTYPE).reshape(q.number, b)
+    cnt = np.frombuffer(counts_pin.numpy().tobytes(), dtype=np.uint32)
+    e2e_same = all(np.array_equal(got[i, :cnt[i]], stored_results[i]) for i in range(q.number))
+    h2d = sum(getattr(q, n).nbytes for n in ("codes", "offsets", "lengths", "cutoffs", "triggers"))
+
+    t_stored, t_streamed, t_e2e = reps.max([stored_ms, streamed_ms, e2e_ms])
+    nq, steps = q.number, args.steps
+    st = {k: v / steps for k, v in acc["stage"].items()}
+    counters = {k: v // steps for k, v in acc["counters"].items()}
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    seed_bytes = (counters.get("distance_seeds", 0) * BYTES_PER_DISTANCE_SEED
+                  + BYTES_PER_UNGAPPED_STEP * counters.get("ungapped_steps", 0))
+    achieved = seed_bytes / (st["seed_kernels"] / 1e3) / 1e9 if st["seed_kernels"] else 0.0
+    total_res = sum(db.length for db in chunks)
+    line = {
+        "metric": METRIC, "value": reps.throughput(nq, steps, t_stored), "unit": UNIT,
+        "n_gpus": world, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": t_stored / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded generator with the config's shapes)",
+        "config": {"workload": args.workload, "chunks": n_chunks,
+                   "db_sequences": sum(db.number_sequences for db in chunks),
+                   "db_residues": total_res, "queries": nq,
+                   "schedule": args.schedule, "tile": tiles,
+                   "mode": "stored: every chunk's codes and index resident in HBM, swapped in "
+                           "per chunk",
+                   "l2": "inputs larger than L2 (each chunk > 126 MB)",
+                   "parallelism": f"replicas x{world}"},
+        "streamed": {"value": reps.throughput(nq, steps, t_streamed), "unit": UNIT,
+                     "ms_per_step": t_streamed / steps,
+                     "h2d_bytes_per_step": int(sum(len(c.codes) + c.offsets.nbytes + len(bl)
+                                                   for c, bl in zip(pinned_chunks, blobs))),
+                     "results_equal_stored": bool(same),
+                     "mode": "two slots, next chunk's codes and index copied from pinned host "
+                             "memory on a side stream during the current chunk's search"},
+        "e2e": {"value": reps.throughput(nq, steps, t_e2e), "unit": UNIT,
+                "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(counts_pin.numel() + res_pin.numel()),
+                "ms_per_step": t_e2e / steps, "results_equal_device_loop": bool(e2e_same)},
+        "stage_ms": st, "counters": counters,
+        "dp_gcups": {"gapped_stage": counters.get("gapped_cells", 0) / (st["gapped"] / 1e3) / 1e9
+                     if st["gapped"] else None},
+        "roofline": {"bound": "hbm", "kernel": "seed_kernel + member_kernel (all chunks)",
+                     "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                     "frac": achieved / hbm_peak, "traffic": None,
+                     "algorithmic_bytes": seed_bytes, "kernel_ms": st["seed_kernels"],
+                     "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)"
+                     if "hbm_gbs" in peaks else "fallback 6650 GB/s"},
+        "setup_s": {"workload_gen": gen_s, "index_build_export_store": setup_s},
+        "cost_model": {"train_pairs": train_pairs, "train_mse_log2": train_loss},
+        "clocks": clocks,
+        "gpu_launches": int(counters.get("kernel_launches", 0)) * steps,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        v, el, sample = cpu_baseline(chunks[0], q, n_queries=min(args.cpu_queries, 2000),
+                                     processes=1)
+        line["cpu_baseline"] = {"value": v * chunks[0].length / total_res, "unit": UNIT,
+                                "cores": 1, "kind": "port",
+                                "sample": sample + f"; scaled to all {n_chunks} chunks"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+    reps.close()
+
+
 KERNEL_NAMES = {0: "flat", 1: "lane", 2: "rows", 3: "static", 4: "deal"}
 ORDER_NAMES = {0: "hits", 1: "cost model"}
 
@@ -347,7 +636,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--schedule", default="batched", choices=["plain", "batched"])
     ap.add_argument("--train-sets", type=int, default=8)
-    ap.add_argument("--workload", default="protein-10k-x-2M", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="protein-10k-x-2M",
+                    choices=sorted(WORKLOADS) + sorted(MULTICHUNK_WORKLOADS))
     ap.add_argument("--cpu-queries", type=int, default=10000)
     ap.add_argument("--ref-queries", type=int, default=10000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -358,6 +648,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload in MULTICHUNK_WORKLOADS:
+        if args.impl == "reference":
+            return run_reference_multichunk(args, world, rank)
+        return run_multichunk(args, world, rank, local_rank)
     if args.impl == "reference":
         return run_reference(args, world, rank)
 
@@ -385,18 +679,7 @@ def main():
     t = time.time()
     train_pairs, train_loss = 0, None
     if args.schedule == "batched":
-        from gzb import workload as W
-        tdb = W.make_database(20000, 101)
-        trainer = N.PresearchEngine(local_rank)
-        trainer.set_params(params)
-        trainer.set_database(tdb)
-        trainer.set_logging(True, 1 << 23)
-        for k in range(args.train_sets):
-            trainer.set_queries(W.make_queries(tdb, 1000, 102 + k))
-            trainer.presearch(N.SCHEDULE_PLAIN)
-        model, train_loss = trainer.train_cost_model(epochs=12, batch=4096, lr=3e-3, seed=7)
-        train_pairs = len(trainer.get_log()[1])
-        trainer.close()
+        model, train_loss, train_pairs = train_cost_model(params, local_rank, args.train_sets)
         eng.set_cost_model(model)
         eng.set_queries(q)
     train_s = time.time() - t

@@ -394,14 +394,21 @@ class PresearchEngine:
         self._pinned_refs = getattr(self, "_pinned_refs", {})
         self._pinned_refs[int(slot)] = (codes, offs, blob)
 
-    def export_index(self, stream=None):
-        """The resident chunk's device index as a host blob (numpy uint8)."""
+    def index_bytes(self):
+        """Bytes of the resident chunk's index blob."""
         n = C.c_uint64()
         check(lib().gzb_engine_index_bytes(self.h, C.byref(n)))
-        blob = np.zeros(n.value, np.uint8)
-        check(lib().gzb_engine_export_index(self.h, hptr(blob), n.value,
-                                            _stream_or_null(stream)))
-        return blob
+        return int(n.value)
+
+    def export_index(self, stream=None, out=None):
+        """The resident chunk's device index as a host blob (numpy uint8),
+        written into `out` (a uint8 array of index_bytes(), pinned memory
+        for example) when given."""
+        n = self.index_bytes()
+        blob = np.zeros(n, np.uint8) if out is None else out
+        assert blob.dtype == np.uint8 and blob.nbytes >= n
+        check(lib().gzb_engine_export_index(self.h, hptr(blob), n, _stream_or_null(stream)))
+        return blob[:n]
 
     def set_queries(self, queries, stream=None):
         codes = np.ascontiguousarray(queries.codes, dtype=np.uint8)
