@@ -58,12 +58,13 @@ extern GappedTile g_tile;
 int check_tile_value(int which, int value);
 int *tile_field(GappedTile &t, int which);
 int any_tile_value(int which);
+int ensure_band_pool(int2 **band_pool, int *band_wmask);
 int run_gapped(const GappedTile &tile, const GappedJob &job, const int32_t *matrix,
                int number_letters, int stride, size_t n, const uint32_t *order, int reverse,
                const uint8_t *dir, uint32_t *d_qpos, uint32_t *d_dpos, int32_t *d_scores,
                uint32_t **spill, size_t *spill_cap, uint32_t *counters,
                unsigned long long *cells, uint32_t *cells_out, int2 **band_pool,
-               int *band_wmask, cudaStream_t s, uint32_t *n_fallback);
+               int *band_wmask, cudaStream_t s, uint32_t *n_fallback, const uint64_t *n_dev);
 
 constexpr uint64_t kPad = 256;  // delimiter bytes kept around device sequences
 
@@ -425,6 +426,7 @@ struct SeedArgs {
   unsigned long long *mwork_count;
   unsigned long long mwork_cap;
   unsigned long long *ctr;  // [0] distance seeds [1] ungapped seeds [2] steps
+  const uint64_t *units_dev = nullptr;  // unit count on the device (else L.n_units)
 };
 
 __device__ __forceinline__ void emit_hit(const SeedArgs &a, uint32_t qid, uint32_t d,
@@ -448,7 +450,7 @@ seed_kernel(SeedArgs a) {
   const int lane = threadIdx.x & 31;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  const uint64_t U = a.L.n_units;
+  const uint64_t U = a.units_dev ? *a.units_dev : a.L.n_units;
   const int thr = a.p.distance_threshold;
   const int maxmd = a.p.max_member_distance;
   unsigned long long n_dist = 0, n_seed = 0, n_steps = 0;
@@ -530,8 +532,10 @@ seed_kernel(SeedArgs a) {
 // search over the scan, so a seed costs one load (the member's position)
 // besides its walk.
 __global__ void __launch_bounds__(kSeedBlock, 5)
-member_kernel(SeedArgs a, const uint2 *__restrict__ mwork, uint64_t n_work) {
+member_kernel(SeedArgs a, const uint2 *__restrict__ mwork, uint64_t n_work,
+              const uint64_t *n_dev) {
   __shared__ __align__(16) int32_t tbl32[kWalkTableBytes / 4];
+  if (n_dev) n_work = *n_dev;
   load_walk_table(tbl32, a.matrix32, a.p.delimiter);
   __syncthreads();
   const char *tbl = reinterpret_cast<const char *>(tbl32);
@@ -588,7 +592,8 @@ member_kernel(SeedArgs a, const uint2 *__restrict__ mwork, uint64_t n_work) {
 
 // first hit index of every query (hits sorted by packed key)
 __global__ void hit_segments_kernel(const uint64_t *hits, uint64_t n, uint32_t nq, int shift,
-                                    uint64_t *begin) {
+                                    uint64_t *begin, const uint64_t *n_dev) {
+  if (n_dev) n = *n_dev;
   for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi <= nq;
        qi += gridDim.x * blockDim.x) {
     const uint64_t key = (uint64_t)qi << shift;
@@ -694,7 +699,9 @@ __global__ void build_ext_kernel(const uint64_t *hits, const uint64_t *begin,
                                  const uint32_t *db_offsets, uint32_t nseq, uint32_t db_len,
                                  int qbits, int dbits, uint64_t n_surv, uint32_t *eq,
                                  uint32_t *ed, uint8_t *dir, uint32_t *elen0,
-                                 uint32_t *elen1, uint32_t *eqid, uint32_t *neighbours) {
+                                 uint32_t *elen1, uint32_t *eqid, uint32_t *neighbours,
+                                 const uint64_t *n_dev) {
+  if (n_dev) n_surv = *n_dev;
   const uint64_t qmask = (1ull << qbits) - 1, dmask = (1ull << dbits) - 1;
   constexpr uint32_t kReach = 256;  // database residues either side
   const int lane = threadIdx.x & 31;
@@ -885,7 +892,11 @@ __global__ void merge_kernel(uint32_t nq, const uint64_t *hits, const uint64_t *
                              int dbits, const uint32_t *db_offsets, uint32_t nseq,
                              uint32_t db_len, int32_t chunk_id, int max_results,
                              int max_one_subject, gzb_result *scratch, uint8_t *taken_all,
-                             gzb_result *results, uint32_t *counts) {
+                             gzb_result *results, uint32_t *counts, const uint64_t *n_dev,
+                             const uint32_t *skip) {
+  // a run whose buffers overflowed merges nothing (it is redone)
+  if (skip && *skip) return;
+  if (n_dev) n_surv = *n_dev;
   const uint64_t qmask = (1ull << qbits) - 1, dmask = (1ull << dbits) - 1;
   const int lane = threadIdx.x & 31;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -1106,6 +1117,20 @@ struct gzb_engine {
   };
   std::vector<DbSlot> db_slots;
   bool x_in_arrays = false;        // X points into index_bufs[40..49]
+  // graph mode: captured presearch graphs, keyed by what they depend on
+  struct GraphEntry {
+    uint64_t key;
+    cudaGraphExec_t exec;
+    uint64_t launches;             // kernels in the graph
+    uint64_t used;                 // last use (for eviction)
+  };
+  bool graph = false;
+  std::vector<GraphEntry> graphs;
+  cudaStream_t gstream = nullptr;
+  cudaEvent_t gev_in = nullptr, gev_out = nullptr;
+  DBuf plan;                       // device counts and the report
+  uint64_t *report_h = nullptr;    // pinned copy of the report
+  uint64_t graph_captures = 0, graph_replays = 0, graph_fallbacks = 0, graph_clock = 0;
 };
 
 namespace {
@@ -1294,6 +1319,14 @@ extern "C" int gzb_engine_destroy(gzb_engine *e) {
                  &e->tb_walk_cap, &e->tb_walk_off, &e->tb_ops, &e->tb_row_meta, &e->tb_walk,
                  &e->tb_walk_n, &e->tb_score, &e->tb_p0, &e->tb_p1, &e->tb_out};
   for (DBuf *b : all) b->release();
+  for (auto &g : e->graphs) cudaGraphExecDestroy(g.exec);
+  e->graphs.clear();
+  if (e->gstream) cudaStreamSynchronize(e->gstream);
+  if (e->gstream) cudaStreamDestroy(e->gstream);
+  if (e->gev_in) cudaEventDestroy(e->gev_in);
+  if (e->gev_out) cudaEventDestroy(e->gev_out);
+  if (e->report_h) cudaFreeHost(e->report_h);
+  e->plan.release();
   for (auto &slot : e->db_slots) {
     if (slot.ready) cudaEventSynchronize(slot.ready);
     slot.db_buf.release();
@@ -2076,7 +2109,7 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
                             &sorted_mw));
       launches += 1;
       member_kernel<<<grid1((n_mwork + 31) / 32 * 32, kSeedBlock, 148 * 16), kSeedBlock, 0, s>>>(
-          a, reinterpret_cast<const uint2 *>(sorted_mw), n_mwork);
+          a, reinterpret_cast<const uint2 *>(sorted_mw), n_mwork, nullptr);
       GZB_CUDA(cudaGetLastError());
       ++launches;
       GZB_CUDA(cudaMemcpyAsync(hctr, c, 64, cudaMemcpyDeviceToHost, s));
@@ -2119,7 +2152,8 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
   uint64_t *begin = e->begin.as<uint64_t>();
   uint32_t *kept = e->kept.as<uint32_t>();
   uint64_t *surv_off = e->surv_off.as<uint64_t>();
-  hit_segments_kernel<<<grid1(nq + 1, 256), 256, 0, s>>>(hits, n_hits, nq, qbits + dbits, begin);
+  hit_segments_kernel<<<grid1(nq + 1, 256), 256, 0, s>>>(hits, n_hits, nq, qbits + dbits, begin,
+                                                          nullptr);
   GZB_CUDA(cudaGetLastError());
     ++launches;
   chain_kernel<<<grid1((uint64_t)nq * 32, 128), 128, 0, s>>>(
@@ -2154,7 +2188,7 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
         e->q_lengths.as<uint32_t>(), e->db_offsets.as<uint32_t>(), e->nseq, (uint32_t)e->db_len,
         qbits, dbits, n_surv, e->eq.as<uint32_t>(), e->ed.as<uint32_t>(), e->edir.as<uint8_t>(),
         e->elen0.as<uint32_t>(), e->elen1.as<uint32_t>(), e->eqid.as<uint32_t>(),
-        e->enb.as<uint32_t>());
+        e->enb.as<uint32_t>(), nullptr);
     GZB_CUDA(cudaGetLastError());
     ++launches;
     GZB_CUDA(cudaMemsetAsync(e->gcells, 0, 8, s));
@@ -2216,7 +2250,7 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
                        e->edir.as<uint8_t>(), e->eq.as<uint32_t>(), e->ed.as<uint32_t>(),
                        e->escore.as<int32_t>(), &e->spill, &e->spill_cap, e->gcounters,
                        e->gcells, scheduled ? e->ecells.as<uint32_t>() : nullptr,
-                       &e->band_pool, &e->band_wmask, s, &fb));
+                       &e->band_pool, &e->band_wmask, s, &fb, nullptr));
     launches += 3;
     if (scheduled) {
       if (e->logging) {
@@ -2267,7 +2301,7 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
         e->db_offsets.as<uint32_t>(), e->nseq, (uint32_t)e->db_len, e->chunk_id,
         e->params.max_number_results, e->params.max_number_one_subject_results,
         e->merge_scratch.as<gzb_result>(), e->heap.as<uint8_t>(), e->results.as<gzb_result>(),
-        e->counts.as<uint32_t>());
+        e->counts.as<uint32_t>(), nullptr, nullptr);
     GZB_CUDA(cudaGetLastError());
     ++launches;
   }
@@ -2282,7 +2316,421 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
   return GZB_OK;
 }
 
+// ---- graph mode: the whole presearch of the resident chunk as one CUDA
+// graph.  Every count comes from device memory and every buffer is sized
+// to a capacity chosen beforehand (hits, member work and the extensions
+// they imply), so nothing reads back between stages; sorts run over the
+// whole capacity with keys past the count set to all ones (they sort last,
+// and the sorts are stable, so the first `count` keys come out as the
+// eager path's).  A count above its capacity sets an overflow bit: the
+// merge then does nothing, and the host redoes the call eagerly with
+// larger capacities.
+
+// count clamped to a capacity; an excess sets `bit` in *overflow
+__global__ void clamp_count_kernel(const unsigned long long *count, uint64_t cap, uint64_t *out,
+                                   uint32_t *overflow, uint32_t bit) {
+  const unsigned long long c = *count;
+  *out = c < cap ? c : cap;
+  if (c > cap) atomicOr(overflow, bit);
+}
+
+// keys[n .. cap) = all ones (n read on the device)
+__global__ void pad_keys_kernel(uint64_t *keys, const uint64_t *n_dev, uint64_t cap) {
+  for (uint64_t i = *n_dev + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < cap;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    keys[i] = ~0ull;
+}
+
+// surviving hits and the extensions they make
+__global__ void ext_count_kernel(const uint64_t *surv_off, uint32_t nq, uint64_t *plan) {
+  plan[2] = surv_off[nq];
+  plan[3] = 2 * surv_off[nq];
+}
+
+// everything the host reads after a graph run, in one place
+__global__ void report_kernel(const unsigned long long *ctr, const uint64_t *plan,
+                              const unsigned long long *gcells, const uint32_t *gcounters,
+                              uint64_t *report) {
+  for (int i = 0; i < 6; ++i) report[i] = ctr[i];
+  report[6] = plan[2];
+  report[7] = *gcells;
+  report[8] = gcounters[0];
+  report[9] = gcounters[1];
+  report[10] = gcounters[2];
+  report[11] = reinterpret_cast<const uint32_t *>(plan + 6)[0];
+  report[12] = plan[1];
+}
+
+constexpr int kGraphCache = 16;        // graphs kept per engine
+constexpr int kReportWords = 16;
+
+struct GraphCaps {
+  uint64_t hits, mwork, ext;           // ext = 2 * hits (every hit may survive)
+};
+
+GraphCaps graph_caps(const gzb_engine *e) {
+  GraphCaps c;
+  c.hits = e->hit_cap;
+  c.mwork = e->mwork_cap;
+  c.ext = 2 * c.hits;
+  return c;
+}
+
+int graph_sort_bytes(const gzb_engine *e, const GraphCaps &c, int hit_bits, int mw_bits,
+                     size_t *bytes) {
+  size_t a = 0, b = 0, d = 0, f = 0;
+  cub::DoubleBuffer<uint64_t> k1(nullptr, nullptr);
+  GZB_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, a, k1, (int64_t)c.hits, 0, hit_bits));
+  GZB_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, b, k1, (int64_t)c.mwork, 0, mw_bits));
+  const uint64_t *u64 = nullptr;
+  uint64_t *o64 = nullptr;
+  const uint32_t *u32 = nullptr;
+  GZB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, d, u64, o64,
+                                         (int64_t)(e->L.n_lists + 1)));
+  GZB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, f, u32, o64, (int64_t)(e->nq + 1)));
+  *bytes = std::max(std::max(a, b), std::max(d, f));
+  return GZB_OK;
+}
+
+// every buffer the graph touches, at its capacity (before capture: the
+// capture itself must not allocate)
+int graph_prepare(gzb_engine *e, const GraphCaps &c, int hit_bits, int mw_bits) {
+  const uint32_t nq = e->nq;
+  GZB_TRY(e->list_bufs[14].ensure(8 * (e->L.n_lists + 1)));
+  GZB_TRY(e->ctr.ensure(64));
+  GZB_TRY(e->plan.ensure(8 * 32));  // [0..3] counts, [6] overflow, [8..20] report
+  GZB_TRY(e->hits.ensure(8 * (c.hits + 1)));
+  GZB_TRY(e->hits_alt.ensure(8 * (c.hits + 1)));
+  GZB_TRY(e->hits_copy.ensure(8 * (c.hits + 1)));
+  GZB_TRY(e->mwork.ensure(8 * (c.mwork + 1)));
+  GZB_TRY(e->mwork_alt.ensure(8 * (c.mwork + 1)));
+  GZB_TRY(e->begin.ensure(8 * (nq + 1)));
+  GZB_TRY(e->kept.ensure(4 * (nq + 1)));
+  GZB_TRY(e->surv_off.ensure(8 * (nq + 1)));
+  GZB_TRY(e->slots.ensure(8 * (e->q_len + nq + 1)));
+  for (DBuf *b : {&e->eq, &e->ed, &e->escore, &e->elen0, &e->elen1, &e->eqid})
+    GZB_TRY(b->ensure(4 * (c.ext + 1)));
+  GZB_TRY(e->edir.ensure(c.ext + 1));
+  GZB_TRY(e->enb.ensure(4 * (c.hits + 1)));
+  GZB_TRY(e->merge_scratch.ensure(sizeof(gzb_result) * (c.hits + 1)));
+  GZB_TRY(e->heap.ensure(c.hits + 1));
+  size_t tb = 0;
+  GZB_TRY(graph_sort_bytes(e, c, hit_bits, mw_bits, &tb));
+  GZB_TRY(e->tmp.ensure(tb));
+  // the gapped stage's spill lists and fallback band pool
+  if (e->spill_cap < 2 * c.ext) {
+    cudaFree(e->spill);
+    e->spill = nullptr;
+    e->spill_cap = 0;
+    GZB_CUDA(cudaMalloc(&e->spill, 4 * 2 * c.ext));
+    e->spill_cap = 2 * c.ext;
+  }
+  GZB_TRY(ensure_band_pool(&e->band_pool, &e->band_wmask));
+  if (!e->report_h) GZB_CUDA(cudaMallocHost(&e->report_h, 8 * kReportWords));
+  if (!e->gstream) GZB_CUDA(cudaStreamCreateWithFlags(&e->gstream, cudaStreamNonBlocking));
+  if (!e->gev_in) GZB_CUDA(cudaEventCreateWithFlags(&e->gev_in, cudaEventDisableTiming));
+  if (!e->gev_out) GZB_CUDA(cudaEventCreateWithFlags(&e->gev_out, cudaEventDisableTiming));
+  return GZB_OK;
+}
+
+// the presearch body recorded into the graph
+int graph_body(gzb_engine *e, int schedule, const GappedTile &tile, const GraphCaps &c,
+               int qbits, int dbits, int nqbits, cudaStream_t s, uint64_t *launches_out) {
+  uint64_t launches = 0;
+  DevLists &L = e->L;
+  const DevIndex &X = e->X;
+  const uint32_t nq = e->nq;
+  uint64_t *plan = e->plan.as<uint64_t>();
+  uint32_t *overflow = reinterpret_cast<uint32_t *>(plan + 6);
+  unsigned long long *ctr = e->ctr.as<unsigned long long>();
+  GZB_CUDA(cudaEventRecord(e->ev[0], s));
+  GZB_CUDA(cudaMemsetAsync(plan, 0, 64, s));
+  GZB_CUDA(cudaMemsetAsync(ctr, 0, 64, s));
+  // list lookup; the unit count stays on the device
+  if (L.n_lists) {
+    uint64_t *unit_counts = e->list_bufs[14].as<uint64_t>();
+    list_lookup_kernel<<<grid1(L.n_lists, 256), 256, 0, s>>>(L, X, e->params.clustering,
+                                                              unit_counts);
+    GZB_CUDA(cudaGetLastError());
+    ++launches;
+    GZB_CUDA(cudaMemsetAsync(unit_counts + L.n_lists, 0, 8, s));
+    GZB_TRY(exclusive_sum(e, unit_counts, L.unit_offsets, L.n_lists + 1, s));
+  }
+  GZB_CUDA(cudaEventRecord(e->ev[1], s));
+  // seed search, distance and ungapped extension
+  SeedArgs a;
+  a.p = e->dp;
+  a.L = L;
+  a.X = X;
+  a.q = e->q_buf.as<uint8_t>() + kPad;
+  a.db = e->db_buf.as<uint8_t>() + kPad;
+  a.q_offsets = e->q_offsets.as<uint32_t>();
+  a.cutoffs = e->q_cut.as<int32_t>();
+  a.triggers = e->q_trig.as<int32_t>();
+  a.matrix32 = e->matrix32.as<int32_t>();
+  a.clustering = e->params.clustering;
+  a.dbits = dbits;
+  a.qbits = qbits;
+  a.hits = e->hits.as<uint64_t>();
+  a.hit_count = ctr + 4;
+  a.hit_cap = c.hits;
+  a.mwork = e->mwork.as<uint2>();
+  a.mwork_count = ctr + 5;
+  a.mwork_cap = c.mwork;
+  a.ctr = ctr;
+  a.units_dev = L.n_lists ? L.unit_offsets + L.n_lists : nullptr;
+  if (L.n_lists) {
+    seed_kernel<<<148 * 16, kSeedBlock, 0, s>>>(a);
+    GZB_CUDA(cudaGetLastError());
+    ++launches;
+  }
+  // member work in cluster-major order, then the member seeds
+  clamp_count_kernel<<<1, 1, 0, s>>>(ctr + 5, c.mwork, plan + 0, overflow, 1u);
+  pad_keys_kernel<<<148 * 4, 256, 0, s>>>(reinterpret_cast<uint64_t *>(a.mwork), plan + 0,
+                                          c.mwork);
+  GZB_CUDA(cudaGetLastError());
+  launches += 2;
+  uint64_t *sorted_mw = nullptr;
+  GZB_TRY(sort_keys_u64(e, reinterpret_cast<uint64_t *>(a.mwork), e->mwork_alt.as<uint64_t>(),
+                        c.mwork, bits_for(X.n_reps + 1), s, &sorted_mw));
+  ++launches;
+  member_kernel<<<148 * 16, kSeedBlock, 0, s>>>(a, reinterpret_cast<const uint2 *>(sorted_mw),
+                                                c.mwork, plan + 0);
+  GZB_CUDA(cudaGetLastError());
+  ++launches;
+  GZB_CUDA(cudaEventRecord(e->ev[6], s));
+  // hits sorted by (query, database position, query position)
+  clamp_count_kernel<<<1, 1, 0, s>>>(ctr + 4, c.hits, plan + 1, overflow, 2u);
+  pad_keys_kernel<<<148 * 4, 256, 0, s>>>(e->hits.as<uint64_t>(), plan + 1, c.hits);
+  GZB_CUDA(cudaGetLastError());
+  launches += 2;
+  uint64_t *hits = nullptr;
+  GZB_TRY(sort_keys_u64(e, e->hits.as<uint64_t>(), e->hits_alt.as<uint64_t>(), c.hits,
+                        qbits + dbits + nqbits, s, &hits));
+  ++launches;
+  GZB_CUDA(cudaMemcpyAsync(e->hits_copy.p, hits, 8 * c.hits, cudaMemcpyDeviceToDevice, s));
+  GZB_CUDA(cudaEventRecord(e->ev[2], s));
+  // chain filter
+  uint64_t *begin = e->begin.as<uint64_t>();
+  uint32_t *kept = e->kept.as<uint32_t>();
+  uint64_t *surv_off = e->surv_off.as<uint64_t>();
+  hit_segments_kernel<<<grid1(nq + 1, 256), 256, 0, s>>>(hits, c.hits, nq, qbits + dbits, begin,
+                                                          plan + 1);
+  GZB_CUDA(cudaGetLastError());
+  ++launches;
+  chain_kernel<<<grid1((uint64_t)nq * 32, 128), 128, 0, s>>>(
+      e->dp, e->q_buf.as<uint8_t>() + kPad, e->db_buf.as<uint8_t>() + kPad,
+      e->q_offsets.as<uint32_t>(), e->q_lengths.as<uint32_t>(), e->q_cut.as<int32_t>(),
+      e->matrix32.as<int32_t>(), nq, hits, begin, qbits, dbits, e->slots.as<uint2>(), kept);
+  GZB_CUDA(cudaGetLastError());
+  ++launches;
+  GZB_CUDA(cudaMemsetAsync(kept + nq, 0, 4, s));
+  GZB_TRY(exclusive_sum(e, kept, surv_off, nq + 1, s));
+  ext_count_kernel<<<1, 1, 0, s>>>(surv_off, nq, plan);
+  GZB_CUDA(cudaGetLastError());
+  launches += 2;
+  GZB_CUDA(cudaEventRecord(e->ev[3], s));
+  // gapped extension of both sides, in hit order
+  build_ext_kernel<<<grid1((uint64_t)nq * 32, 256), 256, 0, s>>>(
+      hits, begin, kept, surv_off, nq, e->q_offsets.as<uint32_t>(),
+      e->q_lengths.as<uint32_t>(), e->db_offsets.as<uint32_t>(), e->nseq, (uint32_t)e->db_len,
+      qbits, dbits, c.hits, e->eq.as<uint32_t>(), e->ed.as<uint32_t>(), e->edir.as<uint8_t>(),
+      e->elen0.as<uint32_t>(), e->elen1.as<uint32_t>(), e->eqid.as<uint32_t>(),
+      e->enb.as<uint32_t>(), plan + 2);
+  GZB_CUDA(cudaGetLastError());
+  ++launches;
+  GZB_CUDA(cudaMemsetAsync(e->gcells, 0, 8, s));
+  GappedJob job;
+  job.query = e->q_buf.as<uint8_t>() + kPad;
+  job.db = e->db_buf.as<uint8_t>() + kPad;
+  job.delim = e->params.delimiter;
+  job.gap_open = e->params.gap_open;
+  job.gap_ext = e->params.gap_extension;
+  job.cutoff = e->params.gapped_cutoff;
+  GappedTile t = tile;
+  if (schedule == GZB_SCHEDULE_PLAIN) t.kernel = GZB_GAPPED_KERNEL_STATIC;
+  GZB_TRY(run_gapped(t, job, e->matrix32.as<int32_t>(), 32, 32, c.ext, nullptr, 0,
+                     e->edir.as<uint8_t>(), e->eq.as<uint32_t>(), e->ed.as<uint32_t>(),
+                     e->escore.as<int32_t>(), &e->spill, &e->spill_cap, e->gcounters,
+                     e->gcells, nullptr, &e->band_pool, &e->band_wmask, s, nullptr, plan + 3));
+  launches += 3;
+  GZB_CUDA(cudaEventRecord(e->ev[4], s));
+  // top-b merge (nothing when a count overflowed)
+  merge_kernel<<<grid1((uint64_t)nq * 32, 128), 128, 0, s>>>(
+      nq, hits, begin, kept, surv_off, c.hits, e->eq.as<uint32_t>(), e->ed.as<uint32_t>(),
+      e->escore.as<int32_t>(), e->q_offsets.as<uint32_t>(), qbits, dbits,
+      e->db_offsets.as<uint32_t>(), e->nseq, (uint32_t)e->db_len, e->chunk_id,
+      e->params.max_number_results, e->params.max_number_one_subject_results,
+      e->merge_scratch.as<gzb_result>(), e->heap.as<uint8_t>(), e->results.as<gzb_result>(),
+      e->counts.as<uint32_t>(), plan + 2, overflow);
+  GZB_CUDA(cudaGetLastError());
+  ++launches;
+  GZB_CUDA(cudaEventRecord(e->ev[5], s));
+  report_kernel<<<1, 1, 0, s>>>(ctr, plan, e->gcells, e->gcounters, plan + 8);
+  GZB_CUDA(cudaGetLastError());
+  ++launches;
+  GZB_CUDA(cudaMemcpyAsync(e->report_h, plan + 8, 8 * 13, cudaMemcpyDeviceToHost, s));
+  *launches_out = launches;
+  return GZB_OK;
+}
+
+uint64_t fnv_mix(uint64_t h, const void *p, size_t n) {
+  const uint8_t *b = (const uint8_t *)p;
+  for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+  return h;
+}
+
+// what a captured graph depends on: every buffer it touches (address and
+// size), the chunk, the queries, the schedule, the tile and the capacities
+uint64_t graph_key(const gzb_engine *e, int schedule, const GappedTile &tile,
+                   const GraphCaps &c) {
+  uint64_t h = 1469598103934665603ull;
+  const DBuf *bufs[] = {&e->db_buf, &e->db_offsets, &e->q_buf, &e->q_offsets, &e->q_lengths,
+                        &e->q_cut, &e->q_trig, &e->matrix32, &e->results, &e->counts,
+                        &e->tmp, &e->hits, &e->hits_alt, &e->hits_copy, &e->mwork,
+                        &e->mwork_alt, &e->begin, &e->kept, &e->surv_off, &e->slots, &e->eq,
+                        &e->ed, &e->edir, &e->escore, &e->elen0, &e->elen1, &e->eqid, &e->enb,
+                        &e->merge_scratch, &e->heap, &e->ctr, &e->plan, &e->list_bufs[14]};
+  for (const DBuf *b : bufs) {
+    h = fnv_mix(h, &b->p, sizeof(b->p));
+    h = fnv_mix(h, &b->bytes, sizeof(b->bytes));
+  }
+  h = fnv_mix(h, &e->X, sizeof(e->X));
+  h = fnv_mix(h, &e->L, sizeof(e->L));
+  h = fnv_mix(h, &e->dp, sizeof(e->dp));
+  h = fnv_mix(h, &e->params, sizeof(e->params));
+  const uint64_t v[] = {e->db_len, e->nseq, (uint64_t)(int64_t)e->chunk_id, e->nq, e->q_len,
+                        e->max_qlen, (uint64_t)schedule, (uint64_t)tile.kernel,
+                        (uint64_t)tile.book_threshold, (uint64_t)tile.order, c.hits, c.mwork,
+                        (uint64_t)(uintptr_t)e->spill, e->spill_cap,
+                        (uint64_t)(uintptr_t)e->band_pool, (uint64_t)(uintptr_t)e->gcounters,
+                        (uint64_t)(uintptr_t)e->gcells, (uint64_t)(uintptr_t)e->report_h};
+  return fnv_mix(h, v, sizeof(v));
+}
+
+void drop_graphs(gzb_engine *e) {
+  for (auto &g : e->graphs) cudaGraphExecDestroy(g.exec);
+  e->graphs.clear();
+}
+
+int presearch_graph(gzb_engine *e, int schedule, const GappedTile &tile, cudaStream_t user) {
+  const uint32_t nq = e->nq;
+  const int qbits = bits_for(e->max_qlen);
+  const int dbits = bits_for(e->db_len + 1);
+  const int nqbits = bits_for(nq);
+  GZB_CHECK(qbits + dbits + nqbits <= 64, GZB_ERR_OVERFLOW,
+            "hit key needs %d bits (queries %u, chunk %llu, longest query %u)",
+            qbits + dbits + nqbits, nq, (unsigned long long)e->db_len, e->max_qlen);
+  const GraphCaps c = graph_caps(e);
+  GZB_TRY(graph_prepare(e, c, qbits + dbits + nqbits, bits_for(e->X.n_reps + 1)));
+  const uint64_t key = graph_key(e, schedule, tile, c);
+  gzb_engine::GraphEntry *g = nullptr;
+  for (auto &x : e->graphs)
+    if (x.key == key) g = &x;
+  cudaStream_t s = e->gstream;
+  if (!g) {
+    if ((int)e->graphs.size() >= kGraphCache) {  // drop the least recently used
+      size_t oldest = 0;
+      for (size_t i = 1; i < e->graphs.size(); ++i)
+        if (e->graphs[i].used < e->graphs[oldest].used) oldest = i;
+      cudaGraphExecDestroy(e->graphs[oldest].exec);
+      e->graphs.erase(e->graphs.begin() + oldest);
+    }
+    GZB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    uint64_t launches = 0;
+    const int rc = graph_body(e, schedule, tile, c, qbits, dbits, nqbits, s, &launches);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    if (rc != GZB_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    GZB_CUDA(ce);
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    GZB_CUDA(ie);
+    e->graphs.push_back(gzb_engine::GraphEntry{key, exec, launches, 0});
+    g = &e->graphs.back();
+    ++e->graph_captures;
+  }
+  g->used = ++e->graph_clock;
+  e->qbits = qbits;
+  e->dbits = dbits;
+  GZB_CUDA(cudaEventRecord(e->gev_in, user));
+  GZB_CUDA(cudaStreamWaitEvent(s, e->gev_in, 0));
+  GZB_CUDA(cudaGraphLaunch(g->exec, s));
+  GZB_CUDA(cudaEventRecord(e->gev_out, s));
+  GZB_CUDA(cudaStreamWaitEvent(user, e->gev_out, 0));
+  GZB_CUDA(cudaStreamSynchronize(s));
+  ++e->graph_replays;
+  const uint64_t *r = e->report_h;
+  if (r[11] != 0) {
+    // a count above its capacity: nothing was merged; grow and redo eagerly
+    ++e->graph_fallbacks;
+    e->hit_cap = std::max<uint64_t>(e->hit_cap, r[4] + r[4] / 8 + 1024);
+    e->mwork_cap = std::max<uint64_t>(e->mwork_cap, r[5] + r[5] / 8 + 1024);
+    drop_graphs(e);
+    return presearch_impl(e, schedule, user);
+  }
+  GZB_CHECK(r[10] == 0, GZB_ERR_OVERFLOW,
+            "%llu gapped extensions need a band wider than the fallback's",
+            (unsigned long long)r[10]);
+  e->counters.distance_seeds = r[0];
+  e->counters.ungapped_seeds = r[1];
+  e->counters.ungapped_steps = r[2];
+  e->counters.ungapped_hits = r[12];
+  e->counters.chained_hits = r[6];
+  e->counters.gapped_extensions = 2 * r[6];
+  e->counters.gapped_cells = r[7];
+  e->counters.gapped_fallbacks = r[8];
+  e->counters.kernel_launches = g->launches;
+  e->last_mae = -1.0f;
+  e->last_mae_n = 0;
+  e->pred_n = 0;
+  e->prev_cells_n = 0;
+  float t[7];
+  bool timed = true;
+  for (int i = 0; i < 5 && timed; ++i)
+    timed = cudaEventElapsedTime(&t[i], e->ev[i], e->ev[i + 1]) == cudaSuccess;
+  if (timed) timed = cudaEventElapsedTime(&t[5], e->ev[0], e->ev[5]) == cudaSuccess;
+  if (timed) timed = cudaEventElapsedTime(&t[6], e->ev[1], e->ev[6]) == cudaSuccess;
+  if (!timed) {
+    cudaGetLastError();
+    for (int i = 0; i < 7; ++i) t[i] = -1.0f;
+  }
+  for (int i = 0; i < 7; ++i) e->stage_ms[i] = t[i];
+  return GZB_OK;
+}
+
 }  // namespace
+
+extern "C" int gzb_engine_set_graph(gzb_engine *e, int enable) {
+  GZB_TRY(check_engine(e));
+  e->graph = enable != 0;
+  if (!e->graph) drop_graphs(e);
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_reserve(gzb_engine *e, uint64_t hits, uint64_t member_work) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(hits >= 1 && member_work >= 1 && hits < (1ull << 40) && member_work < (1ull << 40),
+            GZB_ERR_INVALID, "capacities must be in 1 .. 2^40");
+  e->hit_cap = hits;
+  e->mwork_cap = member_work;
+  drop_graphs(e);
+  return GZB_OK;
+}
+
+extern "C" int gzb_engine_get_graph_stats(gzb_engine *e, uint64_t *captures, uint64_t *replays,
+                                          uint64_t *fallbacks) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(captures && replays && fallbacks, GZB_ERR_INVALID, "null argument");
+  *captures = e->graph_captures;
+  *replays = e->graph_replays;
+  *fallbacks = e->graph_fallbacks;
+  return GZB_OK;
+}
 
 extern "C" int gzb_engine_presearch(gzb_engine *e, int schedule, void *stream) {
   GZB_TRY(check_engine(e));
@@ -2293,6 +2741,15 @@ extern "C" int gzb_engine_presearch(gzb_engine *e, int schedule, void *stream) {
             GZB_ERR_INVALID, "unknown schedule %d", schedule);
   GZB_CHECK(e->params.max_number_one_subject_results <= 4, GZB_ERR_INVALID,
             "max_number_one_subject_results above 4 is not supported");
+  if (e->graph && schedule != GZB_SCHEDULE_ORACLE && !e->logging) {
+    // graph mode covers hit order; a cost-model order runs eagerly
+    GappedTile tile = g_tile;
+    for (int w = 0; w < 3; ++w)
+      if (e->tile[schedule][w] >= 0) *tile_field(tile, w) = e->tile[schedule][w];
+    const bool learned =
+        schedule == GZB_SCHEDULE_BATCHED && e->have_model && tile.order == GZB_ORDER_MODEL;
+    if (!learned) return presearch_graph(e, schedule, tile, (cudaStream_t)stream);
+  }
   return presearch_impl(e, schedule, (cudaStream_t)stream);
 }
 

@@ -42,7 +42,7 @@ __global__ void gapped_lane_kernel(GappedJob job, const int32_t *__restrict__ ma
                                    const uint8_t *__restrict__ dir, uint32_t *qpos,
                                    uint32_t *dpos, int32_t *scores, uint32_t *spill,
                                    uint32_t *spill_count, unsigned long long *cells_total,
-                                   uint32_t *cells_out);
+                                   uint32_t *cells_out, const uint64_t *n_dev);
 __global__ void gapped_warp_kernel(GappedJob job, const int32_t *__restrict__ matrix,
                                    int number_letters, int stride, const uint32_t *list,
                                    const uint32_t *list_count, int reverse,
@@ -137,7 +137,7 @@ extern "C" int gzb_gapped_extend_one_side_score_only_noalloc(
   gapped_lane_kernel<<<(unsigned)(blocks < 148 * 40 ? blocks : 148 * 40), 128, 0, s>>>(
       job, d_score_matrix, (int)number_letters, stride, size, nullptr, reverse, nullptr,
       d_query_concatenated_positions, d_database_positions, d_scores, spill1, counters, cells,
-      nullptr);
+      nullptr, nullptr);
   GZB_CUDA(cudaGetLastError());
   const uint32_t *serial_list = spill1, *serial_count = counters;
   if (warp_path_exact(cutoff)) {

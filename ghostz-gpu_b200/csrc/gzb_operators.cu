@@ -155,10 +155,11 @@ gapped_lane_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
                    int stride, size_t n, const uint32_t *__restrict__ order, int reverse,
                    const uint8_t *__restrict__ dir, uint32_t *qpos, uint32_t *dpos,
                    int32_t *scores, uint32_t *spill, uint32_t *spill_count,
-                   unsigned long long *cells_total, uint32_t *cells_out) {
+                   unsigned long long *cells_total, uint32_t *cells_out, const uint64_t *n_dev) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
   __shared__ uint32_t cells_s[kLaneW * kLaneBlock];
   __shared__ uint8_t res_s[kLaneW * kLaneBlock];
+  if (n_dev) n = *n_dev;
   load_matrix(sm, matrix, number_letters, stride);
   __syncthreads();
   LaneBand band{cells_s, res_s, kLaneBlock, (int)threadIdx.x};
@@ -195,9 +196,10 @@ gapped_flat_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
                    unsigned long long *queue, int reverse, const uint8_t *__restrict__ dir,
                    uint32_t *qpos, uint32_t *dpos, int32_t *scores, uint32_t *spill,
                    uint32_t *spill_count, unsigned long long *cells_total,
-                   uint32_t *cells_out, int book_threshold) {
+                   uint32_t *cells_out, int book_threshold, const uint64_t *n_dev) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
   extern __shared__ int2 flat_band[];
+  if (n_dev) n = *n_dev;
   load_matrix(sm, matrix, number_letters, stride);
   __syncthreads();
   FlatOut o{qpos, dpos, scores, spill, spill_count, cells_out};
@@ -218,10 +220,11 @@ gapped_lane_queue_kernel(GappedJob job, const int32_t *__restrict__ matrix, int 
                          unsigned long long *queue, int reverse, const uint8_t *__restrict__ dir,
                          uint32_t *qpos, uint32_t *dpos, int32_t *scores, uint32_t *spill,
                          uint32_t *spill_count, unsigned long long *cells_total,
-                         uint32_t *cells_out) {
+                         uint32_t *cells_out, const uint64_t *n_dev) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
   __shared__ uint32_t cells_s[kLaneW * kLaneBlock];
   __shared__ uint8_t res_s[kLaneW * kLaneBlock];
+  if (n_dev) n = *n_dev;
   load_matrix(sm, matrix, number_letters, stride);
   __syncthreads();
   LaneBand band{cells_s, res_s, kLaneBlock, (int)threadIdx.x};
@@ -271,10 +274,11 @@ gapped_rows_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
                    unsigned long long *queue, int reverse, const uint8_t *__restrict__ dir,
                    uint32_t *qpos, uint32_t *dpos, int32_t *scores, uint32_t *spill,
                    uint32_t *spill_count, unsigned long long *cells_total,
-                   uint32_t *cells_out, int refill_threshold) {
+                   uint32_t *cells_out, int refill_threshold, const uint64_t *n_dev) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
   __shared__ uint32_t cells_s[kLaneW * kLaneBlock];
   __shared__ uint8_t res_s[kLaneW * kLaneBlock];
+  if (n_dev) n = *n_dev;
   load_matrix(sm, matrix, number_letters, stride);
   __syncthreads();
   LaneBand band{cells_s, res_s, kLaneBlock, (int)threadIdx.x};
@@ -333,10 +337,11 @@ gapped_deal_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
                    int stride, uint64_t n, const uint32_t *__restrict__ order, int reverse,
                    const uint8_t *__restrict__ dir, uint32_t *qpos, uint32_t *dpos,
                    int32_t *scores, uint32_t *spill, uint32_t *spill_count,
-                   unsigned long long *cells_total, uint32_t *cells_out) {
+                   unsigned long long *cells_total, uint32_t *cells_out, const uint64_t *n_dev) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
   __shared__ uint32_t cells_s[kLaneW * kLaneBlock];
   __shared__ uint8_t res_s[kLaneW * kLaneBlock];
+  if (n_dev) n = *n_dev;
   load_matrix(sm, matrix, number_letters, stride);
   __syncthreads();
   LaneBand band{cells_s, res_s, kLaneBlock, (int)threadIdx.x};
@@ -417,31 +422,33 @@ int launch_gapped_thread(const GappedTile &tile, const GappedJob &job, const int
                          unsigned long long *queue, int reverse, const uint8_t *dir,
                          uint32_t *qpos, uint32_t *dpos, int32_t *scores, uint32_t *spill,
                          uint32_t *spill_count, unsigned long long *cells_total,
-                         uint32_t *cells_out, cudaStream_t s) {
+                         uint32_t *cells_out, cudaStream_t s, const uint64_t *n_dev) {
+  // with n_dev the count is read on the device and n is its upper bound
+  // (grids sized for n)
   GZB_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s));
   uint64_t blocks = 1;
   if (tile.kernel == GZB_GAPPED_KERNEL_DEAL) {
     GZB_TRY(persistent_blocks(gapped_deal_kernel, kLaneBlock, 0, n, &blocks));
     gapped_deal_kernel<<<(unsigned)blocks, kLaneBlock, 0, s>>>(
         job, matrix, number_letters, stride, n, order, reverse, dir, qpos, dpos, scores, spill,
-        spill_count, cells_total, cells_out);
+        spill_count, cells_total, cells_out, n_dev);
   } else if (tile.kernel == GZB_GAPPED_KERNEL_STATIC) {
     // one launch, extensions dealt to threads round-robin, no work queue
     blocks = (n + kLaneBlock - 1) / kLaneBlock;
     if (blocks > 148 * 40) blocks = 148 * 40;
     gapped_lane_kernel<<<(unsigned)blocks, kLaneBlock, 0, s>>>(
         job, matrix, number_letters, stride, n, order, reverse, dir, qpos, dpos, scores, spill,
-        spill_count, cells_total, cells_out);
+        spill_count, cells_total, cells_out, n_dev);
   } else if (tile.kernel == GZB_GAPPED_KERNEL_ROWS) {
     GZB_TRY(persistent_blocks(gapped_rows_kernel, kLaneBlock, 0, n, &blocks));
     gapped_rows_kernel<<<(unsigned)blocks, kLaneBlock, 0, s>>>(
         job, matrix, number_letters, stride, n, order, queue, reverse, dir, qpos, dpos, scores,
-        spill, spill_count, cells_total, cells_out, tile.book_threshold);
+        spill, spill_count, cells_total, cells_out, tile.book_threshold, n_dev);
   } else if (tile.kernel == GZB_GAPPED_KERNEL_LANE) {
     GZB_TRY(persistent_blocks(gapped_lane_queue_kernel, kLaneBlock, 0, n, &blocks));
     gapped_lane_queue_kernel<<<(unsigned)blocks, kLaneBlock, 0, s>>>(
         job, matrix, number_letters, stride, n, order, queue, reverse, dir, qpos, dpos, scores,
-        spill, spill_count, cells_total, cells_out);
+        spill, spill_count, cells_total, cells_out, n_dev);
   } else {
     const size_t smem = sizeof(int2) * (size_t)kFlatW * kFlatBlock;
     GZB_CUDA(cudaFuncSetAttribute(gapped_flat_kernel,
@@ -449,7 +456,7 @@ int launch_gapped_thread(const GappedTile &tile, const GappedJob &job, const int
     GZB_TRY(persistent_blocks(gapped_flat_kernel, kFlatBlock, smem, n, &blocks));
     gapped_flat_kernel<<<(unsigned)blocks, kFlatBlock, smem, s>>>(
         job, matrix, number_letters, stride, n, order, queue, reverse, dir, qpos, dpos, scores,
-        spill, spill_count, cells_total, cells_out, tile.book_threshold);
+        spill, spill_count, cells_total, cells_out, tile.book_threshold, n_dev);
   }
   GZB_CUDA(cudaGetLastError());
   return GZB_OK;
@@ -837,12 +844,24 @@ namespace gzb {
 // level is the thread kernel `tile` names.  counters: [0] spilled from the thread
 // kernel, [1] spilled from the warp kernel, [2] too long for the fallback.
 // `spill` needs room for 2n entries.  Synchronises `s` once at the end.
+// the serial fallback's band pool (allocated once)
+int ensure_band_pool(int2 **band_pool, int *band_wmask) {
+  if (!*band_pool) {
+    GZB_CUDA(cudaMalloc(band_pool, sizeof(int2) * (size_t)kSerialThreads * kSerialBand));
+    *band_wmask = kSerialBand - 1;
+  }
+  return GZB_OK;
+}
+
 int run_gapped(const GappedTile &tile, const GappedJob &job, const int32_t *matrix,
                int number_letters, int stride, size_t n, const uint32_t *order, int reverse,
                const uint8_t *dir, uint32_t *d_qpos, uint32_t *d_dpos, int32_t *d_scores,
                uint32_t **spill, size_t *spill_cap, uint32_t *counters,
                unsigned long long *cells, uint32_t *cells_out, int2 **band_pool,
-               int *band_wmask, cudaStream_t s, uint32_t *n_fallback) {
+               int *band_wmask, cudaStream_t s, uint32_t *n_fallback, const uint64_t *n_dev) {
+  // n_dev: the count is read on the device (n bounds it and sizes the
+  // grids), and the spill counts are left in counters for the caller (no
+  // host synchronisation)
   if (n == 0) return GZB_OK;
   if (*spill_cap < 2 * n) {
     cudaFree(*spill);
@@ -851,16 +870,13 @@ int run_gapped(const GappedTile &tile, const GappedJob &job, const int32_t *matr
     GZB_CUDA(cudaMalloc(spill, 4 * 2 * n));
     *spill_cap = 2 * n;
   }
-  if (!*band_pool) {
-    GZB_CUDA(cudaMalloc(band_pool, sizeof(int2) * (size_t)kSerialThreads * kSerialBand));
-    *band_wmask = kSerialBand - 1;
-  }
+  GZB_TRY(ensure_band_pool(band_pool, band_wmask));
   GZB_CUDA(cudaMemsetAsync(counters, 0, 16, s));
   uint32_t *spill1 = *spill, *spill2 = *spill + n;
   // counters[0..3]: spill counts; counters[8..9]: the work queue (64-bit)
   GZB_TRY(launch_gapped_thread(tile, job, matrix, number_letters, stride, n, order,
                                (unsigned long long *)(counters + 8), reverse, dir, d_qpos,
-                               d_dpos, d_scores, spill1, counters, cells, cells_out, s));
+                               d_dpos, d_scores, spill1, counters, cells, cells_out, s, n_dev));
   const uint32_t *serial_list = spill1, *serial_count = counters;
   if (warp_path_exact(job.cutoff)) {
     gapped_warp_kernel<<<148 * 4, kGappedWarps * 32, 0, s>>>(
@@ -874,6 +890,7 @@ int run_gapped(const GappedTile &tile, const GappedJob &job, const int32_t *matr
       job, matrix, number_letters, stride, serial_list, serial_count, reverse, dir, d_qpos,
       d_dpos, d_scores, *band_pool, *band_wmask, cells, counters + 2);
   GZB_CUDA(cudaGetLastError());
+  if (n_dev) return GZB_OK;
   uint32_t h[3] = {0, 0, 0};
   GZB_CUDA(cudaMemcpyAsync(h, counters, 12, cudaMemcpyDeviceToHost, s));
   GZB_CUDA(cudaStreamSynchronize(s));
@@ -902,7 +919,7 @@ extern "C" int gzb_gapped_extender_extend_one_side_score_only_async(
   GZB_TRY(run_gapped(g_tile, job, h->matrix, (int)h->number_letters,
                      (int)h->number_letters + 1, size, nullptr, reverse, nullptr, d_qpos,
                      d_dpos, d_scores, &h->spill, &h->spill_cap, h->counters, h->cells, nullptr,
-                     &h->band_pool, &h->band_wmask, s, nullptr));
+                     &h->band_pool, &h->band_wmask, s, nullptr, nullptr));
   if (qpos) GZB_CUDA(cudaMemcpyAsync(qpos, d_qpos, 4 * size, cudaMemcpyDefault, s));
   if (dpos) GZB_CUDA(cudaMemcpyAsync(dpos, d_dpos, 4 * size, cudaMemcpyDefault, s));
   if (scores) GZB_CUDA(cudaMemcpyAsync(scores, d_scores, 4 * size, cudaMemcpyDefault, s));

@@ -118,6 +118,9 @@ def _declare(L):
                                                C.c_uint64, V],
         "gzb_translate_dna_queries": [V, V, V, U32, V, C.c_uint8, V, V],
         "gzb_engine_swap_database": [V, U32, V],
+        "gzb_engine_set_graph": [V, C.c_int],
+        "gzb_engine_reserve": [V, C.c_uint64, C.c_uint64],
+        "gzb_engine_get_graph_stats": [V, V, V, V],
         "gzb_engine_prefetch_database_with_index": [V, U32, C.c_int32, V, C.c_uint64, V, U32,
                                                     V, C.c_uint64, V],
         "gzb_query_karlin_cutoffs": [V, V, V, U32, V, U32, C.c_float, C.c_float, V, V, V, V],
@@ -377,6 +380,20 @@ class PresearchEngine:
             check(lib().gzb_engine_set_database_with_index(
                 self.h, int(chunk_id), hptr(codes), len(codes), hptr(offs),
                 int(db.number_sequences), hptr(blob), blob.nbytes, _stream_or_null(stream)))
+
+    def set_graph(self, enable=True):
+        """Graph mode: the presearch runs as one captured CUDA graph."""
+        check(lib().gzb_engine_set_graph(self.h, 1 if enable else 0))
+
+    def reserve(self, hits, member_work):
+        """Capacities of the hit and member-work buffers (graph mode)."""
+        check(lib().gzb_engine_reserve(self.h, int(hits), int(member_work)))
+
+    def graph_stats(self):
+        """(captures, graph runs, eager redos) of graph mode."""
+        v = [C.c_uint64() for _ in range(3)]
+        check(lib().gzb_engine_get_graph_stats(self.h, *[C.byref(x) for x in v]))
+        return tuple(int(x.value) for x in v)
 
     def swap_database(self, slot, stream=None):
         """Exchanges the resident chunk with the chunk stored in `slot`."""

@@ -315,6 +315,24 @@ int gzb_engine_set_queries(gzb_engine *e, const uint8_t *codes,
  * and merges into the per-query top-b lists kept on the device.  Call
  * gzb_engine_reset_results before the first chunk of a query set. */
 int gzb_engine_presearch(gzb_engine *e, int schedule, void *stream);
+/* Graph mode (no counterpart in the reference, which launches every stage
+ * from the host with a round trip per buffer): with graph mode on,
+ * gzb_engine_presearch runs the whole presearch of the resident chunk --
+ * list lookup, seed search and ungapped extension, hit sort, chain filter,
+ * gapped extension, merge -- as one CUDA graph, captured on first use for
+ * that chunk, query set, schedule and tile and replayed afterwards (up to
+ * 16 graphs per engine, least recently used dropped), with no host
+ * synchronisation between stages.  Counts stay on the device and the
+ * buffers are sized to capacities for hits and member work (grown by every
+ * eager run, or set by gzb_engine_reserve); a run whose counts exceed them
+ * merges nothing and is redone eagerly with larger capacities, so results
+ * are always those of the eager path.  The cost-model order, the oracle
+ * schedule and logging run eagerly.  gzb_engine_get_graph_stats counts
+ * captures, graph runs and eager redos. */
+int gzb_engine_set_graph(gzb_engine *e, int enable);
+int gzb_engine_reserve(gzb_engine *e, uint64_t hits, uint64_t member_work);
+int gzb_engine_get_graph_stats(gzb_engine *e, uint64_t *captures, uint64_t *replays,
+                               uint64_t *fallbacks);
 int gzb_engine_reset_results(gzb_engine *e, void *stream);
 /* Copies the merged results to the host: counts[number_queries] and
  * results[number_queries * max_number_results] (row i holds counts[i]
