@@ -2347,6 +2347,14 @@ __global__ void ext_count_kernel(const uint64_t *surv_off, uint32_t nq, uint64_t
   plan[3] = 2 * surv_off[nq];
 }
 
+// the device clock (ns) when the stream reaches this point: stage times of
+// a graph run (events recorded inside a graph cannot be timed)
+__global__ void stamp_kernel(uint64_t *t) {
+  uint64_t v;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(v));
+  *t = v;
+}
+
 // everything the host reads after a graph run, in one place
 __global__ void report_kernel(const unsigned long long *ctr, const uint64_t *plan,
                               const unsigned long long *gcells, const uint32_t *gcounters,
@@ -2362,7 +2370,7 @@ __global__ void report_kernel(const unsigned long long *ctr, const uint64_t *pla
 }
 
 constexpr int kGraphCache = 16;        // graphs kept per engine
-constexpr int kReportWords = 16;
+constexpr int kReportWords = 24;   // plan[8..31]: report, then the stage stamps
 
 struct GraphCaps {
   uint64_t hits, mwork, ext;           // ext = 2 * hits (every hit may survive)
@@ -2398,7 +2406,8 @@ int graph_prepare(gzb_engine *e, const GraphCaps &c, int hit_bits, int mw_bits) 
   const uint32_t nq = e->nq;
   GZB_TRY(e->list_bufs[14].ensure(8 * (e->L.n_lists + 1)));
   GZB_TRY(e->ctr.ensure(64));
-  GZB_TRY(e->plan.ensure(8 * 32));  // [0..3] counts, [6] overflow, [8..20] report
+  // [0..3] counts, [6] overflow, [8..20] report, [24..30] stage stamps
+  GZB_TRY(e->plan.ensure(8 * 32));
   GZB_TRY(e->hits.ensure(8 * (c.hits + 1)));
   GZB_TRY(e->hits_alt.ensure(8 * (c.hits + 1)));
   GZB_TRY(e->hits_copy.ensure(8 * (c.hits + 1)));
@@ -2443,7 +2452,7 @@ int graph_body(gzb_engine *e, int schedule, const GappedTile &tile, const GraphC
   uint64_t *plan = e->plan.as<uint64_t>();
   uint32_t *overflow = reinterpret_cast<uint32_t *>(plan + 6);
   unsigned long long *ctr = e->ctr.as<unsigned long long>();
-  GZB_CUDA(cudaEventRecord(e->ev[0], s));
+  stamp_kernel<<<1, 1, 0, s>>>(plan + 24 + 0);
   GZB_CUDA(cudaMemsetAsync(plan, 0, 64, s));
   GZB_CUDA(cudaMemsetAsync(ctr, 0, 64, s));
   // list lookup; the unit count stays on the device
@@ -2456,7 +2465,7 @@ int graph_body(gzb_engine *e, int schedule, const GappedTile &tile, const GraphC
     GZB_CUDA(cudaMemsetAsync(unit_counts + L.n_lists, 0, 8, s));
     GZB_TRY(exclusive_sum(e, unit_counts, L.unit_offsets, L.n_lists + 1, s));
   }
-  GZB_CUDA(cudaEventRecord(e->ev[1], s));
+  stamp_kernel<<<1, 1, 0, s>>>(plan + 24 + 1);
   // seed search, distance and ungapped extension
   SeedArgs a;
   a.p = e->dp;
@@ -2498,7 +2507,7 @@ int graph_body(gzb_engine *e, int schedule, const GappedTile &tile, const GraphC
                                                 c.mwork, plan + 0);
   GZB_CUDA(cudaGetLastError());
   ++launches;
-  GZB_CUDA(cudaEventRecord(e->ev[6], s));
+  stamp_kernel<<<1, 1, 0, s>>>(plan + 24 + 6);
   // hits sorted by (query, database position, query position)
   clamp_count_kernel<<<1, 1, 0, s>>>(ctr + 4, c.hits, plan + 1, overflow, 2u);
   pad_keys_kernel<<<148 * 4, 256, 0, s>>>(e->hits.as<uint64_t>(), plan + 1, c.hits);
@@ -2509,7 +2518,7 @@ int graph_body(gzb_engine *e, int schedule, const GappedTile &tile, const GraphC
                         qbits + dbits + nqbits, s, &hits));
   ++launches;
   GZB_CUDA(cudaMemcpyAsync(e->hits_copy.p, hits, 8 * c.hits, cudaMemcpyDeviceToDevice, s));
-  GZB_CUDA(cudaEventRecord(e->ev[2], s));
+  stamp_kernel<<<1, 1, 0, s>>>(plan + 24 + 2);
   // chain filter
   uint64_t *begin = e->begin.as<uint64_t>();
   uint32_t *kept = e->kept.as<uint32_t>();
@@ -2529,7 +2538,7 @@ int graph_body(gzb_engine *e, int schedule, const GappedTile &tile, const GraphC
   ext_count_kernel<<<1, 1, 0, s>>>(surv_off, nq, plan);
   GZB_CUDA(cudaGetLastError());
   launches += 2;
-  GZB_CUDA(cudaEventRecord(e->ev[3], s));
+  stamp_kernel<<<1, 1, 0, s>>>(plan + 24 + 3);
   // gapped extension of both sides, in hit order
   build_ext_kernel<<<grid1((uint64_t)nq * 32, 256), 256, 0, s>>>(
       hits, begin, kept, surv_off, nq, e->q_offsets.as<uint32_t>(),
@@ -2554,7 +2563,7 @@ int graph_body(gzb_engine *e, int schedule, const GappedTile &tile, const GraphC
                      e->escore.as<int32_t>(), &e->spill, &e->spill_cap, e->gcounters,
                      e->gcells, nullptr, &e->band_pool, &e->band_wmask, s, nullptr, plan + 3));
   launches += 3;
-  GZB_CUDA(cudaEventRecord(e->ev[4], s));
+  stamp_kernel<<<1, 1, 0, s>>>(plan + 24 + 4);
   // top-b merge (nothing when a count overflowed)
   merge_kernel<<<grid1((uint64_t)nq * 32, 128), 128, 0, s>>>(
       nq, hits, begin, kept, surv_off, c.hits, e->eq.as<uint32_t>(), e->ed.as<uint32_t>(),
@@ -2565,12 +2574,12 @@ int graph_body(gzb_engine *e, int schedule, const GappedTile &tile, const GraphC
       e->counts.as<uint32_t>(), plan + 2, overflow);
   GZB_CUDA(cudaGetLastError());
   ++launches;
-  GZB_CUDA(cudaEventRecord(e->ev[5], s));
+  stamp_kernel<<<1, 1, 0, s>>>(plan + 24 + 5);
   report_kernel<<<1, 1, 0, s>>>(ctr, plan, e->gcells, e->gcounters, plan + 8);
   GZB_CUDA(cudaGetLastError());
   ++launches;
-  GZB_CUDA(cudaMemcpyAsync(e->report_h, plan + 8, 8 * 13, cudaMemcpyDeviceToHost, s));
-  *launches_out = launches;
+  GZB_CUDA(cudaMemcpyAsync(e->report_h, plan + 8, 8 * kReportWords, cudaMemcpyDeviceToHost, s));
+  *launches_out = launches + 7;  // and the seven stage stamps
   return GZB_OK;
 }
 
@@ -2689,17 +2698,12 @@ int presearch_graph(gzb_engine *e, int schedule, const GappedTile &tile, cudaStr
   e->last_mae_n = 0;
   e->pred_n = 0;
   e->prev_cells_n = 0;
-  float t[7];
-  bool timed = true;
-  for (int i = 0; i < 5 && timed; ++i)
-    timed = cudaEventElapsedTime(&t[i], e->ev[i], e->ev[i + 1]) == cudaSuccess;
-  if (timed) timed = cudaEventElapsedTime(&t[5], e->ev[0], e->ev[5]) == cudaSuccess;
-  if (timed) timed = cudaEventElapsedTime(&t[6], e->ev[1], e->ev[6]) == cudaSuccess;
-  if (!timed) {
-    cudaGetLastError();
-    for (int i = 0; i < 7; ++i) t[i] = -1.0f;
-  }
-  for (int i = 0; i < 7; ++i) e->stage_ms[i] = t[i];
+  // stage stamps at the points where the eager path records ev[0..6]
+  const uint64_t *stamp = r + 16;
+  auto ms = [&](int a, int b) { return (float)((double)(int64_t)(stamp[b] - stamp[a]) * 1e-6); };
+  for (int i = 0; i < 5; ++i) e->stage_ms[i] = ms(i, i + 1);
+  e->stage_ms[5] = ms(0, 5);
+  e->stage_ms[6] = ms(1, 6);
   return GZB_OK;
 }
 

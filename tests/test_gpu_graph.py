@@ -133,3 +133,25 @@ def test_one_graph_per_stored_chunk(native, params):
         assert fallbacks == 0 and replays == 9 and captures == len(chunks)
     finally:
         e.close()
+
+
+def test_graph_stage_times(native, params):
+    """Graph runs report their stage times from device clock stamps."""
+    N = native
+    db = W.make_database(1500, 905, median=250)
+    q = W.make_queries(db, 120, 906, median=250)
+    e = N.PresearchEngine(0)
+    try:
+        e.set_params(params)
+        e.set_database(db)
+        e.set_queries(q)
+        e.set_graph(True)
+        e.presearch(N.SCHEDULE_BATCHED)
+        st = e.stage_ms()
+        assert all(v >= 0 for v in st.values()), st
+        parts = st["lookup"] + st["seed_ungapped"] + st["chain"] + st["gapped"] + st["merge"]
+        assert abs(parts - st["total"]) < 1e-3 + 1e-3 * st["total"]
+        assert 0 < st["seed_kernels"] <= st["seed_ungapped"] + 1e-3
+        assert st["gapped"] > 0
+    finally:
+        e.close()
