@@ -116,7 +116,7 @@ def oracle_translated_queries(reads, limit=None):
     return W.translated_queries(codes, offs, lens, sources=reads.sources[:n], cutoffs=(cut, trig))
 
 
-def query_prep_bench(db, steps, warmup, cpu=True, seed=302):
+def query_prep_bench(db, steps, warmup, cpu=True, seed=302, reads=None):
     """Query preparation of translated-DNA searches (six-frame translation,
     SEG, per-query cutoffs) on the GPU over PREP_READS 150-nt reads held in
     HBM, timed with CUDA events; the oracle prepares a bounded sample on one
@@ -125,7 +125,7 @@ def query_prep_bench(db, steps, warmup, cpu=True, seed=302):
     from gzb import native as N
     from gzb import params as P
     from gzb import workload as W
-    reads = W.make_reads(db, PREP_READS, seed)
+    reads = W.make_reads(db, PREP_READS if reads is None else reads, seed)
     n = reads.number
     lens = np.diff(reads.offsets).astype(np.uint32)
     offs, qlen, total = N.translated_layout(lens)
@@ -644,12 +644,23 @@ def main():
     ap.add_argument("--ref-queries", type=int, default=10000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--prep-only", type=int, default=0, metavar="READS",
+                    help="time only the query preparation of READS 150-nt reads (reads "
+                         "drawn from a 20,000-protein database) and print its JSON object")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.prep_only:
+        import torch
+        from gzb import workload as W
+        torch.cuda.set_device(local_rank)
+        out = query_prep_bench(W.make_database(20000, 101), args.steps, args.warmup,
+                               cpu=False, reads=args.prep_only)
+        print(json.dumps({"query_preparation": out}), flush=True)
+        return
     if args.workload in MULTICHUNK_WORKLOADS:
         if args.impl == "reference":
             return run_reference_multichunk(args, world, rank)

@@ -13,9 +13,9 @@
 // The reverse strand is built by DnaSequence::GetComplementaryStrand
 // (src/dna_sequence.h:28-42): A/a->T, C/c->G, G/g->C, T/t->A, else N.
 //
-// One warp per read: lane i writes output bytes i, i + 32, ... of the
-// read's translated query, so the stores of a warp are contiguous; the
-// codon's three bases are read from the (L1-resident) read.
+// One warp per read: lane j translates codon j of all six frames, so for
+// each frame the stores of a warp are contiguous; the read's bases come
+// from L1 (a lane reads five consecutive bases per strand).
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -78,29 +78,39 @@ __global__ void __launch_bounds__(kTranslateBlock)
       continue;
     }
     const uint32_t slot = len / 3 + 1;
-    const uint32_t total = 1 + 6 * slot;
-    for (uint32_t i = lane; i < total; i += 32) {
-      uint8_t v = delimiter;
-      if (i > 0) {
-        const uint32_t f = (i - 1) / slot;
-        const uint32_t j = (i - 1) - f * slot;
-        const uint32_t o = f < 3 ? f : f - 3;
-        if (j < (len - o) / 3) {  // codons of this frame: (len - o) / 3
-          const uint32_t p = o + 3 * j;
-          uint8_t x, y, z;
-          if (f < 3) {
-            x = fwd[s[p]];
-            y = fwd[s[p + 1]];
-            z = fwd[s[p + 2]];
-          } else {  // complementary strand position p is read position len-1-p
-            x = rev[s[len - 1 - p]];
-            y = rev[s[len - 2 - p]];
-            z = rev[s[len - 3 - p]];
-          }
-          v = (x | y | z) & kNoBase ? kUnknownCode : codon[x * 16 + y * 4 + z];
-        }
+    const uint32_t n0 = len / 3, n1 = (len - 1) / 3, n2 = (len - 2) / 3;  // codons per offset
+    if (lane == 0) q[0] = delimiter;
+    // lane j: codon j of all six frames (slot position j of each frame)
+    for (uint32_t j = lane; j < slot; j += 32) {
+      const uint32_t p = 3 * j;
+      uint8_t v0 = delimiter, v1 = delimiter, v2 = delimiter;
+      uint8_t r0 = delimiter, r1 = delimiter, r2 = delimiter;
+      if (j < n0) {
+        const uint8_t a = fwd[s[p]], b = fwd[s[p + 1]], c = fwd[s[p + 2]];
+        v0 = (a | b | c) & kNoBase ? kUnknownCode : codon[a * 16 + b * 4 + c];
+        // the complementary strand's codon j, offset 0: read positions len-1-p ..
+        const uint8_t x = rev[s[len - 1 - p]], y = rev[s[len - 2 - p]], z = rev[s[len - 3 - p]];
+        r0 = (x | y | z) & kNoBase ? kUnknownCode : codon[x * 16 + y * 4 + z];
       }
-      q[i] = v;
+      if (j < n1) {
+        const uint8_t a = fwd[s[p + 1]], b = fwd[s[p + 2]], c = fwd[s[p + 3]];
+        v1 = (a | b | c) & kNoBase ? kUnknownCode : codon[a * 16 + b * 4 + c];
+        const uint8_t x = rev[s[len - 2 - p]], y = rev[s[len - 3 - p]], z = rev[s[len - 4 - p]];
+        r1 = (x | y | z) & kNoBase ? kUnknownCode : codon[x * 16 + y * 4 + z];
+      }
+      if (j < n2) {
+        const uint8_t a = fwd[s[p + 2]], b = fwd[s[p + 3]], c = fwd[s[p + 4]];
+        v2 = (a | b | c) & kNoBase ? kUnknownCode : codon[a * 16 + b * 4 + c];
+        const uint8_t x = rev[s[len - 3 - p]], y = rev[s[len - 4 - p]], z = rev[s[len - 5 - p]];
+        r2 = (x | y | z) & kNoBase ? kUnknownCode : codon[x * 16 + y * 4 + z];
+      }
+      uint8_t *f = q + 1 + j;
+      f[0] = v0;
+      f[slot] = v1;
+      f[2 * slot] = v2;
+      f[3 * slot] = r0;
+      f[4 * slot] = r1;
+      f[5 * slot] = r2;
     }
   }
 }
