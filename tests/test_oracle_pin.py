@@ -369,13 +369,13 @@ def test_query_karlin_matches_reference(oracle, reference, params):
 
 
 # --- SEG low-complexity filter (query preparation) -----------------------------
-REF_LN_FACT = "/root/reference/ext/seg/src/ln_factrial_table.h"
-
-
 def test_seg_ln_factorial_table_matches_reference(oracle):
-    # ext/seg/src/ln_factrial_table.h: ln(n!) to 6 decimals, n = 0..10000
+    # ext/seg/src/ln_factrial_table.h: ln(n!) to 6 decimals, n = 0..10000,
+    # read as text from the reference checkout the oracle's recipe uses
     import os
     import re
+    import oracle as O
+    REF_LN_FACT = os.path.join(O.REF_ROOT, "ext", "seg", "src", "ln_factrial_table.h")
     if not os.path.exists(REF_LN_FACT):
         pytest.skip("reference checkout not present")
     text = open(REF_LN_FACT).read()
