@@ -143,7 +143,8 @@ __device__ __forceinline__ float bf16_round(float v) {
 // broadcasts, one sample per thread.
 __global__ void __launch_bounds__(256)
 mlp_predict_kernel(const float *__restrict__ params, const float *__restrict__ X, uint32_t n,
-                   float *__restrict__ out) {
+                   float *__restrict__ out, const uint64_t *n_dev) {
+  if (n_dev) n = (uint32_t)*n_dev;
   __shared__ __align__(16) float P[(kParams + 3) & ~3];
   for (int i = threadIdx.x; i < kParams; i += blockDim.x) P[i] = bf16_round(params[i]);
   __syncthreads();
@@ -228,12 +229,12 @@ int cost_gradients(const float *d_params, const float *d_x, const float *d_y,
 }
 
 int cost_predict(const float *d_params, const float *d_x, uint32_t n, float *d_out,
-                 cudaStream_t s) {
+                 cudaStream_t s, const uint64_t *n_dev) {
   if (n == 0) return GZB_OK;
   GZB_CHECK(((uintptr_t)d_x & 15) == 0, GZB_ERR_INVALID, "features must be 16-byte aligned");
   unsigned g = (unsigned)((n + 255) / 256);
   if (g > 148 * 16) g = 148 * 16;
-  mlp_predict_kernel<<<g, 256, 0, s>>>(d_params, d_x, n, d_out);
+  mlp_predict_kernel<<<g, 256, 0, s>>>(d_params, d_x, n, d_out, n_dev);
   GZB_CUDA(cudaGetLastError());
   return GZB_OK;
 }
@@ -390,7 +391,7 @@ extern "C" int gzb_cost_model_gradients(const float *d_params, const float *d_x,
 extern "C" int gzb_cost_model_predict(const float *d_params, const float *d_x, uint32_t n,
                                       float *d_out, void *stream) {
   GZB_CHECK(d_params && d_x && d_out, GZB_ERR_INVALID, "null argument");
-  return cost_predict(d_params, d_x, n, d_out, (cudaStream_t)stream);
+  return cost_predict(d_params, d_x, n, d_out, (cudaStream_t)stream, nullptr);
 }
 
 extern "C" int gzb_cost_model_train(const float *d_x, const float *d_y, uint32_t n,

@@ -37,7 +37,7 @@ namespace cg = cooperative_groups;
 namespace gzb {
 
 int cost_predict(const float *d_params, const float *d_x, uint32_t n, float *d_out,
-                 cudaStream_t s);
+                 cudaStream_t s, const uint64_t *n_dev);
 int cost_train(const float *d_x, const float *d_y, uint32_t n, float *params, int epochs,
                int batch, float lr, uint64_t seed, float *final_loss, cudaStream_t s);
 __global__ void gapped_warp_kernel(GappedJob job, const int32_t *__restrict__ matrix,
@@ -759,7 +759,8 @@ __global__ void ext_features_kernel(const uint8_t *__restrict__ q, const uint8_t
                                     const uint32_t *eq, const uint32_t *ed,
                                     const uint32_t *elen0, const uint32_t *elen1,
                                     const uint32_t *eqid, const uint32_t *neighbours,
-                                    float *feat) {
+                                    float *feat, const uint64_t *n_dev) {
+  if (n_dev) n_surv = *n_dev;
   for (uint64_t h = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; h < n_surv;
        h += (uint64_t)gridDim.x * blockDim.x) {
     const uint64_t r = h, f = n_surv + h;
@@ -778,8 +779,20 @@ __global__ void ext_features_kernel(const uint8_t *__restrict__ q, const uint8_t
 }
 
 // sort key: larger predicted cost first; ties keep extension order
+// With n_dev the count is read on the device and entries n .. cap get the
+// largest key (they sort last).
 __global__ void cost_keys_kernel(const float *pred, const uint32_t *true_cells, uint64_t n,
-                                 uint32_t *keys, uint32_t *vals) {
+                                 uint32_t *keys, uint32_t *vals, const uint64_t *n_dev,
+                                 uint64_t cap) {
+  if (n_dev) {
+    const uint64_t m = *n_dev;
+    for (uint64_t i = m + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < cap;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+      keys[i] = 0xFFFFFFFFu;
+      vals[i] = (uint32_t)i;
+    }
+    n = m;
+  }
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
        i += (uint64_t)gridDim.x * blockDim.x) {
     float c = pred ? pred[i] : log2f(1.0f + (float)true_cells[i]);
@@ -2214,7 +2227,7 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
           job.query, job.db, job.delim, e->matrix32.as<int32_t>(), e->q_cut.as<int32_t>(),
           n_surv, e->eq.as<uint32_t>(), e->ed.as<uint32_t>(), e->elen0.as<uint32_t>(),
           e->elen1.as<uint32_t>(), e->eqid.as<uint32_t>(), e->enb.as<uint32_t>(),
-          e->efeat.as<float>());
+          e->efeat.as<float>(), nullptr);
       GZB_CUDA(cudaGetLastError());
       ++launches;
     }
@@ -2227,13 +2240,13 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
       if (learned) {
         GZB_TRY(e->epred.ensure(4 * (next + 1)));
         GZB_TRY(cost_predict(e->model_d.as<float>(), e->efeat.as<float>(), (uint32_t)next,
-                             e->epred.as<float>(), s));
+                             e->epred.as<float>(), s, nullptr));
         e->pred_n = next;
         ++launches;
       }
       cost_keys_kernel<<<grid1(next, 256), 256, 0, s>>>(
           learned ? e->epred.as<float>() : nullptr, e->prev_cells.as<uint32_t>(), next,
-          e->okeys.as<uint32_t>(), e->oidx.as<uint32_t>());
+          e->okeys.as<uint32_t>(), e->oidx.as<uint32_t>(), nullptr, 0);
       GZB_CUDA(cudaGetLastError());
       ++launches;
       cub::DoubleBuffer<uint32_t> kb(e->okeys.as<uint32_t>(), e->okeys2.as<uint32_t>());
@@ -2386,7 +2399,9 @@ GraphCaps graph_caps(const gzb_engine *e) {
 
 int graph_sort_bytes(const gzb_engine *e, const GraphCaps &c, int hit_bits, int mw_bits,
                      size_t *bytes) {
-  size_t a = 0, b = 0, d = 0, f = 0;
+  size_t a = 0, b = 0, d = 0, f = 0, g = 0;
+  cub::DoubleBuffer<uint32_t> k32(nullptr, nullptr), v32(nullptr, nullptr);
+  GZB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, g, k32, v32, (int64_t)c.ext, 0, 32));
   cub::DoubleBuffer<uint64_t> k1(nullptr, nullptr);
   GZB_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, a, k1, (int64_t)c.hits, 0, hit_bits));
   GZB_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, b, k1, (int64_t)c.mwork, 0, mw_bits));
@@ -2396,13 +2411,13 @@ int graph_sort_bytes(const gzb_engine *e, const GraphCaps &c, int hit_bits, int 
   GZB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, d, u64, o64,
                                          (int64_t)(e->L.n_lists + 1)));
   GZB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, f, u32, o64, (int64_t)(e->nq + 1)));
-  *bytes = std::max(std::max(a, b), std::max(d, f));
+  *bytes = std::max(std::max(std::max(a, b), std::max(d, f)), g);
   return GZB_OK;
 }
 
 // every buffer the graph touches, at its capacity (before capture: the
 // capture itself must not allocate)
-int graph_prepare(gzb_engine *e, const GraphCaps &c, int hit_bits, int mw_bits) {
+int graph_prepare(gzb_engine *e, const GraphCaps &c, int hit_bits, int mw_bits, bool learned) {
   const uint32_t nq = e->nq;
   GZB_TRY(e->list_bufs[14].ensure(8 * (e->L.n_lists + 1)));
   GZB_TRY(e->ctr.ensure(64));
@@ -2423,6 +2438,11 @@ int graph_prepare(gzb_engine *e, const GraphCaps &c, int hit_bits, int mw_bits) 
   GZB_TRY(e->enb.ensure(4 * (c.hits + 1)));
   GZB_TRY(e->merge_scratch.ensure(sizeof(gzb_result) * (c.hits + 1)));
   GZB_TRY(e->heap.ensure(c.hits + 1));
+  if (learned) {  // the cost-model order
+    GZB_TRY(e->efeat.ensure(4 * kFeat * (c.ext + 1)));
+    for (DBuf *b : {&e->epred, &e->okeys, &e->okeys2, &e->oidx, &e->oidx2})
+      GZB_TRY(b->ensure(4 * (c.ext + 1)));
+  }
   size_t tb = 0;
   GZB_TRY(graph_sort_bytes(e, c, hit_bits, mw_bits, &tb));
   GZB_TRY(e->tmp.ensure(tb));
@@ -2443,8 +2463,9 @@ int graph_prepare(gzb_engine *e, const GraphCaps &c, int hit_bits, int mw_bits) 
 }
 
 // the presearch body recorded into the graph
-int graph_body(gzb_engine *e, int schedule, const GappedTile &tile, const GraphCaps &c,
-               int qbits, int dbits, int nqbits, cudaStream_t s, uint64_t *launches_out) {
+int graph_body(gzb_engine *e, int schedule, const GappedTile &tile, bool learned,
+               const GraphCaps &c, int qbits, int dbits, int nqbits, cudaStream_t s,
+               uint64_t *launches_out) {
   uint64_t launches = 0;
   DevLists &L = e->L;
   const DevIndex &X = e->X;
@@ -2558,7 +2579,29 @@ int graph_body(gzb_engine *e, int schedule, const GappedTile &tile, const GraphC
   job.cutoff = e->params.gapped_cutoff;
   GappedTile t = tile;
   if (schedule == GZB_SCHEDULE_PLAIN) t.kernel = GZB_GAPPED_KERNEL_STATIC;
-  GZB_TRY(run_gapped(t, job, e->matrix32.as<int32_t>(), 32, 32, c.ext, nullptr, 0,
+  const uint32_t *order = nullptr;
+  if (learned) {
+    // longest predicted first: features, the cost model, keys, one sort
+    ext_features_kernel<<<grid1(c.hits, 256), 256, 0, s>>>(
+        job.query, job.db, job.delim, e->matrix32.as<int32_t>(), e->q_cut.as<int32_t>(),
+        c.hits, e->eq.as<uint32_t>(), e->ed.as<uint32_t>(), e->elen0.as<uint32_t>(),
+        e->elen1.as<uint32_t>(), e->eqid.as<uint32_t>(), e->enb.as<uint32_t>(),
+        e->efeat.as<float>(), plan + 2);
+    GZB_CUDA(cudaGetLastError());
+    GZB_TRY(cost_predict(e->model_d.as<float>(), e->efeat.as<float>(), (uint32_t)c.ext,
+                         e->epred.as<float>(), s, plan + 3));
+    cost_keys_kernel<<<grid1(c.ext, 256), 256, 0, s>>>(e->epred.as<float>(), nullptr, c.ext,
+                                                       e->okeys.as<uint32_t>(),
+                                                       e->oidx.as<uint32_t>(), plan + 3, c.ext);
+    GZB_CUDA(cudaGetLastError());
+    cub::DoubleBuffer<uint32_t> kb(e->okeys.as<uint32_t>(), e->okeys2.as<uint32_t>());
+    cub::DoubleBuffer<uint32_t> vb(e->oidx.as<uint32_t>(), e->oidx2.as<uint32_t>());
+    size_t tb = e->tmp.bytes;
+    GZB_CUDA(cub::DeviceRadixSort::SortPairs(e->tmp.p, tb, kb, vb, (int64_t)c.ext, 0, 32, s));
+    order = vb.Current();
+    launches += 4;
+  }
+  GZB_TRY(run_gapped(t, job, e->matrix32.as<int32_t>(), 32, 32, c.ext, order, 0,
                      e->edir.as<uint8_t>(), e->eq.as<uint32_t>(), e->ed.as<uint32_t>(),
                      e->escore.as<int32_t>(), &e->spill, &e->spill_cap, e->gcounters,
                      e->gcells, nullptr, &e->band_pool, &e->band_wmask, s, nullptr, plan + 3));
@@ -2591,7 +2634,7 @@ uint64_t fnv_mix(uint64_t h, const void *p, size_t n) {
 
 // what a captured graph depends on: every buffer it touches (address and
 // size), the chunk, the queries, the schedule, the tile and the capacities
-uint64_t graph_key(const gzb_engine *e, int schedule, const GappedTile &tile,
+uint64_t graph_key(const gzb_engine *e, int schedule, const GappedTile &tile, bool learned,
                    const GraphCaps &c) {
   uint64_t h = 1469598103934665603ull;
   const DBuf *bufs[] = {&e->db_buf, &e->db_offsets, &e->q_buf, &e->q_offsets, &e->q_lengths,
@@ -2599,7 +2642,9 @@ uint64_t graph_key(const gzb_engine *e, int schedule, const GappedTile &tile,
                         &e->tmp, &e->hits, &e->hits_alt, &e->hits_copy, &e->mwork,
                         &e->mwork_alt, &e->begin, &e->kept, &e->surv_off, &e->slots, &e->eq,
                         &e->ed, &e->edir, &e->escore, &e->elen0, &e->elen1, &e->eqid, &e->enb,
-                        &e->merge_scratch, &e->heap, &e->ctr, &e->plan, &e->list_bufs[14]};
+                        &e->merge_scratch, &e->heap, &e->ctr, &e->plan, &e->list_bufs[14],
+                        &e->efeat, &e->epred, &e->okeys, &e->okeys2, &e->oidx, &e->oidx2,
+                        &e->model_d};
   for (const DBuf *b : bufs) {
     h = fnv_mix(h, &b->p, sizeof(b->p));
     h = fnv_mix(h, &b->bytes, sizeof(b->bytes));
@@ -2613,7 +2658,8 @@ uint64_t graph_key(const gzb_engine *e, int schedule, const GappedTile &tile,
                         (uint64_t)tile.book_threshold, (uint64_t)tile.order, c.hits, c.mwork,
                         (uint64_t)(uintptr_t)e->spill, e->spill_cap,
                         (uint64_t)(uintptr_t)e->band_pool, (uint64_t)(uintptr_t)e->gcounters,
-                        (uint64_t)(uintptr_t)e->gcells, (uint64_t)(uintptr_t)e->report_h};
+                        (uint64_t)(uintptr_t)e->gcells, (uint64_t)(uintptr_t)e->report_h,
+                        (uint64_t)learned};
   return fnv_mix(h, v, sizeof(v));
 }
 
@@ -2622,7 +2668,8 @@ void drop_graphs(gzb_engine *e) {
   e->graphs.clear();
 }
 
-int presearch_graph(gzb_engine *e, int schedule, const GappedTile &tile, cudaStream_t user) {
+int presearch_graph(gzb_engine *e, int schedule, const GappedTile &tile, bool learned,
+                    cudaStream_t user) {
   const uint32_t nq = e->nq;
   const int qbits = bits_for(e->max_qlen);
   const int dbits = bits_for(e->db_len + 1);
@@ -2631,8 +2678,9 @@ int presearch_graph(gzb_engine *e, int schedule, const GappedTile &tile, cudaStr
             "hit key needs %d bits (queries %u, chunk %llu, longest query %u)",
             qbits + dbits + nqbits, nq, (unsigned long long)e->db_len, e->max_qlen);
   const GraphCaps c = graph_caps(e);
-  GZB_TRY(graph_prepare(e, c, qbits + dbits + nqbits, bits_for(e->X.n_reps + 1)));
-  const uint64_t key = graph_key(e, schedule, tile, c);
+  GZB_CHECK(c.ext < (1ull << 32), GZB_ERR_OVERFLOW, "graph mode: extension capacity above 2^32");
+  GZB_TRY(graph_prepare(e, c, qbits + dbits + nqbits, bits_for(e->X.n_reps + 1), learned));
+  const uint64_t key = graph_key(e, schedule, tile, learned, c);
   gzb_engine::GraphEntry *g = nullptr;
   for (auto &x : e->graphs)
     if (x.key == key) g = &x;
@@ -2647,7 +2695,7 @@ int presearch_graph(gzb_engine *e, int schedule, const GappedTile &tile, cudaStr
     }
     GZB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     uint64_t launches = 0;
-    const int rc = graph_body(e, schedule, tile, c, qbits, dbits, nqbits, s, &launches);
+    const int rc = graph_body(e, schedule, tile, learned, c, qbits, dbits, nqbits, s, &launches);
     cudaGraph_t graph = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(s, &graph);
     if (rc != GZB_OK) {
@@ -2696,7 +2744,7 @@ int presearch_graph(gzb_engine *e, int schedule, const GappedTile &tile, cudaStr
   e->counters.kernel_launches = g->launches;
   e->last_mae = -1.0f;
   e->last_mae_n = 0;
-  e->pred_n = 0;
+  e->pred_n = learned ? 2 * r[6] : 0;
   e->prev_cells_n = 0;
   // stage stamps at the points where the eager path records ev[0..6]
   const uint64_t *stamp = r + 16;
@@ -2752,7 +2800,7 @@ extern "C" int gzb_engine_presearch(gzb_engine *e, int schedule, void *stream) {
       if (e->tile[schedule][w] >= 0) *tile_field(tile, w) = e->tile[schedule][w];
     const bool learned =
         schedule == GZB_SCHEDULE_BATCHED && e->have_model && tile.order == GZB_ORDER_MODEL;
-    if (!learned) return presearch_graph(e, schedule, tile, (cudaStream_t)stream);
+    return presearch_graph(e, schedule, tile, learned, (cudaStream_t)stream);
   }
   return presearch_impl(e, schedule, (cudaStream_t)stream);
 }

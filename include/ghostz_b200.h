@@ -326,9 +326,10 @@ int gzb_engine_presearch(gzb_engine *e, int schedule, void *stream);
  * buffers are sized to capacities for hits and member work (grown by every
  * eager run, or set by gzb_engine_reserve); a run whose counts exceed them
  * merges nothing and is redone eagerly with larger capacities, so results
- * are always those of the eager path.  The cost-model order, the oracle
- * schedule and logging run eagerly.  gzb_engine_get_graph_stats counts
- * captures, graph runs and eager redos. */
+ * are always those of the eager path.  The cost-model order runs inside
+ * the graph (features, prediction and the key sort); the oracle schedule
+ * and logging run eagerly.  gzb_engine_get_graph_stats counts captures,
+ * graph runs and eager redos. */
 int gzb_engine_set_graph(gzb_engine *e, int enable);
 int gzb_engine_reserve(gzb_engine *e, uint64_t hits, uint64_t member_work);
 int gzb_engine_get_graph_stats(gzb_engine *e, uint64_t *captures, uint64_t *replays,

@@ -155,3 +155,42 @@ def test_graph_stage_times(native, params):
         assert st["gapped"] > 0
     finally:
         e.close()
+
+
+@pytest.mark.parametrize("kernel", ["rows", "lane"])
+def test_graph_with_cost_model_order(native, params, kernel):
+    """The cost-model order inside the graph: same results as the eager
+    path, the order coming from the model's predictions on the device."""
+    N = native
+    db = W.make_database(1500, 907, median=250)
+    q = W.make_queries(db, 120, 908, median=250)
+    model = N.cost_model_init(seed=5)
+    ker = {"rows": N.GAPPED_KERNEL_ROWS, "lane": N.GAPPED_KERNEL_LANE}[kernel]
+
+    def engine(graph):
+        e = N.PresearchEngine(0)
+        e.set_params(params)
+        e.set_database(db)
+        e.set_queries(q)
+        e.set_cost_model(model)
+        e.set_tile(N.SCHEDULE_BATCHED, N.TILE_GAPPED_KERNEL, ker)
+        e.set_tile(N.SCHEDULE_BATCHED, N.TILE_ORDER, N.ORDER_MODEL)
+        e.set_graph(graph)
+        return e
+
+    ref, e = engine(False), engine(True)
+    try:
+        ref.presearch(N.SCHEDULE_BATCHED)
+        exp, cnt = ref.results(), ref.counters()
+        for _ in range(2):
+            e.reset_results()
+            e.presearch(N.SCHEDULE_BATCHED)
+            _same(e.results(), exp)
+            got = e.counters()
+            for k in COUNTERS:
+                assert got[k] == cnt[k], k
+        captures, replays, fallbacks = e.graph_stats()
+        assert captures == 1 and replays == 2 and fallbacks == 0
+    finally:
+        ref.close()
+        e.close()
