@@ -9,7 +9,9 @@
 // ungapped X-drop and the gapped-extension trigger
 // (src/aligner_gpu.cpp:228-238, src/statistics.cpp:28-43).
 //
-// One warp per query.  The composition is counted by the whole warp; the
+// One warp per query, in two passes (buffers for 24 rounds of the K series,
+// then for all 100 for the rare query that needs more).  The composition is
+// counted by the whole warp; the
 // score distribution's j-fold convolutions for K are spread over the lanes
 // (each lane owns whole entries, so every entry is summed in the
 // reference's order); every serial sum stays on lane 0 in the reference's
@@ -28,8 +30,14 @@ namespace gzb {
 
 namespace {
 
-constexpr int kKarlinWarps = 2;               // warps per block
 constexpr int kKarlinIterMax = 100;           // BLAST_KARLIN_K_ITER_MAX
+// A first pass gives each warp convolution buffers for kFastIter rounds of
+// the K series (the series usually ends after 10-15), so more warps fit on
+// an SM; a query that needs more rounds is marked and redone by a second
+// pass with buffers for all kKarlinIterMax rounds.
+constexpr int kFastIter = 24, kFastWarps = 4;
+constexpr int kFullWarps = 2;
+constexpr int32_t kPending = INT32_MIN;       // cutoff of a query left to the second pass
 constexpr int kMaxLetters = 32;
 constexpr int kMaxRange = 31;                 // highest - lowest score
 constexpr int kMaxRegular = 19;               // ARNDCQEGHILKMFPSTWYV
@@ -152,22 +160,26 @@ __device__ double entropy(const double *sp, int lo, int hi, double lambda) {
   return dmul(lambda, av);
 }
 
-__global__ void __launch_bounds__(kKarlinWarps * 32)
+// kIter: rounds of the K series the buffers hold.  kRetry: the second pass
+// (only queries whose cutoff holds kPending).
+template <int kWarps, int kIter, bool kRetry>
+__global__ void __launch_bounds__(kWarps * 32)
     karlin_kernel(KarlinArgs a, const uint8_t *__restrict__ codes,
                   const uint64_t *__restrict__ offsets, const uint32_t *__restrict__ lengths,
                   uint32_t n, int32_t *__restrict__ cutoffs, int32_t *__restrict__ triggers,
                   float *__restrict__ karlin) {
   extern __shared__ double dist[];  // per warp: two convolution buffers
-  __shared__ int count[kKarlinWarps][kMaxLetters];
-  __shared__ double freq[kKarlinWarps][kMaxLetters];
-  __shared__ double prob[kKarlinWarps][kMaxRange + 1];
+  __shared__ int count[kWarps][kMaxLetters];
+  __shared__ double freq[kWarps][kMaxLetters];
+  __shared__ double prob[kWarps][kMaxRange + 1];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int low = a.low, high = a.high, range = high - low;
-  const int cap = kKarlinIterMax * range + 1;
+  const int cap = kIter * range + 1;
   double *buf0 = dist + (size_t)w * 2 * cap, *buf1 = buf0 + cap;
   const int nl = a.number_letters;
-  const uint32_t warps = gridDim.x * kKarlinWarps;
-  for (uint32_t r = blockIdx.x * kKarlinWarps + w; r < n; r += warps) {
+  const uint32_t warps = gridDim.x * kWarps;
+  for (uint32_t r = blockIdx.x * kWarps + w; r < n; r += warps) {
+    if (kRetry && cutoffs[r] != kPending) continue;
     // composition of regular letters over the whole query
     count[w][lane] = 0;
     __syncwarp();
@@ -217,6 +229,7 @@ __global__ void __launch_bounds__(kKarlinWarps * 32)
     // K (BlastKarlinLHtoK)
     const double lambda = (double)l, H = (double)h;
     double K = -1.0;
+    bool pending = false;  // the series needs more rounds than the buffers hold
     if (lambda > 0.0 && H > 0.0) {
       const double av = ddiv(H, lambda);
       const double etolam = exp(lambda);
@@ -229,7 +242,7 @@ __global__ void __launch_bounds__(kKarlinWarps * 32)
         double *cur = buf0, *nxt = buf1;
         if (lane == 0) cur[0] = 1.0;
         __syncwarp();
-        while (j < kKarlinIterMax && sum > sumlimit) {
+        while (j < kIter && sum > sumlimit) {
           lo += low;
           hi += high;
           const int top = hi - lo;
@@ -263,7 +276,9 @@ __global__ void __launch_bounds__(kKarlinWarps * 32)
           Sum = dadd(Sum, sum);
         }
         const double ratio = ddiv(oldsum, oldsum2);
-        if (!(ratio >= dsub(1.0, dmul(sumlimit, 0.001)))) {
+        if (kIter < kKarlinIterMax && j == kIter && sum > sumlimit) {
+          pending = true;
+        } else if (!(ratio >= dsub(1.0, dmul(sumlimit, 0.001)))) {
           sumlimit = dmul(sumlimit, 0.01);
           while (sum > sumlimit) {
             oldsum = dmul(oldsum, ratio);
@@ -285,7 +300,8 @@ __global__ void __launch_bounds__(kKarlinWarps * 32)
         }
       }
     }
-    if (lane == 0) {
+    if (lane == 0 && pending) cutoffs[r] = kPending;
+    if (lane == 0 && !pending) {
       const float k = (float)K;
       // NormalizedCutoff2NominalCutoff and Normalized2Nominal in float; ln K
       // is the float nearest the exact logarithm
@@ -355,17 +371,28 @@ extern "C" int gzb_query_karlin_cutoffs(const uint8_t *d_codes, const uint64_t *
   if (number_queries == 0) return GZB_OK;
   GZB_CHECK(d_codes && d_offsets && d_lengths && d_cutoffs && d_triggers, GZB_ERR_INVALID,
             "gzb_query_karlin_cutoffs: null buffer");
-  const size_t smem = (size_t)kKarlinWarps * 2 * (kKarlinIterMax * (hi - lo) + 1) * sizeof(double);
-  GZB_CUDA(cudaFuncSetAttribute(karlin_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem));
   int device = 0, sms = 148;
   GZB_CUDA(cudaGetDevice(&device));
   GZB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-  const uint64_t want = (number_queries + kKarlinWarps - 1) / kKarlinWarps;
-  const uint64_t most = (uint64_t)sms * 8;
-  const uint32_t blocks = (uint32_t)(want < most ? want : most);
-  karlin_kernel<<<blocks, kKarlinWarps * 32, smem, (cudaStream_t)stream>>>(
-      a, d_codes, d_offsets, d_lengths, number_queries, d_cutoffs, d_triggers, d_karlin);
+  const int range = hi - lo;
+  // pass 1: buffers for kFastIter rounds; pass 2: the queries it left
+  const size_t smem_fast = (size_t)kFastWarps * 2 * (kFastIter * range + 1) * sizeof(double);
+  const size_t smem_full = (size_t)kFullWarps * 2 * (kKarlinIterMax * range + 1) * sizeof(double);
+  auto fast = karlin_kernel<kFastWarps, kFastIter, false>;
+  auto full = karlin_kernel<kFullWarps, kKarlinIterMax, true>;
+  GZB_CUDA(cudaFuncSetAttribute(fast, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fast));
+  GZB_CUDA(cudaFuncSetAttribute(full, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_full));
+  const uint64_t want_fast = (number_queries + kFastWarps - 1) / kFastWarps;
+  const uint64_t most_fast = (uint64_t)sms * 8;
+  fast<<<(unsigned)(want_fast < most_fast ? want_fast : most_fast), kFastWarps * 32, smem_fast,
+         (cudaStream_t)stream>>>(a, d_codes, d_offsets, d_lengths, number_queries, d_cutoffs,
+                                 d_triggers, d_karlin);
+  GZB_CUDA(cudaGetLastError());
+  const uint64_t want_full = (number_queries + kFullWarps - 1) / kFullWarps;
+  const uint64_t most_full = (uint64_t)sms * 4;
+  full<<<(unsigned)(want_full < most_full ? want_full : most_full), kFullWarps * 32, smem_full,
+         (cudaStream_t)stream>>>(a, d_codes, d_offsets, d_lengths, number_queries, d_cutoffs,
+                                 d_triggers, d_karlin);
   GZB_CUDA(cudaGetLastError());
   return GZB_OK;
 }

@@ -16,15 +16,19 @@
 //     a body of code 0 for a protein query, src/protein_query.cpp:39-49).
 // Only the 20 standard amino acids count towards compositions.
 //
-// One thread per sequence (a frame of a translated query or the body of a
-// protein query), working in place: masked positions get bit 6 set while
-// the search runs (so later windows still see the letters) and are turned
-// into the unknown code at the end.  The search's left recursion runs on
-// an explicit stack of at most kSegStack frames; deeper nesting (which the
-// trimming rule bounds well below that) is counted in the status word and
-// leaves the sequence unmasked.  All floating point is adds and subtracts
-// of tables computed on the host with the host's log (plus one multiply
-// per window), in the reference's order, so every comparison matches.
+// Two passes over the sequences (frames of translated queries or bodies of
+// protein queries), in place.  Pass 1, one thread per sequence, only
+// computes the window entropies; a sequence with no window at or below the
+// low cut (most of them) is done, the others are marked.  Pass 2, one warp
+// per marked sequence, runs the whole search: masked positions get bit 6
+// set while it runs (so later windows still see the letters) and become the
+// unknown code at the end; the trimming search, the costly part, is split
+// over the lanes.  The left recursion runs on an explicit stack of at most
+// kSegStack frames; deeper nesting (which the trimming rule bounds well
+// below that) is counted in the status word and leaves the sequence
+// unmasked.  All floating point is adds and subtracts of tables computed on
+// the host with the host's log (plus one multiply per window), in the
+// reference's order, so every comparison matches.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -153,20 +157,27 @@ __device__ double seg_probability(const SegArgs &a, const int *state, int total)
   return __dsub_rn(__dadd_rn(ass, perm), __dmul_rn((double)total, a.ln20));
 }
 
-// the least probable sub-window of s[0..n) over lengths n .. max(1, n-100)+1
-__device__ void seg_trim(const SegArgs &a, const uint8_t *s, int n, int *left, int *right) {
-  int best_left = 0, best_right = n - 1;
-  int min_length = n - kSegMaxTrim > 1 ? n - kSegMaxTrim : 1;
+// The least probable sub-window of s[0..n) over lengths n .. max(1, n-100)+1
+// (the reference's first minimum in the order length descending, start
+// ascending).  The whole warp calls it with the same arguments: lane l
+// takes the lengths n - l, n - l - 32, ..., slides each over s with the
+// reference's count updates, and the warp keeps the smallest (probability,
+// order) pair, which is the serial search's first minimum.
+__device__ void seg_trim_warp(const SegArgs &a, const uint8_t *s, int n, int *left, int *right,
+                              int lane) {
+  const int min_length = n - kSegMaxTrim > 1 ? n - kSegMaxTrim : 1;
+  const int lens = n - min_length;  // lengths n, n-1, ..., min_length+1
   double best = 1.0;
+  uint64_t best_at = ~0ull;         // (length rank, start)
   int comp[20], state[21];
-  for (int len = n; len > min_length; --len) {
+  for (int li = lane; li < lens; li += 32) {
+    const int len = n - li;
     seg_state(s, len, comp, state);
     for (int i = 0;; ++i) {
       const double p = seg_probability(a, state, len);
       if (p < best) {
         best = p;
-        best_left = i;
-        best_right = len + i - 1;
+        best_at = ((uint64_t)li << 32) | (uint32_t)i;
       }
       if (i + 1 + len > n) break;
       const int out = seg_class(s[i]), in = seg_class(s[i + len]);
@@ -180,6 +191,20 @@ __device__ void seg_trim(const SegArgs &a, const uint8_t *s, int n, int *left, i
       }
     }
   }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+    const uint64_t oa = __shfl_xor_sync(0xffffffffu, best_at, o);
+    if (ob < best || (ob == best && oa < best_at)) {
+      best = ob;
+      best_at = oa;
+    }
+  }
+  int best_left = 0, best_right = n - 1;
+  if (best_at != ~0ull) {
+    const int len = n - (int)(best_at >> 32);
+    best_left = (int)(uint32_t)best_at;
+    best_right = len + best_left - 1;
+  }
   *left += best_left;
   *right -= n - best_right - 1;
 }
@@ -188,9 +213,11 @@ struct SegFrame {
   int base, n, i, left_limit;
 };
 
-// masks the low-complexity segments of s[0..n) (n >= the window); returns
-// false if the search nested deeper than the stack
-__device__ bool seg_sequence(const SegArgs &a, uint8_t *s, int n) {
+// Masks the low-complexity segments of s[0..n) (n >= the window); every
+// lane of the warp runs the same search on the same data (so its branches
+// agree), the trimming is split over the lanes, and lane 0 writes the
+// masks.  Returns false if the search nested deeper than the stack.
+__device__ bool seg_sequence(const SegArgs &a, uint8_t *s, int n, int lane) {
   SegFrame stack[kSegStack];
   int depth = 0;
   stack[0] = {0, n, 0, 0};
@@ -224,8 +251,11 @@ __device__ bool seg_sequence(const SegArgs &a, uint8_t *s, int n) {
       while (hi <= f.n - 1 && seg_h(a, w, f.n, hi) <= kSegHighCut) ++hi;
       const int right_i = hi - 1;
       int left_end = left_i, right_end = right_i;
-      seg_trim(a, w + left_end, right_end - left_end + 1, &left_end, &right_end);
-      for (int k = left_end; k <= right_end; ++k) s[f.base + k] |= kMaskBit;
+      seg_trim_warp(a, w + left_end, right_end - left_end + 1, &left_end, &right_end, lane);
+      // the mask bit is invisible to seg_class, so the other lanes' reads
+      // see the same letters whichever value they load
+      if (lane == 0)
+        for (int k = left_end; k <= right_end; ++k) s[f.base + k] |= kMaskBit;
       const int next = right_i < right_end ? right_i : right_end;
       const bool child = i < left_end && left_end - left_i >= kSegWindow;
       // the frame resumes after the segment
@@ -248,45 +278,141 @@ __device__ bool seg_sequence(const SegArgs &a, uint8_t *s, int n) {
   return true;
 }
 
-// mode 0: frames of translated queries; mode 1: bodies of protein queries
+// the sequence of unit u: a frame of a translated query (mode 0) or the
+// body of a protein query (mode 1); n = 0 for none
+__device__ __forceinline__ uint8_t *unit_of(uint8_t *codes, const uint64_t *offsets,
+                                            const uint32_t *lengths, uint64_t u, int mode,
+                                            int *n, uint8_t *fallback) {
+  if (mode == 0) {
+    const uint64_t r = u / 6;
+    const int f = (int)(u % 6);
+    const uint32_t len = lengths[r];  // bases of the read
+    *fallback = kUnknownCode;
+    if (len < 3) {
+      *n = 0;
+      return codes;
+    }
+    const uint32_t slot = len / 3 + 1;
+    *n = (int)((len - (uint32_t)(f % 3)) / 3);
+    return codes + offsets[r] + 1 + (uint64_t)f * slot;
+  }
+  *fallback = 0;
+  *n = (int)lengths[u] - 2;
+  return codes + offsets[u] + 1;
+}
+
+// the letters a caller kept out of the compositions (code + 32) back to
+// their codes, masked positions to the unknown code
+__device__ __forceinline__ uint8_t finish_code(uint8_t v) {
+  return (v & kMaskBit) ? kUnknownCode : ((v & 63) >= 32 ? (uint8_t)((v & 63) - 32) : v);
+}
+
+// Pass 1, one thread per sequence: the window entropies only.  A window's
+// entropy needs its letter counts in decreasing order, which here come from
+// counts-of-counts (how many letters occur v times, v = 12 .. 1) updated in
+// O(1) per step, summed in the same order as the sorted counts.  A sequence
+// with no window at or below the low cut is finished here (nothing is
+// masked); one with such a window gets bit 7 on its first code and is left
+// to pass 2.
 __global__ void __launch_bounds__(kSegBlock)
-    seg_kernel(SegArgs a, uint8_t *__restrict__ codes, const uint64_t *__restrict__ offsets,
-               const uint32_t *__restrict__ lengths, uint64_t units, int mode,
-               uint32_t *__restrict__ status) {
+    seg_scan_kernel(SegArgs a, uint8_t *__restrict__ codes, const uint64_t *__restrict__ offsets,
+                    const uint32_t *__restrict__ lengths, uint64_t units, int mode,
+                    uint32_t *__restrict__ status) {
   for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < units;
        u += (uint64_t)gridDim.x * blockDim.x) {
-    uint8_t *s;
     int n;
     uint8_t fallback;
-    if (mode == 0) {
-      const uint64_t r = u / 6;
-      const int f = (int)(u % 6);
-      const uint32_t len = lengths[r];  // bases of the read
-      if (len < 3) continue;
-      const uint32_t slot = len / 3 + 1;
-      s = codes + offsets[r] + 1 + (uint64_t)f * slot;
-      n = (int)((len - (uint32_t)(f % 3)) / 3);
-      fallback = kUnknownCode;
-    } else {
-      s = codes + offsets[u] + 1;
-      n = (int)lengths[u] - 2;
-      fallback = 0;
-    }
+    uint8_t *s = unit_of(codes, offsets, lengths, u, mode, &n, &fallback);
     if (n <= 0) continue;
     if (n < kSegWindow) {
       for (int i = 0; i < n; ++i) s[i] = fallback;
       continue;
     }
-    bool ok = n <= kSegMaxLength;
-    if (ok) ok = seg_sequence(a, s, n);
-    if (!ok) {
+    if (n > kSegMaxLength) {
       if (status) atomicAdd(status, 1u);
-      for (int i = 0; i < n; ++i) s[i] &= (uint8_t)~kMaskBit;
+      for (int i = 0; i < n; ++i) s[i] = finish_code(s[i]);
+      continue;
     }
-    for (int i = 0; i < n; ++i) {
-      const uint8_t v = s[i];
-      s[i] = (v & kMaskBit) ? kUnknownCode : ((v & 63) >= 32 ? (uint8_t)((v & 63) - 32) : v);
+    uint8_t comp[20];
+    uint8_t per[kSegWindow + 1];  // per[v]: letters occurring v times
+    for (int k = 0; k < 20; ++k) comp[k] = 0;
+    for (int v = 0; v <= kSegWindow; ++v) per[v] = 0;
+    int total = 0;
+    bool marked = false, shifted = false;
+    for (int i = 0; i < kSegWindow; ++i) {
+      const int k = seg_class(s[i]);
+      shifted |= (s[i] & 63) >= 32;
+      if (k >= 0) {
+        ++comp[k];
+        ++total;
+      }
     }
+    for (int k = 0; k < 20; ++k) ++per[comp[k]];
+    for (int start = 0;; ++start) {
+      double ent = 0.0;
+      if (total == kSegWindow) {
+        for (int v = kSegWindow; v >= 1; --v)
+          for (int t = 0; t < per[v]; ++t) ent = __dadd_rn(ent, a.entropy12[v]);
+      } else if (total > 0) {
+        const double r = __ddiv_rn(1.0, (double)total);
+        for (int v = total; v >= 1; --v)
+          for (int t = 0; t < per[v]; ++t)
+            ent = __dadd_rn(ent, __dmul_rn((double)v, a.log_ratio[total][v]));
+        ent = __ddiv_rn(__dmul_rn(-ent, r), a.ln2);
+      }
+      if (ent <= kSegLowCut) {
+        marked = true;
+        break;
+      }
+      if (start + kSegWindow >= n) break;
+      const int out = seg_class(s[start]), in = seg_class(s[start + kSegWindow]);
+      shifted |= (s[start + kSegWindow] & 63) >= 32;
+      if (out >= 0) {
+        --per[comp[out]];
+        --comp[out];
+        ++per[comp[out]];
+        --total;
+      }
+      if (in >= 0) {
+        --per[comp[in]];
+        ++comp[in];
+        ++per[comp[in]];
+        ++total;
+      }
+    }
+    if (marked) {
+      s[0] |= 128;
+    } else if (shifted) {
+      for (int i = 0; i < n; ++i) s[i] = finish_code(s[i]);
+    }
+  }
+}
+
+// Pass 2, one warp per sequence pass 1 marked: the whole search
+__global__ void __launch_bounds__(kSegBlock)
+    seg_search_kernel(SegArgs a, uint8_t *__restrict__ codes, const uint64_t *__restrict__ offsets,
+                      const uint32_t *__restrict__ lengths, uint64_t units, int mode,
+                      uint32_t *__restrict__ status) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t u = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; u < units;
+       u += warps) {
+    int n;
+    uint8_t fallback;
+    uint8_t *s = unit_of(codes, offsets, lengths, u, mode, &n, &fallback);
+    if (n < kSegWindow || n > kSegMaxLength) continue;
+    if (!(s[0] & 128)) continue;
+    __syncwarp();
+    if (lane == 0) s[0] &= 127;
+    __syncwarp();
+    const bool ok = seg_sequence(a, s, n, lane);
+    __syncwarp();
+    if (!ok && lane == 0 && status) atomicAdd(status, 1u);
+    for (int i = lane; i < n; i += 32) {
+      const uint8_t v = ok ? s[i] : (uint8_t)(s[i] & ~kMaskBit);
+      s[i] = finish_code(v);
+    }
+    __syncwarp();
   }
 }
 
@@ -339,8 +465,13 @@ int launch_seg(uint8_t *codes, const uint64_t *offsets, const uint32_t *lengths,
   const uint64_t want = (units + kSegBlock - 1) / kSegBlock;
   const uint64_t most = (uint64_t)sms * 16;
   const uint32_t blocks = (uint32_t)(want < most ? want : most);
-  seg_kernel<<<blocks, kSegBlock, 0, stream>>>(g_args, codes, offsets, lengths, units, mode,
-                                                status);
+  seg_scan_kernel<<<blocks, kSegBlock, 0, stream>>>(g_args, codes, offsets, lengths, units,
+                                                     mode, status);
+  GZB_CUDA(cudaGetLastError());
+  const uint64_t want2 = (units + kSegBlock / 32 - 1) / (kSegBlock / 32);
+  const uint64_t most2 = (uint64_t)sms * 8;
+  seg_search_kernel<<<(uint32_t)(want2 < most2 ? want2 : most2), kSegBlock, 0, stream>>>(
+      g_args, codes, offsets, lengths, units, mode, status);
   GZB_CUDA(cudaGetLastError());
   return GZB_OK;
 }

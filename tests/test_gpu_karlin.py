@@ -39,6 +39,10 @@ def _cases(oracle, seed):
         letters = rng.choice(25, size=int(rng.integers(1, 6)), replace=False)
         body = rng.choice(letters, size=int(rng.integers(1, 400)))
         cases.append(np.concatenate([[25], body, [25]]))
+    # low-complexity queries whose K series needs more rounds (poly-S: 31 and
+    # 32 rounds) than the first pass holds, so the second pass finishes them
+    for n in (1000, 5000):
+        cases.append(np.concatenate([[25], np.full(n, 15), [25]]))
     cases.append(np.array([25, 25]))          # an empty query
     cases.append(np.full(50, 24))             # only unknown letters, no delimiters
     return [np.asarray(c, np.uint8) for c in cases]

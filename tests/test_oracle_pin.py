@@ -360,6 +360,8 @@ def test_query_karlin_matches_reference(oracle, reference, params):
         letters = rng.choice(25, size=int(rng.integers(1, 6)), replace=False)
         body = rng.choice(letters, size=int(rng.integers(1, 400))).astype(np.uint8)
         cases.append(np.concatenate([[25], body, [25]]).astype(np.uint8))
+    for n in (1000, 5000):  # poly-S: the K series needs 31-32 rounds
+        cases.append(np.concatenate([[25], np.full(n, 15), [25]]).astype(np.uint8))
     for q in cases:
         lam, k, h = reference.ungapped_karlin(params, q)
         ol, ok, oh, cut, trig = oracle.query_karlin(params, q)
