@@ -1,0 +1,107 @@
+// gzb_hits.cu -- statistics of the final hit table (host code): the values
+// AlignerCommon::WriteOutput (src/aligner_common.h:344-394) prints beside a
+// result's alignment statistics, and the read coordinates of translated
+// queries.
+//
+// The arithmetic keeps the reference's types and order, because the
+// printed values depend on them: the gapped Karlin parameters are floats;
+// the search space's length adjustment is BLAST's fixed-point iteration
+// (Statistics::CalculateLengthAdjustment, src/statistics.cpp:56-122) with
+// ln K taken in float; the E-value multiplies the search space by K in float
+// before the double exponential (Nominal2EValue, :44-48); the normalized
+// score is computed in float (Nominal2Normalized, :23-27).
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+
+#include "ghostz_b200.h"
+#include "gzb_common.h"
+
+extern "C" int gzb_gapped_karlin_parameters(const char *matrix_name, int gap_open,
+                                            int gap_extension, float *lambda, float *k,
+                                            float *h, double *alpha, double *beta) {
+  GZB_CHECK(matrix_name && lambda && k && h && alpha && beta, GZB_ERR_INVALID,
+            "gzb_gapped_karlin_parameters: null argument");
+  // Statistics::CalculateGappedKarlinParameters / CalculateAlphaBeta
+  // (src/statistics.cpp:232-270): the published values for two matrices
+  if (std::strcmp(matrix_name, "BLOSUM62") == 0 && gap_open == 11 && gap_extension == 1) {
+    *lambda = 0.267f;
+    *k = 0.041f;
+    *h = 0.14f;
+    *alpha = 1.9;
+    *beta = -30;
+    return GZB_OK;
+  }
+  if (std::strcmp(matrix_name, "PAM30") == 0 && gap_open == 9 && gap_extension == 1) {
+    *lambda = 0.294f;
+    *k = 0.11f;
+    *h = 0.61f;
+    *alpha = 0.48;
+    *beta = -6;
+    return GZB_OK;
+  }
+  return gzb::set_error(GZB_ERR_INVALID,
+                        "no gapped Karlin parameters for %s with gap open %d, extension %d",
+                        matrix_name, gap_open, gap_extension);
+}
+
+extern "C" uint64_t gzb_search_space(uint64_t query_length, uint64_t db_length,
+                                     uint64_t db_sequences, float lambda, float k, double alpha,
+                                     double beta) {
+  uint64_t adjust = 0;
+  const double m = (double)query_length, n = (double)db_length, N = (double)db_sequences;
+  const double log_k = std::log(k);  // the float logarithm
+  const double a_l = alpha / lambda;
+  const double a = N, mb = m * N + n;
+  const double c = n * m - (m > n ? m : n) / k;
+  if (c >= 0) {
+    double e_min = 0, e_max = 2 * c / (mb + std::sqrt(mb * mb - 4 * a * c)), e_next = 0.0;
+    bool converged = false;
+    for (int i = 0; i < 20; ++i) {
+      const double e = e_next;
+      const double space = (m - e) * (n - N * e);
+      const double e_bar = a_l * (log_k + std::log(space)) + beta;
+      if (e_bar >= e) {
+        e_min = e;
+        if (e_bar - e_min <= 1.0) {
+          converged = true;
+          break;
+        }
+        if (e_min >= e_max) break;
+      } else {
+        e_max = e;
+      }
+      e_next = (e_min <= e_bar && e_bar <= e_max) ? e_bar : (i == 0 ? e_max : (e_min + e_max) / 2);
+    }
+    adjust = (uint64_t)(int)e_min;
+    if (converged) {
+      const double e = std::ceil(e_min);
+      if (e <= e_max && a_l * (log_k + std::log((m - e) * (n - N * e))) + beta > e)
+        adjust = (uint64_t)(int)e;
+    }
+  }
+  return (db_length - db_sequences * adjust) * (query_length - adjust);
+}
+
+extern "C" double gzb_evalue(int32_t score, uint64_t search_space, float lambda, float k) {
+  const float sk = (float)search_space * k;
+  return sk * std::exp(-1.0 * score * lambda);
+}
+
+extern "C" float gzb_bit_score(int32_t score, float lambda, float k) {
+  return ((float)score * lambda - std::log(k)) / (float)std::log(2.0);
+}
+
+extern "C" uint32_t gzb_translated_real_start(uint32_t position, uint32_t dna_length) {
+  const uint32_t base = dna_length / 3 + 1;
+  const uint32_t f = (position - 1) / base;
+  if (f < 3) return ((position % base) - 1) * 3 + f + 1;
+  return dna_length - (((position % base) - 1) * 3 + f - 2) + 1;
+}
+
+extern "C" uint32_t gzb_translated_real_end(uint32_t position, uint32_t dna_length) {
+  const uint32_t base = dna_length / 3 + 1;
+  const uint32_t f = (position - 1) / base;
+  return f < 3 ? gzb_translated_real_start(position, dna_length) + 2
+               : gzb_translated_real_start(position, dna_length) - 2;
+}

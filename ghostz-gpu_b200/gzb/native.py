@@ -56,6 +56,19 @@ def _declare(L):
     L.gzb_cost_model_param_count.argtypes = []
     L.gzb_translated_query_length.restype = C.c_uint64
     L.gzb_translated_query_length.argtypes = [U32]
+    L.gzb_gapped_karlin_parameters.argtypes = [C.c_char_p, C.c_int, C.c_int] + [V] * 5
+    L.gzb_gapped_karlin_parameters.restype = C.c_int
+    L.gzb_search_space.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, C.c_float, C.c_float,
+                                   C.c_double, C.c_double]
+    L.gzb_search_space.restype = C.c_uint64
+    L.gzb_evalue.argtypes = [C.c_int32, C.c_uint64, C.c_float, C.c_float]
+    L.gzb_evalue.restype = C.c_double
+    L.gzb_bit_score.argtypes = [C.c_int32, C.c_float, C.c_float]
+    L.gzb_bit_score.restype = C.c_float
+    L.gzb_translated_real_start.argtypes = [U32, U32]
+    L.gzb_translated_real_start.restype = U32
+    L.gzb_translated_real_end.argtypes = [U32, U32]
+    L.gzb_translated_real_end.restype = U32
     sigs = {
         "gzb_distance_calculator_create": [V],
         "gzb_distance_calculator_destroy": [V],
@@ -779,3 +792,65 @@ def prepare_protein_queries(codes, offsets, lengths, filter=True, matrix=None,
     if int(d_status.item()) != 0:
         raise GzbError(f"SEG left {int(d_status.item())} queries unmasked")
     return d_codes.cpu().numpy(), cut, trig
+
+
+# -- the final hit table --------------------------------------------------------------
+def gapped_karlin_parameters(matrix_name="BLOSUM62", gap_open=11, gap_extension=1):
+    """(lambda, K, H, alpha, beta) of the gapped protein search."""
+    lam, k, h = C.c_float(), C.c_float(), C.c_float()
+    alpha, beta = C.c_double(), C.c_double()
+    check(lib().gzb_gapped_karlin_parameters(matrix_name.encode(), int(gap_open),
+                                             int(gap_extension), C.byref(lam), C.byref(k),
+                                             C.byref(h), C.byref(alpha), C.byref(beta)))
+    return lam.value, k.value, h.value, alpha.value, beta.value
+
+
+def search_space(query_length, db_length, db_sequences, karlin):
+    lam, k, _, alpha, beta = karlin
+    return int(lib().gzb_search_space(int(query_length), int(db_length), int(db_sequences),
+                                      lam, k, alpha, beta))
+
+
+def evalue(score, space, karlin):
+    return float(lib().gzb_evalue(int(score), int(space), karlin[0], karlin[1]))
+
+
+def bit_score(score, karlin):
+    return float(lib().gzb_bit_score(int(score), karlin[0], karlin[1]))
+
+
+def hit_table(results, query_names, subject_names, db_offsets, db_length, db_sequences,
+              query_real_lengths, dna_lengths=None, karlin=None):
+    """The `aln` tabular output (AlignerCommon::WriteOutput,
+    src/aligner_common.h:344-394) of build_alignments() results of one
+    chunk: per result query name, subject name, identity %, alignment
+    length, mismatches, gap openings, query start and end (bases of the read
+    for translated queries), subject start and end, E-value and normalized
+    score, tab separated, numbers as C++ streams print them.  db_offsets:
+    the chunk's first-residue offsets; db_length / db_sequences: residues
+    and sequences of the whole database; query_real_lengths: residues (a
+    read's bases / 3 for a translated query); dna_lengths: the reads' bases
+    for translated queries (None for protein queries)."""
+    if karlin is None:
+        karlin = gapped_karlin_parameters()
+    L = lib()
+    lines = []
+    for qi, rows in enumerate(results):
+        space = search_space(query_real_lengths[qi], db_length, db_sequences, karlin)
+        for r in rows:
+            n_diff = np.float32(int(r["mismatches"]) + int(r["gap_openings"]) +
+                                int(r["gap_extensions"]))
+            identity = (1.0 - float(n_diff / np.float32(int(r["alignment_length"])))) * 100
+            sq, eq = int(r["start_q"]), int(r["end_q"])
+            if dna_lengths is not None:
+                sq = int(L.gzb_translated_real_start(sq, int(dna_lengths[qi])))
+                eq = int(L.gzb_translated_real_end(eq, int(dna_lengths[qi])))
+            first = int(db_offsets[int(r["subject_id"])]) - 1
+            lines.append("\t".join([
+                query_names[qi], subject_names[int(r["subject_id"])], "%g" % identity,
+                str(int(r["alignment_length"])), str(int(r["mismatches"])),
+                str(int(r["gap_openings"])), str(sq), str(eq),
+                str(int(r["start_d"]) - first), str(int(r["end_d"]) - first),
+                "%g" % evalue(int(r["score"]), space, karlin),
+                "%g" % bit_score(int(r["score"]), karlin)]))
+    return lines

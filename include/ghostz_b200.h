@@ -569,6 +569,35 @@ int gzb_seg_protein_queries(uint8_t *d_codes, const uint64_t *d_offsets,
                             const uint32_t *d_lengths, uint32_t number_queries,
                             uint32_t *d_status, void *stream);
 
+
+/* ---- the final hit table (host functions, no device) ----
+ * What AlignerCommon::WriteOutput (src/aligner_common.h:344-394) prints
+ * beside a result's alignment statistics:
+ *  - gzb_gapped_karlin_parameters: lambda, K, H and the length-adjustment
+ *    alpha, beta of the gapped protein search
+ *    (Statistics::CalculateGappedKarlinParameters / CalculateAlphaBeta,
+ *    src/statistics.cpp:232-270; BLOSUM62 11/1 and PAM30 9/1);
+ *  - gzb_search_space: a query's search space with the length adjustment
+ *    (Statistics::CalculateSearchSpace, src/statistics.cpp:50-122);
+ *    query_length is the query's real length (residues; a read's bases / 3
+ *    for a translated query), db_length and db_sequences those of the whole
+ *    database (residues without delimiters, all chunks);
+ *  - gzb_evalue / gzb_bit_score: Statistics::Nominal2EValue and
+ *    Nominal2Normalized (src/statistics.cpp:23-48);
+ *  - gzb_translated_real_start / _end: a translated query position's base
+ *    in the read (TranslatedDnaQuery::GetRealStart / GetRealEnd,
+ *    src/translated_dna_query.h:43-61); protein query positions are their
+ *    own real positions. */
+int gzb_gapped_karlin_parameters(const char *matrix_name, int gap_open, int gap_extension,
+                                 float *lambda, float *k, float *h, double *alpha,
+                                 double *beta);
+uint64_t gzb_search_space(uint64_t query_length, uint64_t db_length, uint64_t db_sequences,
+                          float lambda, float k, double alpha, double beta);
+double gzb_evalue(int32_t score, uint64_t search_space, float lambda, float k);
+float gzb_bit_score(int32_t score, float lambda, float k);
+uint32_t gzb_translated_real_start(uint32_t position, uint32_t dna_length);
+uint32_t gzb_translated_real_end(uint32_t position, uint32_t dna_length);
+
 #ifdef __cplusplus
 }
 #endif

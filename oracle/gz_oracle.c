@@ -1894,3 +1894,74 @@ void gzo_protein_query_seg(const char *letters, uint32_t length, uint8_t delimit
   }
   free(masked);
 }
+
+/* ---- statistics of the final hit table ---- */
+
+uint64_t gzo_search_space(uint64_t query_length, uint64_t db_length, uint64_t db_sequences,
+                          float lambda, float k, double alpha, double beta) {
+  /* the length adjustment: the BLAST fixed point of
+   * ell = alpha/lambda (ln K + ln((m - ell)(n - N ell))) + beta */
+  uint64_t adjust = 0;
+  const double m = (double)query_length, n = (double)db_length, N = (double)db_sequences;
+  const double log_k = logf(k);
+  const double a_l = alpha / lambda;
+  const double a = N, mb = m * N + n;
+  const double c = n * m - (m > n ? m : n) / k;
+  if (c >= 0) {
+    double e, e_min = 0, e_max = 2 * c / (mb + sqrt(mb * mb - 4 * a * c)), ss, e_next = 0.0;
+    int converged = 0;
+    for (int i = 0; i < 20; ++i) {
+      e = e_next;
+      ss = (m - e) * (n - N * e);
+      const double e_bar = a_l * (log_k + log(ss)) + beta;
+      if (e_bar >= e) {
+        e_min = e;
+        if (e_bar - e_min <= 1.0) {
+          converged = 1;
+          break;
+        }
+        if (e_min >= e_max) break;
+      } else {
+        e_max = e;
+      }
+      if (e_min <= e_bar && e_bar <= e_max)
+        e_next = e_bar;
+      else
+        e_next = i == 0 ? e_max : (e_min + e_max) / 2;
+    }
+    adjust = (uint64_t)(int)e_min;
+    if (converged) {
+      e = ceil(e_min);
+      if (e <= e_max) {
+        ss = (m - e) * (n - N * e);
+        if (a_l * (log_k + log(ss)) + beta > e) adjust = (uint64_t)(int)e;
+      }
+    }
+  }
+  const uint64_t effective_db = db_length - db_sequences * adjust;
+  return effective_db * (query_length - adjust);
+}
+
+double gzo_evalue(int32_t score, uint64_t search_space, float lambda, float k) {
+  /* the search space times K is a float product */
+  const float sk = (float)search_space * k;
+  return sk * exp(-1.0 * score * lambda);
+}
+
+float gzo_bit_score(int32_t score, float lambda, float k) {
+  return ((float)score * lambda - logf(k)) / (float)log(2.0);
+}
+
+uint32_t gzo_translated_real_start(uint32_t position, uint32_t dna_length) {
+  const uint32_t base = dna_length / 3 + 1;
+  const uint32_t f = (position - 1) / base;
+  if (f < 3) return ((position % base) - 1) * 3 + f + 1;
+  return dna_length - (((position % base) - 1) * 3 + f - 2) + 1;
+}
+
+uint32_t gzo_translated_real_end(uint32_t position, uint32_t dna_length) {
+  const uint32_t base = dna_length / 3 + 1;
+  const uint32_t f = (position - 1) / base;
+  return f < 3 ? gzo_translated_real_start(position, dna_length) + 2
+               : gzo_translated_real_start(position, dna_length) - 2;
+}

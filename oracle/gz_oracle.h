@@ -229,6 +229,23 @@ double gzo_ln_factorial6(uint32_t n);
 void gzo_protein_query_seg(const char *letters, uint32_t length, uint8_t delimiter,
                            uint8_t *out);
 
+
+/* Statistics of the final hit table (AlignerCommon::WriteOutput,
+ * src/aligner_common.h:344-394): the search space of a query
+ * (Statistics::CalculateSearchSpace with the protein length adjustment,
+ * src/statistics.cpp:50-122), E-value (Nominal2EValue, :44-48) and
+ * normalized score (Nominal2Normalized, :23-27) under gapped Karlin
+ * parameters lambda, k and length-adjustment alpha, beta. */
+uint64_t gzo_search_space(uint64_t query_length, uint64_t db_length, uint64_t db_sequences,
+                          float lambda, float k, double alpha, double beta);
+double gzo_evalue(int32_t score, uint64_t search_space, float lambda, float k);
+float gzo_bit_score(int32_t score, float lambda, float k);
+/* Read coordinates of a translated query position
+ * (TranslatedDnaQuery::GetRealStart / GetRealEnd,
+ * src/translated_dna_query.h:43-61). */
+uint32_t gzo_translated_real_start(uint32_t position, uint32_t dna_length);
+uint32_t gzo_translated_real_end(uint32_t position, uint32_t dna_length);
+
 #ifdef __cplusplus
 }
 #endif

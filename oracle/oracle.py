@@ -106,6 +106,17 @@ class Oracle:
         L.gzo_translate_query_seg.argtypes = [C.c_char_p, C.c_uint32, C.c_uint8, u8p]
         L.gzo_translate_query_seg.restype = C.c_uint32
         L.gzo_ln_factorial6.argtypes = [C.c_uint32]
+        L.gzo_search_space.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, C.c_float, C.c_float,
+                                       C.c_double, C.c_double]
+        L.gzo_search_space.restype = C.c_uint64
+        L.gzo_evalue.argtypes = [C.c_int32, C.c_uint64, C.c_float, C.c_float]
+        L.gzo_evalue.restype = C.c_double
+        L.gzo_bit_score.argtypes = [C.c_int32, C.c_float, C.c_float]
+        L.gzo_bit_score.restype = C.c_float
+        L.gzo_translated_real_start.argtypes = [C.c_uint32, C.c_uint32]
+        L.gzo_translated_real_start.restype = C.c_uint32
+        L.gzo_translated_real_end.argtypes = [C.c_uint32, C.c_uint32]
+        L.gzo_translated_real_end.restype = C.c_uint32
         L.gzo_protein_query_seg.argtypes = [C.c_char_p, C.c_uint32, C.c_uint8, u8p]
         L.gzo_ln_factorial6.restype = C.c_double
         L.gzo_translated_length.argtypes = [C.c_uint32]
@@ -214,6 +225,19 @@ class Oracle:
         out = np.zeros(len(letters) + 2, np.uint8)
         self.L.gzo_protein_query_seg(letters, len(letters), int(delimiter), _p(out, u8p))
         return out
+
+    # BLOSUM62 with gaps 11/1: the gapped parameters WriteOutput uses
+    GAPPED = (0.267, 0.041, 1.9, -30.0)
+
+    def hit_statistics(self, query_length, db_length, db_sequences, score, gapped=GAPPED):
+        """(search space, E-value, normalized score) of a result."""
+        lam, k, alpha, beta = gapped
+        ss = self.L.gzo_search_space(query_length, db_length, db_sequences, lam, k, alpha, beta)
+        return ss, self.L.gzo_evalue(score, ss, lam, k), self.L.gzo_bit_score(score, lam, k)
+
+    def translated_real(self, position, dna_length):
+        return (self.L.gzo_translated_real_start(position, dna_length),
+                self.L.gzo_translated_real_end(position, dna_length))
 
     def translate_query_seg(self, dna, delimiter):
         """translate_query with the SEG filter on."""
@@ -356,6 +380,11 @@ class Reference:
         L.gzr_translate_query_seg.argtypes = [C.c_void_p, C.c_char_p, C.c_uint32, u8p,
                                               C.c_uint32]
         L.gzr_translate_query_seg.restype = C.c_uint32
+        L.gzr_hit_statistics.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64,
+                                         C.c_int32, C.POINTER(C.c_uint64),
+                                         C.POINTER(C.c_double), C.POINTER(C.c_float)]
+        L.gzr_translated_real.argtypes = [C.c_void_p, C.c_char_p, C.c_uint32, C.c_uint32,
+                                          u32p, u32p]
         L.gzr_protein_query_seg.argtypes = [C.c_void_p, C.c_char_p, C.c_uint32, u8p,
                                             C.c_uint32, C.POINTER(C.c_float),
                                             C.POINTER(C.c_float)]
@@ -495,3 +524,18 @@ class Reference:
                                          len(out), C.byref(lam), C.byref(k))
         assert n == len(out)
         return out, lam.value, k.value
+
+    def hit_statistics(self, params, query_length, db_length, db_sequences, score):
+        pr = _Params(params)
+        ss, ev, bs = C.c_uint64(), C.c_double(), C.c_float()
+        rc = self.L.gzr_hit_statistics(pr.ptr, query_length, db_length, db_sequences, score,
+                                       C.byref(ss), C.byref(ev), C.byref(bs))
+        assert rc == 0
+        return ss.value, ev.value, bs.value
+
+    def translated_real(self, params, dna, position):
+        pr = _Params(params)
+        dna = bytes(dna)
+        st, en = np.zeros(1, np.uint32), np.zeros(1, np.uint32)
+        self.L.gzr_translated_real(pr.ptr, dna, len(dna), position, _p(st, u32p), _p(en, u32p))
+        return int(st[0]), int(en[0])

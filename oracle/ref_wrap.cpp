@@ -315,4 +315,41 @@ uint32_t gzr_protein_query_seg(const gzo_params *p, const char *letters, uint32_
   return n;
 }
 
+
+/* The hit table's statistics as AlignerCommon::WriteOutput takes them
+ * (src/aligner_common.h:344-394), for the protein aligner with the score
+ * matrix and gaps of p (gapped Karlin parameters and alpha, beta from
+ * src/statistics.cpp:232-270). */
+int gzr_hit_statistics(const gzo_params *p, uint64_t query_length, uint64_t db_length,
+                       uint64_t db_sequences, int32_t score, uint64_t *search_space,
+                       double *evalue, float *bit_score) {
+  ProteinType t;
+  Statistics s(t);
+  ScoreMatrix m = make_matrix(p);
+  Statistics::KarlinParameters kp;
+  double alpha = 0, beta = 0;
+  if (!s.CalculateGappedKarlinParameters(m, p->gap_open, p->gap_extension, &kp)) return 1;
+  if (!s.CalculateAlphaBeta(m, p->gap_open, p->gap_extension, &alpha, &beta)) return 1;
+  *search_space = s.CalculateSearchSpace(query_length, db_length, db_sequences, kp, alpha, beta);
+  *evalue = Statistics::Nominal2EValue(score, *search_space, kp);
+  *bit_score = Statistics::Nominal2Normalized(score, kp);
+  return 0;
+}
+
+/* TranslatedDnaQuery::GetRealStart / GetRealEnd of a read's query. */
+void gzr_translated_real(const gzo_params *p, const char *dna, uint32_t length,
+                         uint32_t position, uint32_t *start, uint32_t *end) {
+  Sequence seq("read", std::string(dna, length));
+  Translator translator;
+  SequenceNoFilter filter;
+  ScoreMatrix m = make_matrix(p);
+  ProteinType t;
+  Statistics s(t);
+  Statistics::KarlinParameters ideal;
+  s.CalculateUngappedIdealKarlinParameters(m, &ideal);
+  TranslatedDnaQuery q(seq, p->delimiter, translator, &filter, m, ideal);
+  *start = q.GetRealStart(position);
+  *end = q.GetRealEnd(position);
+}
+
 } /* extern "C" */

@@ -131,3 +131,31 @@ def test_karlin_cutoffs_validate_without_device():
     assert f(None, None, None, 0, N.hptr(wide), 25, 7.0, 22.0, None, None, None, None) == 4
     assert f(None, None, None, 1, N.hptr(np.ascontiguousarray(m, np.int32)), 25, 7.0, 22.0,
              None, None, None, None) == 1
+
+
+def test_hit_statistics_without_device(oracle):
+    """The library's hit-table statistics (host code) equal the oracle's."""
+    import numpy as np
+    from gzb import native as N
+    karlin = N.gapped_karlin_parameters()
+    assert np.float32(karlin[0]) == np.float32(0.267) and np.float32(karlin[1]) == np.float32(0.041)
+    rng = np.random.default_rng(82)
+    for _ in range(300):
+        ql, dl = int(rng.integers(1, 10000)), int(rng.integers(10, 10**10))
+        ns = int(rng.integers(1, min(dl, 10**7)))
+        score = int(rng.integers(0, 3000))
+        space = N.search_space(ql, dl, ns, karlin)
+        exp = oracle.hit_statistics(ql, dl, ns, score)
+        assert space == exp[0]
+        assert N.evalue(score, space, karlin) == exp[1]
+        assert np.float32(N.bit_score(score, karlin)) == np.float32(exp[2])
+    for n in (3, 75, 150, 1000):
+        slot = n // 3 + 1
+        for pos in range(1, 6 * slot):
+            if pos % slot == 0:
+                continue
+            assert (N.lib().gzb_translated_real_start(pos, n),
+                    N.lib().gzb_translated_real_end(pos, n)) == oracle.translated_real(pos, n)
+    import pytest
+    with pytest.raises(N.GzbError):
+        N.gapped_karlin_parameters("BLOSUM62", 10, 1)

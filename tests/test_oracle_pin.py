@@ -459,3 +459,34 @@ def test_protein_query_with_seg_matches_reference(oracle, reference, params):
         assert np.array_equal(m, r), (t, n, s)
         lam, k, _, _, _ = oracle.query_karlin(params, m)
         assert (np.float32(lam), np.float32(k)) == (np.float32(rl), np.float32(rk)), (t, n)
+
+
+# --- the final hit table ----------------------------------------------------------
+def test_hit_statistics_match_reference(oracle, reference, params):
+    # Statistics::CalculateSearchSpace / Nominal2EValue / Nominal2Normalized
+    # (src/statistics.cpp:23-122) as AlignerCommon::WriteOutput uses them
+    rng = np.random.default_rng(80)
+    cases = [(300, 719856279, 2000000), (50, 5762314777, 16000000), (1, 1000, 10),
+             (8000, 71906369, 200000), (12, 36, 3), (150, 1000000, 1)]
+    cases += [(int(rng.integers(1, 10000)), int(rng.integers(1, 10**10)),
+               int(rng.integers(1, 10**7))) for _ in range(200)]
+    for ql, dl, ns in cases:
+        if ns > dl:
+            ns = dl
+        for score in (0, 1, 38, 57, int(rng.integers(20, 3000))):
+            exp = reference.hit_statistics(params, ql, dl, ns, score)
+            got = oracle.hit_statistics(ql, dl, ns, score)
+            assert got[0] == exp[0] and got[1] == exp[1], (ql, dl, ns, score, got, exp)
+            assert np.float32(got[2]) == np.float32(exp[2])
+
+
+def test_translated_coordinates_match_reference(oracle, reference, params):
+    # TranslatedDnaQuery::GetRealStart / GetRealEnd (src/translated_dna_query.h:43-61)
+    rng = np.random.default_rng(81)
+    for n in (3, 4, 5, 75, 150, 151, 152, 1000):
+        read = bytes(np.frombuffer(b"ACGT", np.uint8)[rng.integers(0, 4, n)])
+        slot = n // 3 + 1
+        for f in range(6):
+            for j in range(0, slot - 1):
+                pos = 1 + f * slot + j
+                assert oracle.translated_real(pos, n) == reference.translated_real(params, read, pos)
