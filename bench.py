@@ -335,11 +335,12 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def train_cost_model(params, local_rank, train_sets):
+def train_cost_model(params, local_rank, train_sets, reads=False):
     """Cost model of the learned schedule (untimed set-up): pairs logged by
     the plain path on config-1-shaped runs (20,000 proteins, 1,000 queries x
-    train_sets query seeds), trained on the GPU by the engine's own kernels.
-    Returns (parameters, final loss, pairs)."""
+    train_sets query seeds; with reads=True, 5,000 150-nt reads drawn from
+    the same proteins and prepared on the GPU per set), trained on the GPU by
+    the engine's own kernels.  Returns (parameters, final loss, pairs)."""
     from gzb import native as N
     from gzb import workload as W
     tdb = W.make_database(20000, 101)
@@ -348,7 +349,12 @@ def train_cost_model(params, local_rank, train_sets):
     trainer.set_database(tdb)
     trainer.set_logging(True, 1 << 23)
     for k in range(train_sets):
-        trainer.set_queries(W.make_queries(tdb, 1000, 102 + k))
+        if reads:
+            r = W.make_reads(tdb, 5000, 102 + k)
+            codes, offs, lens, cut, trig = N.prepare_translated_queries(r.dna, r.offsets)
+            trainer.set_queries(W.translated_queries(codes, offs, lens, cutoffs=(cut, trig)))
+        else:
+            trainer.set_queries(W.make_queries(tdb, 1000, 102 + k))
         trainer.presearch(N.SCHEDULE_PLAIN)
     model, loss = trainer.train_cost_model(epochs=12, batch=4096, lr=3e-3, seed=7)
     pairs = len(trainer.get_log()[1])
@@ -692,7 +698,9 @@ def main():
     t = time.time()
     train_pairs, train_loss = 0, None
     if args.schedule == "batched":
-        model, train_loss, train_pairs = train_cost_model(params, local_rank, args.train_sets)
+        model, train_loss, train_pairs = train_cost_model(
+            params, local_rank, args.train_sets,
+            reads="read_length" in WORKLOADS[args.workload][4])
         eng.set_cost_model(model)
         eng.set_queries(q)
     train_s = time.time() - t

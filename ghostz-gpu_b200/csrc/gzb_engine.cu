@@ -690,6 +690,48 @@ __device__ __forceinline__ uint32_t subject_of(const uint32_t *off, uint32_t nse
                                                uint32_t db_len, uint32_t pos);
 
 // Extension list of the chained hits: one warp per query, lanes over its
+// For every position p of a query in the concatenated buffer: the nearest
+// delimiter at or before p (prev) and at or after p (next), within the
+// query (its first and last codes are delimiters).  One warp per query,
+// 32 positions per step with a running maximum (minimum) carried across
+// steps.  The gapped DP cannot cross a delimiter, so these bound how far an
+// extension can run along the query: for a protein query that is its end,
+// for a translated query the end of the hit's frame.
+__global__ void delim_dist_kernel(const uint8_t *q, const uint32_t *offsets,
+                                  const uint32_t *lengths, uint32_t nq, int delim, uint32_t *prev,
+                                  uint32_t *next) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t qi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; qi < nq; qi += warps) {
+    const uint32_t off = offsets[qi], len = lengths[qi];
+    uint32_t carry = off;  // the leading delimiter
+    for (uint32_t b = 0; b < len; b += 32) {
+      const uint32_t p = off + b + lane;
+      uint32_t v = (b + lane < len && q[p] == delim) ? p : 0;
+      v = max(v, carry);
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v = max(v, u);
+      }
+      if (b + lane < len) prev[p] = v;
+      carry = __shfl_sync(0xffffffffu, v, 31);
+    }
+    carry = off + len - 1;  // the closing delimiter
+    for (uint32_t b = 0; b < len; b += 32) {
+      const uint32_t i = len - 1 - b - lane;  // positions from the end
+      const uint32_t p = off + i;
+      uint32_t v = (b + lane < len && q[p] == delim) ? p : 0xFFFFFFFFu;
+      v = min(v, carry);
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v = min(v, u);
+      }
+      if (b + lane < len) next[p] = v;
+      carry = __shfl_sync(0xffffffffu, v, 31);
+    }
+  }
+}
+
 // kept hits (database order).  Reverse extension of hit h at h, forward at
 // n_surv + h; neighbours[h] counts the query's kept hits within 256
 // database residues of h (a cost-model feature).
@@ -700,7 +742,8 @@ __global__ void build_ext_kernel(const uint64_t *hits, const uint64_t *begin,
                                  int qbits, int dbits, uint64_t n_surv, uint32_t *eq,
                                  uint32_t *ed, uint8_t *dir, uint32_t *elen0,
                                  uint32_t *elen1, uint32_t *eqid, uint32_t *neighbours,
-                                 const uint64_t *n_dev) {
+                                 const uint64_t *n_dev, const uint32_t *qprev,
+                                 const uint32_t *qnext) {
   if (n_dev) n_surv = *n_dev;
   const uint64_t qmask = (1ull << qbits) - 1, dmask = (1ull << dbits) - 1;
   constexpr uint32_t kReach = 256;  // database residues either side
@@ -738,13 +781,13 @@ __global__ void build_ext_kernel(const uint64_t *hits, const uint64_t *begin,
       eq[o + k] = qoff + hq - 1;
       ed[o + k] = hd - 1;
       dir[o + k] = 1;
-      elen0[o + k] = hq - 1;
+      elen0[o + k] = qprev ? (qoff + hq - 1) - qprev[qoff + hq - 1] : hq - 1;
       elen1[o + k] = hd - s0;
       eqid[o + k] = qi;
       eq[n_surv + o + k] = qoff + hq;
       ed[n_surv + o + k] = hd;
       dir[n_surv + o + k] = 0;
-      elen0[n_surv + o + k] = qlen - 1 - hq;
+      elen0[n_surv + o + k] = qnext ? qnext[qoff + hq] - (qoff + hq) : qlen - 1 - hq;
       elen1[n_surv + o + k] = s1 - hd;
       eqid[n_surv + o + k] = qi;
     }
@@ -1076,6 +1119,7 @@ struct gzb_engine {
   bool have_db = false;
   // queries
   DBuf q_buf, q_offsets, q_lengths, q_cut, q_trig;
+  DBuf q_prev, q_next;  // nearest delimiters of every query position
   uint64_t q_len = 0;
   uint32_t nq = 0;
   uint32_t max_qlen = 0;
@@ -1320,6 +1364,7 @@ extern "C" int gzb_engine_destroy(gzb_engine *e) {
   for (auto &b : e->index_bufs) b.release();
   for (auto &b : e->list_bufs) b.release();
   DBuf *all[] = {&e->matrix32, &e->db_buf, &e->db_offsets, &e->q_buf, &e->q_offsets,
+                 &e->q_prev, &e->q_next,
                  &e->q_lengths, &e->q_cut, &e->q_trig, &e->results, &e->counts,
                  &e->tmp, &e->hits, &e->hits_alt, &e->mwork, &e->mwork_alt,
                  &e->begin, &e->kept, &e->surv_off, &e->slots, &e->eq, &e->ed, &e->edir,
@@ -1954,6 +1999,12 @@ gzb_engine *e, const uint8_t *codes, uint64_t length,
   GZB_TRY(upload(e->q_lengths, lengths, number_queries, s));
   GZB_TRY(upload(e->q_cut, cutoffs, number_queries, s));
   GZB_TRY(upload(e->q_trig, triggers, number_queries, s));
+  GZB_TRY(e->q_prev.ensure(4 * (length + 1)));
+  GZB_TRY(e->q_next.ensure(4 * (length + 1)));
+  delim_dist_kernel<<<grid1((uint64_t)number_queries * 32, 256), 256, 0, s>>>(
+      e->q_buf.as<uint8_t>() + kPad, e->q_offsets.as<uint32_t>(), e->q_lengths.as<uint32_t>(),
+      number_queries, e->params.delimiter, e->q_prev.as<uint32_t>(), e->q_next.as<uint32_t>());
+  GZB_CUDA(cudaGetLastError());
   std::vector<DBuf> &B = e->list_bufs;
   DBuf &keys = B[0], &alt = B[1];
   GZB_TRY(keys.ensure(8 * (length + 1)));
@@ -2201,7 +2252,7 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
         e->q_lengths.as<uint32_t>(), e->db_offsets.as<uint32_t>(), e->nseq, (uint32_t)e->db_len,
         qbits, dbits, n_surv, e->eq.as<uint32_t>(), e->ed.as<uint32_t>(), e->edir.as<uint8_t>(),
         e->elen0.as<uint32_t>(), e->elen1.as<uint32_t>(), e->eqid.as<uint32_t>(),
-        e->enb.as<uint32_t>(), nullptr);
+        e->enb.as<uint32_t>(), nullptr, e->q_prev.as<uint32_t>(), e->q_next.as<uint32_t>());
     GZB_CUDA(cudaGetLastError());
     ++launches;
     GZB_CUDA(cudaMemsetAsync(e->gcells, 0, 8, s));
@@ -2566,7 +2617,7 @@ int graph_body(gzb_engine *e, int schedule, const GappedTile &tile, bool learned
       e->q_lengths.as<uint32_t>(), e->db_offsets.as<uint32_t>(), e->nseq, (uint32_t)e->db_len,
       qbits, dbits, c.hits, e->eq.as<uint32_t>(), e->ed.as<uint32_t>(), e->edir.as<uint8_t>(),
       e->elen0.as<uint32_t>(), e->elen1.as<uint32_t>(), e->eqid.as<uint32_t>(),
-      e->enb.as<uint32_t>(), plan + 2);
+      e->enb.as<uint32_t>(), plan + 2, e->q_prev.as<uint32_t>(), e->q_next.as<uint32_t>());
   GZB_CUDA(cudaGetLastError());
   ++launches;
   GZB_CUDA(cudaMemsetAsync(e->gcells, 0, 8, s));
@@ -2644,7 +2695,7 @@ uint64_t graph_key(const gzb_engine *e, int schedule, const GappedTile &tile, bo
                         &e->ed, &e->edir, &e->escore, &e->elen0, &e->elen1, &e->eqid, &e->enb,
                         &e->merge_scratch, &e->heap, &e->ctr, &e->plan, &e->list_bufs[14],
                         &e->efeat, &e->epred, &e->okeys, &e->okeys2, &e->oidx, &e->oidx2,
-                        &e->model_d};
+                        &e->model_d, &e->q_prev, &e->q_next};
   for (const DBuf *b : bufs) {
     h = fnv_mix(h, &b->p, sizeof(b->p));
     h = fnv_mix(h, &b->bytes, sizeof(b->bytes));
