@@ -139,57 +139,91 @@ __device__ __forceinline__ float bf16_round(float v) {
 
 // BF16 inference: parameters, inputs and both hidden layers rounded to
 // bf16, products accumulated in fp32.  The parameters sit in shared memory
-// as the fp32 values of their bf16 roundings (exact), read as float4
-// broadcasts, one sample per thread.
-__global__ void __launch_bounds__(256)
+// as the fp32 values of their bf16 roundings (exact), the second layer's
+// weights also transposed, and are read as float4 broadcasts.  Each thread
+// takes two samples (s and s + T, T threads in the grid), so every weight
+// read feeds both.  The first layer's units are taken one at a time and
+// each is added at once into all 32 second-layer sums (kept in registers),
+// which adds the same products in the same order (unit by unit) as summing
+// each second-layer unit over the first layer's.
+__global__ void __launch_bounds__(256, 2)
 mlp_predict_kernel(const float *__restrict__ params, const float *__restrict__ X, uint32_t n,
                    float *__restrict__ out, const uint64_t *n_dev) {
   if (n_dev) n = (uint32_t)*n_dev;
   __shared__ __align__(16) float P[(kParams + 3) & ~3];
+  __shared__ __align__(16) float W2T[kHid * kHid];  // W2T[i][j] = W2[j][i]
   for (int i = threadIdx.x; i < kParams; i += blockDim.x) P[i] = bf16_round(params[i]);
+  for (int t = threadIdx.x; t < kHid * kHid; t += blockDim.x) {
+    const int i = t / kHid, j = t % kHid;
+    W2T[t] = bf16_round(params[kOffW2 + j * kHid + i]);
+  }
   __syncthreads();
   const float4 *P4 = reinterpret_cast<const float4 *>(P);
+  const float4 *T4 = reinterpret_cast<const float4 *>(W2T);
   static_assert(kOffW1 % 4 == 0 && kOffW2 % 4 == 0 && kFeat % 4 == 0 && kHid % 4 == 0,
                 "float4 rows");
-  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
-    float x[kFeat], h1[kHid];
-    const float4 *x4 = reinterpret_cast<const float4 *>(X + (size_t)s * kFeat);
+  const uint32_t T = gridDim.x * blockDim.x;
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += 2 * T) {
+    const uint32_t s1 = s + T;
+    const bool two = s1 < n;
+    float x0[kFeat], x1[kFeat], a0[kHid], a1[kHid];
+    const float4 *u4 = reinterpret_cast<const float4 *>(X + (size_t)s * kFeat);
+    const float4 *v4 = reinterpret_cast<const float4 *>(X + (size_t)(two ? s1 : s) * kFeat);
 #pragma unroll
     for (int k = 0; k < kFeat / 4; ++k) {
-      const float4 v = x4[k];
-      x[4 * k] = bf16_round(v.x);
-      x[4 * k + 1] = bf16_round(v.y);
-      x[4 * k + 2] = bf16_round(v.z);
-      x[4 * k + 3] = bf16_round(v.w);
+      const float4 u = u4[k], v = v4[k];
+      x0[4 * k] = bf16_round(u.x);
+      x0[4 * k + 1] = bf16_round(u.y);
+      x0[4 * k + 2] = bf16_round(u.z);
+      x0[4 * k + 3] = bf16_round(u.w);
+      x1[4 * k] = bf16_round(v.x);
+      x1[4 * k + 1] = bf16_round(v.y);
+      x1[4 * k + 2] = bf16_round(v.z);
+      x1[4 * k + 3] = bf16_round(v.w);
     }
 #pragma unroll
-    for (int j = 0; j < kHid; ++j) {
-      float acc = P[kOffB1 + j];
+    for (int j = 0; j < kHid; ++j) a0[j] = a1[j] = P[kOffB2 + j];
+#pragma unroll 1
+    for (int i = 0; i < kHid; ++i) {
+      // first-layer unit i of both samples
+      float h0 = P[kOffB1 + i], h1 = h0;
 #pragma unroll
       for (int k = 0; k < kFeat / 4; ++k) {
-        const float4 w = P4[(kOffW1 + j * kFeat) / 4 + k];
-        acc = fmaf(w.x, x[4 * k], acc);
-        acc = fmaf(w.y, x[4 * k + 1], acc);
-        acc = fmaf(w.z, x[4 * k + 2], acc);
-        acc = fmaf(w.w, x[4 * k + 3], acc);
+        const float4 w = P4[(kOffW1 + i * kFeat) / 4 + k];
+        h0 = fmaf(w.x, x0[4 * k], h0);
+        h1 = fmaf(w.x, x1[4 * k], h1);
+        h0 = fmaf(w.y, x0[4 * k + 1], h0);
+        h1 = fmaf(w.y, x1[4 * k + 1], h1);
+        h0 = fmaf(w.z, x0[4 * k + 2], h0);
+        h1 = fmaf(w.z, x1[4 * k + 2], h1);
+        h0 = fmaf(w.w, x0[4 * k + 3], h0);
+        h1 = fmaf(w.w, x1[4 * k + 3], h1);
       }
-      h1[j] = bf16_round(acc > 0.f ? acc : 0.f);
-    }
-    float y = P[kOffB3];
-#pragma unroll 4
-    for (int j = 0; j < kHid; ++j) {
-      float acc = P[kOffB2 + j];
+      h0 = bf16_round(h0 > 0.f ? h0 : 0.f);
+      h1 = bf16_round(h1 > 0.f ? h1 : 0.f);
+      // ... added into every second-layer sum
 #pragma unroll
-      for (int k = 0; k < kHid / 4; ++k) {
-        const float4 w = P4[(kOffW2 + j * kHid) / 4 + k];
-        acc = fmaf(w.x, h1[4 * k], acc);
-        acc = fmaf(w.y, h1[4 * k + 1], acc);
-        acc = fmaf(w.z, h1[4 * k + 2], acc);
-        acc = fmaf(w.w, h1[4 * k + 3], acc);
+      for (int q = 0; q < kHid / 4; ++q) {
+        const float4 w = T4[(i * kHid) / 4 + q];
+        a0[4 * q] = fmaf(w.x, h0, a0[4 * q]);
+        a1[4 * q] = fmaf(w.x, h1, a1[4 * q]);
+        a0[4 * q + 1] = fmaf(w.y, h0, a0[4 * q + 1]);
+        a1[4 * q + 1] = fmaf(w.y, h1, a1[4 * q + 1]);
+        a0[4 * q + 2] = fmaf(w.z, h0, a0[4 * q + 2]);
+        a1[4 * q + 2] = fmaf(w.z, h1, a1[4 * q + 2]);
+        a0[4 * q + 3] = fmaf(w.w, h0, a0[4 * q + 3]);
+        a1[4 * q + 3] = fmaf(w.w, h1, a1[4 * q + 3]);
       }
-      y = fmaf(P[kOffW3 + j], bf16_round(acc > 0.f ? acc : 0.f), y);
     }
-    out[s] = y;
+    float y0 = P[kOffB3], y1 = y0;
+#pragma unroll
+    for (int j = 0; j < kHid; ++j) {
+      const float w3 = P[kOffW3 + j];
+      y0 = fmaf(w3, bf16_round(a0[j] > 0.f ? a0[j] : 0.f), y0);
+      y1 = fmaf(w3, bf16_round(a1[j] > 0.f ? a1[j] : 0.f), y1);
+    }
+    out[s] = y0;
+    if (two) out[s1] = y1;
   }
 }
 
