@@ -821,7 +821,8 @@ __global__ void ext_features_kernel(const uint8_t *__restrict__ q, const uint8_t
   }
 }
 
-// sort key: larger predicted cost first; ties keep extension order
+// sort key: larger predicted cost first; ties keep extension order (the
+// sort is stable and reads the low 16 bits)
 // With n_dev the count is read on the device and entries n .. cap get the
 // largest key (they sort last).
 __global__ void cost_keys_kernel(const float *pred, const uint32_t *true_cells, uint64_t n,
@@ -841,8 +842,9 @@ __global__ void cost_keys_kernel(const float *pred, const uint32_t *true_cells, 
     float c = pred ? pred[i] : log2f(1.0f + (float)true_cells[i]);
     if (!(c > -64.0f)) c = -64.0f;
     if (c > 64.0f) c = 64.0f;
-    const uint32_t u = (uint32_t)((c + 64.0f) * 16777216.0f / 128.0f * 255.0f);
-    keys[i] = 0xFFFFFFFFu - u;
+    // 16-bit keys (1/512 of a log2 unit): the order sort takes two passes
+    const uint32_t u = min((uint32_t)((c + 64.0f) * 512.0f), 0xFFFFu);
+    keys[i] = 0xFFFFu - u;
     vals[i] = (uint32_t)i;
   }
 }
@@ -2303,9 +2305,9 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
       cub::DoubleBuffer<uint32_t> kb(e->okeys.as<uint32_t>(), e->okeys2.as<uint32_t>());
       cub::DoubleBuffer<uint32_t> vb(e->oidx.as<uint32_t>(), e->oidx2.as<uint32_t>());
       size_t tb = 0;
-      GZB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb, (int64_t)next, 0, 32, s));
+      GZB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb, (int64_t)next, 0, 16, s));
       GZB_TRY(e->tmp.ensure(tb));
-      GZB_CUDA(cub::DeviceRadixSort::SortPairs(e->tmp.p, tb, kb, vb, (int64_t)next, 0, 32, s));
+      GZB_CUDA(cub::DeviceRadixSort::SortPairs(e->tmp.p, tb, kb, vb, (int64_t)next, 0, 16, s));
       order = vb.Current();
     }
     uint32_t fb = 0;
@@ -2452,7 +2454,7 @@ int graph_sort_bytes(const gzb_engine *e, const GraphCaps &c, int hit_bits, int 
                      size_t *bytes) {
   size_t a = 0, b = 0, d = 0, f = 0, g = 0;
   cub::DoubleBuffer<uint32_t> k32(nullptr, nullptr), v32(nullptr, nullptr);
-  GZB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, g, k32, v32, (int64_t)c.ext, 0, 32));
+  GZB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, g, k32, v32, (int64_t)c.ext, 0, 16));
   cub::DoubleBuffer<uint64_t> k1(nullptr, nullptr);
   GZB_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, a, k1, (int64_t)c.hits, 0, hit_bits));
   GZB_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, b, k1, (int64_t)c.mwork, 0, mw_bits));
@@ -2648,7 +2650,7 @@ int graph_body(gzb_engine *e, int schedule, const GappedTile &tile, bool learned
     cub::DoubleBuffer<uint32_t> kb(e->okeys.as<uint32_t>(), e->okeys2.as<uint32_t>());
     cub::DoubleBuffer<uint32_t> vb(e->oidx.as<uint32_t>(), e->oidx2.as<uint32_t>());
     size_t tb = e->tmp.bytes;
-    GZB_CUDA(cub::DeviceRadixSort::SortPairs(e->tmp.p, tb, kb, vb, (int64_t)c.ext, 0, 32, s));
+    GZB_CUDA(cub::DeviceRadixSort::SortPairs(e->tmp.p, tb, kb, vb, (int64_t)c.ext, 0, 16, s));
     order = vb.Current();
     launches += 4;
   }
