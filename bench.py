@@ -650,6 +650,9 @@ def main():
     ap.add_argument("--ref-queries", type=int, default=10000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--once", action="store_true",
+                    help="one batched presearch (hit order, default tile, no training or "
+                         "autotuning) of the workload, for profiling; prints its stage times")
     ap.add_argument("--prep-only", type=int, default=0, metavar="READS",
                     help="time only the query preparation of READS 150-nt reads (reads "
                          "drawn from a 20,000-protein database) and print its JSON object")
@@ -659,6 +662,22 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.once:
+        import torch
+        from gzb import native as N
+        from gzb import params as P
+        torch.cuda.set_device(local_rank)
+        db, q, _ = make_workload(args.workload)
+        eng = N.PresearchEngine(local_rank)
+        eng.set_params(P.make_params())
+        eng.set_database(db)
+        eng.set_queries(q)
+        eng.set_tile(N.SCHEDULE_BATCHED, N.TILE_ORDER, N.ORDER_HITS)
+        eng.presearch(N.SCHEDULE_BATCHED)
+        print(json.dumps({"workload": args.workload, "stage_ms": eng.stage_ms(),
+                          "counters": eng.counters()}), flush=True)
+        eng.close()
+        return
     if args.prep_only:
         import torch
         from gzb import workload as W

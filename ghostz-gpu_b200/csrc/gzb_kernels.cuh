@@ -610,15 +610,24 @@ namespace gzb {
 // warp kernel.
 constexpr int kLaneW = 64;
 
+// The residue bytes of a band column are laid out so that lane l of every
+// warp uses bank l: byte 4l + w of the column's 128 bytes belongs to lane l
+// of warp w (blocks of four warps), so the lanes of a warp never conflict,
+// whatever columns they are at (with the plain [column][thread] byte layout
+// four lanes share each bank).
 struct LaneBand {
   uint32_t *cell;  // [kLaneW][stride]
-  uint8_t *res;    // [kLaneW][stride]
-  int stride;
-  int t;           // this thread's column in the layout
-  __device__ __forceinline__ int slot(int c) const { return (c & (kLaneW - 1)) * stride + t; }
+  uint8_t *res;    // [kLaneW][stride], lane-major within a column
+  int stride;      // threads of the block (128)
+  int t;           // this thread's column in the cell layout
+  int tr;          // this thread's byte in the residue layout
+  __device__ __forceinline__ LaneBand(uint32_t *cell_, uint8_t *res_, int stride_, int t_)
+      : cell(cell_), res(res_), stride(stride_), t(t_), tr(((t_ & 31) << 2) | (t_ >> 5)) {}
+  __device__ __forceinline__ int base(int c) const { return (c & (kLaneW - 1)) * stride; }
+  __device__ __forceinline__ int slot(int c) const { return base(c) + t; }
   __device__ __forceinline__ uint32_t &at(int c) { return cell[slot(c)]; }
-  __device__ __forceinline__ int residue(int c) const { return res[slot(c)]; }
-  __device__ __forceinline__ void set_residue(int c, int r) { res[slot(c)] = (uint8_t)r; }
+  __device__ __forceinline__ int residue(int c) const { return res[base(c) + tr]; }
+  __device__ __forceinline__ void set_residue(int c, int r) { res[base(c) + tr] = (uint8_t)r; }
 };
 
 __device__ __forceinline__ bool fits16(int v) { return v >= -32768 && v <= 32767; }
@@ -744,10 +753,11 @@ __device__ __forceinline__ int lane_row(const GappedJob &job, const int *sm, Lan
   const int maxs_in = maxs;
   int maxc = bs_row;
   for (int c = bs_row + 1; c < be; ++c) {
-    const int k = band.slot(c);
+    const int b = band.base(c);
+    const int k = b + band.t;
     const uint32_t w = band.cell[k];
     const int old_best = lo16(w), vgap = hi16(w);
-    int s = diag + mrow[band.res[k]];
+    int s = diag + mrow[band.res[b + band.tr]];
     diag = old_best;
     s = imax(s, imax(vgap, row_gap));
     // branch-free: a pruned cell (X-drop) stores the initial score and resets

@@ -137,6 +137,7 @@ __global__ void gather_kernel(size_t n, const uint32_t *idx, const uint32_t *src
 // device memory with device-side counts, so the three launches need no host
 // synchronisation.
 constexpr int kLaneBlock = 128;
+static_assert(kLaneBlock == 128, "the lane band's residue layout assumes four warps per block");
 constexpr int kBandW = 256;
 constexpr int kSerialThreads = 4 * 128;
 constexpr int kSerialBand = 1 << 15;  // columns per fallback thread
@@ -162,7 +163,7 @@ gapped_lane_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
   if (n_dev) n = *n_dev;
   load_matrix(sm, matrix, number_letters, stride);
   __syncthreads();
-  LaneBand band{cells_s, res_s, kLaneBlock, (int)threadIdx.x};
+  LaneBand band(cells_s, res_s, kLaneBlock, (int)threadIdx.x);
   unsigned long long cells = 0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
@@ -227,7 +228,7 @@ gapped_lane_queue_kernel(GappedJob job, const int32_t *__restrict__ matrix, int 
   if (n_dev) n = *n_dev;
   load_matrix(sm, matrix, number_letters, stride);
   __syncthreads();
-  LaneBand band{cells_s, res_s, kLaneBlock, (int)threadIdx.x};
+  LaneBand band(cells_s, res_s, kLaneBlock, (int)threadIdx.x);
   const int lane = threadIdx.x & 31;
   unsigned long long cells = 0;
   for (;;) {
@@ -281,7 +282,7 @@ gapped_rows_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
   if (n_dev) n = *n_dev;
   load_matrix(sm, matrix, number_letters, stride);
   __syncthreads();
-  LaneBand band{cells_s, res_s, kLaneBlock, (int)threadIdx.x};
+  LaneBand band(cells_s, res_s, kLaneBlock, (int)threadIdx.x);
   LaneExt x;
   uint32_t e = 0, q = 0, d = 0;
   bool have = false, done = false;
@@ -344,7 +345,7 @@ gapped_deal_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
   if (n_dev) n = *n_dev;
   load_matrix(sm, matrix, number_letters, stride);
   __syncthreads();
-  LaneBand band{cells_s, res_s, kLaneBlock, (int)threadIdx.x};
+  LaneBand band(cells_s, res_s, kLaneBlock, (int)threadIdx.x);
   const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   // the next extension of this lane, loaded one extension ahead
