@@ -441,7 +441,7 @@ constexpr int kUnitsPerWarp = 256;
 
 // One unit = one representative or one residual database position of a list,
 // tried against every query position of that list.
-__global__ void __launch_bounds__(kSeedBlock, 5)
+__global__ void __launch_bounds__(kSeedBlock, 6)
 seed_kernel(SeedArgs a) {
   __shared__ __align__(16) int32_t tbl32[kWalkTableBytes / 4];
   load_walk_table(tbl32, a.matrix32, a.p.delimiter);
