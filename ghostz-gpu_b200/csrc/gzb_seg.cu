@@ -53,6 +53,9 @@ constexpr int kSegMaxLength = 65535;      // ln(n!) table covers n <= this
 constexpr uint8_t kMaskBit = 64;
 constexpr uint8_t kUnknownCode = 24;      // X
 constexpr int kSegBlock = 128;
+// window entropies a warp of the search pass keeps in shared memory (the
+// windows of sequences up to kSegCache + 11 residues)
+constexpr int kSegCache = 1024;
 
 // ln(n!) rounded to 6 decimals (the precision of the reference's table)
 __device__ double g_seg_ln_fact[kSegMaxLength + 1];
@@ -216,8 +219,12 @@ struct SegFrame {
 // Masks the low-complexity segments of s[0..n) (n >= the window); every
 // lane of the warp runs the same search on the same data (so its branches
 // agree), the trimming is split over the lanes, and lane 0 writes the
-// masks.  Returns false if the search nested deeper than the stack.
-__device__ bool seg_sequence(const SegArgs &a, uint8_t *s, int n, int lane) {
+// masks.  E, when given, holds the entropy of the window starting at every
+// position 0 .. n-12 of s (computed before any mask), so the search reads
+// H instead of computing it; a frame's H(i) is that of the window starting
+// at its position min(i, its length - 12).  Returns false if the search
+// nested deeper than the stack.
+__device__ bool seg_sequence(const SegArgs &a, uint8_t *s, int n, int lane, const double *E) {
   SegFrame stack[kSegStack];
   int depth = 0;
   stack[0] = {0, n, 0, 0};
@@ -226,12 +233,15 @@ __device__ bool seg_sequence(const SegArgs &a, uint8_t *s, int n, int lane) {
     SegFrame f = stack[depth];
     const uint8_t *w = s + f.base;
     bool pushed = false;
-    // H over the frame, sliding from position f.i
+    // H over the frame, sliding from position f.i (or read from E)
+    auto h_at = [&](int i) {
+      return E[f.base + (i < f.n - kSegWindow ? i : f.n - kSegWindow)];
+    };
     int start = f.i < f.n - kSegWindow ? f.i : f.n - kSegWindow;
-    seg_state(w + start, kSegWindow, comp, state);
+    if (!E) seg_state(w + start, kSegWindow, comp, state);
     for (int i = f.i; i <= f.n - 1; ++i) {
       const int want = i < f.n - kSegWindow ? i : f.n - kSegWindow;
-      while (start < want) {  // slide by one
+      while (!E && start < want) {  // slide by one
         const int out = seg_class(w[start]), in = seg_class(w[start + kSegWindow]);
         if (out >= 0) {
           state_shrink(state, comp[out]);
@@ -243,12 +253,12 @@ __device__ bool seg_sequence(const SegArgs &a, uint8_t *s, int n, int lane) {
         }
         ++start;
       }
-      if (seg_entropy(a, state) > kSegLowCut) continue;
+      if ((E ? h_at(i) : seg_entropy(a, state)) > kSegLowCut) continue;
       int lo = i;
-      while (lo >= f.left_limit && seg_h(a, w, f.n, lo) <= kSegHighCut) --lo;
+      while (lo >= f.left_limit && (E ? h_at(lo) : seg_h(a, w, f.n, lo)) <= kSegHighCut) --lo;
       const int left_i = lo + 1;
       int hi = i;
-      while (hi <= f.n - 1 && seg_h(a, w, f.n, hi) <= kSegHighCut) ++hi;
+      while (hi <= f.n - 1 && (E ? h_at(hi) : seg_h(a, w, f.n, hi)) <= kSegHighCut) ++hi;
       const int right_i = hi - 1;
       int left_end = left_i, right_end = right_i;
       seg_trim_warp(a, w + left_end, right_end - left_end + 1, &left_end, &right_end, lane);
@@ -271,7 +281,7 @@ __device__ bool seg_sequence(const SegArgs &a, uint8_t *s, int n, int lane) {
       f.left_limit = next + 1;
       // the window restarts at the new position
       start = next + 1 < f.n - kSegWindow ? next + 1 : f.n - kSegWindow;
-      if (next + 1 <= f.n - 1) seg_state(w + start, kSegWindow, comp, state);
+      if (!E && next + 1 <= f.n - 1) seg_state(w + start, kSegWindow, comp, state);
     }
     if (!pushed) --depth;
   }
@@ -393,7 +403,9 @@ __global__ void __launch_bounds__(kSegBlock)
     seg_search_kernel(SegArgs a, uint8_t *__restrict__ codes, const uint64_t *__restrict__ offsets,
                       const uint32_t *__restrict__ lengths, uint64_t units, int mode,
                       uint32_t *__restrict__ status) {
+  __shared__ double ecache[kSegBlock / 32][kSegCache];
   const int lane = threadIdx.x & 31;
+  double *E = ecache[threadIdx.x >> 5];
   const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   for (uint64_t u = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; u < units;
        u += warps) {
@@ -405,7 +417,31 @@ __global__ void __launch_bounds__(kSegBlock)
     __syncwarp();
     if (lane == 0) s[0] &= 127;
     __syncwarp();
-    const bool ok = seg_sequence(a, s, n, lane);
+    // the window entropies, lane l sliding over its own run of starts
+    const int m = n - kSegWindow + 1;  // window starts 0 .. n-12
+    const bool cached = m <= kSegCache;
+    if (cached) {
+      const int per = (m + 31) / 32, p0 = lane * per, p1 = min(p0 + per, m);
+      if (p0 < p1) {
+        int comp[20], state[21];
+        seg_state(s + p0, kSegWindow, comp, state);
+        for (int p = p0;; ++p) {
+          E[p] = seg_entropy(a, state);
+          if (p + 1 >= p1) break;
+          const int out = seg_class(s[p]), in = seg_class(s[p + kSegWindow]);
+          if (out >= 0) {
+            state_shrink(state, comp[out]);
+            --comp[out];
+          }
+          if (in >= 0) {
+            state_grow(state, comp[in]);
+            ++comp[in];
+          }
+        }
+      }
+      __syncwarp();
+    }
+    const bool ok = seg_sequence(a, s, n, lane, cached ? E : nullptr);
     __syncwarp();
     if (!ok && lane == 0 && status) atomicAdd(status, 1u);
     for (int i = lane; i < n; i += 32) {
