@@ -190,6 +190,105 @@ def query_prep_bench(db, steps, warmup, cpu=True, seed=302, reads=None):
     return out
 
 
+OPS_QUERY_RESIDUES = 3_000_000     # the query set of a 10k-query search
+OPS_DB_RESIDUES = 600_000_000      # a 2M-protein chunk
+
+
+def ops_bench(workload, seeds, steps, warmup):
+    """The per-operator entry points outside the fused presearch.  First one
+    presearch of WORKLOAD (its device query-list lookup, `list_lookup_kernel`,
+    is the lookup stage; timed with the stage events, which also cover the
+    scan of the unit counts); then DistanceCalculatorGpu::CalculateDistancesAsync
+    (src/distance_calculator_gpu.cu:320-355) over SEEDS random seed pairs of a
+    3 M-residue query set against a 600 M-residue chunk, both resident in HBM:
+    device-only (centres already on the device) and end to end (centres and
+    distances in pinned host memory, copies inside the timed region), each
+    timed with CUDA events over STEPS launches after WARMUP."""
+    import torch
+    from gzb import native as N
+    from gzb import params as P
+    dev = torch.device("cuda")
+    params = P.make_params()
+    db, q, _ = make_workload(workload)
+    eng = N.PresearchEngine(torch.cuda.current_device())
+    eng.set_params(params)
+    eng.set_database(db)
+    eng.set_queries(q)
+    eng.presearch(N.SCHEDULE_PLAIN)
+    lookup_ms = eng.stage_ms()["lookup"]
+    eng.close()
+    del db, q
+    torch.cuda.empty_cache()
+
+    L = int(params["subsequence_length"])
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(7)
+    qres = torch.randint(0, 20, (OPS_QUERY_RESIDUES,), dtype=torch.uint8, device=dev,
+                         generator=gen)
+    dres = torch.randint(0, 20, (OPS_DB_RESIDUES,), dtype=torch.uint8, device=dev,
+                         generator=gen)
+    # centres at least L from either end: the window reads c - L/2 .. c + L/2 - 1
+    d_qc = torch.randint(L, OPS_QUERY_RESIDUES - L, (seeds,), dtype=torch.int32, device=dev,
+                         generator=gen)
+    d_dc = torch.randint(L, OPS_DB_RESIDUES - L, (seeds,), dtype=torch.int32, device=dev,
+                         generator=gen)
+    d_out = torch.empty(seeds, dtype=torch.int8, device=dev)
+    h_qc = d_qc.cpu().pin_memory()
+    h_dc = d_dc.cpu().pin_memory()
+    h_out = torch.empty(seeds, dtype=torch.int8).pin_memory()
+    d_qc2 = torch.empty_like(d_qc)
+    d_dc2 = torch.empty_like(d_dc)
+    d_out2 = torch.empty_like(d_out)
+    tmap = torch.from_numpy(np.asarray(params["similarity_code_map"]).copy()).to(dev)
+    dc = N.DistanceCalculatorGpu()
+    dc.SetQueries(qres)
+    dc.SetDatabase(dres)
+    dc.SetReducedCodeMap(tmap)
+    dc.SetSubsequenceLength(L)
+    stream = torch.cuda.current_stream()
+    hq, hd, ho = h_qc.numpy(), h_dc.numpy(), h_out.numpy()
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    dev_ms = timed(lambda: dc.CalculateDistancesAsync(seeds, None, None, None, d_qc, d_dc,
+                                                      d_out))
+    e2e_ms = timed(lambda: dc.CalculateDistancesAsync(seeds, hq, hd, ho, d_qc2, d_dc2,
+                                                      d_out2))
+    same = bool(torch.equal(d_out.cpu(), h_out))
+    dc.close()
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak, src = float(peaks["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, KeyError, ValueError):
+        peak, src = 6650.0, "fallback 6650 GB/s"
+    achieved = seeds * BYTES_PER_DISTANCE_SEED / (dev_ms / 1e3) / 1e9
+    return {
+        "lookup": {"workload": workload, "stage_ms": lookup_ms,
+                   "note": "list_lookup_kernel plus the scan of its unit counts and the "
+                           "read-back of their total"},
+        "distance": {"seeds": seeds, "subsequence_length": L,
+                     "query_residues": OPS_QUERY_RESIDUES, "chunk_residues": OPS_DB_RESIDUES,
+                     "kernel_ms": dev_ms, "seeds_per_s": seeds / (dev_ms / 1e3),
+                     "e2e": {"ms": e2e_ms, "seeds_per_s": seeds / (e2e_ms / 1e3),
+                             "h2d_bytes_per_step": 8 * seeds, "d2h_bytes_per_step": seeds},
+                     "results_equal_e2e": same,
+                     "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                                  "unit": "GB/s", "frac": achieved / peak,
+                                  "algorithmic_bytes_per_seed": BYTES_PER_DISTANCE_SEED,
+                                  "peak_source": src}},
+    }
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons during the timed region."""
 
@@ -656,6 +755,10 @@ def main():
     ap.add_argument("--prep-only", type=int, default=0, metavar="READS",
                     help="time only the query preparation of READS 150-nt reads (reads "
                          "drawn from a 20,000-protein database) and print its JSON object")
+    ap.add_argument("--ops-only", type=int, default=0, metavar="SEEDS",
+                    help="time the standalone distance calculator over SEEDS seeds and one "
+                         "presearch's query-list lookup of the workload; print their JSON "
+                         "object")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -685,6 +788,12 @@ def main():
         out = query_prep_bench(W.make_database(20000, 101), args.steps, args.warmup,
                                cpu=False, reads=args.prep_only)
         print(json.dumps({"query_preparation": out}), flush=True)
+        return
+    if args.ops_only:
+        import torch
+        torch.cuda.set_device(local_rank)
+        out = ops_bench(args.workload, args.ops_only, args.steps, args.warmup)
+        print(json.dumps({"operators": out}), flush=True)
         return
     if args.workload in MULTICHUNK_WORKLOADS:
         if args.impl == "reference":
