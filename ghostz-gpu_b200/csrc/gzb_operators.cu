@@ -28,7 +28,42 @@ int set_error(int code, const char *fmt, ...) {
 // --------------------------------------------------------------------------
 // kernels
 
-// Distance of every seed (one thread per seed).
+// Windows of up to kWordWindow bytes are fetched as the naturally aligned
+// 32-bit words that hold them: at most four words, and only the words that
+// hold at least one byte of the window (so no load reaches past the pages
+// the window lies in).  w[] receives the window's bytes from byte 0 of w[0].
+constexpr int kWordWindow = 13;
+
+__device__ __forceinline__ void window_words(const uint8_t *p, int L, uint32_t w[4]) {
+  const uintptr_t a = (uintptr_t)p;
+  const uint32_t *base = reinterpret_cast<const uint32_t *>(a & ~(uintptr_t)3);
+  const int off = (int)(a & 3);
+  const int nw = (off + L + 3) >> 2;
+  uint32_t r[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) r[j] = j < nw ? __ldg(base + j) : 0u;
+  const unsigned sh = 8u * (unsigned)off;
+  w[0] = __funnelshift_r(r[0], r[1], sh);
+  w[1] = __funnelshift_r(r[1], r[2], sh);
+  w[2] = __funnelshift_r(r[2], r[3], sh);
+  w[3] = __funnelshift_r(r[3], 0u, sh);
+}
+
+// Reduced-alphabet mismatches of two windows held as words (L <= kWordWindow).
+__device__ __forceinline__ int word_distance(const uint32_t *a, const uint32_t *b, int L,
+                                             const uint8_t *map) {
+  int m = 0;
+#pragma unroll
+  for (int i = 0; i < kWordWindow; ++i)
+    if (i < L)
+      m += map[(a[i >> 2] >> (8 * (i & 3))) & 0xFF] != map[(b[i >> 2] >> (8 * (i & 3))) & 0xFF];
+  return m;
+}
+
+// Distance of every seed: the reduced-alphabet mismatches over the L window
+// centred on the seed's query and database positions.  A thread takes two
+// seeds a pass (their loads in flight together); windows up to kWordWindow
+// bytes are read as words, longer ones byte by byte.
 __global__ void distance_kernel(const uint8_t *__restrict__ q,
                                 const uint8_t *__restrict__ d,
                                 const uint8_t *__restrict__ map_g, int L,
@@ -38,9 +73,26 @@ __global__ void distance_kernel(const uint8_t *__restrict__ q,
   __shared__ uint8_t map[256];
   for (int i = threadIdx.x; i < 256; i += blockDim.x) map[i] = i < 32 ? map_g[i] : 0;
   __syncthreads();
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x)
-    out[i] = (int8_t)window_distance(q + qc[i], d + dc[i], L, map);
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const int half = L / 2;
+  if (L > kWordWindow) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += stride)
+      out[i] = (int8_t)window_distance(q + qc[i], d + dc[i], L, map);
+    return;
+  }
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += 2 * stride) {
+    const size_t j = i + stride;
+    const bool two = j < n;
+    const uint32_t qa = qc[i], da = dc[i];
+    const uint32_t qb = two ? qc[j] : qa, db = two ? dc[j] : da;
+    uint32_t wqa[4], wda[4], wqb[4], wdb[4];
+    window_words(q + qa - half, L, wqa);
+    window_words(d + da - half, L, wda);
+    window_words(q + qb - half, L, wqb);
+    window_words(d + db - half, L, wdb);
+    out[i] = (int8_t)word_distance(wqa, wda, L, map);
+    if (two) out[j] = (int8_t)word_distance(wqb, wdb, L, map);
+  }
 }
 
 // Ungapped extension with trigger, one thread per seed.

@@ -182,17 +182,22 @@ def test_ungapped_flags_match_oracle(torch_cuda, oracle, params):
     assert 0 < exp.sum() < n
 
 
-def test_distances_match_oracle(torch_cuda, oracle, params):
+@pytest.mark.parametrize("L", [10, 7, 13, 16])
+def test_distances_match_oracle(torch_cuda, oracle, L):
+    """Windows up to 13 letters are read as aligned words, longer ones byte
+    by byte: both give the reference's distances."""
     from gzb import native as N
+    from gzb import params as P
     torch = torch_cuda
-    rng = np.random.default_rng(6)
+    params = P.make_params(subsequence_length=L)
+    rng = np.random.default_rng(6 + L)
     a = W.random_residues(rng, 20000)
     b = a.copy()
     m = rng.random(len(b)) < 0.15
     b[m] = W.random_residues(rng, int(m.sum()))
     n = 50000
-    c0 = rng.integers(5, len(a) - 6, n).astype(np.uint32)
-    c1 = np.clip(c0.astype(np.int64) + rng.integers(-2, 3, n), 5, len(b) - 6).astype(np.uint32)
+    c0 = rng.integers(L, len(a) - L, n).astype(np.uint32)
+    c1 = np.clip(c0.astype(np.int64) + rng.integers(-2, 3, n), L, len(b) - L).astype(np.uint32)
     tq, qa = N.device_sequence(a, 25)
     td, da = N.device_sequence(b, 25)
     tmap = torch.from_numpy(np.asarray(params["similarity_code_map"]).copy()).cuda()
@@ -200,7 +205,7 @@ def test_distances_match_oracle(torch_cuda, oracle, params):
     dc.SetQueries(qa)
     dc.SetDatabase(da)
     dc.SetReducedCodeMap(tmap)
-    dc.SetSubsequenceLength(10)
+    dc.SetSubsequenceLength(L)
     out = np.zeros(n, np.int8)
     d0 = torch.zeros(n, dtype=torch.int32, device="cuda")
     d1 = torch.zeros(n, dtype=torch.int32, device="cuda")
