@@ -364,6 +364,9 @@ def cpu_baseline(db, q, n_queries=4000, slice_sequences=20000, processes=1):
                       lengths=q.lengths[:n_queries].copy(), cutoffs=q.cutoffs[:n_queries].copy(),
                       triggers=q.triggers[:n_queries].copy())
     import multiprocessing as mp
+    import oracle as O
+    if not os.path.exists(O.LIB):
+        O.build()  # once here, not racing in every worker
     ctx = mp.get_context("spawn")
     bounds = np.linspace(0, n_queries, processes + 1).astype(int)
     # each worker builds the chunk index untimed (the reference's separate
