@@ -139,6 +139,8 @@ def _declare(L):
         "gzb_query_karlin_cutoffs": [V, V, V, U32, V, U32, C.c_float, C.c_float, V, V, V, V],
         "gzb_seg_translated_queries": [V, V, V, U32, V, V],
         "gzb_seg_protein_queries": [V, V, V, U32, V, V],
+        "gzb_index_blob_from_reference": [V, V, C.c_uint64, V, C.c_uint64, V, U32, V,
+                                          C.c_uint64, V],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -596,6 +598,24 @@ def _stream_or_null(stream):
 
 
 # -- query preparation: six-frame translation ---------------------------------
+def index_blob_from_reference(params, sdp, db):
+    """The reference's on-disk seed-searcher index of chunk `db` (the bytes
+    of its .sdp file) as an index blob for PresearchEngine.set_database(db,
+    index=...).  Host only: no device is needed."""
+    rec = np.array([params], dtype=params.dtype)
+    sdp = np.ascontiguousarray(np.frombuffer(sdp, np.uint8) if isinstance(sdp, bytes) else sdp,
+                               dtype=np.uint8)
+    codes = np.ascontiguousarray(db.codes, dtype=np.uint8)
+    offs = np.ascontiguousarray(db.offsets, dtype=np.uint32)
+    n = C.c_uint64()
+    args = (C.c_void_p(rec.ctypes.data), hptr(sdp), sdp.nbytes, hptr(codes), len(codes),
+            hptr(offs), int(db.number_sequences))
+    check(lib().gzb_index_blob_from_reference(*args, None, 0, C.byref(n)))
+    blob = np.zeros(int(n.value), np.uint8)
+    check(lib().gzb_index_blob_from_reference(*args, hptr(blob), blob.nbytes, C.byref(n)))
+    return blob
+
+
 def translated_query_length(length):
     """Codes of a read's translated query, both delimiters included
     (TranslatedDnaQuery::GetSequenceLength, src/translated_dna_query.h:24-31;

@@ -274,6 +274,22 @@ int gzb_engine_set_database_with_index(gzb_engine *e, int32_t chunk_id, const ui
                                        uint64_t length, const uint32_t *offsets,
                                        uint32_t number_sequences, const void *blob,
                                        uint64_t blob_bytes, void *stream);
+/* The reference's on-disk seed-searcher index of one chunk (the bytes of
+ * its `.sdp` file: SeedSearcherDatabaseParameters::Save,
+ * src/seed_searcher_database_parameters.cpp:363-376, written by
+ * DatabaseChunk::SaveSeedSearcherParameters, src/database_chunk.h:461-470,
+ * and read back by SeedSearcherDatabaseParameters::Build(sequence, length,
+ * istream), :321-337) converted to this library's index blob for the chunk
+ * (codes / offsets as gzb_engine_set_database), ready for
+ * gzb_engine_set_database_with_index.  Host only, no device.  The file must
+ * have been built with `params` (clustering, delimiter, window, seed hash,
+ * similarity map, cluster threshold) and be consistent; otherwise
+ * GZB_ERR_INVALID.  *blob_bytes receives the blob's size; blob = NULL asks
+ * only for it. */
+int gzb_index_blob_from_reference(const gzb_params *params, const void *sdp, uint64_t sdp_bytes,
+                                  const uint8_t *codes, uint64_t length, const uint32_t *offsets,
+                                  uint32_t number_sequences, void *blob, uint64_t capacity,
+                                  uint64_t *blob_bytes);
 
 /* Stored database chunks, for streaming a database of many chunks
  * (the reference's chunk loop with its preloading thread,

@@ -10,6 +10,7 @@
 #include <string.h>
 #include <vector>
 #include <string>
+#include <sstream>
 
 #include "gz_oracle.h"
 
@@ -203,6 +204,18 @@ size_t gzr_db_index_members(void *h, uint32_t cluster_id, uint32_t *out,
 
 int gzr_db_index_max_mismatches(void *h) {
   return ((gzr_db_index *)h)->params.GetNumberMaxMismatchs();
+}
+
+/* The index as the reference's `db` command writes it to the chunk's .sdp
+ * file (SeedSearcherDatabaseParameters::Save,
+ * src/seed_searcher_database_parameters.cpp:363-376); returns its size and
+ * copies up to cap bytes. */
+size_t gzr_db_index_save(void *h, uint8_t *out, size_t cap) {
+  std::ostringstream os(std::ios::binary);
+  ((gzr_db_index *)h)->params.Save(os);
+  const std::string b = os.str();
+  if (out) memcpy(out, b.data(), b.size() < cap ? b.size() : cap);
+  return b.size();
 }
 
 /* Cutoffs exactly as the reference derives them from bit scores

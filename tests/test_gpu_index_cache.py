@@ -66,3 +66,35 @@ def test_index_blob_refused_for_other_chunks_and_parameters(engines):
     b.set_params(P.make_params(clustering=False))
     with pytest.raises(N.GzbError, match="other index parameters"):
         b.set_database(db, index=blob)
+
+
+def test_reference_index_file_loads(engines, oracle):
+    """The reference's .sdp file of a chunk (committed fixture) converted on
+    the host is byte for byte the blob the device build exports, and the
+    presearch from it matches the oracle."""
+    import importlib.util
+    import os
+    from gzb import native as N
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                        "make_reference_index.py")
+    spec = importlib.util.spec_from_file_location("make_reference_index", path)
+    g = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(g)
+    a, b = engines
+    p = P.make_params()
+    db = g.chunk()
+    with open(g.FIXTURE, "rb") as f:
+        blob = N.index_blob_from_reference(p, f.read(), db)
+    a.set_params(p)
+    a.set_database(db)
+    assert np.array_equal(a.export_index(), blob)
+    b.set_params(p)
+    b.set_database(db, index=blob)
+    q = W.make_queries(db, 40, 2601, median=80)
+    b.set_queries(q)
+    b.reset_results()
+    b.presearch(0)
+    res, _, _ = oracle.presearch(p, db, q)
+    got = b.results()
+    assert all(np.array_equal(got[i], res[i]) for i in range(q.number))
+    assert sum(len(x) for x in got) > 0
