@@ -141,6 +141,7 @@ def _declare(L):
         "gzb_seg_protein_queries": [V, V, V, U32, V, V],
         "gzb_index_blob_from_reference": [V, V, C.c_uint64, V, C.c_uint64, V, U32, V,
                                           C.c_uint64, V],
+        "gzb_merge_chunk_results": [V, U32, V, V, V, V],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -459,12 +460,19 @@ class PresearchEngine:
     def reset_results(self, stream=None):
         check(lib().gzb_engine_reset_results(self.h, _stream_or_null(stream)))
 
-    def results(self, stream=None):
+    def result_rows(self, stream=None):
+        """The merged lists in the ABI's layout: (counts[number_queries],
+        records[number_queries * max_number_results], RESULT_DTYPE)."""
         b = int(self.params[0]["max_number_results"])
         counts = np.zeros(self.number_queries, np.uint32)
         res = np.zeros(self.number_queries * b, RESULT_DTYPE)
         check(lib().gzb_engine_get_results(self.h, hptr(counts), hptr(res),
                                            _stream_or_null(stream)))
+        return counts, res
+
+    def results(self, stream=None):
+        b = int(self.params[0]["max_number_results"])
+        counts, res = self.result_rows(stream)
         res = res.reshape(self.number_queries, b)
         return [res[i, :counts[i]].copy() for i in range(self.number_queries)]
 
@@ -598,6 +606,19 @@ def _stream_or_null(stream):
 
 
 # -- query preparation: six-frame translation ---------------------------------
+def merge_chunk_results(params, chunk_counts, chunk_records, counts, records):
+    """gzb_merge_chunk_results: one chunk's lists (counts, RESULT_DTYPE rows
+    of max_number_results) merged in place into the running lists."""
+    rec = np.array([params], dtype=params.dtype)
+    b = int(params["max_number_results"])
+    nq = len(counts)
+    for a, dt, n in ((chunk_counts, np.uint32, nq), (counts, np.uint32, nq),
+                     (chunk_records, RESULT_DTYPE, nq * b), (records, RESULT_DTYPE, nq * b)):
+        assert a.dtype == dt and a.flags.c_contiguous and len(a) == n
+    check(lib().gzb_merge_chunk_results(C.c_void_p(rec.ctypes.data), nq, hptr(chunk_counts),
+                                        hptr(chunk_records), hptr(counts), hptr(records)))
+
+
 def index_blob_from_reference(params, sdp, db):
     """The reference's on-disk seed-searcher index of chunk `db` (the bytes
     of its .sdp file) as an index blob for PresearchEngine.set_database(db,

@@ -1,0 +1,89 @@
+"""Database chunks spread over GPUs, one process per GPU.
+
+The path's one exchange step: the reference's chunk loop
+(src/aligner_gpu_presearch_thread.cpp:214-640) merges every chunk's results
+into the per-query top-b lists with AlignerCommon::AddResults
+(src/aligner_common.h:147-274).  Here rank r searches chunks r, r + N,
+r + 2N, ... with its results reset before each chunk, the per-chunk lists
+are all-gathered (NCCL between GPUs, gloo between CPU processes), and every
+rank merges them in chunk order with gzb_merge_chunk_results, which gives
+exactly the lists of one engine searching every chunk in turn.
+"""
+import numpy as np
+
+from . import native as N
+
+RECORD_WORDS = N.RESULT_DTYPE.itemsize // 4
+
+
+def chunks_of(rank, world, n_chunks):
+    """The chunks rank `rank` of `world` searches."""
+    return list(range(rank, n_chunks, world))
+
+
+def merge_in_order(params, lists):
+    """lists[c] = (counts, records) of chunk c alone; returns the running
+    merge of all of them in chunk order."""
+    b = int(params["max_number_results"])
+    nq = len(lists[0][0])
+    counts = np.zeros(nq, np.uint32)
+    records = np.zeros(nq * b, N.RESULT_DTYPE)
+    for chunk_counts, chunk_records in lists:
+        N.merge_chunk_results(params, chunk_counts, chunk_records, counts, records)
+    return counts, records
+
+
+class ChunkShards:
+    """Rank and world of an initialised torch.distributed process group (or
+    one local process when `dist` is None); `device` is where the gathered
+    buffers live ("cuda" for NCCL, "cpu" for gloo)."""
+
+    def __init__(self, dist=None, device="cpu"):
+        self.dist = dist
+        self.device = device
+        self.world = dist.get_world_size() if dist is not None else 1
+        self.rank = dist.get_rank() if dist is not None else 0
+
+    def exchange(self, params, n_chunks, number_queries, local):
+        """local = {chunk id: (counts, records)} for this rank's chunks;
+        returns every chunk's lists, indexed by chunk id, on every rank.  All
+        ranks take part with equal-sized buffers (chunks a rank does not have
+        travel as zeros and are ignored)."""
+        b = int(params["max_number_results"])
+        nq = int(number_queries)
+        words = nq + nq * b * RECORD_WORDS
+        per_rank = -(-n_chunks // self.world)
+        buf = np.zeros((per_rank, words), np.int32)
+        for i, c in enumerate(chunks_of(self.rank, self.world, n_chunks)):
+            counts, records = local[c]
+            buf[i, :nq] = counts.view(np.int32)
+            buf[i, nq:] = np.ascontiguousarray(records, N.RESULT_DTYPE).view(np.int32)
+        if self.dist is None:
+            gathered = [buf]
+        else:
+            import torch
+            t = torch.from_numpy(buf).to(self.device)
+            outs = [torch.empty_like(t) for _ in range(self.world)]
+            self.dist.all_gather(outs, t)
+            gathered = [o.cpu().numpy() for o in outs]
+        lists = [None] * n_chunks
+        for r in range(self.world):
+            for i, c in enumerate(chunks_of(r, self.world, n_chunks)):
+                row = gathered[r][i]
+                lists[c] = (row[:nq].view(np.uint32).copy(),
+                            row[nq:].copy().view(N.RESULT_DTYPE))
+        return lists
+
+    def search(self, engine, params, chunks, schedule=N.SCHEDULE_BATCHED):
+        """Presearch of the engine's resident queries against this rank's
+        chunks (each set in turn, results reset before each), then the
+        exchange and the merge: (counts, records) of all chunks, on every
+        rank."""
+        local = {}
+        for c in chunks_of(self.rank, self.world, len(chunks)):
+            engine.set_database(chunks[c], chunk_id=c)
+            engine.reset_results()
+            engine.presearch(schedule)
+            local[c] = engine.result_rows()
+        lists = self.exchange(params, len(chunks), engine.number_queries, local)
+        return merge_in_order(params, lists)

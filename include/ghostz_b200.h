@@ -356,6 +356,19 @@ int gzb_engine_reset_results(gzb_engine *e, void *stream);
  * valid entries, best first).  Synchronises `stream`. */
 int gzb_engine_get_results(gzb_engine *e, uint32_t *counts,
                            gzb_result *results, void *stream);
+/* The exchange step of a search whose database chunks are spread over GPUs
+ * (one process per GPU, each searching its own chunks): one chunk's lists
+ * merged into the running lists on the host, as the reference's
+ * AlignerCommon::AddResults (src/aligner_common.h:147-274) merges each
+ * chunk's results.  Layout as gzb_engine_get_results.  chunk_counts /
+ * chunk_results: one chunk's lists as the engine gives them after
+ * gzb_engine_reset_results and one gzb_engine_presearch of that chunk;
+ * counts / results: the lists of the chunks merged so far, updated in
+ * place.  Merging every chunk this way in chunk order gives exactly the
+ * lists of presearching the chunks in turn on one engine.  Host only. */
+int gzb_merge_chunk_results(const gzb_params *params, uint32_t number_queries,
+                            const uint32_t *chunk_counts, const gzb_result *chunk_results,
+                            uint32_t *counts, gzb_result *results);
 /* Alignment statistics of one merged result (AlignerCommon::Result,
  * src/aligner_common.h:80-92): the result's fields plus what
  * AlignerCommon::BuildResult (src/aligner_common.h:275-340) derives from the

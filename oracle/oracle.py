@@ -93,6 +93,9 @@ class Oracle:
                                         u32p, C.c_uint32, C.c_uint32, C.c_uint32]
         L.gzo_presearch_run.restype = C.c_void_p
         L.gzo_presearch_free.argtypes = [C.c_void_p]
+        L.gzo_add_results.argtypes = [C.c_void_p, u32p, C.c_uint32, C.c_uint32, C.c_void_p,
+                                      C.c_size_t, C.c_void_p, C.c_size_t]
+        L.gzo_add_results.restype = C.c_size_t
         L.gzo_presearch_results.argtypes = [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]
         L.gzo_presearch_results.restype = C.c_size_t
         L.gzo_presearch_counters.argtypes = [C.c_void_p, C.POINTER(C.c_uint64 * 6)]
@@ -293,6 +296,22 @@ class Oracle:
             out[nm] = np.ctypeslib.as_array(ptr, shape=(n,)).copy() if n else np.zeros(0, np.uint32)
         self.L.gzo_query_lists_free(C.c_void_p(h))
         return out
+
+    def add_results(self, params, db, added, results):
+        """One AddResults step (gzo_add_results): `added` (RESULT_DTYPE, every
+        record's chunk_id set to the chunk being merged; subject ids are
+        recomputed from db's offsets) merged into `results`; returns the
+        new list."""
+        pr = _Params(params)
+        b = int(params["max_number_results"])
+        a = np.ascontiguousarray(added, dtype=RESULT_DTYPE).copy()
+        r = np.zeros(max(b, len(results)) + 1, dtype=RESULT_DTYPE)
+        r[:len(results)] = results
+        offs = np.ascontiguousarray(db.offsets, dtype=np.uint32)
+        n = self.L.gzo_add_results(pr.ptr, _p(offs, u32p), db.number_sequences, len(db.codes),
+                                   C.c_void_p(a.ctypes.data), len(a),
+                                   C.c_void_p(r.ctypes.data), len(results))
+        return r[:n].copy()
 
     # -- presearch --------------------------------------------------------------
     def presearch(self, params, db, queries, query_begin=0, query_end=None):

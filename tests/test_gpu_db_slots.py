@@ -127,3 +127,24 @@ def test_slot_refusals(native, params):
         e.presearch(N.SCHEDULE_PLAIN)
     finally:
         e.close()
+
+
+def test_chunk_shards_match_sequential(native, params):
+    """Each chunk searched alone (results reset before it), its lists merged
+    on the host in chunk order (the exchange step of chunks spread over
+    GPUs, here one process), equals one engine searching the chunks in
+    turn."""
+    from gzb import shards as S
+    N = native
+    chunks, q = _database()
+    exp = _sequential(N, params, chunks, q)
+    e = N.PresearchEngine(0)
+    try:
+        e.set_params(params)
+        e.set_queries(q)
+        counts, records = S.ChunkShards().search(e, params, chunks, N.SCHEDULE_BATCHED)
+    finally:
+        e.close()
+    b = int(params["max_number_results"])
+    rows = records.reshape(q.number, b)
+    _same([rows[i, :counts[i]] for i in range(q.number)], exp)
