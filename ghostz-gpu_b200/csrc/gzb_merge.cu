@@ -14,7 +14,6 @@
 
 #include <algorithm>
 #include <cstring>
-#include <vector>
 
 #include "ghostz_b200.h"
 #include "gzb_common.h"
@@ -42,59 +41,85 @@ bool contained(const gzb_result &a, const gzb_result &b) {
           b.end_d <= a.end_d);
 }
 
+constexpr int kMaxResults = 32;  // max_number_results is at most 32
+
 struct Start {
   uint32_t position, result;  // the reference keys the list by this position
 };
 
 struct SubjectStarts {
   int32_t subject;
-  std::vector<Start> starts;  // ordered by position
+  int n;
+  Start starts[kMaxResults];  // ordered by position
 };
 
-size_t first_not_below(const std::vector<Start> &v, size_t from, uint32_t position) {
-  return std::lower_bound(v.begin() + from, v.end(), position,
-                          [](const Start &s, uint32_t p) { return s.position < p; }) -
-         v.begin();
+// std::lower_bound's bisection over [from, n).  The list need not be sorted
+// by the searched value (entries are inserted where their database start
+// would go but keyed by their query start), so the probes must be the
+// bisection's exactly, not a scan.
+int first_not_below(const Start *v, int from, int n, uint32_t position) {
+  int len = n - from;
+  while (len > 0) {
+    const int half = len >> 1, mid = from + half;
+    if (v[mid].position < position) {
+      from = mid + 1;
+      len -= half + 1;
+    } else {
+      len = half;
+    }
+  }
+  return from;
 }
 
 // One query: `added` (n_added records of one chunk) merged into `row`
-// (n_row records), at most b kept; returns the new count.
-uint32_t merge_row(const gzb_params &p, std::vector<gzb_result> &added, gzb_result *row,
-                   uint32_t n_row, std::vector<gzb_result> &out) {
-  const size_t b = (size_t)p.max_number_results;
-  // stable, best first (stable_sort with PresearchedResultGreaterScore)
-  std::stable_sort(added.begin(), added.end(), [](const gzb_result &x, const gzb_result &y) {
-    return alignment_comp(x, y) > 0;
-  });
-  const int32_t chunk = added.empty() ? -1 : added[0].chunk_id;
-  out.clear();
-  std::vector<SubjectStarts> subjects;
-  size_t ai = 0, ri = 0;
-  while (out.size() < b && (ai < added.size() || ri < n_row)) {
+// (n_row records), at most b kept; returns the new count.  No allocation:
+// every list is bounded by b <= 32.
+uint32_t merge_row(const gzb_params &p, gzb_result *added, uint32_t n_added, gzb_result *row,
+                   uint32_t n_row) {
+  const uint32_t b = (uint32_t)p.max_number_results;
+  // stable, best first (stable_sort with PresearchedResultGreaterScore):
+  // insertion sort moves a record only past strictly worse ones
+  for (uint32_t i = 1; i < n_added; ++i) {
+    const gzb_result x = added[i];
+    uint32_t j = i;
+    while (j > 0 && alignment_comp(x, added[j - 1]) > 0) {
+      added[j] = added[j - 1];
+      --j;
+    }
+    added[j] = x;
+  }
+  const int32_t chunk = n_added ? added[0].chunk_id : -1;
+  gzb_result out[kMaxResults];
+  uint32_t n_out = 0;
+  SubjectStarts subjects[kMaxResults];
+  int n_subjects = 0;
+  uint32_t ai = 0, ri = 0;
+  while (n_out < b && (ai < n_added || ri < n_row)) {
     gzb_result a;
-    if (ai == added.size())
+    if (ai == n_added)
       a = row[ri++];
     else if (ri == n_row || alignment_comp(row[ri], added[ai]) < 0)
       a = added[ai++];
     else
       a = row[ri++];
     if (a.chunk_id != chunk) {  // another chunk's result passes as it is
-      out.push_back(a);
+      out[n_out++] = a;
       continue;
     }
     SubjectStarts *s = nullptr;
-    for (auto &x : subjects)
-      if (x.subject == a.subject_id) s = &x;
+    for (int k = 0; k < n_subjects; ++k)
+      if (subjects[k].subject == a.subject_id) s = &subjects[k];
     if (!s) {
-      subjects.push_back(SubjectStarts{a.subject_id, {}});
-      s = &subjects.back();
+      s = &subjects[n_subjects++];
+      s->subject = a.subject_id;
+      s->n = 0;
     }
-    if (s->starts.size() >= (size_t)p.max_number_one_subject_results) continue;
+    if (s->n >= p.max_number_one_subject_results) continue;
     // accepted results of this subject whose listed position lies in
     // [start_d, end_d) must not contain the candidate
-    size_t it = first_not_below(s->starts, 0, a.start_d);
-    const size_t insert_at = it;
-    const size_t it_end = first_not_below(s->starts, it, a.end_d);
+    int it = first_not_below(s->starts, 0, s->n, a.start_d);
+    const int insert_at = it;
+    const int it_end = first_not_below(s->starts, it, s->n, a.end_d);
     bool keep = true;
     for (; it < it_end; ++it)
       if (contained(out[s->starts[it].result], a)) {
@@ -103,11 +128,13 @@ uint32_t merge_row(const gzb_params &p, std::vector<gzb_result> &added, gzb_resu
       }
     if (!keep) continue;
     // the reference lists the new result under its query start
-    s->starts.insert(s->starts.begin() + insert_at, Start{a.start_q, (uint32_t)out.size()});
-    out.push_back(a);
+    for (int k = s->n; k > insert_at; --k) s->starts[k] = s->starts[k - 1];
+    s->starts[insert_at] = Start{a.start_q, n_out};
+    ++s->n;
+    out[n_out++] = a;
   }
-  std::copy(out.begin(), out.end(), row);
-  return (uint32_t)out.size();
+  for (uint32_t i = 0; i < n_out; ++i) row[i] = out[i];
+  return n_out;
 }
 
 }  // namespace
@@ -127,17 +154,18 @@ extern "C" int gzb_merge_chunk_results(const gzb_params *params, uint32_t number
   for (uint32_t q = 0; q < number_queries; ++q)
     GZB_CHECK(chunk_counts[q] <= b && counts[q] <= b, GZB_ERR_INVALID,
               "query %u holds more than %u results", q, b);
-  std::vector<gzb_result> added, out;
-  added.reserve(b);
-  out.reserve(b);
   for (uint32_t q = 0; q < number_queries; ++q) {
     const gzb_result *c = chunk_results + (size_t)q * b;
-    if (chunk_counts[q] == 0) continue;  // nothing added: the row stays
     for (uint32_t i = 1; i < chunk_counts[q]; ++i)
       GZB_CHECK(c[i].chunk_id == c[0].chunk_id, GZB_ERR_INVALID,
                 "query %u: the added results come from more than one chunk", q);
-    added.assign(c, c + chunk_counts[q]);
-    counts[q] = merge_row(p, added, results + (size_t)q * b, counts[q], out);
+  }
+  gzb_result added[kMaxResults];
+  for (uint32_t q = 0; q < number_queries; ++q) {
+    if (chunk_counts[q] == 0) continue;  // nothing added: the row stays
+    std::copy(chunk_results + (size_t)q * b, chunk_results + (size_t)q * b + chunk_counts[q],
+              added);
+    counts[q] = merge_row(p, added, chunk_counts[q], results + (size_t)q * b, counts[q]);
   }
   return GZB_OK;
 }

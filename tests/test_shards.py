@@ -19,7 +19,7 @@ N_QUERIES = 40
 def _params():
     # several results per subject, so containment decides as well as the limit
     p = P.make_params(max_number_results=10)
-    p["max_number_one_subject_results"] = 3
+    p["max_number_one_subject_results"] = 8
     return p
 
 
@@ -123,6 +123,45 @@ def test_chunk_lists_merged_in_order_equal_the_running_merge(oracle):
     # one process holding every chunk: the exchange is the identity
     sh = S.ChunkShards()
     _same(S.merge_in_order(params, sh.exchange(params, N_CHUNKS, N_QUERIES, local)), exp)
+
+
+def test_merge_of_raw_candidates_is_add_results(oracle):
+    """Raw candidates crowded into a few subjects (up to 32 kept per
+    subject, so the per-subject start lists grow long and, keyed by query
+    start but placed by database start, unsorted) merged into empty lists
+    give the oracle's AddResults exactly."""
+    from gzb import native as N
+    params = P.make_params(max_number_results=32)
+    params["max_number_one_subject_results"] = 32
+    db = W.make_database(3, 77, median=400)
+    b = 32
+    n_cases = 300
+    counts = np.zeros(n_cases, np.uint32)
+    records = np.zeros(n_cases * b, N.RESULT_DTYPE)
+    added_counts = np.zeros(n_cases, np.uint32)
+    added = np.zeros(n_cases * b, N.RESULT_DTYPE)
+    expected = []
+    for case in range(n_cases):
+        rng = np.random.default_rng(5000 + case)
+        n = int(rng.integers(1, b + 1))
+        subj = rng.integers(0, db.number_sequences, n)
+        first = db.offsets[subj].astype(np.int64)
+        sd = first + rng.integers(0, 60, n)
+        ed = sd + rng.integers(0, 40, n)
+        sq = rng.integers(0, 120, n)  # query starts unrelated to database starts
+        r = np.zeros(n, N.RESULT_DTYPE)
+        r["chunk_id"] = 3
+        r["subject_id"] = subj
+        r["score"] = rng.integers(30, 33, n)
+        r["start_d"], r["end_d"], r["start_q"] = sd, ed, sq
+        r["end_q"] = sq + (ed - sd)
+        added_counts[case] = n
+        added[case * b:case * b + n] = r
+        expected.append(oracle.add_results(params, db, r, []))
+    N.merge_chunk_results(params, added_counts, added, counts, records)
+    exp = _rows(params, expected)
+    _same((counts, records), exp)
+    assert exp[0].min() < exp[0].max()  # containment rejected some, not all
 
 
 def test_merge_refuses_rows_over_capacity_and_mixed_chunks(oracle):
