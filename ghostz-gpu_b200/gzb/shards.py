@@ -5,9 +5,10 @@ The path's one exchange step: the reference's chunk loop
 into the per-query top-b lists with AlignerCommon::AddResults
 (src/aligner_common.h:147-274).  Here rank r searches chunks r, r + N,
 r + 2N, ... with its results reset before each chunk, the per-chunk lists
-are all-gathered (NCCL between GPUs, gloo between CPU processes), and every
-rank merges them in chunk order with gzb_merge_chunk_results, which gives
-exactly the lists of one engine searching every chunk in turn.
+are all-gathered (NCCL between GPUs, gloo between CPU processes), every
+rank merges its slice of the queries in chunk order with
+gzb_merge_chunk_results, which gives exactly the lists of one engine
+searching every chunk in turn, and the merged slices are all-gathered.
 """
 import numpy as np
 
@@ -21,15 +22,17 @@ def chunks_of(rank, world, n_chunks):
     return list(range(rank, n_chunks, world))
 
 
-def merge_in_order(params, lists):
+def merge_in_order(params, lists, q0=0, q1=None):
     """lists[c] = (counts, records) of chunk c alone; returns the running
-    merge of all of them in chunk order."""
+    merge of all of them in chunk order, for queries q0 .. q1 - 1."""
     b = int(params["max_number_results"])
-    nq = len(lists[0][0])
-    counts = np.zeros(nq, np.uint32)
-    records = np.zeros(nq * b, N.RESULT_DTYPE)
+    q1 = len(lists[0][0]) if q1 is None else q1
+    counts = np.zeros(q1 - q0, np.uint32)
+    records = np.zeros((q1 - q0) * b, N.RESULT_DTYPE)
     for chunk_counts, chunk_records in lists:
-        N.merge_chunk_results(params, chunk_counts, chunk_records, counts, records)
+        N.merge_chunk_results(params, np.ascontiguousarray(chunk_counts[q0:q1]),
+                              np.ascontiguousarray(chunk_records[q0 * b:q1 * b]), counts,
+                              records)
     return counts, records
 
 
@@ -74,6 +77,36 @@ class ChunkShards:
                             row[nq:].copy().view(N.RESULT_DTYPE))
         return lists
 
+    def merged(self, params, lists):
+        """The merge of every chunk's lists in chunk order, on every rank:
+        each rank merges its own slice of the queries, and the merged slices
+        are all-gathered."""
+        if self.dist is None:
+            return merge_in_order(params, lists)
+        import torch
+        b = int(params["max_number_results"])
+        nq = len(lists[0][0])
+        per = -(-nq // self.world)
+        q0 = min(self.rank * per, nq)
+        q1 = min(q0 + per, nq)
+        counts, records = merge_in_order(params, lists, q0, q1)
+        buf = np.zeros(per + per * b * RECORD_WORDS, np.int32)
+        buf[:q1 - q0] = counts.view(np.int32)
+        buf[per:per + (q1 - q0) * b * RECORD_WORDS] = records.view(np.int32)
+        t = torch.from_numpy(buf).to(self.device)
+        outs = [torch.empty_like(t) for _ in range(self.world)]
+        self.dist.all_gather(outs, t)
+        all_counts = np.zeros(nq, np.uint32)
+        all_records = np.zeros(nq * b, N.RESULT_DTYPE)
+        for r, o in enumerate(outs):
+            a0 = min(r * per, nq)
+            a1 = min(a0 + per, nq)
+            row = o.cpu().numpy()
+            all_counts[a0:a1] = row[:a1 - a0].view(np.uint32)
+            all_records[a0 * b:a1 * b] = \
+                row[per:per + (a1 - a0) * b * RECORD_WORDS].copy().view(N.RESULT_DTYPE)
+        return all_counts, all_records
+
     def search(self, engine, params, chunks, schedule=N.SCHEDULE_BATCHED):
         """Presearch of the engine's resident queries against this rank's
         chunks (each set in turn, results reset before each), then the
@@ -86,4 +119,4 @@ class ChunkShards:
             engine.presearch(schedule)
             local[c] = engine.result_rows()
         lists = self.exchange(params, len(chunks), engine.number_queries, local)
-        return merge_in_order(params, lists)
+        return self.merged(params, lists)

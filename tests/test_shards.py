@@ -122,7 +122,12 @@ def test_chunk_lists_merged_in_order_equal_the_running_merge(oracle):
     assert not np.array_equal(rev[1].view(np.int32), exp[1].view(np.int32))
     # one process holding every chunk: the exchange is the identity
     sh = S.ChunkShards()
-    _same(S.merge_in_order(params, sh.exchange(params, N_CHUNKS, N_QUERIES, local)), exp)
+    _same(sh.merged(params, sh.exchange(params, N_CHUNKS, N_QUERIES, local)), exp)
+    # query slices merge independently
+    b = int(params["max_number_results"])
+    part = S.merge_in_order(params, [local[c] for c in range(N_CHUNKS)], 7, 23)
+    assert np.array_equal(part[0], exp[0][7:23])
+    assert np.array_equal(part[1].view(np.int32), exp[1][7 * b:23 * b].view(np.int32))
 
 
 def test_merge_of_raw_candidates_is_add_results(oracle):
@@ -202,7 +207,7 @@ def _rank(rank, world, port, out):
         sh = S.ChunkShards(dist, "cpu")
         mine = S.chunks_of(rank, world, N_CHUNKS)
         local = _chunk_lists(O.Oracle(), params, chunks, mine)
-        merged = S.merge_in_order(params, sh.exchange(params, N_CHUNKS, N_QUERIES, local))
+        merged = sh.merged(params, sh.exchange(params, N_CHUNKS, N_QUERIES, local))
         out.put((rank, mine, merged[0], merged[1].view(np.int32)))
     finally:
         dist.destroy_process_group()
