@@ -310,3 +310,46 @@ extern "C" int gzb_index_blob_from_reference(const gzb_params *params, const voi
   }
   return GZB_OK;
 }
+
+// The `.scp` file of a chunk (SeedSearcherDatabaseParameters::
+// SaveCommonParameters, src/seed_searcher_database_parameters.cpp:378-387,
+// written by DatabaseChunk::SaveSeedSearcherCommonParameters,
+// src/database_chunk.h:449-458): uint8 delimiter, uint32 subsequence
+// length, the similarity code map, the hash function.
+extern "C" int gzb_params_from_reference_common(const void *scp, uint64_t scp_bytes,
+                                                gzb_params *params) {
+  GZB_CHECK(scp && params, GZB_ERR_INVALID, "null argument");
+  Reader r{(const uint8_t *)scp, scp_bytes, 0, true};
+  uint8_t delimiter = 0;
+  uint32_t L = 0;
+  std::vector<uint8_t> sim_map;
+  RefHash h;
+  r.get(&delimiter) && r.get(&L) && r.get_vector(&sim_map) && read_hash(r, &h);
+  GZB_CHECK(r.ok && r.at == scp_bytes, GZB_ERR_INVALID,
+            "not a seed-searcher common parameter file (%s at byte %llu of %llu)",
+            r.ok ? "trailing bytes" : "stream ends early", (unsigned long long)r.at,
+            (unsigned long long)scp_bytes);
+  GZB_CHECK(delimiter < 32 && L >= 1 && L <= 16 && !sim_map.empty() && sim_map.size() <= 32 &&
+                h.map.size() == sim_map.size() && h.max_code >= 1 && h.max_code <= 32 &&
+                h.scores.size() == (size_t)h.max_code + 1 && h.scores[0] == 0 &&
+                h.max_length >= 1 && h.max_length <= 16,
+            GZB_ERR_INVALID, "common parameter file out of range");
+  for (uint8_t c : h.map)
+    GZB_CHECK(c >= 1, GZB_ERR_INVALID, "hash code map entry 0 (codes are stored plus one)");
+  gzb_params &p = *params;
+  p.delimiter = delimiter;
+  p.subsequence_length = (int32_t)L;
+  p.map_size = (int32_t)sim_map.size();
+  memset(p.similarity_code_map, 0, sizeof(p.similarity_code_map));
+  memset(p.hash_code_map, 0, sizeof(p.hash_code_map));
+  memset(p.code_scores, 0, sizeof(p.code_scores));
+  for (size_t i = 0; i < sim_map.size(); ++i) {
+    p.similarity_code_map[i] = sim_map[i];
+    p.hash_code_map[i] = (uint8_t)(h.map[i] - 1);
+  }
+  p.max_indexing_code = h.max_code - 1;
+  for (int c = 0; c + 1 < (int)h.scores.size(); ++c) p.code_scores[c] = h.scores[c + 1];
+  p.seed_threshold = h.threshold;
+  p.max_hash_length = (int32_t)h.max_length;
+  return GZB_OK;
+}

@@ -142,6 +142,7 @@ def _declare(L):
         "gzb_index_blob_from_reference": [V, V, C.c_uint64, V, C.c_uint64, V, U32, V,
                                           C.c_uint64, V],
         "gzb_merge_chunk_results": [V, U32, V, V, V, V],
+        "gzb_params_from_reference_common": [V, C.c_uint64, V],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -617,6 +618,17 @@ def merge_chunk_results(params, chunk_counts, chunk_records, counts, records):
         assert a.dtype == dt and a.flags.c_contiguous and len(a) == n
     check(lib().gzb_merge_chunk_results(C.c_void_p(rec.ctypes.data), nq, hptr(chunk_counts),
                                         hptr(chunk_records), hptr(counts), hptr(records)))
+
+
+def params_from_reference_common(scp, params):
+    """A copy of `params` with the seed-index fields the reference's .scp
+    file (its bytes) stores; host only."""
+    rec = np.array([params], dtype=params.dtype)
+    scp = np.ascontiguousarray(np.frombuffer(scp, np.uint8) if isinstance(scp, bytes) else scp,
+                               dtype=np.uint8)
+    check(lib().gzb_params_from_reference_common(hptr(scp), scp.nbytes,
+                                                 C.c_void_p(rec.ctypes.data)))
+    return rec[0]
 
 
 def index_blob_from_reference(params, sdp, db):

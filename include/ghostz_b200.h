@@ -290,6 +290,15 @@ int gzb_index_blob_from_reference(const gzb_params *params, const void *sdp, uin
                                   const uint8_t *codes, uint64_t length, const uint32_t *offsets,
                                   uint32_t number_sequences, void *blob, uint64_t capacity,
                                   uint64_t *blob_bytes);
+/* The seed-index parameters stored in the reference's `.scp` file of a
+ * database (SeedSearcherDatabaseParameters::SaveCommonParameters,
+ * src/seed_searcher_database_parameters.cpp:378-387) written into *params:
+ * delimiter, subsequence_length, map_size, similarity_code_map,
+ * hash_code_map, max_indexing_code, code_scores, seed_threshold and
+ * max_hash_length.  The other fields are left as the caller set them (the
+ * score matrix, gap costs, -b / -v, clustering, min_hash_length and the
+ * distance thresholds derived from subsequence_length).  Host only. */
+int gzb_params_from_reference_common(const void *scp, uint64_t scp_bytes, gzb_params *params);
 
 /* Stored database chunks, for streaming a database of many chunks
  * (the reference's chunk loop with its preloading thread,

@@ -391,6 +391,8 @@ class Reference:
         L.gzr_db_index_max_mismatches.argtypes = [C.c_void_p]
         L.gzr_db_index_save.argtypes = [C.c_void_p, u8p, C.c_size_t]
         L.gzr_db_index_save.restype = C.c_size_t
+        L.gzr_db_index_save_common.argtypes = [C.c_void_p, u8p, C.c_size_t]
+        L.gzr_db_index_save_common.restype = C.c_size_t
         L.gzr_ungapped_karlin.argtypes = [C.c_void_p, u8p, C.c_uint32, C.POINTER(C.c_float),
                                           C.POINTER(C.c_float), C.POINTER(C.c_float)]
         L.gzr_normalized_cutoff_to_nominal.argtypes = [C.c_float, C.c_float, C.c_float]
@@ -497,6 +499,13 @@ class Reference:
         n = self.L.gzr_db_index_save(C.c_void_p(h), None, 0)
         out = np.zeros(n, np.uint8)
         self.L.gzr_db_index_save(C.c_void_p(h), _p(out, u8p), n)
+        return out
+
+    def save_common(self, h):
+        """The bytes of the database's .scp file the reference writes for h."""
+        n = self.L.gzr_db_index_save_common(C.c_void_p(h), None, 0)
+        out = np.zeros(n, np.uint8)
+        self.L.gzr_db_index_save_common(C.c_void_p(h), _p(out, u8p), n)
         return out
 
     def free_index(self, h):

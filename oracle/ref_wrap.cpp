@@ -210,6 +210,16 @@ int gzr_db_index_max_mismatches(void *h) {
  * file (SeedSearcherDatabaseParameters::Save,
  * src/seed_searcher_database_parameters.cpp:363-376); returns its size and
  * copies up to cap bytes. */
+/* The database's common parameter file (.scp, SaveCommonParameters,
+ * src/seed_searcher_database_parameters.cpp:378-387); as gzr_db_index_save. */
+size_t gzr_db_index_save_common(void *h, uint8_t *out, size_t cap) {
+  std::ostringstream os(std::ios::binary);
+  ((gzr_db_index *)h)->params.SaveCommonParameters(os);
+  const std::string b = os.str();
+  if (out) memcpy(out, b.data(), b.size() < cap ? b.size() : cap);
+  return b.size();
+}
+
 size_t gzr_db_index_save(void *h, uint8_t *out, size_t cap) {
   std::ostringstream os(std::ios::binary);
   ((gzr_db_index *)h)->params.Save(os);

@@ -147,3 +147,31 @@ def test_golden_file_converts_to_the_oracle_index(native, oracle):
         assert np.array_equal(got[name], exp[name]), name
     assert len(got["rep_positions"]) > 1000 and len(got["member_positions"]) > 1000
     assert np.array_equal(got["rep_windows"], windows(params, db.codes, got["rep_positions"]))
+
+
+def test_common_parameter_file_gives_the_seed_parameters(native, reference):
+    """The reference's .scp file of a database yields the seed-index fields
+    of the parameters it was built with; the caller's other fields stay."""
+    for kw in ({}, {"subsequence_length": 12, "seed_threshold": 35}):
+        params = P.make_params(**kw)
+        db = W.make_database(40, 65, median=80)
+        h = reference.db_index(params, db.codes)
+        try:
+            scp = reference.save_common(h)
+        finally:
+            reference.free_index(h)
+        blank = P.make_params()
+        for f in ("delimiter", "subsequence_length", "map_size", "max_indexing_code",
+                  "seed_threshold", "max_hash_length"):
+            blank[f] = 0
+        for f in ("similarity_code_map", "hash_code_map", "code_scores"):
+            blank[f] = 0
+        blank["gap_open"] = 7
+        got = native.params_from_reference_common(scp, blank)
+        for f in ("delimiter", "subsequence_length", "map_size", "max_indexing_code",
+                  "seed_threshold", "max_hash_length", "similarity_code_map", "hash_code_map",
+                  "code_scores"):
+            assert np.array_equal(got[f], params[f]), f
+        assert got["gap_open"] == 7
+        with pytest.raises(native.GzbError):
+            native.params_from_reference_common(scp[:-1], blank)
