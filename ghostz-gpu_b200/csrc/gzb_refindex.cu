@@ -98,6 +98,26 @@ bool read_dense(Reader &r, RefDense<V> *d) {
   return r.get_vector(&d->offsets) && r.get_vector(&d->values);
 }
 
+// (key, index) pairs sorted by key: two counting passes over 16-bit digits
+// (keys are distinct, so the order among equal keys never matters).
+void sort_by_key(std::vector<std::pair<uint32_t, uint32_t>> *v) {
+  std::vector<std::pair<uint32_t, uint32_t>> tmp(v->size());
+  std::vector<uint64_t> count(1 << 16);
+  for (int pass = 0; pass < 2; ++pass) {
+    const int shift = 16 * pass;
+    std::fill(count.begin(), count.end(), 0);
+    for (const auto &kv : *v) ++count[(kv.first >> shift) & 0xFFFF];
+    uint64_t sum = 0;
+    for (auto &c : count) {
+      const uint64_t n = c;
+      c = sum;
+      sum += n;
+    }
+    for (const auto &kv : *v) tmp[count[(kv.first >> shift) & 0xFFFF]++] = kv;
+    v->swap(tmp);
+  }
+}
+
 // The pairs sorted by key, each key's value range checked; false if the
 // index is inconsistent.
 template <class V>
@@ -107,7 +127,7 @@ bool sorted_ranges(const RefDense<V> &d, std::vector<std::pair<uint32_t, uint32_
   for (uint64_t i = 0; i < nk; ++i)
     if (d.offsets[i] > d.offsets[i + 1]) return false;
   *out = d.keys;
-  std::sort(out->begin(), out->end());
+  sort_by_key(out);
   std::vector<uint8_t> seen(nk, 0);
   for (uint64_t i = 0; i < nk; ++i) {
     const auto &kv = (*out)[i];
