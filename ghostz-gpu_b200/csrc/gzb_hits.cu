@@ -12,7 +12,9 @@
 // score is computed in float (Nominal2Normalized, :23-27).
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
+#include <string>
 
 #include "ghostz_b200.h"
 #include "gzb_common.h"
@@ -104,4 +106,64 @@ extern "C" uint32_t gzb_translated_real_end(uint32_t position, uint32_t dna_leng
   const uint32_t f = (position - 1) / base;
   return f < 3 ? gzb_translated_real_start(position, dna_length) + 2
                : gzb_translated_real_start(position, dna_length) - 2;
+}
+
+// The tabular lines of AlignerCommon::WriteOutput (src/aligner_common.h:
+// 344-394): query and subject names, identity %, alignment length,
+// mismatches, gap openings, query start and end (a read's bases for a
+// translated query), subject start and end (1-based in the subject),
+// E-value and normalized score, numbers as a C++ stream prints them (six
+// significant digits).  The identity is 1 - (differences / length) with the
+// division in float.  Rows with alignment_length 0 (results no build step
+// filled) are skipped.
+extern "C" int gzb_write_hit_table(uint32_t number_queries, uint32_t stride,
+                                   const uint32_t *counts, const gzb_alignment *alignments,
+                                   const char *const *query_names,
+                                   const char *const *subject_names, uint32_t number_subjects,
+                                   const uint32_t *db_offsets, uint64_t db_length,
+                                   uint64_t db_sequences, const uint32_t *query_real_lengths,
+                                   const uint32_t *dna_lengths, float lambda, float k,
+                                   double alpha, double beta, char *out, uint64_t capacity,
+                                   uint64_t *written) {
+  GZB_CHECK(written && (number_queries == 0 || (counts && alignments && query_names &&
+                                                subject_names && db_offsets &&
+                                                query_real_lengths)),
+            GZB_ERR_INVALID, "null argument");
+  std::string text;
+  char buf[160];
+  for (uint32_t q = 0; q < number_queries; ++q) {
+    GZB_CHECK(counts[q] <= stride, GZB_ERR_INVALID, "query %u: %u results in rows of %u", q,
+              counts[q], stride);
+    if (counts[q] == 0) continue;
+    const uint64_t space =
+        gzb_search_space(query_real_lengths[q], db_length, db_sequences, lambda, k, alpha, beta);
+    for (uint32_t i = 0; i < counts[q]; ++i) {
+      const gzb_alignment &a = alignments[(size_t)q * stride + i];
+      if (a.alignment_length == 0) continue;
+      GZB_CHECK(a.subject_id >= 0 && (uint32_t)a.subject_id < number_subjects, GZB_ERR_INVALID,
+                "query %u: subject %d out of range", q, a.subject_id);
+      const float diff = (float)(a.mismatches + a.gap_openings + a.gap_extensions);
+      const double identity = (1.0 - (double)(diff / (float)a.alignment_length)) * 100;
+      uint32_t sq = a.start_q, eq = a.end_q;
+      if (dna_lengths) {
+        sq = gzb_translated_real_start(sq, dna_lengths[q]);
+        eq = gzb_translated_real_end(eq, dna_lengths[q]);
+      }
+      const uint32_t first = db_offsets[a.subject_id] - 1;
+      text += query_names[q];
+      text += '\t';
+      text += subject_names[a.subject_id];
+      snprintf(buf, sizeof(buf), "\t%g\t%u\t%u\t%u\t%u\t%u\t%u\t%u\t%g\t%g\n", identity,
+               a.alignment_length, a.mismatches, a.gap_openings, sq, eq, a.start_d - first,
+               a.end_d - first, gzb_evalue(a.score, space, lambda, k),
+               (double)gzb_bit_score(a.score, lambda, k));
+      text += buf;
+    }
+  }
+  *written = text.size();
+  if (!out) return GZB_OK;
+  GZB_CHECK(capacity >= text.size(), GZB_ERR_INVALID, "hit table needs %llu bytes",
+            (unsigned long long)text.size());
+  memcpy(out, text.data(), text.size());
+  return GZB_OK;
 }

@@ -143,6 +143,8 @@ def _declare(L):
                                           C.c_uint64, V],
         "gzb_merge_chunk_results": [V, U32, V, V, V, V],
         "gzb_params_from_reference_common": [V, C.c_uint64, V],
+        "gzb_write_hit_table": [U32, U32, V, V, V, V, U32, V, C.c_uint64, C.c_uint64, V, V,
+                                C.c_float, C.c_float, C.c_double, C.c_double, V, C.c_uint64, V],
     }
     for name, args in sigs.items():
         f = getattr(L, name)
@@ -875,35 +877,34 @@ def bit_score(score, karlin):
 def hit_table(results, query_names, subject_names, db_offsets, db_length, db_sequences,
               query_real_lengths, dna_lengths=None, karlin=None):
     """The `aln` tabular output (AlignerCommon::WriteOutput,
-    src/aligner_common.h:344-394) of build_alignments() results of one
-    chunk: per result query name, subject name, identity %, alignment
-    length, mismatches, gap openings, query start and end (bases of the read
-    for translated queries), subject start and end, E-value and normalized
-    score, tab separated, numbers as C++ streams print them.  db_offsets:
-    the chunk's first-residue offsets; db_length / db_sequences: residues
-    and sequences of the whole database; query_real_lengths: residues (a
-    read's bases / 3 for a translated query); dna_lengths: the reads' bases
-    for translated queries (None for protein queries)."""
+    src/aligner_common.h:344-394) of build_alignments() results, written by
+    the library (gzb_write_hit_table): per result query name, subject name,
+    identity %, alignment length, mismatches, gap openings, query start and
+    end (bases of the read for translated queries), subject start and end,
+    E-value and normalized score, tab separated, numbers as C++ streams
+    print them; returns the lines.  db_offsets: the chunk's first-residue
+    offsets; db_length / db_sequences: residues and sequences of the whole
+    database; query_real_lengths: residues (a read's bases / 3 for a
+    translated query); dna_lengths: the reads' bases for translated queries
+    (None for protein queries)."""
     if karlin is None:
         karlin = gapped_karlin_parameters()
-    L = lib()
-    lines = []
-    for qi, rows in enumerate(results):
-        space = search_space(query_real_lengths[qi], db_length, db_sequences, karlin)
-        for r in rows:
-            n_diff = np.float32(int(r["mismatches"]) + int(r["gap_openings"]) +
-                                int(r["gap_extensions"]))
-            identity = (1.0 - float(n_diff / np.float32(int(r["alignment_length"])))) * 100
-            sq, eq = int(r["start_q"]), int(r["end_q"])
-            if dna_lengths is not None:
-                sq = int(L.gzb_translated_real_start(sq, int(dna_lengths[qi])))
-                eq = int(L.gzb_translated_real_end(eq, int(dna_lengths[qi])))
-            first = int(db_offsets[int(r["subject_id"])]) - 1
-            lines.append("\t".join([
-                query_names[qi], subject_names[int(r["subject_id"])], "%g" % identity,
-                str(int(r["alignment_length"])), str(int(r["mismatches"])),
-                str(int(r["gap_openings"])), str(sq), str(eq),
-                str(int(r["start_d"]) - first), str(int(r["end_d"]) - first),
-                "%g" % evalue(int(r["score"]), space, karlin),
-                "%g" % bit_score(int(r["score"]), karlin)]))
-    return lines
+    lam, k, _, alpha, beta = karlin
+    nq = len(results)
+    stride = max([len(r) for r in results] + [1])
+    counts = np.array([len(r) for r in results], np.uint32)
+    rows = np.zeros(nq * stride, ALIGNMENT_DTYPE)
+    for i, r in enumerate(results):
+        rows[i * stride:i * stride + len(r)] = r
+    qn = (C.c_char_p * max(nq, 1))(*[n.encode() for n in query_names[:nq]])
+    sn = (C.c_char_p * max(len(subject_names), 1))(*[n.encode() for n in subject_names])
+    offs = np.ascontiguousarray(db_offsets, dtype=np.uint32)
+    real = np.ascontiguousarray(query_real_lengths, dtype=np.uint32)
+    dna = None if dna_lengths is None else np.ascontiguousarray(dna_lengths, dtype=np.uint32)
+    args = [nq, stride, hptr(counts), hptr(rows), qn, sn, len(subject_names), hptr(offs),
+            int(db_length), int(db_sequences), hptr(real), hptr(dna), lam, k, alpha, beta]
+    n = C.c_uint64()
+    check(lib().gzb_write_hit_table(*args, None, 0, C.byref(n)))
+    out = C.create_string_buffer(max(int(n.value), 1))
+    check(lib().gzb_write_hit_table(*args, out, n.value, C.byref(n)))
+    return out.raw[:n.value].decode().splitlines()

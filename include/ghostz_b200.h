@@ -635,6 +635,25 @@ double gzb_evalue(int32_t score, uint64_t search_space, float lambda, float k);
 float gzb_bit_score(int32_t score, float lambda, float k);
 uint32_t gzb_translated_real_start(uint32_t position, uint32_t dna_length);
 uint32_t gzb_translated_real_end(uint32_t position, uint32_t dna_length);
+/* The tabular lines AlignerCommon::WriteOutput (src/aligner_common.h:344-394)
+ * prints for the alignment records of gzb_engine_build_alignments (counts,
+ * rows of `stride` records per query; rows with alignment_length 0 are
+ * skipped), one '\n'-terminated line per result: query name, subject name,
+ * identity %, alignment length, mismatches, gap openings, query start and
+ * end (read bases when dna_lengths is given), subject start and end,
+ * E-value, normalized score.  db_offsets: the chunk's first-residue offsets
+ * (subject_id indexes them and subject_names); db_length / db_sequences:
+ * residues and sequences of the whole database; query_real_lengths as for
+ * gzb_search_space; lambda, k, alpha, beta from
+ * gzb_gapped_karlin_parameters.  *written receives the bytes of the text;
+ * out = NULL asks only for it.  Host only. */
+int gzb_write_hit_table(uint32_t number_queries, uint32_t stride, const uint32_t *counts,
+                        const gzb_alignment *alignments, const char *const *query_names,
+                        const char *const *subject_names, uint32_t number_subjects,
+                        const uint32_t *db_offsets, uint64_t db_length, uint64_t db_sequences,
+                        const uint32_t *query_real_lengths, const uint32_t *dna_lengths,
+                        float lambda, float k, double alpha, double beta, char *out,
+                        uint64_t capacity, uint64_t *written);
 
 #ifdef __cplusplus
 }
