@@ -175,3 +175,60 @@ def test_common_parameter_file_gives_the_seed_parameters(native, reference):
         assert got["gap_open"] == 7
         with pytest.raises(native.GzbError):
             native.params_from_reference_common(scp[:-1], blank)
+
+
+def test_c_caller_converts_the_golden_file(tmp_path):
+    """A plain C program (the reference host's side of the boundary) reads
+    the committed .sdp file, converts it through the C ABI and finds the
+    blob's counts: the host entry points need nothing but the header and
+    the library."""
+    import os
+    import subprocess
+    from gzb import build as B
+    g = _golden()
+    params = P.make_params()
+    db = g.chunk()
+    codes, offsets = tmp_path / "codes.bin", tmp_path / "offsets.bin"
+    prm = tmp_path / "params.bin"
+    db.codes.astype(np.uint8).tofile(codes)
+    db.offsets.astype(np.uint32).tofile(offsets)
+    np.array([params]).tofile(prm)
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "convert.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include <stdlib.h>
+#include "ghostz_b200.h"
+static void *slurp(const char *path, long *n) {
+  FILE *f = fopen(path, "rb"); void *p; fseek(f, 0, SEEK_END); *n = ftell(f);
+  fseek(f, 0, SEEK_SET); p = malloc(*n ? *n : 1); fread(p, 1, *n, f); fclose(f); return p;
+}
+int main(int argc, char **argv) {
+  long ns, nc, no, np_;
+  void *sdp = slurp(argv[1], &ns);
+  unsigned char *codes = slurp(argv[2], &nc);
+  unsigned int *offsets = slurp(argv[3], &no);
+  gzb_params *p = slurp(argv[4], &np_);
+  uint64_t n = 0;
+  unsigned int nseq = (unsigned int)(no / 4 - 1);
+  if (np_ != (long)sizeof(gzb_params)) return 3;
+  if (gzb_index_blob_from_reference(p, sdp, ns, codes, nc, offsets, nseq, 0, 0, &n)) return 1;
+  uint64_t *blob = malloc(n);
+  if (gzb_index_blob_from_reference(p, sdp, ns, codes, nc, offsets, nseq, blob, n, &n)) return 2;
+  /* header: magic, fingerprint, length, sequences, check, then the counts */
+  printf("%llu %llu %llu %llu %llu\n", (unsigned long long)n, (unsigned long long)blob[2],
+         (unsigned long long)blob[3], (unsigned long long)blob[8], (unsigned long long)blob[9]);
+  return 0;
+}
+''')
+    exe = tmp_path / "convert"
+    subprocess.check_call(["gcc", "-std=c99", "-I", os.path.join(root, "include"), str(src),
+                           "-o", str(exe), B.LIB, "-Wl,-rpath," + os.path.dirname(B.LIB)])
+    out = subprocess.run([str(exe), g.FIXTURE, str(codes), str(offsets), str(prm)],
+                         capture_output=True, text=True, check=True).stdout.split()
+    from gzb import native as N
+    with open(g.FIXTURE, "rb") as f:
+        blob = N.index_blob_from_reference(params, f.read(), db)
+    got = parse_blob(blob)
+    assert [int(x) for x in out] == [len(blob), len(db.codes), db.number_sequences,
+                                     len(got["rep_positions"]), len(got["member_positions"])]
