@@ -232,3 +232,41 @@ def test_two_gloo_ranks_exchange_their_chunks(oracle):
     for _, _, counts, words in got:
         assert np.array_equal(counts, exp[0])
         assert np.array_equal(words, exp[1].view(np.int32))
+
+
+class _FakeEngine:
+    """The engine calls ChunkShards.search makes, answered on the host: a
+    chunk's lists are its candidates added into empty lists (what the
+    engine holds after a reset and one presearch of that chunk)."""
+
+    def __init__(self, oracle, params):
+        self.oracle, self.params = oracle, params
+        self.number_queries = N_QUERIES
+        self.calls = []
+
+    def set_database(self, db, chunk_id=0):
+        self.db, self.chunk = db, chunk_id
+        self.calls.append(("set_database", chunk_id))
+
+    def reset_results(self):
+        self.calls.append(("reset_results",))
+
+    def presearch(self, schedule):
+        self.calls.append(("presearch", schedule))
+        self.rows = _rows(self.params, [
+            self.oracle.add_results(self.params, self.db, _raw(self.db, self.chunk, q), [])
+            for q in range(N_QUERIES)])
+
+    def result_rows(self):
+        return self.rows
+
+
+def test_search_drives_the_engine_chunk_by_chunk(oracle):
+    from gzb import shards as S
+    params = _params()
+    chunks = _chunks()
+    e = _FakeEngine(oracle, params)
+    got = S.ChunkShards().search(e, params, chunks, schedule=1)
+    _same(got, _expected(oracle, params, chunks))
+    assert e.calls == [c for k in range(N_CHUNKS)
+                       for c in (("set_database", k), ("reset_results",), ("presearch", 1))]
