@@ -138,6 +138,11 @@ bool sorted_ranges(const RefDense<V> &d, std::vector<std::pair<uint32_t, uint32_
   return true;
 }
 
+// a representative as the file stores it: (cluster id, position)
+struct RefRep {
+  uint32_t cluster, position;
+};
+
 struct RefPerfect {
   uint32_t max_key = 0;
   std::vector<uint32_t> offsets, values;
@@ -201,7 +206,7 @@ extern "C" int gzb_index_blob_from_reference(const gzb_params *params, const voi
   uint32_t L = 0;
   RefHash seq_hash, clu_hash;
   RefDense<uint32_t> nc;
-  RefDense<std::pair<uint32_t, uint32_t>> reps;
+  RefDense<RefRep> reps;
   RefPerfect members;
   float rate = 0.f;
   std::vector<uint8_t> sim_map;
@@ -244,8 +249,8 @@ extern "C" int gzb_index_blob_from_reference(const gzb_params *params, const voi
     for (uint32_t v : members.values)
       GZB_CHECK(v < length, GZB_ERR_INVALID, "member position %u outside the chunk", v);
     for (const auto &cp : reps.values)
-      GZB_CHECK(cp.second < length, GZB_ERR_INVALID,
-                "representative position %u outside the chunk", cp.second);
+      GZB_CHECK(cp.position < length, GZB_ERR_INVALID,
+                "representative position %u outside the chunk", cp.position);
   }
 
   // the blob: keys ascending, each key's values in the file's order; cluster
@@ -264,8 +269,8 @@ extern "C" int gzb_index_blob_from_reference(const gzb_params *params, const voi
     h.n_rep_keys = rep_keys.size();
     h.n_reps = reps.values.size();
     for (const auto &cp : reps.values)
-      if (cp.first <= members.max_key)
-        n_members += members.offsets[cp.first + 1] - members.offsets[cp.first];
+      if (cp.cluster <= members.max_key)
+        n_members += members.offsets[cp.cluster + 1] - members.offsets[cp.cluster];
     h.n_members = n_members;
   }
   GZB_CHECK(h.n_nc_values < (1ull << 32) && h.n_reps < (1ull << 32) && n_members < (1ull << 32),
@@ -310,7 +315,7 @@ extern "C" int gzb_index_blob_from_reference(const gzb_params *params, const voi
       const uint32_t b = reps.offsets[kv.second], e = reps.offsets[kv.second + 1];
       keys[k] = kv.first;
       for (uint32_t i = b; i < e; ++i, ++rep) {
-        const uint32_t cid = reps.values[i].first, at_pos = reps.values[i].second;
+        const uint32_t cid = reps.values[i].cluster, at_pos = reps.values[i].position;
         rpos[rep] = at_pos;
         cids[rep] = rep;
         wins[rep] = host_window(p, codes, length, at_pos);
