@@ -22,6 +22,10 @@
 #include <stdint.h>
 #include <stddef.h>
 
+#include <istream>
+#include <iterator>
+#include <vector>
+
 #include "ghostz_b200.h"
 
 namespace ghostz_b200 {
@@ -162,6 +166,31 @@ class GappedExtenderGpu {
   GappedExtenderGpu &operator=(const GappedExtenderGpu &);
   gzb_gapped_extender *h_;
 };
+
+// The counterpart of SeedSearcherDatabaseParameters::Build(sequence,
+// length, istream) (src/seed_searcher_database_parameters.cpp:321-337): a
+// chunk and the index the reference's `db` command saved for it (the
+// chunk's `.sdp` stream) made resident in `engine`, the index converted on
+// the host instead of being rebuilt.  offsets: first residue of each of the
+// number_sequences sequences, then the chunk length.
+inline int LoadChunkWithReferenceIndex(gzb_engine *engine, const gzb_params &params,
+                                       int32_t chunk_id, const Code *sequence,
+                                       uint64_t length, const uint32_t *offsets,
+                                       uint32_t number_sequences, std::istream &sdp,
+                                       cudaStream_t stream) {
+  std::vector<char> bytes((std::istreambuf_iterator<char>(sdp)),
+                          std::istreambuf_iterator<char>());
+  uint64_t n = 0;
+  int rc = gzb_index_blob_from_reference(&params, bytes.data(), bytes.size(), sequence, length,
+                                         offsets, number_sequences, 0, 0, &n);
+  if (rc) return rc;
+  std::vector<uint8_t> blob(n);
+  rc = gzb_index_blob_from_reference(&params, bytes.data(), bytes.size(), sequence, length,
+                                     offsets, number_sequences, blob.data(), n, &n);
+  if (rc) return rc;
+  return gzb_engine_set_database_with_index(engine, chunk_id, sequence, length, offsets,
+                                            number_sequences, blob.data(), n, (void *)stream);
+}
 
 }  // namespace ghostz_b200
 

@@ -75,6 +75,9 @@ def test_cpp_adapters_compile_and_link(tmp_path):
         '  u.ExtendWithTriggerAsync(0, p, p, p, f, p, p, p, f, i, s);\n'
         '  return g.ExtendOneSideScoreOnlyAsync(0, true, p, p, i, p, p, i, s);\n'
         '}\n'
+        'int load(gzb_engine *e, const gzb_params &prm, std::istream &in, cudaStream_t s) {\n'
+        '  return LoadChunkWithReferenceIndex(e, prm, 0, 0, 0, 0, 0, in, s);\n'
+        '}\n'
         'int main() { return 0; }\n')
     exe = tmp_path / "use"
     subprocess.check_call([
