@@ -2841,7 +2841,8 @@ extern "C" int gzb_engine_build_alignments(gzb_engine *e, uint32_t *counts,
   a.delim = e->params.delimiter;
   a.gap_open = e->params.gap_open;
   a.gap_ext = e->params.gap_extension;
-  a.cutoff = e->params.gapped_cutoff;
+  // the build results step's own X-drop (src/aligner_gpu.cpp:254-256)
+  a.cutoff = e->params.result_gapped_cutoff;
   // band columns per side, then the DP's storage per side
   GZB_TRY(e->tb_cols.ensure(8 * (n_sides + 1)));
   tb_band_kernel<<<grid1(n_sides, 256), 256, 0, s>>>(a, n_sides, e->tb_cols.as<uint64_t>());

@@ -10,11 +10,13 @@
 // ln K taken in float; the E-value multiplies the search space by K in float
 // before the double exponential (Nominal2EValue, :44-48); the normalized
 // score is computed in float (Nominal2Normalized, :23-27).
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "ghostz_b200.h"
 #include "gzb_common.h"
@@ -106,6 +108,60 @@ extern "C" uint32_t gzb_translated_real_end(uint32_t position, uint32_t dna_leng
   const uint32_t f = (position - 1) / base;
   return f < 3 ? gzb_translated_real_start(position, dna_length) + 2
                : gzb_translated_real_start(position, dna_length) - 2;
+}
+
+namespace {
+// One record with the coordinates AlignerCommon::BuildResult leaves in a
+// Result (src/aligner_common.h:326-340): the query's real start and end, the
+// subject-relative database start and end.
+struct FinalRow {
+  gzb_alignment a;
+  uint32_t q_start, q_end, d_start, d_end;
+};
+
+// AlignerCommon::AlignmentComp(...) > 0 (src/aligner_common.cpp:12-52): a
+// comes first on a higher score, then a longer query span, then a longer
+// subject span, then a smaller subject start; equal subject starts compare
+// as "not first" both ways.
+bool result_greater(const FinalRow &x, const FinalRow &y) {
+  if (x.a.score != y.a.score) return x.a.score > y.a.score;
+  const uint32_t xq = x.q_end - x.q_start, yq = y.q_end - y.q_start;
+  if (xq != yq) return xq > yq;
+  const uint32_t xs = x.d_end - x.d_start, ys = y.d_end - y.d_start;
+  if (xs != ys) return xs > ys;
+  return x.d_start < y.d_start;
+}
+}  // namespace
+
+extern "C" int gzb_sort_alignments(uint32_t number_queries, uint32_t stride,
+                                   const uint32_t *counts, gzb_alignment *alignments,
+                                   uint32_t number_subjects, const uint32_t *db_offsets,
+                                   const uint32_t *dna_lengths) {
+  GZB_CHECK(number_queries == 0 || (counts && alignments && db_offsets), GZB_ERR_INVALID,
+            "null argument");
+  std::vector<FinalRow> rows;
+  for (uint32_t q = 0; q < number_queries; ++q) {
+    GZB_CHECK(counts[q] <= stride, GZB_ERR_INVALID, "query %u: %u results in rows of %u", q,
+              counts[q], stride);
+    gzb_alignment *row = alignments + (size_t)q * stride;
+    rows.clear();
+    for (uint32_t i = 0; i < counts[q]; ++i) {
+      const gzb_alignment &a = row[i];
+      GZB_CHECK(a.subject_id >= 0 && (uint32_t)a.subject_id < number_subjects, GZB_ERR_INVALID,
+                "query %u: subject %d out of range", q, a.subject_id);
+      FinalRow r;
+      r.a = a;
+      r.q_start = dna_lengths ? gzb_translated_real_start(a.start_q, dna_lengths[q]) : a.start_q;
+      r.q_end = dna_lengths ? gzb_translated_real_end(a.end_q, dna_lengths[q]) : a.end_q;
+      const uint32_t first = db_offsets[a.subject_id] - 1;
+      r.d_start = a.start_d - first;
+      r.d_end = a.end_d - first;
+      rows.push_back(r);
+    }
+    std::sort(rows.begin(), rows.end(), result_greater);
+    for (uint32_t i = 0; i < counts[q]; ++i) row[i] = rows[i].a;
+  }
+  return GZB_OK;
 }
 
 // The tabular lines of AlignerCommon::WriteOutput (src/aligner_common.h:

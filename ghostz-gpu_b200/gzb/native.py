@@ -143,6 +143,7 @@ def _declare(L):
                                           C.c_uint64, V],
         "gzb_merge_chunk_results": [V, U32, V, V, V, V],
         "gzb_params_from_reference_common": [V, C.c_uint64, V],
+        "gzb_sort_alignments": [U32, U32, V, V, U32, V, V],
         "gzb_write_hit_table": [U32, U32, V, V, V, V, U32, V, C.c_uint64, C.c_uint64, V, V,
                                 C.c_float, C.c_float, C.c_double, C.c_double, V, C.c_uint64, V],
     }
@@ -872,6 +873,32 @@ def evalue(score, space, karlin):
 
 def bit_score(score, karlin):
     return float(lib().gzb_bit_score(int(score), karlin[0], karlin[1]))
+
+
+def _rows(results):
+    nq = len(results)
+    stride = max([len(r) for r in results] + [1])
+    counts = np.array([len(r) for r in results], np.uint32)
+    rows = np.zeros(nq * stride, ALIGNMENT_DTYPE)
+    for i, r in enumerate(results):
+        rows[i * stride:i * stride + len(r)] = r
+    return stride, counts, rows
+
+
+def sort_alignments(results, db_offsets, number_subjects, dna_lengths=None):
+    """Each query's alignment records (build_alignments() rows in merged
+    order) in the order the reference writes them (gzb_sort_alignments:
+    AlignerCommon::ResultGreaterScore over the printed coordinates)."""
+    nq = len(results)
+    if nq == 0:
+        return []
+    stride, counts, rows = _rows(results)
+    offs = np.ascontiguousarray(db_offsets, dtype=np.uint32)
+    dna = None if dna_lengths is None else np.ascontiguousarray(dna_lengths, dtype=np.uint32)
+    check(lib().gzb_sort_alignments(nq, stride, hptr(counts), hptr(rows), int(number_subjects),
+                                    hptr(offs), hptr(dna)))
+    rows = rows.reshape(nq, stride)
+    return [rows[i, :counts[i]].copy() for i in range(nq)]
 
 
 def hit_table(results, query_names, subject_names, db_offsets, db_length, db_sequences,

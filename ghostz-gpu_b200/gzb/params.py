@@ -141,6 +141,7 @@ PARAMS_DTYPE = np.dtype([
     ("max_number_results", "<i4"),
     ("max_number_one_subject_results", "<i4"),
     ("clustering", "<i4"),
+    ("result_gapped_cutoff", "<i4"),
 ], align=False)
 
 
@@ -162,7 +163,8 @@ def make_params(*, subsequence_length=10, seed_threshold=39, gap_open=11,
                 gap_extension=1, gapped_bits=15.0, max_number_results=10,
                 max_number_one_subject_results=1, clustering=True,
                 matrix=None, reduced_sets=DEFAULT_REDUCED_SETS,
-                gapped_cutoff=None) -> np.ndarray:
+                gapped_cutoff=None, result_gapped_bits=25.0,
+                result_gapped_cutoff=None) -> np.ndarray:
     """One record of PARAMS_DTYPE with the `aln` defaults
     (src/align_main.cpp:104-127, src/database_build_main.cpp:72-81)."""
     p = np.zeros(1, dtype=PARAMS_DTYPE)[0]
@@ -202,6 +204,11 @@ def make_params(*, subsequence_length=10, seed_threshold=39, gap_open=11,
     p["max_number_results"] = max_number_results
     p["max_number_one_subject_results"] = max_number_one_subject_results
     p["clustering"] = 1 if clustering else 0
+    # the build results step re-extends with a wider X-drop than the
+    # presearch (normalized_result_gapped_extension_cutoff, 25 bits)
+    if result_gapped_cutoff is None:
+        result_gapped_cutoff = normalized_to_nominal(result_gapped_bits, GAPPED_LAMBDA, GAPPED_K)
+    p["result_gapped_cutoff"] = result_gapped_cutoff
     return p
 
 

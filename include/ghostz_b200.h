@@ -68,6 +68,10 @@ typedef struct {
   int32_t max_number_results;    /* top-b per query (-b) */
   int32_t max_number_one_subject_results; /* per subject (-v) */
   int32_t clustering;            /* database built with -C T */
+  int32_t result_gapped_cutoff;  /* X-drop of the build results step's
+                                    traceback (25 normalized bits against 15
+                                    for the presearch, src/align_main.cpp:124-125,
+                                    src/aligner_gpu.cpp:254-256) */
 } gzb_params;
 
 /* Device sequence buffers given to the operators below hold one residue
@@ -647,6 +651,20 @@ uint32_t gzb_translated_real_end(uint32_t position, uint32_t dna_length);
  * gzb_search_space; lambda, k, alpha, beta from
  * gzb_gapped_karlin_parameters.  *written receives the bytes of the text;
  * out = NULL asks only for it.  Host only. */
+/* The last step of the build results stage before the table is written
+ * (AlignerBuildResultsThread::Run, src/aligner_build_results_thread.h:179-190):
+ * each query's alignment records reordered in place by
+ * AlignerCommon::ResultGreaterScore (src/aligner_common.h:116-121,
+ * src/aligner_common.cpp:12-52): higher score first, then the longer
+ * query span, the longer subject span, the smaller subject-relative start;
+ * spans are the uint32 differences of the printed coordinates (read bases
+ * for translated queries).  The records must be in merged-result order
+ * (the order of gzb_engine_get_results), which is the order the reference
+ * sorts from; the sort is std::sort with that comparator, as the
+ * reference's.  Arguments as for gzb_write_hit_table.  Host only. */
+int gzb_sort_alignments(uint32_t number_queries, uint32_t stride, const uint32_t *counts,
+                        gzb_alignment *alignments, uint32_t number_subjects,
+                        const uint32_t *db_offsets, const uint32_t *dna_lengths);
 int gzb_write_hit_table(uint32_t number_queries, uint32_t stride, const uint32_t *counts,
                         const gzb_alignment *alignments, const char *const *query_names,
                         const char *const *subject_names, uint32_t number_subjects,

@@ -466,10 +466,13 @@ int gzo_build_alignment(const gzo_params *p, const uint8_t *query, uint32_t hit_
   uint8_t *rev = (uint8_t *)xmalloc(cap), *fwd = (uint8_t *)xmalloc(cap);
   size_t nr = 0, nf = 0;
   int sr, r0, r1, sf, f0, f1;
-  int rc = gzo_gapped_one_side_edits(p, query + hit_q - 1, db + hit_d - 1, 1, p->gapped_cutoff,
+  /* the build results step's X-drop is normalized_result_gapped_extension_cutoff
+   * (src/aligner_gpu.cpp:254-256, src/aligner.cpp), not the presearch one */
+  const int cutoff = p->result_gapped_cutoff;
+  int rc = gzo_gapped_one_side_edits(p, query + hit_q - 1, db + hit_d - 1, 1, cutoff,
                                      &sr, &r0, &r1, rev, cap, &nr);
   if (rc == 0)
-    rc = gzo_gapped_one_side_edits(p, query + hit_q, db + hit_d, 0, p->gapped_cutoff, &sf, &f0,
+    rc = gzo_gapped_one_side_edits(p, query + hit_q, db + hit_d, 0, cutoff, &sf, &f0,
                                    &f1, fwd, cap, &nf);
   if (rc != 0) {
     free(rev);

@@ -44,6 +44,7 @@ typedef struct {
   int32_t max_number_results;    /* -b */
   int32_t max_number_one_subject_results; /* -v */
   int32_t clustering;            /* 1 when the database was built with -C T */
+  int32_t result_gapped_cutoff;  /* X-drop of the build results traceback */
 } gzo_params;
 
 /* ---- stage primitives ------------------------------------------------ */

@@ -16,8 +16,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libgzref.so")
-# reference checkout the pin library is compiled from (build-time only)
-REF_ROOT = os.environ.get("GZ_REFERENCE_ROOT", "/root/reference")
+# reference checkout the pin library and programs are compiled from
+# (build-time only; unset where there is no checkout)
+REF_ROOT = os.environ.get("GZ_REFERENCE_ROOT")
 
 u8p = C.POINTER(C.c_uint8)
 u32p = C.POINTER(C.c_uint32)
@@ -33,9 +34,13 @@ COUNTER_NAMES = ("distance_seeds", "ungapped_seeds", "ungapped_hits",
 
 
 def build(ref: bool = False) -> None:
+    """Compile liboracle.so; with ref=True and GZ_REFERENCE_ROOT naming a
+    reference checkout, also the reference's units (_ref/libgzref.so) and
+    programs (_ref/ghostz, _ref/ghostz-gpu-host)."""
     subprocess.check_call(["make", "-s", "-C", HERE, "oracle"])
-    if ref and os.path.isdir(os.path.join(REF_ROOT, "src")):
-        subprocess.check_call(["make", "-s", "-C", HERE, "ref", f"REF_ROOT={REF_ROOT}"])
+    if ref and REF_ROOT and os.path.isdir(os.path.join(REF_ROOT, "src")):
+        subprocess.check_call(["make", "-s", "-j8", "-C", HERE, "ref", "aln", "alngpu",
+                               f"REF_ROOT={REF_ROOT}"])
 
 
 def _p(a, t):

@@ -4,7 +4,7 @@ import sys
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-for sub in ("ghostz-gpu_b200", "oracle"):
+for sub in ("ghostz-gpu_b200", "oracle", "tests"):
     p = os.path.join(ROOT, sub)
     if p not in sys.path:
         sys.path.insert(0, p)

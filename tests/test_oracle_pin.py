@@ -377,6 +377,8 @@ def test_seg_ln_factorial_table_matches_reference(oracle):
     import os
     import re
     import oracle as O
+    if not O.REF_ROOT:
+        pytest.skip("GZ_REFERENCE_ROOT (the reference checkout) not set")
     REF_LN_FACT = os.path.join(O.REF_ROOT, "ext", "seg", "src", "ln_factrial_table.h")
     if not os.path.exists(REF_LN_FACT):
         pytest.skip("reference checkout not present")
