@@ -308,11 +308,17 @@ __global__ void tb_combine_kernel(TbArgs a, uint64_t n_slots, const uint64_t *wa
     o.end_q = r.end_q;
     o.end_d = r.end_d;
     o.alignment_length = o.mismatches = o.gap_openings = o.gap_extensions = 0;
-    o.extension_score = 0;
+    o.presearch_score = r.score;
     if (r.chunk_id == a.chunk_id) {
       const uint64_t sr = 2 * slot, sf = 2 * slot + 1;
       const uint8_t *qs = a.query + a.q_offsets[qi];
-      o.extension_score = side_score[sr] + side_score[sf];
+      // AlignerBuildResultsThread::Run hands BuildResult the build step's
+      // own score, start and end (src/aligner_build_results_thread.h:124-160)
+      o.score = side_score[sr] + side_score[sf];
+      o.start_q = r.hit_q - 1 + (uint32_t)side_p0[sr];
+      o.start_d = r.hit_d - 1 + (uint32_t)side_p1[sr];
+      o.end_q = r.hit_q + (uint32_t)side_p0[sf];
+      o.end_d = r.hit_d + (uint32_t)side_p1[sf];
       uint32_t qp = r.hit_q - 1 + (uint32_t)side_p0[sr];
       uint32_t dp = r.hit_d - 1 + (uint32_t)side_p1[sr];
       uint32_t mm = 0, op_n = 0, ext_n = 0;

@@ -325,7 +325,7 @@ ALIGNMENT_DTYPE = np.dtype([
     ("chunk_id", "<i4"), ("subject_id", "<i4"), ("score", "<i4"),
     ("hit_q", "<u4"), ("hit_d", "<u4"), ("start_q", "<u4"), ("start_d", "<u4"),
     ("end_q", "<u4"), ("end_d", "<u4"), ("alignment_length", "<u4"), ("mismatches", "<u4"),
-    ("gap_openings", "<u4"), ("gap_extensions", "<u4"), ("extension_score", "<i4"),
+    ("gap_openings", "<u4"), ("gap_extensions", "<u4"), ("presearch_score", "<i4"),
 ])
 COUNTER_NAMES = ("distance_seeds", "ungapped_seeds", "ungapped_hits",
                  "chained_hits", "gapped_extensions", "gapped_cells", "gapped_fallbacks",
@@ -692,7 +692,7 @@ def translate_reads(dna, offsets, delimiter, device="cuda", stream=None):
     out_offs, qlen, total = translated_layout(lengths)
     if n == 0:
         return np.zeros(0, np.uint8), np.zeros(0, np.uint32), np.zeros(0, np.uint32)
-    d_dna = torch.from_numpy(np.ascontiguousarray(dna, dtype=np.uint8)).to(device)
+    d_dna = torch.from_numpy(np.require(dna, np.uint8, ["C", "W"])).to(device)
     d_offs = torch.from_numpy(offsets[:-1].view(np.int64).copy()).to(device)
     d_lens = torch.from_numpy(lengths.view(np.int32).copy()).to(device)
     d_out_offs = torch.from_numpy(out_offs.view(np.int64).copy()).to(device)
@@ -785,7 +785,7 @@ def prepare_translated_queries(dna, offsets, filter=True, matrix=None, ungapped_
     if n == 0:
         z = np.zeros(0, np.uint32)
         return np.zeros(0, np.uint8), z, z, z.astype(np.int32), z.astype(np.int32)
-    d_dna = torch.from_numpy(np.ascontiguousarray(dna, dtype=np.uint8)).to(device)
+    d_dna = torch.from_numpy(np.require(dna, np.uint8, ["C", "W"])).to(device)
     d_offs = torch.from_numpy(offsets[:-1].view(np.int64).copy()).to(device)
     d_lens = torch.from_numpy(lengths.view(np.int32).copy()).to(device)
     d_qoffs = torch.from_numpy(out_offs.view(np.int64).copy()).to(device)

@@ -383,22 +383,27 @@ int gzb_merge_chunk_results(const gzb_params *params, uint32_t number_queries,
                             const uint32_t *chunk_counts, const gzb_result *chunk_results,
                             uint32_t *counts, gzb_result *results);
 /* Alignment statistics of one merged result (AlignerCommon::Result,
- * src/aligner_common.h:80-92): the result's fields plus what
- * AlignerCommon::BuildResult (src/aligner_common.h:275-340) derives from the
- * edit path of both gapped extensions.  alignment_length == 0 marks a result
- * of another chunk (not computed by this call). */
+ * src/aligner_common.h:80-92) as AlignerCommon::BuildResult
+ * (src/aligner_common.h:275-340) fills it from the build step's two gapped
+ * extensions at the merged result's hit: their summed score, the alignment
+ * start and end they reach (concatenated coordinates, end = hit + forward
+ * best offset) and what the joined edit path counts.  The build step's
+ * X-drop (result_gapped_cutoff) is wider than the presearch's, so score,
+ * start and end may exceed the merged result's.  alignment_length == 0
+ * marks a result of another chunk (not computed by this call; its score,
+ * start and end are then the merged result's). */
 typedef struct {
   int32_t chunk_id;
   int32_t subject_id;
-  int32_t score;
-  uint32_t hit_q, hit_d;
-  uint32_t start_q, start_d;
-  uint32_t end_q, end_d;
+  int32_t score;              /* build step: reverse + forward best score */
+  uint32_t hit_q, hit_d;      /* the merged result's hit */
+  uint32_t start_q, start_d;  /* build step's alignment start */
+  uint32_t end_q, end_d;      /* build step's alignment end */
   uint32_t alignment_length;  /* edit ops of the joined path */
   uint32_t mismatches;
   uint32_t gap_openings;
   uint32_t gap_extensions;
-  int32_t extension_score;    /* both sides' scores again (equals score) */
+  int32_t presearch_score;    /* the merged result's (presearch) score */
 } gzb_alignment;
 /* The build results step for the resident chunk
  * (AlignerBuildResultsThread::Run, src/aligner_build_results_thread.h:64-190):
