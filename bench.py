@@ -4,23 +4,34 @@ workload (synthetic, seeded; DB 2M proteins with log-normal lengths, median
 at 30-90 % identity; BLOSUM62, open 11 / extend 1, clustered index L=10,
 seed threshold 39, top 10 per query, one result per subject).
 
-One step = one presearch of all queries against the resident database
-chunk: device query-list lookup, seed search + distance filter + ungapped
-X-drop with trigger, chain filter, gapped X-drop on both sides, top-b merge.
+Queries are SEG-masked and get their cutoffs on the GPU, as `aln -F T`
+prepares them.  One step = one presearch of all queries against the
+resident database chunk: device query-list lookup, seed search + distance
+filter + ungapped X-drop with trigger, chain filter, gapped X-drop on both
+sides, top-b merge.
 
-  value : queries/s with the queries already resident in HBM
-  e2e   : queries/s through the C ABI with host buffers: every step uploads
-          the queries (and builds their hash lists), runs the presearch and
-          reads the per-query top-b lists back.
+  value : queries/s with the prepared queries already resident in HBM
+  e2e   : queries/s of the search through the C ABI from host buffers: every
+          step copies the raw query residues in, prepares them (SEG,
+          cutoffs), uploads them and builds their hash lists, runs the
+          presearch and the build results step, and reads every query's
+          alignment records back (the work of `aln` after its database is
+          loaded, except formatting the text lines).
 The database index build is not in the timed region (it is reported as
 index_build_s), as the reference's `db` step is separate from `aln`.
+`parity` compares the library's hit table with the reference GPU aligner's
+(compiled from the reference's sources) on 1,000 queries x the first
+20,000 database sequences.
 
 Multi-GPU: replicas -- every rank runs the full workload on its own GPU
 (the reference's -g threads replicate the work too); value sums the ranks'
 queries over the slowest rank's device time.
 
---impl reference times the reference algorithm on the host cores instead
-(the CPU restatement in oracle/, all host threads, one process per core).
+--impl reference times the reference's own CPU search (`ghostz aln -g 0`
+with every host core, compiled from the reference's sources into
+oracle/_ref) on two slices of the database and reads the whole database's
+time off the line through them (oracle/ref_bench.py); where that program
+is not built it falls back to the CPU restatement in oracle/.
 """
 from __future__ import annotations
 
@@ -74,25 +85,42 @@ def log(msg):
 
 
 def make_workload(name, prepare="gpu", limit=None):
-    """Database and queries of a workload.  Translated-DNA reads are
-    prepared (translation, SEG, cutoffs) on the GPU, or by the oracle for
-    the reference arm; both give the same queries."""
+    """Database and queries of a workload, and the raw queries (residue
+    codes per protein query, or the Reads).  Queries are prepared as `aln`
+    prepares them (SEG, per-query cutoffs; translated-DNA reads six-frame
+    translated first) on the GPU, by the oracle (prepare="oracle"), or not
+    at all (prepare=None: raw queries only, q is None)."""
     from gzb import workload as W
     ndb, sdb, nq, sq, law = WORKLOADS[name]
     t = time.time()
     db = W.make_database(ndb, sdb)
     if "read_length" in law:
         reads = W.make_reads(db, nq, sq, read_length=law["read_length"])
+        raw = reads
         if prepare == "gpu":
             from gzb import native as N
             codes, offs, lens, cut, trig = N.prepare_translated_queries(reads.dna, reads.offsets)
             q = W.translated_queries(codes, offs, lens, sources=reads.sources,
                                      cutoffs=(cut, trig))
-        else:
+        elif prepare == "oracle":
             q = oracle_translated_queries(reads, limit=limit)
+        else:
+            q = None
     else:
-        q = W.make_queries(db, nq, sq, **law)
-    return db, q, time.time() - t
+        zeros = (np.zeros(nq, np.int32), np.zeros(nq, np.int32))
+        q = W.make_queries(db, nq, sq, cutoffs=zeros, **law)
+        raw = W.query_sequences(q)
+        if prepare == "gpu":
+            from gzb import native as N
+            q.codes, q.cutoffs, q.triggers = N.prepare_protein_queries(q.codes, q.offsets,
+                                                                       q.lengths)
+        elif prepare == "oracle":
+            from gzb import params as P
+            q = W.pack_queries(raw)  # cutoffs on the CPU, no SEG (restatement fallback)
+            q.cutoffs, q.triggers = P.query_cutoffs(raw)
+        else:
+            q = None
+    return db, q, time.time() - t, raw
 
 
 def oracle_translated_queries(reads, limit=None):
@@ -209,7 +237,7 @@ def ops_bench(workload, seeds, steps, warmup):
     from gzb import params as P
     dev = torch.device("cuda")
     params = P.make_params()
-    db, q, _ = make_workload(workload)
+    db, q, _, _ = make_workload(workload)
     eng = N.PresearchEngine(torch.cuda.current_device())
     eng.set_params(params)
     eng.set_database(db)
@@ -413,24 +441,94 @@ def build_results_cpu(db, q, aligned, budget_s=10.0):
             "sample": f"{n} alignments of the first {qi + 1} queries in {el:.2f} s"}
 
 
+def reference_program_baseline(db, raw, n_queries, steps, warmup):
+    """The reference's own CPU search on two database slices (oracle/
+    ref_bench.py): queries/s of the whole database, the sample text, the
+    threads and the per-step values; None where the program is not built."""
+    import ref_aln as R
+    import ref_bench as RB
+    if not R.available() or not isinstance(raw, list):
+        return None
+    sl = RB.ReferenceSlices(db, raw[:n_queries])
+    try:
+        runs = [sl.time_slices() for _ in range(warmup + steps)][warmup:]
+        t1 = float(np.median([r[0] for r in runs]))
+        t2 = float(np.median([r[1] for r in runs]))
+        full = sl.full_seconds(t1, t2)
+        per_step = [sl.n_queries / sl.full_seconds(a, b) for a, b in runs]
+        return {"value": sl.n_queries / full, "sample": sl.describe(t1, t2),
+                "cores": sl.threads, "per_step": per_step, "db_build_s": sl.db_build_s}
+    finally:
+        sl.close()
+
+
+def reference_parity(db, raw, n_queries=1000, n_sequences=20000):
+    """The library's hit table of the first n_queries queries against the
+    first n_sequences database sequences, against the reference GPU
+    aligner's (compiled from the reference's sources) on the same inputs."""
+    import ref_aln as R
+    import ref_bench as RB
+    if not R.available(gpu_aligner=True) or not isinstance(raw, list):
+        return {"checked": False, "why": "reference programs not built here"}
+    from gzb import native as N
+    from gzb import params as P
+    from gzb import search as S
+    from gzb import workload as W
+    n_queries = min(n_queries, len(raw))
+    n_sequences = min(n_sequences, db.number_sequences)
+    sl = RB.ReferenceSlices(db, raw[:n_queries], slices=(n_sequences,))
+    try:
+        t = time.time()
+        exp = sl.gpu_aligner_table(n_queries)
+        ref_s = time.time() - t
+    finally:
+        sl.close()
+    end = int(db.offsets[n_sequences])
+    chunk = W.Database(codes=db.codes[:end].copy(),
+                       offsets=np.concatenate([db.offsets[:n_sequences], [end]]).astype(np.uint32),
+                       number_sequences=n_sequences)
+    letters = [RB._letters(s) for s in raw[:n_queries]]
+    prepared = S.protein_queries(letters)
+    eng = N.PresearchEngine(int(os.environ.get("LOCAL_RANK", "0")))
+    try:
+        eng.set_graph(True)
+        rows = S.search(eng, P.make_params(), prepared, [chunk])
+    finally:
+        eng.close()
+    got = S.hit_table(rows, prepared, [chunk], [f"q{i}" for i in range(n_queries)],
+                      [f"s{j}" for j in range(n_sequences)])
+    same = sum(a == b for a, b in zip(got, exp))
+    return {"checked": True, "queries": n_queries, "db_sequences": n_sequences,
+            "lines": len(exp), "lines_equal": int(same),
+            "equal": bool(got == exp),
+            "reference": "ghostz-gpu aln -g 1 (the reference's GPU aligner compiled from its "
+                         "sources, device operators on CPU stand-ins)",
+            "reference_s": ref_s}
+
+
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    db, q, gen_s = make_workload(args.workload, prepare="oracle", limit=args.ref_queries)
     cores = os.cpu_count() or 1
-    vals = []
-    for i in range(args.warmup + args.steps):
-        v, el, sample = cpu_baseline(db, q, n_queries=args.ref_queries, processes=cores)
-        if i >= args.warmup:
-            vals.append(v)
-    value = float(np.mean(vals))
+    db, q, gen_s, raw = make_workload(args.workload, prepare=None)
+    ref = reference_program_baseline(db, raw, args.ref_queries, args.steps, args.warmup)
+    if ref is not None:
+        kind, value, sample, cores = "reference", ref["value"], ref["sample"], ref["cores"]
+    else:
+        _, q, _, _ = make_workload(args.workload, prepare="oracle", limit=args.ref_queries)
+        vals = []
+        for i in range(args.warmup + args.steps):
+            v, el, sample = cpu_baseline(db, q, n_queries=args.ref_queries, processes=cores)
+            if i >= args.warmup:
+                vals.append(v)
+        kind, value = "port", float(np.mean(vals))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": None,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded generator, config shapes)",
         "config": {"workload": args.workload, "sample": sample},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -748,9 +846,10 @@ def main():
     ap.add_argument("--train-sets", type=int, default=8)
     ap.add_argument("--workload", default="protein-10k-x-2M",
                     choices=sorted(WORKLOADS) + sorted(MULTICHUNK_WORKLOADS))
-    ap.add_argument("--cpu-queries", type=int, default=10000)
-    ap.add_argument("--ref-queries", type=int, default=10000)
+    ap.add_argument("--cpu-queries", type=int, default=2000)
+    ap.add_argument("--ref-queries", type=int, default=2000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--once", action="store_true",
                     help="one batched presearch (hit order, default tile, no training or "
@@ -773,7 +872,7 @@ def main():
         from gzb import native as N
         from gzb import params as P
         torch.cuda.set_device(local_rank)
-        db, q, _ = make_workload(args.workload)
+        db, q, _, _ = make_workload(args.workload)
         eng = N.PresearchEngine(local_rank)
         eng.set_params(P.make_params())
         eng.set_database(db)
@@ -812,7 +911,7 @@ def main():
     from gzb.replicas import Replicas
     torch.cuda.set_device(local_rank)
     reps = Replicas("nccl", timeout_s=600)
-    db, q, gen_s = make_workload(args.workload)
+    db, q, gen_s, raw = make_workload(args.workload)
     params = P.make_params()
     eng = N.PresearchEngine(local_rank)
     eng.set_params(params)
@@ -925,45 +1024,6 @@ def main():
                     for k in results_by)
     schedule = sched_id[head]
 
-    # ---- end-to-end loop through the C ABI with host buffers
-    import ctypes
-    pinned = {}
-    for name in ("codes", "offsets", "lengths", "cutoffs", "triggers"):
-        a = getattr(q, name)
-        t_pin = torch.empty(a.nbytes, dtype=torch.uint8).pin_memory()
-        t_pin.numpy()[:] = np.frombuffer(np.ascontiguousarray(a).tobytes(), dtype=np.uint8)
-        pinned[name] = (t_pin, a.dtype)
-    from gzb import workload as W
-    qp = W.Queries(**{n: pinned[n][0].numpy().view(pinned[n][1]) for n in pinned})
-    b = int(params["max_number_results"])
-    counts_pin = torch.empty(q.number * 4, dtype=torch.uint8).pin_memory()
-    res_pin = torch.empty(q.number * b * N.RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
-    L = N.lib()
-
-    def e2e_step():
-        eng.set_queries(qp, stream)
-        eng.presearch(schedule, stream)
-        N.check(L.gzb_engine_get_results(eng.h, ctypes.c_void_p(counts_pin.data_ptr()),
-                                         ctypes.c_void_p(res_pin.data_ptr()),
-                                         ctypes.c_void_p(stream.cuda_stream)))
-
-    for _ in range(args.warmup):
-        e2e_step()
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        e2e_step()
-    e1.record(stream)
-    barrier()
-    e2e_ms = e0.elapsed_time(e1)
-    h2d = sum(getattr(q, n).nbytes for n in ("codes", "offsets", "lengths", "cutoffs", "triggers"))
-    d2h = counts_pin.numel() + res_pin.numel()
-    # the e2e results must equal the device loop's
-    got = np.frombuffer(res_pin.numpy().tobytes(), dtype=N.RESULT_DTYPE).reshape(q.number, b)
-    cnt = np.frombuffer(counts_pin.numpy().tobytes(), dtype=np.uint32)
-    e2e_same = all(np.array_equal(got[i, :cnt[i]], results[i]) for i in range(q.number))
-
     # the build results step (traceback statistics of the merged results),
     # outside the presearch metric: device time of one call after a warm-up
     eng.build_alignments(stream)
@@ -975,6 +1035,75 @@ def main():
     n_aligned = int(sum(len(x) for x in aligned))
     build_results = {"ms": b0.elapsed_time(b1), "alignments": n_aligned,
                      "alignments_per_s": n_aligned / (b0.elapsed_time(b1) / 1e3)}
+
+    # ---- end to end through the C ABI from host buffers: the raw queries in
+    # pinned memory are copied in and prepared (SEG, cutoffs), uploaded with
+    # their hash lists built, searched, their results built (traceback
+    # statistics) and every query's alignment records read back
+    import ctypes
+    from gzb import workload as W
+    b = int(params["max_number_results"])
+    L = N.lib()
+
+    def pinned_copy(a):
+        t_pin = torch.empty(a.nbytes, dtype=torch.uint8).pin_memory()
+        t_pin.numpy()[:] = np.frombuffer(np.ascontiguousarray(a).tobytes(), dtype=np.uint8)
+        return t_pin.numpy().view(a.dtype), t_pin
+
+    keep = []
+    if isinstance(raw, list):
+        rq = W.pack_queries(raw, cutoffs=(np.zeros(len(raw), np.int32),
+                                          np.zeros(len(raw), np.int32)))
+        (p_codes, t1), (p_offs, t2), (p_lens, t3) = (pinned_copy(rq.codes),
+                                                     pinned_copy(rq.offsets),
+                                                     pinned_copy(rq.lengths))
+        keep += [t1, t2, t3]
+        raw_bytes = rq.codes.nbytes + rq.offsets.nbytes * 2 + rq.lengths.nbytes
+
+        def prepare():
+            codes, cut, trig = N.prepare_protein_queries(p_codes, p_offs, p_lens)
+            return W.Queries(codes=codes, offsets=p_offs, lengths=p_lens, cutoffs=cut,
+                             triggers=trig)
+    else:
+        (p_dna, t1), (p_roffs, t2) = pinned_copy(raw.dna), pinned_copy(raw.offsets)
+        keep += [t1, t2]
+        raw_bytes = raw.dna.nbytes + raw.offsets.nbytes * 2
+
+        def prepare():
+            codes, offs, lens, cut, trig = N.prepare_translated_queries(p_dna, p_roffs)
+            return W.translated_queries(codes, offs, lens, cutoffs=(cut, trig))
+    counts_pin = torch.empty(q.number * 4, dtype=torch.uint8).pin_memory()
+    al_pin = torch.empty(q.number * b * N.ALIGNMENT_DTYPE.itemsize,
+                         dtype=torch.uint8).pin_memory()
+
+    def e2e_step():
+        qq = prepare()
+        eng.set_queries(qq, stream)
+        eng.presearch(schedule, stream)
+        N.check(L.gzb_engine_build_alignments(eng.h, ctypes.c_void_p(counts_pin.data_ptr()),
+                                              ctypes.c_void_p(al_pin.data_ptr()),
+                                              ctypes.c_void_p(stream.cuda_stream)))
+        return qq
+
+    for _ in range(args.warmup):
+        qq = e2e_step()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    prepared_bytes = sum(getattr(qq, n).nbytes
+                         for n in ("codes", "offsets", "lengths", "cutoffs", "triggers"))
+    h2d = raw_bytes + prepared_bytes
+    d2h = (qq.codes.nbytes + qq.cutoffs.nbytes + qq.triggers.nbytes + counts_pin.numel()
+           + al_pin.numel())
+    # the e2e alignment records must equal the device loop's
+    got = np.frombuffer(al_pin.numpy().tobytes(), dtype=N.ALIGNMENT_DTYPE).reshape(q.number, b)
+    cnt = np.frombuffer(counts_pin.numpy().tobytes(), dtype=np.uint32)
+    e2e_same = all(np.array_equal(got[i, :cnt[i]], aligned[i]) for i in range(q.number))
 
     # the device index cache: export the chunk's index once, then set the
     # chunk again from it instead of building (outside the timed region)
@@ -1066,7 +1195,10 @@ def main():
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": t_e2e / steps,
-                "results_equal_device_loop": bool(e2e_same)},
+                "results_equal_device_loop": bool(e2e_same),
+                "step": "raw queries from pinned host memory -> SEG + cutoffs -> upload + "
+                        "hash lists -> presearch -> build results -> alignment records "
+                        "(no text formatting)"},
         "dp_gcups": {"gapped_stage": gcups_stage, "whole_step": gcups_step},
         "stage_ms": st, "counters": counters, "schedules": sched_report,
         "index_build_s": index_s, "index_cache": index_cache, "build_results": build_results,
@@ -1075,10 +1207,17 @@ def main():
         "gpu_launches": int(counters.get("kernel_launches", 0)) * steps,
     }
     if rank == 0 and not args.no_cpu_baseline:
-        v, el, sample = cpu_baseline(db, q, n_queries=args.cpu_queries, processes=1)
-        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-                                "sample": sample}
+        ref = reference_program_baseline(db, raw, args.cpu_queries, steps=2, warmup=1)
+        if ref is not None:
+            line["cpu_baseline"] = {"value": ref["value"], "unit": UNIT, "cores": ref["cores"],
+                                    "kind": "reference", "sample": ref["sample"]}
+        else:
+            v, el, sample = cpu_baseline(db, q, n_queries=args.cpu_queries, processes=1)
+            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+                                    "sample": sample}
         line["build_results"]["cpu_baseline"] = build_results_cpu(db, q, aligned)
+    if rank == 0 and not args.no_parity:
+        line["parity"] = reference_parity(db, raw)
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()
