@@ -1142,6 +1142,7 @@ struct gzb_engine {
   DBuf codeflag;
   uint64_t db_check = 0;     // of the resident chunk (index cache key)
   // build results step
+  DBuf tb_redo;
   DBuf tb_cols, tb_band_off, tb_band, tb_ops_bytes, tb_ops_off, tb_rows, tb_rows_off, tb_walk_cap,
       tb_walk_off, tb_ops, tb_row_meta, tb_walk, tb_walk_n, tb_score, tb_p0, tb_p1, tb_out;
   uint64_t pred_n = 0;       // extensions with a prediction in epred (last run)
@@ -1376,6 +1377,7 @@ extern "C" int gzb_engine_destroy(gzb_engine *e) {
                  &e->ecells, &e->okeys, &e->okeys2, &e->oidx, &e->oidx2, &e->queue,
                  &e->prev_cells, &e->model_d, &e->mae_acc, &e->log_x, &e->log_y,
                  &e->log_ctr, &e->enb, &e->codeflag, &e->tb_cols, &e->tb_band_off,
+                 &e->tb_redo,
                  &e->tb_band, &e->tb_ops_bytes, &e->tb_ops_off, &e->tb_rows, &e->tb_rows_off,
                  &e->tb_walk_cap, &e->tb_walk_off, &e->tb_ops, &e->tb_row_meta, &e->tb_walk,
                  &e->tb_walk_n, &e->tb_score, &e->tb_p0, &e->tb_p1, &e->tb_out};
@@ -2817,6 +2819,23 @@ int scan_total(gzb_engine *e, DBuf &in, DBuf &out, uint64_t n, cudaStream_t s,
   GZB_CUDA(cudaStreamSynchronize(s));
   return GZB_OK;
 }
+
+// the three scans of the build step's pass-1 sizes with one host wait
+int scan_totals3(gzb_engine *e, uint64_t n, cudaStream_t s, uint64_t *ops_total,
+                 uint64_t *rows_total, uint64_t *walk_total) {
+  DBuf *in[3] = {&e->tb_ops_bytes, &e->tb_rows, &e->tb_walk_cap};
+  DBuf *out[3] = {&e->tb_ops_off, &e->tb_rows_off, &e->tb_walk_off};
+  uint64_t *total[3] = {ops_total, rows_total, walk_total};
+  for (int k = 0; k < 3; ++k) {
+    GZB_TRY(out[k]->ensure(8 * (n + 1)));
+    GZB_CUDA(cudaMemsetAsync(in[k]->as<uint64_t>() + n, 0, 8, s));
+    GZB_TRY(exclusive_sum(e, in[k]->as<uint64_t>(), out[k]->as<uint64_t>(), n + 1, s));
+    GZB_CUDA(cudaMemcpyAsync(total[k], out[k]->as<uint64_t>() + n, 8, cudaMemcpyDeviceToHost,
+                             s));
+  }
+  GZB_CUDA(cudaStreamSynchronize(s));
+  return GZB_OK;
+}
 }  // namespace
 
 extern "C" int gzb_engine_build_alignments(gzb_engine *e, uint32_t *counts,
@@ -2853,14 +2872,19 @@ extern "C" int gzb_engine_build_alignments(gzb_engine *e, uint32_t *counts,
   GZB_TRY(e->tb_ops_bytes.ensure(8 * (n_sides + 1)));
   GZB_TRY(e->tb_rows.ensure(8 * (n_sides + 1)));
   GZB_TRY(e->tb_walk_cap.ensure(8 * (n_sides + 1)));
+  GZB_TRY(e->tb_redo.ensure(n_sides + 1));
+  // pass 1 by warps; the sides a warp cannot run, by threads
+  tb_count_warp_kernel<<<grid1(32 * n_sides, kTbWarpBlock), kTbWarpBlock, 0, s>>>(
+      a, n_sides, e->tb_ops_bytes.as<uint64_t>(), e->tb_rows.as<uint64_t>(),
+      e->tb_walk_cap.as<uint64_t>(), e->tb_redo.as<uint8_t>());
+  GZB_CUDA(cudaGetLastError());
   tb_count_kernel<<<grid1(n_sides, 128), 128, 0, s>>>(
       a, n_sides, e->tb_band_off.as<uint64_t>(), e->tb_band.as<int2>(),
-      e->tb_ops_bytes.as<uint64_t>(), e->tb_rows.as<uint64_t>(), e->tb_walk_cap.as<uint64_t>());
+      e->tb_ops_bytes.as<uint64_t>(), e->tb_rows.as<uint64_t>(), e->tb_walk_cap.as<uint64_t>(),
+      e->tb_redo.as<uint8_t>());
   GZB_CUDA(cudaGetLastError());
   uint64_t ops_total = 0, rows_total = 0, walk_total = 0;
-  GZB_TRY(scan_total(e, e->tb_ops_bytes, e->tb_ops_off, n_sides, s, &ops_total));
-  GZB_TRY(scan_total(e, e->tb_rows, e->tb_rows_off, n_sides, s, &rows_total));
-  GZB_TRY(scan_total(e, e->tb_walk_cap, e->tb_walk_off, n_sides, s, &walk_total));
+  GZB_TRY(scan_totals3(e, n_sides, s, &ops_total, &rows_total, &walk_total));
   GZB_TRY(e->tb_ops.ensure(ops_total + 1));
   GZB_TRY(e->tb_row_meta.ensure(8 * (rows_total + 1)));
   GZB_TRY(e->tb_walk.ensure(walk_total + 1));
@@ -2871,12 +2895,17 @@ extern "C" int gzb_engine_build_alignments(gzb_engine *e, uint32_t *counts,
   GZB_TRY(e->tb_out.ensure(sizeof(gzb_alignment) * (n_slots + 1)));
   // a cell the DP prunes keeps op 0, as in a fresh GappedExtender
   GZB_CUDA(cudaMemsetAsync(e->tb_ops.p, 0, ops_total + 1, s));
+  tb_store_warp_kernel<<<grid1(32 * n_sides, kTbWarpBlock), kTbWarpBlock, 0, s>>>(
+      a, n_sides, e->tb_ops_off.as<uint64_t>(), e->tb_ops.as<uint8_t>(),
+      e->tb_rows_off.as<uint64_t>(), e->tb_row_meta.as<uint32_t>(), e->tb_score.as<int32_t>(),
+      e->tb_p0.as<int32_t>(), e->tb_p1.as<int32_t>(), e->tb_redo.as<uint8_t>());
+  GZB_CUDA(cudaGetLastError());
   tb_walk_kernel<<<grid1(n_sides, 128), 128, 0, s>>>(
       a, n_sides, e->tb_band_off.as<uint64_t>(), e->tb_band.as<int2>(),
       e->tb_ops_off.as<uint64_t>(), e->tb_ops.as<uint8_t>(), e->tb_rows_off.as<uint64_t>(),
       e->tb_row_meta.as<uint32_t>(), e->tb_walk_off.as<uint64_t>(), e->tb_walk.as<uint8_t>(),
       e->tb_walk_n.as<uint32_t>(), e->tb_score.as<int32_t>(), e->tb_p0.as<int32_t>(),
-      e->tb_p1.as<int32_t>());
+      e->tb_p1.as<int32_t>(), e->tb_redo.as<uint8_t>());
   GZB_CUDA(cudaGetLastError());
   tb_combine_kernel<<<grid1(n_slots, 128), 128, 0, s>>>(
       a, n_slots, e->tb_walk_off.as<uint64_t>(), e->tb_walk.as<uint8_t>(),

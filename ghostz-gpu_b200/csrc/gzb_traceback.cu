@@ -4,10 +4,21 @@
 // AlignerCommon::BuildResult reports (alignment length, mismatches, gap
 // openings and extensions).
 //
-// One thread per side.  Pass 1 runs the DP to size each side's op storage;
-// pass 2 runs it again storing one op byte per kept cell, row by row, then
-// walks the optimal path back from the best cell (PickOptimalPath); a last
-// kernel joins the two sides per result in the reference's order.
+// Pass 1 runs the DP to size each side's op storage; pass 2 runs it again
+// storing one op byte per kept cell, row by row; then each side's optimal
+// path is walked back from the best cell (PickOptimalPath); a last kernel
+// joins the two sides per result in the reference's order.
+//
+// Both DP passes give one warp to a side: the warp evaluates 32 consecutive
+// columns of a row at once, with the presearch's warp DP
+// (gapped_extend_warp in gzb_kernels.cuh: band edges and stored values
+// exact for X-drops below 1024).  A kept cell's edit op also needs the
+// reference's horizontal-gap value *with* its reset to kInitScore at pruned
+// cells (src/gapped_extender.cpp:428-446); once a chunk's pruned flags are
+// known that value is a segmented max-plus scan whose segments start after
+// the pruned cells.  Sides whose band outgrows the warp's circular buffer,
+// or whose X-drop is 1024 or more, are flagged and run by one thread each
+// with the band in global memory (the serial form of the same DP).
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -186,7 +197,294 @@ __device__ void tb_extend(const TbArgs &a, const int *sm, const TbSide &t, int2 
   *best_p1 = max_p1;
 }
 
+constexpr int kTbWarpColumns = 256;  // circular band of one warp (int2 columns)
+constexpr int kTbWarpsPerBlock = 8;
+static_assert(kTbWarpBlock == kTbWarpsPerBlock * 32, "launch block of the warp kernels");
+
+// tb_extend by one warp (lanes must all call it with the same side); with
+// STORE it also writes the ops and row table as tb_extend does.  Returns
+// false when the band outgrows kTbWarpColumns (outputs then meaningless).
+template <bool STORE>
+__device__ bool tb_extend_warp(const TbArgs &a, const int *sm, const TbSide &t, int2 *band,
+                               uint8_t *ops, uint32_t *row_meta, uint64_t *ops_bytes,
+                               uint32_t *rows, int *best_score, int *best_p0, int *best_p1) {
+  constexpr int W = kTbWarpColumns;
+  constexpr int wmask = W - 1;
+  constexpr unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int inc = t.inc;
+  const int delim = a.delim;
+  const int ge = a.gap_ext;
+  const int gi = a.gap_open + a.gap_ext;
+  const int cutoff = a.cutoff;
+  const uint8_t *q0 = t.seq0, *d0 = t.seq1;
+  *best_score = 0;
+  *best_p0 = -inc;
+  *best_p1 = -inc;
+  *ops_bytes = 0;
+  *rows = 0;
+  if (q0[0] == delim || d0[0] == delim) return true;
+  // row -1: the horizontal gap run from column 1 while >= -cutoff
+  int k0;
+  if (-gi < -cutoff) {
+    k0 = 0;
+  } else if (ge == 0) {
+    k0 = 1 << 30;
+  } else {
+    const long long kk = ((long long)cutoff - gi) / ge + 1;
+    k0 = kk > (1 << 30) ? (1 << 30) : (int)kk;
+  }
+  int col = find_delimiter_column(q0, inc, delim, 1, k0 > W ? W + 1 : k0);
+  if (col > W) return false;
+  for (int c = 1 + lane; c < col; c += 32) {
+    const int s = -gi - (c - 1) * ge;
+    band[c & wmask] = make_int2(s, s - gi);
+  }
+  if (lane == 0) band[0] = make_int2(0, -gi);
+  int bs = 0, be;
+  if (q0[(col - 1) * inc] != delim) {
+    if (col + 1 > W) return false;
+    if (lane == 0) band[col & wmask] = make_int2(kInitScore, kInitScore);
+    be = col + 1;
+  } else {
+    be = col;
+  }
+  __syncwarp();
+
+  int maxs = 0, mp0 = -inc, mp1 = -inc;
+  uint64_t used = 0;
+  uint32_t r = 0;
+  for (;; ++r) {
+    const int x = d0[(int)r * inc];
+    if (x == delim) break;
+    const int *mrow = sm + x * kMatrixStride;
+    const int row_start = bs;
+    uint8_t *row_ops = nullptr;
+    if (STORE) {
+      if (lane == 0) {
+        row_meta[2 * r] = (uint32_t)used;
+        row_meta[2 * r + 1] = (uint32_t)row_start;
+      }
+      row_ops = ops + used - row_start;
+    }
+    // column bs: vertical gap only
+    const int2 st0 = band[bs & wmask];
+    int diag = st0.x;
+    const int nb0 = (maxs - st0.y > cutoff) ? kInitScore : st0.y;
+    int F = nb0 - gi;   // horizontal gap without the reset at pruned cells
+    int Fs = nb0 - gi;  // the reference's horizontal gap
+    __syncwarp();
+    if (lane == 0) {
+      band[bs & wmask] = make_int2(nb0, st0.y - ge);
+      if (STORE) row_ops[bs] = kTbGap0 + kTbExt0;
+    }
+    int M = maxs;
+    int first_kept = -1, last_kept = bs;
+    for (int cs = bs + 1; cs < be; cs += 32) {
+      const int c = cs + lane;
+      const bool active = c < be;
+      int2 st = make_int2(kInitScore, kInitScore);
+      int qres = 0;
+      if (active) {
+        st = band[c & wmask];
+        qres = q0[(c - 1) * inc];
+      }
+      int prev = __shfl_up_sync(full, st.x, 1);
+      if (lane == 0) prev = diag;
+      const int sd = prev + mrow[qres];
+      const int G = imax(sd, st.y);
+      int P = active ? G - gi + (lane + 1) * ge : kNegBig;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int tv = __shfl_up_sync(full, P, o);
+        if (lane >= o) P = imax(P, tv);
+      }
+      int Pex = __shfl_up_sync(full, P, 1);
+      if (lane == 0) Pex = kNegBig;
+      const int raw = imax(G, imax(F, Pex) - lane * ge);
+      int R = active ? raw : kNegBig;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int tv = __shfl_up_sync(full, R, o);
+        if (lane >= o) R = imax(R, tv);
+      }
+      const int Mrow = imax(M, R);
+      const bool pruned = (Mrow - raw > cutoff);
+      if (active) {
+        const int nb = pruned ? kInitScore : raw;
+        const int ng = pruned ? kInitScore : imax(raw - gi, st.y - ge);
+        band[c & wmask] = make_int2(nb, ng);
+      }
+      const int nact = imin(32, be - cs);
+      if (STORE) {
+        // the reference's horizontal gap entering each cell: normalized
+        // N(j) = F(j) + j ge obeys N(j + 1) = max(N(j), G(j) - gi + (j + 1) ge)
+        // after a kept cell and restarts at kInitScore + (j + 1) ge after a
+        // pruned one (a segment head)
+        const bool head = active && pruned;
+        int v = head ? kInitScore + (lane + 1) * ge : (active ? G - gi + (lane + 1) * ge : kNegBig);
+        if (lane == 0 && !head) v = imax(v, Fs);
+        bool seg = head;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int tv = __shfl_up_sync(full, v, o);
+          const bool ts = __shfl_up_sync(full, seg, o);
+          if (lane >= o) {
+            if (!seg) v = imax(v, tv);
+            seg = seg || ts;
+          }
+        }
+        int Nin = __shfl_up_sync(full, v, 1);
+        if (lane == 0) Nin = Fs;
+        if (active && !pruned) {
+          const int Fb = Nin - lane * ge;
+          int op = kTbSub, sc = sd;
+          if (sc < st.y) {
+            op = kTbGap0;
+            sc = st.y;
+          }
+          if (sc < Fb) {
+            op = kTbGap1;
+            sc = Fb;
+          }
+          if (!(st.y - ge < sc - gi)) op += kTbExt0;
+          if (!(Fb - ge < sc - gi)) op += kTbExt1;
+          row_ops[c] = (uint8_t)op;
+        }
+        Fs = __shfl_sync(full, v, nact - 1) - nact * ge;
+      }
+      // new maximum: first column reaching the chunk maximum
+      const int cm = __shfl_sync(full, R, 31);
+      if (cm > M) {
+        const unsigned hitm = __ballot_sync(full, active && raw == cm);
+        const int l = __ffs(hitm) - 1;
+        maxs = cm;
+        mp0 = (cs + l - 1) * inc;
+        mp1 = (int)r * inc;
+      }
+      const unsigned kept = __ballot_sync(full, active && !pruned);
+      if (kept) {
+        if (first_kept < 0) first_kept = cs + __ffs(kept) - 1;
+        last_kept = cs + 31 - __clz(kept);
+      }
+      const int Plast = __shfl_sync(full, P, nact - 1);
+      F = imax(F, Plast) - nact * ge;
+      M = imax(M, cm);
+      diag = __shfl_sync(full, st.x, 31);
+    }
+    __syncwarp();
+    if (first_kept < 0) {  // every cell pruned: array_start + 1 == array_end
+      ++r;
+      break;
+    }
+    bs = first_kept - 1;
+    bool edge_residue;
+    if (last_kept < be - 1) {
+      edge_residue = q0[(be - 1) * inc] != delim;
+      be = last_kept + 1;
+    } else {
+      int k;
+      const long long room = (long long)F - ((long long)maxs - cutoff);
+      if (room < 0) {
+        k = 0;
+      } else if (ge == 0) {
+        k = 1 << 30;
+      } else {
+        const long long kk = room / ge + 1;
+        k = kk > (1 << 30) ? (1 << 30) : (int)kk;
+      }
+      if (k > 0) {
+        const int lim = (be + k - bs > W) ? (W - (be - bs) + 1) : k;
+        k = find_delimiter_column(q0, inc, delim, be, lim) - be;
+        if (be + k - bs > W) return false;
+        for (int j = lane; j < k; j += 32) {
+          const int v = F - j * ge;
+          band[(be + j) & wmask] = make_int2(v, v - gi);
+          if (STORE) row_ops[be + j] = kTbGap0 + kTbExt0;
+        }
+        be += k;
+      }
+      edge_residue = q0[(be - 1) * inc] != delim;
+    }
+    if (edge_residue) {
+      if (be + 1 - bs > W) return false;
+      if (lane == 0) band[be & wmask] = make_int2(kInitScore, kInitScore);
+      ++be;
+    }
+    used += (uint64_t)(be - row_start);
+    __syncwarp();
+  }
+  *ops_bytes = used + (uint64_t)(t.len0 + 2);
+  *rows = r;
+  *best_score = maxs;
+  *best_p0 = mp0;
+  *best_p1 = mp1;
+  return true;
+}
+
 }  // namespace
+
+// pass 1 by one warp per side; a side the warp cannot run exactly is
+// flagged in `redo` for tb_count_kernel
+__global__ void __launch_bounds__(kTbWarpsPerBlock * 32)
+    tb_count_warp_kernel(TbArgs a, uint64_t n_sides, uint64_t *ops_bytes, uint64_t *rows,
+                         uint64_t *walk_cap, uint8_t *redo) {
+  __shared__ int sm[kMatrixStride * kMatrixStride];
+  __shared__ int2 bands[kTbWarpsPerBlock][kTbWarpColumns];
+  load_matrix(sm, a.matrix32, kMatrixStride, kMatrixStride);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint64_t s = blockIdx.x * (uint64_t)kTbWarpsPerBlock + warp; s < n_sides;
+       s += (uint64_t)gridDim.x * kTbWarpsPerBlock) {
+    const TbSide t = side_of(a, s);
+    bool ok = true;
+    uint64_t nb = 0;
+    uint32_t nr = 0;
+    if (t.active) {
+      int sc, p0, p1;
+      ok = a.cutoff < 1024 &&
+           tb_extend_warp<false>(a, sm, t, bands[warp], nullptr, nullptr, &nb, &nr, &sc, &p0,
+                                 &p1);
+    }
+    if (lane == 0) {
+      redo[s] = ok ? 0 : 1;
+      ops_bytes[s] = t.active ? nb : 0;
+      rows[s] = t.active ? nr : 0;
+      walk_cap[s] = t.active ? (uint64_t)nr + t.len0 + 2 : 0;
+    }
+    __syncwarp();
+  }
+}
+
+// pass 2 by one warp per side for the sides pass 1 ran by warp: the DP with
+// its ops and row table, and the side's best score and positions
+__global__ void __launch_bounds__(kTbWarpsPerBlock * 32)
+    tb_store_warp_kernel(TbArgs a, uint64_t n_sides, const uint64_t *ops_off, uint8_t *ops,
+                         const uint64_t *rows_off, uint32_t *row_meta, int32_t *side_score,
+                         int32_t *side_p0, int32_t *side_p1, const uint8_t *redo) {
+  __shared__ int sm[kMatrixStride * kMatrixStride];
+  __shared__ int2 bands[kTbWarpsPerBlock][kTbWarpColumns];
+  load_matrix(sm, a.matrix32, kMatrixStride, kMatrixStride);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (uint64_t s = blockIdx.x * (uint64_t)kTbWarpsPerBlock + warp; s < n_sides;
+       s += (uint64_t)gridDim.x * kTbWarpsPerBlock) {
+    if (redo[s]) continue;
+    const TbSide t = side_of(a, s);
+    if (!t.active) continue;
+    uint64_t nb;
+    uint32_t nr;
+    int sc, p0, p1;
+    tb_extend_warp<true>(a, sm, t, bands[warp], ops + ops_off[s], row_meta + 2 * rows_off[s],
+                         &nb, &nr, &sc, &p0, &p1);
+    if (lane == 0) {
+      side_score[s] = sc;
+      side_p0[s] = p0;
+      side_p1[s] = p1;
+    }
+    __syncwarp();
+  }
+}
 
 // per side: band columns (len0 + 2) for the scan
 __global__ void tb_band_kernel(TbArgs a, uint64_t n_sides, uint64_t *band_cols) {
@@ -197,15 +495,17 @@ __global__ void tb_band_kernel(TbArgs a, uint64_t n_sides, uint64_t *band_cols) 
   }
 }
 
-// pass 1: op bytes and rows of every side
+// pass 1 by one thread per side for the sides flagged in `redo`, the band in
+// global memory
 __global__ void tb_count_kernel(TbArgs a, uint64_t n_sides, const uint64_t *band_off,
                                 int2 *band, uint64_t *ops_bytes, uint64_t *rows,
-                                uint64_t *walk_cap) {
+                                uint64_t *walk_cap, const uint8_t *redo) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
   load_matrix(sm, a.matrix32, kMatrixStride, kMatrixStride);
   __syncthreads();
   for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < n_sides;
        s += (uint64_t)gridDim.x * blockDim.x) {
+    if (!redo[s]) continue;
     const TbSide t = side_of(a, s);
     uint64_t nb = 0;
     uint32_t nr = 0;
@@ -220,14 +520,16 @@ __global__ void tb_count_kernel(TbArgs a, uint64_t n_sides, const uint64_t *band
   }
 }
 
-// pass 2: the DP with its ops, then PickOptimalPath
-// (src/gapped_extender.cpp:473-531); the path is written in walk order
-// (from the best cell back to the origin).
+// pass 2 for the flagged sides (the DP with its ops by one thread, the band
+// in global memory), then PickOptimalPath (src/gapped_extender.cpp:473-531)
+// for every side; the path is written in walk order (from the best cell
+// back to the origin).
 __global__ void tb_walk_kernel(TbArgs a, uint64_t n_sides, const uint64_t *band_off,
                                int2 *band, const uint64_t *ops_off, uint8_t *ops,
                                const uint64_t *rows_off, uint32_t *row_meta,
                                const uint64_t *walk_off, uint8_t *walk, uint32_t *walk_n,
-                               int32_t *side_score, int32_t *side_p0, int32_t *side_p1) {
+                               int32_t *side_score, int32_t *side_p0, int32_t *side_p1,
+                               const uint8_t *redo) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
   load_matrix(sm, a.matrix32, kMatrixStride, kMatrixStride);
   __syncthreads();
@@ -237,13 +539,19 @@ __global__ void tb_walk_kernel(TbArgs a, uint64_t n_sides, const uint64_t *band_
     if (!t.active) continue;
     uint8_t *sops = ops + ops_off[s];
     uint32_t *meta = row_meta + 2 * rows_off[s];
-    uint64_t nb;
-    uint32_t nr;
-    int sc, p0, p1;
-    tb_extend(a, sm, t, band + band_off[s], sops, meta, &nb, &nr, &sc, &p0, &p1);
-    side_score[s] = sc;
-    side_p0[s] = p0;
-    side_p1[s] = p1;
+    int p0, p1;
+    if (redo[s]) {
+      uint64_t nb;
+      uint32_t nr;
+      int sc;
+      tb_extend(a, sm, t, band + band_off[s], sops, meta, &nb, &nr, &sc, &p0, &p1);
+      side_score[s] = sc;
+      side_p0[s] = p0;
+      side_p1[s] = p1;
+    } else {
+      p0 = side_p0[s];
+      p1 = side_p1[s];
+    }
     uint8_t *path = walk + walk_off[s];
     uint32_t m = 0;
     {

@@ -24,14 +24,23 @@ struct TbArgs {
 };
 
 __global__ void tb_band_kernel(TbArgs a, uint64_t n_sides, uint64_t *band_cols);
+// warps per block of the one-warp-per-side kernels
+constexpr int kTbWarpBlock = 8 * 32;
+__global__ void tb_count_warp_kernel(TbArgs a, uint64_t n_sides, uint64_t *ops_bytes,
+                                     uint64_t *rows, uint64_t *walk_cap, uint8_t *redo);
 __global__ void tb_count_kernel(TbArgs a, uint64_t n_sides, const uint64_t *band_off,
                                 int2 *band, uint64_t *ops_bytes, uint64_t *rows,
-                                uint64_t *walk_cap);
+                                uint64_t *walk_cap, const uint8_t *redo);
+__global__ void tb_store_warp_kernel(TbArgs a, uint64_t n_sides, const uint64_t *ops_off,
+                                     uint8_t *ops, const uint64_t *rows_off, uint32_t *row_meta,
+                                     int32_t *side_score, int32_t *side_p0, int32_t *side_p1,
+                                     const uint8_t *redo);
 __global__ void tb_walk_kernel(TbArgs a, uint64_t n_sides, const uint64_t *band_off,
                                int2 *band, const uint64_t *ops_off, uint8_t *ops,
                                const uint64_t *rows_off, uint32_t *row_meta,
                                const uint64_t *walk_off, uint8_t *walk, uint32_t *walk_n,
-                               int32_t *side_score, int32_t *side_p0, int32_t *side_p1);
+                               int32_t *side_score, int32_t *side_p0, int32_t *side_p1,
+                               const uint8_t *redo);
 __global__ void tb_combine_kernel(TbArgs a, uint64_t n_slots, const uint64_t *walk_off,
                                   const uint8_t *walk, const uint32_t *walk_n,
                                   const int32_t *side_score, const int32_t *side_p0,
