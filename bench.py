@@ -832,7 +832,8 @@ def run_multichunk(args, world, rank, local_rank):
     reps.close()
 
 
-KERNEL_NAMES = {0: "flat", 1: "lane", 2: "rows", 3: "static", 4: "deal"}
+KERNEL_NAMES = {0: "flat", 1: "lane", 2: "rows", 3: "static", 4: "deal", 5: "group4", 6: "group8",
+                7: "group16", 8: "group32"}
 ORDER_NAMES = {0: "hits", 1: "cost model"}
 
 

@@ -56,6 +56,7 @@ __global__ void gapped_serial_kernel(GappedJob job, const int32_t *__restrict__ 
                                      uint32_t *too_long_count);
 
 extern GappedTile g_tile;
+constexpr int kTileParameters = 4;  // GZB_TILE_BOOK_THRESHOLD .. GZB_TILE_SEED_WALKER
 int check_tile_value(int which, int value);
 int *tile_field(GappedTile &t, int which);
 int any_tile_value(int which);
@@ -442,7 +443,7 @@ constexpr int kUnitsPerWarp = 256;
 
 // One unit = one representative or one residual database position of a list,
 // tried against every query position of that list.
-__global__ void __launch_bounds__(kSeedBlock, 6)
+__global__ void __launch_bounds__(kSeedBlock, 5)
 seed_kernel(SeedArgs a) {
   __shared__ __align__(16) int32_t tbl32[kWalkTableBytes / 4];
   load_walk_table(tbl32, a.matrix32, a.p.delimiter);
@@ -587,6 +588,125 @@ member_kernel(SeedArgs a, const uint2 *__restrict__ mwork, uint64_t n_work,
     }
   }
   __syncwarp();
+  add_counter(&a.ctr[1], n_seed);
+  add_counter(&a.ctr[2], n_steps);
+}
+
+// ---------------------------------------------------------------------------
+// Dealt seed walker.  seed_kernel gives each lane whole units (a unit's
+// every list entry in turn), so a warp waits for its lane with the longest
+// list.  Here the seeds of 32 units -- every (unit, list entry) pair -- form
+// one stream that is dealt to the lanes 32 at a time, as member_kernel deals
+// member seeds: a warp then waits only for the longest single walk of a
+// round.  A lane finds its seed's unit with a shuffle search over the
+// units' exclusive count scan.  Every seed gets the same decisions and
+// counts as in seed_kernel.
+
+constexpr unsigned kFullMask = 0xffffffffu;
+
+// the last lane whose exclusive offset is <= p (the owner of stream seed p)
+__device__ __forceinline__ int stream_owner(uint32_t excl, uint32_t p) {
+  int o = 0;
+  for (int step = 16; step >= 1; step >>= 1) {
+    const uint32_t e = __shfl_sync(kFullMask, excl, (o + step) & 31);
+    if (o + step < 32 && e <= p) o += step;
+  }
+  return o;
+}
+
+__global__ void __launch_bounds__(kSeedBlock, 4)
+seed_dealt_kernel(SeedArgs a) {
+  __shared__ __align__(16) int32_t tbl32[kWalkTableBytes / 4];
+  load_walk_table(tbl32, a.matrix32, a.p.delimiter);
+  __syncthreads();
+  const char *tbl = reinterpret_cast<const char *>(tbl32);
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const uint64_t U = a.units_dev ? *a.units_dev : a.L.n_units;
+  const int thr = a.p.distance_threshold;
+  const int maxmd = a.p.max_member_distance;
+  unsigned long long n_dist = 0, n_seed = 0, n_steps = 0;
+  for (uint64_t base = warp * kUnitsPerWarp; base < U; base += nwarps * kUnitsPerWarp) {
+    const uint64_t last = min(base + kUnitsPerWarp, U) - 1;
+    uint64_t l_lo = 0, l_hi = 0;
+    if (lane == 0) {
+      l_lo = upper_segment(a.L.unit_offsets, 0, a.L.n_lists - 1, base);
+      l_hi = upper_segment(a.L.unit_offsets, l_lo, a.L.n_lists - 1, last);
+    }
+    l_lo = __shfl_sync(kFullMask, l_lo, 0);
+    l_hi = __shfl_sync(kFullMask, l_hi, 0);
+    for (uint64_t b0 = base; b0 <= last; b0 += 32) {
+      // this lane's unit: database position, entry range, filter data
+      const uint64_t u = b0 + lane;
+      uint32_t cnt = 0, pb = 0, chk_end = 0, upos = 0, cid = 0;
+      uint64_t rwin = 0;
+      bool rep = false, members = false;
+      if (u <= last) {
+        const uint64_t l = upper_segment(a.L.unit_offsets, l_lo, l_hi, u);
+        const uint32_t j = (uint32_t)(u - a.L.unit_offsets[l]);
+        pb = a.L.offsets[l];
+        cnt = a.L.offsets[l + 1] - pb;
+        const uint32_t nrep = a.L.rep_count[l];
+        if (j < nrep) {
+          const uint32_t r = a.L.rep_begin[l] + j;
+          rep = true;
+          upos = a.X.rep_positions[r];
+          cid = a.X.rep_cluster_ids[r];
+          members = a.X.member_offsets[cid + 1] > a.X.member_offsets[cid];
+          rwin = a.X.rep_windows[r];
+          chk_end = pb + a.L.nchk[l];
+        } else {
+          upos = a.X.nc_values[a.L.nc_begin[l] + (j - nrep)];
+        }
+      }
+      uint32_t incl = cnt;
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFullMask, incl, d);
+        if (lane >= d) incl += t;
+      }
+      const uint32_t excl = incl - cnt;
+      const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+      for (uint32_t r0 = 0; r0 < total; r0 += 32) {
+        const uint32_t p = r0 + lane;
+        const int o = stream_owner(excl, p < total ? p : 0);
+        const uint32_t opb = __shfl_sync(kFullMask, pb, o);
+        const uint32_t oexcl = __shfl_sync(kFullMask, excl, o);
+        const uint32_t ochk = __shfl_sync(kFullMask, chk_end, o);
+        const uint32_t opos = __shfl_sync(kFullMask, upos, o);
+        const uint32_t ocid = __shfl_sync(kFullMask, cid, o);
+        const uint64_t owin = __shfl_sync(kFullMask, rwin, o);
+        const bool orep = __shfl_sync(kFullMask, rep, o);
+        const bool omem = __shfl_sync(kFullMask, members, o);
+        if (p < total) {
+          const uint32_t k = opb + (p - oexcl);
+          bool walk = true;
+          if (orep) {
+            bool pass = true;
+            if (k < ochk) {
+              const int dist = nibble_mismatches(a.L.entry_window[k], owin);
+              ++n_dist;
+              walk = dist <= thr;
+              pass = max(dist - maxmd, 0) <= thr;
+            }
+            if (pass && omem) append(a.mwork, a.mwork_count, a.mwork_cap, make_uint2(ocid, k));
+          }
+          if (walk) {
+            const uint32_t qid = a.L.entry_qid[k], cpos = a.L.entry_cpos[k];
+            const uint32_t ct = a.L.entry_ct[k];
+            int steps = 0;
+            ++n_seed;
+            if (walk_hit(a.q + cpos, a.db + opos, tbl, (int)(ct >> 16),
+                         (int)(int16_t)(ct & 0xffffu), &steps))
+              emit_hit(a, qid, opos, cpos - a.q_offsets[qid]);
+            n_steps += steps;
+          }
+        }
+      }
+    }
+  }
+  __syncwarp();
+  add_counter(&a.ctr[0], n_dist);
   add_counter(&a.ctr[1], n_seed);
   add_counter(&a.ctr[2], n_steps);
 }
@@ -1147,7 +1267,8 @@ struct gzb_engine {
       tb_walk_off, tb_ops, tb_row_meta, tb_walk, tb_walk_n, tb_score, tb_p0, tb_p1, tb_out;
   uint64_t pred_n = 0;       // extensions with a prediction in epred (last run)
   DBuf enb;                  // per surviving hit: chained neighbours (cost feature)
-  int tile[3][3] = {{-1, -1, -1}, {-1, -1, -1}, {-1, -1, -1}};  // [schedule][which], -1 = default
+  int tile[3][kTileParameters] = {{-1, -1, -1, -1}, {-1, -1, -1, -1}, {-1, -1, -1, -1}};
+  // [schedule][which], -1 = default
   bool logging = false;
   uint64_t log_cap = 0;
   bool have_model = false;
@@ -2031,8 +2152,10 @@ extern "C" int gzb_engine_reset_results(gzb_engine *e, void *stream) {
 namespace {
 
 int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
-  (void)schedule;
   uint64_t launches = 0;
+  GappedTile stile = g_tile;
+  for (int w = 0; w < kTileParameters; ++w)
+    if (e->tile[schedule][w] >= 0) *tile_field(stile, w) = e->tile[schedule][w];
   DevLists &L = e->L;
   const DevIndex &X = e->X;
   const uint32_t nq = e->nq;
@@ -2090,9 +2213,12 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
     a.ctr = c;
     if (L.n_units) {
       const uint64_t warps = (L.n_units + kUnitsPerWarp - 1) / kUnitsPerWarp;
-      seed_kernel<<<grid1(warps * 32, kSeedBlock, 148 * 16), kSeedBlock, 0, s>>>(a);
+      if (stile.seed_walker == GZB_SEED_WALKER_DEALT)
+        seed_dealt_kernel<<<grid1(warps * 32, kSeedBlock, 148 * 16), kSeedBlock, 0, s>>>(a);
+      else
+        seed_kernel<<<grid1(warps * 32, kSeedBlock, 148 * 16), kSeedBlock, 0, s>>>(a);
       GZB_CUDA(cudaGetLastError());
-    ++launches;
+      ++launches;
     }
     GZB_CUDA(cudaMemcpyAsync(hctr, c, 64, cudaMemcpyDeviceToHost, s));
     GZB_CUDA(cudaStreamSynchronize(s));
@@ -2203,7 +2329,7 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
     job.gap_ext = e->params.gap_extension;
     job.cutoff = e->params.gapped_cutoff;
     GappedTile tile = g_tile;
-    for (int w = 0; w < 3; ++w)
+    for (int w = 0; w < kTileParameters; ++w)
       if (e->tile[schedule][w] >= 0) *tile_field(tile, w) = e->tile[schedule][w];
     if (schedule == GZB_SCHEDULE_PLAIN) tile.kernel = GZB_GAPPED_KERNEL_STATIC;
     const bool learned =
@@ -2500,7 +2626,10 @@ int graph_body(gzb_engine *e, int schedule, const GappedTile &tile, bool learned
   a.ctr = ctr;
   a.units_dev = L.n_lists ? L.unit_offsets + L.n_lists : nullptr;
   if (L.n_lists) {
-    seed_kernel<<<148 * 16, kSeedBlock, 0, s>>>(a);
+    if (tile.seed_walker == GZB_SEED_WALKER_DEALT)
+      seed_dealt_kernel<<<148 * 16, kSeedBlock, 0, s>>>(a);
+    else
+      seed_kernel<<<148 * 16, kSeedBlock, 0, s>>>(a);
     GZB_CUDA(cudaGetLastError());
     ++launches;
   }
@@ -2645,7 +2774,8 @@ uint64_t graph_key(const gzb_engine *e, int schedule, const GappedTile &tile, bo
   h = fnv_mix(h, &e->params, sizeof(e->params));
   const uint64_t v[] = {e->db_len, e->nseq, (uint64_t)(int64_t)e->chunk_id, e->nq, e->q_len,
                         e->max_qlen, (uint64_t)schedule, (uint64_t)tile.kernel,
-                        (uint64_t)tile.book_threshold, (uint64_t)tile.order, c.hits, c.mwork,
+                        (uint64_t)tile.book_threshold, (uint64_t)tile.order,
+                        (uint64_t)tile.seed_walker, c.hits, c.mwork,
                         (uint64_t)(uintptr_t)e->spill, e->spill_cap,
                         (uint64_t)(uintptr_t)e->band_pool, (uint64_t)(uintptr_t)e->gcounters,
                         (uint64_t)(uintptr_t)e->gcells, (uint64_t)(uintptr_t)e->report_h,
@@ -2786,7 +2916,7 @@ extern "C" int gzb_engine_presearch(gzb_engine *e, int schedule, void *stream) {
   if (e->graph && schedule != GZB_SCHEDULE_ORACLE && !e->logging) {
     // graph mode covers hit order; a cost-model order runs eagerly
     GappedTile tile = g_tile;
-    for (int w = 0; w < 3; ++w)
+    for (int w = 0; w < kTileParameters; ++w)
       if (e->tile[schedule][w] >= 0) *tile_field(tile, w) = e->tile[schedule][w];
     const bool learned =
         schedule == GZB_SCHEDULE_BATCHED && e->have_model && tile.order == GZB_ORDER_MODEL;
@@ -3147,7 +3277,8 @@ extern "C" int gzb_engine_autotune(gzb_engine *e, int schedule, int which, const
         e->tile[schedule][which] = keep;
         return rc;
       }
-      t = e->stage_ms[3];
+      // the stage the parameter acts on: seed search or gapped
+      t = e->stage_ms[which == GZB_TILE_SEED_WALKER ? 1 : 3];
     }
     if (ms) ms[i] = t;
     if (t < best_ms) {

@@ -157,30 +157,82 @@ __device__ __forceinline__ uint32_t walk_offset(uint32_t x4, uint32_t qa) {
   return prmt_imm<(uint32_t)(J | ((4 + J) << 4) | ((8 | J) << 8) | ((8 | J) << 12))>(x4, qa);
 }
 
-// One side of SeedSearcher::UngappedExtend (src/seed_searcher.h:133-158 with
-// UngappedExtender::ExtendOneSideScoreOnly, src/ungapped_extender.h:34-82)
-// from s0[0]/s1[0] (query/database) stepping by INC: returns the best prefix
-// score, stopping at the X-drop (best - score >= cutoff, cutoff >= 1), at a
-// delimiter, or once the best exceeds stop_above.  The reference's
-// (best, run) pair is (best, score - best) here.  Reads four residue pairs
-// per pair of aligned 32-bit loads; the sequences carry delimiter padding
-// of at least 8 bytes on each side.  *steps counts pairs examined.
+constexpr int kWalkPrefetch = 5;
+
+// One sequence's words around a walk start: chunk k covers residues
+// s[4k .. 4k+3] (INC > 0) or s[-4k-3 .. -4k] (INC < 0), and reads the words
+// (p[k], p[k + 1]) forward or (p[-k], p[1 - k]) reverse; w[i] holds p[i]
+// forward and p[1 - i] reverse for the first kWalkPrefetch chunks.
 template <int INC>
-__device__ __forceinline__ int walk_side(const uint8_t *s0, const uint8_t *s1,
-                                         const char *tbl, int cutoff, int stop_above,
-                                         int *steps) {
-  // chunk k covers residues s[4k .. 4k+3] (INC > 0) or s[-4k-3 .. -4k] (INC < 0)
-  const uintptr_t a0 = (uintptr_t)s0 - (INC > 0 ? 0 : 3);
-  const uintptr_t b0 = (uintptr_t)s1 - (INC > 0 ? 0 : 3);
-  const uint32_t *pa = (const uint32_t *)(a0 & ~(uintptr_t)3);
-  const uint32_t *pb = (const uint32_t *)(b0 & ~(uintptr_t)3);
-  const uint32_t sha = 8u * (uint32_t)(a0 & 3), shb = 8u * (uint32_t)(b0 & 3);
-  uint32_t a_lo = __ldg(pa), a_hi = __ldg(pa + 1);
-  uint32_t b_lo = __ldg(pb), b_hi = __ldg(pb + 1);
+struct WalkWords {
+  const uint32_t *p;
+  uint32_t sh;
+  uint32_t w[kWalkPrefetch + 1];
+};
+
+template <int INC>
+__device__ __forceinline__ void load_walk_words(WalkWords<INC> &ww, const uint8_t *s) {
+  const uintptr_t a = (uintptr_t)s - (INC > 0 ? 0 : 3);
+  ww.p = (const uint32_t *)(a & ~(uintptr_t)3);
+  ww.sh = 8u * (uint32_t)(a & 3);
+#pragma unroll
+  for (int i = 0; i <= kWalkPrefetch; ++i) ww.w[i] = __ldg(ww.p + (INC > 0 ? i : 1 - i));
+}
+
+// walk_side over words already loaded (see walk_side)
+template <int INC>
+__device__ __forceinline__ int walk_side_words(const WalkWords<INC> &A, const WalkWords<INC> &B,
+                                               const char *tbl, int cutoff, int stop_above,
+                                               int *steps) {
+  constexpr int K = kWalkPrefetch;
+  const uint32_t sha = A.sh, shb = B.sh;
   int score = 0, best = 0, n = 0, v = 0;
-  for (;;) {
-    const uint32_t qa = __funnelshift_r(a_lo, a_hi, sha);
-    const uint32_t x4 = (qa ^ __funnelshift_r(b_lo, b_hi, shb)) << 2;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const uint32_t qa = INC > 0 ? __funnelshift_r(A.w[k], A.w[k + 1], sha)
+                                : __funnelshift_r(A.w[k + 1], A.w[k], sha);
+    const uint32_t qb = INC > 0 ? __funnelshift_r(B.w[k], B.w[k + 1], shb)
+                                : __funnelshift_r(B.w[k + 1], B.w[k], shb);
+    const uint32_t x4p = (qa ^ qb) << 2;
+#define GZB_WALK_PRE(J)                                                    \
+  {                                                                        \
+    v = *(const int32_t *)(tbl + walk_offset<(INC > 0 ? (J) : 3 - (J))>(x4p, qa)); \
+    score += v;                                                            \
+    best = imax(best, score);                                              \
+    if (best - score >= cutoff || best > stop_above) {                     \
+      n += (J) + 1;                                                        \
+      goto done;                                                           \
+    }                                                                      \
+  }
+    GZB_WALK_PRE(0)
+    GZB_WALK_PRE(1)
+    GZB_WALK_PRE(2)
+    GZB_WALK_PRE(3)
+#undef GZB_WALK_PRE
+    n += 4;
+  }
+  {
+    // past the prefetched chunks: one new word per chunk
+    const uint32_t *pa = A.p, *pb = B.p;
+    uint32_t a_lo, a_hi, b_lo, b_hi;
+    if (INC > 0) {
+      pa += K;
+      pb += K;
+      a_lo = A.w[K];
+      b_lo = B.w[K];
+      a_hi = __ldg(pa + 1);
+      b_hi = __ldg(pb + 1);
+    } else {
+      pa -= K;
+      pb -= K;
+      a_hi = A.w[K];
+      b_hi = B.w[K];
+      a_lo = __ldg(pa);
+      b_lo = __ldg(pb);
+    }
+    for (;;) {
+      const uint32_t qa = __funnelshift_r(a_lo, a_hi, sha);
+      const uint32_t x4 = (qa ^ __funnelshift_r(b_lo, b_hi, shb)) << 2;
 #define GZB_WALK_STEP(J)                                                   \
   {                                                                        \
     v = *(const int32_t *)(tbl + walk_offset<(INC > 0 ? (J) : 3 - (J))>(x4, qa)); \
@@ -188,33 +240,56 @@ __device__ __forceinline__ int walk_side(const uint8_t *s0, const uint8_t *s1,
     best = imax(best, score);                                              \
     if (best - score >= cutoff || best > stop_above) {                     \
       n += (J) + 1;                                                        \
-      break;                                                               \
+      goto done;                                                           \
     }                                                                      \
   }
-    GZB_WALK_STEP(0)
-    GZB_WALK_STEP(1)
-    GZB_WALK_STEP(2)
-    GZB_WALK_STEP(3)
+      GZB_WALK_STEP(0)
+      GZB_WALK_STEP(1)
+      GZB_WALK_STEP(2)
+      GZB_WALK_STEP(3)
 #undef GZB_WALK_STEP
-    n += 4;
-    if (INC > 0) {
-      a_lo = a_hi;
-      b_lo = b_hi;
-      pa += 1;
-      pb += 1;
-      a_hi = __ldg(pa + 1);
-      b_hi = __ldg(pb + 1);
-    } else {
-      a_hi = a_lo;
-      b_hi = b_lo;
-      pa -= 1;
-      pb -= 1;
-      a_lo = __ldg(pa);
-      b_lo = __ldg(pb);
+      n += 4;
+      if (INC > 0) {
+        a_lo = a_hi;
+        b_lo = b_hi;
+        pa += 1;
+        pb += 1;
+        a_hi = __ldg(pa + 1);
+        b_hi = __ldg(pb + 1);
+      } else {
+        a_hi = a_lo;
+        b_hi = b_lo;
+        pa -= 1;
+        pb -= 1;
+        a_lo = __ldg(pa);
+        b_lo = __ldg(pb);
+      }
     }
   }
+done:
   *steps += n - (v == kWalkDelim ? 1 : 0);
   return best;
+}
+
+// One side of SeedSearcher::UngappedExtend (src/seed_searcher.h:133-158 with
+// UngappedExtender::ExtendOneSideScoreOnly, src/ungapped_extender.h:34-82)
+// from s0[0]/s1[0] (query/database) stepping by INC: returns the best prefix
+// score, stopping at the X-drop (best - score >= cutoff, cutoff >= 1), at a
+// delimiter, or once the best exceeds stop_above.  The reference's
+// (best, run) pair is (best, score - best) here.  Reads four residue pairs
+// per pair of aligned 32-bit words.  The first kWalkPrefetch chunks' words
+// are loaded together up front (most walks end inside them, so a walk waits
+// for one round of loads instead of one per chunk); a longer walk goes on
+// one word per chunk.  The sequences carry delimiter padding of at least
+// 4 (kWalkPrefetch + 1) bytes on each side.  *steps counts pairs examined.
+template <int INC>
+__device__ __forceinline__ int walk_side(const uint8_t *s0, const uint8_t *s1,
+                                         const char *tbl, int cutoff, int stop_above,
+                                         int *steps) {
+  WalkWords<INC> A, B;
+  load_walk_words(A, s0);
+  load_walk_words(B, s1);
+  return walk_side_words(A, B, tbl, cutoff, stop_above, steps);
 }
 
 // SeedSearcher::UngappedExtend on the walk table: reverse from (q-1, d-1),
@@ -245,14 +320,17 @@ struct GappedJob {
   int delim, gap_open, gap_ext, cutoff;
 };
 
-// Tile of the gapped stage: the one-thread-per-extension kernel
-// (GZB_GAPPED_KERNEL_*), the flat kernel's bookkeeping threshold, and
-// whether the batched schedule orders extensions by the cost model
-// (GZB_ORDER_MODEL) or keeps hit order (GZB_ORDER_HITS).
+// Tile of the presearch: the gapped stage's one-thread-per-extension kernel
+// (GZB_GAPPED_KERNEL_*), the flat kernel's bookkeeping threshold, whether
+// the batched schedule orders extensions by the cost model (GZB_ORDER_MODEL)
+// or keeps hit order (GZB_ORDER_HITS), and the seed search's walker (one
+// lane per seed-search unit, GZB_SEED_WALKER_UNIT; or the unit batch's seeds
+// dealt to the lanes, GZB_SEED_WALKER_DEALT).
 struct GappedTile {
   int kernel;
   int book_threshold;
   int order;
+  int seed_walker;
 };
 
 struct GappedOut {
@@ -278,6 +356,222 @@ __device__ __forceinline__ int find_delimiter_column(const uint8_t *q0, int inc,
     if (m) return c + base + __ffs(m) - 1;
   }
   return c + limit;
+}
+
+// ---------------------------------------------------------------------------
+// One extension by a group of G lanes (G = 4, 8, 16 or 32; the warp's
+// 32 / G groups each run their own extension).  The same DP as
+// gapped_extend_warp below, the row cut into chunks of G columns: a chunk's
+// scans are G-wide shuffles within the group, and the row's running
+// maximum, horizontal gap and diagonal carry over from chunk to chunk, so
+// the result does not depend on G.  `band` is this group's circular buffer
+// of W int2 columns; exact under the same X-drop condition.
+template <int G>
+struct LaneGroup {
+  int lane;        // lane within the group
+  int shift;       // the group's first lane within the warp
+  unsigned mask;   // the group's lanes
+  __device__ LaneGroup() {
+    const int l = threadIdx.x & 31;
+    lane = l & (G - 1);
+    shift = l & ~(G - 1);
+    mask = G == 32 ? 0xffffffffu : (((1u << (G & 31)) - 1u) << shift);
+  }
+  // the group's lanes' predicates as bits 0..G-1
+  __device__ unsigned ballot(bool p) const {
+    const unsigned b = __ballot_sync(mask, p) >> shift;
+    return G == 32 ? b : (b & ((1u << (G & 31)) - 1u));
+  }
+  __device__ int up(int v, int o) const { return __shfl_up_sync(mask, v, o, G); }
+  __device__ int at(int v, int src) const { return __shfl_sync(mask, v, src, G); }
+  __device__ void sync() const { __syncwarp(mask); }
+};
+
+template <int G>
+__device__ __forceinline__ int find_delimiter_column_group(const LaneGroup<G> &g,
+                                                           const uint8_t *q0, int inc,
+                                                           int delim, int c, int limit) {
+  for (int base = 0; base < limit; base += G) {
+    const int k = base + g.lane;
+    bool is_delim = false;
+    if (k < limit) is_delim = q0[(c + k - 1) * inc] == delim;
+    const unsigned m = g.ballot(is_delim);
+    if (m) return c + base + __ffs(m) - 1;
+  }
+  return c + limit;
+}
+
+template <int G, int W>
+__device__ GappedOut gapped_extend_group(const GappedJob &job, const int *sm, int2 *band,
+                                         uint32_t qpos, uint32_t dpos, bool reverse) {
+  const LaneGroup<G> g;
+  constexpr int wmask = W - 1;
+  const int lane = g.lane;
+  const int inc = reverse ? -1 : 1;
+  const int delim = job.delim;
+  const int ge = job.gap_ext;
+  const int gi = job.gap_open + job.gap_ext;
+  const int cutoff = job.cutoff;
+  const uint8_t *q0 = job.query + qpos;
+  const uint8_t *d0 = job.db + dpos;
+  GappedOut out;
+  out.score = 0;
+  out.pos0 = -inc;
+  out.pos1 = -inc;
+  out.cells = 0;
+  out.overflow = false;
+  if (q0[0] == delim || d0[0] == delim) return out;
+
+  // row -1: horizontal gap run from column 1 while >= -cutoff
+  int k0;
+  if (-gi < -cutoff) {
+    k0 = 0;
+  } else if (ge == 0) {
+    k0 = 1 << 30;
+  } else {
+    long long kk = ((long long)cutoff - gi) / ge + 1;
+    k0 = kk > (1 << 30) ? (1 << 30) : (int)kk;
+  }
+  int col = find_delimiter_column_group(g, q0, inc, delim, 1, k0 > W ? W + 1 : k0);
+  if (col > W) {
+    out.overflow = true;
+    return out;
+  }
+  for (int c = 1 + lane; c < col; c += G) {
+    const int s = -gi - (c - 1) * ge;
+    band[c & wmask] = make_int2(s, s - gi);
+  }
+  if (lane == 0) band[0] = make_int2(0, -gi);
+  int bs = 0, be;
+  if (q0[(col - 1) * inc] != delim) {
+    if (col + 1 > W) {
+      out.overflow = true;
+      return out;
+    }
+    if (lane == 0) band[col & wmask] = make_int2(kInitScore, kInitScore);
+    be = col + 1;
+  } else {
+    be = col;
+  }
+  g.sync();
+
+  int maxs = 0, mp0 = -inc, mp1 = -inc;
+  uint64_t cells = 0;
+  for (int r = 0;; ++r) {
+    const int x = d0[r * inc];
+    if (x == delim) break;
+    const int *mrow = sm + x * kMatrixStride;
+    const int2 st0 = band[bs & wmask];
+    int diag = st0.x;
+    const int nb0 = (maxs - st0.y > cutoff) ? kInitScore : st0.y;
+    int F = nb0 - gi;
+    g.sync();
+    if (lane == 0) band[bs & wmask] = make_int2(nb0, st0.y - ge);
+    int M = maxs;
+    int first_kept = -1, last_kept = bs;
+    for (int cs = bs + 1; cs < be; cs += G) {
+      const int c = cs + lane;
+      const bool active = c < be;
+      int2 st = make_int2(kInitScore, kInitScore);
+      int qres = 0;
+      if (active) {
+        st = band[c & wmask];
+        qres = q0[(c - 1) * inc];
+      }
+      int prev = g.up(st.x, 1);
+      if (lane == 0) prev = diag;
+      const int Gv = imax(prev + mrow[qres], st.y);
+      int P = active ? Gv - gi + (lane + 1) * ge : kNegBig;
+#pragma unroll
+      for (int o = 1; o < G; o <<= 1) {
+        const int t = g.up(P, o);
+        if (lane >= o) P = imax(P, t);
+      }
+      int Pex = g.up(P, 1);
+      if (lane == 0) Pex = kNegBig;
+      const int raw = imax(Gv, imax(F, Pex) - lane * ge);
+      int R = active ? raw : kNegBig;
+#pragma unroll
+      for (int o = 1; o < G; o <<= 1) {
+        const int t = g.up(R, o);
+        if (lane >= o) R = imax(R, t);
+      }
+      const int Mrow = imax(M, R);
+      const bool pruned = (Mrow - raw > cutoff);
+      if (active) {
+        const int nb = pruned ? kInitScore : raw;
+        const int ng = pruned ? kInitScore : imax(raw - gi, st.y - ge);
+        band[c & wmask] = make_int2(nb, ng);
+      }
+      const int nact = imin(G, be - cs);
+      const int cm = g.at(R, G - 1);
+      if (cm > M) {
+        const unsigned hitm = g.ballot(active && raw == cm);
+        const int l = __ffs(hitm) - 1;
+        maxs = cm;
+        mp0 = (cs + l - 1) * inc;
+        mp1 = r * inc;
+      }
+      const unsigned kept = g.ballot(active && !pruned);
+      if (kept) {
+        if (first_kept < 0) first_kept = cs + __ffs(kept) - 1;
+        last_kept = cs + 31 - __clz(kept);
+      }
+      const int Plast = g.at(P, nact - 1);
+      F = imax(F, Plast) - nact * ge;
+      M = imax(M, cm);
+      diag = g.at(st.x, G - 1);
+      cells += (uint64_t)nact;
+    }
+    g.sync();
+    if (first_kept < 0) break;  // every cell pruned: array_start + 1 == array_end
+    bs = first_kept - 1;
+    bool edge_residue;
+    if (last_kept < be - 1) {
+      edge_residue = q0[(be - 1) * inc] != delim;
+      be = last_kept + 1;
+    } else {
+      int k;
+      const long long room = (long long)F - ((long long)maxs - cutoff);
+      if (room < 0) {
+        k = 0;
+      } else if (ge == 0) {
+        k = 1 << 30;
+      } else {
+        long long kk = room / ge + 1;
+        k = kk > (1 << 30) ? (1 << 30) : (int)kk;
+      }
+      if (k > 0) {
+        const int lim = (be + k - bs > W) ? (W - (be - bs) + 1) : k;
+        k = find_delimiter_column_group(g, q0, inc, delim, be, lim) - be;
+        if (be + k - bs > W) {
+          out.overflow = true;
+          return out;
+        }
+        for (int j = lane; j < k; j += G) {
+          const int v = F - j * ge;
+          band[(be + j) & wmask] = make_int2(v, v - gi);
+        }
+        be += k;
+        cells += (uint64_t)k;
+      }
+      edge_residue = q0[(be - 1) * inc] != delim;
+    }
+    if (edge_residue) {
+      if (be + 1 - bs > W) {
+        out.overflow = true;
+        return out;
+      }
+      if (lane == 0) band[be & wmask] = make_int2(kInitScore, kInitScore);
+      ++be;
+    }
+    g.sync();
+  }
+  out.score = maxs;
+  out.pos0 = mp0;
+  out.pos1 = mp1;
+  out.cells = cells;
+  return out;
 }
 
 // One extension by one full warp.  `band` is a circular buffer of W int2

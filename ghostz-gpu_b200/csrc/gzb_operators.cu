@@ -454,7 +454,7 @@ gapped_deal_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
 }
 
 // process-wide tile defaults (gzb_set_tile_parameter)
-GappedTile g_tile = {GZB_GAPPED_KERNEL_ROWS, 4, GZB_ORDER_MODEL};
+GappedTile g_tile = {GZB_GAPPED_KERNEL_ROWS, 4, GZB_ORDER_MODEL, GZB_SEED_WALKER_UNIT};
 
 template <typename K>
 static int persistent_blocks(K kernel, int block, size_t smem, uint64_t n, uint64_t *blocks) {
@@ -470,6 +470,73 @@ static int persistent_blocks(K kernel, int block, size_t smem, uint64_t n, uint6
   return GZB_OK;
 }
 
+// G lanes per extension (gapped_extend_group), each group pulling the next
+// extension from the work queue as soon as its own ends; a band wider than
+// kGroupBandW columns goes to the spill list (then the warp kernel).
+constexpr int kGroupBlock = 128;
+constexpr int kGroupBandW = 64;
+
+template <int G>
+__global__ void __launch_bounds__(kGroupBlock)
+gapped_group_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number_letters,
+                    int stride, uint64_t n, const uint32_t *__restrict__ order,
+                    unsigned long long *queue, int reverse, const uint8_t *__restrict__ dir,
+                    uint32_t *qpos, uint32_t *dpos, int32_t *scores, uint32_t *spill,
+                    uint32_t *spill_count, unsigned long long *cells_total, uint32_t *cells_out,
+                    const uint64_t *n_dev) {
+  __shared__ int sm[kMatrixStride * kMatrixStride];
+  __shared__ int2 bands[kGroupBlock / G][kGroupBandW];
+  if (n_dev) n = *n_dev;
+  load_matrix(sm, matrix, number_letters, stride);
+  __syncthreads();
+  const LaneGroup<G> g;
+  const int grp = threadIdx.x / G;
+  unsigned long long cells = 0;
+  for (;;) {
+    uint32_t e = 0;
+    int got = 0;
+    if (g.lane == 0) got = flat_fetch(queue, n, order, &e) ? 1 : 0;
+    got = g.at(got, 0);
+    if (!got) break;
+    e = (uint32_t)g.at((int)e, 0);
+    const bool rev = dir ? dir[e] != 0 : reverse != 0;
+    const uint32_t q = qpos[e], d = dpos[e];
+    const GappedOut o = gapped_extend_group<G, kGroupBandW>(job, sm, bands[grp], q, d, rev);
+    if (g.lane == 0) {
+      if (o.overflow) {
+        spill[atomicAdd(spill_count, 1u)] = e;
+        if (cells_out) cells_out[e] = 0xFFFFFFFFu;
+      } else {
+        cells += o.cells;
+        store_result(e, q, d, o, qpos, dpos, scores);
+        if (cells_out) cells_out[e] = (uint32_t)o.cells;
+      }
+    }
+    g.sync();
+  }
+  cells += __shfl_down_sync(0xffffffffu, cells, 16);
+  cells += __shfl_down_sync(0xffffffffu, cells, 8);
+  cells += __shfl_down_sync(0xffffffffu, cells, 4);
+  cells += __shfl_down_sync(0xffffffffu, cells, 2);
+  cells += __shfl_down_sync(0xffffffffu, cells, 1);
+  if ((threadIdx.x & 31) == 0 && cells) atomicAdd(cells_total, cells);
+}
+
+template <int G>
+static int launch_gapped_group(const GappedJob &job, const int32_t *matrix, int number_letters,
+                               int stride, uint64_t n, const uint32_t *order,
+                               unsigned long long *queue, int reverse, const uint8_t *dir,
+                               uint32_t *qpos, uint32_t *dpos, int32_t *scores, uint32_t *spill,
+                               uint32_t *spill_count, unsigned long long *cells_total,
+                               uint32_t *cells_out, cudaStream_t s, const uint64_t *n_dev) {
+  uint64_t blocks = 1;
+  GZB_TRY(persistent_blocks(gapped_group_kernel<G>, kGroupBlock, 0, n * G, &blocks));
+  gapped_group_kernel<G><<<(unsigned)blocks, kGroupBlock, 0, s>>>(
+      job, matrix, number_letters, stride, n, order, queue, reverse, dir, qpos, dpos, scores,
+      spill, spill_count, cells_total, cells_out, n_dev);
+  return GZB_OK;
+}
+
 int launch_gapped_thread(const GappedTile &tile, const GappedJob &job, const int32_t *matrix,
                          int number_letters, int stride, uint64_t n, const uint32_t *order,
                          unsigned long long *queue, int reverse, const uint8_t *dir,
@@ -480,7 +547,27 @@ int launch_gapped_thread(const GappedTile &tile, const GappedJob &job, const int
   // (grids sized for n)
   GZB_CUDA(cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s));
   uint64_t blocks = 1;
-  if (tile.kernel == GZB_GAPPED_KERNEL_DEAL) {
+  const bool group = tile.kernel >= GZB_GAPPED_KERNEL_GROUP4 &&
+                     tile.kernel <= GZB_GAPPED_KERNEL_GROUP32 && warp_path_exact(job.cutoff);
+  if (group) {
+    const int G = 4 << (tile.kernel - GZB_GAPPED_KERNEL_GROUP4);
+    if (G == 4)
+      GZB_TRY(launch_gapped_group<4>(job, matrix, number_letters, stride, n, order, queue,
+                                     reverse, dir, qpos, dpos, scores, spill, spill_count,
+                                     cells_total, cells_out, s, n_dev));
+    else if (G == 8)
+      GZB_TRY(launch_gapped_group<8>(job, matrix, number_letters, stride, n, order, queue,
+                                     reverse, dir, qpos, dpos, scores, spill, spill_count,
+                                     cells_total, cells_out, s, n_dev));
+    else if (G == 16)
+      GZB_TRY(launch_gapped_group<16>(job, matrix, number_letters, stride, n, order, queue,
+                                      reverse, dir, qpos, dpos, scores, spill, spill_count,
+                                      cells_total, cells_out, s, n_dev));
+    else
+      GZB_TRY(launch_gapped_group<32>(job, matrix, number_letters, stride, n, order, queue,
+                                      reverse, dir, qpos, dpos, scores, spill, spill_count,
+                                      cells_total, cells_out, s, n_dev));
+  } else if (tile.kernel == GZB_GAPPED_KERNEL_DEAL) {
     GZB_TRY(persistent_blocks(gapped_deal_kernel, kLaneBlock, 0, n, &blocks));
     gapped_deal_kernel<<<(unsigned)blocks, kLaneBlock, 0, s>>>(
         job, matrix, number_letters, stride, n, order, reverse, dir, qpos, dpos, scores, spill,
@@ -492,7 +579,8 @@ int launch_gapped_thread(const GappedTile &tile, const GappedJob &job, const int
     gapped_lane_kernel<<<(unsigned)blocks, kLaneBlock, 0, s>>>(
         job, matrix, number_letters, stride, n, order, reverse, dir, qpos, dpos, scores, spill,
         spill_count, cells_total, cells_out, n_dev);
-  } else if (tile.kernel == GZB_GAPPED_KERNEL_ROWS) {
+  } else if (tile.kernel == GZB_GAPPED_KERNEL_ROWS || tile.kernel >= GZB_GAPPED_KERNEL_GROUP4) {
+    // (a group kernel's X-drop outside the warp DP's exact range runs here)
     GZB_TRY(persistent_blocks(gapped_rows_kernel, kLaneBlock, 0, n, &blocks));
     gapped_rows_kernel<<<(unsigned)blocks, kLaneBlock, 0, s>>>(
         job, matrix, number_letters, stride, n, order, queue, reverse, dir, qpos, dpos, scores,
@@ -502,7 +590,7 @@ int launch_gapped_thread(const GappedTile &tile, const GappedJob &job, const int
     gapped_lane_queue_kernel<<<(unsigned)blocks, kLaneBlock, 0, s>>>(
         job, matrix, number_letters, stride, n, order, queue, reverse, dir, qpos, dpos, scores,
         spill, spill_count, cells_total, cells_out, n_dev);
-  } else {
+  } else if (tile.kernel == GZB_GAPPED_KERNEL_FLAT) {
     const size_t smem = sizeof(int2) * (size_t)kFlatW * kFlatBlock;
     GZB_CUDA(cudaFuncSetAttribute(gapped_flat_kernel,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -990,14 +1078,20 @@ extern "C" int gzb_gapped_extender_cells(gzb_gapped_extender *h, uint64_t *cells
 namespace gzb {
 int check_tile_value(int which, int value) {
   if (which == GZB_TILE_GAPPED_KERNEL) {
-    GZB_CHECK(value >= GZB_GAPPED_KERNEL_FLAT && value <= GZB_GAPPED_KERNEL_DEAL,
+    GZB_CHECK(value >= GZB_GAPPED_KERNEL_FLAT && value <= GZB_GAPPED_KERNEL_GROUP32,
               GZB_ERR_INVALID,
-              "gapped kernel %d is none of GZB_GAPPED_KERNEL_FLAT/LANE/ROWS/STATIC/DEAL", value);
+              "gapped kernel %d is none of GZB_GAPPED_KERNEL_FLAT/LANE/ROWS/STATIC/DEAL/GROUP*",
+              value);
     return GZB_OK;
   }
   if (which == GZB_TILE_ORDER) {
     GZB_CHECK(value == GZB_ORDER_HITS || value == GZB_ORDER_MODEL, GZB_ERR_INVALID,
               "order %d is neither GZB_ORDER_HITS nor GZB_ORDER_MODEL", value);
+    return GZB_OK;
+  }
+  if (which == GZB_TILE_SEED_WALKER) {
+    GZB_CHECK(value == GZB_SEED_WALKER_UNIT || value == GZB_SEED_WALKER_DEALT, GZB_ERR_INVALID,
+              "seed walker %d is neither GZB_SEED_WALKER_UNIT nor GZB_SEED_WALKER_DEALT", value);
     return GZB_OK;
   }
   GZB_CHECK(which == GZB_TILE_BOOK_THRESHOLD, GZB_ERR_INVALID, "unknown tile parameter %d", which);
@@ -1007,12 +1101,14 @@ int check_tile_value(int which, int value) {
 int *tile_field(GappedTile &t, int which) {
   return which == GZB_TILE_GAPPED_KERNEL ? &t.kernel
          : which == GZB_TILE_ORDER      ? &t.order
+         : which == GZB_TILE_SEED_WALKER ? &t.seed_walker
                                         : &t.book_threshold;
 }
 // a valid value of tile parameter `which` (for checking `which` alone)
 int any_tile_value(int which) {
   return which == GZB_TILE_GAPPED_KERNEL ? GZB_GAPPED_KERNEL_FLAT
          : which == GZB_TILE_ORDER      ? GZB_ORDER_HITS
+         : which == GZB_TILE_SEED_WALKER ? GZB_SEED_WALKER_UNIT
                                         : 1;
 }
 }  // namespace gzb

@@ -339,6 +339,9 @@ SCHEDULE_ORACLE = 2
 TILE_BOOK_THRESHOLD = 0
 TILE_GAPPED_KERNEL = 1
 TILE_ORDER = 2
+TILE_SEED_WALKER = 3
+SEED_WALKER_UNIT = 0
+SEED_WALKER_DEALT = 1
 ORDER_HITS = 0
 ORDER_MODEL = 1
 GAPPED_KERNEL_FLAT = 0
@@ -346,7 +349,23 @@ GAPPED_KERNEL_LANE = 1
 GAPPED_KERNEL_ROWS = 2
 GAPPED_KERNEL_STATIC = 3
 GAPPED_KERNEL_DEAL = 4
+GAPPED_KERNEL_GROUP4 = 5
+GAPPED_KERNEL_GROUP8 = 6
+GAPPED_KERNEL_GROUP16 = 7
+GAPPED_KERNEL_GROUP32 = 8
 COST_FEATURES = 8
+
+
+def set_tile_parameter(which, value):
+    """Process-wide default of tile parameter `which` (the operators' and
+    engines' without a tuned tile)."""
+    check(lib().gzb_set_tile_parameter(int(which), int(value)))
+
+
+def get_tile_parameter(which):
+    v = C.c_int()
+    check(lib().gzb_get_tile_parameter(int(which), C.byref(v)))
+    return int(v.value)
 
 
 def cost_param_count():

@@ -478,22 +478,42 @@ int gzb_engine_get_extension_costs(gzb_engine *e, float *predicted, uint32_t *ce
 #define GZB_TILE_ORDER 2
 #define GZB_ORDER_HITS 0
 #define GZB_ORDER_MODEL 1
+/* GZB_TILE_SEED_WALKER: how the seed search deals its ungapped walks.
+ * GZB_SEED_WALKER_UNIT gives each lane whole seed-search units (a
+ * representative or residual position with every query position of its
+ * list); GZB_SEED_WALKER_DEALT makes the seeds of a warp's 32 units one
+ * stream dealt to the lanes 32 at a time, so lanes wait for the longest
+ * walk of a round instead of the longest list.  Member seeds are dealt in
+ * both.  Results and counters are the same. */
+#define GZB_TILE_SEED_WALKER 3
+#define GZB_SEED_WALKER_UNIT 0
+#define GZB_SEED_WALKER_DEALT 1
 #define GZB_GAPPED_KERNEL_FLAT 0
 #define GZB_GAPPED_KERNEL_LANE 1
 #define GZB_GAPPED_KERNEL_ROWS 2
 #define GZB_GAPPED_KERNEL_STATIC 3
 #define GZB_GAPPED_KERNEL_DEAL 4
+/* GZB_GAPPED_KERNEL_GROUP4 .. _GROUP32: 4, 8, 16 or 32 lanes per extension
+ * (the threads-per-extension axis): a group evaluates a database row's band
+ * columns that many at a time with shuffle scans (exact for X-drops below
+ * 1024, else the _ROWS kernel runs), pulling extensions from the work queue
+ * as soon as its own has ended; a band wider than 64 columns goes to the
+ * warp kernel. */
+#define GZB_GAPPED_KERNEL_GROUP4 5
+#define GZB_GAPPED_KERNEL_GROUP8 6
+#define GZB_GAPPED_KERNEL_GROUP16 7
+#define GZB_GAPPED_KERNEL_GROUP32 8
 int gzb_set_tile_parameter(int which, int value);
 int gzb_get_tile_parameter(int which, int *value);
 /* Per-engine, per-schedule tile: value -1 falls back to the process-wide
  * default.  gzb_engine_autotune stores its pick here. */
 int gzb_engine_set_tile(gzb_engine *e, int schedule, int which, int value);
 int gzb_engine_get_tile(gzb_engine *e, int schedule, int which, int *value);
-/* Times the gapped stage of the resident queries and chunk under each
+/* Times the presearch of the resident queries and chunk under each
  * candidate value (candidates[n]) of tile parameter `which` with
  * `schedule`, keeps the fastest for that schedule (gzb_engine_get_tile) and
- * returns it in *best (gapped-stage ms per candidate in ms[n] if not
- * NULL).  Runs the presearch twice per candidate and clears the engine's
+ * returns it in *best (ms per candidate in ms[n] if not NULL: the seed
+ * search stage's for GZB_TILE_SEED_WALKER, the gapped stage's otherwise).  Runs the presearch twice per candidate and clears the engine's
  * results.  Results are identical under every tile. */
 int gzb_engine_autotune(gzb_engine *e, int schedule, int which, const int *candidates,
                         int n, int *best, float *ms, void *stream);

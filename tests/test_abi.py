@@ -91,15 +91,17 @@ def test_tile_parameters_validate_without_device():
     from gzb import native as N
     L = N.lib()
     v = ctypes.c_int()
-    for which in (N.TILE_BOOK_THRESHOLD, N.TILE_GAPPED_KERNEL, N.TILE_ORDER):
+    for which in (N.TILE_BOOK_THRESHOLD, N.TILE_GAPPED_KERNEL, N.TILE_ORDER,
+                  N.TILE_SEED_WALKER):
         assert L.gzb_get_tile_parameter(which, ctypes.byref(v)) == 0
         keep = v.value
         assert L.gzb_set_tile_parameter(which, keep) == 0
     assert L.gzb_set_tile_parameter(N.TILE_BOOK_THRESHOLD, 0) == 1
     assert L.gzb_set_tile_parameter(N.TILE_BOOK_THRESHOLD, 33) == 1
-    assert L.gzb_set_tile_parameter(N.TILE_GAPPED_KERNEL, 5) == 1
+    assert L.gzb_set_tile_parameter(N.TILE_GAPPED_KERNEL, 9) == 1
     assert b"none of" in L.gzb_last_error()
     assert L.gzb_set_tile_parameter(N.TILE_ORDER, 2) == 1
+    assert L.gzb_set_tile_parameter(N.TILE_SEED_WALKER, 2) == 1
     assert L.gzb_set_tile_parameter(7, 1) == 1
     assert L.gzb_get_tile_parameter(7, ctypes.byref(v)) == 1
 

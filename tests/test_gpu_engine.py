@@ -108,7 +108,8 @@ def test_presearch_repeated_calls_identical(engine, params):
     assert all(np.array_equal(x, y) for x, y in zip(a, b))
 
 
-@pytest.mark.parametrize("kernel,threshold", [(0, 1), (0, 32), (1, 8), (2, 1), (2, 8), (2, 32), (3, 8), (4, 8)])
+@pytest.mark.parametrize("kernel,threshold", [(0, 1), (0, 32), (1, 8), (2, 1), (2, 8), (2, 32), (3, 8), (4, 8),
+                                              (5, 8), (6, 8), (7, 8), (8, 8)])
 def test_presearch_every_gapped_tile(engine, oracle, params, kernel, threshold):
     # every one-thread-per-extension kernel on the work-queue schedule (no
     # model: hit order), and the flat kernel's extreme bookkeeping
@@ -123,3 +124,25 @@ def test_presearch_every_gapped_tile(engine, oracle, params, kernel, threshold):
     finally:
         engine.set_tile(N.SCHEDULE_BATCHED, N.TILE_GAPPED_KERNEL, -1)
         engine.set_tile(N.SCHEDULE_BATCHED, N.TILE_BOOK_THRESHOLD, -1)
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_dealt_seed_walker_matches_oracle(engine, oracle, params, graph):
+    """The dealt seed walker (GZB_SEED_WALKER_DEALT) gives the oracle's
+    survivors, counters and lists, eager and in graph mode, and the same
+    residue-pair count as the per-unit walker."""
+    from gzb import native as N
+    db, q = _small(seed_db=701, seed_q=702)
+    engine.set_tile(N.SCHEDULE_BATCHED, N.TILE_SEED_WALKER, N.SEED_WALKER_DEALT)
+    engine.set_graph(graph)
+    try:
+        cnt = _compare(engine, oracle, params, db, q, schedule=N.SCHEDULE_BATCHED)
+        assert cnt["ungapped_hits"] > 0
+        steps = engine.counters()["ungapped_steps"]
+        engine.set_tile(N.SCHEDULE_BATCHED, N.TILE_SEED_WALKER, N.SEED_WALKER_UNIT)
+        engine.reset_results()
+        engine.presearch(N.SCHEDULE_BATCHED)
+        assert engine.counters()["ungapped_steps"] == steps
+    finally:
+        engine.set_graph(False)
+        engine.set_tile(N.SCHEDULE_BATCHED, N.TILE_SEED_WALKER, -1)

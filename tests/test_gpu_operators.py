@@ -245,3 +245,51 @@ def test_set_query_seeds_expansion(torch_cuda):
     owner = np.repeat(seed_ids, runs)
     assert np.array_equal(d_qid.cpu().numpy().view(np.uint32), list_qid[owner])
     assert np.array_equal(d_qp.cpu().numpy().view(np.uint32), list_qpos[owner])
+
+
+@pytest.mark.parametrize("group", [5, 6, 7, 8])
+def test_gapped_group_kernels_match_oracle(torch_cuda, oracle, params, group):
+    """GZB_GAPPED_KERNEL_GROUP4..32 (4..32 lanes per extension) through the
+    operator API: every X-drop in both directions against the oracle (X-drops
+    outside the group DP's exact range run the rows kernel), and long
+    homologs whose bands outgrow the group's 64 columns."""
+    from gzb import native as N
+    keep = N.get_tile_parameter(N.TILE_GAPPED_KERNEL)
+    N.set_tile_parameter(N.TILE_GAPPED_KERNEL, group)
+    try:
+        for cutoff in (0, 5, 26, 60, 2000, INT_MAX):
+            for reverse in (False, True):
+                rng = np.random.default_rng(3000 + group * 31 + cutoff % 89 + (5 if reverse else 0))
+                n = 200 if cutoff not in (2000, INT_MAX) else 60
+                A, B = _pairs(rng, n, hi=600 if cutoff < 1000 else 250)
+                qc, qs = _concat(A, 25)
+                dc, ds = _concat(B, 25)
+                qpos = [qs[i] + int(rng.integers(0, len(A[i]))) for i in range(n)]
+                dpos = [ds[i] + int(np.clip(qpos[i] - qs[i] + rng.integers(-4, 5), 0,
+                                            len(B[i]) - 1)) for i in range(n)]
+                s, q, d, cells = _gapped_gpu(torch_cuda, params, qc, dc, qpos, dpos, reverse,
+                                             cutoff)
+                total = 0
+                for i in range(n):
+                    es, eq, ed, ec = oracle.gapped_one_side(params, qc, qpos[i], dc, dpos[i],
+                                                            reverse, cutoff)
+                    total += ec
+                    assert (int(s[i]), int(q[i]), int(d[i])) == \
+                        (es, int(qpos[i]) + eq, int(dpos[i]) + ed), (group, cutoff, reverse, i)
+                assert cells == total
+        rng = np.random.default_rng(78)
+        A, B = _pairs(rng, 24, lo=2000, hi=8000)
+        qc, qs = _concat(A, 25)
+        dc, ds = _concat(B, 25)
+        qpos = [qs[i] + len(A[i]) // 2 for i in range(24)]
+        dpos = [ds[i] + len(A[i]) // 2 for i in range(24)]
+        cutoff = int(params["gapped_cutoff"])
+        for rev in (False, True):
+            s, q, d, _ = _gapped_gpu(torch_cuda, params, qc, dc, qpos, dpos, rev, cutoff)
+            for i in range(24):
+                es, eq, ed, _ = oracle.gapped_one_side(params, qc, qpos[i], dc, dpos[i], rev,
+                                                       cutoff)
+                assert (int(s[i]), int(q[i]), int(d[i])) == (es, int(qpos[i]) + eq,
+                                                             int(dpos[i]) + ed)
+    finally:
+        N.set_tile_parameter(N.TILE_GAPPED_KERNEL, keep)
