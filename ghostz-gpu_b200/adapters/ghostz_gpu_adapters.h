@@ -172,7 +172,10 @@ class GappedExtenderGpu {
 // chunk and the index the reference's `db` command saved for it (the
 // chunk's `.sdp` stream) made resident in `engine`, the index converted on
 // the host instead of being rebuilt.  offsets: first residue of each of the
-// number_sequences sequences, then the chunk length.
+// number_sequences sequences, then the chunk length.  Unlike the reference,
+// which reads only its own record, this reads `in` to its end and refuses
+// trailing bytes: the stream must hold exactly one chunk's `.sdp` (open the
+// chunk's own file, or hand over a stream limited to its record).
 inline int LoadChunkWithReferenceIndex(gzb_engine *engine, const gzb_params &params,
                                        int32_t chunk_id, const Code *sequence,
                                        uint64_t length, const uint32_t *offsets,

@@ -15,15 +15,20 @@
 //    rejected with GZB_ERR_OVERFLOW);
 //  * the rare extensions that need the serial fallback may use a band of at
 //    most kNoAllocBand columns (query remainders up to kNoAllocBand - 2
-//    residues); wider ones are reported as GZB_ERR_OVERFLOW;
+//    residues); wider ones are reported as GZB_ERR_OVERFLOW after every
+//    kernel has run, so on that return the position and score buffers are
+//    undefined (the other extensions have already moved their positions in
+//    place): a caller that wants to retry must keep its own copy of the
+//    input positions;
 //  * the array (about 12 MB) is held by every GPU that loads the library
 //    until the process exits;
 //  * every call shares the array, and it keeps the last call's contents:
 //    calls that overlap on the GPU (from several host threads or streams at
 //    once) race with each other and must be serialised by the caller;
-//  * the first call on a device looks up the array's device address
-//    (cudaGetSymbolAddress), so that first call should come before any
-//    stream capture.
+//  * every call ends by copying a counter to host memory and synchronising
+//    `stream`, so the entry point cannot run inside a stream capture at all;
+//    the first call on a device also looks up the array's device address
+//    (cudaGetSymbolAddress) once.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -133,15 +138,18 @@ extern "C" int gzb_gapped_extend_one_side_score_only_noalloc(
   job.gap_ext = gap_extension;
   job.cutoff = cutoff;
   const int stride = (int)number_letters + 1;
-  const size_t blocks = (size + 127) / 128;
-  gapped_lane_kernel<<<(unsigned)(blocks < 148 * 40 ? blocks : 148 * 40), 128, 0, s>>>(
+  int dev = 0, sms = 0;
+  GZB_CUDA(cudaGetDevice(&dev));
+  GZB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const size_t blocks = (size + 127) / 128, cap = (size_t)sms * 40;
+  gapped_lane_kernel<<<(unsigned)(blocks < cap ? blocks : cap), 128, 0, s>>>(
       job, d_score_matrix, (int)number_letters, stride, size, nullptr, reverse, nullptr,
       d_query_concatenated_positions, d_database_positions, d_scores, spill1, counters, cells,
       nullptr, nullptr);
   GZB_CUDA(cudaGetLastError());
   const uint32_t *serial_list = spill1, *serial_count = counters;
   if (warp_path_exact(cutoff)) {
-    gapped_warp_kernel<<<148 * 4, 256, 0, s>>>(job, d_score_matrix, (int)number_letters,
+    gapped_warp_kernel<<<sms * 4, 256, 0, s>>>(job, d_score_matrix, (int)number_letters,
                                                 stride, spill1, counters, reverse, nullptr,
                                                 d_query_concatenated_positions,
                                                 d_database_positions, d_scores, spill2,

@@ -197,12 +197,14 @@ int gzb_gapped_extender_cells(gzb_gapped_extender *h, uint64_t *cells);
  * loop that cannot take an allocation's implicit device synchronisation.
  * Its scratch is one fixed device array in the library (about 12 MB, held on
  * every GPU that loads the library until exit).  Limits: at most 2^20
- * extensions per call, and extensions needing the serial fallback may use
- * bands of at most 8192 columns; larger requests return GZB_ERR_OVERFLOW.
- * Every call shares that array: calls that overlap on the GPU race and must
- * be serialised by the caller.  The first call on a device looks up the
- * array's address, so make it before any stream capture.  Synchronises
- * `stream` before returning. */
+ * extensions per call (more: GZB_ERR_OVERFLOW before any device work), and
+ * extensions needing the serial fallback may use bands of at most 8192
+ * columns (wider: GZB_ERR_OVERFLOW after the kernels have run, the position
+ * and score buffers then undefined, so a caller that wants to retry keeps
+ * its own copy of the input positions).  Every call shares that array:
+ * calls that overlap on the GPU race and must be serialised by the caller.
+ * Every call ends by reading a counter into host memory and synchronising
+ * `stream`, so it cannot be used inside a stream capture. */
 int gzb_gapped_extend_one_side_score_only_noalloc(
     const uint8_t *d_query_sequence, const uint8_t *d_database_sequence,
     uint8_t sequence_delimiter, const int32_t *d_score_matrix,
