@@ -23,9 +23,12 @@ index_build_s), as the reference's `db` step is separate from `aln`.
 (compiled from the reference's sources) on 1,000 queries x the first
 20,000 database sequences.
 
-Multi-GPU: replicas -- every rank runs the full workload on its own GPU
-(the reference's -g threads replicate the work too); value sums the ranks'
-queries over the slowest rank's device time.
+Multi-GPU (one process per GPU, each with its own copy of the chunk):
+--split queries (the default) gives each rank a contiguous slice of the
+query set -- queries are independent, so no exchange -- and value is the
+whole query set over the slowest rank's device time (strong scaling);
+--split replicas runs the whole workload on every rank, as the reference's
+-g threads replicate the work (weak scaling).
 
 --impl reference times the reference's own CPU search (`ghostz aln -g 0`
 with every host core, compiled from the reference's sources into
@@ -793,7 +796,8 @@ def run_multichunk(args, world, rank, local_rank):
                    "mode": "stored: every chunk's codes and index resident in HBM, swapped in "
                            "per chunk",
                    "l2": "inputs larger than L2 (each chunk > 126 MB)",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": (f"queries split over {world} GPUs" if split == "queries"
+                                   else f"replicas x{world}")},
         "streamed": {"value": reps.throughput(nq, steps, t_streamed), "unit": UNIT,
                      "ms_per_step": t_streamed / steps,
                      "h2d_bytes_per_step": int(sum(len(c.codes) + c.offsets.nbytes + len(bl)
@@ -851,6 +855,9 @@ def main():
     ap.add_argument("--ref-queries", type=int, default=2000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true")
+    ap.add_argument("--split", default="queries", choices=["queries", "replicas"],
+                    help="several GPUs: split the queries over them (default) or run a "
+                         "replica of the whole workload on each")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--once", action="store_true",
                     help="one batched presearch (hit order, default tile, no training or "
@@ -913,6 +920,22 @@ def main():
     torch.cuda.set_device(local_rank)
     reps = Replicas("nccl", timeout_s=600)
     db, q, gen_s, raw = make_workload(args.workload)
+    # several GPUs: each searches its slice of the queries against its own
+    # copy of the chunk (--split queries, strong scaling) or the whole query
+    # set (--split replicas, weak scaling)
+    split = args.split if world > 1 else "replicas"
+    if split == "queries":
+        from gzb import shards as S
+        from gzb import workload as W
+        qb, qe = S.query_range(rank, world, q.number)
+        q = S.slice_queries(q, qb, qe)
+        if isinstance(raw, list):
+            raw = raw[qb:qe]
+        else:
+            o0, o1 = int(raw.offsets[qb]), int(raw.offsets[qe])
+            raw = W.Reads(dna=raw.dna[o0:o1].copy(),
+                          offsets=(raw.offsets[qb:qe + 1] - raw.offsets[qb]).astype(np.uint64),
+                          sources=raw.sources[qb:qe])
     params = P.make_params()
     eng = N.PresearchEngine(local_rank)
     eng.set_params(params)
@@ -1126,14 +1149,16 @@ def main():
     # max over ranks
     t_dev, t_e2e = reps.max([dev_ms, e2e_ms])
     nq = q.number
-    value = reps.throughput(nq, args.steps, t_dev)
-    e2e_value = reps.throughput(nq, args.steps, t_e2e)
+    # queries every step searches over all ranks
+    step_units = int(reps.sum([nq])[0]) if split == "queries" else world * nq
+    value = step_units * args.steps / (t_dev / 1e3)
+    e2e_value = step_units * args.steps / (t_e2e / 1e3)
     steps = args.steps
     st = stage
     sched_report = {}
     for name, r in runs.items():
         sched_report[name] = {
-            "value": world * nq * steps / (r["ms"] / 1e3), "ms_per_step": r["ms"] / steps,
+            "value": step_units * steps / (r["ms"] / 1e3), "ms_per_step": r["ms"] / steps,
             "gapped_ms": r["stage"]["gapped"], "seed_ungapped_ms": r["stage"]["seed_ungapped"],
             "dp_gcups_gapped_stage": (r["counters"]["gapped_cells"] / (r["stage"]["gapped"] / 1e3)
                                       / 1e9) if r["stage"]["gapped"] else None}
@@ -1183,7 +1208,8 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
         "warmup": args.warmup, "ms_per_step": t_dev / steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "scaling": "strong" if split == "queries" else "weak", "vs_baseline": None,
+        "dtype": "int32",
         "data": "synthetic (seeded generator with the config's shapes)",
         "config": {"workload": args.workload,
                    "schedule": (f"batched in graph mode (one CUDA graph per chunk): "
@@ -1192,7 +1218,8 @@ def main():
                                 f"(autotuned), cost model trained on the GPU"
                                 if args.schedule == "batched" else "plain static"),
                    "db_sequences": db.number_sequences, "db_residues": db.length,
-                   "queries": nq, "l2": "inputs larger than L2 (database chunk > 126 MB)",
+                   "queries": step_units,
+                   "l2": "inputs larger than L2 (database chunk > 126 MB)",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": t_e2e / steps,

@@ -1,8 +1,10 @@
-"""Multi-GPU plumbing of the benchmark: one process per GPU, each running
-the whole presearch on its own copy of the chunk and its queries.  The
-reference's -g threads replicate the work the same way; nothing on this path
-is exchanged between devices, so the process group carries only the barrier
-around the timed region and the slowest rank's time."""
+"""Multi-GPU plumbing of the benchmark: one process per GPU, each holding
+its own copy of the chunk and searching either the whole query set (a
+replica, as the reference's -g threads replicate the work) or its slice of
+the queries (gzb.shards.query_range).  Queries are independent of each
+other, so nothing on this path is exchanged between devices: the process
+group carries only the barrier around the timed region, the slowest rank's
+time and the ranks' query counts."""
 import os
 from datetime import timedelta
 
@@ -39,6 +41,15 @@ class Replicas:
     def throughput(self, units_per_rank, steps, max_ms):
         """Whole-job rate: every rank's units over the slowest rank's time."""
         return self.world * units_per_rank * steps / (max_ms / 1e3)
+
+    def sum(self, values):
+        """Element-wise sum over ranks of a list of numbers."""
+        if self.dist is None:
+            return [float(v) for v in values]
+        import torch
+        t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return [float(v) for v in t.cpu()]
 
     def close(self):
         if self.dist is not None:

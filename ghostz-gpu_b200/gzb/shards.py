@@ -22,6 +22,34 @@ def chunks_of(rank, world, n_chunks):
     return list(range(rank, n_chunks, world))
 
 
+def query_range(rank, world, n_queries):
+    """The queries [begin, end) rank `rank` of `world` searches when the
+    query set is split over GPUs (every query is independent of the others,
+    so the split needs no exchange): contiguous, sizes differing by at most
+    one."""
+    return rank * n_queries // world, (rank + 1) * n_queries // world
+
+
+def slice_queries(queries, begin, end):
+    """Queries begin .. end - 1 of a query set in the engine layout
+    (concatenated, shared delimiters) as a query set of their own."""
+    from . import workload as W
+    if end <= begin:
+        return W.Queries(codes=np.full(1, queries.codes[0], np.uint8),
+                         offsets=np.zeros(0, np.uint32), lengths=np.zeros(0, np.uint32),
+                         cutoffs=np.zeros(0, np.int32), triggers=np.zeros(0, np.int32),
+                         sources=np.zeros(0, np.int64))
+    o0 = int(queries.offsets[begin])
+    o1 = int(queries.offsets[end - 1]) + int(queries.lengths[end - 1])
+    src = queries.sources[begin:end] if queries.sources is not None else None
+    return W.Queries(codes=np.ascontiguousarray(queries.codes[o0:o1]),
+                     offsets=(queries.offsets[begin:end].astype(np.int64) - o0).astype(np.uint32),
+                     lengths=np.ascontiguousarray(queries.lengths[begin:end]),
+                     cutoffs=np.ascontiguousarray(queries.cutoffs[begin:end]),
+                     triggers=np.ascontiguousarray(queries.triggers[begin:end]),
+                     sources=src)
+
+
 def merge_in_order(params, lists, q0=0, q1=None):
     """lists[c] = (counts, records) of chunk c alone; returns the running
     merge of all of them in chunk order, for queries q0 .. q1 - 1."""

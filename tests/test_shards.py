@@ -270,3 +270,23 @@ def test_search_drives_the_engine_chunk_by_chunk(oracle):
     _same(got, _expected(oracle, params, chunks))
     assert e.calls == [c for k in range(N_CHUNKS)
                        for c in (("set_database", k), ("reset_results",), ("presearch", 1))]
+
+
+def test_query_split_covers_every_query_once():
+    from gzb import shards as S
+    from gzb import workload as W
+    db = W.make_database(200, 41, median=120)
+    q = W.make_queries(db, 37, 42, median=120)
+    for world in (1, 2, 3, 8, 40):
+        seen = []
+        for r in range(world):
+            b, e = S.query_range(r, world, q.number)
+            part = S.slice_queries(q, b, e)
+            assert part.number == e - b
+            for i in range(part.number):
+                o, n = int(part.offsets[i]), int(part.lengths[i])
+                oo, nn = int(q.offsets[b + i]), int(q.lengths[b + i])
+                assert np.array_equal(part.codes[o:o + n], q.codes[oo:oo + nn])
+                assert part.cutoffs[i] == q.cutoffs[b + i]
+            seen += list(range(b, e))
+        assert seen == list(range(q.number))
