@@ -64,6 +64,9 @@ WORKLOADS = {
     "protein-50k-uneven-x-2M": (2_000_000, 201, 50_000, 402,
                                 {"median": 250, "sigma": 1.0, "lo": 20, "hi": 8000}),
     "protein-1k-x-200k": (200_000, 211, 1_000, 212, {}),   # small case for profiling
+    # small case whose chunk (360 MB of codes) is larger than L2, for DRAM
+    # traffic captures
+    "protein-1k-x-1M": (1_000_000, 221, 1_000, 222, {}),
     # translated DNA: 150-nt reads, 40 % reverse-translated DB fragments with
     # 1 % substitutions; six-frame translation, SEG and cutoffs on the GPU
     "dna-200k-reads-x-2M": (2_000_000, 201, 200_000, 302, {"read_length": 150}),
@@ -77,10 +80,17 @@ PREP_CPU_READS = 15_000  # oracle sample of the CPU baseline
 # 8 B of centres + 2L window bytes + 1 B result.
 BYTES_PER_UNGAPPED_STEP = 2
 BYTES_PER_DISTANCE_SEED = 8 + 2 * 10 + 1
-# DRAM bytes (read + write) of one launch of the seed-search kernels
-# (seed_kernel + member_kernel) on each workload, from one ncu capture of the
-# bench command (profiles/seed_kernels_dram_*.txt); None when not captured
-SEED_KERNEL_DRAM_BYTES = {"protein-10k-x-2M": (40.96e9 + 0.074e9) + (64.54e9 + 0.005e9)}
+# DRAM traffic of the seed-search kernels (seed_kernel + member_kernel, read +
+# write) per algorithmic byte, from one ncu capture on the 1,000-query x
+# 1,000,000-protein case, whose chunk is larger than L2
+# (profiles/seed_kernels_dram_protein-1k-x-1M.md: 7.994 GB of DRAM traffic
+# for 6.321 GB of algorithmic bytes); the bench scales it by each run's own
+# algorithmic bytes
+SEED_KERNEL_TRAFFIC_PER_BYTE = 7.994e9 / 6.321e9
+# B200 integer throughput for the DP roofline: 148 SMs x 128 INT32 lanes per
+# clock (nominal; no measured integer peak exists), at the sampled SM clock
+B200_SMS, INT32_LANES_PER_SM = 148, 128
+DP_INT_OPS_PER_CELL = 10
 
 
 def log(msg):
@@ -836,6 +846,20 @@ def run_multichunk(args, world, rank, local_rank):
     reps.close()
 
 
+def dp_int_pipe(gcups, clocks):
+    """The gapped DP's integer throughput against B200's INT32 lanes: ten
+    integer operations per DP cell (the oracle's inner-loop body) at the
+    stage's GCUPS, over 148 SMs x 128 lanes at the median SM clock sampled
+    during the timed region (a nominal peak: no measured integer peak)."""
+    mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    peak = B200_SMS * INT32_LANES_PER_SM * mhz * 1e6
+    achieved = gcups * 1e9 * DP_INT_OPS_PER_CELL
+    return {"achieved_int_ops_per_s": achieved, "peak_int_ops_per_s": peak,
+            "frac": achieved / peak, "ops_per_cell": DP_INT_OPS_PER_CELL,
+            "peak_source": f"nominal: {B200_SMS} SMs x {INT32_LANES_PER_SM} INT32 lanes x "
+                           f"{mhz:.0f} MHz (sampled)"}
+
+
 KERNEL_NAMES = {0: "flat", 1: "lane", 2: "rows", 3: "static", 4: "deal", 5: "group4", 6: "group8",
                 7: "group16", 8: "group32"}
 ORDER_NAMES = {0: "hits", 1: "cost model"}
@@ -861,7 +885,9 @@ def main():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--once", action="store_true",
                     help="one batched presearch (hit order, default tile, no training or "
-                         "autotuning) of the workload, for profiling; prints its stage times")
+                         "autotuning) of the workload after a first one that sizes the "
+                         "buffers, then its build-results step, for profiling; prints the "
+                         "stage times")
     ap.add_argument("--prep-only", type=int, default=0, metavar="READS",
                     help="time only the query preparation of READS 150-nt reads (reads "
                          "drawn from a 20,000-protein database) and print its JSON object")
@@ -886,9 +912,21 @@ def main():
         eng.set_database(db)
         eng.set_queries(q)
         eng.set_tile(N.SCHEDULE_BATCHED, N.TILE_ORDER, N.ORDER_HITS)
-        eng.presearch(N.SCHEDULE_BATCHED)
-        print(json.dumps({"workload": args.workload, "stage_ms": eng.stage_ms(),
-                          "counters": eng.counters()}), flush=True)
+        eng.presearch(N.SCHEDULE_BATCHED)   # sizes the buffers
+        eng.reset_results()
+        eng.presearch(N.SCHEDULE_BATCHED)   # the profiled one
+        stage_ms, counters = eng.stage_ms(), eng.counters()
+        stream = torch.cuda.current_stream()
+        b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        b0.record(stream)
+        aligned = eng.build_alignments(stream)   # build results of the profiled presearch
+        b1.record(stream)
+        torch.cuda.synchronize()
+        print(json.dumps({"workload": args.workload, "stage_ms": stage_ms,
+                          "counters": counters,
+                          "build_results": {"ms": b0.elapsed_time(b1),
+                                            "alignments": int(sum(len(a) for a in aligned))}}),
+              flush=True)
         eng.close()
         return
     if args.prep_only:
@@ -1195,10 +1233,14 @@ def main():
     seed_bytes = (counters["distance_seeds"] * BYTES_PER_DISTANCE_SEED
                   + BYTES_PER_UNGAPPED_STEP * steps_pairs)
     achieved = seed_bytes / (st["seed_kernels"] / 1e3) / 1e9 if st["seed_kernels"] else 0.0
-    traffic = SEED_KERNEL_DRAM_BYTES.get(args.workload)
+    traffic = SEED_KERNEL_TRAFFIC_PER_BYTE * seed_bytes
     roofline = {"bound": "hbm", "kernel": "seed_kernel + member_kernel (seed search, distance, "
                 "ungapped X-drop)", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak, "traffic": traffic,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
+                                  "seed_kernel + member_kernel on protein-1k-x-1M (1.265 B "
+                                  "per algorithmic byte), scaled by this run's algorithmic "
+                                  "bytes",
                 "algorithmic_bytes": seed_bytes, "kernel_ms": st["seed_kernels"],
                 "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)"
                 if peak_src == "measured" else "fallback 6650 GB/s",
@@ -1228,6 +1270,7 @@ def main():
                         "hash lists -> presearch -> build results -> alignment records "
                         "(no text formatting)"},
         "dp_gcups": {"gapped_stage": gcups_stage, "whole_step": gcups_step},
+        "dp_int_pipe": dp_int_pipe(gcups_stage, clocks),
         "stage_ms": st, "counters": counters, "schedules": sched_report,
         "index_build_s": index_s, "index_cache": index_cache, "build_results": build_results,
         "query_preparation": query_prep,
