@@ -1,7 +1,10 @@
-"""Stored and prefetched database chunks: a database of several chunks
-searched through the engine's slots (every chunk stored on the device, or
-streamed through two slots with copies on a side stream) gives the merged
-results of setting each chunk in turn."""
+"""A database of several chunks, searched chunk after chunk (each set in
+turn), through the engine's slots (every chunk stored on the device, or
+streamed through two slots with copies on a side stream) and as shards
+merged on the host: every mode gives the oracle's chunk loop, i.e. each
+chunk's presearch merged into the running lists by AddResults in chunk
+order (src/aligner_gpu_presearch_thread.cpp:214-640 with
+AlignerCommon::AddResults, src/aligner_common.h:147-274)."""
 import numpy as np
 import pytest
 
@@ -29,6 +32,31 @@ def _database(n_chunks=3):
     return chunks, W.pack_queries(seqs)
 
 
+def _oracle_chunk_loop(oracle, params, chunks, q):
+    """Each chunk's presearch lists (chunk_id set to the chunk) merged into
+    the running lists in chunk order.  Merging a chunk's own top-b lists
+    gives the running merge of its raw candidates (tests/test_shards.py
+    checks that on the CPU)."""
+    import oracle as O
+    running = [np.zeros(0, O.RESULT_DTYPE) for _ in range(q.number)]
+    for k, db in enumerate(chunks):
+        res, _, _ = oracle.presearch(params, db, q)
+        for i in range(q.number):
+            added = res[i].copy()
+            added["chunk_id"] = k
+            running[i] = oracle.add_results(params, db, added, running[i])
+    return running
+
+
+@pytest.fixture(scope="module")
+def case(oracle, params):
+    chunks, q = _database()
+    exp = _oracle_chunk_loop(oracle, params, chunks, q)
+    assert sum(len(r) for r in exp) > 0
+    assert len({int(x["chunk_id"]) for r in exp for x in r}) == len(chunks)
+    return chunks, q, exp
+
+
 def _sequential(N, params, chunks, q):
     e = N.PresearchEngine(0)
     try:
@@ -49,12 +77,14 @@ def _same(a, b):
         assert np.array_equal(x, y), i
 
 
-def test_stored_chunks_match_sequential(native, params):
+def test_sequential_chunks_match_oracle(native, params, case):
+    chunks, q, exp = case
+    _same(_sequential(native, params, chunks, q), exp)
+
+
+def test_stored_chunks_match_oracle(native, params, case):
     N = native
-    chunks, q = _database()
-    exp = _sequential(N, params, chunks, q)
-    assert sum(len(r) for r in exp) > 0
-    assert len({int(x["chunk_id"]) for r in exp for x in r}) == len(chunks)
+    chunks, q, exp = case
     e = N.PresearchEngine(0)
     try:
         e.set_params(params)
@@ -73,11 +103,10 @@ def test_stored_chunks_match_sequential(native, params):
         e.close()
 
 
-def test_prefetched_chunks_match_sequential(native, params):
+def test_prefetched_chunks_match_oracle(native, params, case):
     import torch
     N = native
-    chunks, q = _database()
-    exp = _sequential(N, params, chunks, q)
+    chunks, q, exp = case
     e = N.PresearchEngine(0)
     try:
         e.set_params(params)
@@ -129,15 +158,13 @@ def test_slot_refusals(native, params):
         e.close()
 
 
-def test_chunk_shards_match_sequential(native, params):
+def test_chunk_shards_match_oracle(native, params, case):
     """Each chunk searched alone (results reset before it), its lists merged
     on the host in chunk order (the exchange step of chunks spread over
-    GPUs, here one process), equals one engine searching the chunks in
-    turn."""
+    GPUs, here one process), equals the oracle's chunk loop."""
     from gzb import shards as S
     N = native
-    chunks, q = _database()
-    exp = _sequential(N, params, chunks, q)
+    chunks, q, exp = case
     e = N.PresearchEngine(0)
     try:
         e.set_params(params)
