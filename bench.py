@@ -806,8 +806,7 @@ def run_multichunk(args, world, rank, local_rank):
                    "mode": "stored: every chunk's codes and index resident in HBM, swapped in "
                            "per chunk",
                    "l2": "inputs larger than L2 (each chunk > 126 MB)",
-                   "parallelism": (f"queries split over {world} GPUs" if split == "queries"
-                                   else f"replicas x{world}")},
+                   "parallelism": f"replicas x{world}"},
         "streamed": {"value": reps.throughput(nq, steps, t_streamed), "unit": UNIT,
                      "ms_per_step": t_streamed / steps,
                      "h2d_bytes_per_step": int(sum(len(c.codes) + c.offsets.nbytes + len(bl)
@@ -863,6 +862,7 @@ def dp_int_pipe(gcups, clocks):
 KERNEL_NAMES = {0: "flat", 1: "lane", 2: "rows", 3: "static", 4: "deal", 5: "group4", 6: "group8",
                 7: "group16", 8: "group32"}
 ORDER_NAMES = {0: "hits", 1: "cost model"}
+WALKER_NAMES = {0: "unit", 1: "dealt"}
 
 
 def main():
@@ -961,8 +961,8 @@ def main():
     # several GPUs: each searches its slice of the queries against its own
     # copy of the chunk (--split queries, strong scaling) or the whole query
     # set (--split replicas, weak scaling)
-    split = args.split if world > 1 else "replicas"
-    if split == "queries":
+    split = args.split
+    if split == "queries" and world > 1:
         from gzb import shards as S
         from gzb import workload as W
         qb, qe = S.query_range(rank, world, q.number)
@@ -1046,17 +1046,38 @@ def main():
             thr_ms = {}
             if ker in (N.GAPPED_KERNEL_FLAT, N.GAPPED_KERNEL_ROWS):
                 thr, thr_ms = eng.autotune(sid, (1, 2, 4, 8, 16), N.TILE_BOOK_THRESHOLD)
+            # threads per extension: the chosen one-lane kernel against 4, 8,
+            # 16 and 32 lanes per extension
+            groups = (N.GAPPED_KERNEL_GROUP4, N.GAPPED_KERNEL_GROUP8, N.GAPPED_KERNEL_GROUP16,
+                      N.GAPPED_KERNEL_GROUP32)
+            ker, thr_ext_ms = eng.autotune(sid, (ker,) + groups, N.TILE_GAPPED_KERNEL)
+            lanes = {k: 4 << (k - N.GAPPED_KERNEL_GROUP4) if k in groups else 1
+                     for k in thr_ext_ms}
+            # band columns per lane of the rows kernel (shared memory against
+            # blocks per SM and hand-offs to the warp kernel)
+            band_ms = {}
+            if ker == N.GAPPED_KERNEL_ROWS:
+                band, band_ms = eng.autotune(sid, (32, 64, 128), N.TILE_BAND_WIDTH)
             # whether the cost model's order pays for its features and
             # prediction on this workload (hit order otherwise)
             order_t, order_ms = eng.autotune(sid, (N.ORDER_MODEL, N.ORDER_HITS), N.TILE_ORDER)
+            # the seed search's walker (seed-stage times)
+            walker, walker_ms = eng.autotune(sid, (N.SEED_WALKER_UNIT, N.SEED_WALKER_DEALT),
+                                             N.TILE_SEED_WALKER)
             tiles = {"gapped_ms_by_kernel": {KERNEL_NAMES[k]: v for k, v in ker_ms.items()},
                      "gapped_ms_by_book_threshold": thr_ms,
-                     "gapped_ms_by_order": {ORDER_NAMES[k]: v for k, v in order_ms.items()}}
-        for w in (N.TILE_GAPPED_KERNEL, N.TILE_BOOK_THRESHOLD):
+                     "gapped_ms_by_threads": {lanes[k]: v for k, v in thr_ext_ms.items()},
+                     "gapped_ms_by_band": band_ms,
+                     "gapped_ms_by_order": {ORDER_NAMES[k]: v for k, v in order_ms.items()},
+                     "seed_ms_by_walker": {WALKER_NAMES[k]: v for k, v in walker_ms.items()}}
+        for w in (N.TILE_GAPPED_KERNEL, N.TILE_BOOK_THRESHOLD, N.TILE_BAND_WIDTH,
+                  N.TILE_SEED_WALKER):
             eng.set_tile(N.SCHEDULE_ORACLE, w, eng.tile(sid, w))
         tiles.update(kernel=KERNEL_NAMES[eng.tile(sid, N.TILE_GAPPED_KERNEL)],
                      book_threshold=eng.tile(sid, N.TILE_BOOK_THRESHOLD),
-                     order=ORDER_NAMES[eng.tile(sid, N.TILE_ORDER)])
+                     band_width=eng.tile(sid, N.TILE_BAND_WIDTH),
+                     order=ORDER_NAMES[eng.tile(sid, N.TILE_ORDER)],
+                     seed_walker=WALKER_NAMES[eng.tile(sid, N.TILE_SEED_WALKER)])
 
     sampler = ClockSampler(local_rank)
     sampler.start()
@@ -1256,13 +1277,16 @@ def main():
         "config": {"workload": args.workload,
                    "schedule": (f"batched in graph mode (one CUDA graph per chunk): "
                                 f"persistent work-queue kernel "
-                                f"'{tiles.get('kernel')}', order '{tiles.get('order')}' "
-                                f"(autotuned), cost model trained on the GPU"
+                                f"'{tiles.get('kernel')}' ({tiles.get('band_width')} band "
+                                f"columns), order '{tiles.get('order')}', seed walker "
+                                f"'{tiles.get('seed_walker')}' (autotuned), cost model "
+                                f"trained on the GPU"
                                 if args.schedule == "batched" else "plain static"),
                    "db_sequences": db.number_sequences, "db_residues": db.length,
                    "queries": step_units,
                    "l2": "inputs larger than L2 (database chunk > 126 MB)",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": (f"queries split over {world} GPUs" if split == "queries"
+                                   else f"replicas x{world}")},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": t_e2e / steps,
                 "results_equal_device_loop": bool(e2e_same),

@@ -1,17 +1,19 @@
 // reference_device_layer.cu -- the device layer of GHOSTZ-GPU's own GPU
 // aligner, implemented over this library.
 //
-// GHOSTZ-GPU keeps everything that touches the GPU in seven CUDA files:
-// the three operators (src/distance_calculator_gpu.cu,
-// src/ungapped_extender_gpu.cu, src/gapped_extender_gpu.cu and their kernel
-// files), the device data holder (src/aligner_gpu_data.cu), the per-stream
-// device buffers (src/device_seeds_memory.cu) and the code packing
-// (src/packed_alphabet_code.cu).  This file defines the classes those files
-// define -- DistanceCalculatorGpu, UngappedExtenderGpu, GappedExtenderGpu,
-// AlignerGpuData, DeviceSeedsMemory -- against the reference's own headers,
-// calling libghostz_b200.so.  Compiled with the reference's headers on the
-// include path and linked in place of those seven objects (plus
-// -lghostz_b200), it makes the reference's `ghostz-gpu aln -g N` run its
+// GHOSTZ-GPU keeps everything that touches the GPU in nine CUDA files
+// (CU_SRC of its Makefile): the three operators (src/distance_calculator_gpu.cu,
+// src/ungapped_extender_gpu.cu, src/gapped_extender_gpu.cu and their three
+// kernel files), the device data holder (src/aligner_gpu_data.cu), the
+// per-stream device buffers (src/device_seeds_memory.cu) and the code
+// packing (src/packed_alphabet_code.cu).  This file defines the classes the
+// first eight define -- DistanceCalculatorGpu, UngappedExtenderGpu,
+// GappedExtenderGpu, AlignerGpuData, DeviceSeedsMemory -- against the
+// reference's own headers, calling libghostz_b200.so.  Compiled with the
+// reference's headers on the include path and linked in place of those
+// eight objects (plus -lghostz_b200; the packing file's host functions are
+// compiled from the reference as they are), it makes the reference's
+// `ghostz-gpu aln -g N` run its
 // unchanged host code (AlignerGpu, AlignerGpuPresearchThread,
 // SeedSearcherGpu, GpuStreamController / GpuStreamRunner, ...) on this
 // library's kernels.

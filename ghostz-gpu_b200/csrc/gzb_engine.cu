@@ -56,7 +56,7 @@ __global__ void gapped_serial_kernel(GappedJob job, const int32_t *__restrict__ 
                                      uint32_t *too_long_count);
 
 extern GappedTile g_tile;
-constexpr int kTileParameters = 4;  // GZB_TILE_BOOK_THRESHOLD .. GZB_TILE_SEED_WALKER
+constexpr int kTileParameters = 5;  // GZB_TILE_BOOK_THRESHOLD .. GZB_TILE_BAND_WIDTH
 int check_tile_value(int which, int value);
 int *tile_field(GappedTile &t, int which);
 int any_tile_value(int which);
@@ -1267,7 +1267,8 @@ struct gzb_engine {
       tb_walk_off, tb_ops, tb_row_meta, tb_walk, tb_walk_n, tb_score, tb_p0, tb_p1, tb_out;
   uint64_t pred_n = 0;       // extensions with a prediction in epred (last run)
   DBuf enb;                  // per surviving hit: chained neighbours (cost feature)
-  int tile[3][kTileParameters] = {{-1, -1, -1, -1}, {-1, -1, -1, -1}, {-1, -1, -1, -1}};
+  int tile[3][kTileParameters] = {
+      {-1, -1, -1, -1, -1}, {-1, -1, -1, -1, -1}, {-1, -1, -1, -1, -1}};
   // [schedule][which], -1 = default
   bool logging = false;
   uint64_t log_cap = 0;
@@ -2775,7 +2776,7 @@ uint64_t graph_key(const gzb_engine *e, int schedule, const GappedTile &tile, bo
   const uint64_t v[] = {e->db_len, e->nseq, (uint64_t)(int64_t)e->chunk_id, e->nq, e->q_len,
                         e->max_qlen, (uint64_t)schedule, (uint64_t)tile.kernel,
                         (uint64_t)tile.book_threshold, (uint64_t)tile.order,
-                        (uint64_t)tile.seed_walker, c.hits, c.mwork,
+                        (uint64_t)tile.seed_walker, (uint64_t)tile.band_width, c.hits, c.mwork,
                         (uint64_t)(uintptr_t)e->spill, e->spill_cap,
                         (uint64_t)(uintptr_t)e->band_pool, (uint64_t)(uintptr_t)e->gcounters,
                         (uint64_t)(uintptr_t)e->gcells, (uint64_t)(uintptr_t)e->report_h,

@@ -325,12 +325,14 @@ struct GappedJob {
 // the batched schedule orders extensions by the cost model (GZB_ORDER_MODEL)
 // or keeps hit order (GZB_ORDER_HITS), and the seed search's walker (one
 // lane per seed-search unit, GZB_SEED_WALKER_UNIT; or the unit batch's seeds
-// dealt to the lanes, GZB_SEED_WALKER_DEALT).
+// dealt to the lanes, GZB_SEED_WALKER_DEALT), and the rows kernel's band
+// columns per lane (GZB_TILE_BAND_WIDTH: 32, 64 or 128).
 struct GappedTile {
   int kernel;
   int book_threshold;
   int order;
   int seed_walker;
+  int band_width;
 };
 
 struct GappedOut {
@@ -896,10 +898,11 @@ namespace gzb {
 // ---------------------------------------------------------------------------
 // Gapped extension, one thread per extension (the common, narrow-band case).
 // The exact serial recurrence of GappedExtender::ExtendOneSideScoreOnly with
-// the band in shared memory: kLaneW columns per thread, each a packed int16
-// pair (best, best_gap), plus the query residue of each band column (one
-// byte), laid out [column][thread] so that a warp touching one column per
-// thread is bank-conflict free.  A band wider than kLaneW, or a value
+// the band in shared memory: W columns per thread (a power of two; kLaneW
+// unless the rows kernel's band-width tile says otherwise), each a packed
+// int16 pair (best, best_gap), plus the query residue of each band column
+// (one byte), laid out [column][thread] so that a warp touching one column
+// per thread is bank-conflict free.  A band wider than W, or a value
 // outside int16, makes the extension overflow; the caller reruns it on the
 // warp kernel.
 constexpr int kLaneW = 64;
@@ -909,15 +912,18 @@ constexpr int kLaneW = 64;
 // of warp w (blocks of four warps), so the lanes of a warp never conflict,
 // whatever columns they are at (with the plain [column][thread] byte layout
 // four lanes share each bank).
+template <int W = kLaneW>
 struct LaneBand {
-  uint32_t *cell;  // [kLaneW][stride]
-  uint8_t *res;    // [kLaneW][stride], lane-major within a column
+  static_assert(W >= 8 && (W & (W - 1)) == 0, "the band width is a power of two");
+  static constexpr int kW = W;
+  uint32_t *cell;  // [W][stride]
+  uint8_t *res;    // [W][stride], lane-major within a column
   int stride;      // threads of the block (128)
   int t;           // this thread's column in the cell layout
   int tr;          // this thread's byte in the residue layout
   __device__ __forceinline__ LaneBand(uint32_t *cell_, uint8_t *res_, int stride_, int t_)
       : cell(cell_), res(res_), stride(stride_), t(t_), tr(((t_ & 31) << 2) | (t_ >> 5)) {}
-  __device__ __forceinline__ int base(int c) const { return (c & (kLaneW - 1)) * stride; }
+  __device__ __forceinline__ int base(int c) const { return (c & (W - 1)) * stride; }
   __device__ __forceinline__ int slot(int c) const { return base(c) + t; }
   __device__ __forceinline__ uint32_t &at(int c) { return cell[slot(c)]; }
   __device__ __forceinline__ int residue(int c) const { return res[base(c) + tr]; }
@@ -950,7 +956,8 @@ enum : int { kLaneRunning = 0, kLaneDone = 1, kLaneOverflow = 2 };
 // Row -1 of GappedExtender::ExtendOneSideScoreOnly
 // (src/gapped_extender.cpp:345-364): the gap-open row along the query until
 // it drops below -cutoff, plus the sentinel column.
-__device__ __forceinline__ int lane_init(const GappedJob &job, LaneBand &band, LaneExt &x,
+template <int W>
+__device__ __forceinline__ int lane_init(const GappedJob &job, LaneBand<W> &band, LaneExt &x,
                                          const uint8_t *q0, const uint8_t *d0, bool reverse) {
   const int inc = reverse ? -1 : 1;
   const int delim = job.delim;
@@ -987,7 +994,7 @@ __device__ __forceinline__ int lane_init(const GappedJob &job, LaneBand &band, L
     for (int j = 0; j < 4; ++j) {
       r = (int)((w >> (8 * j)) & 0xffu);
       if (r == delim || score < -job.cutoff) goto init_done;
-      if (col >= kLaneW) return kLaneOverflow;
+      if (col >= W) return kLaneOverflow;
       band.at(col) = pack16(score, score - gi);
       band.set_residue(col, r);
       score -= ge;
@@ -1006,7 +1013,7 @@ __device__ __forceinline__ int lane_init(const GappedJob &job, LaneBand &band, L
 init_done:
   x.bs = 0;
   if (r != delim) {
-    if (col >= kLaneW) return kLaneOverflow;
+    if (col >= W) return kLaneOverflow;
     band.at(col) = pack16(kInitScore, kInitScore);
     band.set_residue(col, r);
     x.be = col + 1;
@@ -1019,7 +1026,8 @@ init_done:
 // One database row of the recurrence (src/gapped_extender.cpp:366-470):
 // the cells of the band, the X-drop trimming of its left edge, and the
 // right edge moving or growing along the gap row.
-__device__ __forceinline__ int lane_row(const GappedJob &job, const int *sm, LaneBand &band,
+template <int W>
+__device__ __forceinline__ int lane_row(const GappedJob &job, const int *sm, LaneBand<W> &band,
                                         LaneExt &x) {
   const int inc = x.inc;
   const int delim = job.delim;
@@ -1084,7 +1092,7 @@ __device__ __forceinline__ int lane_row(const GappedJob &job, const int *sm, Lan
   } else {
     edge = q0[(be - 1) * inc];
     while (row_gap >= maxs - cutoff && edge != delim) {
-      if (be - bs >= kLaneW) return kLaneOverflow;
+      if (be - bs >= W) return kLaneOverflow;
       x.ovf |= !fits16(row_gap) || !fits16(row_gap - gi);
       band.at(be) = pack16(row_gap, row_gap - gi);
       band.set_residue(be, edge);
@@ -1095,7 +1103,7 @@ __device__ __forceinline__ int lane_row(const GappedJob &job, const int *sm, Lan
     }
   }
   if (edge != delim) {
-    if (be - bs >= kLaneW) return kLaneOverflow;
+    if (be - bs >= W) return kLaneOverflow;
     band.at(be) = pack16(kInitScore, kInitScore);
     // the sentinel column's own residue (differs from `edge` when the band shrank)
     band.set_residue(be, q0[(be - 1) * inc]);
@@ -1106,8 +1114,9 @@ __device__ __forceinline__ int lane_row(const GappedJob &job, const int *sm, Lan
   return kLaneRunning;
 }
 
+template <int W>
 __device__ inline GappedOut gapped_extend_lane(const GappedJob &job, const int *sm,
-                                               LaneBand band, uint32_t qpos, uint32_t dpos,
+                                               LaneBand<W> band, uint32_t qpos, uint32_t dpos,
                                                bool reverse) {
   LaneExt x;
   int st = lane_init(job, band, x, job.query + qpos, job.db + dpos, reverse);

@@ -215,7 +215,7 @@ gapped_lane_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
   if (n_dev) n = *n_dev;
   load_matrix(sm, matrix, number_letters, stride);
   __syncthreads();
-  LaneBand band(cells_s, res_s, kLaneBlock, (int)threadIdx.x);
+  LaneBand<kLaneW> band(cells_s, res_s, kLaneBlock, (int)threadIdx.x);
   unsigned long long cells = 0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
@@ -280,7 +280,7 @@ gapped_lane_queue_kernel(GappedJob job, const int32_t *__restrict__ matrix, int 
   if (n_dev) n = *n_dev;
   load_matrix(sm, matrix, number_letters, stride);
   __syncthreads();
-  LaneBand band(cells_s, res_s, kLaneBlock, (int)threadIdx.x);
+  LaneBand<kLaneW> band(cells_s, res_s, kLaneBlock, (int)threadIdx.x);
   const int lane = threadIdx.x & 31;
   unsigned long long cells = 0;
   for (;;) {
@@ -321,6 +321,17 @@ gapped_lane_queue_kernel(GappedJob job, const int32_t *__restrict__ matrix, int 
 // `refill_threshold` lanes of its warp are idle (or no lane has work left):
 // those lanes then fetch, load and start their next extensions together, so
 // one round of memory latency and one pass of the set-up code serve them all.
+// W: band columns per lane (the GZB_TILE_BAND_WIDTH tile): a narrower band
+// fits more blocks on an SM and hands more extensions to the warp kernel.
+// Bands up to 64 columns live in static shared memory (the fastest form
+// measured); wider ones, above the 48 KB static limit, in dynamic shared
+// memory, rows_band_bytes(W) per block.
+__host__ __device__ constexpr bool rows_band_static(int W) { return W <= 64; }
+constexpr size_t rows_band_bytes(int W) {
+  return rows_band_static(W) ? 0 : (size_t)W * kLaneBlock * 5;
+}
+
+template <int W>
 __global__ void __launch_bounds__(kLaneBlock)
 gapped_rows_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number_letters,
                    int stride, uint64_t n, const uint32_t *__restrict__ order,
@@ -329,12 +340,17 @@ gapped_rows_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
                    uint32_t *spill_count, unsigned long long *cells_total,
                    uint32_t *cells_out, int refill_threshold, const uint64_t *n_dev) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
-  __shared__ uint32_t cells_s[kLaneW * kLaneBlock];
-  __shared__ uint8_t res_s[kLaneW * kLaneBlock];
+  constexpr bool kStatic = rows_band_static(W);
+  __shared__ uint32_t cells_st[kStatic ? W * kLaneBlock : 1];
+  __shared__ uint8_t res_st[kStatic ? W * kLaneBlock : 1];
+  extern __shared__ __align__(16) uint8_t rows_band[];
+  // [W][kLaneBlock] each
+  uint32_t *cells_s = kStatic ? cells_st : reinterpret_cast<uint32_t *>(rows_band);
+  uint8_t *res_s = kStatic ? res_st : rows_band + (size_t)W * kLaneBlock * 4;
   if (n_dev) n = *n_dev;
   load_matrix(sm, matrix, number_letters, stride);
   __syncthreads();
-  LaneBand band(cells_s, res_s, kLaneBlock, (int)threadIdx.x);
+  LaneBand<W> band(cells_s, res_s, kLaneBlock, (int)threadIdx.x);
   LaneExt x;
   uint32_t e = 0, q = 0, d = 0;
   bool have = false, done = false;
@@ -397,7 +413,7 @@ gapped_deal_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
   if (n_dev) n = *n_dev;
   load_matrix(sm, matrix, number_letters, stride);
   __syncthreads();
-  LaneBand band(cells_s, res_s, kLaneBlock, (int)threadIdx.x);
+  LaneBand<kLaneW> band(cells_s, res_s, kLaneBlock, (int)threadIdx.x);
   const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   // the next extension of this lane, loaded one extension ahead
@@ -454,7 +470,7 @@ gapped_deal_kernel(GappedJob job, const int32_t *__restrict__ matrix, int number
 }
 
 // process-wide tile defaults (gzb_set_tile_parameter)
-GappedTile g_tile = {GZB_GAPPED_KERNEL_ROWS, 4, GZB_ORDER_MODEL, GZB_SEED_WALKER_UNIT};
+GappedTile g_tile = {GZB_GAPPED_KERNEL_ROWS, 4, GZB_ORDER_MODEL, GZB_SEED_WALKER_UNIT, kLaneW};
 
 template <typename K>
 static int persistent_blocks(K kernel, int block, size_t smem, uint64_t n, uint64_t *blocks) {
@@ -537,6 +553,25 @@ static int launch_gapped_group(const GappedJob &job, const int32_t *matrix, int 
   return GZB_OK;
 }
 
+template <int W>
+static int launch_gapped_rows(const GappedTile &tile, const GappedJob &job, const int32_t *matrix,
+                              int number_letters, int stride, uint64_t n, const uint32_t *order,
+                              unsigned long long *queue, int reverse, const uint8_t *dir,
+                              uint32_t *qpos, uint32_t *dpos, int32_t *scores, uint32_t *spill,
+                              uint32_t *spill_count, unsigned long long *cells_total,
+                              uint32_t *cells_out, cudaStream_t s, const uint64_t *n_dev) {
+  const size_t smem = rows_band_bytes(W);
+  if (smem)
+    GZB_CUDA(cudaFuncSetAttribute(gapped_rows_kernel<W>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  uint64_t blocks = 1;
+  GZB_TRY(persistent_blocks(gapped_rows_kernel<W>, kLaneBlock, smem, n, &blocks));
+  gapped_rows_kernel<W><<<(unsigned)blocks, kLaneBlock, smem, s>>>(
+      job, matrix, number_letters, stride, n, order, queue, reverse, dir, qpos, dpos, scores,
+      spill, spill_count, cells_total, cells_out, tile.book_threshold, n_dev);
+  return GZB_OK;
+}
+
 int launch_gapped_thread(const GappedTile &tile, const GappedJob &job, const int32_t *matrix,
                          int number_letters, int stride, uint64_t n, const uint32_t *order,
                          unsigned long long *queue, int reverse, const uint8_t *dir,
@@ -581,10 +616,18 @@ int launch_gapped_thread(const GappedTile &tile, const GappedJob &job, const int
         spill_count, cells_total, cells_out, n_dev);
   } else if (tile.kernel == GZB_GAPPED_KERNEL_ROWS || tile.kernel >= GZB_GAPPED_KERNEL_GROUP4) {
     // (a group kernel's X-drop outside the warp DP's exact range runs here)
-    GZB_TRY(persistent_blocks(gapped_rows_kernel, kLaneBlock, 0, n, &blocks));
-    gapped_rows_kernel<<<(unsigned)blocks, kLaneBlock, 0, s>>>(
-        job, matrix, number_letters, stride, n, order, queue, reverse, dir, qpos, dpos, scores,
-        spill, spill_count, cells_total, cells_out, tile.book_threshold, n_dev);
+    if (tile.band_width == 32)
+      GZB_TRY(launch_gapped_rows<32>(tile, job, matrix, number_letters, stride, n, order, queue,
+                                     reverse, dir, qpos, dpos, scores, spill, spill_count,
+                                     cells_total, cells_out, s, n_dev));
+    else if (tile.band_width == 128)
+      GZB_TRY(launch_gapped_rows<128>(tile, job, matrix, number_letters, stride, n, order,
+                                      queue, reverse, dir, qpos, dpos, scores, spill,
+                                      spill_count, cells_total, cells_out, s, n_dev));
+    else
+      GZB_TRY(launch_gapped_rows<64>(tile, job, matrix, number_letters, stride, n, order, queue,
+                                     reverse, dir, qpos, dpos, scores, spill, spill_count,
+                                     cells_total, cells_out, s, n_dev));
   } else if (tile.kernel == GZB_GAPPED_KERNEL_LANE) {
     GZB_TRY(persistent_blocks(gapped_lane_queue_kernel, kLaneBlock, 0, n, &blocks));
     gapped_lane_queue_kernel<<<(unsigned)blocks, kLaneBlock, 0, s>>>(
@@ -1094,6 +1137,11 @@ int check_tile_value(int which, int value) {
               "seed walker %d is neither GZB_SEED_WALKER_UNIT nor GZB_SEED_WALKER_DEALT", value);
     return GZB_OK;
   }
+  if (which == GZB_TILE_BAND_WIDTH) {
+    GZB_CHECK(value == 32 || value == 64 || value == 128, GZB_ERR_INVALID,
+              "band width %d is none of 32, 64, 128", value);
+    return GZB_OK;
+  }
   GZB_CHECK(which == GZB_TILE_BOOK_THRESHOLD, GZB_ERR_INVALID, "unknown tile parameter %d", which);
   GZB_CHECK(value >= 1 && value <= 32, GZB_ERR_INVALID, "book threshold %d outside 1..32", value);
   return GZB_OK;
@@ -1102,6 +1150,7 @@ int *tile_field(GappedTile &t, int which) {
   return which == GZB_TILE_GAPPED_KERNEL ? &t.kernel
          : which == GZB_TILE_ORDER      ? &t.order
          : which == GZB_TILE_SEED_WALKER ? &t.seed_walker
+         : which == GZB_TILE_BAND_WIDTH  ? &t.band_width
                                         : &t.book_threshold;
 }
 // a valid value of tile parameter `which` (for checking `which` alone)
@@ -1109,6 +1158,7 @@ int any_tile_value(int which) {
   return which == GZB_TILE_GAPPED_KERNEL ? GZB_GAPPED_KERNEL_FLAT
          : which == GZB_TILE_ORDER      ? GZB_ORDER_HITS
          : which == GZB_TILE_SEED_WALKER ? GZB_SEED_WALKER_UNIT
+         : which == GZB_TILE_BAND_WIDTH  ? kLaneW
                                         : 1;
 }
 }  // namespace gzb

@@ -342,6 +342,7 @@ TILE_ORDER = 2
 TILE_SEED_WALKER = 3
 SEED_WALKER_UNIT = 0
 SEED_WALKER_DEALT = 1
+TILE_BAND_WIDTH = 4        # the rows kernel's band columns per lane: 32, 64, 128
 ORDER_HITS = 0
 ORDER_MODEL = 1
 GAPPED_KERNEL_FLAT = 0

@@ -490,6 +490,13 @@ int gzb_engine_get_extension_costs(gzb_engine *e, float *predicted, uint32_t *ce
 #define GZB_TILE_SEED_WALKER 3
 #define GZB_SEED_WALKER_UNIT 0
 #define GZB_SEED_WALKER_DEALT 1
+/* GZB_TILE_BAND_WIDTH: band columns per lane of the _ROWS kernel, 32, 64
+ * (the default) or 128.  The band lives in shared memory (5 bytes per column
+ * and lane), so a narrower band fits more blocks on an SM and hands the
+ * extensions whose band outgrows it to the warp kernel; a wider one keeps
+ * more extensions on one lane with fewer blocks per SM.  Results are the
+ * same. */
+#define GZB_TILE_BAND_WIDTH 4
 #define GZB_GAPPED_KERNEL_FLAT 0
 #define GZB_GAPPED_KERNEL_LANE 1
 #define GZB_GAPPED_KERNEL_ROWS 2

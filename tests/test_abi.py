@@ -92,7 +92,7 @@ def test_tile_parameters_validate_without_device():
     L = N.lib()
     v = ctypes.c_int()
     for which in (N.TILE_BOOK_THRESHOLD, N.TILE_GAPPED_KERNEL, N.TILE_ORDER,
-                  N.TILE_SEED_WALKER):
+                  N.TILE_SEED_WALKER, N.TILE_BAND_WIDTH):
         assert L.gzb_get_tile_parameter(which, ctypes.byref(v)) == 0
         keep = v.value
         assert L.gzb_set_tile_parameter(which, keep) == 0
@@ -102,6 +102,9 @@ def test_tile_parameters_validate_without_device():
     assert b"none of" in L.gzb_last_error()
     assert L.gzb_set_tile_parameter(N.TILE_ORDER, 2) == 1
     assert L.gzb_set_tile_parameter(N.TILE_SEED_WALKER, 2) == 1
+    assert L.gzb_get_tile_parameter(N.TILE_BAND_WIDTH, ctypes.byref(v)) == 0 and v.value == 64
+    for bad in (0, 16, 48, 96, 256):
+        assert L.gzb_set_tile_parameter(N.TILE_BAND_WIDTH, bad) == 1
     assert L.gzb_set_tile_parameter(7, 1) == 1
     assert L.gzb_get_tile_parameter(7, ctypes.byref(v)) == 1
 

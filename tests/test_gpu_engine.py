@@ -126,6 +126,26 @@ def test_presearch_every_gapped_tile(engine, oracle, params, kernel, threshold):
         engine.set_tile(N.SCHEDULE_BATCHED, N.TILE_BOOK_THRESHOLD, -1)
 
 
+@pytest.mark.parametrize("band,graph", [(32, False), (32, True), (128, False), (128, True)])
+def test_presearch_every_band_width(engine, oracle, params, band, graph):
+    """The rows kernel with 32 and 128 band columns per lane (a narrower
+    band hands more extensions to the warp kernel) gives the oracle's
+    results, eager and in graph mode, with the DP's cell count unchanged."""
+    from gzb import native as N
+    engine.set_cost_model(None)
+    engine.set_tile(N.SCHEDULE_BATCHED, N.TILE_GAPPED_KERNEL, N.GAPPED_KERNEL_ROWS)
+    engine.set_tile(N.SCHEDULE_BATCHED, N.TILE_BAND_WIDTH, band)
+    engine.set_graph(graph)
+    try:
+        db, q = _small(1101, 1102, n_db=900, n_q=70, median=400)
+        cnt = _compare(engine, oracle, params, db, q, schedule=N.SCHEDULE_BATCHED)
+        assert cnt["gapped_cells"] > 0
+    finally:
+        engine.set_graph(False)
+        engine.set_tile(N.SCHEDULE_BATCHED, N.TILE_GAPPED_KERNEL, -1)
+        engine.set_tile(N.SCHEDULE_BATCHED, N.TILE_BAND_WIDTH, -1)
+
+
 @pytest.mark.parametrize("graph", [False, True])
 def test_dealt_seed_walker_matches_oracle(engine, oracle, params, graph):
     """The dealt seed walker (GZB_SEED_WALKER_DEALT) gives the oracle's

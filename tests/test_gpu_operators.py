@@ -293,3 +293,41 @@ def test_gapped_group_kernels_match_oracle(torch_cuda, oracle, params, group):
                                                              int(dpos[i]) + ed)
     finally:
         N.set_tile_parameter(N.TILE_GAPPED_KERNEL, keep)
+
+
+@pytest.mark.parametrize("band", [32, 128])
+def test_rows_kernel_band_widths_match_oracle(torch_cuda, oracle, params, band):
+    """GZB_TILE_BAND_WIDTH 32 and 128 on the rows kernel through the operator
+    API: every X-drop in both directions against the oracle, the cell count
+    included (a band outgrowing the lane's columns goes to the warp kernel,
+    or to the serial kernel for X-drops outside the warp DP's range)."""
+    from gzb import native as N
+    keep_k = N.get_tile_parameter(N.TILE_GAPPED_KERNEL)
+    keep_w = N.get_tile_parameter(N.TILE_BAND_WIDTH)
+    N.set_tile_parameter(N.TILE_GAPPED_KERNEL, N.GAPPED_KERNEL_ROWS)
+    N.set_tile_parameter(N.TILE_BAND_WIDTH, band)
+    try:
+        for cutoff in (0, 5, 26, 60, 2000, INT_MAX):
+            for reverse in (False, True):
+                rng = np.random.default_rng(4000 + band + cutoff % 97 + (7 if reverse else 0))
+                n = 200 if cutoff not in (2000, INT_MAX) else 60
+                A, B = _pairs(rng, n, hi=600 if cutoff < 1000 else 250)
+                qc, qs = _concat(A, 25)
+                dc, ds = _concat(B, 25)
+                qpos = [qs[i] + int(rng.integers(0, len(A[i]))) for i in range(n)]
+                dpos = [ds[i] + int(np.clip(qpos[i] - qs[i] + rng.integers(-4, 5), 0,
+                                            len(B[i]) - 1)) for i in range(n)]
+                s, q, d, cells = _gapped_gpu(torch_cuda, params, qc, dc, qpos, dpos, reverse,
+                                             cutoff)
+                total = 0
+                for i in range(n):
+                    es, eq, ed, ec = oracle.gapped_one_side(params, qc, qpos[i], dc, dpos[i],
+                                                            reverse, cutoff)
+                    total += ec
+                    assert (int(s[i]), int(q[i]), int(d[i])) == \
+                        (es, int(qpos[i]) + eq, int(dpos[i]) + ed), (band, cutoff, reverse, i)
+                assert cells == total
+    finally:
+        N.set_tile_parameter(N.TILE_GAPPED_KERNEL, keep_k)
+        N.set_tile_parameter(N.TILE_BAND_WIDTH, keep_w)
+
