@@ -179,14 +179,43 @@ __device__ __forceinline__ void load_walk_words(WalkWords<INC> &ww, const uint8_
   for (int i = 0; i <= kWalkPrefetch; ++i) ww.w[i] = __ldg(ww.p + (INC > 0 ? i : 1 - i));
 }
 
-// walk_side over words already loaded (see walk_side)
+// walk_side over words already loaded (see walk_side).  A chunk's four
+// pairs are scored without an exit test each: the chunk keeps the largest
+// drop below the running best (best_j - score_j) and tests it, and the best
+// against stop_above, once at its end.  A chunk in which the walk ends is
+// then replayed pair by pair from its start (the exact exit pair, its best
+// and the step count); no pair after a delimiter changes a value the walk
+// returns, since the delimiter's -32768 ends the replay first.
 template <int INC>
 __device__ __forceinline__ int walk_side_words(const WalkWords<INC> &A, const WalkWords<INC> &B,
                                                const char *tbl, int cutoff, int stop_above,
                                                int *steps) {
   constexpr int K = kWalkPrefetch;
   const uint32_t sha = A.sh, shb = B.sh;
-  int score = 0, best = 0, n = 0, v = 0;
+  int score = 0, best = 0, n = 0;
+  uint32_t rx4 = 0, rqa = 0;  // the chunk the walk ends in
+#define GZB_WALK_V(J, X4, QA) \
+  (*(const int32_t *)(tbl + walk_offset<(INC > 0 ? (J) : 3 - (J))>(X4, QA)))
+// the four pairs of chunk (X4, QA); leaves the loop for the replay when the
+// walk ends inside the chunk
+#define GZB_WALK_CHUNK(X4, QA)                                                  \
+  {                                                                            \
+    const int v0 = GZB_WALK_V(0, X4, QA), v1 = GZB_WALK_V(1, X4, QA);          \
+    const int v2 = GZB_WALK_V(2, X4, QA), v3 = GZB_WALK_V(3, X4, QA);          \
+    const int s0 = score + v0, b0 = imax(best, s0);                           \
+    const int s1 = s0 + v1, b1 = imax(b0, s1);                                \
+    const int s2 = s1 + v2, b2 = imax(b1, s2);                                \
+    const int s3 = s2 + v3, b3 = imax(b2, s3);                                \
+    const int drop = imax(imax(b0 - s0, b1 - s1), imax(b2 - s2, b3 - s3));    \
+    if (drop >= cutoff || b3 > stop_above) {                                   \
+      rx4 = X4;                                                                \
+      rqa = QA;                                                                \
+      goto replay;                                                             \
+    }                                                                          \
+    score = s3;                                                                \
+    best = b3;                                                                 \
+    n += 4;                                                                    \
+  }
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const uint32_t qa = INC > 0 ? __funnelshift_r(A.w[k], A.w[k + 1], sha)
@@ -194,22 +223,7 @@ __device__ __forceinline__ int walk_side_words(const WalkWords<INC> &A, const Wa
     const uint32_t qb = INC > 0 ? __funnelshift_r(B.w[k], B.w[k + 1], shb)
                                 : __funnelshift_r(B.w[k + 1], B.w[k], shb);
     const uint32_t x4p = (qa ^ qb) << 2;
-#define GZB_WALK_PRE(J)                                                    \
-  {                                                                        \
-    v = *(const int32_t *)(tbl + walk_offset<(INC > 0 ? (J) : 3 - (J))>(x4p, qa)); \
-    score += v;                                                            \
-    best = imax(best, score);                                              \
-    if (best - score >= cutoff || best > stop_above) {                     \
-      n += (J) + 1;                                                        \
-      goto done;                                                           \
-    }                                                                      \
-  }
-    GZB_WALK_PRE(0)
-    GZB_WALK_PRE(1)
-    GZB_WALK_PRE(2)
-    GZB_WALK_PRE(3)
-#undef GZB_WALK_PRE
-    n += 4;
+    GZB_WALK_CHUNK(x4p, qa)
   }
   {
     // past the prefetched chunks: one new word per chunk
@@ -233,22 +247,7 @@ __device__ __forceinline__ int walk_side_words(const WalkWords<INC> &A, const Wa
     for (;;) {
       const uint32_t qa = __funnelshift_r(a_lo, a_hi, sha);
       const uint32_t x4 = (qa ^ __funnelshift_r(b_lo, b_hi, shb)) << 2;
-#define GZB_WALK_STEP(J)                                                   \
-  {                                                                        \
-    v = *(const int32_t *)(tbl + walk_offset<(INC > 0 ? (J) : 3 - (J))>(x4, qa)); \
-    score += v;                                                            \
-    best = imax(best, score);                                              \
-    if (best - score >= cutoff || best > stop_above) {                     \
-      n += (J) + 1;                                                        \
-      goto done;                                                           \
-    }                                                                      \
-  }
-      GZB_WALK_STEP(0)
-      GZB_WALK_STEP(1)
-      GZB_WALK_STEP(2)
-      GZB_WALK_STEP(3)
-#undef GZB_WALK_STEP
-      n += 4;
+      GZB_WALK_CHUNK(x4, qa)
       if (INC > 0) {
         a_lo = a_hi;
         b_lo = b_hi;
@@ -266,9 +265,28 @@ __device__ __forceinline__ int walk_side_words(const WalkWords<INC> &A, const Wa
       }
     }
   }
+#undef GZB_WALK_CHUNK
+replay : {
+  // the chunk the walk ends in, pair by pair (it ends at one of them)
+  int v = 0;
+#define GZB_WALK_PAIR(J)                                                       \
+  v = GZB_WALK_V(J, rx4, rqa);                                                 \
+  score += v;                                                                  \
+  best = imax(best, score);                                                    \
+  if (best - score >= cutoff || best > stop_above) {                           \
+    n += (J) + 1;                                                              \
+    goto done;                                                                 \
+  }
+  GZB_WALK_PAIR(0)
+  GZB_WALK_PAIR(1)
+  GZB_WALK_PAIR(2)
+  GZB_WALK_PAIR(3)
+#undef GZB_WALK_PAIR
+#undef GZB_WALK_V
 done:
   *steps += n - (v == kWalkDelim ? 1 : 0);
   return best;
+}
 }
 
 // One side of SeedSearcher::UngappedExtend (src/seed_searcher.h:133-158 with
