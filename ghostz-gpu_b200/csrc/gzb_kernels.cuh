@@ -919,7 +919,8 @@ namespace gzb {
 // the band in shared memory: W columns per thread (a power of two; kLaneW
 // unless the rows kernel's band-width tile says otherwise), each a packed
 // int16 pair (best, best_gap), plus the query residue of each band column
-// (one byte), laid out [column][thread] so that a warp touching one column
+// (one byte: the residue's byte offset in a score-matrix row), laid out
+// [column][thread] so that a warp touching one column
 // per thread is bank-conflict free.  A band wider than W, or a value
 // outside int16, makes the extension overflow; the caller reruns it on the
 // warp kernel.
@@ -944,8 +945,10 @@ struct LaneBand {
   __device__ __forceinline__ int base(int c) const { return (c & (W - 1)) * stride; }
   __device__ __forceinline__ int slot(int c) const { return base(c) + t; }
   __device__ __forceinline__ uint32_t &at(int c) { return cell[slot(c)]; }
-  __device__ __forceinline__ int residue(int c) const { return res[base(c) + tr]; }
-  __device__ __forceinline__ void set_residue(int c, int r) { res[base(c) + tr] = (uint8_t)r; }
+  // a column's query residue r is kept as its byte offset in a matrix row (4r)
+  __device__ __forceinline__ void set_residue(int c, int r) {
+    res[base(c) + tr] = (uint8_t)(r << 2);
+  }
 };
 
 __device__ __forceinline__ bool fits16(int v) { return v >= -32768 && v <= 32767; }
@@ -1072,18 +1075,20 @@ __device__ __forceinline__ int lane_row(const GappedJob &job, const int *sm, Lan
   const int bs_row = bs;
   const int maxs_in = maxs;
   int maxc = bs_row;
+  bool lead = true;  // every cell of the row so far pruned
   for (int c = bs_row + 1; c < be; ++c) {
     const int b = band.base(c);
     const int k = b + band.t;
     const uint32_t w = band.cell[k];
     const int old_best = lo16(w), vgap = hi16(w);
-    int s = diag + mrow[band.res[b + band.tr]];
+    int s = diag + *(const int *)((const char *)mrow + band.res[b + band.tr]);
     diag = old_best;
     s = imax(s, imax(vgap, row_gap));
     // branch-free: a pruned cell (X-drop) stores the initial score and resets
     // the row gap; the left edge moves past a leading run of pruned cells
     const bool drop = maxs - s > cutoff;
-    bs += (drop && bs + 1 == c) ? 1 : 0;
+    lead = lead && drop;
+    bs = lead ? c : bs;
     last = drop ? last : c;
     maxc = s > maxs ? c : maxc;  // a pruned cell is below maxs
     maxs = imax(maxs, s);
