@@ -732,22 +732,32 @@ __global__ void hit_segments_kernel(const uint64_t *hits, uint64_t n, uint32_t n
 
 // Chain filter (ChainFilter::Filter, src/chain_filter.cpp), one warp per
 // query, over its hits in (database, query) position order; survivors are
-// compacted to the front of the query's segment.  Hit i is handled by the
-// lane that owns its diagonal slot (slot % 32), so each slot sees its hits
-// in order; the warp steps through the hits together and the owner's
-// decision is shared by ballot.  slots: per-query scratch of query_length
-// (diagonal, end) pairs.
-__global__ void chain_kernel(DevParams p, const uint8_t *__restrict__ q,
-                             const uint8_t *__restrict__ db, const uint32_t *q_offsets,
-                             const uint32_t *q_lengths, const int32_t *cutoffs,
-                             const int32_t *matrix32, uint32_t nq, uint64_t *hits,
-                             const uint64_t *begin, int qbits, int dbits, uint2 *slots,
-                             uint32_t *kept_count) {
+// compacted to the front of the query's segment.  A hit only reads and
+// writes its diagonal slot (diagonal % query length), so hits of different
+// slots are independent and only a slot's own hits must be taken in order.
+// The warp takes 32 hits at a time, one per lane, groups the lanes by slot
+// (match.any) and runs rounds: in round r every lane whose hit is the r-th
+// of its slot group applies it, so a round never touches a slot twice and
+// a slot sees its hits in order.  The lanes' keep flags, in hit order, then
+// place the survivors.  A query's (diagonal, end) slots live in the block's
+// shared memory when its length fits `smem_slots` (one warp per block),
+// else in `slots` (per-query scratch of query_length pairs).
+constexpr int kChainSmemSlots = 4096;
+
+__global__ void __launch_bounds__(32)
+chain_kernel(DevParams p, const uint8_t *__restrict__ q, const uint8_t *__restrict__ db,
+             const uint32_t *q_offsets, const uint32_t *q_lengths, const int32_t *cutoffs,
+             const int32_t *matrix32, uint32_t nq, uint64_t *hits, const uint64_t *begin,
+             int qbits, int dbits, uint2 *slots, uint32_t *kept_count, uint32_t smem_slots) {
+  __shared__ __align__(16) int32_t tbl32[kWalkTableBytes / 4];
+  extern __shared__ uint2 chain_slots[];
+  load_walk_table(tbl32, matrix32, p.delimiter);
+  __syncthreads();
+  const char *tbl = reinterpret_cast<const char *>(tbl32);
   const uint64_t qmask = (1ull << qbits) - 1, dmask = (1ull << dbits) - 1;
-  const int n = kMatrixStride;
   const int lane = threadIdx.x & 31;
-  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t qi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; qi < nq; qi += warps) {
+  const unsigned below = (1u << lane) - 1;
+  for (uint32_t qi = blockIdx.x; qi < nq; qi += gridDim.x) {
     const uint64_t b = begin[qi], e = begin[qi + 1];
     if (b == e) {
       if (lane == 0) kept_count[qi] = 0;
@@ -755,50 +765,49 @@ __global__ void chain_kernel(DevParams p, const uint8_t *__restrict__ q,
     }
     const uint8_t *qs = q + q_offsets[qi];
     const uint32_t qlen = q_lengths[qi];
-    uint2 *slot = slots + q_offsets[qi] + qi;  // qlen entries of this query
+    uint2 *slot = qlen <= smem_slots ? chain_slots : slots + q_offsets[qi] + qi;
     for (uint32_t i = lane; i < qlen; i += 32) slot[i] = make_uint2(0, 0);
     __syncwarp();
     const int cutoff = cutoffs[qi];
     uint64_t w = b;
-    for (uint64_t i = b; i < e; ++i) {
-      const uint64_t key = hits[i];
+    for (uint64_t i0 = b; i0 < e; i0 += 32) {
+      // this round's hits, one per lane (the compaction below only writes
+      // positions before i0 + 32)
+      const bool valid = i0 + lane < e;
+      const uint64_t key = valid ? hits[i0 + lane] : 0;
       const uint32_t hq = (uint32_t)(key & qmask);
       const uint32_t hd = (uint32_t)((key >> qbits) & dmask);
       const uint32_t diagonal = qlen - 1 + hd - hq;
-      const uint32_t si = diagonal % qlen;
+      const uint32_t si = valid ? diagonal % qlen : 0;
+      // slot groups (an idle lane is a group of its own)
+      const unsigned grp = __match_any_sync(0xffffffffu, valid ? si : (0x80000000u | lane));
+      const int rank = __popc(grp & below);
+      const int rounds = (int)__reduce_max_sync(0xffffffffu, (unsigned)__popc(grp));
       bool keep = false;
-      if ((si & 31) == (uint32_t)lane) {
-        uint2 sl = slot[si];  // x = diagonal, y = query end
-        bool connected = false;
-        if (sl.x == diagonal) {
-          if (hq <= sl.y + 1) {
-            connected = true;
-          } else {
-            // back-extension toward the chain end (ChainFilter::Connected)
-            uint32_t qo = hq, dof = hd;
-            int score = 0, best = 0, c = -cutoff;
-            do {
-              --dof;
-              --qo;
-              if (db[dof] == p.delimiter || qs[qo] == p.delimiter || qo <= sl.y) break;
-              score += matrix32[db[dof] * n + qs[qo]];
-              if (best < score) {
-                best = score;
-                c = best - cutoff;
-              }
-            } while (score > c);
-            connected = qo <= sl.y;
+      for (int r = 0; r < rounds; ++r) {
+        if (valid && rank == r) {
+          uint2 sl = slot[si];  // x = diagonal, y = query end
+          bool connected = false;
+          if (sl.x == diagonal) {
+            if (hq <= sl.y + 1) {
+              connected = true;
+            } else {
+              // back-extension toward the chain end (ChainFilter::Connected):
+              // the hq - 1 - end pairs before the hit
+              connected = walk_reaches<-1>(qs + hq - 1, db + hd - 1, tbl, cutoff,
+                                           hq - 1 - sl.y);
+            }
           }
+          sl.y = hq;
+          if (!connected) sl.x = diagonal;
+          slot[si] = sl;
+          keep = !connected;
         }
-        sl.y = hq;
-        if (!connected) sl.x = diagonal;
-        slot[si] = sl;
-        keep = !connected;
+        __syncwarp();  // the round's slot writes before the next round reads
       }
-      if (__ballot_sync(0xffffffffu, keep)) {
-        if (keep) hits[w] = key;
-        ++w;
-      }
+      const unsigned kept = __ballot_sync(0xffffffffu, keep);
+      if (keep) hits[w + __popc(kept & below)] = key;
+      w += __popc(kept);
     }
     if (lane == 0) kept_count[qi] = (uint32_t)(w - b);
     __syncwarp();
@@ -2152,6 +2161,21 @@ extern "C" int gzb_engine_reset_results(gzb_engine *e, void *stream) {
 
 namespace {
 
+// chain_kernel over the queries, one warp per block, the diagonal slots in
+// shared memory for queries up to kChainSmemSlots long
+int launch_chain(gzb_engine *e, uint32_t nq, uint64_t *hits, const uint64_t *begin, int qbits,
+                 int dbits, uint32_t *kept, cudaStream_t s) {
+  const uint32_t smem_slots = std::min<uint32_t>(e->max_qlen, kChainSmemSlots);
+  const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>(nq, 148u * 64u));
+  chain_kernel<<<blocks, 32, sizeof(uint2) * smem_slots, s>>>(
+      e->dp, e->q_buf.as<uint8_t>() + kPad, e->db_buf.as<uint8_t>() + kPad,
+      e->q_offsets.as<uint32_t>(), e->q_lengths.as<uint32_t>(), e->q_cut.as<int32_t>(),
+      e->matrix32.as<int32_t>(), nq, hits, begin, qbits, dbits, e->slots.as<uint2>(), kept,
+      smem_slots);
+  GZB_CUDA(cudaGetLastError());
+  return GZB_OK;
+}
+
 int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
   uint64_t launches = 0;
   GappedTile stile = g_tile;
@@ -2286,10 +2310,7 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
                                                           nullptr);
   GZB_CUDA(cudaGetLastError());
     ++launches;
-  chain_kernel<<<grid1((uint64_t)nq * 32, 128), 128, 0, s>>>(
-      e->dp, e->q_buf.as<uint8_t>() + kPad, e->db_buf.as<uint8_t>() + kPad,
-      e->q_offsets.as<uint32_t>(), e->q_lengths.as<uint32_t>(), e->q_cut.as<int32_t>(),
-      e->matrix32.as<int32_t>(), nq, hits, begin, qbits, dbits, e->slots.as<uint2>(), kept);
+  GZB_TRY(launch_chain(e, nq, hits, begin, qbits, dbits, kept, s));
   GZB_CUDA(cudaGetLastError());
     ++launches;
   GZB_CUDA(cudaMemsetAsync(kept + nq, 0, 4, s));
@@ -2668,10 +2689,7 @@ int graph_body(gzb_engine *e, int schedule, const GappedTile &tile, bool learned
                                                           plan + 1);
   GZB_CUDA(cudaGetLastError());
   ++launches;
-  chain_kernel<<<grid1((uint64_t)nq * 32, 128), 128, 0, s>>>(
-      e->dp, e->q_buf.as<uint8_t>() + kPad, e->db_buf.as<uint8_t>() + kPad,
-      e->q_offsets.as<uint32_t>(), e->q_lengths.as<uint32_t>(), e->q_cut.as<int32_t>(),
-      e->matrix32.as<int32_t>(), nq, hits, begin, qbits, dbits, e->slots.as<uint2>(), kept);
+  GZB_TRY(launch_chain(e, nq, hits, begin, qbits, dbits, kept, s));
   GZB_CUDA(cudaGetLastError());
   ++launches;
   GZB_CUDA(cudaMemsetAsync(kept + nq, 0, 4, s));

@@ -310,6 +310,70 @@ __device__ __forceinline__ int walk_side(const uint8_t *s0, const uint8_t *s1,
   return walk_side_words(A, B, tbl, cutoff, stop_above, steps);
 }
 
+// Whether the X-drop walk from s0[0]/s1[0] stepping by INC survives its
+// first `length` residue pairs: no pair among them is a delimiter, and the
+// score never falls `cutoff` (>= 1) below its running best (from 0) after
+// one of them.  This is ChainFilter::Connected's back-extension
+// (src/chain_filter.cpp:60-99) toward a chain end `length` pairs away,
+// four pairs per chunk on the walk table (a chunk in which the walk ends
+// ends it before `length`, so its exact pair does not matter).
+template <int INC>
+__device__ __forceinline__ bool walk_reaches(const uint8_t *s0, const uint8_t *s1,
+                                             const char *tbl, int cutoff, uint32_t length) {
+  const uintptr_t a0 = (uintptr_t)s0 - (INC > 0 ? 0 : 3);
+  const uintptr_t a1 = (uintptr_t)s1 - (INC > 0 ? 0 : 3);
+  const uint32_t *pa = (const uint32_t *)(a0 & ~(uintptr_t)3);
+  const uint32_t *pb = (const uint32_t *)(a1 & ~(uintptr_t)3);
+  const uint32_t sha = 8u * (uint32_t)(a0 & 3), shb = 8u * (uint32_t)(a1 & 3);
+  uint32_t a_lo = __ldg(pa), a_hi = __ldg(pa + 1), b_lo = __ldg(pb), b_hi = __ldg(pb + 1);
+  int score = 0, best = 0;
+  uint32_t done = 0;
+#define GZB_REACH_V(J, X4, QA) \
+  (*(const int32_t *)(tbl + walk_offset<(INC > 0 ? (J) : 3 - (J))>(X4, QA)))
+  for (;;) {
+    const uint32_t qa = __funnelshift_r(a_lo, a_hi, sha);
+    const uint32_t x4 = (qa ^ __funnelshift_r(b_lo, b_hi, shb)) << 2;
+    if (done + 4 > length) {
+      // the last pairs before the chain end, one at a time
+      const uint32_t left = length - done;
+#pragma unroll
+      for (uint32_t j = 0; j < 3; ++j) {
+        if (j >= left) break;
+        const int v = j == 0 ? GZB_REACH_V(0, x4, qa)
+                             : (j == 1 ? GZB_REACH_V(1, x4, qa) : GZB_REACH_V(2, x4, qa));
+        score += v;
+        best = imax(best, score);
+        if (best - score >= cutoff) return false;
+      }
+      return true;
+    }
+    const int s0v = score + GZB_REACH_V(0, x4, qa), b0 = imax(best, s0v);
+    const int s1v = s0v + GZB_REACH_V(1, x4, qa), b1 = imax(b0, s1v);
+    const int s2v = s1v + GZB_REACH_V(2, x4, qa), b2 = imax(b1, s2v);
+    const int s3v = s2v + GZB_REACH_V(3, x4, qa), b3 = imax(b2, s3v);
+    if (imax(imax(b0 - s0v, b1 - s1v), imax(b2 - s2v, b3 - s3v)) >= cutoff) return false;
+    score = s3v;
+    best = b3;
+    done += 4;
+    if (INC > 0) {
+      a_lo = a_hi;
+      b_lo = b_hi;
+      pa += 1;
+      pb += 1;
+      a_hi = __ldg(pa + 1);
+      b_hi = __ldg(pb + 1);
+    } else {
+      a_hi = a_lo;
+      b_hi = b_lo;
+      pa -= 1;
+      pb -= 1;
+      a_lo = __ldg(pa);
+      b_lo = __ldg(pb);
+    }
+  }
+#undef GZB_REACH_V
+}
+
 // SeedSearcher::UngappedExtend on the walk table: reverse from (q-1, d-1),
 // forward from (q, d) unless the reverse best already exceeds trigger; true
 // when the sum exceeds trigger.

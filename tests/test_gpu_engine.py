@@ -72,6 +72,17 @@ def test_presearch_matches_oracle_small(engine, oracle, params):
     assert cnt["chained_hits"] > 0 and cnt["gapped_cells"] > 0
 
 
+def test_presearch_long_queries(engine, oracle, params):
+    """Queries longer than the chain filter's shared-memory slots (4,096
+    diagonals) keep their slots in global memory; results equal the
+    oracle's."""
+    db = W.make_database(300, 1201, median=5000, lo=4200, hi=7000)
+    q = W.make_queries(db, 24, 1202, median=5000, lo=4200, hi=7000)
+    assert int(q.lengths.max()) > 4096
+    cnt = _compare(engine, oracle, params, db, q)
+    assert cnt["chained_hits"] > 0
+
+
 def test_presearch_without_clustering(engine, oracle):
     p = P.make_params(clustering=False)
     db, q = _small(601, 602, n_db=800, n_q=60)
