@@ -1028,15 +1028,6 @@ __device__ __forceinline__ int alignment_comp(const gzb_result &a, const gzb_res
   return (a.start_d < b.start_d) ? 1 : -1;
 }
 
-// strict order used for the stable sort: AlignmentComp, then input order
-// (AlignmentComp is antisymmetric except on full ties, where it returns -1
-// both ways; the reference's stable_sort keeps such ties in input order.)
-__device__ __forceinline__ bool before(const gzb_result *r, uint32_t i, uint32_t j) {
-  if (alignment_comp(r[i], r[j]) > 0) return true;
-  if (alignment_comp(r[j], r[i]) > 0) return false;
-  return i < j;
-}
-
 __device__ __forceinline__ bool is_contained(const gzb_result &a, const gzb_result &b) {
   return (a.start_q == b.start_q && a.start_d == b.start_d) ||
          (a.end_q == b.end_q && a.end_d == b.end_d) ||
@@ -1059,27 +1050,68 @@ __device__ __forceinline__ uint32_t subject_of(const uint32_t *off, uint32_t nse
 }
 
 
-// index of the first (in `before` order) untaken candidate among
-// i = lane, lane + 32, ... (< k), or UINT32_MAX
-__device__ __forceinline__ uint32_t lane_first(const gzb_result *added, const uint8_t *taken,
-                                               uint32_t k, int lane) {
-  uint32_t best = 0xFFFFFFFFu;
-  for (uint32_t i = lane; i < k; i += 32)
-    if (!taken[i] && (best == 0xFFFFFFFFu || before(added, i, best))) best = i;
-  return best;
+// Sort key of a candidate in AlignerCommon::AddResults' order (its stable
+// sort by AlignmentComp): score, then query extent, then database extent
+// descending, then database start ascending (k1 = score | query extent,
+// k2 = database extent | ~database start, compared as unsigned).
+// AlignmentComp is antisymmetric except on full ties, where it returns -1
+// both ways and the reference's stable_sort keeps input order; equal keys
+// are ordered by index here.
+__device__ __forceinline__ ulonglong2 merge_key(const gzb_result &r) {
+  return make_ulonglong2(
+      ((unsigned long long)((uint32_t)r.score ^ 0x80000000u) << 32) |
+          (uint32_t)(r.end_q - r.start_q),
+      ((unsigned long long)(uint32_t)(r.end_d - r.start_d) << 32) | (uint32_t)~r.start_d);
+}
+
+__device__ __forceinline__ bool key_before(unsigned long long a1, unsigned long long a2,
+                                           uint32_t ai, unsigned long long b1,
+                                           unsigned long long b2, uint32_t bi) {
+  return a1 > b1 || (a1 == b1 && (a2 > b2 || (a2 == b2 && ai < bi)));
+}
+
+// A lane's candidates as a binary heap of indices, first in `key_before`
+// order at the root; element t at heap[32 t] (heap is offset by the lane).
+// Sifts element t down through the m elements.
+__device__ __forceinline__ void heap_sift(uint32_t *heap, const ulonglong2 *keys, uint32_t m,
+                                          uint32_t t) {
+  const uint32_t x = heap[32 * t];
+  const ulonglong2 kx = keys[x];
+  for (;;) {
+    uint32_t c = 2 * t + 1;
+    if (c >= m) break;
+    uint32_t y = heap[32 * c];
+    ulonglong2 ky = keys[y];
+    if (c + 1 < m) {
+      const uint32_t z = heap[32 * (c + 1)];
+      const ulonglong2 kz = keys[z];
+      if (key_before(kz.x, kz.y, z, ky.x, ky.y, y)) {
+        c = c + 1;
+        y = z;
+        ky = kz;
+      }
+    }
+    if (!key_before(ky.x, ky.y, y, kx.x, kx.y, x)) break;
+    heap[32 * t] = y;
+    t = c;
+  }
+  heap[32 * t] = x;
 }
 
 // One warp per query: the lanes build the candidates of the query's
-// survivors and find, 32-wide, the next one in AlignerCommon::AddResults
-// order; lane 0 merges it with the query's running top-b list, exactly as
-// AddResults orders and prunes (src/aligner_common.cpp).
+// survivors, each lane keeps its own (i = lane, lane + 32, ...) as a heap in
+// AlignerCommon::AddResults order, and the warp finds the next candidate as
+// the best of the 32 heap roots; lane 0 merges it with the query's running
+// top-b list, exactly as AddResults orders and prunes
+// (src/aligner_common.h:147-274).
 __global__ void merge_kernel(uint32_t nq, const uint64_t *hits, const uint64_t *begin,
                              const uint32_t *kept, const uint64_t *surv_off,
                              uint64_t n_surv, const uint32_t *eq, const uint32_t *ed,
                              const int32_t *escore, const uint32_t *q_offsets, int qbits,
                              int dbits, const uint32_t *db_offsets, uint32_t nseq,
                              uint32_t db_len, int32_t chunk_id, int max_results,
-                             int max_one_subject, gzb_result *scratch, uint8_t *taken_all,
+                             int max_one_subject, gzb_result *scratch, ulonglong2 *keys_all,
+                             uint32_t *heap_all,
                              gzb_result *results, uint32_t *counts, const uint64_t *n_dev,
                              const uint32_t *skip) {
   // a run whose buffers overflowed merges nothing (it is redone)
@@ -1088,13 +1120,16 @@ __global__ void merge_kernel(uint32_t nq, const uint64_t *hits, const uint64_t *
   const uint64_t qmask = (1ull << qbits) - 1, dmask = (1ull << dbits) - 1;
   const int lane = threadIdx.x & 31;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  constexpr uint32_t kNone = 0xFFFFFFFFu;
   for (uint32_t qi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; qi < nq; qi += warps) {
     const uint32_t k = kept[qi];
     if (k == 0) continue;
     const uint64_t b = begin[qi], o = surv_off[qi];
     const uint32_t qoff = q_offsets[qi];
     gzb_result *added = scratch + o;
-    uint8_t *taken = taken_all + o;
+    ulonglong2 *keys = keys_all + o;
+    uint32_t *heap = heap_all + o + lane;
+    uint32_t m = 0;
     for (uint32_t i = lane; i < k; i += 32) {
       const uint64_t key = hits[b + i];
       gzb_result r;
@@ -1108,10 +1143,14 @@ __global__ void merge_kernel(uint32_t nq, const uint64_t *hits, const uint64_t *
       r.end_q = eq[n_surv + o + i] - qoff;
       r.end_d = ed[n_surv + o + i];
       added[i] = r;
-      taken[i] = 0;
+      keys[i] = merge_key(r);
+      heap[32 * m] = i;
+      ++m;
     }
+    for (uint32_t t = m / 2; t-- > 0;) heap_sift(heap, keys, m, t);
     __syncwarp();
-    uint32_t mine = lane_first(added, taken, k, lane);
+    uint32_t mine = m ? heap[0] : kNone;
+    ulonglong2 mk = m ? keys[mine] : make_ulonglong2(0, 0);
     // lane 0's merge state: previous list of this query (earlier chunks)
     gzb_result *prev = results + (uint64_t)qi * max_results;
     const uint32_t n_prev = counts[qi];
@@ -1127,11 +1166,18 @@ __global__ void merge_kernel(uint32_t nq, const uint64_t *hits, const uint64_t *
     uint32_t sp_id[32][4];
     uint32_t n_subj = 0;
     for (;;) {
-      // first untaken candidate of the warp
+      // first untaken candidate of the warp: the best of the lanes' roots
       uint32_t g = mine;
+      unsigned long long g1 = mk.x, g2 = mk.y;
       for (int d = 16; d >= 1; d >>= 1) {
-        const uint32_t other = __shfl_xor_sync(0xffffffffu, g, d);
-        if (other != 0xFFFFFFFFu && (g == 0xFFFFFFFFu || before(added, other, g))) g = other;
+        const uint32_t og = __shfl_xor_sync(0xffffffffu, g, d);
+        const unsigned long long o1 = __shfl_xor_sync(0xffffffffu, g1, d);
+        const unsigned long long o2 = __shfl_xor_sync(0xffffffffu, g2, d);
+        if (og != kNone && (g == kNone || key_before(o1, o2, og, g1, g2, g))) {
+          g = og;
+          g1 = o1;
+          g2 = o2;
+        }
       }
       int popped = -1, cont = 0;
       if (lane == 0) {
@@ -1220,8 +1266,16 @@ __global__ void merge_kernel(uint32_t nq, const uint64_t *hits, const uint64_t *
       if (!cont) break;
       popped = __shfl_sync(0xffffffffu, popped, 0);
       if (popped >= 0 && (uint32_t)popped % 32 == (uint32_t)lane) {
-        taken[popped] = 1;
-        mine = lane_first(added, taken, k, lane);
+        // the candidate taken is this lane's root
+        --m;
+        if (m) {
+          heap[0] = heap[32 * m];
+          heap_sift(heap, keys, m, 0);
+          mine = heap[0];
+          mk = keys[mine];
+        } else {
+          mine = kNone;
+        }
       }
       __syncwarp();
     }
@@ -2445,14 +2499,16 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
   // ---- top-b merge
   if (n_surv) {
     GZB_TRY(e->merge_scratch.ensure(sizeof(gzb_result) * (n_surv + 1)));
-    GZB_TRY(e->heap.ensure(n_surv + 1));
+    // per candidate: its sort key (16 B), then its heap slot (4 B)
+    GZB_TRY(e->heap.ensure(20 * (n_surv + 1)));
     merge_kernel<<<grid1((uint64_t)nq * 32, 128), 128, 0, s>>>(
         nq, hits, begin, kept, surv_off, n_surv, e->eq.as<uint32_t>(), e->ed.as<uint32_t>(),
         e->escore.as<int32_t>(), e->q_offsets.as<uint32_t>(), qbits, dbits,
         e->db_offsets.as<uint32_t>(), e->nseq, (uint32_t)e->db_len, e->chunk_id,
         e->params.max_number_results, e->params.max_number_one_subject_results,
-        e->merge_scratch.as<gzb_result>(), e->heap.as<uint8_t>(), e->results.as<gzb_result>(),
-        e->counts.as<uint32_t>(), nullptr, nullptr);
+        e->merge_scratch.as<gzb_result>(), e->heap.as<ulonglong2>(),
+        reinterpret_cast<uint32_t *>(e->heap.as<ulonglong2>() + n_surv + 1),
+        e->results.as<gzb_result>(), e->counts.as<uint32_t>(), nullptr, nullptr);
     GZB_CUDA(cudaGetLastError());
     ++launches;
   }
@@ -2575,7 +2631,7 @@ int graph_prepare(gzb_engine *e, const GraphCaps &c, int hit_bits, int mw_bits, 
   GZB_TRY(e->edir.ensure(c.ext + 1));
   GZB_TRY(e->enb.ensure(4 * (c.hits + 1)));
   GZB_TRY(e->merge_scratch.ensure(sizeof(gzb_result) * (c.hits + 1)));
-  GZB_TRY(e->heap.ensure(c.hits + 1));
+  GZB_TRY(e->heap.ensure(20 * (c.hits + 1)));  // merge keys and heap slots
   if (learned) {  // the cost-model order
     GZB_TRY(e->efeat.ensure(4 * kFeat * (c.ext + 1)));
     for (DBuf *b : {&e->epred, &e->okeys, &e->okeys2, &e->oidx, &e->oidx2})
@@ -2751,8 +2807,9 @@ int graph_body(gzb_engine *e, int schedule, const GappedTile &tile, bool learned
       e->escore.as<int32_t>(), e->q_offsets.as<uint32_t>(), qbits, dbits,
       e->db_offsets.as<uint32_t>(), e->nseq, (uint32_t)e->db_len, e->chunk_id,
       e->params.max_number_results, e->params.max_number_one_subject_results,
-      e->merge_scratch.as<gzb_result>(), e->heap.as<uint8_t>(), e->results.as<gzb_result>(),
-      e->counts.as<uint32_t>(), plan + 2, overflow);
+      e->merge_scratch.as<gzb_result>(), e->heap.as<ulonglong2>(),
+      reinterpret_cast<uint32_t *>(e->heap.as<ulonglong2>() + c.hits + 1),
+      e->results.as<gzb_result>(), e->counts.as<uint32_t>(), plan + 2, overflow);
   GZB_CUDA(cudaGetLastError());
   ++launches;
   stamp_kernel<<<1, 1, 0, s>>>(plan + 24 + 5);
