@@ -13,7 +13,8 @@ sides, top-b merge.
   value : queries/s with the prepared queries already resident in HBM
   e2e   : queries/s of the search through the C ABI from host buffers: every
           step copies the raw query residues in, prepares them (SEG,
-          cutoffs), uploads them and builds their hash lists, runs the
+          cutoffs) and builds their hash lists on the device (protein
+          queries: one gzb_engine_set_protein_queries call), runs the
           presearch and the build results step, and reads every query's
           alignment records back (the work of `aln` after its database is
           loaded, except formatting the text lines).
@@ -1142,15 +1143,12 @@ def main():
                                                      pinned_copy(rq.lengths))
         keep += [t1, t2, t3]
         raw_bytes = rq.codes.nbytes + rq.offsets.nbytes * 2 + rq.lengths.nbytes
-
-        def prepare():
-            codes, cut, trig = N.prepare_protein_queries(p_codes, p_offs, p_lens)
-            return W.Queries(codes=codes, offsets=p_offs, lengths=p_lens, cutoffs=cut,
-                             triggers=trig)
+        protein_on_device = True
     else:
         (p_dna, t1), (p_roffs, t2) = pinned_copy(raw.dna), pinned_copy(raw.offsets)
         keep += [t1, t2]
         raw_bytes = raw.dna.nbytes + raw.offsets.nbytes * 2
+        protein_on_device = False
 
         def prepare():
             codes, offs, lens, cut, trig = N.prepare_translated_queries(p_dna, p_roffs)
@@ -1160,8 +1158,13 @@ def main():
                          dtype=torch.uint8).pin_memory()
 
     def e2e_step():
-        qq = prepare()
-        eng.set_queries(qq, stream)
+        if protein_on_device:
+            # SEG, cutoffs and lists on the device (gzb_engine_set_protein_queries)
+            eng.set_protein_queries(p_codes, p_offs, p_lens, stream=stream)
+            qq = None
+        else:
+            qq = prepare()
+            eng.set_queries(qq, stream)
         eng.presearch(schedule, stream)
         N.check(L.gzb_engine_build_alignments(eng.h, ctypes.c_void_p(counts_pin.data_ptr()),
                                               ctypes.c_void_p(al_pin.data_ptr()),
@@ -1178,11 +1181,16 @@ def main():
     e1.record(stream)
     barrier()
     e2e_ms = e0.elapsed_time(e1)
-    prepared_bytes = sum(getattr(qq, n).nbytes
-                         for n in ("codes", "offsets", "lengths", "cutoffs", "triggers"))
-    h2d = raw_bytes + prepared_bytes
-    d2h = (qq.codes.nbytes + qq.cutoffs.nbytes + qq.triggers.nbytes + counts_pin.numel()
-           + al_pin.numel())
+    if protein_on_device:
+        # raw queries in; cutoffs and triggers, counts and records back
+        h2d = raw_bytes
+        d2h = 8 * q.number + counts_pin.numel() + al_pin.numel()
+    else:
+        prepared_bytes = sum(getattr(qq, n).nbytes
+                             for n in ("codes", "offsets", "lengths", "cutoffs", "triggers"))
+        h2d = raw_bytes + prepared_bytes
+        d2h = (qq.codes.nbytes + qq.cutoffs.nbytes + qq.triggers.nbytes + counts_pin.numel()
+               + al_pin.numel())
     # the e2e alignment records must equal the device loop's
     got = np.frombuffer(al_pin.numpy().tobytes(), dtype=N.ALIGNMENT_DTYPE).reshape(q.number, b)
     cnt = np.frombuffer(counts_pin.numpy().tobytes(), dtype=np.uint32)
@@ -1290,9 +1298,13 @@ def main():
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": t_e2e / steps,
                 "results_equal_device_loop": bool(e2e_same),
-                "step": "raw queries from pinned host memory -> SEG + cutoffs -> upload + "
-                        "hash lists -> presearch -> build results -> alignment records "
-                        "(no text formatting)"},
+                "step": ("raw protein queries from pinned host memory -> "
+                         "gzb_engine_set_protein_queries (SEG, cutoffs and hash lists on the "
+                         "device) -> presearch -> build results -> alignment records "
+                         "(no text formatting)" if protein_on_device else
+                         "raw reads from pinned host memory -> translation + SEG + cutoffs "
+                         "-> upload + hash lists -> presearch -> build results -> "
+                         "alignment records (no text formatting)")},
         "dp_gcups": {"gapped_stage": gcups_stage, "whole_step": gcups_step},
         "dp_int_pipe": dp_int_pipe(gcups_stage, clocks),
         "stage_ms": st, "counters": counters, "schedules": sched_report,

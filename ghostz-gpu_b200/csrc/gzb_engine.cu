@@ -285,37 +285,39 @@ __global__ void low32(const uint64_t *in, uint64_t n, uint32_t *out) {
 // ---------------------------------------------------------------------------
 // query lists
 
-// One thread per query: every position of a delimiter-free stretch of at
-// least L residues is hashed; key = hash<<32 | nocheck<<31 | concat pos.
+// One warp per query, a lane per position: every position of a
+// delimiter-free stretch of at least L residues is hashed; key = hash<<32 |
+// nocheck<<31 | concat pos.  A position's stretch is bounded by its nearest
+// delimiters (prev, next: delim_dist_kernel); keys are appended warp-wide.
 __global__ void query_entries_kernel(DevParams p, const uint8_t *__restrict__ q,
                                      const uint32_t *__restrict__ offsets,
-                                     const uint32_t *__restrict__ lengths, uint32_t nq,
+                                     const uint32_t *__restrict__ lengths,
+                                     const uint32_t *__restrict__ prev,
+                                     const uint32_t *__restrict__ next, uint32_t nq,
                                      uint64_t *keys, unsigned long long *count,
                                      unsigned long long cap) {
   const uint32_t L = (uint32_t)p.subsequence_length;
-  for (uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x; qi < nq;
-       qi += gridDim.x * blockDim.x) {
-    const uint8_t *s = q + offsets[qi];
-    const uint32_t len = lengths[qi];
-    uint32_t off = 0;
-    while (off < len) {
-      uint32_t end = off;
-      while (end < len && s[end] != p.delimiter) ++end;
-      if (end - off >= L) {
-        const uint32_t cs = off + L / 2, ce = end - L / 2;
-        for (uint32_t i = off; i < end; ++i) {
-          uint32_t h;
-          int hl;
-          if (seed_hash(p, s + i, &h, &hl)) {
-            const uint64_t nocheck = (cs <= i && i < ce) ? 0 : 1;
-            const uint64_t k = ((uint64_t)h << 32) | (nocheck << 31) |
-                               (uint64_t)(offsets[qi] + i);
-            const unsigned long long slot = atomicAdd(count, 1ull);
-            if (slot < cap) keys[slot] = k;
-          }
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t qi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; qi < nq; qi += warps) {
+    const uint32_t base = offsets[qi], len = lengths[qi];
+    for (uint32_t i0 = 0; i0 < len; i0 += 32) {
+      const uint32_t i = i0 + lane;
+      const uint32_t pos = base + i;
+      bool have = false;
+      uint64_t k = 0;
+      if (i < len && q[pos] != p.delimiter) {
+        const uint32_t off = prev[pos] + 1 - base, end = next[pos] - base;  // the stretch
+        uint32_t h;
+        int hl;
+        if (end - off >= L && seed_hash(p, q + pos, &h, &hl)) {
+          const uint32_t cs = off + L / 2, ce = end - L / 2;
+          const uint64_t nocheck = (cs <= i && i < ce) ? 0 : 1;
+          k = ((uint64_t)h << 32) | (nocheck << 31) | (uint64_t)pos;
+          have = true;
         }
       }
-      off = end + 1;
+      if (have) append(keys, count, cap, k);
     }
   }
 }
@@ -1305,6 +1307,7 @@ struct gzb_engine {
   bool have_db = false;
   // queries
   DBuf q_buf, q_offsets, q_lengths, q_cut, q_trig;
+  DBuf q_off64, q_prep;  // query preparation on the device: 64-bit offsets, scratch
   DBuf q_prev, q_next;  // nearest delimiters of every query position
   uint64_t q_len = 0;
   uint32_t nq = 0;
@@ -1456,6 +1459,22 @@ __global__ void code_range_kernel(const uint8_t *p, uint64_t n, unsigned int *ba
   if (blockIdx.x == 0 && threadIdx.x < 16 && n16 * 16 + threadIdx.x < n)
     acc |= p[n16 * 16 + threadIdx.x];
   if (acc & 0xE0E0E0E0u) atomicOr(bad, 1u);
+}
+
+// the query cutoffs the engine takes (1..32767) and triggers (int16)
+__global__ void cutoff_range_kernel(const int32_t *cut, const int32_t *trig, uint32_t n,
+                                    unsigned int *bad) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if (cut[i] < 1 || cut[i] > 32767 || trig[i] < -32768 || trig[i] > 32767) atomicOr(bad, 1u);
+}
+
+// cut[idx[i]] = c[i], trig[idx[i]] = t[i]
+__global__ void scatter_cutoffs_kernel(const uint32_t *idx, const int32_t *c, const int32_t *t,
+                                       uint32_t n, int32_t *cut, int32_t *trig) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    cut[idx[i]] = c[i];
+    trig[idx[i]] = t[i];
+  }
 }
 
 // Uploads `len` residue codes between kPad delimiter bytes on each side and
@@ -2091,38 +2110,11 @@ extern "C" int gzb_engine_prefetch_database_with_index(
   return GZB_OK;
 }
 
-extern "C" int gzb_engine_set_queries(
-gzb_engine *e, const uint8_t *codes, uint64_t length,
-                                      const uint32_t *offsets, const uint32_t *lengths,
-                                      uint32_t number_queries, const int32_t *cutoffs,
-                                      const int32_t *triggers, void *stream) {
-  GZB_TRY(check_engine(e));
-  GZB_CHECK(e->have_params, GZB_ERR_INVALID, "set_params first");
-  GZB_CHECK(codes && offsets && lengths && cutoffs && triggers && number_queries > 0,
-            GZB_ERR_INVALID, "empty query set");
-  GZB_CHECK(length < (1ull << 31), GZB_ERR_OVERFLOW, "query buffer exceeds 2^31 residues");
-  cudaStream_t s = (cudaStream_t)stream;
-  e->have_queries = false;
-  uint32_t maxl = 0;
-  for (uint32_t i = 0; i < number_queries; ++i) {
-    GZB_CHECK(lengths[i] >= 2 && (uint64_t)offsets[i] + lengths[i] <= length, GZB_ERR_INVALID,
-              "query %u outside the buffer", i);
-    GZB_CHECK(i == 0 || offsets[i] >= offsets[i - 1], GZB_ERR_INVALID,
-              "query offsets must be non-decreasing");
-    GZB_CHECK(cutoffs[i] >= 1 && cutoffs[i] <= 32767, GZB_ERR_INVALID,
-              "ungapped cutoff of query %u outside 1..32767", i);
-    GZB_CHECK(triggers[i] >= -32768 && triggers[i] <= 32767, GZB_ERR_INVALID,
-              "gapped trigger of query %u outside int16", i);
-    maxl = std::max(maxl, lengths[i]);
-  }
-  e->nq = number_queries;
-  e->q_len = length;
-  e->max_qlen = maxl;
-  GZB_TRY(upload_padded(e->q_buf, e->codeflag, codes, length, (uint8_t)e->params.delimiter, s));
-  GZB_TRY(upload(e->q_offsets, offsets, number_queries, s));
-  GZB_TRY(upload(e->q_lengths, lengths, number_queries, s));
-  GZB_TRY(upload(e->q_cut, cutoffs, number_queries, s));
-  GZB_TRY(upload(e->q_trig, triggers, number_queries, s));
+namespace {
+// The device side of a new query set whose codes, offsets, lengths, cutoffs
+// and triggers are on the device: nearest delimiters, the hash lists
+// (SeedSearcherGpuQueryParameters::Build) and empty results.
+int build_query_lists(gzb_engine *e, uint64_t length, uint32_t number_queries, cudaStream_t s) {
   GZB_TRY(e->q_prev.ensure(4 * (length + 1)));
   GZB_TRY(e->q_next.ensure(4 * (length + 1)));
   delim_dist_kernel<<<grid1((uint64_t)number_queries * 32, 256), 256, 0, s>>>(
@@ -2135,10 +2127,10 @@ gzb_engine *e, const uint8_t *codes, uint64_t length,
   GZB_TRY(alt.ensure(8 * (length + 1)));
   GZB_TRY(e->ctr.ensure(64));
   GZB_CUDA(cudaMemsetAsync(e->ctr.p, 0, 8, s));
-  query_entries_kernel<<<grid1(number_queries, 128), 128, 0, s>>>(
+  query_entries_kernel<<<grid1((uint64_t)number_queries * 32, 256), 256, 0, s>>>(
       e->dp, e->q_buf.as<uint8_t>() + kPad, e->q_offsets.as<uint32_t>(),
-      e->q_lengths.as<uint32_t>(), number_queries, keys.as<uint64_t>(),
-      e->ctr.as<unsigned long long>(), length + 1);
+      e->q_lengths.as<uint32_t>(), e->q_prev.as<uint32_t>(), e->q_next.as<uint32_t>(),
+      number_queries, keys.as<uint64_t>(), e->ctr.as<unsigned long long>(), length + 1);
   GZB_CUDA(cudaGetLastError());
   uint64_t n = 0;
   GZB_CUDA(cudaMemcpyAsync(&n, e->ctr.p, 8, cudaMemcpyDeviceToHost, s));
@@ -2204,6 +2196,159 @@ gzb_engine *e, const uint8_t *codes, uint64_t length,
   GZB_CUDA(cudaStreamSynchronize(s));
   e->have_queries = true;
   return GZB_OK;
+}
+}  // namespace
+
+extern "C" int gzb_engine_set_queries(
+gzb_engine *e, const uint8_t *codes, uint64_t length,
+                                      const uint32_t *offsets, const uint32_t *lengths,
+                                      uint32_t number_queries, const int32_t *cutoffs,
+                                      const int32_t *triggers, void *stream) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(e->have_params, GZB_ERR_INVALID, "set_params first");
+  GZB_CHECK(codes && offsets && lengths && cutoffs && triggers && number_queries > 0,
+            GZB_ERR_INVALID, "empty query set");
+  GZB_CHECK(length < (1ull << 31), GZB_ERR_OVERFLOW, "query buffer exceeds 2^31 residues");
+  cudaStream_t s = (cudaStream_t)stream;
+  e->have_queries = false;
+  uint32_t maxl = 0;
+  for (uint32_t i = 0; i < number_queries; ++i) {
+    GZB_CHECK(lengths[i] >= 2 && (uint64_t)offsets[i] + lengths[i] <= length, GZB_ERR_INVALID,
+              "query %u outside the buffer", i);
+    GZB_CHECK(i == 0 || offsets[i] + 1 >= offsets[i - 1] + lengths[i - 1], GZB_ERR_INVALID,
+              "query %u overlaps the previous one beyond their shared delimiter", i);
+    GZB_CHECK(codes[offsets[i]] == e->params.delimiter &&
+                  codes[offsets[i] + lengths[i] - 1] == e->params.delimiter,
+              GZB_ERR_INVALID, "query %u does not start and end with the delimiter", i);
+    GZB_CHECK(cutoffs[i] >= 1 && cutoffs[i] <= 32767, GZB_ERR_INVALID,
+              "ungapped cutoff of query %u outside 1..32767", i);
+    GZB_CHECK(triggers[i] >= -32768 && triggers[i] <= 32767, GZB_ERR_INVALID,
+              "gapped trigger of query %u outside int16", i);
+    maxl = std::max(maxl, lengths[i]);
+  }
+  e->nq = number_queries;
+  e->q_len = length;
+  e->max_qlen = maxl;
+  GZB_TRY(upload_padded(e->q_buf, e->codeflag, codes, length, (uint8_t)e->params.delimiter, s));
+  GZB_TRY(upload(e->q_offsets, offsets, number_queries, s));
+  GZB_TRY(upload(e->q_lengths, lengths, number_queries, s));
+  GZB_TRY(upload(e->q_cut, cutoffs, number_queries, s));
+  GZB_TRY(upload(e->q_trig, triggers, number_queries, s));
+  return build_query_lists(e, length, number_queries, s);
+}
+
+extern "C" int gzb_engine_set_protein_queries(gzb_engine *e, const uint8_t *codes,
+                                              uint64_t length, const uint32_t *offsets,
+                                              const uint32_t *lengths, uint32_t number_queries,
+                                              int filter, float ungapped_bits,
+                                              float trigger_bits, int32_t *cutoffs,
+                                              int32_t *triggers, void *stream) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(e->have_params, GZB_ERR_INVALID, "set_params first");
+  GZB_CHECK(codes && offsets && lengths && number_queries > 0, GZB_ERR_INVALID,
+            "empty query set");
+  GZB_CHECK(length < (1ull << 31), GZB_ERR_OVERFLOW, "query buffer exceeds 2^31 residues");
+  cudaStream_t s = (cudaStream_t)stream;
+  e->have_queries = false;
+  uint32_t maxl = 0;
+  std::vector<uint64_t> off64(number_queries);
+  std::vector<uint32_t> short_ids;
+  for (uint32_t i = 0; i < number_queries; ++i) {
+    GZB_CHECK(lengths[i] >= 2 && (uint64_t)offsets[i] + lengths[i] <= length, GZB_ERR_INVALID,
+              "query %u outside the buffer", i);
+    GZB_CHECK(i == 0 || offsets[i] + 1 >= offsets[i - 1] + lengths[i - 1], GZB_ERR_INVALID,
+              "query %u overlaps the previous one beyond their shared delimiter", i);
+    GZB_CHECK(codes[offsets[i]] == e->params.delimiter &&
+                  codes[offsets[i] + lengths[i] - 1] == e->params.delimiter,
+              GZB_ERR_INVALID, "query %u does not start and end with the delimiter", i);
+    maxl = std::max(maxl, lengths[i]);
+    off64[i] = offsets[i];
+    // a protein the filter refuses (fewer residues than SEG's 12-letter
+    // window) is held as its leading delimiter and a zero-filled body, its
+    // last code 0 rather than a delimiter (ProteinQuery,
+    // src/protein_query.cpp:39-49), and its statistics are those of that
+    // buffer
+    if (filter && lengths[i] - 2 < 12) short_ids.push_back(i);
+  }
+  e->nq = number_queries;
+  e->q_len = length;
+  e->max_qlen = maxl;
+  const uint8_t delim = (uint8_t)e->params.delimiter;
+  GZB_TRY(e->q_buf.ensure(length + 2 * kPad));
+  GZB_TRY(e->codeflag.ensure(16));
+  GZB_CUDA(cudaMemsetAsync(e->q_buf.p, delim, length + 2 * kPad, s));
+  GZB_CUDA(cudaMemcpyAsync(e->q_buf.as<uint8_t>() + kPad, codes, length, cudaMemcpyHostToDevice,
+                           s));
+  GZB_CUDA(cudaMemsetAsync(e->codeflag.p, 0, 16, s));
+  GZB_TRY(upload(e->q_offsets, offsets, number_queries, s));
+  GZB_TRY(upload(e->q_lengths, lengths, number_queries, s));
+  GZB_TRY(upload(e->q_off64, off64.data(), number_queries, s));
+  GZB_TRY(e->q_cut.ensure(4 * (uint64_t)number_queries));
+  GZB_TRY(e->q_trig.ensure(4 * (uint64_t)number_queries));
+  uint8_t *q = e->q_buf.as<uint8_t>() + kPad;
+  unsigned int *flags = e->codeflag.as<unsigned int>();  // codes, SEG status, cutoffs
+  if (filter)
+    GZB_TRY(gzb_seg_protein_queries(q, e->q_off64.as<uint64_t>(), e->q_lengths.as<uint32_t>(),
+                                    number_queries, flags + 1, s));
+  code_range_kernel<<<grid1(length / 16 + 1, 256), 256, 0, s>>>(q, length, flags);
+  GZB_CUDA(cudaGetLastError());
+  GZB_TRY(gzb_query_karlin_cutoffs(q, e->q_off64.as<uint64_t>(), e->q_lengths.as<uint32_t>(),
+                                   number_queries, e->params.score_matrix,
+                                   (uint32_t)e->params.number_letters, ungapped_bits,
+                                   trigger_bits, e->q_cut.as<int32_t>(),
+                                   e->q_trig.as<int32_t>(), nullptr, s));
+  const uint32_t ns = (uint32_t)short_ids.size();
+  if (ns) {
+    // the short proteins' buffers, back to back, then their cutoffs
+    std::vector<uint64_t> so(ns);
+    std::vector<uint32_t> sl(ns);
+    uint64_t total = 0;
+    for (uint32_t j = 0; j < ns; ++j) {
+      so[j] = total;
+      sl[j] = lengths[short_ids[j]];
+      total += sl[j];
+    }
+    std::vector<uint8_t> buf(total, 0);
+    for (uint32_t j = 0; j < ns; ++j) buf[so[j]] = delim;
+    const uint64_t at_idx = 0, at_off = 4 * (ns + 1) / 8 * 8 + 8, at_len = at_off + 8 * ns,
+                   at_c = at_len + 4 * ns, at_t = at_c + 4 * ns, at_buf = at_t + 4 * ns;
+    GZB_TRY(e->q_prep.ensure(at_buf + total + 2 * kPad));
+    uint8_t *base = e->q_prep.as<uint8_t>();
+    GZB_CUDA(cudaMemcpyAsync(base + at_idx, short_ids.data(), 4 * ns, cudaMemcpyHostToDevice, s));
+    GZB_CUDA(cudaMemcpyAsync(base + at_off, so.data(), 8 * ns, cudaMemcpyHostToDevice, s));
+    GZB_CUDA(cudaMemcpyAsync(base + at_len, sl.data(), 4 * ns, cudaMemcpyHostToDevice, s));
+    GZB_CUDA(cudaMemsetAsync(base + at_buf, delim, total + 2 * kPad, s));
+    GZB_CUDA(cudaMemcpyAsync(base + at_buf + kPad, buf.data(), total, cudaMemcpyHostToDevice, s));
+    GZB_TRY(gzb_query_karlin_cutoffs(
+        base + at_buf + kPad, reinterpret_cast<const uint64_t *>(base + at_off),
+        reinterpret_cast<const uint32_t *>(base + at_len), ns, e->params.score_matrix,
+        (uint32_t)e->params.number_letters, ungapped_bits, trigger_bits,
+        reinterpret_cast<int32_t *>(base + at_c), reinterpret_cast<int32_t *>(base + at_t),
+        nullptr, s));
+    scatter_cutoffs_kernel<<<grid1(ns, 128), 128, 0, s>>>(
+        reinterpret_cast<const uint32_t *>(base + at_idx),
+        reinterpret_cast<const int32_t *>(base + at_c),
+        reinterpret_cast<const int32_t *>(base + at_t), ns, e->q_cut.as<int32_t>(),
+        e->q_trig.as<int32_t>());
+    GZB_CUDA(cudaGetLastError());
+  }
+  cutoff_range_kernel<<<grid1(number_queries, 256), 256, 0, s>>>(
+      e->q_cut.as<int32_t>(), e->q_trig.as<int32_t>(), number_queries, flags + 2);
+  GZB_CUDA(cudaGetLastError());
+  if (cutoffs)
+    GZB_CUDA(cudaMemcpyAsync(cutoffs, e->q_cut.p, 4 * (uint64_t)number_queries,
+                             cudaMemcpyDeviceToHost, s));
+  if (triggers)
+    GZB_CUDA(cudaMemcpyAsync(triggers, e->q_trig.p, 4 * (uint64_t)number_queries,
+                             cudaMemcpyDeviceToHost, s));
+  unsigned int bad[3] = {0, 0, 0};
+  GZB_CUDA(cudaMemcpyAsync(bad, flags, 12, cudaMemcpyDeviceToHost, s));
+  GZB_CUDA(cudaStreamSynchronize(s));
+  GZB_CHECK(bad[0] == 0, GZB_ERR_INVALID, "residue codes must be below 32 (after SEG)");
+  GZB_CHECK(bad[1] == 0, GZB_ERR_INVALID, "SEG left %u queries unmasked", bad[1]);
+  GZB_CHECK(bad[2] == 0, GZB_ERR_INVALID,
+            "a query's cutoff is outside 1..32767 or its trigger outside int16");
+  return build_query_lists(e, length, number_queries, s);
 }
 
 extern "C" int gzb_engine_reset_results(gzb_engine *e, void *stream) {

@@ -101,6 +101,8 @@ def _declare(L):
         "gzb_engine_set_params": [V, V],
         "gzb_engine_set_database": [V, I32, V, C.c_uint64, V, U32, V],
         "gzb_engine_set_queries": [V, V, C.c_uint64, V, V, U32, V, V, V],
+        "gzb_engine_set_protein_queries": [V, V, C.c_uint64, V, V, U32, C.c_int, C.c_float,
+                                           C.c_float, V, V, V],
         "gzb_engine_presearch": [V, C.c_int, V],
         "gzb_engine_reset_results": [V, V],
         "gzb_engine_get_results": [V, V, V, V],
@@ -477,6 +479,24 @@ class PresearchEngine:
                                            hptr(lens), int(queries.number), hptr(cut),
                                            hptr(trig), _stream_or_null(stream)))
         self.number_queries = int(queries.number)
+
+    def set_protein_queries(self, codes, offsets, lengths, filter=True, ungapped_bits=7.0,
+                            trigger_bits=22.0, stream=None):
+        """Raw protein queries in the engine layout (codes from
+        encode_protein_for_seg) prepared on the device -- SEG when filter,
+        per-query cutoffs -- and set (gzb_engine_set_protein_queries).
+        Returns the (cutoffs, triggers) host arrays."""
+        codes = np.ascontiguousarray(codes, dtype=np.uint8)
+        offs = np.ascontiguousarray(offsets, dtype=np.uint32)
+        lens = np.ascontiguousarray(lengths, dtype=np.uint32)
+        n = len(offs)
+        cut, trig = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        check(lib().gzb_engine_set_protein_queries(
+            self.h, hptr(codes), len(codes), hptr(offs), hptr(lens), n, 1 if filter else 0,
+            float(ungapped_bits), float(trigger_bits), hptr(cut), hptr(trig),
+            _stream_or_null(stream)))
+        self.number_queries = n
+        return cut, trig
 
     def presearch(self, schedule=SCHEDULE_PLAIN, stream=None):
         check(lib().gzb_engine_presearch(self.h, int(schedule), _stream_or_null(stream)))

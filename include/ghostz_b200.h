@@ -342,6 +342,23 @@ int gzb_engine_set_queries(gzb_engine *e, const uint8_t *codes,
                            const uint32_t *lengths, uint32_t number_queries,
                            const int32_t *ungapped_cutoffs,
                            const int32_t *gapped_triggers, void *stream);
+/* Query preparation and gzb_engine_set_queries in one call, the prepared
+ * codes never leaving the device: protein queries in the engine layout
+ * (host codes; a letter the reference's SEG does not count, lower case,
+ * passed as its code + 32) are uploaded, SEG-masked in place when filter is
+ * non-zero (gzb_seg_protein_queries; a protein shorter than SEG's window
+ * keeps a zero-filled body and the statistics of ProteinQuery's buffer),
+ * given their cutoffs by gzb_query_karlin_cutoffs with the engine's score
+ * matrix (ungapped_bits / trigger_bits: 7 and 22 for aln), and their hash
+ * lists are built.  cutoffs / triggers (optional, host) receive the
+ * per-query values.  Replaces Queries::BuildQuery (src/queries.cpp:83-107)
+ * and AlignerGpu::SetQueriesData (src/aligner_gpu.cpp:213-242) for -q p.
+ * Synchronises `stream`. */
+int gzb_engine_set_protein_queries(gzb_engine *e, const uint8_t *codes, uint64_t length,
+                                   const uint32_t *offsets, const uint32_t *lengths,
+                                   uint32_t number_queries, int filter, float ungapped_bits,
+                                   float trigger_bits, int32_t *cutoffs, int32_t *triggers,
+                                   void *stream);
 /* Runs the presearch of the resident queries against the resident chunk
  * and merges into the per-query top-b lists kept on the device.  Call
  * gzb_engine_reset_results before the first chunk of a query set. */

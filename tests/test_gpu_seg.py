@@ -120,3 +120,50 @@ def test_seg_prepared_queries_search_like_oracle(native, oracle, params):
             assert np.array_equal(got[i], res[i]), i
     finally:
         e.close()
+
+
+@pytest.mark.parametrize("filter_", [True, False])
+def test_engine_prepares_protein_queries_on_device(native, oracle, params, filter_):
+    """gzb_engine_set_protein_queries (SEG, cutoffs and hash lists on the
+    device, the prepared codes never read back) gives the cutoffs, lists and
+    presearch results of prepare_protein_queries + set_queries, whose
+    preparation the oracle pins; with the filter, short, low-complexity and
+    lower-case proteins are mixed in."""
+    rng = np.random.default_rng(91)
+    db = W.make_database(1200, 93, median=250)
+    seqs = W.query_sequences(W.make_queries(db, 150, 94, median=250))
+    if filter_:
+        seqs += [native.encode_protein_for_seg(_low_complexity_protein(rng, n))
+                 for n in (0, 1, 5, 11, 12, 13, 50, 300, 900)]
+    q = W.pack_queries(seqs, cutoffs=(np.zeros(len(seqs), np.int32),
+                                      np.zeros(len(seqs), np.int32)))
+    codes, cut, trig = native.prepare_protein_queries(q.codes, q.offsets, q.lengths,
+                                                      filter=filter_)
+    ref = W.Queries(codes=codes, offsets=q.offsets, lengths=q.lengths, cutoffs=cut,
+                    triggers=trig)
+    e = native.PresearchEngine(0)
+    try:
+        e.set_params(params)
+        e.set_database(db)
+        e.set_queries(ref)
+        lists_a = e.list_arrays()
+        e.reset_results()
+        e.presearch(native.SCHEDULE_BATCHED)
+        res_a = e.results()
+        cut_b, trig_b = e.set_protein_queries(q.codes, q.offsets, q.lengths, filter=filter_)
+        assert np.array_equal(cut_b, cut) and np.array_equal(trig_b, trig)
+        lists_b = e.list_arrays()
+        for name in lists_a:
+            assert np.array_equal(lists_a[name], lists_b[name]), name
+        e.reset_results()
+        e.presearch(native.SCHEDULE_BATCHED)
+        res_b = e.results()
+        assert sum(len(r) for r in res_a) > 0
+        for i in range(q.number):
+            assert np.array_equal(res_a[i], res_b[i]), i
+        if filter_:
+            exp, _, _ = oracle.presearch(params, db, ref)
+            for i in range(q.number):
+                assert np.array_equal(res_b[i], exp[i]), i
+    finally:
+        e.close()
