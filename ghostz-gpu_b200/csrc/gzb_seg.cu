@@ -17,8 +17,9 @@
 // Only the 20 standard amino acids count towards compositions.
 //
 // Two passes over the sequences (frames of translated queries or bodies of
-// protein queries), in place.  Pass 1, one thread per sequence, only
-// computes the window entropies; a sequence with no window at or below the
+// protein queries), in place.  Pass 1, one thread per frame (a warp per
+// protein, its windows split over the lanes), only computes the window
+// entropies; a sequence with no window at or below the
 // low cut (most of them) is done, the others are marked.  Pass 2, one warp
 // per marked sequence, runs the whole search: masked positions get bit 6
 // set while it runs (so later windows still see the letters) and become the
@@ -398,6 +399,95 @@ __global__ void __launch_bounds__(kSegBlock)
   }
 }
 
+// Pass 1 for protein queries (long sequences), one warp per sequence: the
+// window starts split into 32 runs, each lane sliding over its own with the
+// counts-of-counts of seg_scan_kernel (the same sums in the same order, so
+// the same decisions); the sequence is marked when any lane finds a window
+// at or below the low cut.
+__global__ void __launch_bounds__(kSegBlock)
+    seg_scan_warp_kernel(SegArgs a, uint8_t *__restrict__ codes,
+                         const uint64_t *__restrict__ offsets,
+                         const uint32_t *__restrict__ lengths, uint64_t units, int mode,
+                         uint32_t *__restrict__ status) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t u = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; u < units;
+       u += warps) {
+    int n;
+    uint8_t fallback;
+    uint8_t *s = unit_of(codes, offsets, lengths, u, mode, &n, &fallback);
+    if (n <= 0) continue;
+    if (n < kSegWindow) {
+      for (int i = lane; i < n; i += 32) s[i] = fallback;
+      continue;
+    }
+    if (n > kSegMaxLength) {
+      if (status && lane == 0) atomicAdd(status, 1u);
+      for (int i = lane; i < n; i += 32) s[i] = finish_code(s[i]);
+      continue;
+    }
+    bool shifted = false;
+    for (int i = lane; i < n; i += 32) shifted |= (s[i] & 63) >= 32;
+    const int m = n - kSegWindow + 1;  // window starts 0 .. n-12
+    const int run = (m + 31) / 32, p0 = lane * run, p1 = min(p0 + run, m);
+    bool low = false;
+    if (p0 < p1) {
+      uint8_t comp[20];
+      uint8_t per[kSegWindow + 1];  // per[v]: letters occurring v times
+      for (int k = 0; k < 20; ++k) comp[k] = 0;
+      for (int v = 0; v <= kSegWindow; ++v) per[v] = 0;
+      int total = 0;
+      for (int i = p0; i < p0 + kSegWindow; ++i) {
+        const int k = seg_class(s[i]);
+        if (k >= 0) {
+          ++comp[k];
+          ++total;
+        }
+      }
+      for (int k = 0; k < 20; ++k) ++per[comp[k]];
+      for (int start = p0;; ++start) {
+        double ent = 0.0;
+        if (total == kSegWindow) {
+          for (int v = kSegWindow; v >= 1; --v)
+            for (int t = 0; t < per[v]; ++t) ent = __dadd_rn(ent, a.entropy12[v]);
+        } else if (total > 0) {
+          const double r = __ddiv_rn(1.0, (double)total);
+          for (int v = total; v >= 1; --v)
+            for (int t = 0; t < per[v]; ++t)
+              ent = __dadd_rn(ent, __dmul_rn((double)v, a.log_ratio[total][v]));
+          ent = __ddiv_rn(__dmul_rn(-ent, r), a.ln2);
+        }
+        if (ent <= kSegLowCut) {
+          low = true;
+          break;
+        }
+        if (start + 1 >= p1) break;
+        const int out = seg_class(s[start]), in = seg_class(s[start + kSegWindow]);
+        if (out >= 0) {
+          --per[comp[out]];
+          --comp[out];
+          ++per[comp[out]];
+          --total;
+        }
+        if (in >= 0) {
+          --per[comp[in]];
+          ++comp[in];
+          ++per[comp[in]];
+          ++total;
+        }
+      }
+    }
+    const bool marked = __any_sync(0xffffffffu, low);
+    shifted = __any_sync(0xffffffffu, shifted);
+    if (marked) {
+      if (lane == 0) s[0] |= 128;
+    } else if (shifted) {
+      for (int i = lane; i < n; i += 32) s[i] = finish_code(s[i]);
+    }
+    __syncwarp();
+  }
+}
+
 // Pass 2, one warp per sequence pass 1 marked: the whole search
 __global__ void __launch_bounds__(kSegBlock)
     seg_search_kernel(SegArgs a, uint8_t *__restrict__ codes, const uint64_t *__restrict__ offsets,
@@ -498,11 +588,16 @@ int launch_seg(uint8_t *codes, const uint64_t *offsets, const uint32_t *lengths,
   int device = 0, sms = 148;
   GZB_CUDA(cudaGetDevice(&device));
   GZB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
-  const uint64_t want = (units + kSegBlock - 1) / kSegBlock;
   const uint64_t most = (uint64_t)sms * 16;
-  const uint32_t blocks = (uint32_t)(want < most ? want : most);
-  seg_scan_kernel<<<blocks, kSegBlock, 0, stream>>>(g_args, codes, offsets, lengths, units,
-                                                     mode, status);
+  if (mode == 0) {  // frames of translated reads: short, one thread each
+    const uint64_t want = (units + kSegBlock - 1) / kSegBlock;
+    seg_scan_kernel<<<(uint32_t)(want < most ? want : most), kSegBlock, 0, stream>>>(
+        g_args, codes, offsets, lengths, units, mode, status);
+  } else {  // protein bodies: a warp each
+    const uint64_t want = (units + kSegBlock / 32 - 1) / (kSegBlock / 32);
+    seg_scan_warp_kernel<<<(uint32_t)(want < most ? want : most), kSegBlock, 0, stream>>>(
+        g_args, codes, offsets, lengths, units, mode, status);
+  }
   GZB_CUDA(cudaGetLastError());
   const uint64_t want2 = (units + kSegBlock / 32 - 1) / (kSegBlock / 32);
   const uint64_t most2 = (uint64_t)sms * 8;
