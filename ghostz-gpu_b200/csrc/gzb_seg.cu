@@ -55,8 +55,10 @@ constexpr uint8_t kMaskBit = 64;
 constexpr uint8_t kUnknownCode = 24;      // X
 constexpr int kSegBlock = 128;
 // window entropies a warp of the search pass keeps in shared memory (the
-// windows of sequences up to kSegCache + 11 residues)
-constexpr int kSegCache = 1024;
+// windows of sequences up to `cache` + 11 residues): 1024 for the short
+// frames of translated reads (four warps a block), 4096 for proteins (two)
+constexpr int kSegCacheFrames = 1024;
+constexpr int kSegCacheProteins = 4096;
 
 // ln(n!) rounded to 6 decimals (the precision of the reference's table)
 __device__ double g_seg_ln_fact[kSegMaxLength + 1];
@@ -492,10 +494,10 @@ __global__ void __launch_bounds__(kSegBlock)
 __global__ void __launch_bounds__(kSegBlock)
     seg_search_kernel(SegArgs a, uint8_t *__restrict__ codes, const uint64_t *__restrict__ offsets,
                       const uint32_t *__restrict__ lengths, uint64_t units, int mode,
-                      uint32_t *__restrict__ status) {
-  __shared__ double ecache[kSegBlock / 32][kSegCache];
+                      uint32_t *__restrict__ status, int cache) {
+  extern __shared__ double ecache[];  // [warps of the block][cache]
   const int lane = threadIdx.x & 31;
-  double *E = ecache[threadIdx.x >> 5];
+  double *E = ecache + (size_t)(threadIdx.x >> 5) * cache;
   const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   for (uint64_t u = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; u < units;
        u += warps) {
@@ -509,7 +511,7 @@ __global__ void __launch_bounds__(kSegBlock)
     __syncwarp();
     // the window entropies, lane l sliding over its own run of starts
     const int m = n - kSegWindow + 1;  // window starts 0 .. n-12
-    const bool cached = m <= kSegCache;
+    const bool cached = m <= cache;
     if (cached) {
       const int per = (m + 31) / 32, p0 = lane * per, p1 = min(p0 + per, m);
       if (p0 < p1) {
@@ -599,10 +601,15 @@ int launch_seg(uint8_t *codes, const uint64_t *offsets, const uint32_t *lengths,
         g_args, codes, offsets, lengths, units, mode, status);
   }
   GZB_CUDA(cudaGetLastError());
-  const uint64_t want2 = (units + kSegBlock / 32 - 1) / (kSegBlock / 32);
-  const uint64_t most2 = (uint64_t)sms * 8;
-  seg_search_kernel<<<(uint32_t)(want2 < most2 ? want2 : most2), kSegBlock, 0, stream>>>(
-      g_args, codes, offsets, lengths, units, mode, status);
+  const int cache = mode == 0 ? kSegCacheFrames : kSegCacheProteins;
+  const int block = mode == 0 ? 128 : 64;
+  const uint64_t want2 = (units + block / 32 - 1) / (block / 32);
+  const uint64_t most2 = (uint64_t)sms * (mode == 0 ? 8 : 16);
+  const size_t cache_bytes = sizeof(double) * (block / 32) * cache;
+  GZB_CUDA(cudaFuncSetAttribute(seg_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)cache_bytes));
+  seg_search_kernel<<<(uint32_t)(want2 < most2 ? want2 : most2), block, cache_bytes, stream>>>(
+      g_args, codes, offsets, lengths, units, mode, status, cache);
   GZB_CUDA(cudaGetLastError());
   return GZB_OK;
 }
