@@ -1112,8 +1112,7 @@ __global__ void merge_kernel(uint32_t nq, const uint64_t *hits, const uint64_t *
                              const int32_t *escore, const uint32_t *q_offsets, int qbits,
                              int dbits, const uint32_t *db_offsets, uint32_t nseq,
                              uint32_t db_len, int32_t chunk_id, int max_results,
-                             int max_one_subject, gzb_result *scratch, ulonglong2 *keys_all,
-                             uint32_t *heap_all,
+                             int max_one_subject, ulonglong2 *keys_all, uint32_t *heap_all,
                              gzb_result *results, uint32_t *counts, const uint64_t *n_dev,
                              const uint32_t *skip) {
   // a run whose buffers overflowed merges nothing (it is redone)
@@ -1128,11 +1127,10 @@ __global__ void merge_kernel(uint32_t nq, const uint64_t *hits, const uint64_t *
     if (k == 0) continue;
     const uint64_t b = begin[qi], o = surv_off[qi];
     const uint32_t qoff = q_offsets[qi];
-    gzb_result *added = scratch + o;
     ulonglong2 *keys = keys_all + o;
     uint32_t *heap = heap_all + o + lane;
-    uint32_t m = 0;
-    for (uint32_t i = lane; i < k; i += 32) {
+    // candidate i of the query from its hit and its two extensions
+    auto candidate = [&](uint32_t i) {
       const uint64_t key = hits[b + i];
       gzb_result r;
       r.chunk_id = chunk_id;
@@ -1144,8 +1142,11 @@ __global__ void merge_kernel(uint32_t nq, const uint64_t *hits, const uint64_t *
       r.start_d = ed[o + i];
       r.end_q = eq[n_surv + o + i] - qoff;
       r.end_d = ed[n_surv + o + i];
-      added[i] = r;
-      keys[i] = merge_key(r);
+      return r;
+    };
+    uint32_t m = 0;
+    for (uint32_t i = lane; i < k; i += 32) {
+      keys[i] = merge_key(candidate(i));
       heap[32 * m] = i;
       ++m;
     }
@@ -1186,15 +1187,16 @@ __global__ void merge_kernel(uint32_t nq, const uint64_t *hits, const uint64_t *
         if ((int)n_out < max_results && (left > 0 || ri < n_old)) {
           cont = 1;
           gzb_result a;
+          const gzb_result cand = left ? candidate(g) : gzb_result{};
           bool take_added;
           if (left == 0)
             take_added = false;
           else if (ri == n_old)
             take_added = true;
           else
-            take_added = alignment_comp(old[ri], added[g]) < 0;
+            take_added = alignment_comp(old[ri], cand) < 0;
           if (take_added) {
-            a = added[g];
+            a = cand;
             a.subject_id = (int32_t)subject_of(db_offsets, nseq, db_len, a.start_d);
             popped = (int)g;
             --left;
@@ -1319,7 +1321,7 @@ struct gzb_engine {
   DBuf results, counts;
   // scratch
   DBuf tmp, hits, hits_alt, mwork, mwork_alt, begin, kept, surv_off, slots, eq, ed, edir,
-      escore, merge_scratch, heap, ctr, misc, hits_copy;
+      escore, heap, ctr, misc, hits_copy;
   int qbits = 1, dbits = 1;
   // schedule of the gapped stage
   DBuf elen0, elen1, eqid, efeat, epred, ecells, okeys, okeys2, oidx, oidx2, queue, prev_cells,
@@ -1572,11 +1574,11 @@ extern "C" int gzb_engine_destroy(gzb_engine *e) {
   for (auto &b : e->index_bufs) b.release();
   for (auto &b : e->list_bufs) b.release();
   DBuf *all[] = {&e->matrix32, &e->db_buf, &e->db_offsets, &e->q_buf, &e->q_offsets,
-                 &e->q_prev, &e->q_next,
+                 &e->q_prev, &e->q_next, &e->q_off64, &e->q_prep,
                  &e->q_lengths, &e->q_cut, &e->q_trig, &e->results, &e->counts,
                  &e->tmp, &e->hits, &e->hits_alt, &e->mwork, &e->mwork_alt,
                  &e->begin, &e->kept, &e->surv_off, &e->slots, &e->eq, &e->ed, &e->edir,
-                 &e->escore, &e->merge_scratch, &e->heap, &e->ctr, &e->misc,
+                 &e->escore, &e->heap, &e->ctr, &e->misc,
                  &e->hits_copy, &e->elen0, &e->elen1, &e->eqid, &e->efeat, &e->epred,
                  &e->ecells, &e->okeys, &e->okeys2, &e->oidx, &e->oidx2, &e->queue,
                  &e->prev_cells, &e->model_d, &e->mae_acc, &e->log_x, &e->log_y,
@@ -2643,7 +2645,6 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
   GZB_CUDA(cudaEventRecord(e->ev[4], s));
   // ---- top-b merge
   if (n_surv) {
-    GZB_TRY(e->merge_scratch.ensure(sizeof(gzb_result) * (n_surv + 1)));
     // per candidate: its sort key (16 B), then its heap slot (4 B)
     GZB_TRY(e->heap.ensure(20 * (n_surv + 1)));
     merge_kernel<<<grid1((uint64_t)nq * 32, 128), 128, 0, s>>>(
@@ -2651,7 +2652,7 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
         e->escore.as<int32_t>(), e->q_offsets.as<uint32_t>(), qbits, dbits,
         e->db_offsets.as<uint32_t>(), e->nseq, (uint32_t)e->db_len, e->chunk_id,
         e->params.max_number_results, e->params.max_number_one_subject_results,
-        e->merge_scratch.as<gzb_result>(), e->heap.as<ulonglong2>(),
+        e->heap.as<ulonglong2>(),
         reinterpret_cast<uint32_t *>(e->heap.as<ulonglong2>() + n_surv + 1),
         e->results.as<gzb_result>(), e->counts.as<uint32_t>(), nullptr, nullptr);
     GZB_CUDA(cudaGetLastError());
@@ -2775,7 +2776,6 @@ int graph_prepare(gzb_engine *e, const GraphCaps &c, int hit_bits, int mw_bits, 
     GZB_TRY(b->ensure(4 * (c.ext + 1)));
   GZB_TRY(e->edir.ensure(c.ext + 1));
   GZB_TRY(e->enb.ensure(4 * (c.hits + 1)));
-  GZB_TRY(e->merge_scratch.ensure(sizeof(gzb_result) * (c.hits + 1)));
   GZB_TRY(e->heap.ensure(20 * (c.hits + 1)));  // merge keys and heap slots
   if (learned) {  // the cost-model order
     GZB_TRY(e->efeat.ensure(4 * kFeat * (c.ext + 1)));
@@ -2952,7 +2952,7 @@ int graph_body(gzb_engine *e, int schedule, const GappedTile &tile, bool learned
       e->escore.as<int32_t>(), e->q_offsets.as<uint32_t>(), qbits, dbits,
       e->db_offsets.as<uint32_t>(), e->nseq, (uint32_t)e->db_len, e->chunk_id,
       e->params.max_number_results, e->params.max_number_one_subject_results,
-      e->merge_scratch.as<gzb_result>(), e->heap.as<ulonglong2>(),
+      e->heap.as<ulonglong2>(),
       reinterpret_cast<uint32_t *>(e->heap.as<ulonglong2>() + c.hits + 1),
       e->results.as<gzb_result>(), e->counts.as<uint32_t>(), plan + 2, overflow);
   GZB_CUDA(cudaGetLastError());
@@ -2982,7 +2982,7 @@ uint64_t graph_key(const gzb_engine *e, int schedule, const GappedTile &tile, bo
                         &e->tmp, &e->hits, &e->hits_alt, &e->hits_copy, &e->mwork,
                         &e->mwork_alt, &e->begin, &e->kept, &e->surv_off, &e->slots, &e->eq,
                         &e->ed, &e->edir, &e->escore, &e->elen0, &e->elen1, &e->eqid, &e->enb,
-                        &e->merge_scratch, &e->heap, &e->ctr, &e->plan, &e->list_bufs[14],
+                        &e->heap, &e->ctr, &e->plan, &e->list_bufs[14],
                         &e->efeat, &e->epred, &e->okeys, &e->okeys2, &e->oidx, &e->oidx2,
                         &e->model_d, &e->q_prev, &e->q_next};
   for (const DBuf *b : bufs) {

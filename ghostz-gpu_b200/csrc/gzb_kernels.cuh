@@ -42,12 +42,16 @@ namespace cg = cooperative_groups;
 
 constexpr int kInitScore = -(1 << 10);  // src/gapped_extender.h:40
 constexpr int kNegBig = -(1 << 29);
-constexpr int kMatrixStride = 32;       // shared-memory score matrix row
+// shared-memory score matrix row: 33 words, so that lanes reading different
+// rows (their own database residues) at the same column (query residue) hit
+// different banks
+constexpr int kMatrixStride = 33;
 
 __device__ __forceinline__ int imax(int a, int b) { return a > b ? a : b; }
 __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
 
-// Loads a score matrix with row stride `stride` into a 32x32 shared tile.
+// Loads a score matrix with row stride `stride` into the shared tile
+// (kMatrixStride x kMatrixStride, entries past number_letters zero).
 __device__ __forceinline__ void load_matrix(int *sm, const int32_t *m,
                                             int number_letters, int stride) {
   for (int i = threadIdx.x; i < kMatrixStride * kMatrixStride; i += blockDim.x) {

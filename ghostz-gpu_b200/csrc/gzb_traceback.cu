@@ -431,7 +431,7 @@ __global__ void __launch_bounds__(kTbWarpsPerBlock * 32)
                          uint64_t *walk_cap, uint8_t *redo) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
   __shared__ int2 bands[kTbWarpsPerBlock][kTbWarpColumns];
-  load_matrix(sm, a.matrix32, kMatrixStride, kMatrixStride);
+  load_matrix(sm, a.matrix32, 32, 32);  // the 32 x 32 device matrix
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (uint64_t s = blockIdx.x * (uint64_t)kTbWarpsPerBlock + warp; s < n_sides;
@@ -464,7 +464,7 @@ __global__ void __launch_bounds__(kTbWarpsPerBlock * 32)
                          int32_t *side_p0, int32_t *side_p1, const uint8_t *redo) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
   __shared__ int2 bands[kTbWarpsPerBlock][kTbWarpColumns];
-  load_matrix(sm, a.matrix32, kMatrixStride, kMatrixStride);
+  load_matrix(sm, a.matrix32, 32, 32);  // the 32 x 32 device matrix
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (uint64_t s = blockIdx.x * (uint64_t)kTbWarpsPerBlock + warp; s < n_sides;
@@ -501,7 +501,7 @@ __global__ void tb_count_kernel(TbArgs a, uint64_t n_sides, const uint64_t *band
                                 int2 *band, uint64_t *ops_bytes, uint64_t *rows,
                                 uint64_t *walk_cap, const uint8_t *redo) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
-  load_matrix(sm, a.matrix32, kMatrixStride, kMatrixStride);
+  load_matrix(sm, a.matrix32, 32, 32);  // the 32 x 32 device matrix
   __syncthreads();
   for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < n_sides;
        s += (uint64_t)gridDim.x * blockDim.x) {
@@ -531,7 +531,7 @@ __global__ void tb_walk_kernel(TbArgs a, uint64_t n_sides, const uint64_t *band_
                                int32_t *side_score, int32_t *side_p0, int32_t *side_p1,
                                const uint8_t *redo) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
-  load_matrix(sm, a.matrix32, kMatrixStride, kMatrixStride);
+  load_matrix(sm, a.matrix32, 32, 32);  // the 32 x 32 device matrix
   __syncthreads();
   for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < n_sides;
        s += (uint64_t)gridDim.x * blockDim.x) {
