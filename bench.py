@@ -12,9 +12,9 @@ sides, top-b merge.
 
   value : queries/s with the prepared queries already resident in HBM
   e2e   : queries/s of the search through the C ABI from host buffers: every
-          step copies the raw query residues in, prepares them (SEG,
-          cutoffs) and builds their hash lists on the device (protein
-          queries: one gzb_engine_set_protein_queries call), runs the
+          step copies the raw queries in, prepares them (translation, SEG,
+          cutoffs) and builds their hash lists on the device (one
+          gzb_engine_set_protein_queries / _set_translated_queries call), runs the
           presearch and the build results step, and reads every query's
           alignment records back (the work of `aln` after its database is
           loaded, except formatting the text lines).
@@ -1147,32 +1147,26 @@ def main():
     else:
         (p_dna, t1), (p_roffs, t2) = pinned_copy(raw.dna), pinned_copy(raw.offsets)
         keep += [t1, t2]
-        raw_bytes = raw.dna.nbytes + raw.offsets.nbytes * 2
+        raw_bytes = raw.dna.nbytes + raw.offsets.nbytes
         protein_on_device = False
-
-        def prepare():
-            codes, offs, lens, cut, trig = N.prepare_translated_queries(p_dna, p_roffs)
-            return W.translated_queries(codes, offs, lens, cutoffs=(cut, trig))
     counts_pin = torch.empty(q.number * 4, dtype=torch.uint8).pin_memory()
     al_pin = torch.empty(q.number * b * N.ALIGNMENT_DTYPE.itemsize,
                          dtype=torch.uint8).pin_memory()
 
     def e2e_step():
+        # query preparation (translation, SEG, cutoffs) and hash lists on the
+        # device: gzb_engine_set_protein_queries / _set_translated_queries
         if protein_on_device:
-            # SEG, cutoffs and lists on the device (gzb_engine_set_protein_queries)
             eng.set_protein_queries(p_codes, p_offs, p_lens, stream=stream)
-            qq = None
         else:
-            qq = prepare()
-            eng.set_queries(qq, stream)
+            eng.set_translated_queries(p_dna, p_roffs, stream=stream)
         eng.presearch(schedule, stream)
         N.check(L.gzb_engine_build_alignments(eng.h, ctypes.c_void_p(counts_pin.data_ptr()),
                                               ctypes.c_void_p(al_pin.data_ptr()),
                                               ctypes.c_void_p(stream.cuda_stream)))
-        return qq
 
     for _ in range(args.warmup):
-        qq = e2e_step()
+        e2e_step()
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -1181,16 +1175,9 @@ def main():
     e1.record(stream)
     barrier()
     e2e_ms = e0.elapsed_time(e1)
-    if protein_on_device:
-        # raw queries in; cutoffs and triggers, counts and records back
-        h2d = raw_bytes
-        d2h = 8 * q.number + counts_pin.numel() + al_pin.numel()
-    else:
-        prepared_bytes = sum(getattr(qq, n).nbytes
-                             for n in ("codes", "offsets", "lengths", "cutoffs", "triggers"))
-        h2d = raw_bytes + prepared_bytes
-        d2h = (qq.codes.nbytes + qq.cutoffs.nbytes + qq.triggers.nbytes + counts_pin.numel()
-               + al_pin.numel())
+    # raw queries in; cutoffs and triggers, counts and records back
+    h2d = raw_bytes
+    d2h = 8 * q.number + counts_pin.numel() + al_pin.numel()
     # the e2e alignment records must equal the device loop's
     got = np.frombuffer(al_pin.numpy().tobytes(), dtype=N.ALIGNMENT_DTYPE).reshape(q.number, b)
     cnt = np.frombuffer(counts_pin.numpy().tobytes(), dtype=np.uint32)
@@ -1302,8 +1289,9 @@ def main():
                          "gzb_engine_set_protein_queries (SEG, cutoffs and hash lists on the "
                          "device) -> presearch -> build results -> alignment records "
                          "(no text formatting)" if protein_on_device else
-                         "raw reads from pinned host memory -> translation + SEG + cutoffs "
-                         "-> upload + hash lists -> presearch -> build results -> "
+                         "raw reads from pinned host memory -> "
+                         "gzb_engine_set_translated_queries (translation, SEG, cutoffs and "
+                         "hash lists on the device) -> presearch -> build results -> "
                          "alignment records (no text formatting)")},
         "dp_gcups": {"gapped_stage": gcups_stage, "whole_step": gcups_step},
         "dp_int_pipe": dp_int_pipe(gcups_stage, clocks),

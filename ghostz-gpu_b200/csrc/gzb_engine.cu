@@ -2353,6 +2353,91 @@ extern "C" int gzb_engine_set_protein_queries(gzb_engine *e, const uint8_t *code
   return build_query_lists(e, length, number_queries, s);
 }
 
+extern "C" int gzb_engine_set_translated_queries(gzb_engine *e, const uint8_t *dna,
+                                                 const uint64_t *read_offsets,
+                                                 uint32_t number_reads, int filter,
+                                                 float ungapped_bits, float trigger_bits,
+                                                 int32_t *cutoffs, int32_t *triggers,
+                                                 void *stream) {
+  GZB_TRY(check_engine(e));
+  GZB_CHECK(e->have_params, GZB_ERR_INVALID, "set_params first");
+  GZB_CHECK(dna && read_offsets && number_reads > 0, GZB_ERR_INVALID, "empty read set");
+  cudaStream_t s = (cudaStream_t)stream;
+  e->have_queries = false;
+  // the shared-delimiter layout of the six-frame queries
+  const uint32_t n = number_reads;
+  std::vector<uint32_t> read_len(n), qoff(n), qlen(n);
+  std::vector<uint64_t> qoff64(n);
+  uint64_t total = 1, maxl = 0;
+  for (uint32_t r = 0; r < n; ++r) {
+    GZB_CHECK(read_offsets[r + 1] >= read_offsets[r] &&
+                  read_offsets[r + 1] - read_offsets[r] <= 0xFFFFFFFFull,
+              GZB_ERR_INVALID, "read %u: offsets must be non-decreasing", r);
+    read_len[r] = (uint32_t)(read_offsets[r + 1] - read_offsets[r]);
+    const uint64_t ql = gzb_translated_query_length(read_len[r]);
+    qoff64[r] = total - 1;
+    total += ql - 1;
+    GZB_CHECK(total < (1ull << 31), GZB_ERR_OVERFLOW,
+              "translated queries exceed 2^31 codes");
+    qoff[r] = (uint32_t)qoff64[r];
+    qlen[r] = (uint32_t)ql;
+    maxl = std::max<uint64_t>(maxl, ql);
+  }
+  const uint64_t bases = read_offsets[n] - read_offsets[0];
+  e->nq = n;
+  e->q_len = total;
+  e->max_qlen = (uint32_t)maxl;
+  const uint8_t delim = (uint8_t)e->params.delimiter;
+  GZB_TRY(e->q_buf.ensure(total + 2 * kPad));
+  GZB_TRY(e->codeflag.ensure(16));
+  GZB_CUDA(cudaMemsetAsync(e->q_buf.p, delim, total + 2 * kPad, s));
+  GZB_CUDA(cudaMemsetAsync(e->codeflag.p, 0, 16, s));
+  // reads and their offsets (relative to the first read) after the layout
+  const uint64_t at_len = ((bases + 15) / 16) * 16, at_off = at_len + ((4ull * n + 15) / 16) * 16;
+  GZB_TRY(e->q_prep.ensure(at_off + 8ull * n + 16));
+  uint8_t *base = e->q_prep.as<uint8_t>();
+  std::vector<uint64_t> roff(n);
+  for (uint32_t r = 0; r < n; ++r) roff[r] = read_offsets[r] - read_offsets[0];
+  if (bases)
+    GZB_CUDA(cudaMemcpyAsync(base, dna + read_offsets[0], bases, cudaMemcpyHostToDevice, s));
+  GZB_CUDA(cudaMemcpyAsync(base + at_len, read_len.data(), 4ull * n, cudaMemcpyHostToDevice, s));
+  GZB_CUDA(cudaMemcpyAsync(base + at_off, roff.data(), 8ull * n, cudaMemcpyHostToDevice, s));
+  GZB_TRY(upload(e->q_offsets, qoff.data(), n, s));
+  GZB_TRY(upload(e->q_lengths, qlen.data(), n, s));
+  GZB_TRY(upload(e->q_off64, qoff64.data(), n, s));
+  GZB_TRY(e->q_cut.ensure(4 * (uint64_t)n));
+  GZB_TRY(e->q_trig.ensure(4 * (uint64_t)n));
+  uint8_t *q = e->q_buf.as<uint8_t>() + kPad;
+  const uint32_t *d_read_len = reinterpret_cast<const uint32_t *>(base + at_len);
+  unsigned int *flags = e->codeflag.as<unsigned int>();  // codes, SEG status, cutoffs
+  GZB_TRY(gzb_translate_dna_queries(base, reinterpret_cast<const uint64_t *>(base + at_off),
+                                    d_read_len, n, e->q_off64.as<uint64_t>(), delim, q, s));
+  if (filter)
+    GZB_TRY(gzb_seg_translated_queries(q, e->q_off64.as<uint64_t>(), d_read_len, n, flags + 1,
+                                       s));
+  code_range_kernel<<<grid1(total / 16 + 1, 256), 256, 0, s>>>(q, total, flags);
+  GZB_CUDA(cudaGetLastError());
+  GZB_TRY(gzb_query_karlin_cutoffs(q, e->q_off64.as<uint64_t>(), e->q_lengths.as<uint32_t>(), n,
+                                   e->params.score_matrix, (uint32_t)e->params.number_letters,
+                                   ungapped_bits, trigger_bits, e->q_cut.as<int32_t>(),
+                                   e->q_trig.as<int32_t>(), nullptr, s));
+  cutoff_range_kernel<<<grid1(n, 256), 256, 0, s>>>(e->q_cut.as<int32_t>(),
+                                                      e->q_trig.as<int32_t>(), n, flags + 2);
+  GZB_CUDA(cudaGetLastError());
+  if (cutoffs)
+    GZB_CUDA(cudaMemcpyAsync(cutoffs, e->q_cut.p, 4ull * n, cudaMemcpyDeviceToHost, s));
+  if (triggers)
+    GZB_CUDA(cudaMemcpyAsync(triggers, e->q_trig.p, 4ull * n, cudaMemcpyDeviceToHost, s));
+  unsigned int bad[3] = {0, 0, 0};
+  GZB_CUDA(cudaMemcpyAsync(bad, flags, 12, cudaMemcpyDeviceToHost, s));
+  GZB_CUDA(cudaStreamSynchronize(s));
+  GZB_CHECK(bad[0] == 0, GZB_ERR_INVALID, "residue codes must be below 32");
+  GZB_CHECK(bad[1] == 0, GZB_ERR_INVALID, "SEG left %u frames unmasked", bad[1]);
+  GZB_CHECK(bad[2] == 0, GZB_ERR_INVALID,
+            "a query's cutoff is outside 1..32767 or its trigger outside int16");
+  return build_query_lists(e, total, n, s);
+}
+
 extern "C" int gzb_engine_reset_results(gzb_engine *e, void *stream) {
   GZB_TRY(check_engine(e));
   GZB_CHECK(e->have_queries, GZB_ERR_INVALID, "no queries");

@@ -103,6 +103,8 @@ def _declare(L):
         "gzb_engine_set_queries": [V, V, C.c_uint64, V, V, U32, V, V, V],
         "gzb_engine_set_protein_queries": [V, V, C.c_uint64, V, V, U32, C.c_int, C.c_float,
                                            C.c_float, V, V, V],
+        "gzb_engine_set_translated_queries": [V, V, V, U32, C.c_int, C.c_float, C.c_float, V,
+                                              V, V],
         "gzb_engine_presearch": [V, C.c_int, V],
         "gzb_engine_reset_results": [V, V],
         "gzb_engine_get_results": [V, V, V, V],
@@ -495,6 +497,22 @@ class PresearchEngine:
             self.h, hptr(codes), len(codes), hptr(offs), hptr(lens), n, 1 if filter else 0,
             float(ungapped_bits), float(trigger_bits), hptr(cut), hptr(trig),
             _stream_or_null(stream)))
+        self.number_queries = n
+        return cut, trig
+
+    def set_translated_queries(self, dna, offsets, filter=True, ungapped_bits=7.0,
+                               trigger_bits=22.0, stream=None):
+        """Reads (ASCII bases back to back, number_reads + 1 offsets)
+        translated, SEG-masked (filter) and given their cutoffs on the device
+        and set as the query set (gzb_engine_set_translated_queries).
+        Returns the (cutoffs, triggers) host arrays."""
+        dna = np.ascontiguousarray(dna, dtype=np.uint8)
+        offs = np.ascontiguousarray(offsets, dtype=np.uint64)
+        n = len(offs) - 1
+        cut, trig = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        check(lib().gzb_engine_set_translated_queries(
+            self.h, hptr(dna), hptr(offs), n, 1 if filter else 0, float(ungapped_bits),
+            float(trigger_bits), hptr(cut), hptr(trig), _stream_or_null(stream)))
         self.number_queries = n
         return cut, trig
 

@@ -359,6 +359,19 @@ int gzb_engine_set_protein_queries(gzb_engine *e, const uint8_t *codes, uint64_t
                                    uint32_t number_queries, int filter, float ungapped_bits,
                                    float trigger_bits, int32_t *cutoffs, int32_t *triggers,
                                    void *stream);
+/* The same for translated searches (-q d): number_reads reads of ASCII
+ * bases, read r = dna[read_offsets[r] .. read_offsets[r + 1]) (host), are
+ * uploaded, translated in six frames into the engine's shared-delimiter
+ * layout (query r at the offset the reads before it take,
+ * gzb_translated_query_length(read length) codes), SEG-masked per frame
+ * when filter is non-zero, given their cutoffs and their hash lists.
+ * Replaces Queries::BuildQuery with TranslatedDnaQuery
+ * (src/translated_dna_query.cpp:44-74) and AlignerGpu::SetQueriesData.
+ * Synchronises `stream`. */
+int gzb_engine_set_translated_queries(gzb_engine *e, const uint8_t *dna,
+                                      const uint64_t *read_offsets, uint32_t number_reads,
+                                      int filter, float ungapped_bits, float trigger_bits,
+                                      int32_t *cutoffs, int32_t *triggers, void *stream);
 /* Runs the presearch of the resident queries against the resident chunk
  * and merges into the per-query top-b lists kept on the device.  Call
  * gzb_engine_reset_results before the first chunk of a query set. */

@@ -167,3 +167,42 @@ def test_engine_prepares_protein_queries_on_device(native, oracle, params, filte
                 assert np.array_equal(res_b[i], exp[i]), i
     finally:
         e.close()
+
+
+@pytest.mark.parametrize("filter_", [True, False])
+def test_engine_prepares_translated_queries_on_device(native, oracle, params, filter_):
+    """gzb_engine_set_translated_queries (translation, SEG, cutoffs and hash
+    lists on the device) gives the cutoffs, lists and presearch results of
+    prepare_translated_queries + set_queries, on reads with N, lower case,
+    short reads and tandem repeats mixed into reads of the database."""
+    rng = np.random.default_rng(95)
+    db = W.make_database(1200, 97, median=250)
+    reads = W.make_reads(db, 120, 98)
+    extra, extra_dna, extra_off = _reads(rng, 40)
+    dna = np.concatenate([reads.dna, extra_dna]).astype(np.uint8)
+    offsets = np.concatenate([reads.offsets, reads.offsets[-1] + extra_off[1:]]).astype(np.uint64)
+    codes, offs, lens, cut, trig = native.prepare_translated_queries(dna, offsets,
+                                                                     filter=filter_)
+    ref = W.translated_queries(codes, offs, lens, cutoffs=(cut, trig))
+    e = native.PresearchEngine(0)
+    try:
+        e.set_params(params)
+        e.set_database(db)
+        e.set_queries(ref)
+        lists_a = e.list_arrays()
+        e.reset_results()
+        e.presearch(native.SCHEDULE_BATCHED)
+        res_a = e.results()
+        cut_b, trig_b = e.set_translated_queries(dna, offsets, filter=filter_)
+        assert np.array_equal(cut_b, cut) and np.array_equal(trig_b, trig)
+        lists_b = e.list_arrays()
+        for name in lists_a:
+            assert np.array_equal(lists_a[name], lists_b[name]), name
+        e.reset_results()
+        e.presearch(native.SCHEDULE_BATCHED)
+        res_b = e.results()
+        assert sum(len(r) for r in res_a) > 0
+        for i in range(ref.number):
+            assert np.array_equal(res_a[i], res_b[i]), i
+    finally:
+        e.close()
