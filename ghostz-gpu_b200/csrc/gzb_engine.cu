@@ -1331,8 +1331,8 @@ struct gzb_engine {
   uint64_t db_check = 0;     // of the resident chunk (index cache key)
   // build results step
   DBuf tb_redo;
-  DBuf tb_cols, tb_band_off, tb_band, tb_ops_bytes, tb_ops_off, tb_rows, tb_rows_off, tb_walk_cap,
-      tb_walk_off, tb_ops, tb_row_meta, tb_walk, tb_walk_n, tb_score, tb_p0, tb_p1, tb_out;
+  DBuf tb_cols, tb_band_off, tb_band, tb_ops_bytes, tb_ops_off, tb_rows, tb_rows_off, tb_ops,
+      tb_row_meta, tb_score, tb_p0, tb_p1, tb_out, tb_stats, tb_scratch;
   uint64_t pred_n = 0;       // extensions with a prediction in epred (last run)
   DBuf enb;                  // per surviving hit: chained neighbours (cost feature)
   int tile[3][kTileParameters] = {
@@ -1585,8 +1585,8 @@ extern "C" int gzb_engine_destroy(gzb_engine *e) {
                  &e->log_ctr, &e->enb, &e->codeflag, &e->tb_cols, &e->tb_band_off,
                  &e->tb_redo,
                  &e->tb_band, &e->tb_ops_bytes, &e->tb_ops_off, &e->tb_rows, &e->tb_rows_off,
-                 &e->tb_walk_cap, &e->tb_walk_off, &e->tb_ops, &e->tb_row_meta, &e->tb_walk,
-                 &e->tb_walk_n, &e->tb_score, &e->tb_p0, &e->tb_p1, &e->tb_out};
+                 &e->tb_ops, &e->tb_row_meta, &e->tb_score, &e->tb_p0, &e->tb_p1, &e->tb_out, &e->tb_stats,
+                 &e->tb_scratch};
   for (DBuf *b : all) b->release();
   for (auto &g : e->graphs) cudaGraphExecDestroy(g.exec);
   e->graphs.clear();
@@ -3256,13 +3256,13 @@ int scan_total(gzb_engine *e, DBuf &in, DBuf &out, uint64_t n, cudaStream_t s,
   return GZB_OK;
 }
 
-// the three scans of the build step's pass-1 sizes with one host wait
-int scan_totals3(gzb_engine *e, uint64_t n, cudaStream_t s, uint64_t *ops_total,
-                 uint64_t *rows_total, uint64_t *walk_total) {
-  DBuf *in[3] = {&e->tb_ops_bytes, &e->tb_rows, &e->tb_walk_cap};
-  DBuf *out[3] = {&e->tb_ops_off, &e->tb_rows_off, &e->tb_walk_off};
-  uint64_t *total[3] = {ops_total, rows_total, walk_total};
-  for (int k = 0; k < 3; ++k) {
+// the two scans of the flagged sides' storage sizes with one host wait
+int scan_totals2(gzb_engine *e, uint64_t n, cudaStream_t s, uint64_t *ops_total,
+                 uint64_t *rows_total) {
+  DBuf *in[2] = {&e->tb_ops_bytes, &e->tb_rows};
+  DBuf *out[2] = {&e->tb_ops_off, &e->tb_rows_off};
+  uint64_t *total[2] = {ops_total, rows_total};
+  for (int k = 0; k < 2; ++k) {
     GZB_TRY(out[k]->ensure(8 * (n + 1)));
     GZB_CUDA(cudaMemsetAsync(in[k]->as<uint64_t>() + n, 0, 8, s));
     GZB_TRY(exclusive_sum(e, in[k]->as<uint64_t>(), out[k]->as<uint64_t>(), n + 1, s));
@@ -3298,55 +3298,57 @@ extern "C" int gzb_engine_build_alignments(gzb_engine *e, uint32_t *counts,
   a.gap_ext = e->params.gap_extension;
   // the build results step's own X-drop (src/aligner_gpu.cpp:254-256)
   a.cutoff = e->params.result_gapped_cutoff;
-  // band columns per side, then the DP's storage per side
+  GZB_TRY(e->tb_ops_bytes.ensure(8 * (n_sides + 1)));
+  GZB_TRY(e->tb_rows.ensure(8 * (n_sides + 1)));
+  GZB_TRY(e->tb_redo.ensure(n_sides + 1));
+  GZB_TRY(e->tb_score.ensure(4 * (n_sides + 1)));
+  GZB_TRY(e->tb_p0.ensure(4 * (n_sides + 1)));
+  GZB_TRY(e->tb_p1.ensure(4 * (n_sides + 1)));
+  GZB_TRY(e->tb_stats.ensure(sizeof(TbStats) * (n_sides + 1)));
+  GZB_TRY(e->tb_out.ensure(sizeof(gzb_alignment) * (n_slots + 1)));
+  // one DP pass by warps (each gathering sides' ops and rows in its own
+  // scratch, then walking them); the sides a warp cannot run go to the
+  // thread kernels
+  int sms = 148, per_sm = 1;
+  GZB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device));
+  GZB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tb_side_warp_kernel,
+                                                         kTbWarpBlock, 0));
+  const uint64_t want = (n_sides + kTbWarpBlock / 32 - 1) / (kTbWarpBlock / 32);
+  const uint64_t blocks = std::max<uint64_t>(
+      1, std::min<uint64_t>(want, (uint64_t)sms * std::max(per_sm, 1)));
+  GZB_TRY(e->tb_scratch.ensure(blocks * (kTbWarpBlock / 32) * kTbScratchBytes));
+  tb_side_warp_kernel<<<(unsigned)blocks, kTbWarpBlock, 0, s>>>(
+      a, n_sides, e->tb_scratch.as<uint8_t>(), e->tb_score.as<int32_t>(),
+      e->tb_p0.as<int32_t>(), e->tb_p1.as<int32_t>(), e->tb_stats.as<TbStats>(),
+      e->tb_ops_bytes.as<uint64_t>(), e->tb_rows.as<uint64_t>(), e->tb_redo.as<uint8_t>());
+  GZB_CUDA(cudaGetLastError());
+  // the flagged sides' bands (global memory) and storage sizes
   GZB_TRY(e->tb_cols.ensure(8 * (n_sides + 1)));
-  tb_band_kernel<<<grid1(n_sides, 256), 256, 0, s>>>(a, n_sides, e->tb_cols.as<uint64_t>());
+  tb_band_kernel<<<grid1(n_sides, 256), 256, 0, s>>>(a, n_sides, e->tb_redo.as<uint8_t>(),
+                                                     e->tb_cols.as<uint64_t>());
   GZB_CUDA(cudaGetLastError());
   uint64_t band_total = 0;
   GZB_TRY(scan_total(e, e->tb_cols, e->tb_band_off, n_sides, s, &band_total));
   GZB_TRY(e->tb_band.ensure(sizeof(int2) * (band_total + 1)));
-  GZB_TRY(e->tb_ops_bytes.ensure(8 * (n_sides + 1)));
-  GZB_TRY(e->tb_rows.ensure(8 * (n_sides + 1)));
-  GZB_TRY(e->tb_walk_cap.ensure(8 * (n_sides + 1)));
-  GZB_TRY(e->tb_redo.ensure(n_sides + 1));
-  // pass 1 by warps; the sides a warp cannot run, by threads
-  tb_count_warp_kernel<<<grid1(32 * n_sides, kTbWarpBlock), kTbWarpBlock, 0, s>>>(
-      a, n_sides, e->tb_ops_bytes.as<uint64_t>(), e->tb_rows.as<uint64_t>(),
-      e->tb_walk_cap.as<uint64_t>(), e->tb_redo.as<uint8_t>());
-  GZB_CUDA(cudaGetLastError());
   tb_count_kernel<<<grid1(n_sides, 128), 128, 0, s>>>(
       a, n_sides, e->tb_band_off.as<uint64_t>(), e->tb_band.as<int2>(),
-      e->tb_ops_bytes.as<uint64_t>(), e->tb_rows.as<uint64_t>(), e->tb_walk_cap.as<uint64_t>(),
-      e->tb_redo.as<uint8_t>());
+      e->tb_ops_bytes.as<uint64_t>(), e->tb_rows.as<uint64_t>(), e->tb_redo.as<uint8_t>());
   GZB_CUDA(cudaGetLastError());
-  uint64_t ops_total = 0, rows_total = 0, walk_total = 0;
-  GZB_TRY(scan_totals3(e, n_sides, s, &ops_total, &rows_total, &walk_total));
+  uint64_t ops_total = 0, rows_total = 0;
+  GZB_TRY(scan_totals2(e, n_sides, s, &ops_total, &rows_total));
   GZB_TRY(e->tb_ops.ensure(ops_total + 1));
   GZB_TRY(e->tb_row_meta.ensure(8 * (rows_total + 1)));
-  GZB_TRY(e->tb_walk.ensure(walk_total + 1));
-  GZB_TRY(e->tb_walk_n.ensure(4 * (n_sides + 1)));
-  GZB_TRY(e->tb_score.ensure(4 * (n_sides + 1)));
-  GZB_TRY(e->tb_p0.ensure(4 * (n_sides + 1)));
-  GZB_TRY(e->tb_p1.ensure(4 * (n_sides + 1)));
-  GZB_TRY(e->tb_out.ensure(sizeof(gzb_alignment) * (n_slots + 1)));
-  // a cell the DP prunes keeps op 0, as in a fresh GappedExtender
+  // a cell the thread DP prunes keeps op 0, as in a fresh GappedExtender
   GZB_CUDA(cudaMemsetAsync(e->tb_ops.p, 0, ops_total + 1, s));
-  tb_store_warp_kernel<<<grid1(32 * n_sides, kTbWarpBlock), kTbWarpBlock, 0, s>>>(
-      a, n_sides, e->tb_ops_off.as<uint64_t>(), e->tb_ops.as<uint8_t>(),
-      e->tb_rows_off.as<uint64_t>(), e->tb_row_meta.as<uint32_t>(), e->tb_score.as<int32_t>(),
-      e->tb_p0.as<int32_t>(), e->tb_p1.as<int32_t>(), e->tb_redo.as<uint8_t>());
-  GZB_CUDA(cudaGetLastError());
   tb_walk_kernel<<<grid1(n_sides, 128), 128, 0, s>>>(
       a, n_sides, e->tb_band_off.as<uint64_t>(), e->tb_band.as<int2>(),
       e->tb_ops_off.as<uint64_t>(), e->tb_ops.as<uint8_t>(), e->tb_rows_off.as<uint64_t>(),
-      e->tb_row_meta.as<uint32_t>(), e->tb_walk_off.as<uint64_t>(), e->tb_walk.as<uint8_t>(),
-      e->tb_walk_n.as<uint32_t>(), e->tb_score.as<int32_t>(), e->tb_p0.as<int32_t>(),
-      e->tb_p1.as<int32_t>(), e->tb_redo.as<uint8_t>());
+      e->tb_row_meta.as<uint32_t>(), e->tb_score.as<int32_t>(), e->tb_p0.as<int32_t>(),
+      e->tb_p1.as<int32_t>(), e->tb_stats.as<TbStats>(), e->tb_redo.as<uint8_t>());
   GZB_CUDA(cudaGetLastError());
   tb_combine_kernel<<<grid1(n_slots, 128), 128, 0, s>>>(
-      a, n_slots, e->tb_walk_off.as<uint64_t>(), e->tb_walk.as<uint8_t>(),
-      e->tb_walk_n.as<uint32_t>(), e->tb_score.as<int32_t>(), e->tb_p0.as<int32_t>(),
-      e->tb_p1.as<int32_t>(), e->tb_out.as<gzb_alignment>());
+      a, n_slots, e->tb_score.as<int32_t>(), e->tb_p0.as<int32_t>(), e->tb_p1.as<int32_t>(),
+      e->tb_stats.as<TbStats>(), e->tb_out.as<gzb_alignment>());
   GZB_CUDA(cudaGetLastError());
   GZB_CUDA(cudaMemcpyAsync(counts, e->counts.p, 4 * (uint64_t)e->nq, cudaMemcpyDeviceToHost, s));
   GZB_CUDA(cudaMemcpyAsync(alignments, e->tb_out.p, sizeof(gzb_alignment) * n_slots,

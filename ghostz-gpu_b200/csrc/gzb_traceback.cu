@@ -4,21 +4,23 @@
 // AlignerCommon::BuildResult reports (alignment length, mismatches, gap
 // openings and extensions).
 //
-// Pass 1 runs the DP to size each side's op storage; pass 2 runs it again
-// storing one op byte per kept cell, row by row; then each side's optimal
-// path is walked back from the best cell (PickOptimalPath); a last kernel
-// joins the two sides per result in the reference's order.
+// One warp per side runs the DP once, storing one op byte per cell row by
+// row in the warp's own scratch (so no pass sizes the storage first),
+// walks the optimal path back from the best cell (PickOptimalPath) and
+// counts what BuildResult counts over it; a last kernel joins the two sides
+// of each result in the reference's order.
 //
-// Both DP passes give one warp to a side: the warp evaluates 32 consecutive
-// columns of a row at once, with the presearch's warp DP
-// (gapped_extend_warp in gzb_kernels.cuh: band edges and stored values
-// exact for X-drops below 1024).  A kept cell's edit op also needs the
-// reference's horizontal-gap value *with* its reset to kInitScore at pruned
-// cells (src/gapped_extender.cpp:428-446); once a chunk's pruned flags are
-// known that value is a segmented max-plus scan whose segments start after
-// the pruned cells.  Sides whose band outgrows the warp's circular buffer,
-// or whose X-drop is 1024 or more, are flagged and run by one thread each
-// with the band in global memory (the serial form of the same DP).
+// The warp evaluates 32 consecutive columns of a row at once, with the
+// presearch's warp DP (gapped_extend_warp in gzb_kernels.cuh: band edges and
+// stored values exact for X-drops below 1024).  A kept cell's edit op also
+// needs the reference's horizontal-gap value *with* its reset to
+// kInitScore at pruned cells (src/gapped_extender.cpp:428-446); once a
+// chunk's pruned flags are known that value is a segmented max-plus scan
+// whose segments start after the pruned cells.  Sides whose band outgrows
+// the warp's circular buffer, whose storage outgrows the warp's scratch, or
+// whose X-drop is 1024 or more are flagged and run by one thread each: a
+// pass to size their storage, then the DP with the band in global memory
+// (the serial form of the same DP), the walk and the counts.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -202,12 +204,18 @@ constexpr int kTbWarpsPerBlock = 8;
 static_assert(kTbWarpBlock == kTbWarpsPerBlock * 32, "launch block of the warp kernels");
 
 // tb_extend by one warp (lanes must all call it with the same side); with
-// STORE it also writes the ops and row table as tb_extend does.  Returns
-// false when the band outgrows kTbWarpColumns (outputs then meaningless).
+// STORE it also writes the ops and row table as tb_extend does, into
+// storage of ops_cap bytes and rows_cap rows that need not be zeroed: every
+// byte of a row's range is written (0 for a pruned cell and the sentinel,
+// as a fresh GappedExtender holds), and the bytes past the last row up to
+// *ops_bytes are zeroed at the end.  Returns false when the band outgrows
+// kTbWarpColumns or the side outgrows the storage (outputs then
+// meaningless).
 template <bool STORE>
 __device__ bool tb_extend_warp(const TbArgs &a, const int *sm, const TbSide &t, int2 *band,
-                               uint8_t *ops, uint32_t *row_meta, uint64_t *ops_bytes,
-                               uint32_t *rows, int *best_score, int *best_p0, int *best_p1) {
+                               uint8_t *ops, uint32_t *row_meta, uint64_t ops_cap,
+                               uint32_t rows_cap, uint64_t *ops_bytes, uint32_t *rows,
+                               int *best_score, int *best_p0, int *best_p1) {
   constexpr int W = kTbWarpColumns;
   constexpr int wmask = W - 1;
   constexpr unsigned full = 0xffffffffu;
@@ -253,6 +261,7 @@ __device__ bool tb_extend_warp(const TbArgs &a, const int *sm, const TbSide &t, 
 
   int maxs = 0, mp0 = -inc, mp1 = -inc;
   uint64_t used = 0;
+  uint64_t written = 0;  // end of the bytes the rows wrote
   uint32_t r = 0;
   for (;; ++r) {
     const int x = d0[(int)r * inc];
@@ -261,6 +270,10 @@ __device__ bool tb_extend_warp(const TbArgs &a, const int *sm, const TbSide &t, 
     const int row_start = bs;
     uint8_t *row_ops = nullptr;
     if (STORE) {
+      // a row's storage runs from its first band column to the next row's
+      // band end: at most 2 W + 1 columns (the band, W wide, may move right
+      // by up to W within the row), and the sentinel
+      if (used + 2 * W + 2 > ops_cap || r >= rows_cap) return false;
       if (lane == 0) {
         row_meta[2 * r] = (uint32_t)used;
         row_meta[2 * r + 1] = (uint32_t)row_start;
@@ -336,6 +349,7 @@ __device__ bool tb_extend_warp(const TbArgs &a, const int *sm, const TbSide &t, 
         }
         int Nin = __shfl_up_sync(full, v, 1);
         if (lane == 0) Nin = Fs;
+        if (active && pruned) row_ops[c] = 0;
         if (active && !pruned) {
           const int Fb = Nin - lane * ge;
           int op = kTbSub, sc = sd;
@@ -374,6 +388,7 @@ __device__ bool tb_extend_warp(const TbArgs &a, const int *sm, const TbSide &t, 
     }
     __syncwarp();
     if (first_kept < 0) {  // every cell pruned: array_start + 1 == array_end
+      written = used + (uint64_t)(be - row_start);
       ++r;
       break;
     }
@@ -408,13 +423,23 @@ __device__ bool tb_extend_warp(const TbArgs &a, const int *sm, const TbSide &t, 
     }
     if (edge_residue) {
       if (be + 1 - bs > W) return false;
-      if (lane == 0) band[be & wmask] = make_int2(kInitScore, kInitScore);
+      if (lane == 0) {
+        band[be & wmask] = make_int2(kInitScore, kInitScore);
+        if (STORE) row_ops[be] = 0;  // the sentinel
+      }
       ++be;
     }
     used += (uint64_t)(be - row_start);
+    written = used;
     __syncwarp();
   }
   *ops_bytes = used + (uint64_t)(t.len0 + 2);
+  if (STORE) {
+    // past the rows: zeros up to the storage the reference would keep
+    if (*ops_bytes > ops_cap) return false;
+    for (uint64_t j = written + lane; j < *ops_bytes; j += 32) ops[j] = 0;
+    __syncwarp();
+  }
   *rows = r;
   *best_score = maxs;
   *best_p0 = mp0;
@@ -424,82 +449,188 @@ __device__ bool tb_extend_warp(const TbArgs &a, const int *sm, const TbSide &t, 
 
 }  // namespace
 
-// pass 1 by one warp per side; a side the warp cannot run exactly is
-// flagged in `redo` for tb_count_kernel
-__global__ void __launch_bounds__(kTbWarpsPerBlock * 32)
-    tb_count_warp_kernel(TbArgs a, uint64_t n_sides, uint64_t *ops_bytes, uint64_t *rows,
-                         uint64_t *walk_cap, uint8_t *redo) {
+// Where BuildResult starts counting a side (src/aligner_build_results_thread.h:
+// 110-160, src/aligner_common.h:275-340): the reverse side from the
+// alignment start, the forward side from the hit.
+__device__ __forceinline__ void tb_count_start(const TbArgs &a, uint64_t side, int p0, int p1,
+                                               const uint8_t **qs, uint32_t *qp, uint32_t *dp) {
+  const uint64_t slot = side >> 1;
+  const uint32_t qi = (uint32_t)(slot / (uint64_t)a.max_results);
+  const gzb_result r = a.results[slot];
+  *qs = a.query + a.q_offsets[qi];
+  if (side & 1) {
+    *qp = r.hit_q;
+    *dp = r.hit_d;
+  } else {
+    *qp = r.hit_q - 1 + (uint32_t)p0;
+    *dp = r.hit_d - 1 + (uint32_t)p1;
+  }
+}
+
+// PickOptimalPath (src/gapped_extender.cpp:473-531) from the best cell (p0,
+// p1 in side coordinates) back to the origin, and BuildResult's counts over
+// the path as AlignerBuildResultsThread::Run hands it over: the ops taken in
+// reverse walk order, positions advancing from (qp, dp).  Op k of the walk
+// is taken after the walk's later ops, so its positions are (qp, dp) plus
+// the advances of the ops after it: the whole side's advance (p0 + 1 along
+// the query, p1 + 1 along the database) less those of ops 0..k.  Row rr's
+// op of column c sits at ops[meta[2 rr] + c - meta[2 rr + 1]]; a column
+// left of the side's first row reads as 0, the byte the reference keeps
+// before it.  Gap runs count as if the side followed a substitution.
+__device__ TbStats tb_walk_stats(const uint8_t *ops, const uint32_t *meta, int inc, int p0,
+                                 int p1, const uint8_t *qs, const uint8_t *db, uint32_t qp,
+                                 uint32_t dp) {
+  TbStats st;
+  st.n = st.mismatches = st.openings = st.extensions = 0;
+  int rr = p1 * inc, c0 = p0 * inc;
+  const uint32_t qend = qp + (uint32_t)(c0 + 1), dend = dp + (uint32_t)(rr + 1);
+  uint32_t qdone = 0, ddone = 0;  // advances of the ops walked so far
+  int op = kTbSub;                // the DP's op state
+  int last = -1;                  // the previous path op
+  // a path op: its mismatch, and the gap count of the op walked before it
+  // (taken right after this one)
+  auto take = [&](int p) {
+    if (p != kPathGap0) ++qdone;
+    if (p != kPathGap1) ++ddone;
+    if (p == kPathSub && qs[qend - qdone] != db[dend - ddone]) ++st.mismatches;
+    if (last == kPathGap0 || last == kPathGap1) {
+      if (p != last) ++st.openings; else ++st.extensions;
+    }
+    if (st.n == 0) st.last = (uint8_t)p;
+    last = p;
+    ++st.n;
+  };
+  while (rr >= 0 && c0 >= 0) {
+    const long long at = (long long)meta[2 * rr] + (c0 + 1) - (long long)meta[2 * rr + 1];
+    const int next = at >= 0 ? ops[at] : 0;
+    if (op == kTbGap0) {
+      op = next & 3;
+      if (next & kTbExt0) op = kTbGap0;
+    } else if (op == kTbGap1) {
+      op = next & 3;
+      if (next & kTbExt1) op = kTbGap1;
+    } else {
+      op = next & 3;
+    }
+    if (op == kTbGap0) {
+      take(kPathGap0);
+      --rr;
+    } else if (op == kTbGap1) {
+      take(kPathGap1);
+      --c0;
+    } else {
+      take(kPathSub);
+      --rr;
+      --c0;
+    }
+  }
+  for (; rr >= 0; --rr) take(kPathGap0);
+  for (; c0 >= 0; --c0) take(kPathGap1);
+  // the op walked last is taken first, after a substitution
+  if (last == kPathGap0 || last == kPathGap1) ++st.openings;
+  st.first = (uint8_t)(st.n ? last : kPathSub);
+  if (st.n == 0) st.last = kPathSub;
+  return st;
+}
+
+// One warp per side runs the DP with its ops and row table into the warp's
+// own scratch (kTbScratchOps bytes, kTbScratchRows rows), where up to 32
+// sides gather; then each lane walks one of them (PickOptimalPath and
+// BuildResult's counts), the 32 walks in parallel, and the scratch is
+// reused.  A side the warp cannot run exactly (X-drop >= 1024, a band wider
+// than kTbWarpColumns) or whose storage outgrows an empty scratch is
+// flagged in `redo` with its sizes left to the thread kernels; the others
+// get zero sizes.
+__global__ void __launch_bounds__(kTbWarpsPerBlock * 32, 4)
+    tb_side_warp_kernel(TbArgs a, uint64_t n_sides, uint8_t *scratch, int32_t *side_score,
+                        int32_t *side_p0, int32_t *side_p1, TbStats *stats, uint64_t *ops_bytes,
+                        uint64_t *rows, uint8_t *redo) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
   __shared__ int2 bands[kTbWarpsPerBlock][kTbWarpColumns];
   load_matrix(sm, a.matrix32, 32, 32);  // the 32 x 32 device matrix
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  uint8_t *mine = scratch + (blockIdx.x * (uint64_t)kTbWarpsPerBlock + warp) * kTbScratchBytes;
+  uint8_t *ops_arena = mine;
+  uint32_t *meta_arena = reinterpret_cast<uint32_t *>(mine + kTbScratchOps);
+  uint64_t ops_pos = 0;
+  uint32_t meta_pos = 0, nacc = 0;
+  // lane i: the i-th gathered side
+  uint64_t my_side = 0, my_ops = 0;
+  uint32_t my_meta = 0;
+  int my_p0 = 0, my_p1 = 0, my_inc = 1;
+  auto flush = [&]() {
+    if ((uint32_t)lane < nacc) {
+      const uint8_t *qs;
+      uint32_t qp, dp;
+      tb_count_start(a, my_side, my_p0, my_p1, &qs, &qp, &dp);
+      stats[my_side] = tb_walk_stats(ops_arena + my_ops, meta_arena + 2 * (uint64_t)my_meta,
+                                     my_inc, my_p0, my_p1, qs, a.db, qp, dp);
+    }
+    __syncwarp();
+    ops_pos = 0;
+    meta_pos = 0;
+    nacc = 0;
+  };
   for (uint64_t s = blockIdx.x * (uint64_t)kTbWarpsPerBlock + warp; s < n_sides;
        s += (uint64_t)gridDim.x * kTbWarpsPerBlock) {
     const TbSide t = side_of(a, s);
-    bool ok = true;
-    uint64_t nb = 0;
-    uint32_t nr = 0;
-    if (t.active) {
-      int sc, p0, p1;
-      ok = a.cutoff < 1024 &&
-           tb_extend_warp<false>(a, sm, t, bands[warp], nullptr, nullptr, &nb, &nr, &sc, &p0,
-                                 &p1);
+    bool ok = !t.active;
+    if (t.active && a.cutoff < 1024) {
+      for (int attempt = 0; attempt < 2 && !ok; ++attempt) {
+        if (attempt == 1) {
+          if (nacc == 0) break;  // outgrows even an empty scratch
+          flush();
+        }
+        uint64_t nb;
+        uint32_t nr;
+        int sc, p0, p1;
+        ok = tb_extend_warp<true>(a, sm, t, bands[warp], ops_arena + ops_pos,
+                                  meta_arena + 2 * (uint64_t)meta_pos, kTbScratchOps - ops_pos,
+                                  kTbScratchRows - meta_pos, &nb, &nr, &sc, &p0, &p1);
+        if (ok) {
+          if ((uint32_t)lane == nacc) {
+            my_side = s;
+            my_ops = ops_pos;
+            my_meta = meta_pos;
+            my_p0 = p0;
+            my_p1 = p1;
+            my_inc = t.inc;
+            side_score[s] = sc;
+            side_p0[s] = p0;
+            side_p1[s] = p1;
+          }
+          ops_pos += nb;
+          meta_pos += nr;
+          if (++nacc == 32) flush();
+        }
+      }
     }
     if (lane == 0) {
       redo[s] = ok ? 0 : 1;
-      ops_bytes[s] = t.active ? nb : 0;
-      rows[s] = t.active ? nr : 0;
-      walk_cap[s] = t.active ? (uint64_t)nr + t.len0 + 2 : 0;
+      ops_bytes[s] = 0;
+      rows[s] = 0;
     }
     __syncwarp();
   }
+  flush();
 }
 
-// pass 2 by one warp per side for the sides pass 1 ran by warp: the DP with
-// its ops and row table, and the side's best score and positions
-__global__ void __launch_bounds__(kTbWarpsPerBlock * 32)
-    tb_store_warp_kernel(TbArgs a, uint64_t n_sides, const uint64_t *ops_off, uint8_t *ops,
-                         const uint64_t *rows_off, uint32_t *row_meta, int32_t *side_score,
-                         int32_t *side_p0, int32_t *side_p1, const uint8_t *redo) {
-  __shared__ int sm[kMatrixStride * kMatrixStride];
-  __shared__ int2 bands[kTbWarpsPerBlock][kTbWarpColumns];
-  load_matrix(sm, a.matrix32, 32, 32);  // the 32 x 32 device matrix
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (uint64_t s = blockIdx.x * (uint64_t)kTbWarpsPerBlock + warp; s < n_sides;
-       s += (uint64_t)gridDim.x * kTbWarpsPerBlock) {
-    if (redo[s]) continue;
-    const TbSide t = side_of(a, s);
-    if (!t.active) continue;
-    uint64_t nb;
-    uint32_t nr;
-    int sc, p0, p1;
-    tb_extend_warp<true>(a, sm, t, bands[warp], ops + ops_off[s], row_meta + 2 * rows_off[s],
-                         &nb, &nr, &sc, &p0, &p1);
-    if (lane == 0) {
-      side_score[s] = sc;
-      side_p0[s] = p0;
-      side_p1[s] = p1;
-    }
-    __syncwarp();
-  }
-}
-
-// per side: band columns (len0 + 2) for the scan
-__global__ void tb_band_kernel(TbArgs a, uint64_t n_sides, uint64_t *band_cols) {
+// per side flagged in `redo`: band columns (len0 + 2) for the scan
+__global__ void tb_band_kernel(TbArgs a, uint64_t n_sides, const uint8_t *redo,
+                               uint64_t *band_cols) {
   for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < n_sides;
        s += (uint64_t)gridDim.x * blockDim.x) {
     const TbSide t = side_of(a, s);
-    band_cols[s] = t.active ? (uint64_t)t.len0 + 2 : 0;
+    band_cols[s] = (t.active && redo[s]) ? (uint64_t)t.len0 + 2 : 0;
   }
 }
 
-// pass 1 by one thread per side for the sides flagged in `redo`, the band in
-// global memory
+// the storage of the sides flagged in `redo` (one thread per side, the band
+// in global memory)
 __global__ void tb_count_kernel(TbArgs a, uint64_t n_sides, const uint64_t *band_off,
                                 int2 *band, uint64_t *ops_bytes, uint64_t *rows,
-                                uint64_t *walk_cap, const uint8_t *redo) {
+                                const uint8_t *redo) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
   load_matrix(sm, a.matrix32, 32, 32);  // the 32 x 32 device matrix
   __syncthreads();
@@ -515,90 +646,48 @@ __global__ void tb_count_kernel(TbArgs a, uint64_t n_sides, const uint64_t *band
     }
     ops_bytes[s] = t.active ? nb : 0;
     rows[s] = t.active ? nr : 0;
-    // the path has at most one op per row plus one per seq0 residue
-    walk_cap[s] = t.active ? (uint64_t)nr + t.len0 + 2 : 0;
   }
 }
 
-// pass 2 for the flagged sides (the DP with its ops by one thread, the band
-// in global memory), then PickOptimalPath (src/gapped_extender.cpp:473-531)
-// for every side; the path is written in walk order (from the best cell
-// back to the origin).
+// The flagged sides by one thread each: the DP with its ops (the band in
+// global memory) into their own storage, then the walk and counts.
 __global__ void tb_walk_kernel(TbArgs a, uint64_t n_sides, const uint64_t *band_off,
                                int2 *band, const uint64_t *ops_off, uint8_t *ops,
-                               const uint64_t *rows_off, uint32_t *row_meta,
-                               const uint64_t *walk_off, uint8_t *walk, uint32_t *walk_n,
-                               int32_t *side_score, int32_t *side_p0, int32_t *side_p1,
+                               const uint64_t *rows_off, uint32_t *row_meta, int32_t *side_score,
+                               int32_t *side_p0, int32_t *side_p1, TbStats *stats,
                                const uint8_t *redo) {
   __shared__ int sm[kMatrixStride * kMatrixStride];
   load_matrix(sm, a.matrix32, 32, 32);  // the 32 x 32 device matrix
   __syncthreads();
   for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < n_sides;
        s += (uint64_t)gridDim.x * blockDim.x) {
+    if (!redo[s]) continue;
     const TbSide t = side_of(a, s);
     if (!t.active) continue;
     uint8_t *sops = ops + ops_off[s];
     uint32_t *meta = row_meta + 2 * rows_off[s];
-    int p0, p1;
-    if (redo[s]) {
-      uint64_t nb;
-      uint32_t nr;
-      int sc;
-      tb_extend(a, sm, t, band + band_off[s], sops, meta, &nb, &nr, &sc, &p0, &p1);
-      side_score[s] = sc;
-      side_p0[s] = p0;
-      side_p1[s] = p1;
-    } else {
-      p0 = side_p0[s];
-      p1 = side_p1[s];
-    }
-    uint8_t *path = walk + walk_off[s];
-    uint32_t m = 0;
-    {
-      int op = kTbSub;
-      int rr = p1 * t.inc, c0 = p0 * t.inc;
-      while (rr >= 0 && c0 >= 0) {
-        // op of column c0 + 1 of row rr; a column left of the side's first
-        // row reads as 0, the byte the reference keeps before its first row
-        const long long at = (long long)meta[2 * rr] + (c0 + 1) - (long long)meta[2 * rr + 1];
-        const int next = at >= 0 ? sops[at] : 0;
-        if (op == kTbGap0) {
-          op = next & 3;
-          if (next & kTbExt0) op = kTbGap0;
-        } else if (op == kTbGap1) {
-          op = next & 3;
-          if (next & kTbExt1) op = kTbGap1;
-        } else {
-          op = next & 3;
-        }
-        if (op == kTbGap0) {
-          path[m++] = kPathGap0;
-          --rr;
-        } else if (op == kTbGap1) {
-          path[m++] = kPathGap1;
-          --c0;
-        } else {
-          path[m++] = kPathSub;
-          --rr;
-          --c0;
-        }
-      }
-      for (; rr >= 0; --rr) path[m++] = kPathGap0;
-      for (; c0 >= 0; --c0) path[m++] = kPathGap1;
-    }
-    walk_n[s] = m;
+    uint64_t nb;
+    uint32_t nr;
+    int sc, p0, p1;
+    tb_extend(a, sm, t, band + band_off[s], sops, meta, &nb, &nr, &sc, &p0, &p1);
+    side_score[s] = sc;
+    side_p0[s] = p0;
+    side_p1[s] = p1;
+    const uint8_t *qs;
+    uint32_t qp, dp;
+    tb_count_start(a, s, p0, p1, &qs, &qp, &dp);
+    stats[s] = tb_walk_stats(sops, meta, t.inc, p0, p1, qs, a.db, qp, dp);
   }
 }
 
 // Joins the sides of each result as AlignerBuildResultsThread::Run does
-// (src/aligner_build_results_thread.h:110-160): the reverse side's edit
-// blocks reversed, then the forward side's, where both sides' blocks are
-// their paths in walk order reversed; then AlignerCommon::BuildResult
-// (src/aligner_common.h:275-340) counts from the alignment start.
-__global__ void tb_combine_kernel(TbArgs a, uint64_t n_slots, const uint64_t *walk_off,
-                                  const uint8_t *walk, const uint32_t *walk_n,
-                                  const int32_t *side_score, const int32_t *side_p0,
-                                  const int32_t *side_p1, gzb_alignment *out) {
+// (src/aligner_build_results_thread.h:110-160): BuildResult
+// (src/aligner_common.h:275-340) counts the reverse side's ops, then the
+// forward side's, in one run, so a gap run that crosses from one side to
+// the other is one opening.
+__global__ void tb_combine_kernel(TbArgs a, uint64_t n_slots, const int32_t *side_score,
+                                  const int32_t *side_p0, const int32_t *side_p1,
+                                  const TbStats *stats, gzb_alignment *out) {
   for (uint64_t slot = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; slot < n_slots;
        slot += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t qi = (uint32_t)(slot / (uint64_t)a.max_results);
@@ -619,7 +708,6 @@ __global__ void tb_combine_kernel(TbArgs a, uint64_t n_slots, const uint64_t *wa
     o.presearch_score = r.score;
     if (r.chunk_id == a.chunk_id) {
       const uint64_t sr = 2 * slot, sf = 2 * slot + 1;
-      const uint8_t *qs = a.query + a.q_offsets[qi];
       // AlignerBuildResultsThread::Run hands BuildResult the build step's
       // own score, start and end (src/aligner_build_results_thread.h:124-160)
       o.score = side_score[sr] + side_score[sf];
@@ -627,29 +715,14 @@ __global__ void tb_combine_kernel(TbArgs a, uint64_t n_slots, const uint64_t *wa
       o.start_d = r.hit_d - 1 + (uint32_t)side_p1[sr];
       o.end_q = r.hit_q + (uint32_t)side_p0[sf];
       o.end_d = r.hit_d + (uint32_t)side_p1[sf];
-      uint32_t qp = r.hit_q - 1 + (uint32_t)side_p0[sr];
-      uint32_t dp = r.hit_d - 1 + (uint32_t)side_p1[sr];
-      uint32_t mm = 0, op_n = 0, ext_n = 0;
-      int prev = kPathSub;
-      const uint32_t nr = walk_n[sr], nf = walk_n[sf];
-      const uint8_t *pr = walk + walk_off[sr], *pf = walk + walk_off[sf];
-      for (uint32_t i = 0; i < nr + nf; ++i) {
-        const int op = i < nr ? pr[nr - 1 - i] : pf[nr + nf - 1 - i];
-        if (op == kPathSub) {
-          if (qs[qp] != a.db[dp]) ++mm;
-          ++qp;
-          ++dp;
-        } else if (op == kPathGap0) {
-          if (prev != kPathGap0) ++op_n; else ++ext_n;
-          ++dp;
-        } else {
-          if (prev != kPathGap1) ++op_n; else ++ext_n;
-          ++qp;
-        }
-        prev = op;
+      const TbStats rv = stats[sr], fw = stats[sf];
+      uint32_t op_n = rv.openings + fw.openings, ext_n = rv.extensions + fw.extensions;
+      if (rv.n && fw.n && fw.first != kPathSub && fw.first == rv.last) {
+        --op_n;  // the forward side's first gap continues the reverse side's last
+        ++ext_n;
       }
-      o.alignment_length = nr + nf;
-      o.mismatches = mm;
+      o.alignment_length = rv.n + fw.n;
+      o.mismatches = rv.mismatches + fw.mismatches;
       o.gap_openings = op_n;
       o.gap_extensions = ext_n;
     }

@@ -23,27 +23,39 @@ struct TbArgs {
   int delim, gap_open, gap_ext, cutoff;
 };
 
-__global__ void tb_band_kernel(TbArgs a, uint64_t n_sides, uint64_t *band_cols);
-// warps per block of the one-warp-per-side kernels
+// One side's counts for BuildResult, its ops taken in reverse walk order:
+// ops, mismatches, gap openings and extensions (as if the side followed a
+// substitution), and the first and last op taken (kPath* codes).
+struct TbStats {
+  uint32_t n, mismatches, openings, extensions;
+  uint8_t first, last;
+};
+
+// each warp of tb_side_warp_kernel gathers up to 32 sides' ops
+// (kTbScratchOps bytes) and row tables (kTbScratchRows rows) in its own
+// kTbScratchBytes of scratch before walking them
+constexpr uint64_t kTbScratchOps = 256 * 1024;
+constexpr uint32_t kTbScratchRows = 8192;
+constexpr uint64_t kTbScratchBytes = kTbScratchOps + 8ull * kTbScratchRows;
+
+__global__ void tb_band_kernel(TbArgs a, uint64_t n_sides, const uint8_t *redo,
+                               uint64_t *band_cols);
+// warps per block of the one-warp-per-side kernel
 constexpr int kTbWarpBlock = 8 * 32;
-__global__ void tb_count_warp_kernel(TbArgs a, uint64_t n_sides, uint64_t *ops_bytes,
-                                     uint64_t *rows, uint64_t *walk_cap, uint8_t *redo);
+__global__ void tb_side_warp_kernel(TbArgs a, uint64_t n_sides, uint8_t *scratch,
+                                    int32_t *side_score, int32_t *side_p0, int32_t *side_p1,
+                                    TbStats *stats, uint64_t *ops_bytes, uint64_t *rows,
+                                    uint8_t *redo);
 __global__ void tb_count_kernel(TbArgs a, uint64_t n_sides, const uint64_t *band_off,
                                 int2 *band, uint64_t *ops_bytes, uint64_t *rows,
-                                uint64_t *walk_cap, const uint8_t *redo);
-__global__ void tb_store_warp_kernel(TbArgs a, uint64_t n_sides, const uint64_t *ops_off,
-                                     uint8_t *ops, const uint64_t *rows_off, uint32_t *row_meta,
-                                     int32_t *side_score, int32_t *side_p0, int32_t *side_p1,
-                                     const uint8_t *redo);
+                                const uint8_t *redo);
 __global__ void tb_walk_kernel(TbArgs a, uint64_t n_sides, const uint64_t *band_off,
                                int2 *band, const uint64_t *ops_off, uint8_t *ops,
-                               const uint64_t *rows_off, uint32_t *row_meta,
-                               const uint64_t *walk_off, uint8_t *walk, uint32_t *walk_n,
-                               int32_t *side_score, int32_t *side_p0, int32_t *side_p1,
+                               const uint64_t *rows_off, uint32_t *row_meta, int32_t *side_score,
+                               int32_t *side_p0, int32_t *side_p1, TbStats *stats,
                                const uint8_t *redo);
-__global__ void tb_combine_kernel(TbArgs a, uint64_t n_slots, const uint64_t *walk_off,
-                                  const uint8_t *walk, const uint32_t *walk_n,
-                                  const int32_t *side_score, const int32_t *side_p0,
-                                  const int32_t *side_p1, gzb_alignment *out);
+__global__ void tb_combine_kernel(TbArgs a, uint64_t n_slots, const int32_t *side_score,
+                                  const int32_t *side_p0, const int32_t *side_p1,
+                                  const TbStats *stats, gzb_alignment *out);
 
 }  // namespace gzb
