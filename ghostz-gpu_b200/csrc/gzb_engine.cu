@@ -875,7 +875,7 @@ __global__ void build_ext_kernel(const uint64_t *hits, const uint64_t *begin,
                                  uint32_t *ed, uint8_t *dir, uint32_t *elen0,
                                  uint32_t *elen1, uint32_t *eqid, uint32_t *neighbours,
                                  const uint64_t *n_dev, const uint32_t *qprev,
-                                 const uint32_t *qnext) {
+                                 const uint32_t *qnext, int features) {
   if (n_dev) n_surv = *n_dev;
   const uint64_t qmask = (1ull << qbits) - 1, dmask = (1ull << dbits) - 1;
   constexpr uint32_t kReach = 256;  // database residues either side
@@ -908,20 +908,22 @@ __global__ void build_ext_kernel(const uint64_t *hits, const uint64_t *begin,
         }
         neighbours[o + k] = lo - first;
       }
-      const uint32_t sj = subject_of(db_offsets, nseq, db_len, hd);
-      const uint32_t s0 = db_offsets[sj], s1 = db_offsets[sj + 1] - 1;  // residues [s0, s1)
       eq[o + k] = qoff + hq - 1;
       ed[o + k] = hd - 1;
       dir[o + k] = 1;
-      elen0[o + k] = qprev ? (qoff + hq - 1) - qprev[qoff + hq - 1] : hq - 1;
-      elen1[o + k] = hd - s0;
-      eqid[o + k] = qi;
       eq[n_surv + o + k] = qoff + hq;
       ed[n_surv + o + k] = hd;
       dir[n_surv + o + k] = 0;
-      elen0[n_surv + o + k] = qnext ? qnext[qoff + hq] - (qoff + hq) : qlen - 1 - hq;
-      elen1[n_surv + o + k] = s1 - hd;
-      eqid[n_surv + o + k] = qi;
+      if (features) {  // the cost model's inputs (remaining lengths, query)
+        const uint32_t sj = subject_of(db_offsets, nseq, db_len, hd);
+        const uint32_t s0 = db_offsets[sj], s1 = db_offsets[sj + 1] - 1;  // residues [s0, s1)
+        elen0[o + k] = qprev ? (qoff + hq - 1) - qprev[qoff + hq - 1] : hq - 1;
+        elen1[o + k] = hd - s0;
+        eqid[o + k] = qi;
+        elen0[n_surv + o + k] = qnext ? qnext[qoff + hq] - (qoff + hq) : qlen - 1 - hq;
+        elen1[n_surv + o + k] = s1 - hd;
+        eqid[n_surv + o + k] = qi;
+      }
     }
   }
 }
@@ -2620,12 +2622,22 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
   e->last_mae_n = 0;
   e->pred_n = 0;
   if (n_surv) {
+    GappedTile tile = g_tile;
+    for (int w = 0; w < kTileParameters; ++w)
+      if (e->tile[schedule][w] >= 0) *tile_field(tile, w) = e->tile[schedule][w];
+    if (schedule == GZB_SCHEDULE_PLAIN) tile.kernel = GZB_GAPPED_KERNEL_STATIC;
+    const bool learned =
+        schedule == GZB_SCHEDULE_BATCHED && e->have_model && tile.order == GZB_ORDER_MODEL;
+    const bool oracle_order = schedule == GZB_SCHEDULE_ORACLE && e->prev_cells_n == next;
+    const bool scheduled = schedule != GZB_SCHEDULE_PLAIN || e->logging;
+    const bool want_feat = learned || e->logging;
     build_ext_kernel<<<grid1((uint64_t)nq * 32, 256), 256, 0, s>>>(
         hits, begin, kept, surv_off, nq, e->q_offsets.as<uint32_t>(),
         e->q_lengths.as<uint32_t>(), e->db_offsets.as<uint32_t>(), e->nseq, (uint32_t)e->db_len,
         qbits, dbits, n_surv, e->eq.as<uint32_t>(), e->ed.as<uint32_t>(), e->edir.as<uint8_t>(),
         e->elen0.as<uint32_t>(), e->elen1.as<uint32_t>(), e->eqid.as<uint32_t>(),
-        e->enb.as<uint32_t>(), nullptr, e->q_prev.as<uint32_t>(), e->q_next.as<uint32_t>());
+        e->enb.as<uint32_t>(), nullptr, e->q_prev.as<uint32_t>(), e->q_next.as<uint32_t>(),
+        want_feat ? 1 : 0);
     GZB_CUDA(cudaGetLastError());
     ++launches;
     GZB_CUDA(cudaMemsetAsync(e->gcells, 0, 8, s));
@@ -2636,15 +2648,6 @@ int presearch_impl(gzb_engine *e, int schedule, cudaStream_t s) {
     job.gap_open = e->params.gap_open;
     job.gap_ext = e->params.gap_extension;
     job.cutoff = e->params.gapped_cutoff;
-    GappedTile tile = g_tile;
-    for (int w = 0; w < kTileParameters; ++w)
-      if (e->tile[schedule][w] >= 0) *tile_field(tile, w) = e->tile[schedule][w];
-    if (schedule == GZB_SCHEDULE_PLAIN) tile.kernel = GZB_GAPPED_KERNEL_STATIC;
-    const bool learned =
-        schedule == GZB_SCHEDULE_BATCHED && e->have_model && tile.order == GZB_ORDER_MODEL;
-    const bool oracle_order = schedule == GZB_SCHEDULE_ORACLE && e->prev_cells_n == next;
-    const bool scheduled = schedule != GZB_SCHEDULE_PLAIN || e->logging;
-    const bool want_feat = learned || e->logging;
     if (want_feat) {
       GZB_TRY(e->efeat.ensure(4 * kFeat * (next + 1)));
       ext_features_kernel<<<grid1(n_surv, 256), 256, 0, s>>>(
@@ -2990,7 +2993,8 @@ int graph_body(gzb_engine *e, int schedule, const GappedTile &tile, bool learned
       e->q_lengths.as<uint32_t>(), e->db_offsets.as<uint32_t>(), e->nseq, (uint32_t)e->db_len,
       qbits, dbits, c.hits, e->eq.as<uint32_t>(), e->ed.as<uint32_t>(), e->edir.as<uint8_t>(),
       e->elen0.as<uint32_t>(), e->elen1.as<uint32_t>(), e->eqid.as<uint32_t>(),
-      e->enb.as<uint32_t>(), plan + 2, e->q_prev.as<uint32_t>(), e->q_next.as<uint32_t>());
+      e->enb.as<uint32_t>(), plan + 2, e->q_prev.as<uint32_t>(), e->q_next.as<uint32_t>(),
+      learned ? 1 : 0);
   GZB_CUDA(cudaGetLastError());
   ++launches;
   GZB_CUDA(cudaMemsetAsync(e->gcells, 0, 8, s));
