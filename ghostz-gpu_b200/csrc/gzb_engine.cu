@@ -483,7 +483,6 @@ seed_kernel(SeedArgs a) {
         const uint64_t rwin = a.X.rep_windows[r];
         const uint8_t *dptr = a.db + rpos;
         for (uint32_t k = pb; k < pe; ++k) {
-          const uint32_t qid = a.L.entry_qid[k];
           const uint32_t cpos = a.L.entry_cpos[k];
           const uint8_t *qptr = a.q + cpos;
           bool try_rep, pass;
@@ -500,8 +499,11 @@ seed_kernel(SeedArgs a) {
             int steps = 0;
             ++n_seed;
             const uint32_t ct = a.L.entry_ct[k];
-            if (walk_hit(qptr, dptr, tbl, (int)(ct >> 16), (int)(int16_t)(ct & 0xffffu), &steps))
+            if (walk_hit(qptr, dptr, tbl, (int)(ct >> 16), (int)(int16_t)(ct & 0xffffu),
+                         &steps)) {
+              const uint32_t qid = a.L.entry_qid[k];  // only a hit needs its query
               emit_hit(a, qid, rpos, cpos - a.q_offsets[qid]);
+            }
             n_steps += steps;
           }
           if (pass && members) append(a.mwork, a.mwork_count, a.mwork_cap, make_uint2(cid, k));
@@ -510,14 +512,15 @@ seed_kernel(SeedArgs a) {
         const uint32_t d = a.X.nc_values[a.L.nc_begin[l] + (j - nrep)];
         const uint8_t *dptr = a.db + d;
         for (uint32_t k = pb; k < pe; ++k) {
-          const uint32_t qid = a.L.entry_qid[k];
           const uint32_t cpos = a.L.entry_cpos[k];
           int steps = 0;
           ++n_seed;
           const uint32_t ct = a.L.entry_ct[k];
           if (walk_hit(a.q + cpos, dptr, tbl, (int)(ct >> 16), (int)(int16_t)(ct & 0xffffu),
-                       &steps))
+                       &steps)) {
+            const uint32_t qid = a.L.entry_qid[k];  // only a hit needs its query
             emit_hit(a, qid, d, cpos - a.q_offsets[qid]);
+          }
           n_steps += steps;
         }
       }
