@@ -25,10 +25,10 @@
 //  * every call shares the array, and it keeps the last call's contents:
 //    calls that overlap on the GPU (from several host threads or streams at
 //    once) race with each other and must be serialised by the caller;
-//  * every call ends by copying a counter to host memory and synchronising
-//    `stream`, so the entry point cannot run inside a stream capture at all;
-//    the first call on a device also looks up the array's device address
-//    (cudaGetSymbolAddress) once.
+//  * the first call on a device looks up the array's device address
+//    (cudaGetSymbolAddress) once for that device, so it should come before
+//    any stream capture; every call ends by copying a counter to host memory
+//    and synchronising `stream`.
 #include <cuda_runtime.h>
 
 #include <cstdint>

@@ -203,8 +203,10 @@ int gzb_gapped_extender_cells(gzb_gapped_extender *h, uint64_t *cells);
  * and score buffers then undefined, so a caller that wants to retry keeps
  * its own copy of the input positions).  Every call shares that array:
  * calls that overlap on the GPU race and must be serialised by the caller.
- * Every call ends by reading a counter into host memory and synchronising
- * `stream`, so it cannot be used inside a stream capture. */
+ * The first call on a device looks up the array's device address (a
+ * one-time set-up per device), so make that first call before any stream
+ * capture.  Every call ends by reading a counter into host memory and
+ * synchronising `stream`. */
 int gzb_gapped_extend_one_side_score_only_noalloc(
     const uint8_t *d_query_sequence, const uint8_t *d_database_sequence,
     uint8_t sequence_delimiter, const int32_t *d_score_matrix,
