@@ -776,7 +776,7 @@ chain_kernel(DevParams p, const uint8_t *__restrict__ q, const uint8_t *__restri
     const int cutoff = cutoffs[qi];
     uint64_t w = b;
     for (uint64_t i0 = b; i0 < e; i0 += 32) {
-      // this round's hits, one per lane (the compaction below only writes
+      // these 32 hits, one per lane (the compaction below only writes
       // positions before i0 + 32)
       const bool valid = i0 + lane < e;
       const uint64_t key = valid ? hits[i0 + lane] : 0;
