@@ -346,8 +346,9 @@ int gzb_engine_set_queries(gzb_engine *e, const uint8_t *codes,
                            const int32_t *gapped_triggers, void *stream);
 /* Query preparation and gzb_engine_set_queries in one call, the prepared
  * codes never leaving the device: protein queries in the engine layout
- * (host codes; a letter the reference's SEG does not count, lower case,
- * passed as its code + 32) are uploaded, SEG-masked in place when filter is
+ * (host codes; with the filter, a letter the reference's SEG does not
+ * count, lower case, passed as its code + 32; without it, plain codes below
+ * 32) are uploaded, SEG-masked in place when filter is
  * non-zero (gzb_seg_protein_queries; a protein shorter than SEG's window
  * keeps a zero-filled body and the statistics of ProteinQuery's buffer),
  * given their cutoffs by gzb_query_karlin_cutoffs with the engine's score
