@@ -444,8 +444,10 @@ constexpr int kSeedBlock = 256;
 constexpr int kUnitsPerWarp = 256;
 
 // One unit = one representative or one residual database position of a list,
-// tried against every query position of that list.
-__global__ void __launch_bounds__(kSeedBlock, 5)
+// tried against every query position of that list.  Bounded to six blocks
+// per SM (40 registers, a few spilled): the walks' global loads want the
+// warps more than the registers.
+__global__ void __launch_bounds__(kSeedBlock, 6)
 seed_kernel(SeedArgs a) {
   __shared__ __align__(16) int32_t tbl32[kWalkTableBytes / 4];
   load_walk_table(tbl32, a.matrix32, a.p.delimiter);
@@ -537,8 +539,8 @@ seed_kernel(SeedArgs a) {
 // together, scans their member counts, and deals the (item, member) seeds
 // to its lanes 32 at a time: a lane finds its item with a five-step shuffle
 // search over the scan, so a seed costs one load (the member's position)
-// besides its walk.
-__global__ void __launch_bounds__(kSeedBlock, 5)
+// besides its walk.  Six blocks per SM, as seed_kernel.
+__global__ void __launch_bounds__(kSeedBlock, 6)
 member_kernel(SeedArgs a, const uint2 *__restrict__ mwork, uint64_t n_work,
               const uint64_t *n_dev) {
   __shared__ __align__(16) int32_t tbl32[kWalkTableBytes / 4];
