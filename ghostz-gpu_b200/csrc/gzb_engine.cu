@@ -459,7 +459,9 @@ seed_kernel(SeedArgs a) {
   const uint64_t U = a.units_dev ? *a.units_dev : a.L.n_units;
   const int thr = a.p.distance_threshold;
   const int maxmd = a.p.max_member_distance;
-  unsigned long long n_dist = 0, n_seed = 0, n_steps = 0;
+  // a thread's counts stay far below 2^32 (about 4 s of its own walking);
+  // 32-bit counters leave the six-block register budget for the walk
+  uint32_t n_dist = 0, n_seed = 0, n_steps = 0;
   for (uint64_t base = warp * kUnitsPerWarp; base < U; base += nwarps * kUnitsPerWarp) {
     const uint64_t last = min(base + kUnitsPerWarp, U) - 1;
     // list range of this warp's units
@@ -551,7 +553,7 @@ member_kernel(SeedArgs a, const uint2 *__restrict__ mwork, uint64_t n_work,
   const int lane = threadIdx.x & 31;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  unsigned long long n_seed = 0, n_steps = 0;
+  uint32_t n_seed = 0, n_steps = 0;  // per thread, as in seed_kernel
   for (uint64_t i0 = warp * 32; i0 < n_work; i0 += nwarps * 32) {
     const uint64_t i = i0 + lane;
     uint32_t mb = 0, cnt = 0, qid = 0, cpos = 0, ct = 0;
