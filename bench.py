@@ -84,10 +84,10 @@ BYTES_PER_DISTANCE_SEED = 8 + 2 * 10 + 1
 # DRAM traffic of the seed-search kernels (seed_kernel + member_kernel, read +
 # write) per algorithmic byte, from one ncu capture on the 1,000-query x
 # 1,000,000-protein case, whose chunk is larger than L2
-# (profiles/seed_kernels_dram_protein-1k-x-1M.md: 8.424 GB of DRAM traffic
+# (profiles/seed_kernels_dram_protein-1k-x-1M.md: 8.228 GB of DRAM traffic
 # for 6.321 GB of algorithmic bytes); the bench scales it by each run's own
 # algorithmic bytes
-SEED_KERNEL_TRAFFIC_PER_BYTE = 8.424e9 / 6.321e9
+SEED_KERNEL_TRAFFIC_PER_BYTE = 8.228e9 / 6.321e9
 # B200 integer throughput for the DP roofline: 148 SMs x 128 INT32 lanes per
 # clock (nominal; no measured integer peak exists), at the sampled SM clock
 B200_SMS, INT32_LANES_PER_SM = 148, 128
@@ -1266,7 +1266,7 @@ def main():
                 "ungapped X-drop)", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved / hbm_peak, "traffic": traffic,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
-                                  "seed_kernel + member_kernel on protein-1k-x-1M (1.333 B "
+                                  "seed_kernel + member_kernel on protein-1k-x-1M (1.302 B "
                                   "per algorithmic byte), scaled by this run's algorithmic "
                                   "bytes",
                 "algorithmic_bytes": seed_bytes, "kernel_ms": st["seed_kernels"],
