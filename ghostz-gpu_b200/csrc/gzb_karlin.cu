@@ -161,9 +161,11 @@ __device__ double entropy(const double *sp, int lo, int hi, double lambda) {
 }
 
 // kIter: rounds of the K series the buffers hold.  kRetry: the second pass
-// (only queries whose cutoff holds kPending).
+// (only queries whose cutoff holds kPending).  The first pass runs eight
+// blocks per SM (its grid), so it is bounded to the 64 registers that let
+// all eight stay resident at once.
 template <int kWarps, int kIter, bool kRetry>
-__global__ void __launch_bounds__(kWarps * 32)
+__global__ void __launch_bounds__(kWarps * 32, kRetry ? 1 : 8)
     karlin_kernel(KarlinArgs a, const uint8_t *__restrict__ codes,
                   const uint64_t *__restrict__ offsets, const uint32_t *__restrict__ lengths,
                   uint32_t n, int32_t *__restrict__ cutoffs, int32_t *__restrict__ triggers,
