@@ -604,10 +604,15 @@ int launch_seg(uint8_t *codes, const uint64_t *offsets, const uint32_t *lengths,
   const int cache = mode == 0 ? kSegCacheFrames : kSegCacheProteins;
   const int block = mode == 0 ? 128 : 64;
   const uint64_t want2 = (units + block / 32 - 1) / (block / 32);
-  const uint64_t most2 = (uint64_t)sms * (mode == 0 ? 8 : 16);
   const size_t cache_bytes = sizeof(double) * (block / 32) * cache;
   GZB_CUDA(cudaFuncSetAttribute(seg_search_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)cache_bytes));
+  // the warps stride over the sequences, so the grid is what stays resident
+  // at once (the caches' shared memory bounds it): one wave, no tail
+  int per_sm = 1;
+  GZB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, seg_search_kernel, block,
+                                                         cache_bytes));
+  const uint64_t most2 = (uint64_t)sms * (per_sm > 0 ? per_sm : 1);
   seg_search_kernel<<<(uint32_t)(want2 < most2 ? want2 : most2), block, cache_bytes, stream>>>(
       g_args, codes, offsets, lengths, units, mode, status, cache);
   GZB_CUDA(cudaGetLastError());
