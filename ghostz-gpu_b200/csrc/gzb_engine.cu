@@ -459,8 +459,9 @@ seed_kernel(SeedArgs a) {
   const uint64_t U = a.units_dev ? *a.units_dev : a.L.n_units;
   const int thr = a.p.distance_threshold;
   const int maxmd = a.p.max_member_distance;
-  // a thread's counts stay far below 2^32 (about 4 s of its own walking);
-  // 32-bit counters leave the six-block register budget for the walk
+  // a thread's counts stay far below 2^32 (that many walk steps would take
+  // one thread seconds); 32-bit counters leave the six-block register
+  // budget to the walk
   uint32_t n_dist = 0, n_seed = 0, n_steps = 0;
   for (uint64_t base = warp * kUnitsPerWarp; base < U; base += nwarps * kUnitsPerWarp) {
     const uint64_t last = min(base + kUnitsPerWarp, U) - 1;
