@@ -10,6 +10,10 @@ step).  Its time is taken as t(R) = a + b R over the slices' residues R (a:
 per-query work that does not depend on the database -- reading, SEG,
 statistics, query lists; b: the search), and the whole database's time is
 read off that line: t_full = t1 + (t2 - t1) (R_full - R1) / (R2 - R1).
+The slices are the first 40,000 and 160,000 sequences: the search's time
+per residue falls as the database grows, so a line through smaller slices
+(20,000 and 40,000) over-estimated the whole database's time, and its
+short difference t2 - t1 made the estimate noisy.
 
 The parity check runs the reference's GPU aligner (`ghostz-gpu aln -g 1`,
 its host code on CPU stand-in operators) on the first slice.
@@ -37,7 +41,7 @@ class ReferenceSlices:
     for the parity check), written as the reference's FASTA inputs and
     databases under a scratch directory."""
 
-    def __init__(self, db, query_sequences, slices=(20_000, 40_000), threads=None,
+    def __init__(self, db, query_sequences, slices=(40_000, 160_000), threads=None,
                  clustering=True):
         self.dir = tempfile.mkdtemp(prefix="gz_ref_")
         self.threads = threads or os.cpu_count() or 1
